@@ -1,0 +1,211 @@
+/*
+ * quoin — C ABI of the B200-native quoin library (libquoin_b200.so).
+ *
+ * Lossless compressor for typed numeric columns.  The first part of this header
+ * is the reference C ABI, symbol for symbol, with the same codes, ownership
+ * and buffer rules; the second part adds the B200-specific entry points
+ * (typed column with a level/block-size knob, device-resident buffers and CUDA
+ * streams, a reusable decode index and the per-mode win counters).
+ *
+ * Each declaration cites the reference interface it replaces
+ * (capi/include/quoin.h, capi/src/lib.rs, capi/src/typed.rs, src/lib.rs).
+ *
+ * Differences from the reference, by design:
+ *  - compression runs on the GPU (sm_100a); the competition pool covers
+ *    Level::Fastest and Level::Fast, whose streams are byte-identical to the
+ *    reference encoder's.  The reference symbols compress at Level::Fast
+ *    (the reference default, Level::Max, needs Pco, Lz, the range coder and
+ *    the FCM/DFCM predictors, which are outside this library);
+ *  - decompression accepts every stream whose block modes and entropy tags
+ *    are in the covered pool; blocks outside it return QUOIN_ERR_CORRUPT
+ *    (reference symbols) or QUOIN_ERR_UNSUPPORTED (extended symbols).
+ *  - a "context" owns a CUDA stream and device arenas instead of a thread pool.
+ *
+ * Threading: every call is synchronous with respect to the caller's buffers.
+ * Not async-signal-safe; do not fork after first use.
+ */
+#ifndef QUOIN_H
+#define QUOIN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return / error codes (capi/include/quoin.h:28-33). */
+#define QUOIN_OK                    0
+#define QUOIN_ERR_NULL             (-1) /* a required pointer argument was NULL  */
+#define QUOIN_ERR_BUFFER_TOO_SMALL (-2) /* dst too small; needed size in out_*   */
+#define QUOIN_ERR_CORRUPT          (-3) /* malformed / truncated input stream    */
+#define QUOIN_ERR_PANIC            (-4) /* internal error caught at the boundary  */
+
+/* Extended codes, returned only by the quoin_b200_* symbols (the error kinds
+ * of src/error.rs:5-25, plus device and scope errors). */
+#define QUOIN_ERR_BAD_MAGIC           (-10)
+#define QUOIN_ERR_UNSUPPORTED_VERSION (-11)
+#define QUOIN_ERR_TRUNCATED           (-12)
+#define QUOIN_ERR_UNKNOWN_MODE        (-13)
+#define QUOIN_ERR_CORRUPT_PAYLOAD     (-14)
+#define QUOIN_ERR_LENGTH_MISMATCH     (-15)
+#define QUOIN_ERR_UNSUPPORTED_DTYPE   (-16)
+#define QUOIN_ERR_DTYPE_MISMATCH      (-17)
+#define QUOIN_ERR_UNSUPPORTED         (-18) /* mode / entropy tag / level outside the pool */
+#define QUOIN_ERR_CUDA                (-19) /* a CUDA call failed (no device, OOM, ...)   */
+#define QUOIN_ERR_BAD_ARG             (-20)
+
+/* ---------------- reference ABI (capi/include/quoin.h:35-142) ---------------- */
+
+/* capi/include/quoin.h:36 — NUL-terminated version string (static). */
+const char *quoin_version(void);
+
+/* capi/include/quoin.h:39, capi/src/lib.rs:39-41 — 9n + 1024. */
+size_t quoin_compress_bound(size_t n_values);
+
+/* capi/include/quoin.h:47-48, capi/src/lib.rs:117-125 (Level::Fast on the GPU). */
+int quoin_compress(const double *src, size_t n_values,
+                   uint8_t *dst, size_t dst_cap, size_t *out_len);
+
+/* capi/include/quoin.h:56-57, capi/src/lib.rs:132-140. */
+int quoin_decompress(const uint8_t *src, size_t src_len,
+                     double *dst, size_t dst_cap_values, size_t *out_values);
+
+/* capi/include/quoin.h:64, capi/src/lib.rs:145-158. */
+ptrdiff_t quoin_decompressed_value_count(const uint8_t *src, size_t src_len);
+
+/* capi/include/quoin.h:67-81, capi/src/lib.rs:161-224.  A context owns a CUDA
+ * stream and device/pinned arenas; `threads` selects nothing on the GPU and is
+ * kept for source compatibility.  NULL ctx = the lazily created default. */
+typedef struct QuoinCtx QuoinCtx;
+QuoinCtx *quoin_ctx_create(size_t threads);
+void quoin_ctx_free(QuoinCtx *ctx);
+int quoin_compress_ctx(const QuoinCtx *ctx, const double *src, size_t n_values,
+                       uint8_t *dst, size_t dst_cap, size_t *out_len);
+int quoin_decompress_ctx(const QuoinCtx *ctx, const uint8_t *src, size_t src_len,
+                         double *dst, size_t dst_cap_values, size_t *out_values);
+
+/* Arrow-native dtype tags (capi/include/quoin.h:96-114). */
+typedef enum {
+    QUOIN_DTYPE_BOOL = 0,
+    QUOIN_DTYPE_I8   = 1,
+    QUOIN_DTYPE_I16  = 2,
+    QUOIN_DTYPE_I32  = 3,
+    QUOIN_DTYPE_I64  = 4,
+    QUOIN_DTYPE_U8   = 5,
+    QUOIN_DTYPE_U16  = 6,
+    QUOIN_DTYPE_U32  = 7,
+    QUOIN_DTYPE_U64  = 8,
+    QUOIN_DTYPE_F32  = 9,
+    QUOIN_DTYPE_F64  = 10,
+    QUOIN_DTYPE_DECIMAL32  = 11,
+    QUOIN_DTYPE_DECIMAL64  = 12,
+    QUOIN_DTYPE_DECIMAL128 = 13,
+    QUOIN_DTYPE_DECIMAL256 = 14
+} QuoinDType;
+
+/* capi/include/quoin.h:118, capi/src/typed.rs:50-61. */
+size_t quoin_dtype_width(int32_t dtype);
+/* capi/include/quoin.h:121, capi/src/typed.rs:65-69 — n*(max(w,8)+1)+1024. */
+size_t quoin_typed_compress_bound(int32_t dtype, size_t n);
+/* capi/include/quoin.h:126-127, capi/src/typed.rs:125-174 — bytes, 0 on failure. */
+size_t quoin_typed_compress(int32_t dtype, size_t n, const void *values,
+                            const uint8_t *validity, uint8_t *dst, size_t dst_cap);
+/* capi/include/quoin.h:133-135, capi/src/typed.rs:183-227. */
+size_t quoin_typed_compress_decimal(int32_t dtype, size_t n, const void *values,
+                                    const uint8_t *validity, int8_t scale,
+                                    uint8_t precision, uint8_t *dst, size_t dst_cap);
+/* capi/include/quoin.h:141-142, capi/src/typed.rs:311-338. */
+int quoin_typed_decompress(int32_t dtype, size_t n, const uint8_t *src,
+                           size_t src_len, void *values_out, uint8_t *validity_out);
+
+/* ---------------- B200 extensions ---------------- */
+
+/* Speed/ratio levels (src/lib.rs:93-119).  The GPU competition covers
+ * FASTEST and FAST; higher levels return QUOIN_ERR_UNSUPPORTED. */
+#define QUOIN_LEVEL_FASTEST  0
+#define QUOIN_LEVEL_FAST     1
+#define QUOIN_LEVEL_BALANCED 2
+#define QUOIN_LEVEL_HIGH     3
+#define QUOIN_LEVEL_MAX      4
+
+/* Stream dtype wire ids (src/dtype.rs:68-78). */
+#define QUOIN_WIRE_F64 0
+#define QUOIN_WIRE_I64 1
+#define QUOIN_WIRE_U64 2
+#define QUOIN_WIRE_I32 3
+#define QUOIN_WIRE_U32 4
+#define QUOIN_WIRE_F32 5
+#define QUOIN_WIRE_DECIMAL128 6
+#define QUOIN_WIRE_DECIMAL256 7
+
+/* Encoder configuration (src/lib.rs:195-245): predictor_log2 (clamped 10..16,
+ * recorded in the header), level, block_size (0 = adaptive; else clamped to
+ * [1, 131072]). */
+typedef struct {
+    int32_t level;
+    int64_t block_size;
+    int32_t predictor_log2;
+} QuoinConfig;
+
+/* Replaces compress_column(ColumnRef, Option<&[u8]>, Config) (src/lib.rs:429-455)
+ * for host buffers: `values` holds n values of the wire dtype's native width
+ * (8 B f64/i64/u64, 4 B i32/u32/f32, 16 B Decimal128, 32 B Decimal256,
+ * little-endian), `validity` an Arrow bitmap or NULL; scale/precision are used
+ * by the decimal dtypes.  Writes the stream to dst and its length to *out_len
+ * (the needed size with QUOIN_ERR_BUFFER_TOO_SMALL). */
+int quoin_b200_compress_column(QuoinCtx *ctx, int32_t wire_dtype, size_t n, const void *values,
+                               const uint8_t *validity, int8_t scale, uint8_t precision,
+                               const QuoinConfig *cfg, uint8_t *dst, size_t dst_cap,
+                               size_t *out_len);
+
+/* Header of a stream (src/format.rs:65-94, src/decimal.rs:100-168): wire
+ * dtype, logical n, validity flag, decimal scale/precision (0 otherwise). */
+int quoin_b200_stream_info(const uint8_t *src, size_t src_len, int32_t *wire_dtype,
+                           uint64_t *n, int32_t *has_validity, int8_t *scale,
+                           uint8_t *precision);
+
+/* Replaces decompress_column(&[u8]) (src/lib.rs:462-508) for host buffers:
+ * writes n native values to values_out (null slots 0) and, when the stream has
+ * a validity bitmap and validity_out is non-NULL, ceil(n/8) bitmap bytes. */
+int quoin_b200_decompress_column(QuoinCtx *ctx, const uint8_t *src, size_t src_len,
+                                 void *values_out, uint8_t *validity_out);
+
+/* Device-resident variants: every pointer is device memory on the context's
+ * device; `stream` is a cudaStream_t (NULL = the context's own stream).  The
+ * call returns after the work on `stream` has completed. */
+int quoin_b200_compress_column_device(QuoinCtx *ctx, int32_t wire_dtype, size_t n,
+                                      const void *d_values, const uint8_t *d_validity,
+                                      int8_t scale, uint8_t precision, const QuoinConfig *cfg,
+                                      uint8_t *d_dst, size_t dst_cap, size_t *out_len,
+                                      void *stream);
+
+/* A decode index: the header, validity and frame table of a stream, parsed
+ * and validated once on the host (src/decoder.rs:43-94) and kept resident on
+ * the device so the stream can be decoded again without re-walking it. */
+typedef struct QuoinDecodeIndex QuoinDecodeIndex;
+int quoin_b200_index_create(QuoinCtx *ctx, const uint8_t *src, size_t src_len,
+                            QuoinDecodeIndex **out);
+void quoin_b200_index_free(QuoinDecodeIndex *idx);
+/* n and wire dtype of an indexed stream. */
+int quoin_b200_index_info(const QuoinDecodeIndex *idx, int32_t *wire_dtype, uint64_t *n,
+                          int32_t *has_validity);
+/* Decode the device copy d_src of the indexed stream into d_values_out (and
+ * d_validity_out when non-NULL and the stream has a bitmap). */
+int quoin_b200_decompress_indexed_device(QuoinCtx *ctx, const QuoinDecodeIndex *idx,
+                                         const uint8_t *d_src, void *d_values_out,
+                                         uint8_t *d_validity_out, void *stream);
+
+/* Per-mode win counts of the GPU competition since the last reset, indexed by
+ * mode id (src/lib.rs:540-547, src/diag.rs). */
+void quoin_b200_mode_win_counts(uint64_t out[64]);
+void quoin_b200_reset_mode_win_counts(void);
+
+/* Number of GPU kernels this library has launched in the calling process. */
+uint64_t quoin_b200_kernel_launches(void);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* QUOIN_H */

@@ -1,0 +1,1631 @@
+// Block planner, per-block codec competition and winner emission
+// (reference src/encoder.rs:154-469,644-759 and the encode functions of the
+// in-path codecs).  One CTA per block.  The competition never materialises a
+// candidate payload: every candidate's exact byte length is computed in closed
+// form from warp-reduced statistics (sub-block widths, exception counts,
+// distinct/run counts, ALP (e,f) search, ALP-RD cut search), the argmin of
+// `len + penalty` is taken in the reference's candidate order with a strict
+// `<`, and only the winner is written by k_emit.
+#include "qb_common.cuh"
+#include "qb_layout.h"
+#include "qb_kernels.h"
+
+namespace qb {
+
+constexpr int kEncThreads = 256;
+constexpr int kEncWarps = kEncThreads / 32;
+constexpr int kSubsMax = kMaxBlock / kSub;  // 128
+constexpr uint32_t kHashCap = 2048;         // smem hash slots (dict / ALP-RD left parts)
+constexpr uint32_t kHashLimit = 1536;       // distinct keys before falling back to scratch
+constexpr uint32_t kLbBits = 1u << 17;      // dict cardinality lower-bound bitset
+constexpr uint32_t kRunsSmem = 4096;
+constexpr uint64_t kEmpty64 = ~0ull;
+constexpr uint32_t kEmpty32 = 0xFFFFFFFFu;
+
+__device__ unsigned long long g_wins[64];  // reference src/diag.rs:8-23
+
+// Candidate decode weights (reference encoder.rs:79-89).
+__host__ __device__ inline uint64_t decode_weight(int m) {
+  switch (m) {
+    case M_RAW: case M_CONST: case M_STRIDE: return 0;
+    case M_XORZ: case M_FOR_BITPACK: case M_DELTA_BITPACK: case M_RLE: return 1;
+    case M_ALP: case M_ALP_RD: case M_DICT: return 2;
+    case M_PRED: return 3;
+    case M_BYTE_TRANSPOSE: case M_FLOAT_MULT: return 6;
+    case M_PRED_RC: case M_PRED2: return 10;
+    default: return 7;
+  }
+}
+__host__ __device__ inline uint64_t level_lambda(int level) {  // reference lib.rs:126-138
+  return level == 0 ? 16 : level == 1 ? 4 : level == 2 ? 2 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Small device utilities
+// ---------------------------------------------------------------------------
+__device__ inline void put_u8(uint8_t* d, uint32_t v) { *d = (uint8_t)v; }
+__device__ inline void put_u16(uint8_t* d, uint32_t v) { d[0] = (uint8_t)v; d[1] = (uint8_t)(v >> 8); }
+__device__ inline void put_u32(uint8_t* d, uint32_t v) {
+#pragma unroll
+  for (int i = 0; i < 4; i++) d[i] = (uint8_t)(v >> (8 * i));
+}
+__device__ inline void put_u64(uint8_t* d, uint64_t v) {
+#pragma unroll
+  for (int i = 0; i < 8; i++) d[i] = (uint8_t)(v >> (8 * i));
+}
+__device__ inline uint32_t put_varint(uint8_t* d, uint64_t v) {
+  uint32_t n = 0;
+  for (;;) {
+    uint8_t b = (uint8_t)(v & 0x7f);
+    v >>= 7;
+    if (v) { d[n++] = b | 0x80; } else { d[n++] = b; return n; }
+  }
+}
+__device__ inline uint64_t u64min(uint64_t a, uint64_t b) { return a < b ? a : b; }
+__device__ inline uint64_t u64max(uint64_t a, uint64_t b) { return a > b ? a : b; }
+__device__ inline uint32_t warp_or(uint32_t v) {
+  for (int o = 16; o; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ inline int64_t warp_min_i64(int64_t v) {
+  for (int o = 16; o; o >>= 1) { int64_t u = __shfl_xor_sync(0xffffffffu, v, o); v = u < v ? u : v; }
+  return v;
+}
+__device__ inline int64_t warp_max_i64(int64_t v) {
+  for (int o = 16; o; o >>= 1) { int64_t u = __shfl_xor_sync(0xffffffffu, v, o); v = u > v ? u : v; }
+  return v;
+}
+__device__ inline uint32_t pow2_at_least(uint32_t x) {
+  uint32_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+__device__ inline void atomic_min_u64(unsigned long long* a, uint64_t v) { atomicMin(a, (unsigned long long)v); }
+__device__ inline void atomic_max_u64(unsigned long long* a, uint64_t v) { atomicMax(a, (unsigned long long)v); }
+
+// In-place ascending bitonic sort of P (power of two) keys; all threads.
+__device__ void block_bitonic_sort(uint64_t* a, uint32_t P) {
+  for (uint32_t k = 2; k <= P; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+        uint32_t ixj = i ^ j;
+        if (ixj > i) {
+          uint64_t x = a[i], y = a[ixj];
+          bool up = (i & k) == 0;
+          if ((x > y) == up) { a[i] = y; a[ixj] = x; }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// (e, f) of the c-th pair in the reference's search order (alp.rs:61-62).
+__device__ inline void alp_combo(uint32_t c, int* e, int* f) {
+  int ee = 0;
+  while ((uint32_t)((ee + 1) * (ee + 2) / 2) <= c) ee++;
+  *e = ee;
+  *f = (int)(c - (uint32_t)(ee * (ee + 1) / 2));
+}
+
+// FLOAT_MULT scale test (reference codecs/float_mult.rs:45-64): bit s set in
+// the result when value x does NOT round-trip exactly through scale s.
+__device__ inline uint32_t fm_fail_bits(uint64_t x, uint32_t alive) {
+  uint32_t fail = 0;
+  double xd = as_f64(x);
+  while (alive) {
+    int s = __ffs(alive) - 1;
+    alive &= alive - 1;
+    double sc = kFmScales[s];
+    double k = round_half_away(__dmul_rn(xd, sc));
+    bool ok = is_finite_f64(k) && fabs(k) < 9.0e18 && f64_bits(__ddiv_rn(k, sc)) == x;
+    if (!ok) fail |= 1u << s;
+  }
+  return fail;
+}
+__device__ inline int64_t fm_k(uint64_t x, int s) {
+  return __double2ll_rz(round_half_away(__dmul_rn(as_f64(x), kFmScales[s])));
+}
+
+// ---------------------------------------------------------------------------
+// Shared memory of the competition and emission kernels
+// ---------------------------------------------------------------------------
+struct RdArea {
+  uint64_t smp[4096];
+  uint32_t hkey[kHashCap];
+  uint32_t hcnt[kHashCap];
+};
+struct DictArea {
+  uint64_t hkey[kHashCap];
+  uint32_t hval[kHashCap];
+  uint64_t sorted[kHashCap];
+  uint32_t lb[kLbBits / 32];
+};
+struct RleArea {
+  uint32_t starts[kRunsSmem];
+};
+union BigArea {
+  RdArea rd;
+  DictArea dict;
+  RleArea rle;
+};
+
+struct EncSmem {
+  uint8_t w_a[kSubsMax];   // FoR widths (also ALP widths in emit)
+  uint8_t w_b[kSubsMax];   // delta / rights widths
+  uint8_t w_c[kSubsMax];   // ALP / codes widths
+  uint8_t w_d[kSubsMax];   // FLOAT_MULT widths
+  uint8_t alp_ef[kSubsMax][2];
+  uint16_t alp_exc[kSubsMax];
+  uint32_t neq_k[kSubsMax];
+  uint32_t subsz[kSubsMax + 1];
+  uint64_t submin[kSubsMax];
+  unsigned long long xor_bytes, umin, umax, e_vmin, e_vmax, e_dmax, acc64;
+  uint32_t neq, stride_bad, fm_mask, alp_fail, flag, ovf, card, has_max, max_rank, cnt32, dl;
+  uint32_t distinct_bits[512];
+  uint64_t alp_smp[kEncWarps][32];
+  double rd_pv[24];
+  uint64_t dict8[8];
+  uint64_t red[kEncWarps];
+  uint32_t red32[kEncWarps];
+  uint64_t sc[8];
+  BigArea big;
+};
+
+// ---------------------------------------------------------------------------
+// Warp-level FoR statistics of one sub-block: width of (max - min).
+// ---------------------------------------------------------------------------
+template <class V>
+__device__ inline void warp_minmax(uint32_t cnt, bool sgn, V val, uint64_t* mn_out, uint32_t* w_out) {
+  int lane = threadIdx.x & 31;
+  uint64_t umn = kEmpty64, umx = 0;
+  int64_t smn = INT64_MAX, smx = INT64_MIN;
+  for (uint32_t i = lane; i < cnt; i += 32) {
+    uint64_t x = val(i);
+    umn = u64min(umn, x);
+    umx = u64max(umx, x);
+    int64_t s = (int64_t)x;
+    smn = s < smn ? s : smn;
+    smx = s > smx ? s : smx;
+  }
+  if (sgn) {
+    smn = warp_min_i64(smn);
+    smx = warp_max_i64(smx);
+    *mn_out = (uint64_t)smn;
+    *w_out = bit_width64((uint64_t)smx - (uint64_t)smn);
+  } else {
+    umn = warp_min(umn);
+    umx = warp_max(umx);
+    *mn_out = umn;
+    *w_out = bit_width64(umx - umn);
+  }
+}
+
+// Pack one FoR sub-block (header + FastLanes words) at dst; residual of
+// index i = val(i) - mn for i < cnt, 0 for the padding (reference
+// for_bitpack.rs:47-96, bitpack.rs:48-133).
+template <class V>
+__device__ inline void warp_for_pack(uint8_t* dst, uint32_t cnt, uint64_t mn, uint32_t w, V val) {
+  int lane = threadIdx.x & 31;
+  if (lane == 0) {
+    put_u8(dst, w);
+    put_u64(dst + 1, mn);
+  }
+  if (w == 0) return;
+  uint8_t* words = dst + 9;
+  if (w <= 32) {
+    uint64_t acc = 0;
+    uint32_t nb = 0, wd = 0;
+    for (uint32_t r = 0; r < 32; r++) {
+      uint32_t i = r * 32 + lane;
+      uint32_t res = i < cnt ? (uint32_t)(val(i) - mn) : 0u;
+      if (w < 32) res &= (1u << w) - 1u;
+      acc |= (uint64_t)res << nb;
+      nb += w;
+      if (nb >= 32) {
+        put_u32(words + 4u * (wd * 32u + lane), (uint32_t)acc);
+        wd++;
+        acc >>= 32;
+        nb -= 32;
+      }
+    }
+  } else if (lane < 16) {
+    unsigned __int128 acc = 0;
+    uint32_t nb = 0, wd = 0;
+    for (uint32_t r = 0; r < 64; r++) {
+      uint32_t i = r * 16 + lane;
+      uint64_t res = i < cnt ? (val(i) - mn) : 0ull;
+      if (w < 64) res &= (1ull << w) - 1ull;
+      acc |= (unsigned __int128)res << nb;
+      nb += w;
+      if (nb >= 64) {
+        put_u64(words + 8u * (wd * 16u + lane), (uint64_t)acc);
+        wd++;
+        acc >>= 64;
+        nb -= 64;
+      }
+    }
+  }
+}
+
+// Whole-CTA FoR stream writer: varint(M) + sub-blocks of val(0..M).  When
+// dst is null only the size is computed.  Returns the byte length (all threads).
+template <class V>
+__device__ uint64_t block_for(EncSmem& S, uint8_t* dst, uint32_t M, bool sgn, V val) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nsub = (M + kSub - 1) / kSub;
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t cnt = min((uint32_t)kSub, M - k * kSub);
+    uint64_t mn;
+    uint32_t w;
+    warp_minmax(cnt, sgn, [&](uint32_t i) { return val(k * kSub + i); }, &mn, &w);
+    if (lane == 0) {
+      S.w_a[k] = (uint8_t)w;
+      S.submin[k] = mn;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t off = varint_len(M);
+    for (uint32_t k = 0; k < nsub; k++) {
+      S.subsz[k] = off;
+      off += 9 + 128u * S.w_a[k];
+    }
+    S.subsz[nsub] = off;
+    if (dst) put_varint(dst, M);
+  }
+  __syncthreads();
+  uint64_t total = S.subsz[nsub];
+  if (dst) {
+    for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+      uint32_t cnt = min((uint32_t)kSub, M - k * kSub);
+      warp_for_pack(dst + S.subsz[k], cnt, S.submin[k], S.w_a[k], [&](uint32_t i) { return val(k * kSub + i); });
+    }
+  }
+  __syncthreads();
+  return total;
+}
+
+// ---------------------------------------------------------------------------
+// Block features (reference encoder.rs:705-750) and the integer early-out
+// (encoder.rs:655-683).  Requires S.neq from the stats pass.
+// ---------------------------------------------------------------------------
+__device__ void sample_features(EncSmem& S, const uint64_t* v, uint32_t n) {
+  for (uint32_t i = threadIdx.x; i < 512; i += blockDim.x) S.distinct_bits[i] = 0;
+  if (threadIdx.x == 0) {
+    S.e_vmin = v[0];
+    S.e_vmax = v[0];
+    S.e_dmax = 0;
+  }
+  __syncthreads();
+  uint32_t dstride = max(n / 4096u, 1u);
+  for (uint32_t i = threadIdx.x; (uint64_t)i * dstride < n; i += blockDim.x) {
+    uint64_t h = v[(uint64_t)i * dstride] * 0x9E3779B97F4A7C15ull;
+    uint32_t b = (uint32_t)((h >> 50) & 0x3FFF);
+    atomicOr(&S.distinct_bits[b >> 5], 1u << (b & 31));
+  }
+  uint32_t estep = max(n / 2048u, 1u);
+  for (uint32_t i = threadIdx.x; (uint64_t)i * estep < n; i += blockDim.x) {
+    uint32_t idx = i * estep;
+    uint64_t x = v[idx];
+    atomic_min_u64(&S.e_vmin, x);
+    atomic_max_u64(&S.e_vmax, x);
+    if (idx >= estep) atomic_max_u64(&S.e_dmax, zigzag64(x - v[idx - 1]));
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Stats pass: one warp per 1024-value sub-block.
+// ---------------------------------------------------------------------------
+__device__ void stats_pass(EncSmem& S, const uint64_t* v, uint32_t n, int dtype, bool do_fm) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nsub = (n + kSub - 1) / kSub;
+  uint64_t v0 = v[0], stride = n > 1 ? v[1] - v[0] : 0;
+  bool sgn = dtype_signed(dtype);
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+    uint64_t carry = base ? v[base - 1] : v0;
+    uint64_t umn = kEmpty64, umx = 0, dzmn = kEmpty64, dzmx = 0, xb = 0;
+    int64_t smn = INT64_MAX, smx = INT64_MIN;
+    uint32_t nq = 0, sbad = 0, fmfail = 0;
+    uint32_t alive = do_fm ? *(volatile uint32_t*)&S.fm_mask : 0u;
+#pragma unroll 4
+    for (uint32_t j = 0; j < 32; j++) {
+      uint32_t li = j * 32 + lane;
+      bool ok = li < cnt;
+      uint32_t idx = base + li;
+      uint64_t x = ok ? v[idx] : 0;
+      uint64_t up = __shfl_up_sync(0xffffffffu, x, 1);
+      uint64_t pv = lane ? up : carry;
+      carry = __shfl_sync(0xffffffffu, x, 31);
+      if (ok) {
+        umn = u64min(umn, x);
+        umx = u64max(umx, x);
+        int64_t sx = (int64_t)x;
+        smn = sx < smn ? sx : smn;
+        smx = sx > smx ? sx : smx;
+        uint64_t dz = zigzag64(x - (idx ? pv : x));
+        dzmn = u64min(dzmn, dz);
+        dzmx = u64max(dzmx, dz);
+        xb += varint_len(x ^ (idx ? pv : 0ull));
+        nq += (idx && x != pv) ? 1u : 0u;
+        sbad |= (x != v0 + (uint64_t)idx * stride) ? 1u : 0u;
+        if (alive) fmfail |= fm_fail_bits(x, alive);
+      }
+      if (do_fm && (j & 7) == 7) {
+        uint32_t f = warp_or(fmfail);
+        if (f && lane == 0) atomicAnd(&S.fm_mask, ~f);
+        alive = *(volatile uint32_t*)&S.fm_mask & ~f;
+        fmfail = 0;
+      }
+    }
+    umn = warp_min(umn);
+    umx = warp_max(umx);
+    smn = warp_min_i64(smn);
+    smx = warp_max_i64(smx);
+    dzmn = warp_min(dzmn);
+    dzmx = warp_max(dzmx);
+    xb = warp_sum(xb);
+    nq = warp_sum(nq);
+    sbad = warp_or(sbad);
+    if (lane == 0) {
+      S.w_a[k] = (uint8_t)(sgn ? bit_width64((uint64_t)smx - (uint64_t)smn) : bit_width64(umx - umn));
+      S.w_b[k] = (uint8_t)bit_width64(dzmx - dzmn);
+      S.neq_k[k] = nq;
+      atomicAdd(&S.xor_bytes, (unsigned long long)xb);
+      atomicAdd(&S.neq, nq);
+      atomicOr(&S.stride_bad, sbad);
+      atomic_min_u64(&S.umin, umn);
+      atomic_max_u64(&S.umax, umx);
+    }
+  }
+}
+
+// FLOAT_MULT k widths for the chosen scale (signed FoR of k).
+__device__ void fm_widths(EncSmem& S, const uint64_t* v, uint32_t n, int s) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nsub = (n + kSub - 1) / kSub;
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+    uint64_t mn;
+    uint32_t w;
+    warp_minmax(cnt, true, [&](uint32_t i) { return (uint64_t)fm_k(v[base + i], s); }, &mn, &w);
+    if (lane == 0) S.w_d[k] = (uint8_t)w;
+  }
+}
+
+// ALP for one sub-block (reference alp.rs:49-166): find_ef on the 32-value
+// sample, then the full encode statistics.  Warp-cooperative; returns false
+// when the sub-block (hence the block) bails.
+struct AlpSub {
+  int e, f;
+  uint32_t w, exc;
+  int64_t mn, filler;
+};
+__device__ bool alp_subblock(const uint64_t* sv, uint32_t cnt, uint64_t* smp, AlpSub* out) {
+  int lane = threadIdx.x & 31;
+  uint32_t st = max(cnt / 32u, 1u);
+  uint32_t sl = min(32u, (cnt + st - 1) / st);
+  smp[lane] = (uint32_t)lane < sl ? sv[lane * st] : 0ull;
+  __syncwarp();
+  uint64_t best_cost = kEmpty64;
+  uint32_t best_c = 0xFFFF, best_exc = 0;
+  for (uint32_t c = lane; c < 190; c += 32) {
+    int e, f;
+    alp_combo(c, &e, &f);
+    uint32_t ex = 0;
+    int64_t lo = INT64_MAX, hi = INT64_MIN;
+    for (uint32_t s = 0; s < sl; s++) {
+      int64_t d;
+      if (alp_roundtrips(smp[s], e, f, &d)) {
+        lo = d < lo ? d : lo;
+        hi = d > hi ? d : hi;
+      } else {
+        ex++;
+      }
+    }
+    uint32_t width = (ex == sl) ? 64u : (hi <= lo ? 0u : bit_width64((uint64_t)hi - (uint64_t)lo));
+    uint64_t cost = (uint64_t)width * sl + (uint64_t)ex * 80;
+    if (cost < best_cost) {
+      best_cost = cost;
+      best_c = c;
+      best_exc = ex;
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    uint64_t oc = __shfl_xor_sync(0xffffffffu, best_cost, o);
+    uint32_t occ = __shfl_xor_sync(0xffffffffu, best_c, o);
+    uint32_t oe = __shfl_xor_sync(0xffffffffu, best_exc, o);
+    if (oc < best_cost || (oc == best_cost && occ < best_c)) {
+      best_cost = oc;
+      best_c = occ;
+      best_exc = oe;
+    }
+  }
+  __syncwarp();
+  if (best_exc * 2 > sl) return false;
+  int e, f;
+  alp_combo(best_c, &e, &f);
+  uint32_t exc = 0, first_li = 0xFFFFFFFFu;
+  int64_t dmn = INT64_MAX, dmx = INT64_MIN, first_d = 0;
+  for (uint32_t j = 0; j < 32; j++) {
+    uint32_t li = j * 32 + lane;
+    bool ok = li < cnt;
+    int64_t d = 0;
+    bool rt = ok && alp_roundtrips(sv[li], e, f, &d);
+    if (rt) {
+      dmn = d < dmn ? d : dmn;
+      dmx = d > dmx ? d : dmx;
+      if (li < first_li) {
+        first_li = li;
+        first_d = d;
+      }
+    }
+    exc += __popc(__ballot_sync(0xffffffffu, ok && !rt));
+  }
+  dmn = warp_min_i64(dmn);
+  dmx = warp_max_i64(dmx);
+  for (int o = 16; o; o >>= 1) {
+    uint32_t ol = __shfl_xor_sync(0xffffffffu, first_li, o);
+    int64_t od = __shfl_xor_sync(0xffffffffu, first_d, o);
+    if (ol < first_li) {
+      first_li = ol;
+      first_d = od;
+    }
+  }
+  int64_t filler = first_li == 0xFFFFFFFFu ? 0 : first_d;
+  if (first_li == 0xFFFFFFFFu) dmn = dmx = 0;
+  uint32_t w = bit_width64((uint64_t)dmx - (uint64_t)dmn);
+  if (w > 32) return false;
+  out->e = e;
+  out->f = f;
+  out->w = w;
+  out->exc = exc;
+  out->mn = dmn;
+  out->filler = filler;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// ALP-RD: cut search on the sample (reference alp_rd.rs:80-107).  Uses the
+// sorted sample: for a cut, the equal-left groups are runs of the sorted
+// sample, and only the sum of the 8 largest group counts matters.
+// ---------------------------------------------------------------------------
+__device__ inline void top8_insert(uint32_t (&t)[8], uint32_t c) {
+  if (c <= t[7]) return;
+  t[7] = c;
+#pragma unroll
+  for (int i = 7; i > 0; i--) {
+    if (t[i] > t[i - 1]) {
+      uint32_t x = t[i];
+      t[i] = t[i - 1];
+      t[i - 1] = x;
+    }
+  }
+}
+__device__ inline uint32_t rd_code_bits(uint32_t dl) {
+  if (dl <= 1) return 1;
+  uint32_t b = bit_width64((uint64_t)(dl - 1));
+  return b ? b : 1;
+}
+
+// Returns the chosen left bit width, or 0 when ALP-RD does not apply.
+__device__ uint32_t rd_choose_cut(EncSmem& S, const uint64_t* v, uint32_t n) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t step = max(n / 2048u, 1u);
+  uint32_t sn = (n + step - 1) / step;
+  uint32_t P = pow2_at_least(sn);
+  uint64_t* smp = S.big.rd.smp;
+  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) smp[i] = i < sn ? v[(uint64_t)i * step] : kEmpty64;
+  __syncthreads();
+  block_bitonic_sort(smp, P);
+  for (uint32_t lbw = warp + 1; lbw <= 24; lbw += kEncWarps) {
+    uint32_t rbw = 64 - lbw;
+    uint32_t t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t last_start = 0, G = 0;
+    for (uint32_t base = 0; base < sn; base += 32) {
+      uint32_t i = base + lane;
+      bool ok = i < sn;
+      bool bnd = ok && (i == 0 || (smp[i] >> rbw) != (smp[i - 1] >> rbw));
+      uint32_t m = __ballot_sync(0xffffffffu, bnd);
+      G += __popc(m);
+      if (bnd && i > 0) {
+        uint32_t below = m & ((1u << lane) - 1u);
+        uint32_t ps = below ? base + (31 - __clz(below)) : last_start;
+        top8_insert(t, i - ps);
+      }
+      if (m) last_start = base + (31 - __clz(m));
+    }
+    if (lane == 0) top8_insert(t, sn - last_start);
+    uint64_t cov = 0;
+    for (int r = 0; r < 8; r++) {
+      uint32_t mx = warp_max(t[0]);
+      if (mx == 0) break;
+      uint32_t who = __ballot_sync(0xffffffffu, t[0] == mx);
+      if (lane == __ffs(who) - 1) {
+#pragma unroll
+        for (int i = 0; i < 7; i++) t[i] = t[i + 1];
+        t[7] = 0;
+      }
+      cov += mx;
+    }
+    uint32_t dl = min(G, 8u);
+    uint64_t num = (uint64_t)sn * (uint64_t)(rbw + rd_code_bits(dl)) + ((uint64_t)sn - cov) * 96ull;
+    if (lane == 0) S.rd_pv[lbw - 1] = __ddiv_rn(__ull2double_rn(num), __ull2double_rn((uint64_t)sn));
+  }
+  __syncthreads();
+  uint32_t best = 0;
+  if (threadIdx.x == 0) {
+    double bb = __longlong_as_double(0x7FF0000000000000ll);  // +inf
+    for (uint32_t lbw = 1; lbw <= 24; lbw++) {
+      if (S.rd_pv[lbw - 1] < bb) {
+        bb = S.rd_pv[lbw - 1];
+        best = lbw;
+      }
+    }
+    if (best == 0 || bb >= 63.0) best = 0;
+    S.sc[0] = best;
+  }
+  __syncthreads();
+  best = (uint32_t)S.sc[0];
+  __syncthreads();
+  return best;
+}
+
+// Full-block top-8 left parts by (count desc, key asc) (reference
+// alp_rd.rs:47-68).  Counts go to a smem hash; when the block has more
+// distinct left parts than the smem table holds, a scratch table is used.
+__device__ void rd_top8(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t lbw, uint8_t* scratch) {
+  uint32_t rbw = 64 - lbw;
+  uint32_t* hk = S.big.rd.hkey;
+  uint32_t* hc = S.big.rd.hcnt;
+  for (uint32_t i = threadIdx.x; i < kHashCap; i += blockDim.x) {
+    hk[i] = kEmpty32;
+    hc[i] = 0;
+  }
+  if (threadIdx.x == 0) {
+    S.ovf = 0;
+    S.cnt32 = 0;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    if (*(volatile uint32_t*)&S.ovf) break;
+    uint32_t key = (uint32_t)(v[i] >> rbw);
+    uint32_t h = (uint32_t)(((uint64_t)key * 0x9E3779B97F4A7C15ull) >> 53);  // 11 bits
+    for (uint32_t probe = 0; probe < kHashCap; probe++) {
+      uint32_t cur = hk[h];
+      if (cur == kEmpty32) {
+        uint32_t old = atomicCAS(&hk[h], kEmpty32, key);
+        if (old == kEmpty32) {
+          if (atomicAdd(&S.cnt32, 1u) >= kHashLimit) S.ovf = 1;
+          cur = key;
+        } else {
+          cur = old;
+        }
+      }
+      if (cur == key) {
+        atomicAdd(&hc[h], 1u);
+        break;
+      }
+      h = (h + 1) & (kHashCap - 1);
+    }
+  }
+  __syncthreads();
+  uint32_t* tk = hk;
+  uint32_t* tc = hc;
+  uint32_t cap = kHashCap;
+  if (S.ovf) {  // scratch table: capacity >= 2n, (key, count) pairs
+    cap = pow2_at_least(2 * n);
+    tk = reinterpret_cast<uint32_t*>(scratch);
+    tc = tk + cap;
+    uint32_t lg = 31 - __clz(cap);
+    for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) {
+      tk[i] = kEmpty32;
+      tc[i] = 0;
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      uint32_t key = (uint32_t)(v[i] >> rbw);
+      uint32_t h = (uint32_t)(((uint64_t)key * 0x9E3779B97F4A7C15ull) >> (64 - lg));
+      for (uint32_t probe = 0; probe < cap; probe++) {
+        uint32_t cur = tk[h];
+        if (cur == kEmpty32) {
+          uint32_t old = atomicCAS(&tk[h], kEmpty32, key);
+          cur = old == kEmpty32 ? key : old;
+        }
+        if (cur == key) {
+          atomicAdd(&tc[h], 1u);
+          break;
+        }
+        h = (h + 1) & (cap - 1);
+      }
+    }
+    __syncthreads();
+  }
+  // 8 rounds of block argmax over (count desc, key asc).
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) S.dl = 0;
+  for (int r = 0; r < 8; r++) {
+    uint64_t best = 0;  // (count << 32) | (0xFFFFFFFF - key); 0 = none
+    uint32_t bslot = 0;
+    for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) {
+      uint32_t c = tc[i];
+      if (c) {
+        uint64_t kk = ((uint64_t)c << 32) | (uint64_t)(0xFFFFFFFFu - tk[i]);
+        if (kk > best) {
+          best = kk;
+          bslot = i;
+        }
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      uint64_t ob = __shfl_xor_sync(0xffffffffu, best, o);
+      uint32_t os = __shfl_xor_sync(0xffffffffu, bslot, o);
+      if (ob > best) {
+        best = ob;
+        bslot = os;
+      }
+    }
+    if (lane == 0) {
+      S.red[warp] = best;
+      S.red32[warp] = bslot;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint64_t b = 0;
+      uint32_t s = 0;
+      for (int w = 0; w < kEncWarps; w++)
+        if (S.red[w] > b) {
+          b = S.red[w];
+          s = S.red32[w];
+        }
+      if (b) {
+        S.dict8[S.dl++] = tk[s];
+        tc[s] = 0;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Code (0..dl-1) of a left part, or -1 for an exception.
+__device__ inline int rd_code(const EncSmem& S, uint64_t left) {
+  int c = -1;
+  for (uint32_t j = 0; j < S.dl; j++)
+    if (S.dict8[j] == left && c < 0) c = (int)j;
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// DICT preparation (reference dict.rs:87-123): distinct values, the sorted
+// dictionary and a value -> rank lookup.  Fast path: smem hash.  Fallback:
+// scratch hash + scratch bitonic sort + binary-search ranks.  Sets S.card and
+// S.flag (1 = dictionary bails: cardinality > n/2+1).
+// ---------------------------------------------------------------------------
+struct DictView {
+  bool smem;
+  const uint64_t* sorted;  // card values ascending
+  uint32_t card;
+};
+
+__device__ inline uint32_t dict_hash_slot(const uint64_t* hk, uint64_t x) {
+  uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 53);
+  for (uint32_t probe = 0; probe < kHashCap; probe++) {
+    uint64_t cur = hk[h];
+    if (cur == x || cur == kEmpty64) return h;
+    h = (h + 1) & (kHashCap - 1);
+  }
+  return 0;
+}
+
+__device__ inline uint32_t dict_rank(const EncSmem& S, const DictView& dv, uint64_t x) {
+  if (dv.smem) {
+    if (x == kEmpty64) return S.max_rank;
+    return S.big.dict.hval[dict_hash_slot(S.big.dict.hkey, x)];
+  }
+  uint32_t lo = 0, hi = dv.card;  // first index with sorted[i] >= x
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (dv.sorted[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scratch) {
+  DictArea& D = S.big.dict;
+  uint32_t max_card = n / 2 + 1;
+  for (uint32_t i = threadIdx.x; i < kHashCap; i += blockDim.x) {
+    D.hkey[i] = kEmpty64;
+    D.hval[i] = 0;
+  }
+  for (uint32_t i = threadIdx.x; i < kLbBits / 32; i += blockDim.x) D.lb[i] = 0;
+  if (threadIdx.x == 0) {
+    S.ovf = 0;
+    S.card = 0;
+    S.has_max = 0;
+    S.flag = 0;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    uint64_t x = v[i];
+    uint32_t b = (uint32_t)((x * 0xD6E8FEB86659FD93ull) >> (64 - 17));
+    atomicOr(&D.lb[b >> 5], 1u << (b & 31));
+    if (*(volatile uint32_t*)&S.ovf) continue;
+    if (x == kEmpty64) {
+      if (atomicExch(&S.has_max, 1u) == 0) atomicAdd(&S.card, 1u);
+      continue;
+    }
+    uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 53);
+    bool done = false;
+    for (uint32_t probe = 0; probe < kHashCap && !done; probe++) {
+      uint64_t cur = D.hkey[h];
+      if (cur == kEmpty64) {
+        unsigned long long old = atomicCAS((unsigned long long*)&D.hkey[h], kEmpty64, x);
+        if (old == kEmpty64) {
+          if (atomicAdd(&S.card, 1u) >= kHashLimit) S.ovf = 1;
+          done = true;
+          break;
+        }
+        cur = old;
+      }
+      if (cur == x) done = true;
+      else h = (h + 1) & (kHashCap - 1);
+    }
+    if (!done) S.ovf = 1;
+  }
+  __syncthreads();
+  DictView dv;
+  if (!S.ovf) {
+    uint32_t card = S.card;
+    if (card > max_card) {
+      if (threadIdx.x == 0) S.flag = 1;
+      __syncthreads();
+      dv.smem = true;
+      dv.sorted = nullptr;
+      dv.card = card;
+      return dv;
+    }
+    if (threadIdx.x == 0) S.cnt32 = 0;
+    __syncthreads();
+    uint32_t P = pow2_at_least(max(card, 1u));
+    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) D.sorted[i] = kEmpty64;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kHashCap; i += blockDim.x)
+      if (D.hkey[i] != kEmpty64) D.sorted[atomicAdd(&S.cnt32, 1u)] = D.hkey[i];
+    __syncthreads();
+    block_bitonic_sort(D.sorted, P);
+    for (uint32_t r = threadIdx.x; r < card; r += blockDim.x) {
+      uint64_t x = D.sorted[r];
+      if (x == kEmpty64) S.max_rank = r;
+      else D.hval[dict_hash_slot(D.hkey, x)] = r;
+    }
+    __syncthreads();
+    dv.smem = true;
+    dv.sorted = D.sorted;
+    dv.card = card;
+    return dv;
+  }
+  // Overflow: the lower-bound bitset may prove the bail outright.
+  uint32_t lbc = 0;
+  for (uint32_t i = threadIdx.x; i < kLbBits / 32; i += blockDim.x) lbc += __popc(D.lb[i]);
+  lbc = warp_sum(lbc);
+  if ((threadIdx.x & 31) == 0) S.red32[threadIdx.x >> 5] = lbc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kEncWarps; w++) t += S.red32[w];
+    S.cnt32 = t;
+  }
+  __syncthreads();
+  if (S.cnt32 > max_card) {
+    if (threadIdx.x == 0) S.flag = 1;
+    __syncthreads();
+    dv.smem = false;
+    dv.sorted = nullptr;
+    dv.card = S.cnt32;
+    return dv;
+  }
+  // Scratch path: u32 table of (first index + 1), capacity >= 2n; then sort.
+  uint32_t cap = pow2_at_least(2 * n), lg = 31 - __clz(cap);
+  uint32_t* T = reinterpret_cast<uint32_t*>(scratch);
+  uint64_t* srt = reinterpret_cast<uint64_t*>(scratch + 4ull * cap);
+  for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) T[i] = 0;
+  if (threadIdx.x == 0) {
+    S.card = 0;
+    S.cnt32 = 0;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    uint64_t x = v[i];
+    uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> (64 - lg));
+    for (uint32_t probe = 0; probe < cap; probe++) {
+      uint32_t cur = T[h];
+      if (cur == 0) {
+        uint32_t old = atomicCAS(&T[h], 0u, i + 1);
+        if (old == 0) {
+          atomicAdd(&S.card, 1u);
+          break;
+        }
+        cur = old;
+      }
+      if (v[cur - 1] == x) break;
+      h = (h + 1) & (cap - 1);
+    }
+  }
+  __syncthreads();
+  uint32_t card = S.card;
+  dv.smem = false;
+  dv.card = card;
+  if (card > max_card) {
+    if (threadIdx.x == 0) S.flag = 1;
+    __syncthreads();
+    dv.sorted = nullptr;
+    return dv;
+  }
+  uint32_t P = pow2_at_least(max(card, 1u));
+  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) srt[i] = kEmpty64;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x)
+    if (T[i]) srt[atomicAdd(&S.cnt32, 1u)] = v[T[i] - 1];
+  __syncthreads();
+  block_bitonic_sort(srt, P);
+  dv.sorted = srt;
+  return dv;
+}
+
+// Byte length of the dictionary value blob and its tag (reference dict.rs:40-61).
+__device__ uint64_t dict_values_len(EncSmem& S, const DictView& dv, uint32_t* tag) {
+  const uint64_t* s = dv.sorted;
+  uint64_t raw = 8ull * dv.card;
+  uint64_t delta = 8 + block_for(S, nullptr, dv.card, false, [&](uint32_t i) {
+                     return zigzag64(s[i] - (i ? s[i - 1] : s[0]));
+                   });
+  if (delta < raw) {
+    *tag = 1;
+    return delta;
+  }
+  *tag = 0;
+  return raw;
+}
+
+// ---------------------------------------------------------------------------
+// RLE run starts (reference rle.rs:10-42).  Requires S.neq_k (transitions per
+// sub-block).  Returns the starts array (smem or scratch).
+// ---------------------------------------------------------------------------
+__device__ uint32_t* rle_starts(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t runs, uint8_t* scratch) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t* st = runs <= kRunsSmem ? S.big.rle.starts : reinterpret_cast<uint32_t*>(scratch);
+  uint32_t nsub = (n + kSub - 1) / kSub;
+  if (threadIdx.x == 0) {  // exclusive prefix of transitions per sub-block
+    uint32_t acc = 0;
+    for (uint32_t k = 0; k < nsub; k++) {
+      uint32_t c = S.neq_k[k];
+      S.subsz[k] = acc;
+      acc += c;
+    }
+    st[0] = 0;
+  }
+  __syncthreads();
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+    uint64_t carry = base ? v[base - 1] : v[0];
+    uint32_t before = S.subsz[k];
+    for (uint32_t j = 0; j < 32; j++) {
+      uint32_t li = j * 32 + lane;
+      bool ok = li < cnt;
+      uint32_t idx = base + li;
+      uint64_t x = ok ? v[idx] : 0;
+      uint64_t up = __shfl_up_sync(0xffffffffu, x, 1);
+      uint64_t pv = lane ? up : carry;
+      carry = __shfl_sync(0xffffffffu, x, 31);
+      bool tr = ok && idx && x != pv;
+      uint32_t m = __ballot_sync(0xffffffffu, tr);
+      if (tr) st[1 + before + __popc(m & ((1u << lane) - 1u))] = idx;
+      before += __popc(m);
+    }
+  }
+  __syncthreads();
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// The competition kernel.
+// ---------------------------------------------------------------------------
+struct Cand {
+  uint64_t len;
+  bool ok;
+};
+
+__device__ void init_smem(EncSmem& S, const uint64_t* v) {
+  if (threadIdx.x == 0) {
+    S.xor_bytes = 0;
+    S.umin = kEmpty64;
+    S.umax = 0;
+    S.neq = 0;
+    S.stride_bad = 0;
+    S.fm_mask = 0x7F;
+    S.alp_fail = 0;
+    S.flag = 0;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kEncThreads) k_compete(const uint64_t* __restrict__ lane, FrameDesc* frames,
+                                                         const uint32_t* __restrict__ nbp, int dtype, int level,
+                                                         uint8_t* __restrict__ scratch) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  EncSmem& S = *reinterpret_cast<EncSmem*>(smem_raw);
+  uint32_t b = blockIdx.x;
+  if (b >= *nbp) return;
+  FrameDesc fd = frames[b];
+  const uint64_t* v = lane + fd.value_off;
+  uint32_t n = fd.n;
+  uint8_t* scr = scratch + fd.value_off * kEncScratchPerValue;
+  bool fam_float = dtype_float(dtype);
+  bool reduced = level == 0;
+  uint64_t lambda = level_lambda(level);
+  uint64_t lb = lane_bytes(dtype);
+  uint64_t decoded_bytes = (uint64_t)n * lb, raw_bytes = (uint64_t)n * 8;
+  uint32_t nsub = (n + kSub - 1) / kSub;
+
+  init_smem(S, v);
+  stats_pass(S, v, n, dtype, fam_float && !reduced);
+  __syncthreads();
+  sample_features(S, v, n);
+
+  // Integer early-out (reference encoder.rs:295-298,655-683).
+  if (threadIdx.x == 0) {
+    uint32_t distinct = 0;
+    for (int i = 0; i < 512; i++) distinct += __popc(S.distinct_bits[i]);
+    bool distinct_low = distinct < 2048;
+    uint32_t consec_eq = n - S.neq;
+    bool repeats = (uint64_t)consec_eq * 2 > (uint64_t)n;
+    bool eo = false;
+    if (!fam_float && !(distinct_low || repeats || n < 256)) {
+      uint32_t thr = (uint32_t)(lb * 8) - 4;
+      uint32_t vw = bit_width64(S.e_vmax - S.e_vmin), dw = bit_width64(S.e_dmax);
+      eo = vw >= thr && dw >= thr;
+    }
+    S.flag = eo ? 1u : 0u;
+  }
+  __syncthreads();
+  if (S.flag) {
+    if (threadIdx.x == 0) {
+      frames[b].mode = M_RAW;
+      frames[b].plen = (uint32_t)decoded_bytes;
+      frames[b].aux = 0;
+      atomicAdd(&g_wins[M_RAW], 1ull);
+    }
+    return;
+  }
+
+  // Candidates in the reference's consideration order (encoder.rs:301-344).
+  uint64_t vl = varint_len(n);
+  uint64_t sz_for = vl, sz_delta = 8 + vl;
+  if (threadIdx.x == 0) {
+    for (uint32_t k = 0; k < nsub; k++) {
+      sz_for += 9 + 128ull * S.w_a[k];
+      sz_delta += 9 + 128ull * S.w_b[k];
+    }
+    S.sc[1] = sz_for;
+    S.sc[2] = sz_delta;
+  }
+  __syncthreads();
+  sz_for = S.sc[1];
+  sz_delta = S.sc[2];
+
+  Cand c_fm = {0, false}, c_alp = {0, false}, c_rd = {0, false};
+  uint32_t fm_scale = 0, rd_lbw = 0;
+  if (fam_float && !reduced) {
+    // FLOAT_MULT (float_mult.rs:66-98, bit-packed k)
+    uint32_t mask = S.fm_mask;
+    if (mask) {
+      fm_scale = __ffs(mask) - 1;
+      fm_widths(S, v, n, (int)fm_scale);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        uint64_t s = 2 + vl;
+        for (uint32_t k = 0; k < nsub; k++) s += 9 + 128ull * S.w_d[k];
+        S.sc[3] = s;
+      }
+      __syncthreads();
+      c_fm.ok = true;
+      c_fm.len = S.sc[3];
+    }
+    // ALP (alp.rs:93-166)
+    {
+      int lane_id = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+        if (__shfl_sync(0xffffffffu, *(volatile uint32_t*)&S.alp_fail, 0)) break;
+        uint32_t cnt = min((uint32_t)kSub, n - k * kSub);
+        AlpSub a;
+        bool ok = alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], &a);
+        if (lane_id == 0) {
+          if (!ok) S.alp_fail = 1;
+          else {
+            S.w_c[k] = (uint8_t)a.w;
+            S.alp_exc[k] = (uint16_t)a.exc;
+          }
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0 && !S.alp_fail) {
+        uint64_t s = vl;
+        for (uint32_t k = 0; k < nsub; k++) s += 13 + 128ull * S.w_c[k] + 10ull * S.alp_exc[k];
+        S.sc[4] = s;
+      }
+      __syncthreads();
+      c_alp.ok = !S.alp_fail;
+      c_alp.len = S.sc[4];
+    }
+    // ALP-RD (alp_rd.rs:132-206, bit-packed streams)
+    rd_lbw = rd_choose_cut(S, v, n);
+    if (rd_lbw) {
+      rd_top8(S, v, n, rd_lbw, scr);
+      uint32_t rbw = 64 - rd_lbw;
+      uint64_t rmask = (1ull << rbw) - 1ull;
+      if (threadIdx.x == 0) {
+        S.acc64 = 0;
+        S.cnt32 = 0;
+      }
+      __syncthreads();
+      int lane_id = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+        uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+        uint64_t cmx = 0, rmn = kEmpty64, rmx = 0, cmn = kEmpty64, eb = 0;
+        uint32_t ne = 0;
+        for (uint32_t i = lane_id; i < cnt; i += 32) {
+          uint64_t x = v[base + i];
+          int c = rd_code(S, x >> rbw);
+          uint64_t code = c < 0 ? 0 : (uint64_t)c;
+          if (c < 0) {
+            ne++;
+            eb += varint_len(base + i) + 8;
+          }
+          cmn = u64min(cmn, code);
+          cmx = u64max(cmx, code);
+          rmn = u64min(rmn, x & rmask);
+          rmx = u64max(rmx, x & rmask);
+        }
+        cmn = warp_min(cmn);
+        cmx = warp_max(cmx);
+        rmn = warp_min(rmn);
+        rmx = warp_max(rmx);
+        ne = warp_sum(ne);
+        eb = warp_sum(eb);
+        if (lane_id == 0) {
+          S.w_a[k] = (uint8_t)bit_width64(cmx - cmn);
+          S.w_b[k] = (uint8_t)bit_width64(rmx - rmn);
+          atomicAdd(&S.cnt32, ne);
+          atomicAdd(&S.acc64, (unsigned long long)eb);
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        uint64_t nexc = S.cnt32;
+        uint64_t clen = vl, rlen = vl;
+        for (uint32_t k = 0; k < nsub; k++) {
+          clen += 9 + 128ull * S.w_a[k];
+          rlen += 9 + 128ull * S.w_b[k];
+        }
+        S.sc[5] = (nexc * 4 > n) ? 0ull
+                                 : 2 + 8ull * S.dl + varint_len(nexc) + S.acc64 + 1 + varint_len(clen) + clen + 1 + rlen;
+      }
+      __syncthreads();
+      c_rd.ok = S.sc[5] != 0;
+      c_rd.len = S.sc[5];
+    }
+  }
+
+  // Selection up to ALP-RD (encoder.rs:301-344), then the compressibility gate.
+  int best_mode = M_RAW;
+  uint64_t best_len = decoded_bytes;
+  uint64_t best_score = best_len + ((lambda * decode_weight(M_RAW) * decoded_bytes) >> 8);
+  auto consider = [&](int m, uint64_t len) {
+    uint64_t s = len + ((lambda * decode_weight(m) * decoded_bytes) >> 8);
+    if (s < best_score) {
+      best_score = s;
+      best_mode = m;
+      best_len = len;
+    }
+  };
+  if (S.umin == S.umax) consider(M_CONST, 8);
+  if (n >= 2 && !S.stride_bad) consider(M_STRIDE, 16);
+  if (!reduced) consider(M_XORZ, S.xor_bytes);
+  consider(M_FOR_BITPACK, sz_for);
+  consider(M_DELTA_BITPACK, sz_delta);
+  if (c_fm.ok) consider(M_FLOAT_MULT, c_fm.len);
+  if (c_alp.ok) consider(M_ALP, c_alp.len);
+  if (c_rd.ok) consider(M_ALP_RD, c_rd.len);
+  bool block_compressible = best_len * 20 < raw_bytes * 19;  // encoder.rs:394,644-646
+
+  if (block_compressible && !reduced) {
+    // DICT (dict.rs:87-152, bit-packed codes)
+    DictView dv = dict_prepare(S, v, n, scr);
+    if (!S.flag) {
+      uint32_t vtag;
+      uint64_t vlen = dict_values_len(S, dv, &vtag);
+      uint64_t clen = block_for(S, nullptr, n, false, [&](uint32_t i) { return (uint64_t)dict_rank(S, dv, v[i]); });
+      consider(M_DICT, varint_len(dv.card) + 1 + varint_len(vlen) + vlen + 1 + clen);
+    }
+    __syncthreads();
+    // RLE (rle.rs:10-42)
+    uint32_t neq = S.neq;
+    if (neq <= n / 2 + 1) {
+      uint32_t runs = neq + 1;
+      uint32_t* st = rle_starts(S, v, n, runs, scr);
+      uint64_t lens = block_for(S, nullptr, runs, false, [&](uint32_t r) {
+        return (uint64_t)((r + 1 < runs ? st[r + 1] : n) - st[r]);
+      });
+      consider(M_RLE, varint_len(runs) + 8ull * runs + lens);
+    }
+  }
+  if (threadIdx.x == 0) {
+    frames[b].mode = (uint32_t)best_mode;
+    frames[b].plen = (uint32_t)best_len;
+    frames[b].aux = best_mode == M_FLOAT_MULT ? fm_scale : best_mode == M_ALP_RD ? rd_lbw : 0;
+    atomicAdd(&g_wins[best_mode], 1ull);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Emission kernel: writes the frame header and the winner's payload.
+// ---------------------------------------------------------------------------
+__device__ void emit_raw(const uint64_t* v, uint32_t n, int dtype, uint8_t* out) {
+  uint32_t lb = lane_bytes(dtype);
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    uint64_t x = v[i];
+    if (dtype == DT_F32) put_u32(out + 4ull * i, f64bits_to_f32bits(x));
+    else if (lb == 4) put_u32(out + 4ull * i, (uint32_t)x);
+    else put_u64(out + 8ull * i, x);
+  }
+}
+
+__device__ void emit_xorz(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* out) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nsub = (n + kSub - 1) / kSub;
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+    uint32_t tot = 0;
+    for (uint32_t i = lane; i < cnt; i += 32) {
+      uint32_t idx = base + i;
+      tot += varint_len(v[idx] ^ (idx ? v[idx - 1] : 0ull));
+    }
+    tot = warp_sum(tot);
+    if (lane == 0) S.subsz[k] = tot;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (uint32_t k = 0; k < nsub; k++) {
+      uint32_t c = S.subsz[k];
+      S.subsz[k] = acc;
+      acc += c;
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+    uint32_t off = S.subsz[k];
+    for (uint32_t j = 0; j < 32; j++) {
+      uint32_t li = j * 32 + lane;
+      bool ok = li < cnt;
+      uint32_t idx = base + li;
+      uint64_t x = ok ? v[idx] ^ (idx ? v[idx - 1] : 0ull) : 0ull;
+      uint32_t sz = ok ? varint_len(x) : 0u;
+      uint32_t inc = warp_incl_scan(sz);
+      if (ok) put_varint(out + off + inc - sz, x);
+      off += __shfl_sync(0xffffffffu, inc, 31);
+    }
+  }
+}
+
+__device__ void emit_alp(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* out) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nsub = (n + kSub - 1) / kSub;
+  __shared__ int64_t s_fill[kSubsMax];
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t cnt = min((uint32_t)kSub, n - k * kSub);
+    AlpSub a;
+    alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], &a);  // succeeded in the competition
+    if (lane == 0) {
+      S.alp_ef[k][0] = (uint8_t)a.e;
+      S.alp_ef[k][1] = (uint8_t)a.f;
+      S.w_c[k] = (uint8_t)a.w;
+      S.alp_exc[k] = (uint16_t)a.exc;
+      S.submin[k] = (uint64_t)a.mn;
+      s_fill[k] = a.filler;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t off = put_varint(out, n);
+    for (uint32_t k = 0; k < nsub; k++) {
+      S.subsz[k] = off;
+      off += 13 + 128u * S.w_c[k] + 10u * S.alp_exc[k];
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+    uint8_t* d = out + S.subsz[k];
+    int e = S.alp_ef[k][0], f = S.alp_ef[k][1];
+    uint32_t w = S.w_c[k];
+    int64_t mn = (int64_t)S.submin[k], fill = s_fill[k];
+    if (lane == 0) {
+      put_u8(d, e);
+      put_u8(d + 1, f);
+      put_u16(d + 2, S.alp_exc[k]);
+      put_u64(d + 4, (uint64_t)mn);
+      put_u8(d + 12, w);
+    }
+    const uint64_t* sv = v + base;
+    // Digits (exceptions and padding take the filler digit), FastLanes packed.
+    if (w > 0) {
+      uint64_t acc = 0;
+      uint32_t nb = 0, wd = 0;
+      for (uint32_t r = 0; r < 32; r++) {
+        uint32_t i = r * 32 + lane;
+        int64_t dg = fill;
+        if (i < cnt) {
+          int64_t dd;
+          if (alp_roundtrips(sv[i], e, f, &dd)) dg = dd;
+        }
+        uint32_t res = (uint32_t)((uint64_t)dg - (uint64_t)mn);
+        if (w < 32) res &= (1u << w) - 1u;
+        acc |= (uint64_t)res << nb;
+        nb += w;
+        if (nb >= 32) {
+          put_u32(d + 13 + 4u * (wd * 32u + lane), (uint32_t)acc);
+          wd++;
+          acc >>= 32;
+          nb -= 32;
+        }
+      }
+    }
+    // Exceptions in position order.
+    uint8_t* xp = d + 13 + 128u * w;
+    uint32_t before = 0;
+    for (uint32_t j = 0; j < 32; j++) {
+      uint32_t li = j * 32 + lane;
+      bool ok = li < cnt;
+      int64_t dd;
+      bool ex = ok && !alp_roundtrips(sv[li], e, f, &dd);
+      uint32_t m = __ballot_sync(0xffffffffu, ex);
+      if (ex) {
+        uint8_t* q = xp + 10u * (before + __popc(m & ((1u << lane) - 1u)));
+        put_u16(q, li);
+        put_u64(q + 2, sv[li]);
+      }
+      before += __popc(m);
+    }
+  }
+}
+
+__device__ void emit_alprd(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t lbw, uint8_t* scr, uint8_t* out) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nsub = (n + kSub - 1) / kSub;
+  rd_top8(S, v, n, lbw, scr);
+  uint32_t rbw = 64 - lbw;
+  uint64_t rmask = (1ull << rbw) - 1ull;
+  // exception bytes per sub-block
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+    uint32_t eb = 0, ne = 0;
+    for (uint32_t i = lane; i < cnt; i += 32) {
+      if (rd_code(S, v[base + i] >> rbw) < 0) {
+        eb += varint_len(base + i) + 8;
+        ne++;
+      }
+    }
+    eb = warp_sum(eb);
+    ne = warp_sum(ne);
+    if (lane == 0) {
+      S.subsz[k] = eb;
+      S.neq_k[k] = ne;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t pos = 0;
+    put_u8(out + pos++, lbw);
+    put_u8(out + pos++, S.dl);
+    for (uint32_t j = 0; j < S.dl; j++, pos += 8) put_u64(out + pos, S.dict8[j]);
+    uint64_t nexc = 0;
+    for (uint32_t k = 0; k < nsub; k++) nexc += S.neq_k[k];
+    pos += put_varint(out + pos, nexc);
+    for (uint32_t k = 0; k < nsub; k++) {
+      uint32_t c = S.subsz[k];
+      S.subsz[k] = pos;
+      pos += c;
+    }
+    S.sc[6] = pos;  // codes tag position
+  }
+  __syncthreads();
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+    uint32_t off = S.subsz[k];
+    for (uint32_t j = 0; j < 32; j++) {
+      uint32_t li = j * 32 + lane;
+      bool ok = li < cnt;
+      uint64_t x = ok ? v[base + li] : 0;
+      bool ex = ok && rd_code(S, x >> rbw) < 0;
+      uint32_t sz = ex ? varint_len(base + li) + 8 : 0u;
+      uint32_t inc = warp_incl_scan(sz);
+      if (ex) {
+        uint8_t* q = out + off + inc - sz;
+        uint32_t vlb = put_varint(q, base + li);
+        put_u64(q + vlb, x >> rbw);
+      }
+      off += __shfl_sync(0xffffffffu, inc, 31);
+    }
+  }
+  __syncthreads();
+  uint64_t pos = S.sc[6];
+  auto code_of = [&](uint32_t i) -> uint64_t {
+    int c = rd_code(S, v[i] >> rbw);
+    return c < 0 ? 0ull : (uint64_t)c;
+  };
+  uint64_t clen = block_for(S, nullptr, n, false, code_of);
+  uint32_t cvl = varint_len(clen);
+  if (threadIdx.x == 0) {
+    put_u8(out + pos, 0);
+    put_varint(out + pos + 1, clen);
+  }
+  block_for(S, out + pos + 1 + cvl, n, false, code_of);
+  uint64_t rpos = pos + 1 + cvl + clen;
+  if (threadIdx.x == 0) put_u8(out + rpos, 0);
+  block_for(S, out + rpos + 1, n, false, [&](uint32_t i) { return v[i] & rmask; });
+}
+
+__device__ void emit_dict(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scr, uint8_t* out) {
+  DictView dv = dict_prepare(S, v, n, scr);
+  uint32_t vtag;
+  uint64_t vlen = dict_values_len(S, dv, &vtag);
+  uint64_t pos = 0;
+  if (threadIdx.x == 0) {
+    pos = put_varint(out, dv.card);
+    put_u8(out + pos++, vtag);
+    pos += put_varint(out + pos, vlen);
+    S.sc[6] = pos;
+  }
+  __syncthreads();
+  pos = S.sc[6];
+  const uint64_t* s = dv.sorted;
+  if (vtag == 0) {
+    for (uint32_t i = threadIdx.x; i < dv.card; i += blockDim.x) put_u64(out + pos + 8ull * i, s[i]);
+  } else {
+    if (threadIdx.x == 0) put_u64(out + pos, s[0]);
+    block_for(S, out + pos + 8, dv.card, false, [&](uint32_t i) { return zigzag64(s[i] - (i ? s[i - 1] : s[0])); });
+  }
+  __syncthreads();
+  pos += vlen;
+  if (threadIdx.x == 0) put_u8(out + pos, 0);
+  block_for(S, out + pos + 1, n, false, [&](uint32_t i) { return (uint64_t)dict_rank(S, dv, v[i]); });
+}
+
+__device__ void emit_rle(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scr, uint8_t* out) {
+  // transitions per sub-block (the competition's counts are not kept)
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nsub = (n + kSub - 1) / kSub;
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+    uint32_t nq = 0;
+    for (uint32_t i = lane; i < cnt; i += 32) {
+      uint32_t idx = base + i;
+      nq += (idx && v[idx] != v[idx - 1]) ? 1u : 0u;
+    }
+    nq = warp_sum(nq);
+    if (lane == 0) S.neq_k[k] = nq;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (uint32_t k = 0; k < nsub; k++) t += S.neq_k[k];
+    S.cnt32 = t + 1;
+  }
+  __syncthreads();
+  uint32_t runs = S.cnt32;
+  uint32_t* st = rle_starts(S, v, n, runs, scr);
+  uint32_t vl = varint_len(runs);
+  if (threadIdx.x == 0) put_varint(out, runs);
+  for (uint32_t r = threadIdx.x; r < runs; r += blockDim.x) put_u64(out + vl + 8ull * r, v[st[r]]);
+  block_for(S, out + vl + 8ull * runs, runs, false,
+            [&](uint32_t r) { return (uint64_t)((r + 1 < runs ? st[r + 1] : n) - st[r]); });
+}
+
+__global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict__ lane,
+                                                      const FrameDesc* __restrict__ frames,
+                                                      const uint32_t* __restrict__ nbp, int dtype,
+                                                      uint8_t* __restrict__ scratch, uint8_t* __restrict__ outbuf) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  EncSmem& S = *reinterpret_cast<EncSmem*>(smem_raw);
+  uint32_t b = blockIdx.x;
+  if (b >= *nbp) return;
+  FrameDesc fd = frames[b];
+  const uint64_t* v = lane + fd.value_off;
+  uint32_t n = fd.n;
+  uint8_t* scr = scratch + fd.value_off * kEncScratchPerValue;
+  uint8_t* hdr = outbuf + fd.payload_off - 9;
+  uint8_t* out = outbuf + fd.payload_off;
+  if (threadIdx.x == 0) {
+    put_u8(hdr, fd.mode);
+    put_u32(hdr + 1, n);
+    put_u32(hdr + 5, fd.plen);
+  }
+  bool sgn = dtype_signed(dtype);
+  switch (fd.mode) {
+    case M_RAW: emit_raw(v, n, dtype, out); break;
+    case M_CONST:
+      if (threadIdx.x == 0) put_u64(out, v[0]);
+      break;
+    case M_STRIDE:
+      if (threadIdx.x == 0) {
+        put_u64(out, v[0]);
+        put_u64(out + 8, v[1] - v[0]);
+      }
+      break;
+    case M_XORZ: emit_xorz(S, v, n, out); break;
+    case M_FOR_BITPACK: block_for(S, out, n, sgn, [&](uint32_t i) { return v[i]; }); break;
+    case M_DELTA_BITPACK:
+      if (threadIdx.x == 0) put_u64(out, v[0]);
+      block_for(S, out + 8, n, false, [&](uint32_t i) { return zigzag64(v[i] - (i ? v[i - 1] : v[0])); });
+      break;
+    case M_FLOAT_MULT: {
+      int s = (int)fd.aux;
+      if (threadIdx.x == 0) {
+        put_u8(out, 0);
+        put_u8(out + 1, s);
+      }
+      block_for(S, out + 2, n, true, [&](uint32_t i) { return (uint64_t)fm_k(v[i], s); });
+      break;
+    }
+    case M_ALP: emit_alp(S, v, n, out); break;
+    case M_ALP_RD: emit_alprd(S, v, n, fd.aux, scr, out); break;
+    case M_DICT: emit_dict(S, v, n, scr, out); break;
+    case M_RLE: emit_rle(S, v, n, scr, out); break;
+    default: break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Window probe, block planning and frame offsets.
+// ---------------------------------------------------------------------------
+
+// One CTA per 32768-value window: grow flag = distinct_low || repeats
+// (reference encoder.rs:166-176, 705-750).
+__global__ void k_probe_windows(const uint64_t* __restrict__ v, uint64_t n, uint8_t* __restrict__ grow) {
+  __shared__ uint32_t bits[512];
+  __shared__ uint32_t s_neq;
+  uint64_t s = (uint64_t)blockIdx.x * kBaseQuantum;
+  uint32_t len = (uint32_t)qmin(kBaseQuantum, n - s);
+  const uint64_t* w = v + s;
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) bits[i] = 0;
+  if (threadIdx.x == 0) s_neq = 0;
+  __syncthreads();
+  uint32_t nq = 0;
+  for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) nq += (i && w[i] != w[i - 1]) ? 1u : 0u;
+  nq = warp_sum(nq);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&s_neq, nq);
+  uint32_t stride = max(len / 4096u, 1u);
+  for (uint32_t i = threadIdx.x; (uint64_t)i * stride < len; i += blockDim.x) {
+    uint64_t h = w[(uint64_t)i * stride] * 0x9E3779B97F4A7C15ull;
+    uint32_t b = (uint32_t)((h >> 50) & 0x3FFF);
+    atomicOr(&bits[b >> 5], 1u << (b & 31));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t d = 0;
+    for (int i = 0; i < 512; i++) d += __popc(bits[i]);
+    uint32_t consec = len - s_neq;
+    grow[blockIdx.x] = (d < 2048 || (uint64_t)consec * 2 > len) ? 1 : 0;
+  }
+}
+
+// Block plan (reference encoder.rs:154-178): fills frames[].value_off / .n.
+__global__ void k_plan(const uint8_t* __restrict__ grow, uint64_t n, uint64_t fixed_bs, FrameDesc* frames,
+                       uint32_t* nb) {
+  if (fixed_bs) {
+    uint64_t nblk = (n + fixed_bs - 1) / fixed_bs;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nblk; i += (uint64_t)gridDim.x * blockDim.x) {
+      FrameDesc f;
+      f.value_off = i * fixed_bs;
+      f.n = (uint32_t)qmin(fixed_bs, n - f.value_off);
+      f.payload_off = 0;
+      f.plen = 0;
+      f.mode = 0;
+      f.aux = 0;
+      frames[i] = f;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nb = (uint32_t)nblk;
+    return;
+  }
+  if (blockIdx.x || threadIdx.x) return;
+  uint64_t s = 0;
+  uint32_t c = 0;
+  while (s < n) {
+    uint64_t end = grow[s / kBaseQuantum] ? qmin(s + kMaxBlock, n) : qmin(s + kBaseQuantum, n);
+    FrameDesc f;
+    f.value_off = s;
+    f.n = (uint32_t)(end - s);
+    f.payload_off = 0;
+    f.plen = 0;
+    f.mode = 0;
+    f.aux = 0;
+    frames[c++] = f;
+    s = end;
+  }
+  *nb = c;
+}
+
+__global__ void k_frame_sizes(const FrameDesc* __restrict__ frames, const uint32_t* __restrict__ nbp, uint32_t maxb,
+                              uint64_t* __restrict__ sizes) {
+  uint32_t nb = *nbp;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < maxb; i += gridDim.x * blockDim.x)
+    sizes[i] = i < nb ? 9ull + frames[i].plen : 0ull;
+}
+__global__ void k_frame_apply(FrameDesc* frames, const uint32_t* __restrict__ nbp, const uint64_t* __restrict__ offs,
+                              const uint64_t* __restrict__ base_p) {
+  uint32_t nb = *nbp;
+  uint64_t base = *base_p;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    frames[i].payload_off = base + offs[i] + 9;
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+static size_t enc_smem_bytes() { return sizeof(EncSmem); }
+
+void launch_probe_windows(const uint64_t* lane, uint64_t n, uint8_t* grow, cudaStream_t st) {
+  uint64_t nw = (n + kBaseQuantum - 1) / kBaseQuantum;
+  if (nw) k_probe_windows<<<(unsigned)nw, 256, 0, st>>>(lane, n, grow);
+  count_launches(nw ? 1 : 0);
+}
+
+void launch_plan(const uint8_t* grow, uint64_t n, uint64_t fixed_bs, FrameDesc* frames, uint32_t* nb,
+                 cudaStream_t st) {
+  unsigned g = 1;
+  if (fixed_bs) g = (unsigned)qmin(((n + fixed_bs - 1) / fixed_bs + 255) / 256, 4096);
+  if (g == 0) g = 1;
+  k_plan<<<g, 256, 0, st>>>(grow, n, fixed_bs, frames, nb);
+  count_launches(1);
+}
+
+void launch_compete(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, int dtype,
+                    int level, uint8_t* scratch, unsigned long long* wins, cudaStream_t st) {
+  (void)wins;
+  cudaFuncSetAttribute(k_compete, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)enc_smem_bytes());
+  cudaFuncSetAttribute(k_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)enc_smem_bytes());
+  if (max_blocks) k_compete<<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, dtype, level, scratch);
+  count_launches(max_blocks ? 1 : 0);
+}
+
+void launch_emit(const uint64_t* lane, const FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, int dtype,
+                 uint8_t* scratch, uint8_t* out, cudaStream_t st) {
+  if (max_blocks) k_emit<<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, dtype, scratch, out);
+  count_launches(max_blocks ? 1 : 0);
+}
+
+unsigned long long* device_win_counters() {
+  void* p = nullptr;
+  cudaGetSymbolAddress(&p, g_wins);
+  return reinterpret_cast<unsigned long long*>(p);
+}
+
+}  // namespace qb
+
+#include "qb_scan.cuh"
+
+namespace qb {
+void launch_frame_offsets(FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, const uint64_t* base,
+                          uint64_t* sizes_tmp, uint64_t* tile_tmp, uint64_t* total, cudaStream_t st) {
+  unsigned g = (unsigned)qmin((max_blocks + 255) / 256, 1024);
+  if (g == 0) g = 1;
+  k_frame_sizes<<<g, 256, 0, st>>>(frames, nb, max_blocks, sizes_tmp);
+  scan_exclusive_u64(sizes_tmp, sizes_tmp, max_blocks ? max_blocks : 1, tile_tmp, total, st);
+  k_frame_apply<<<g, 256, 0, st>>>(frames, nb, sizes_tmp, base);
+  count_launches(5);
+}
+}  // namespace qb

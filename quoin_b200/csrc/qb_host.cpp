@@ -1,0 +1,1209 @@
+// Host side of the B200 quoin library: stream format writer/reader
+// (reference src/format.rs, src/decoder.rs:43-118, src/decimal.rs), column
+// lowering orchestration (src/lib.rs:389-508), the GPU pipeline drivers and
+// the C ABI of include/quoin.h (capi/src/lib.rs, capi/src/typed.rs).
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/quoin.h"
+#include "qb_kernels.h"
+#include "qb_layout.h"
+
+namespace qb {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(uint64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
+
+}  // namespace qb
+
+using namespace qb;
+
+namespace {
+
+enum { WT_F64 = 0, WT_I64, WT_U64, WT_I32, WT_U32, WT_F32, WT_DEC128, WT_DEC256 };
+enum { K_OK = 0, K_BAD_MAGIC = 1, K_VERSION = 2, K_TRUNC = 3, K_UNKNOWN_MODE = 4, K_CORRUPT = 5,
+       K_LENGTH = 6, K_DTYPE = 7, K_DTYPE_MISMATCH = 8, K_UNSUPPORTED = 9 };
+constexpr uint64_t kMaxBlockValues = 131072;
+constexpr uint64_t kBaseQuantumH = 32768;
+constexpr uint64_t kMaxBitmapBytes = 1ull << 36;
+
+inline uint32_t lane_bytes_h(int dt) { return (dt == WT_I32 || dt == WT_U32 || dt == WT_F32) ? 4u : 8u; }
+inline uint32_t native_width(int dt) {
+  switch (dt) {
+    case WT_I32: case WT_U32: case WT_F32: return 4;
+    case WT_DEC128: return 16;
+    case WT_DEC256: return 32;
+    default: return 8;
+  }
+}
+inline uint32_t varint_len_h(uint64_t v) {
+  uint32_t n = 1;
+  while (v >= 0x80) { v >>= 7; n++; }
+  return n;
+}
+inline void put_varint_h(std::vector<uint8_t>& o, uint64_t v) {
+  for (;;) {
+    uint8_t b = (uint8_t)(v & 0x7f);
+    v >>= 7;
+    if (v) o.push_back(b | 0x80); else { o.push_back(b); return; }
+  }
+}
+inline uint64_t rd64(const uint8_t* p) {
+  uint64_t v = 0;
+  for (int i = 7; i >= 0; i--) v = (v << 8) | p[i];
+  return v;
+}
+inline uint32_t rd32(const uint8_t* p) {
+  return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+// LEB128 (reference varint.rs:24-39); returns a K_* kind.
+int rd_varint_h(const uint8_t* p, uint64_t len, uint64_t* pos, uint64_t* out) {
+  uint64_t r = 0;
+  uint32_t shift = 0;
+  for (;;) {
+    if (*pos >= len) return K_TRUNC;
+    uint8_t b = p[(*pos)++];
+    r |= (uint64_t)(b & 0x7f) << shift;
+    if (!(b & 0x80)) { *out = r; return K_OK; }
+    shift += 7;
+    if (shift >= 64) return K_CORRUPT;
+  }
+}
+inline int kind_to_code(int kind) {
+  switch (kind) {
+    case K_OK: return QUOIN_OK;
+    case K_BAD_MAGIC: return QUOIN_ERR_BAD_MAGIC;
+    case K_VERSION: return QUOIN_ERR_UNSUPPORTED_VERSION;
+    case K_TRUNC: return QUOIN_ERR_TRUNCATED;
+    case K_UNKNOWN_MODE: return QUOIN_ERR_UNKNOWN_MODE;
+    case K_CORRUPT: return QUOIN_ERR_CORRUPT_PAYLOAD;
+    case K_LENGTH: return QUOIN_ERR_LENGTH_MISMATCH;
+    case K_DTYPE: return QUOIN_ERR_UNSUPPORTED_DTYPE;
+    case K_DTYPE_MISMATCH: return QUOIN_ERR_DTYPE_MISMATCH;
+    default: return QUOIN_ERR_UNSUPPORTED;
+  }
+}
+inline bool mode_known(int id) {  // reference mode.rs:60-84
+  switch (id) {
+    case 0: case 1: case 2: case 3: case 4: case 5: case 7: case 9: case 11: case 17:
+    case 19: case 20: case 25: case 29: case 45: case 50: case 51: case 52: case 53: case 54:
+      return true;
+    default: return false;
+  }
+}
+inline uint64_t popcount_bits(const uint8_t* bm, uint64_t n) {  // reference validity.rs:28-37
+  uint64_t c = 0, full = n / 8;
+  uint64_t i = 0;
+  for (; i + 8 <= full; i += 8) {
+    uint64_t w;
+    memcpy(&w, bm + i, 8);
+    c += (uint64_t)__builtin_popcountll(w);
+  }
+  for (; i < full; i++) c += (uint64_t)__builtin_popcount(bm[i]);
+  uint64_t rem = n & 7;
+  if (rem) c += (uint64_t)__builtin_popcount(bm[full] & ((1u << rem) - 1u));
+  return c;
+}
+// Public code for the reference symbols.
+inline int plain_code(int ext) {
+  if (ext == QUOIN_OK || ext == QUOIN_ERR_NULL || ext == QUOIN_ERR_BUFFER_TOO_SMALL) return ext;
+  if (ext == QUOIN_ERR_CUDA || ext == QUOIN_ERR_BAD_ARG) return QUOIN_ERR_PANIC;
+  return QUOIN_ERR_CORRUPT;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context: CUDA stream + grow-only device arenas.
+// ---------------------------------------------------------------------------
+enum Slot {
+  S_IN, S_BM, S_RANK, S_LANE, S_GROW, S_FRAMES, S_NB, S_SIZES, S_TILE, S_SCRATCH, S_OUT, S_VTMP, S_VBLOB,
+  S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_COUNT
+};
+
+struct QuoinCtx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  void* buf[S_COUNT] = {};
+  size_t cap[S_COUNT] = {};
+  std::mutex mu;
+
+  cudaError_t ensure(int s, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    bytes = (bytes + 255) & ~(size_t)255;
+    if (cap[s] >= bytes) return cudaSuccess;
+    if (buf[s]) {
+      cudaStreamSynchronize(stream);
+      cudaFree(buf[s]);
+      buf[s] = nullptr;
+      cap[s] = 0;
+    }
+    size_t want = bytes + bytes / 4;
+    cudaError_t e = cudaMalloc(&buf[s], want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      e = cudaMalloc(&buf[s], bytes);
+      want = bytes;
+    }
+    if (e == cudaSuccess) cap[s] = want; else cudaGetLastError();
+    return e;
+  }
+  template <class T>
+  T* p(int s) { return reinterpret_cast<T*>(buf[s]); }
+};
+
+namespace {
+
+QuoinCtx* ctx_new() {
+  QuoinCtx* c = new (std::nothrow) QuoinCtx();
+  if (!c) return nullptr;
+  if (cudaGetDevice(&c->device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return nullptr;
+  }
+  return c;
+}
+
+QuoinCtx* g_default = nullptr;
+std::mutex g_default_mu;
+QuoinCtx* default_ctx() {
+  std::lock_guard<std::mutex> l(g_default_mu);
+  if (!g_default) g_default = ctx_new();
+  return g_default;
+}
+QuoinCtx* pick(const QuoinCtx* c) { return c ? const_cast<QuoinCtx*>(c) : default_ctx(); }
+
+struct DeviceScope {
+  int prev = -1;
+  bool changed = false;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) {
+      cudaSetDevice(dev);
+      changed = true;
+    }
+  }
+  ~DeviceScope() {
+    if (changed) cudaSetDevice(prev);
+  }
+};
+
+#define CK(x)                    \
+  do {                           \
+    cudaError_t _e = (x);        \
+    if (_e != cudaSuccess) {     \
+      cudaGetLastError();        \
+      return QUOIN_ERR_CUDA;     \
+    }                            \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Encoder pipeline
+// ---------------------------------------------------------------------------
+struct LaneJob {
+  const uint64_t* lane;  // device, n_valid values
+  uint64_t n_valid;
+  int dtype;
+  uint64_t logical_n;
+  const uint8_t* d_bm;  // device bitmap when the column has nulls, else null
+  int level;
+  uint64_t block_size;  // 0 = adaptive, else clamped to [1, 131072]
+  uint8_t plog2;
+};
+
+uint64_t max_blocks_for(uint64_t n, uint64_t bs) {
+  if (n == 0) return 0;
+  return bs ? (n + bs - 1) / bs : (n + kBaseQuantumH - 1) / kBaseQuantumH;
+}
+
+// Bound on a lane stream's length: header, validity blob and, per block, a
+// 9-byte frame header plus at most the RAW payload (RAW always competes and
+// has no penalty, so no winner is longer).
+uint64_t lane_bound(uint64_t n_valid, uint64_t logical_n, int dtype, bool validity, uint64_t bs) {
+  uint64_t b = 16 + (validity ? 12 + (logical_n + 7) / 8 : 0);
+  b += 9 * max_blocks_for(n_valid, bs) + (uint64_t)lane_bytes_h(dtype) * n_valid;
+  return b + 64;
+}
+
+// Runs the GPU competition and emission for one lane (reference
+// encoder.rs:184-214).  Writes the stream at d_dst and its length to *out_len.
+int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, size_t dst_cap, size_t* out_len) {
+  uint64_t n = j.n_valid;
+  uint64_t bs = j.block_size ? (j.block_size > kMaxBlockValues ? kMaxBlockValues : j.block_size) : 0;
+  uint64_t maxb = max_blocks_for(n, bs);
+  CK(c->ensure(S_MISC, 64 * 8));
+  uint64_t* d_misc = c->p<uint64_t>(S_MISC);  // [0] frames base, [1] frames bytes, [2] blob len
+  if (dst_cap < 16) {
+    *out_len = lane_bound(n, j.logical_n, j.dtype, j.d_bm != nullptr, bs);
+    return QUOIN_ERR_BUFFER_TOO_SMALL;
+  }
+  Bytes16 h;
+  memcpy(h.b, "FCR1", 4);
+  h.b[4] = 2;
+  h.b[5] = j.d_bm ? 1 : 0;
+  h.b[6] = j.plog2;
+  h.b[7] = (uint8_t)j.dtype;
+  for (int i = 0; i < 8; i++) h.b[8 + i] = (uint8_t)(j.logical_n >> (8 * i));
+  launch_put_header(d_dst, h, d_misc, st);
+  if (j.d_bm) {
+    uint64_t ln = j.logical_n, nw = (ln + 31) / 32;
+    uint64_t blob_cap = 1 + (ln + 7) / 8 + 16;
+    if (dst_cap < 16 + 10 + blob_cap) {
+      *out_len = lane_bound(n, ln, j.dtype, true, bs);
+      return QUOIN_ERR_BUFFER_TOO_SMALL;
+    }
+    CK(c->ensure(S_VTMP, (validity_tmp_words(ln) + scan_tile_count(nw) + 16) * 8));
+    CK(c->ensure(S_VBLOB, blob_cap));
+    uint64_t* vtmp = c->p<uint64_t>(S_VTMP);
+    uint64_t* vtile = vtmp + validity_tmp_words(ln);
+    launch_validity_blob(j.d_bm, ln, vtmp, vtile, c->p<uint8_t>(S_VBLOB), d_misc + 2, st);
+    launch_put_validity(d_dst + 16, 16, c->p<uint8_t>(S_VBLOB), d_misc + 2, d_misc, st);
+  }
+  if (maxb == 0) {
+    uint64_t base = 0;
+    CK(cudaMemcpyAsync(&base, d_misc, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *out_len = base;
+    return QUOIN_OK;
+  }
+  CK(c->ensure(S_FRAMES, maxb * sizeof(FrameDesc)));
+  CK(c->ensure(S_NB, 64));
+  CK(c->ensure(S_SIZES, maxb * 8));
+  CK(c->ensure(S_TILE, (scan_tile_count(maxb) + 16) * 8));
+  CK(c->ensure(S_SCRATCH, n * kEncScratchPerValue + 256));
+  CK(c->ensure(S_GROW, (n + kBaseQuantumH - 1) / kBaseQuantumH + 16));
+  FrameDesc* fr = c->p<FrameDesc>(S_FRAMES);
+  uint32_t* nb = c->p<uint32_t>(S_NB);
+  if (!bs) launch_probe_windows(j.lane, n, c->p<uint8_t>(S_GROW), st);
+  launch_plan(c->p<uint8_t>(S_GROW), n, bs, fr, nb, st);
+  launch_compete(j.lane, fr, nb, (uint32_t)maxb, j.dtype, j.level, c->p<uint8_t>(S_SCRATCH), nullptr, st);
+  launch_frame_offsets(fr, nb, (uint32_t)maxb, d_misc, c->p<uint64_t>(S_SIZES), c->p<uint64_t>(S_TILE), d_misc + 1,
+                       st);
+  uint64_t hm[2] = {0, 0};
+  CK(cudaMemcpyAsync(hm, d_misc, 16, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  uint64_t total = hm[0] + hm[1];
+  *out_len = total;
+  if (total > dst_cap) return QUOIN_ERR_BUFFER_TOO_SMALL;
+  launch_emit(j.lane, fr, nb, (uint32_t)maxb, j.dtype, c->p<uint8_t>(S_SCRATCH), d_dst, st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return QUOIN_OK;
+}
+
+int check_level(const QuoinConfig* cfg, int* level, uint64_t* bs, uint8_t* plog2) {
+  int lv = cfg ? cfg->level : QUOIN_LEVEL_FAST;
+  if (lv < 0 || lv > 4) return QUOIN_ERR_BAD_ARG;
+  if (lv >= QUOIN_LEVEL_BALANCED) return QUOIN_ERR_UNSUPPORTED;
+  int64_t b = cfg ? cfg->block_size : 0;
+  int32_t p = cfg ? cfg->predictor_log2 : 16;
+  *level = lv;
+  *bs = b <= 0 ? 0 : (uint64_t)b;
+  *plog2 = (uint8_t)(p < 10 ? 10 : p > 16 ? 16 : p);  // reference lib.rs:236-238
+  return QUOIN_OK;
+}
+
+// Count the valid bits of a device bitmap; fills S_RANK with per-word ranks.
+int device_valid_count(QuoinCtx* c, cudaStream_t st, const uint8_t* d_bm, uint64_t n, uint64_t* n_valid) {
+  uint64_t nw = (n + 31) / 32;
+  CK(c->ensure(S_RANK, nw * 8 + 64));
+  CK(c->ensure(S_TILE, (scan_tile_count(nw) + 16) * 8));
+  CK(c->ensure(S_MISC, 64 * 8));
+  uint64_t* rank = c->p<uint64_t>(S_RANK);
+  launch_word_popcount(d_bm, n, rank, st);
+  launch_scan_sum(rank, rank, nw, c->p<uint64_t>(S_TILE), c->p<uint64_t>(S_MISC) + 8, st);
+  CK(cudaMemcpyAsync(n_valid, c->p<uint64_t>(S_MISC) + 8, 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return QUOIN_OK;
+}
+
+uint64_t column_bound(int wire, uint64_t n, bool validity, uint64_t bs) {
+  if (wire == WT_DEC128 || wire == WT_DEC256) {
+    uint64_t nl = wire == WT_DEC128 ? 2 : 4;
+    return 19 + 32 + (validity ? 12 + (n + 7) / 8 : 0) + nl * (10 + lane_bound(n, n, WT_U64, false, bs)) + 64;
+  }
+  return lane_bound(n, n, wire, validity, bs);
+}
+
+// Decimal container (reference decimal.rs:56-85, 174-212, 339-377).
+int compress_decimal_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, const uint8_t* d_values,
+                            const uint8_t* d_validity, int8_t scale, uint8_t precision, int level, uint64_t bs,
+                            uint8_t plog2, uint8_t* d_dst, size_t dst_cap, size_t* out_len) {
+  int nl = wire == WT_DEC128 ? 2 : 4;
+  uint64_t n_valid = n;
+  const uint8_t* d_bm = nullptr;
+  if (d_validity && n) {
+    int rc = device_valid_count(c, st, d_validity, n, &n_valid);
+    if (rc) return rc;
+    if (n_valid < n) d_bm = d_validity;
+  }
+  CK(c->ensure(S_VTMP, (148 * 4 * 5 + 64) * 8));
+  CK(c->ensure(S_MISC, 64 * 8));
+  uint64_t* d_vmin = c->p<uint64_t>(S_MISC) + 16;
+  launch_decimal_vmin(d_values, nl, d_bm, n, c->p<uint64_t>(S_VTMP), d_vmin, st);
+  CK(c->ensure(S_LIMBS, (uint64_t)nl * n_valid * 8 + 64));
+  uint64_t* limbs = c->p<uint64_t>(S_LIMBS);
+  launch_decimal_split(d_values, nl, d_bm, d_bm ? c->p<uint64_t>(S_RANK) : nullptr, n, d_vmin, limbs, n_valid, st);
+  uint64_t vmin[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(vmin, d_vmin, 32, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::vector<uint8_t> hdr;
+  const char* magic = "FCR1";
+  hdr.insert(hdr.end(), magic, magic + 4);
+  hdr.push_back(2);
+  hdr.push_back((uint8_t)(2 | (d_bm ? 1 : 0)));
+  hdr.push_back(0);
+  hdr.push_back((uint8_t)wire);
+  for (int i = 0; i < 8; i++) hdr.push_back((uint8_t)(n >> (8 * i)));
+  hdr.push_back((uint8_t)scale);
+  hdr.push_back(precision);
+  hdr.push_back((uint8_t)nl);
+  for (int k = 0; k < nl; k++)
+    for (int i = 0; i < 8; i++) hdr.push_back((uint8_t)(vmin[k] >> (8 * i)));
+  uint64_t need_bound = column_bound(wire, n, d_bm != nullptr, bs);
+  if (dst_cap < hdr.size()) {
+    *out_len = need_bound;
+    return QUOIN_ERR_BUFFER_TOO_SMALL;
+  }
+  CK(cudaMemcpyAsync(d_dst, hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
+  uint64_t pos = hdr.size();
+  if (d_bm) {
+    uint64_t nw = (n + 31) / 32;
+    uint64_t blob_cap = 1 + (n + 7) / 8 + 16;
+    if (dst_cap < pos + 10 + blob_cap) {
+      *out_len = need_bound;
+      return QUOIN_ERR_BUFFER_TOO_SMALL;
+    }
+    CK(c->ensure(S_VTMP, (validity_tmp_words(n) + scan_tile_count(nw) + 16) * 8));
+    CK(c->ensure(S_VBLOB, blob_cap));
+    uint64_t* vtmp = c->p<uint64_t>(S_VTMP);
+    uint64_t* d_misc = c->p<uint64_t>(S_MISC);
+    launch_validity_blob(d_bm, n, vtmp, vtmp + validity_tmp_words(n), c->p<uint8_t>(S_VBLOB), d_misc + 2, st);
+    launch_put_validity(d_dst + pos, pos, c->p<uint8_t>(S_VBLOB), d_misc + 2, d_misc + 3, st);
+    uint64_t np = 0;
+    CK(cudaMemcpyAsync(&np, d_misc + 3, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    pos = np;
+  }
+  uint64_t sub_cap = lane_bound(n_valid, n_valid, WT_U64, false, bs);
+  CK(c->ensure(S_LIMBOUT, sub_cap));
+  for (int k = 0; k < nl; k++) {
+    LaneJob j{limbs + (uint64_t)k * n_valid, n_valid, WT_U64, n_valid, nullptr, level, bs, plog2};
+    size_t sl = 0;
+    int rc = encode_lane(c, st, j, c->p<uint8_t>(S_LIMBOUT), sub_cap, &sl);
+    if (rc) return rc;
+    std::vector<uint8_t> vl;
+    put_varint_h(vl, sl);
+    if (pos + vl.size() + sl > dst_cap) {
+      *out_len = need_bound;
+      return QUOIN_ERR_BUFFER_TOO_SMALL;
+    }
+    CK(cudaMemcpyAsync(d_dst + pos, vl.data(), vl.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_dst + pos + vl.size(), c->p<uint8_t>(S_LIMBOUT), sl, cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    pos += vl.size() + sl;
+  }
+  *out_len = pos;
+  return QUOIN_OK;
+}
+
+// compress_column (reference lib.rs:429-455) with device buffers.
+int compress_column_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, const void* d_values,
+                           const uint8_t* d_validity, int8_t scale, uint8_t precision, const QuoinConfig* cfg,
+                           uint8_t* d_dst, size_t dst_cap, size_t* out_len) {
+  if (wire < 0 || wire > 7) return QUOIN_ERR_BAD_ARG;
+  int level;
+  uint64_t bs;
+  uint8_t plog2;
+  int rc = check_level(cfg, &level, &bs, &plog2);
+  if (rc) return rc;
+  if (wire == WT_DEC128 || wire == WT_DEC256)
+    return compress_decimal_device(c, st, wire, n, (const uint8_t*)d_values, d_validity, scale, precision, level, bs,
+                                   plog2, d_dst, dst_cap, out_len);
+  uint64_t n_valid = n;
+  const uint8_t* d_bm = nullptr;
+  if (d_validity && n) {
+    rc = device_valid_count(c, st, d_validity, n, &n_valid);
+    if (rc) return rc;
+    if (n_valid < n) d_bm = d_validity;
+  }
+  const uint64_t* lane;
+  bool direct = !d_bm && lane_bytes_h(wire) == 8 && wire != WT_F32 && ((uintptr_t)d_values & 7) == 0;
+  if (direct) {
+    lane = (const uint64_t*)d_values;
+  } else {
+    CK(c->ensure(S_LANE, n_valid * 8 + 64));
+    launch_lower(d_values, wire, d_bm, d_bm ? c->p<uint64_t>(S_RANK) : nullptr, n, c->p<uint64_t>(S_LANE), st);
+    lane = c->p<uint64_t>(S_LANE);
+  }
+  LaneJob j{lane, n_valid, wire, n, d_bm, level, bs, plog2};
+  return encode_lane(c, st, j, d_dst, dst_cap, out_len);
+}
+
+// ---------------------------------------------------------------------------
+// Decoder: host-side header / validity / frame walk (reference
+// decoder.rs:43-94, decimal.rs:100-168), device decode.
+// ---------------------------------------------------------------------------
+struct LaneIdx {
+  int dtype = 0;
+  uint64_t logical_n = 0, n_total = 0;
+  bool has_validity = false;
+  std::vector<uint8_t> bitmap;  // ceil(n/8), trailing bits cleared
+  std::vector<FrameDesc> frames;
+  bool any_dict = false;
+  uint64_t frame_base = 0;  // index of the first frame in the device table
+};
+
+// Reference validity.rs:73-119.
+int validity_decode_h(const uint8_t* blob, uint64_t blen, uint64_t n, std::vector<uint8_t>& bm) {
+  uint64_t raw_len = (n + 7) / 8;
+  if (n > UINT64_MAX - 7 || raw_len > kMaxBitmapBytes) return K_CORRUPT;
+  if (blen == 0) return K_TRUNC;
+  uint8_t tag = blob[0];
+  const uint8_t* rest = blob + 1;
+  uint64_t rlen = blen - 1;
+  if (tag == 0) {
+    if (rlen < raw_len) return K_TRUNC;
+    bm.assign(rest, rest + raw_len);
+    if (n & 7) bm[raw_len - 1] &= (uint8_t)((1u << (n & 7)) - 1u);
+    return K_OK;
+  }
+  if (tag == 1) {
+    bm.assign(raw_len, 0);
+    uint64_t pos = 0, i = 0;
+    int cur = 0;
+    while (i < n) {
+      uint64_t run;
+      int k = rd_varint_h(rest, rlen, &pos, &run);
+      if (k) return k;
+      if (run > n - i) return K_CORRUPT;
+      uint64_t end = i + run;
+      if (cur == 1) {
+        uint64_t a = i;
+        while (a < end && (a & 7)) { bm[a >> 3] |= (uint8_t)(1u << (a & 7)); a++; }
+        uint64_t full_end = end & ~7ull;
+        if (a < full_end) { memset(bm.data() + (a >> 3), 0xFF, (full_end - a) >> 3); a = full_end; }
+        while (a < end) { bm[a >> 3] |= (uint8_t)(1u << (a & 7)); a++; }
+      }
+      i = end;
+      cur ^= 1;
+    }
+    return K_OK;
+  }
+  return K_CORRUPT;
+}
+
+// Reference format.rs:65-94 + decoder.rs:43-94 for the lane stream at
+// src[base .. base + len).  Frame payload offsets are relative to `src`.
+int parse_lane(const uint8_t* src, uint64_t base, uint64_t len, LaneIdx& L) {
+  const uint8_t* s = src + base;
+  if (len < 16) return K_TRUNC;
+  if (memcmp(s, "FCR1", 4) != 0) return K_BAD_MAGIC;
+  if (s[4] != 2) return K_VERSION;
+  if (s[5] & ~1u) return K_CORRUPT;
+  if (s[6] < 10 || s[6] > 16) return K_CORRUPT;
+  if (s[7] > 7) return K_DTYPE;
+  L.dtype = s[7];
+  L.has_validity = s[5] & 1;
+  L.logical_n = rd64(s + 8);
+  uint64_t pos = 16;
+  L.n_total = L.logical_n;
+  if (L.has_validity) {
+    uint64_t vlen;
+    int k = rd_varint_h(s, len, &pos, &vlen);
+    if (k) return k;
+    if (vlen > len - pos) return K_TRUNC;
+    k = validity_decode_h(s + pos, vlen, L.logical_n, L.bitmap);
+    if (k) return k;
+    pos += vlen;
+    L.n_total = popcount_bits(L.bitmap.data(), L.logical_n);
+  }
+  uint64_t counted = 0;
+  while (counted < L.n_total) {
+    if (len - pos < 9) return K_TRUNC;
+    int mode = s[pos];
+    if (!mode_known(mode)) return K_UNKNOWN_MODE;
+    uint64_t fn = rd32(s + pos + 1), plen = rd32(s + pos + 5);
+    pos += 9;
+    if (fn > kMaxBlockValues) return K_CORRUPT;
+    if (len - pos < plen) return K_TRUNC;
+    FrameDesc f;
+    f.payload_off = base + pos;
+    f.value_off = counted;
+    f.n = (uint32_t)fn;
+    f.plen = (uint32_t)plen;
+    f.mode = (uint32_t)mode;
+    f.aux = 0;
+    L.frames.push_back(f);
+    if (mode == 19) L.any_dict = true;
+    pos += plen;
+    counted += fn;
+    if (counted > L.n_total) return K_CORRUPT;
+  }
+  return K_OK;
+}
+
+}  // namespace
+
+struct QuoinDecodeIndex {
+  int wire = 0;
+  uint64_t n = 0;
+  bool has_validity = false, decimal = false;
+  int8_t scale = 0;
+  uint8_t precision = 0;
+  int nl = 0;
+  uint64_t vmin[4] = {0, 0, 0, 0};
+  uint64_t n_valid = 0;
+  std::vector<uint8_t> bitmap;  // logical bitmap (decimal container or lane)
+  std::vector<LaneIdx> lanes;
+  // device copies (owned when `owned`)
+  bool owned = false;
+  int device = 0;
+  FrameDesc* d_frames = nullptr;
+  uint8_t* d_bm = nullptr;
+  uint64_t* d_rank = nullptr;
+  uint64_t* d_vmin = nullptr;
+};
+
+namespace {
+
+// Reference lib.rs:462-490 + decimal.rs:100-168: parse a whole stream.
+int parse_stream(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
+  if (len > 5 && (src[5] & 2)) {  // decimal container (decimal.rs:39-41)
+    if (len < 8) return K_TRUNC;
+    if (src[7] > 7) return K_DTYPE;
+    int expect = src[7] == WT_DEC256 ? WT_DEC256 : WT_DEC128;
+    if (len < 19) return K_TRUNC;
+    if (memcmp(src, "FCR1", 4) != 0) return K_BAD_MAGIC;
+    if (src[4] != 2) return K_VERSION;
+    if (src[7] != expect) return K_DTYPE_MISMATCH;
+    X.decimal = true;
+    X.wire = expect;
+    X.has_validity = src[5] & 1;
+    X.n = rd64(src + 8);
+    X.scale = (int8_t)src[16];
+    X.precision = src[17];
+    int nl = src[18];
+    if (nl == 0 || nl > 4) return K_CORRUPT;
+    uint64_t vmin_off = 19, pos = 19 + (uint64_t)nl * 8;
+    if (pos > len) return K_TRUNC;
+    X.n_valid = X.n;
+    if (X.has_validity) {
+      uint64_t vlen;
+      int k = rd_varint_h(src, len, &pos, &vlen);
+      if (k) return k;
+      if (vlen > len - pos) return K_TRUNC;
+      k = validity_decode_h(src + pos, vlen, X.n, X.bitmap);
+      if (k) return k;
+      pos += vlen;
+      X.n_valid = popcount_bits(X.bitmap.data(), X.n);
+    }
+    for (int k = 0; k < nl; k++) {
+      uint64_t sl;
+      int r = rd_varint_h(src, len, &pos, &sl);
+      if (r) return r;
+      if (sl > len - pos) return K_TRUNC;
+      LaneIdx L;
+      r = parse_lane(src, pos, sl, L);
+      if (r) return r;
+      if (L.logical_n != X.n_valid) return K_CORRUPT;
+      X.lanes.push_back(std::move(L));
+      pos += sl;
+    }
+    int want = expect == WT_DEC128 ? 2 : 4;
+    if (nl != want) return K_CORRUPT;
+    X.nl = nl;
+    for (int k = 0; k < nl; k++) X.vmin[k] = rd64(src + vmin_off + 8 * k);
+    return K_OK;
+  }
+  LaneIdx L;
+  int r = parse_lane(src, 0, len, L);
+  if (r) return r;
+  if (L.dtype == WT_DEC128 || L.dtype == WT_DEC256) return K_CORRUPT;  // lib.rs:503-505
+  X.wire = L.dtype;
+  X.n = L.logical_n;
+  X.has_validity = L.has_validity;
+  X.bitmap = L.bitmap;
+  X.n_valid = L.n_total;
+  X.lanes.push_back(std::move(L));
+  return K_OK;
+}
+
+uint64_t total_frames(const QuoinDecodeIndex& X) {
+  uint64_t t = 0;
+  for (auto& L : X.lanes) t += L.frames.size();
+  return t;
+}
+
+// Upload the index tables into device buffers (dfr, dbm, drank, dvmin) and
+// compute the validity word ranks on the device.
+int upload_index(QuoinCtx* c, cudaStream_t st, QuoinDecodeIndex& X, FrameDesc* dfr, uint8_t* dbm, uint64_t* drank,
+                 uint64_t* dvmin) {
+  uint64_t fb = 0;
+  for (auto& L : X.lanes) {
+    L.frame_base = fb;
+    if (!L.frames.empty())
+      CK(cudaMemcpyAsync(dfr + fb, L.frames.data(), L.frames.size() * sizeof(FrameDesc), cudaMemcpyHostToDevice, st));
+    fb += L.frames.size();
+  }
+  if (X.has_validity && X.n) {
+    uint64_t nw = (X.n + 31) / 32;
+    CK(cudaMemcpyAsync(dbm, X.bitmap.data(), X.bitmap.size(), cudaMemcpyHostToDevice, st));
+    CK(c->ensure(S_TILE, (scan_tile_count(nw) + 16) * 8));
+    launch_word_popcount(dbm, X.n, drank, st);
+    launch_scan_sum(drank, drank, nw, c->p<uint64_t>(S_TILE), nullptr, st);
+  }
+  if (X.decimal) CK(cudaMemcpyAsync(dvmin, X.vmin, 32, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  return QUOIN_OK;
+}
+
+// Decode the lanes of an uploaded index from the device stream d_src.
+int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, const FrameDesc* dfr, const uint8_t* dbm,
+                   const uint64_t* drank, const uint64_t* dvmin, const uint8_t* d_src, void* d_out,
+                   uint8_t* d_valid_out) {
+  CK(c->ensure(S_ERR, 64));
+  unsigned long long* d_err = c->p<unsigned long long>(S_ERR);
+  CK(cudaMemsetAsync(d_err, 0xFF, 8, st));
+  const uint8_t* bm = X.has_validity ? dbm : nullptr;
+  if (!X.decimal) {
+    const LaneIdx& L = X.lanes[0];
+    bool direct = !X.has_validity && lane_bytes_h(X.wire) == 8 && ((uintptr_t)d_out & 7) == 0;
+    uint64_t* lane_out;
+    if (direct) {
+      lane_out = (uint64_t*)d_out;
+    } else {
+      CK(c->ensure(S_LANE, L.n_total * 8 + 64));
+      lane_out = c->p<uint64_t>(S_LANE);
+    }
+    uint64_t* scr = nullptr;
+    if (L.any_dict) {
+      CK(c->ensure(S_DSCR, L.n_total * 8 + 64));
+      scr = c->p<uint64_t>(S_DSCR);
+    }
+    launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, lane_out, scr, d_err, st);
+    if (!direct && X.n) launch_finalize(lane_out, bm, drank, X.n, X.wire, d_out, st);
+  } else {
+    CK(c->ensure(S_LIMBS, (uint64_t)X.nl * X.n_valid * 8 + 64));
+    uint64_t* limbs = c->p<uint64_t>(S_LIMBS);
+    uint64_t scr_need = 0;
+    for (auto& L : X.lanes)
+      if (L.any_dict) scr_need = L.n_total;
+    uint64_t* scr = nullptr;
+    if (scr_need) {
+      CK(c->ensure(S_DSCR, scr_need * 8 + 64));
+      scr = c->p<uint64_t>(S_DSCR);
+    }
+    for (int k = 0; k < X.nl; k++) {
+      const LaneIdx& L = X.lanes[k];
+      launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), WT_U64, limbs + (uint64_t)k * X.n_valid,
+                           scr, d_err, st);
+    }
+    if (X.n) launch_decimal_combine(limbs, X.n_valid, X.nl, dvmin, bm, drank, X.n, (uint8_t*)d_out, st);
+  }
+  if (d_valid_out && X.has_validity && X.n)
+    CK(cudaMemcpyAsync(d_valid_out, dbm, (X.n + 7) / 8, cudaMemcpyDeviceToDevice, st));
+  unsigned long long herr = 0;
+  CK(cudaMemcpyAsync(&herr, d_err, 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  if (herr != ~0ull) return kind_to_code((int)(herr & 0xFF));
+  return QUOIN_OK;
+}
+
+// Decode a host stream into host buffers (values_out: n native values;
+// validity_out: ceil(n/8) bytes or null).  *X_out receives the parsed index.
+int decompress_host(QuoinCtx* c, const uint8_t* src, uint64_t len, void* values_out, uint8_t* validity_out,
+                    QuoinDecodeIndex* X) {
+  int k = parse_stream(src, len, *X);
+  if (k) return kind_to_code(k);
+  cudaStream_t st = c->stream;
+  uint64_t nf = total_frames(*X);
+  CK(c->ensure(S_DFRAMES, (nf + 1) * sizeof(FrameDesc)));
+  CK(c->ensure(S_DBM, X->bitmap.size() + 16));
+  CK(c->ensure(S_DRANK, ((X->n + 31) / 32 + 1) * 8));
+  CK(c->ensure(S_MISC, 64 * 8));
+  uint64_t* dvmin = c->p<uint64_t>(S_MISC) + 32;
+  int rc = upload_index(c, st, *X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK), dvmin);
+  if (rc) return rc;
+  CK(c->ensure(S_SRC, len + 64));
+  if (len) CK(cudaMemcpyAsync(c->p<uint8_t>(S_SRC), src, len, cudaMemcpyHostToDevice, st));
+  uint64_t out_bytes = X->n * native_width(X->wire);
+  CK(c->ensure(S_OUTVALS, out_bytes + 64));
+  rc = decode_indexed(c, st, *X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK), dvmin,
+                      c->p<uint8_t>(S_SRC), c->p<void>(S_OUTVALS), nullptr);
+  if (rc) return rc;
+  if (out_bytes) CK(cudaMemcpyAsync(values_out, c->p<void>(S_OUTVALS), out_bytes, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (validity_out && X->has_validity && X->n) memcpy(validity_out, X->bitmap.data(), X->bitmap.size());
+  return QUOIN_OK;
+}
+
+// Host-buffer compress of a typed column (wire dtype, native little-endian values).
+int compress_host(QuoinCtx* c, int wire, uint64_t n, const void* values, const uint8_t* validity, int8_t scale,
+                  uint8_t precision, const QuoinConfig* cfg, uint8_t* dst, size_t dst_cap, size_t* out_len) {
+  if (wire < 0 || wire > 7) return QUOIN_ERR_BAD_ARG;
+  cudaStream_t st = c->stream;
+  uint64_t bytes = n * native_width(wire);
+  CK(c->ensure(S_IN, bytes + 64));
+  if (bytes) CK(cudaMemcpyAsync(c->p<uint8_t>(S_IN), values, bytes, cudaMemcpyHostToDevice, st));
+  const uint8_t* d_bm = nullptr;
+  if (validity && n) {
+    CK(c->ensure(S_BM, (n + 7) / 8 + 64));
+    CK(cudaMemcpyAsync(c->p<uint8_t>(S_BM), validity, (n + 7) / 8, cudaMemcpyHostToDevice, st));
+    d_bm = c->p<uint8_t>(S_BM);
+  }
+  uint64_t bs = cfg && cfg->block_size > 0 ? (uint64_t)cfg->block_size : 0;
+  uint64_t bound = column_bound(wire, n, validity != nullptr, bs > kMaxBlockValues ? kMaxBlockValues : bs);
+  CK(c->ensure(S_OUT, bound + 64));
+  size_t len = 0;
+  int rc = compress_column_device(c, st, wire, n, c->p<void>(S_IN), d_bm, scale, precision, cfg, c->p<uint8_t>(S_OUT),
+                                  bound, &len);
+  if (rc) return rc;
+  *out_len = len;
+  if (len > dst_cap) return QUOIN_ERR_BUFFER_TOO_SMALL;
+  if (len) CK(cudaMemcpyAsync(dst, c->p<uint8_t>(S_OUT), len, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return QUOIN_OK;
+}
+
+const QuoinConfig kFastCfg = {QUOIN_LEVEL_FAST, 0, 16};
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* quoin_version(void) { return "quoin-b200 0.1.0 (sm_100a)"; }
+
+size_t quoin_compress_bound(size_t n_values) {
+  size_t a = n_values > SIZE_MAX / 9 ? SIZE_MAX : n_values * 9;
+  return a > SIZE_MAX - 1024 ? SIZE_MAX : a + 1024;
+}
+
+static int compress_f64(const QuoinCtx* cc, const double* src, size_t n, uint8_t* dst, size_t cap, size_t* out_len) {
+  if (!src || !dst || !out_len) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = pick(cc);
+    if (!c) return QUOIN_ERR_PANIC;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    size_t len = 0;
+    int rc = compress_host(c, WT_F64, n, src, nullptr, 0, 0, &kFastCfg, dst, cap, &len);
+    if (rc == QUOIN_ERR_BUFFER_TOO_SMALL) {
+      *out_len = len;
+      return rc;
+    }
+    if (rc) return plain_code(rc);
+    *out_len = len;
+    return QUOIN_OK;
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+static int decompress_f64(const QuoinCtx* cc, const uint8_t* src, size_t len, double* dst, size_t cap,
+                          size_t* out_values) {
+  if (!src || !dst || !out_values) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = pick(cc);
+    if (!c) return QUOIN_ERR_PANIC;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    QuoinDecodeIndex X;
+    int k = parse_stream(src, len, X);
+    if (k) return QUOIN_ERR_CORRUPT;
+    if (X.wire != WT_F64) return QUOIN_ERR_CORRUPT;  // DTypeMismatch (lib.rs:522-527)
+    std::vector<double> tmp;
+    double* out = dst;
+    if (X.n > cap) {
+      tmp.resize(X.n ? X.n : 1);
+      out = tmp.data();
+    }
+    QuoinDecodeIndex Y;
+    int rc = decompress_host(c, src, len, out, nullptr, &Y);
+    if (rc) return plain_code(rc);
+    *out_values = X.n;
+    if (X.n > cap) return QUOIN_ERR_BUFFER_TOO_SMALL;
+    return QUOIN_OK;
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+int quoin_compress(const double* src, size_t n, uint8_t* dst, size_t cap, size_t* out_len) {
+  return compress_f64(nullptr, src, n, dst, cap, out_len);
+}
+int quoin_decompress(const uint8_t* src, size_t len, double* dst, size_t cap, size_t* out_values) {
+  return decompress_f64(nullptr, src, len, dst, cap, out_values);
+}
+int quoin_compress_ctx(const QuoinCtx* ctx, const double* src, size_t n, uint8_t* dst, size_t cap, size_t* out_len) {
+  return compress_f64(ctx, src, n, dst, cap, out_len);
+}
+int quoin_decompress_ctx(const QuoinCtx* ctx, const uint8_t* src, size_t len, double* dst, size_t cap,
+                         size_t* out_values) {
+  return decompress_f64(ctx, src, len, dst, cap, out_values);
+}
+
+ptrdiff_t quoin_decompressed_value_count(const uint8_t* src, size_t len) {
+  if (!src) return QUOIN_ERR_NULL;
+  // Header::read (format.rs:65-94)
+  if (len < 16 || memcmp(src, "FCR1", 4) != 0 || src[4] != 2 || (src[5] & ~1u) || src[6] < 10 || src[6] > 16 ||
+      src[7] > 7)
+    return QUOIN_ERR_CORRUPT;
+  uint64_t n = rd64(src + 8);
+  if (n > (uint64_t)PTRDIFF_MAX) return QUOIN_ERR_CORRUPT;
+  return (ptrdiff_t)n;
+}
+
+QuoinCtx* quoin_ctx_create(size_t threads) {
+  (void)threads;
+  try {
+    return ctx_new();
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+void quoin_ctx_free(QuoinCtx* ctx) {
+  if (!ctx) return;
+  {
+    DeviceScope ds(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (int s = 0; s < S_COUNT; s++)
+      if (ctx->buf[s]) cudaFree(ctx->buf[s]);
+    cudaStreamDestroy(ctx->stream);
+  }
+  delete ctx;
+}
+
+size_t quoin_dtype_width(int32_t dtype) {  // capi/src/typed.rs:50-61
+  switch (dtype) {
+    case QUOIN_DTYPE_BOOL: case QUOIN_DTYPE_I8: case QUOIN_DTYPE_U8: return 1;
+    case QUOIN_DTYPE_I16: case QUOIN_DTYPE_U16: return 2;
+    case QUOIN_DTYPE_I32: case QUOIN_DTYPE_U32: case QUOIN_DTYPE_F32: case QUOIN_DTYPE_DECIMAL32: return 4;
+    case QUOIN_DTYPE_I64: case QUOIN_DTYPE_U64: case QUOIN_DTYPE_F64: case QUOIN_DTYPE_DECIMAL64: return 8;
+    case QUOIN_DTYPE_DECIMAL128: return 16;
+    case QUOIN_DTYPE_DECIMAL256: return 32;
+    default: return 0;
+  }
+}
+
+size_t quoin_typed_compress_bound(int32_t dtype, size_t n) {  // capi/src/typed.rs:65-69
+  size_t w = quoin_dtype_width(dtype);
+  if (w < 8) w = 8;
+  size_t a = n > SIZE_MAX / (w + 1) ? SIZE_MAX : n * (w + 1);
+  return a > SIZE_MAX - 1024 ? SIZE_MAX : a + 1024;
+}
+
+// capi/src/typed.rs:125-174: widen the Arrow dtype to a lane dtype.
+static size_t typed_compress_impl(int32_t dtype, size_t n, const void* values, const uint8_t* validity, int8_t scale,
+                                  uint8_t precision, bool decimal_call, uint8_t* dst, size_t cap) {
+  if (!values || !dst) return 0;
+  try {
+    QuoinCtx* c = default_ctx();
+    if (!c) return 0;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    const uint8_t* in = (const uint8_t*)values;
+    std::vector<uint8_t> conv;
+    int wire;
+    auto widen = [&](size_t from, bool sgn, size_t to) {
+      conv.resize(n * to);
+      for (size_t i = 0; i < n; i++) {
+        int64_t v = 0;
+        uint64_t u = 0;
+        memcpy(&u, in + i * from, from);
+        if (sgn) {
+          int sh = 64 - (int)from * 8;
+          v = (int64_t)(u << sh) >> sh;
+        } else {
+          v = (int64_t)u;
+        }
+        for (size_t b = 0; b < to; b++) conv[i * to + b] = b < 8 ? (uint8_t)((uint64_t)v >> (8 * b)) : (uint8_t)(v < 0 ? 0xFF : 0);
+      }
+      in = conv.data();
+    };
+    if (!decimal_call) {
+      switch (dtype) {
+        case QUOIN_DTYPE_F64: wire = WT_F64; break;
+        case QUOIN_DTYPE_F32: wire = WT_F32; break;
+        case QUOIN_DTYPE_I64: wire = WT_I64; break;
+        case QUOIN_DTYPE_U64: wire = WT_U64; break;
+        case QUOIN_DTYPE_I32: wire = WT_I32; break;
+        case QUOIN_DTYPE_U32: wire = WT_U32; break;
+        case QUOIN_DTYPE_I16: widen(2, true, 4); wire = WT_I32; break;
+        case QUOIN_DTYPE_I8: widen(1, true, 4); wire = WT_I32; break;
+        case QUOIN_DTYPE_U16: widen(2, false, 4); wire = WT_U32; break;
+        case QUOIN_DTYPE_U8: case QUOIN_DTYPE_BOOL: widen(1, false, 4); wire = WT_U32; break;
+        default: return 0;
+      }
+    } else {
+      switch (dtype) {
+        case QUOIN_DTYPE_DECIMAL128: wire = WT_DEC128; break;
+        case QUOIN_DTYPE_DECIMAL256: wire = WT_DEC256; break;
+        case QUOIN_DTYPE_DECIMAL64: widen(8, true, 16); wire = WT_DEC128; break;
+        case QUOIN_DTYPE_DECIMAL32: widen(4, true, 16); wire = WT_DEC128; break;
+        default: return 0;
+      }
+    }
+    size_t len = 0;
+    int rc = compress_host(c, wire, n, in, validity, scale, precision, &kFastCfg, dst, cap, &len);
+    if (rc) return 0;
+    return len;
+  } catch (...) {
+    return 0;
+  }
+}
+
+size_t quoin_typed_compress(int32_t dtype, size_t n, const void* values, const uint8_t* validity, uint8_t* dst,
+                            size_t dst_cap) {
+  return typed_compress_impl(dtype, n, values, validity, 0, 0, false, dst, dst_cap);
+}
+
+size_t quoin_typed_compress_decimal(int32_t dtype, size_t n, const void* values, const uint8_t* validity,
+                                    int8_t scale, uint8_t precision, uint8_t* dst, size_t dst_cap) {
+  return typed_compress_impl(dtype, n, values, validity, scale, precision, true, dst, dst_cap);
+}
+
+// capi/src/typed.rs:232-338
+int quoin_typed_decompress(int32_t dtype, size_t n, const uint8_t* src, size_t src_len, void* values_out,
+                           uint8_t* validity_out) {
+  if (!src || !values_out) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = default_ctx();
+    if (!c) return QUOIN_ERR_PANIC;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    QuoinDecodeIndex X;
+    int k = parse_stream(src, src_len, X);
+    if (k) return QUOIN_ERR_CORRUPT;
+    // (Arrow dtype, decoded column) pairs accepted by scatter_values (typed.rs:256-273)
+    int narrow_to = 0;  // bytes when narrowing
+    bool sgn = false;
+    bool ok = false;
+    switch (dtype) {
+      case QUOIN_DTYPE_F64: ok = X.wire == WT_F64; break;
+      case QUOIN_DTYPE_F32: ok = X.wire == WT_F32; break;
+      case QUOIN_DTYPE_I64: ok = X.wire == WT_I64; break;
+      case QUOIN_DTYPE_U64: ok = X.wire == WT_U64; break;
+      case QUOIN_DTYPE_I32: ok = X.wire == WT_I32; break;
+      case QUOIN_DTYPE_U32: ok = X.wire == WT_U32; break;
+      case QUOIN_DTYPE_I16: ok = X.wire == WT_I32; narrow_to = 2; sgn = true; break;
+      case QUOIN_DTYPE_I8: ok = X.wire == WT_I32; narrow_to = 1; sgn = true; break;
+      case QUOIN_DTYPE_U16: ok = X.wire == WT_U32; narrow_to = 2; break;
+      case QUOIN_DTYPE_U8: case QUOIN_DTYPE_BOOL: ok = X.wire == WT_U32; narrow_to = 1; break;
+      case QUOIN_DTYPE_DECIMAL128: ok = X.wire == WT_DEC128; break;
+      case QUOIN_DTYPE_DECIMAL256: ok = X.wire == WT_DEC256; break;
+      case QUOIN_DTYPE_DECIMAL64: ok = X.wire == WT_DEC128; narrow_to = 8; sgn = true; break;
+      case QUOIN_DTYPE_DECIMAL32: ok = X.wire == WT_DEC128; narrow_to = 4; sgn = true; break;
+      default: ok = false;
+    }
+    (void)sgn;
+    std::vector<uint8_t> full(X.n * native_width(X.wire) + 8);
+    QuoinDecodeIndex Y;
+    int rc = decompress_host(c, src, src_len, full.data(), nullptr, &Y);
+    if (rc) return plain_code(rc);
+    if (!ok || X.n != n) return QUOIN_ERR_CORRUPT;
+    uint32_t w = native_width(X.wire);
+    uint8_t* out = (uint8_t*)values_out;
+    if (!narrow_to) {
+      memcpy(out, full.data(), n * w);
+    } else {
+      for (size_t i = 0; i < n; i++) memcpy(out + i * narrow_to, full.data() + i * w, narrow_to);  // `as` truncation
+    }
+    if (validity_out) {  // typed.rs:280-300
+      size_t nbytes = (n + 7) / 8;
+      if (X.has_validity) {
+        size_t take = X.bitmap.size() < nbytes ? X.bitmap.size() : nbytes;
+        memcpy(validity_out, X.bitmap.data(), take);
+        if (take < nbytes) memset(validity_out + take, 0, nbytes - take);
+      } else if (nbytes) {
+        memset(validity_out, 0xFF, nbytes);
+        if (n % 8) validity_out[nbytes - 1] = (uint8_t)((1u << (n % 8)) - 1u);
+      }
+    }
+    return QUOIN_OK;
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+// ---------------- B200 extensions ----------------
+
+int quoin_b200_compress_column(QuoinCtx* ctx, int32_t wire, size_t n, const void* values, const uint8_t* validity,
+                               int8_t scale, uint8_t precision, const QuoinConfig* cfg, uint8_t* dst, size_t dst_cap,
+                               size_t* out_len) {
+  if (!out_len || (!values && n) || !dst) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = pick(ctx);
+    if (!c) return QUOIN_ERR_CUDA;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    static const uint8_t kZero[8] = {0};
+    return compress_host(c, wire, n, values ? values : kZero, validity, scale, precision, cfg, dst, dst_cap, out_len);
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+int quoin_b200_stream_info(const uint8_t* src, size_t len, int32_t* wire, uint64_t* n, int32_t* has_validity,
+                           int8_t* scale, uint8_t* precision) {
+  if (!src || !wire || !n || !has_validity || !scale || !precision) return QUOIN_ERR_NULL;
+  if (len > 5 && (src[5] & 2)) {
+    if (len < 19) return QUOIN_ERR_TRUNCATED;
+    if (src[7] > 7) return QUOIN_ERR_UNSUPPORTED_DTYPE;
+    *wire = src[7];
+    *n = rd64(src + 8);
+    *has_validity = src[5] & 1;
+    *scale = (int8_t)src[16];
+    *precision = src[17];
+    return QUOIN_OK;
+  }
+  if (len < 16) return QUOIN_ERR_TRUNCATED;
+  if (memcmp(src, "FCR1", 4) != 0) return QUOIN_ERR_BAD_MAGIC;
+  if (src[4] != 2) return QUOIN_ERR_UNSUPPORTED_VERSION;
+  if ((src[5] & ~1u) || src[6] < 10 || src[6] > 16) return QUOIN_ERR_CORRUPT_PAYLOAD;
+  if (src[7] > 7) return QUOIN_ERR_UNSUPPORTED_DTYPE;
+  *wire = src[7];
+  *n = rd64(src + 8);
+  *has_validity = src[5] & 1;
+  *scale = 0;
+  *precision = 0;
+  return QUOIN_OK;
+}
+
+int quoin_b200_decompress_column(QuoinCtx* ctx, const uint8_t* src, size_t len, void* values_out,
+                                 uint8_t* validity_out) {
+  if (!src || !values_out) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = pick(ctx);
+    if (!c) return QUOIN_ERR_CUDA;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    QuoinDecodeIndex X;
+    return decompress_host(c, src, len, values_out, validity_out, &X);
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+int quoin_b200_compress_column_device(QuoinCtx* ctx, int32_t wire, size_t n, const void* d_values,
+                                      const uint8_t* d_validity, int8_t scale, uint8_t precision,
+                                      const QuoinConfig* cfg, uint8_t* d_dst, size_t dst_cap, size_t* out_len,
+                                      void* stream) {
+  if (!out_len || (!d_values && n) || !d_dst) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = pick(ctx);
+    if (!c) return QUOIN_ERR_CUDA;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    return compress_column_device(c, st, wire, n, d_values, d_validity, scale, precision, cfg, d_dst, dst_cap,
+                                  out_len);
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+int quoin_b200_index_create(QuoinCtx* ctx, const uint8_t* src, size_t len, QuoinDecodeIndex** out) {
+  if (!src || !out) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = pick(ctx);
+    if (!c) return QUOIN_ERR_CUDA;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    QuoinDecodeIndex* X = new QuoinDecodeIndex();
+    int k = parse_stream(src, len, *X);
+    if (k) {
+      delete X;
+      return kind_to_code(k);
+    }
+    X->owned = true;
+    X->device = c->device;
+    uint64_t nf = total_frames(*X);
+    bool ok = cudaMalloc(&X->d_frames, (nf + 1) * sizeof(FrameDesc)) == cudaSuccess &&
+              cudaMalloc(&X->d_bm, X->bitmap.size() + 16) == cudaSuccess &&
+              cudaMalloc(&X->d_rank, ((X->n + 31) / 32 + 1) * 8) == cudaSuccess &&
+              cudaMalloc(&X->d_vmin, 64) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      quoin_b200_index_free(X);
+      return QUOIN_ERR_CUDA;
+    }
+    int rc = upload_index(c, c->stream, *X, X->d_frames, X->d_bm, X->d_rank, X->d_vmin);
+    if (rc) {
+      quoin_b200_index_free(X);
+      return rc;
+    }
+    *out = X;
+    return QUOIN_OK;
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+void quoin_b200_index_free(QuoinDecodeIndex* X) {
+  if (!X) return;
+  if (X->owned) {
+    DeviceScope ds(X->device);
+    if (X->d_frames) cudaFree(X->d_frames);
+    if (X->d_bm) cudaFree(X->d_bm);
+    if (X->d_rank) cudaFree(X->d_rank);
+    if (X->d_vmin) cudaFree(X->d_vmin);
+  }
+  delete X;
+}
+
+int quoin_b200_index_info(const QuoinDecodeIndex* X, int32_t* wire, uint64_t* n, int32_t* has_validity) {
+  if (!X || !wire || !n || !has_validity) return QUOIN_ERR_NULL;
+  *wire = X->wire;
+  *n = X->n;
+  *has_validity = X->has_validity;
+  return QUOIN_OK;
+}
+
+int quoin_b200_decompress_indexed_device(QuoinCtx* ctx, const QuoinDecodeIndex* X, const uint8_t* d_src,
+                                         void* d_values_out, uint8_t* d_validity_out, void* stream) {
+  if (!X || !d_src || !d_values_out) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = pick(ctx);
+    if (!c) return QUOIN_ERR_CUDA;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    return decode_indexed(c, st, *X, X->d_frames, X->d_bm, X->d_rank, X->d_vmin, d_src, d_values_out, d_validity_out);
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+void quoin_b200_mode_win_counts(uint64_t out[64]) {
+  if (!out) return;
+  memset(out, 0, 64 * 8);
+  unsigned long long* d = device_win_counters();
+  if (!d) return;
+  if (cudaMemcpy(out, d, 64 * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    memset(out, 0, 64 * 8);
+  }
+}
+
+void quoin_b200_reset_mode_win_counts(void) {
+  unsigned long long* d = device_win_counters();
+  if (d && cudaMemset(d, 0, 64 * 8) != cudaSuccess) cudaGetLastError();
+}
+
+uint64_t quoin_b200_kernel_launches(void) { return launches_total(); }
+
+}  // extern "C"

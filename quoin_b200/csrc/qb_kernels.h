@@ -1,0 +1,76 @@
+// Host-side launchers of the quoin B200 kernels (declared here, defined in the
+// .cu files).  All take an explicit CUDA stream and only plain device pointers.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "qb_layout.h"
+
+namespace qb {
+
+// ---- decoder (qb_decode.cu) ----
+void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, uint64_t* lane,
+                          uint64_t* scratch, unsigned long long* err, cudaStream_t st);
+void launch_word_popcount(const uint8_t* bm, uint64_t n, uint64_t* cnt, cudaStream_t st);
+void launch_finalize(const uint64_t* lane, const uint8_t* bm, const uint64_t* word_rank, uint64_t n, int dtype,
+                     void* out, cudaStream_t st);
+void launch_decimal_combine(const uint64_t* limbs, uint64_t limb_stride, int nlimbs, const uint64_t* vmin,
+                            const uint8_t* bm, const uint64_t* word_rank, uint64_t n, uint8_t* out, cudaStream_t st);
+
+// ---- encoder (qb_encode.cu) ----
+// Per-block scratch the competition may use: 32 bytes per lane value.
+constexpr uint64_t kEncScratchPerValue = 32;
+
+void launch_probe_windows(const uint64_t* lane, uint64_t n, uint8_t* grow, cudaStream_t st);
+void launch_plan(const uint8_t* grow, uint64_t n, uint64_t fixed_bs, FrameDesc* frames, uint32_t* nb,
+                 cudaStream_t st);
+void launch_compete(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, int dtype,
+                    int level, uint8_t* scratch, unsigned long long* wins, cudaStream_t st);
+// `base` (device) holds the byte offset at which the first frame starts.
+void launch_frame_offsets(FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, const uint64_t* base,
+                          uint64_t* sizes_tmp, uint64_t* tile_tmp, uint64_t* total, cudaStream_t st);
+void launch_emit(const uint64_t* lane, const FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, int dtype,
+                 uint8_t* scratch, uint8_t* out, cudaStream_t st);
+
+// ---- lowering / validity (qb_lower.cu) ----
+// Lower n native values (dtype width) to the u64 lane, keeping only positions
+// whose validity bit is set when `word_rank` is given (compaction).
+void launch_lower(const void* values, int dtype, const uint8_t* bm, const uint64_t* word_rank, uint64_t n,
+                  uint64_t* lane, cudaStream_t st);
+// Decimal: compacted limbs of (v - vmin).  `vmin` is computed on device.
+void launch_decimal_vmin(const uint8_t* values, int nlimbs, const uint8_t* bm, uint64_t n, uint64_t* vmin_tmp,
+                         uint64_t* vmin, cudaStream_t st);
+void launch_decimal_split(const uint8_t* values, int nlimbs, const uint8_t* bm, const uint64_t* word_rank,
+                          uint64_t n, const uint64_t* vmin, uint64_t* limbs, uint64_t limb_stride, cudaStream_t st);
+// Validity run-length blob (reference validity.rs:40-70): the blob is written
+// to out (tag + payload) and its length to *blob_len.
+void launch_validity_blob(const uint8_t* bm, uint64_t n, uint64_t* tmp, uint64_t* tile_tmp, uint8_t* out,
+                          uint64_t* blob_len, cudaStream_t st);
+uint64_t validity_tmp_words(uint64_t n);
+void launch_write_bytes(uint8_t* dst, const uint8_t* src_dev, uint64_t len, cudaStream_t st);
+
+// Mode win counters (reference src/diag.rs).
+unsigned long long* device_win_counters();
+
+// Small writers used by the stream assembly.
+struct Bytes16 {
+  uint8_t b[16];
+};
+void launch_put_header(uint8_t* dst, Bytes16 hdr, uint64_t* d_base, cudaStream_t st);
+// Writes varint(*blob_len) ++ blob at dst and sets *d_base = dst_off + varint + blob.
+void launch_put_validity(uint8_t* dst, uint64_t dst_off, const uint8_t* blob, const uint64_t* blob_len,
+                         uint64_t* d_base, cudaStream_t st);
+
+// Exclusive prefix sum of n u64 (in may alias out); grand total to *grand.
+void launch_scan_sum(const uint64_t* in, uint64_t* out, uint64_t n, uint64_t* tile_tmp, uint64_t* grand,
+                     cudaStream_t st);
+inline uint64_t scan_tile_count(uint64_t n) {
+  uint64_t t = (n + 2047) / 2048;  // kScanTile
+  return t ? t : 1;
+}
+
+// Number of kernels launched by this library (all launchers add to it).
+void count_launches(uint64_t k);
+uint64_t launches_total();
+
+}  // namespace qb

@@ -1,0 +1,319 @@
+// Column lowering and validity handling on the device: typed values -> u64
+// lane with null compaction (reference lib.rs:389-403,446-454,
+// validity.rs:122-127), the decimal limb split (decimal.rs:174-212,339-377)
+// and the validity run-length blob (validity.rs:40-70).
+#include "qb_common.cuh"
+#include "qb_kernels.h"
+#include "qb_scan.cuh"
+
+namespace qb {
+
+__device__ inline uint64_t lower_one(const uint8_t* base, uint64_t i, int dtype) {
+  switch (dtype) {
+    case DT_I32: return (uint64_t)(int64_t)reinterpret_cast<const int32_t*>(base)[i];
+    case DT_U32: return (uint64_t)reinterpret_cast<const uint32_t*>(base)[i];
+    case DT_F32: return f32bits_to_f64bits(reinterpret_cast<const uint32_t*>(base)[i]);
+    default: return reinterpret_cast<const uint64_t*>(base)[i];
+  }
+}
+
+// Warp w handles bitmap word w; lane l position 32w + l.
+__global__ void k_lower(const uint8_t* __restrict__ values, int dtype, const uint8_t* __restrict__ bm,
+                        const uint64_t* __restrict__ word_rank, uint64_t n, uint64_t* __restrict__ lane) {
+  uint64_t nw = (n + 31) / 32, nbytes = (n + 7) / 8;
+  int l = threadIdx.x & 31;
+  uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t w = warp; w < nw; w += nwarps) {
+    uint64_t i = w * 32 + l;
+    if (bm) {
+      uint32_t byte = (w * 4 + (l >> 3) < nbytes) ? bm[w * 4 + (l >> 3)] : 0u;
+      uint32_t bits = 0;
+      for (int k = 0; k < 4; k++) bits |= __shfl_sync(0xffffffffu, byte, k * 8) << (8 * k);
+      if (i < n && ((bits >> l) & 1u)) lane[word_rank[w] + __popc(bits & ((1u << l) - 1u))] = lower_one(values, i, dtype);
+    } else if (i < n) {
+      lane[i] = lower_one(values, i, dtype);
+    }
+  }
+}
+
+static unsigned grid_for_words(uint64_t n) {
+  uint64_t nw = (n + 31) / 32;
+  uint64_t g = (nw + 7) / 8;
+  if (g > 148ull * 32) g = 148ull * 32;
+  return g ? (unsigned)g : 1u;
+}
+
+void launch_lower(const void* values, int dtype, const uint8_t* bm, const uint64_t* word_rank, uint64_t n,
+                  uint64_t* lane, cudaStream_t st) {
+  if (n) k_lower<<<grid_for_words(n), 256, 0, st>>>((const uint8_t*)values, dtype, bm, word_rank, n, lane);
+  count_launches(n ? 1 : 0);
+}
+
+// ---------------------------------------------------------------------------
+// Decimal: signed minimum over valid values, then limbs of (v - vmin).
+// ---------------------------------------------------------------------------
+struct L4 {
+  uint64_t l[4];
+};
+__device__ inline L4 load_dec(const uint8_t* values, uint64_t i, int nl) {
+  const uint64_t* p = reinterpret_cast<const uint64_t*>(values + i * 8ull * nl);
+  L4 r;
+  for (int k = 0; k < 4; k++) r.l[k] = k < nl ? p[k] : (uint64_t)((int64_t)p[nl - 1] >> 63);
+  return r;
+}
+__device__ inline bool lt_signed4(const L4& a, const L4& b) {  // reference decimal.rs:254-269
+  uint64_t sa = a.l[3] >> 63, sb = b.l[3] >> 63;
+  if (sa != sb) return sa == 1;
+  for (int i = 3; i >= 0; i--)
+    if (a.l[i] != b.l[i]) return a.l[i] < b.l[i];
+  return false;
+}
+__device__ inline bool is_valid_bit(const uint8_t* bm, uint64_t i) { return !bm || ((bm[i >> 3] >> (i & 7)) & 1); }
+
+// Partial minima: tmp[b] = {valid flag, 4 limbs}.
+__global__ void k_decimal_vmin_partial(const uint8_t* __restrict__ values, int nl, const uint8_t* __restrict__ bm,
+                                       uint64_t n, uint64_t* __restrict__ tmp) {
+  __shared__ L4 s_v[256];
+  __shared__ int s_ok[256];
+  L4 best;
+  int ok = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (!is_valid_bit(bm, i)) continue;
+    L4 x = load_dec(values, i, nl);
+    if (!ok || lt_signed4(x, best)) best = x;
+    ok = 1;
+  }
+  s_ok[threadIdx.x] = ok;
+  if (ok) s_v[threadIdx.x] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int any = 0;
+    L4 m;
+    for (int t = 0; t < (int)blockDim.x; t++)
+      if (s_ok[t] && (!any || lt_signed4(s_v[t], m))) {
+        m = s_v[t];
+        any = 1;
+      }
+    tmp[blockIdx.x * 5] = any;
+    for (int k = 0; k < 4; k++) tmp[blockIdx.x * 5 + 1 + k] = any ? m.l[k] : 0;
+  }
+}
+__global__ void k_decimal_vmin_final(const uint64_t* __restrict__ tmp, int nparts, uint64_t* __restrict__ vmin) {
+  if (threadIdx.x || blockIdx.x) return;
+  int any = 0;
+  L4 m;
+  for (int k = 0; k < 4; k++) m.l[k] = 0;
+  for (int b = 0; b < nparts; b++) {
+    if (!tmp[b * 5]) continue;
+    L4 x;
+    for (int k = 0; k < 4; k++) x.l[k] = tmp[b * 5 + 1 + k];
+    if (!any || lt_signed4(x, m)) m = x;
+    any = 1;
+  }
+  for (int k = 0; k < 4; k++) vmin[k] = m.l[k];
+}
+
+void launch_decimal_vmin(const uint8_t* values, int nlimbs, const uint8_t* bm, uint64_t n, uint64_t* vmin_tmp,
+                         uint64_t* vmin, cudaStream_t st) {
+  int parts = 148 * 4;
+  k_decimal_vmin_partial<<<parts, 256, 0, st>>>(values, nlimbs, bm, n, vmin_tmp);
+  k_decimal_vmin_final<<<1, 32, 0, st>>>(vmin_tmp, parts, vmin);
+  count_launches(2);
+}
+
+// limbs[k * stride + j] = limb k of (v_i - vmin) for the j-th valid value i.
+__global__ void k_decimal_split(const uint8_t* __restrict__ values, int nl, const uint8_t* __restrict__ bm,
+                                const uint64_t* __restrict__ word_rank, uint64_t n, const uint64_t* __restrict__ vmin,
+                                uint64_t* __restrict__ limbs, uint64_t stride) {
+  uint64_t nw = (n + 31) / 32, nbytes = (n + 7) / 8;
+  int l = threadIdx.x & 31;
+  uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  uint64_t vm[4];
+  for (int k = 0; k < 4; k++) vm[k] = vmin[k];
+  for (uint64_t w = warp; w < nw; w += nwarps) {
+    uint64_t i = w * 32 + l;
+    uint64_t j = i;
+    bool valid = i < n;
+    if (bm) {
+      uint32_t byte = (w * 4 + (l >> 3) < nbytes) ? bm[w * 4 + (l >> 3)] : 0u;
+      uint32_t bits = 0;
+      for (int k = 0; k < 4; k++) bits |= __shfl_sync(0xffffffffu, byte, k * 8) << (8 * k);
+      valid = valid && ((bits >> l) & 1u);
+      j = word_rank[w] + __popc(bits & ((1u << l) - 1u));
+    }
+    if (!valid) continue;
+    const uint64_t* p = reinterpret_cast<const uint64_t*>(values + i * 8ull * nl);
+    uint64_t borrow = 0;
+    for (int k = 0; k < nl; k++) {  // reference decimal.rs:281-293 (sub with borrow)
+      uint64_t a = p[k], b = vm[k];
+      uint64_t d1 = a - b;
+      uint64_t b1 = a < b;
+      uint64_t d2 = d1 - borrow;
+      uint64_t b2 = d1 < borrow;
+      limbs[k * stride + j] = d2;
+      borrow = b1 | b2;
+    }
+  }
+}
+
+void launch_decimal_split(const uint8_t* values, int nlimbs, const uint8_t* bm, const uint64_t* word_rank,
+                          uint64_t n, const uint64_t* vmin, uint64_t* limbs, uint64_t limb_stride, cudaStream_t st) {
+  if (n) k_decimal_split<<<grid_for_words(n), 256, 0, st>>>(values, nlimbs, bm, word_rank, n, vmin, limbs, limb_stride);
+  count_launches(n ? 1 : 0);
+}
+
+// ---------------------------------------------------------------------------
+// Validity blob: the smaller of [1] ++ LEB128 alternating run lengths
+// (starting with a null run) or [0] ++ the raw bitmap bytes.
+// ---------------------------------------------------------------------------
+__device__ inline uint32_t bm_word(const uint8_t* bm, uint64_t w, uint64_t n) {
+  uint64_t nbytes = (n + 7) / 8;
+  uint32_t bits = 0;
+  for (int k = 0; k < 4; k++)
+    if (w * 4 + k < nbytes) bits |= (uint32_t)bm[w * 4 + k] << (8 * k);
+  uint64_t rem = n - w * 32;
+  if (rem < 32) bits &= (1u << rem) - 1u;
+  return bits;
+}
+// Transition mask of word w: bit j set when bit (32w + j) differs from its
+// predecessor (the bit before position 0 is taken as 0, i.e. a null).
+__device__ inline uint32_t trans_mask(const uint8_t* bm, uint64_t w, uint64_t n) {
+  uint32_t b = bm_word(bm, w, n);
+  uint32_t prev = w ? (bm_word(bm, w - 1, n) >> 31) : 0u;
+  uint32_t t = b ^ ((b << 1) | prev);
+  uint64_t rem = n - w * 32;
+  if (rem < 32) t &= (1u << rem) - 1u;
+  return t;
+}
+
+__global__ void k_vb_last(const uint8_t* __restrict__ bm, uint64_t n, uint64_t* __restrict__ last) {
+  uint64_t nw = (n + 31) / 32;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t t = trans_mask(bm, w, n);
+    last[w] = t ? w * 32 + (31 - __clz(t)) : 0ull;
+  }
+}
+__global__ void k_vb_sizes(const uint8_t* __restrict__ bm, uint64_t n, const uint64_t* __restrict__ prevpos,
+                           uint64_t* __restrict__ sizes) {
+  uint64_t nw = (n + 31) / 32;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t t = trans_mask(bm, w, n);
+    uint64_t prev = prevpos[w], bytes = 0;
+    while (t) {
+      uint64_t p = w * 32 + (__ffs(t) - 1);
+      t &= t - 1;
+      bytes += varint_len(p - prev);
+      prev = p;
+    }
+    sizes[w] = bytes;
+  }
+}
+// state[0] = last transition (max-scan grand), state[1] = bytes of runs that
+// end at a transition (sum-scan grand); writes the blob and its length.
+__global__ void k_vb_write(const uint8_t* __restrict__ bm, uint64_t n, const uint64_t* __restrict__ prevpos,
+                           const uint64_t* __restrict__ offs, const uint64_t* __restrict__ state,
+                           uint8_t* __restrict__ out, uint64_t* __restrict__ blob_len) {
+  uint64_t nw = (n + 31) / 32, raw_len = (n + 7) / 8;
+  uint64_t t_last = state[0];
+  uint64_t rle_len = state[1] + varint_len(n - t_last);
+  bool rle = rle_len < raw_len;
+  uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, gsz = (uint64_t)gridDim.x * blockDim.x;
+  if (gtid == 0) {
+    out[0] = rle ? 1 : 0;
+    *blob_len = 1 + (rle ? rle_len : raw_len);
+  }
+  if (rle) {
+    for (uint64_t w = gtid; w < nw; w += gsz) {
+      uint32_t t = trans_mask(bm, w, n);
+      uint64_t prev = prevpos[w], pos = 1 + offs[w];
+      while (t) {
+        uint64_t p = w * 32 + (__ffs(t) - 1);
+        t &= t - 1;
+        uint64_t v = p - prev;
+        do {
+          uint8_t b = (uint8_t)(v & 0x7f);
+          v >>= 7;
+          out[pos++] = v ? (b | 0x80) : b;
+        } while (v);
+        prev = p;
+      }
+    }
+    if (gtid == 0) {
+      uint64_t v = n - t_last, pos = 1 + state[1];
+      do {
+        uint8_t b = (uint8_t)(v & 0x7f);
+        v >>= 7;
+        out[pos++] = v ? (b | 0x80) : b;
+      } while (v);
+    }
+  } else {
+    for (uint64_t i = gtid; i < raw_len; i += gsz) out[1 + i] = bm[i];
+  }
+}
+
+uint64_t validity_tmp_words(uint64_t n) {
+  uint64_t nw = (n + 31) / 32;
+  return 3 * nw + scan_tiles(nw) + 8;
+}
+
+void launch_validity_blob(const uint8_t* bm, uint64_t n, uint64_t* tmp, uint64_t* tile_tmp, uint8_t* out,
+                          uint64_t* blob_len, cudaStream_t st) {
+  uint64_t nw = (n + 31) / 32;
+  uint64_t* last = tmp;
+  uint64_t* sizes = tmp + nw;
+  uint64_t* state = tmp + 2 * nw;  // [0] t_last, [1] bytes
+  unsigned g = (unsigned)qmin((nw + 255) / 256, 148ull * 16);
+  if (g == 0) g = 1;
+  k_vb_last<<<g, 256, 0, st>>>(bm, n, last);
+  scan_exclusive<ScanMax>(last, last, nw, tile_tmp, state, st);
+  k_vb_sizes<<<g, 256, 0, st>>>(bm, n, last, sizes);
+  scan_exclusive<ScanSum>(sizes, sizes, nw, tile_tmp, state + 1, st);
+  k_vb_write<<<g, 256, 0, st>>>(bm, n, last, sizes, state, out, blob_len);
+  count_launches(9);
+}
+
+void launch_scan_sum(const uint64_t* in, uint64_t* out, uint64_t n, uint64_t* tile_tmp, uint64_t* grand,
+                     cudaStream_t st) {
+  scan_exclusive<ScanSum>(in, out, n ? n : 1, tile_tmp, grand, st);
+  count_launches(3);
+}
+
+void launch_write_bytes(uint8_t* dst, const uint8_t* src_dev, uint64_t len, cudaStream_t st) {
+  if (len) cudaMemcpyAsync(dst, src_dev, len, cudaMemcpyDeviceToDevice, st);
+}
+
+__global__ void k_put_header(uint8_t* dst, Bytes16 hdr, uint64_t* d_base) {
+  if (threadIdx.x < 16) dst[threadIdx.x] = hdr.b[threadIdx.x];
+  if (threadIdx.x == 0 && d_base) *d_base = 16;
+}
+void launch_put_header(uint8_t* dst, Bytes16 hdr, uint64_t* d_base, cudaStream_t st) {
+  k_put_header<<<1, 32, 0, st>>>(dst, hdr, d_base);
+  count_launches(1);
+}
+
+__global__ void k_put_validity(uint8_t* dst, uint64_t dst_off, const uint8_t* __restrict__ blob,
+                               const uint64_t* __restrict__ blob_len, uint64_t* d_base) {
+  uint64_t len = *blob_len;
+  uint32_t vl = varint_len(len);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    uint64_t v = len;
+    uint32_t k = 0;
+    do {
+      uint8_t b = (uint8_t)(v & 0x7f);
+      v >>= 7;
+      dst[k++] = v ? (b | 0x80) : b;
+    } while (v);
+    *d_base = dst_off + vl + len;
+  }
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x)
+    dst[vl + i] = blob[i];
+}
+void launch_put_validity(uint8_t* dst, uint64_t dst_off, const uint8_t* blob, const uint64_t* blob_len,
+                         uint64_t* d_base, cudaStream_t st) {
+  k_put_validity<<<148 * 4, 256, 0, st>>>(dst, dst_off, blob, blob_len, d_base);
+  count_launches(1);
+}
+
+}  // namespace qb
