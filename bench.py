@@ -1,0 +1,405 @@
+#!/usr/bin/env python3
+"""Benchmark: quoin column compression/decompression on B200.
+
+Workload (one "step"): the integer-lane configuration — three columns of
+N = 67,108,864 values each (i64 ns timestamps with Poisson jitter, u64
+base+U[0,2^k) runs, i32 Zipf categories in geometric runs), each 10 % null,
+compressed at Level::Fast (the byte-identical level) and decompressed again.
+
+  value   = uncompressed bytes of the three columns / (encode + decode time)
+            with inputs resident in HBM (device API), CUDA events on the
+            launching stream, max over ranks;
+  e2e     = the same metric through the host-buffer C ABI
+            (quoin_b200_compress_column / quoin_b200_decompress_column) from
+            pinned host memory, host<->device copies inside the timed region.
+
+`--impl reference` times the reference algorithm's CPU implementation (the
+C restatement in oracle/, since the Rust reference cannot be built here) on
+all host cores, on a bounded sample of the same columns.
+
+Run: python bench.py [--gpus N --steps K --warmup W] (torchrun for N > 1).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "encode+decode GB/s (uncompressed bytes; Level::Fast, bit-exact round trip)"
+N_DEFAULT = 67_108_864
+TIMER_NAMES = ["compete", "emit", "decode", "finalize", "lower", "plan", "validity", "other"]
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Reference arm: the reference's CPU algorithm (C restatement) on host cores.
+# ---------------------------------------------------------------------------
+def cpu_reference_run(cols, threads: int, sample: int):
+    from oracle import oracle as O
+    enc_s = dec_s = 0.0
+    nbytes = 0
+    for name, dt, v, bm in cols:
+        vs = v[:sample]
+        bs = None if bm is None else bm[: (sample + 7) // 8]
+        t0 = time.perf_counter()
+        s = O.compress_column(vs, dt, bs, level=O.LEVEL_FAST, threads=threads)
+        t1 = time.perf_counter()
+        O.decompress_column(s, threads=threads)
+        t2 = time.perf_counter()
+        enc_s += t1 - t0
+        dec_s += t2 - t1
+        nbytes += vs.nbytes
+    return nbytes, enc_s, dec_s
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    from quoin_b200 import synth
+    threads = os.cpu_count() or 1
+    sample = args.cpu_sample
+    cols = synth.config_columns("1", sample)
+    for _ in range(args.warmup):
+        cpu_reference_run(cols, threads, sample)
+    tot_b = 0
+    tot_s = 0.0
+    e_s = d_s = 0.0
+    for _ in range(args.steps):
+        b, e, d = cpu_reference_run(cols, threads, sample)
+        tot_b += b
+        tot_s += e + d
+        e_s += e
+        d_s += d
+    gbs = tot_b / tot_s / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(gbs, 4), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot_s / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64/uint64/int32",
+        "data": "synthetic",
+        "config": {"workload": "config1 integer lanes (i64 timestamps, u64 runs, i32 categories), 10% nulls, "
+                               "Level::Fast", "values_per_column": sample, "columns": 3},
+        "encode_gbs": round(tot_b / e_s / 1e9, 4), "decode_gbs": round(tot_b / d_s / 1e9, 4),
+        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": f"first {sample} values of each config-1 column, oracle C restatement, "
+                                   f"{threads} threads over plan_blocks ranges / frames"},
+        "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the Rust reference cannot be built here (no cargo, unvendored crates); its CPU path is timed "
+                "through the repository's C restatement of the same algorithm",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    import quoin_b200 as Q
+    from quoin_b200 import synth
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    n = args.n
+    cols = synth.config_columns("1", n)
+    L = Q.lib
+    stream = torch.cuda.Stream(device=dev)
+    ctx = ctypes.c_void_p(L.quoin_ctx_create(0))
+    cfg = Q._QuoinConfig(int(Q.Level.FAST), 0, 16)
+    P = ctypes.c_void_p
+
+    gcols = []
+    for name, wire, v, bm in cols:
+        w = Q.NATIVE_WIDTH[wire]
+        d_vals = torch.from_numpy(np.ascontiguousarray(v).view(np.uint8).copy()).to(dev)
+        d_bm = torch.from_numpy(bm.copy()).to(dev) if bm is not None else None
+        cap = Q._stream_bound(wire, n, bm is not None)
+        d_dst = torch.empty(cap, dtype=torch.uint8, device=dev)
+        d_out = torch.empty(n * w, dtype=torch.uint8, device=dev)
+        d_vout = torch.empty((n + 7) // 8, dtype=torch.uint8, device=dev)
+        gcols.append(dict(name=name, wire=wire, v=v, bm=bm, w=w, d_vals=d_vals, d_bm=d_bm, cap=cap, d_dst=d_dst,
+                          d_out=d_out, d_vout=d_vout, len=0, idx=None))
+    torch.cuda.synchronize()
+
+    def compress_all():
+        for c in gcols:
+            olen = ctypes.c_size_t()
+            rc = L.quoin_b200_compress_column_device(
+                ctx, c["wire"], n, P(c["d_vals"].data_ptr()), P(c["d_bm"].data_ptr()) if c["d_bm"] is not None else None,
+                0, 0, ctypes.byref(cfg), P(c["d_dst"].data_ptr()), c["cap"], ctypes.byref(olen), P(stream.cuda_stream))
+            if rc:
+                raise Q.Error(rc)
+            c["len"] = olen.value
+
+    def decompress_all():
+        for c in gcols:
+            rc = L.quoin_b200_decompress_indexed_device(ctx, c["idx"], P(c["d_dst"].data_ptr()),
+                                                        P(c["d_out"].data_ptr()), P(c["d_vout"].data_ptr()),
+                                                        P(stream.cuda_stream))
+            if rc:
+                raise Q.Error(rc)
+
+    # First pass: compress, build the decode index from the host copy, verify
+    # the round trip bit for bit (null slots decode to 0).
+    with torch.cuda.stream(stream):
+        compress_all()
+    host_streams = []
+    for c in gcols:
+        hs = c["d_dst"][: c["len"]].cpu().numpy().tobytes()
+        host_streams.append(hs)
+        idx = P()
+        rc = L.quoin_b200_index_create(ctx, hs, len(hs), ctypes.byref(idx))
+        if rc:
+            raise Q.Error(rc)
+        c["idx"] = idx
+    with torch.cuda.stream(stream):
+        decompress_all()
+    torch.cuda.synchronize()
+    bit_exact = True
+    for c in gcols:
+        got = c["d_out"].cpu().numpy()
+        want = np.ascontiguousarray(c["v"]).view(np.uint8).reshape(n, c["w"]).copy()
+        if c["bm"] is not None:
+            valid = np.unpackbits(c["bm"], bitorder="little")[:n].astype(bool)
+            want[~valid] = 0
+            if c["d_vout"].cpu().numpy().tobytes() != c["bm"].tobytes():
+                bit_exact = False
+        if got.tobytes() != want.tobytes():
+            bit_exact = False
+    raw_bytes = sum(int(np.asarray(c["v"]).nbytes) for c in gcols)
+    stream_bytes = sum(c["len"] for c in gcols)
+
+    for _ in range(args.warmup):
+        with torch.cuda.stream(stream):
+            compress_all()
+            decompress_all()
+    torch.cuda.synchronize()
+
+    # Timed region.
+    L.quoin_b200_timing_enable(1)
+    launches0 = Q.kernel_launches()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for k in range(args.steps):
+            compress_all()
+            ev[2 * k + 1].record(stream)
+            decompress_all()
+            ev[2 * k + 2].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    launches = Q.kernel_launches() - launches0
+    ms_arr = (ctypes.c_double * 8)()
+    calls_arr = (ctypes.c_uint64 * 8)()
+    L.quoin_b200_timing_read(ms_arr, calls_arr, 8)
+    L.quoin_b200_timing_enable(0)
+    enc_ms = sum(ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps))
+    dec_ms = sum(ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps))
+    total_ms = ev[0].elapsed_time(ev[-1])
+    if world > 1:
+        t = torch.tensor([total_ms, enc_ms, dec_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, enc_ms, dec_ms = t.tolist()
+    value = raw_bytes * world * args.steps / (total_ms / 1e3) / 1e9
+
+    # Roofline of the dominant kernel class (algorithmic bytes / event time).
+    peak, peak_kind = load_peaks()
+    n_valid = [int(np.unpackbits(c["bm"], bitorder="little")[:n].sum()) if c["bm"] is not None else n for c in gcols]
+    alg = {
+        "compete": sum(nv * 8 for nv in n_valid),
+        "emit": sum(nv * 8 for nv in n_valid) + stream_bytes,
+        "decode": stream_bytes + sum(nv * 8 for nv in n_valid),
+        "finalize": sum(nv * 8 + (n + 7) // 8 + n * c["w"] for nv, c in zip(n_valid, gcols)),
+    }
+    per_class = {TIMER_NAMES[i]: (ms_arr[i], int(calls_arr[i])) for i in range(8)}
+    dom = max(alg, key=lambda k: per_class[k][0])
+    dom_ms, dom_calls = per_class[dom]
+    achieved = alg[dom] * args.steps / (dom_ms / 1e3) / 1e9 if dom_ms else 0.0
+
+    # e2e through the host-buffer C ABI with pinned host memory.
+    pinned = []
+    for c in gcols:
+        hv = torch.from_numpy(np.ascontiguousarray(c["v"]).view(np.uint8).copy()).pin_memory()
+        hb = torch.from_numpy(c["bm"].copy()).pin_memory() if c["bm"] is not None else None
+        hdst = torch.empty(c["len"] + (1 << 20), dtype=torch.uint8).pin_memory()
+        hout = torch.empty(n * c["w"], dtype=torch.uint8).pin_memory()
+        hvout = torch.empty((n + 7) // 8, dtype=torch.uint8).pin_memory()
+        pinned.append((hv, hb, hdst, hout, hvout))
+
+    def e2e_step():
+        h2d = d2h = 0
+        for c, (hv, hb, hdst, hout, hvout) in zip(gcols, pinned):
+            olen = ctypes.c_size_t()
+            rc = L.quoin_b200_compress_column(ctx, c["wire"], n, P(hv.data_ptr()),
+                                              P(hb.data_ptr()) if hb is not None else None, 0, 0,
+                                              ctypes.byref(cfg), P(hdst.data_ptr()), hdst.numel(), ctypes.byref(olen))
+            if rc:
+                raise Q.Error(rc)
+            rc = L.quoin_b200_decompress_column(ctx, P(hdst.data_ptr()), olen.value, P(hout.data_ptr()),
+                                                P(hvout.data_ptr()))
+            if rc:
+                raise Q.Error(rc)
+            h2d += hv.numel() + (hb.numel() if hb is not None else 0) + olen.value
+            d2h += olen.value + hout.numel() + (hvout.numel() if hb is not None else 0)
+        return h2d, d2h
+
+    e2e_step()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        h2d, d2h = e2e_step()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = t.item()
+    e2e_gbs = raw_bytes * world * args.steps / e2e_s / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        sample = args.cpu_sample
+        runs = [cpu_reference_run(cols, threads, sample) for _ in range(3)]
+        gb = sorted(b / (e + d) / 1e9 for b, e, d in runs)[1]
+        cpu = {"value": round(gb, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": f"first {sample} values of each column (of {n}), oracle C restatement, {threads} threads, "
+                         f"median of 3 compress+decompress runs"}
+
+    for c in gcols:
+        L.quoin_b200_index_free(c["idx"])
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64/uint64/int32", "data": "synthetic",
+            "config": {"workload": "config1 integer lanes: i64 timestamps (1e6+Poisson(5000) steps), u64 "
+                                   "base+U[0,2^k) runs, i32 Zipf(1.1) 64-category geometric runs; 10% nulls; "
+                                   "Level::Fast", "values_per_column": n, "columns": 3, "global_values": n * 3 * world,
+                       "l2": "inputs (1.25 GiB per rank) exceed the 126 MB L2; no flush needed",
+                       "parallelism": f"replicas x{world} (independent columns per rank)"},
+            "encode_gbs": round(raw_bytes * world * args.steps / (enc_ms / 1e3) / 1e9, 3),
+            "decode_gbs": round(raw_bytes * world * args.steps / (dec_ms / 1e3) / 1e9, 3),
+            "ratio": round(raw_bytes / stream_bytes, 4), "bit_exact": bit_exact,
+            "kernel_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in per_class.items()},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": None, "launches_per_step": dom_calls // max(args.steps, 1)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "timing": "wall clock around synchronous host-buffer C-ABI calls, pinned host memory"},
+            "gpu_launches": int(launches // max(args.steps, 1) * args.steps),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    L.quoin_ctx_free(ctx)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT, help="values per column")
+    ap.add_argument("--cpu-sample", type=int, default=1 << 24)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_gpu(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

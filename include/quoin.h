@@ -165,6 +165,12 @@ int quoin_b200_stream_info(const uint8_t *src, size_t src_len, int32_t *wire_dty
                            uint64_t *n, int32_t *has_validity, int8_t *scale,
                            uint8_t *precision);
 
+/* Host-only validation of a whole stream: header, validity blob and frame
+ * table walk (src/decoder.rs:43-94, src/decimal.rs:100-168), no device work.
+ * Returns the wire dtype, logical n and validity flag, or the error kind. */
+int quoin_b200_parse(const uint8_t *src, size_t src_len, int32_t *wire_dtype, uint64_t *n,
+                     int32_t *has_validity);
+
 /* Replaces decompress_column(&[u8]) (src/lib.rs:462-508) for host buffers:
  * writes n native values to values_out (null slots 0) and, when the stream has
  * a validity bitmap and validity_out is non-NULL, ceil(n/8) bitmap bytes. */
@@ -203,6 +209,14 @@ void quoin_b200_reset_mode_win_counts(void);
 
 /* Number of GPU kernels this library has launched in the calling process. */
 uint64_t quoin_b200_kernel_launches(void);
+
+/* Per-kernel-class device time, measured with CUDA events recorded on the
+ * launching stream around each launch: 0 competition, 1 emission, 2 block
+ * decode, 3 final scatter/narrow, 4 lowering, 5 probe+plan, 6 validity,
+ * 7 other.  enable(1) resets and starts recording; read() returns the number
+ * of classes written (ms totals and call counts). */
+void quoin_b200_timing_enable(int on);
+int quoin_b200_timing_read(double *ms_out, uint64_t *calls_out, int n);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -1952,6 +1952,9 @@ static int decompress_lane(const uint8_t *src, size_t len, int threads, int *dty
     uint64_t n64;
     int rc = header_read(src, len, &dtype, &hv, &n64);
     if (rc) return rc;
+    /* The reference fails the logical-length allocation (decoder.rs:105-106,
+     * validity.rs:135-136) and reports CorruptPayload for absurd lengths. */
+    if (n64 > ((uint64_t)1 << 36)) return OQ_CORRUPT;
     size_t logical_n = (size_t)n64;
     size_t pos = 16;
     uint8_t *bm = NULL;
@@ -2163,6 +2166,7 @@ static int decimal_decompress(const uint8_t *src, size_t len, int expect, int th
     if (src[7] > 7) return OQ_UNSUPPORTED_DTYPE;
     if (src[7] != expect) return OQ_DTYPE_MISMATCH;
     uint64_t n64 = rd_u64(src + 8);
+    if (n64 > ((uint64_t)1 << 36)) return OQ_CORRUPT;
     size_t logical_n = (size_t)n64;
     *scale = (int8_t)src[16];
     *precision = src[17];

@@ -111,6 +111,10 @@ def _load():
                                          ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int8),
                                          ctypes.POINTER(ctypes.c_uint8)]
     L.quoin_b200_decompress_column.argtypes = [P, P, S, P, P]
+    L.quoin_b200_parse.argtypes = [P, S, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint64),
+                                   ctypes.POINTER(ctypes.c_int32)]
+    L.quoin_b200_timing_enable.argtypes = [ctypes.c_int]
+    L.quoin_b200_timing_read.argtypes = [P, P, ctypes.c_int]
     L.quoin_b200_compress_column_device.argtypes = [P, ctypes.c_int32, S, P, P, ctypes.c_int8, ctypes.c_uint8,
                                                     ctypes.POINTER(_QuoinConfig), P, S, ctypes.POINTER(S), P]
     L.quoin_b200_index_create.argtypes = [P, P, S, ctypes.POINTER(P)]
@@ -150,14 +154,17 @@ def _bitmap(validity, n: int):
     return a
 
 
-def _stream_bound(wire: int, n: int, has_validity: bool) -> int:
+def _stream_bound(wire: int, n: int, has_validity: bool, block_size: Optional[int] = None) -> int:
+    """Upper bound of a stream's length: header, validity blob, and per block a
+    9-byte frame header plus at most the RAW payload (no winner is longer)."""
     lb = 4 if wire in (I32, U32, F32) else 8
+    bs = min(max(int(block_size), 1), MAX_BLOCK_SIZE) if block_size else 32768
+    blocks = (n + bs - 1) // bs
     vb = 12 + (n + 7) // 8 if has_validity else 0
-    lane = 16 + vb + 9 * n + lb * n + 64
     if wire in (DECIMAL128, DECIMAL256):
         nl = 2 if wire == DECIMAL128 else 4
-        return 19 + 32 + vb + nl * (10 + 16 + 9 * n + 8 * n + 64) + 64
-    return lane
+        return 19 + 32 + vb + nl * (10 + 16 + 9 * blocks + 8 * n + 64) + 64
+    return 16 + vb + 9 * blocks + lb * n + 64
 
 
 def compress_column(values, validity=None, cfg: Optional[Config] = None, dtype: Optional[int] = None,
@@ -176,7 +183,7 @@ def compress_column(values, validity=None, cfg: Optional[Config] = None, dtype: 
             raise TypeError(f"unsupported column dtype {arr.dtype}")
     n = arr.nbytes // NATIVE_WIDTH[dtype]
     bm = _bitmap(validity, n)
-    cap = _stream_bound(dtype, n, bm is not None)
+    cap = _stream_bound(dtype, n, bm is not None, (cfg or Config()).block_size)
     out = np.empty(max(cap, 16), dtype=np.uint8)
     olen = ctypes.c_size_t()
     c = _cfg(cfg)
@@ -212,13 +219,13 @@ def stream_info(stream: bytes):
 
 def decompress_column(stream: bytes, ctx=None) -> DecodedColumn:
     """Decompress a stream from ``compress_column`` (reference src/lib.rs:462-508)."""
+    buf = np.frombuffer(stream, dtype=np.uint8) if stream else np.zeros(1, np.uint8)
+    pw, pn, phv = ctypes.c_int32(), ctypes.c_uint64(), ctypes.c_int32()
+    _check(lib.quoin_b200_parse(buf.ctypes.data, len(stream), ctypes.byref(pw), ctypes.byref(pn), ctypes.byref(phv)))
     wire, n, hv, sc, pr = stream_info(stream)
-    if n > (1 << 40):
-        raise Error(-14)
     w = NATIVE_WIDTH[wire]
     out = np.zeros(max(n * w, 8), dtype=np.uint8)
     bm = np.zeros(max((n + 7) // 8, 1), dtype=np.uint8) if hv else None
-    buf = np.frombuffer(stream, dtype=np.uint8)
     _check(lib.quoin_b200_decompress_column(ctx, buf.ctypes.data, len(stream), out.ctypes.data,
                                             None if bm is None else bm.ctypes.data))
     raw = out[: n * w]

@@ -1,251 +1,137 @@
 // Block decoder (reference src/decoder.rs:145-190 and the per-codec decode
-// functions).  One CTA per frame: thread 0 walks and validates the frame's
-// sub-block chain (the sub-block sizes are data-dependent), then the whole CTA
-// unpacks the FastLanes-transposed words with coalesced loads and stores.
+// functions).  Two kernels:
+//  * k_walk_frames — one thread per frame: validates the frame's payload
+//    structure in the reference's check order and records the byte offsets of
+//    its FastLanes sub-blocks (the sub-block sizes are data-dependent, so this
+//    is a short dependent walk; every frame walks concurrently);
+//  * k_decode_frames — one CTA per frame, one warp per 1024-value sub-block:
+//    coalesced unpack of the lane-transposed words, delta / RLE prefix sums
+//    across sub-blocks, ALP / FLOAT_MULT reconstruction, exception patching,
+//    and a byte-parallel LEB128 + prefix-XOR decoder for XORZ.
 // Every payload read is bounded by the frame's plen; malformed frames set an
 // error word instead of faulting.
 #include "qb_common.cuh"
-#include "qb_layout.h"
 #include "qb_kernels.h"
+#include "qb_layout.h"
 
 namespace qb {
 
 constexpr int kDecThreads = 256;
+constexpr int kDecWarps = kDecThreads / 32;
 constexpr int kMaxSubs = kMaxBlock / kSub;  // 128
 constexpr int kDictSmem = 2048;
+constexpr int kXorzChunk = kDecThreads * 8;  // payload bytes per XORZ step
 
-struct DecSmem {
-  uint32_t offs[kMaxSubs + 1];
-  uint32_t offs2[kMaxSubs + 1];
-  uint64_t buf[kSub];
-  uint64_t warp_tot[kDecThreads / 32 + 1];
-  uint64_t dict8[8];
-  uint64_t dict[kDictSmem];
-  uint64_t sc[8];  // scalars broadcast from thread 0
+// Per-frame results of the walk (device memory, one per frame).
+struct FrameAux {
   uint32_t err;
-  uint32_t flag;
+  uint32_t pad;
+  uint64_t a, b, c, d;  // mode-specific scalars
+  uint64_t dict8[8];    // ALP-RD dictionary
+  uint32_t offs[2][kMaxSubs + 1];  // chain 0 / chain 1 sub-block header offsets (payload-relative)
 };
 
 // ---------------------------------------------------------------------------
-// FoR sub-block chain (reference codecs/for_bitpack.rs:108-157).  Thread 0
-// only.  Sub-block k = [width u8][min u64][128*width bytes].
+// FoR sub-block chain (reference codecs/for_bitpack.rs:108-157), walked over
+// p[pos .. bound): varint(n) then sub-blocks [width u8][min u64][128*width B].
 // ---------------------------------------------------------------------------
-__device__ uint32_t for_walk(const uint8_t* p, uint64_t plen, uint64_t pos, uint64_t n_values, uint32_t* offs,
-                             uint64_t* end) {
+__device__ uint32_t for_walk(const uint8_t* p, uint64_t bound, uint64_t pos, uint64_t n_values, uint32_t* offs) {
   uint64_t n64;
-  uint32_t e = rd_varint(p, plen, &pos, &n64);
+  uint32_t e = rd_varint(p, bound, &pos, &n64);
   if (e) return e;
   if (n64 != n_values) return E_CORRUPT;
   uint32_t nsub = (uint32_t)((n_values + kSub - 1) / kSub);
   for (uint32_t k = 0; k < nsub; k++) {
-    if (pos >= plen) return E_TRUNCATED;
+    if (pos >= bound) return E_TRUNCATED;
     uint32_t w = p[pos];
     if (w > 64) return E_CORRUPT;
-    if (plen - pos - 1 < 8) return E_TRUNCATED;
+    if (bound - pos - 1 < 8) return E_TRUNCATED;
     uint64_t need = 128ull * w;
-    if (plen - pos - 9 < need) return E_TRUNCATED;
+    if (bound - pos - 9 < need) return E_TRUNCATED;
     offs[k] = (uint32_t)pos;
     pos += 9 + need;
   }
   offs[nsub] = (uint32_t)pos;
-  if (end) *end = pos;
   return E_OK;
 }
 
-// Unpack one FoR sub-block whose header starts at p[off]; calls f(i, min + r)
-// for i < count.  Thread t owns FastLanes lane (t % 32) [or t % 16 for the
-// 64-bit kernel], so each warp load/store touches consecutive words.
-template <class F>
-__device__ inline void for_unpack(const uint8_t* p, uint32_t off, uint32_t count, F f) {
-  uint32_t w = p[off];
-  uint64_t mn = ld_u64(p + off + 1);
-  const uint8_t* words = p + off + 9;
-  int t = threadIdx.x;
-  if (w == 0) {
-    for (uint32_t i = t; i < count; i += kDecThreads) f(i, mn);
-  } else if (w <= 32) {
-    uint32_t mask = w == 32 ? 0xFFFFFFFFu : ((1u << w) - 1u);
-    int l = t & 31;
-#pragma unroll 4
-    for (int r = t >> 5; r < 32; r += kDecThreads / 32) {
-      uint32_t idx = (uint32_t)(r * 32 + l);
-      uint32_t bit = (uint32_t)r * w, word = bit >> 5, sh = bit & 31;
-      uint32_t v = ld_u32(words + 4u * (word * 32u + l)) >> sh;
-      if (sh + w > 32) v |= ld_u32(words + 4u * ((word + 1) * 32u + l)) << (32 - sh);
-      v &= mask;
-      if (idx < count) f(idx, mn + (uint64_t)v);
-    }
-  } else {
-    uint64_t mask = w == 64 ? ~0ull : ((1ull << w) - 1ull);
-    int l = t & 15;
-#pragma unroll 4
-    for (int r = t >> 4; r < 64; r += kDecThreads / 16) {
-      uint32_t idx = (uint32_t)(r * 16 + l);
-      uint32_t bit = (uint32_t)r * w, word = bit >> 6, sh = bit & 63;
-      uint64_t v = ld_u64(words + 8u * (word * 16u + l)) >> sh;
-      if (sh + w > 64) v |= ld_u64(words + 8u * ((word + 1) * 16u + l)) << (64 - sh);
-      v &= mask;
-      if (idx < count) f(idx, mn + v);
-    }
-  }
-}
-
-__device__ inline uint32_t bcast_err(DecSmem& S, uint32_t e) {
-  if (threadIdx.x == 0) S.err = e;
-  __syncthreads();
-  uint32_t r = S.err;
-  __syncthreads();
-  return r;
-}
-
-// Block-wide inclusive prefix of S.buf[0..count) (u64, wrapping) plus carry;
-// writes the running values with `write(i, value)`.  Returns the new carry.
-template <class W>
-__device__ inline uint64_t chunk_prefix(DecSmem& S, uint32_t count, uint64_t carry, W write) {
-  int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  uint32_t i0 = (uint32_t)t * 4;
-  uint64_t v[4], s = 0;
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    v[k] = (i0 + k < count) ? S.buf[i0 + k] : 0;
-    s += v[k];
-  }
-  uint64_t inc = s;
-  for (int o = 1; o < 32; o <<= 1) {
-    uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += u;
-  }
-  if (lane == 31) S.warp_tot[wid] = inc;
-  __syncthreads();
-  uint64_t wo = 0;
-  for (int w = 0; w < wid; w++) wo += S.warp_tot[w];
-  uint64_t tot = 0;
-  for (int w = 0; w < kDecThreads / 32; w++) tot += S.warp_tot[w];
-  uint64_t run = carry + wo + inc - s;
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    run += v[k];
-    if (i0 + k < count) write(i0 + k, run);
-  }
-  __syncthreads();
-  return carry + tot;
-}
-
-// FoR-decode n values at p[pos..plen) into dst (generic pointer).
-__device__ uint32_t dec_for(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t pos, uint64_t n, uint64_t* dst) {
-  uint32_t e = E_OK;
-  if (threadIdx.x == 0) e = for_walk(p, plen, pos, n, S.offs, nullptr);
-  e = bcast_err(S, e);
+// ALP sub-block chain (reference codecs/alp.rs:168-248).
+__device__ uint32_t alp_walk(const uint8_t* p, uint64_t plen, uint64_t n, uint32_t* offs) {
+  uint64_t pos = 0, n64;
+  uint32_t e = rd_varint(p, plen, &pos, &n64);
   if (e) return e;
+  if (n64 != n) return E_CORRUPT;
   uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
   for (uint32_t k = 0; k < nsub; k++) {
-    uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-    uint64_t* o = dst + (size_t)k * kSub;
-    for_unpack(p, S.offs[k], cnt, [&](uint32_t i, uint64_t v) { o[i] = v; });
+    uint64_t count = qmin(kSub, n - (uint64_t)k * kSub);
+    if (pos >= plen) return E_TRUNCATED;
+    uint32_t ee = p[pos];
+    if (pos + 1 >= plen) return E_TRUNCATED;
+    uint32_t ff = p[pos + 1];
+    if (ee > 18 || ff > ee) return E_CORRUPT;
+    if (plen < pos + 4) return E_TRUNCATED;
+    uint32_t exc = ld_u16(p + pos + 2);
+    if (plen < pos + 12 || pos + 12 >= plen) return E_TRUNCATED;
+    uint32_t w = p[pos + 12];
+    if (w > 32) return E_CORRUPT;
+    offs[k] = (uint32_t)pos;
+    uint64_t q = pos + 13;
+    if (plen - q < 128ull * w) return E_TRUNCATED;
+    q += 128ull * w;
+    for (uint32_t x = 0; x < exc; x++) {
+      if (plen < q + 2 || plen < q + 10) return E_TRUNCATED;
+      if (ld_u16(p + q) >= count) return E_CORRUPT;
+      q += 10;
+    }
+    pos = q;
   }
   return E_OK;
 }
 
-// DeltaBitpack (reference codecs/delta_bitpack.rs:48-64).
-__device__ uint32_t dec_delta(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, uint64_t* dst) {
-  if (plen < 8) return E_TRUNCATED;
-  uint64_t base = ld_u64(p);
-  const uint8_t* q = p + 8;
-  uint64_t qlen = plen - 8;
+// One thread per frame.
+__global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDesc* __restrict__ frames, int nf,
+                              int dtype, FrameAux* __restrict__ aux, unsigned long long* __restrict__ err) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  FrameDesc d = frames[f];
+  const uint8_t* p = stream + d.payload_off;
+  uint64_t plen = d.plen, n = d.n;
+  FrameAux& A = aux[f];
   uint32_t e = E_OK;
-  if (threadIdx.x == 0) e = for_walk(q, qlen, 0, n, S.offs, nullptr);
-  e = bcast_err(S, e);
-  if (e) return e;
-  uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
-  uint64_t carry = base;
-  for (uint32_t k = 0; k < nsub; k++) {
-    uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-    for_unpack(q, S.offs[k], cnt, [&](uint32_t i, uint64_t v) { S.buf[i] = unzigzag64(v); });
-    __syncthreads();
-    uint64_t* o = dst + (size_t)k * kSub;
-    carry = chunk_prefix(S, cnt, carry, [&](uint32_t i, uint64_t v) { o[i] = v; });
-  }
-  return E_OK;
-}
-
-// ALP (reference codecs/alp.rs:168-248).
-__device__ uint32_t dec_alp(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, uint64_t* dst) {
-  uint32_t e = E_OK;
-  if (threadIdx.x == 0) {
-    uint64_t pos = 0, n64;
-    e = rd_varint(p, plen, &pos, &n64);
-    if (!e && n64 != n) e = E_CORRUPT;
-    uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
-    for (uint32_t k = 0; !e && k < nsub; k++) {
-      uint64_t count = qmin(kSub, n - (uint64_t)k * kSub);
-      if (pos >= plen) { e = E_TRUNCATED; break; }
-      uint32_t ee = p[pos];
-      if (pos + 1 >= plen) { e = E_TRUNCATED; break; }
-      uint32_t ff = p[pos + 1];
-      if (ee > 18 || ff > ee) { e = E_CORRUPT; break; }
-      if (plen < pos + 4) { e = E_TRUNCATED; break; }
-      uint32_t exc = ld_u16(p + pos + 2);
-      if (plen < pos + 12 || pos + 12 >= plen) { e = E_TRUNCATED; break; }
-      uint32_t w = p[pos + 12];
-      if (w > 32) { e = E_CORRUPT; break; }
-      S.offs[k] = (uint32_t)pos;
-      uint64_t q = pos + 13;
-      if (plen - q < 128ull * w) { e = E_TRUNCATED; break; }
-      q += 128ull * w;
-      for (uint32_t x = 0; x < exc; x++) {
-        if (plen < q + 2 || plen < q + 10) { e = E_TRUNCATED; break; }
-        if (ld_u16(p + q) >= count) { e = E_CORRUPT; break; }
-        q += 10;
-      }
-      pos = q;
+  switch (d.mode) {
+    case M_RAW:
+      if (plen != n * lane_bytes(dtype)) e = E_CORRUPT;
+      break;
+    case M_CONST:
+      if (plen != 8) e = E_CORRUPT;
+      break;
+    case M_STRIDE:
+      if (plen != 16) e = E_CORRUPT;
+      break;
+    case M_XORZ:
+      break;  // validated by the parallel decoder
+    case M_FOR_BITPACK:
+      e = for_walk(p, plen, 0, n, A.offs[0]);
+      break;
+    case M_DELTA_BITPACK:  // delta_bitpack.rs:48-64
+      if (plen < 8) { e = E_TRUNCATED; break; }
+      e = for_walk(p, plen, 8, n, A.offs[0]);
+      break;
+    case M_FLOAT_MULT: {  // float_mult.rs:100-133
+      if (plen < 1 || plen < 2) { e = E_TRUNCATED; break; }
+      uint32_t tag = p[0], si = p[1];
+      if (si >= 7) { e = E_CORRUPT; break; }
+      if (tag == 1) { e = E_UNSUPPORTED; break; }
+      if (tag != 0) { e = E_CORRUPT; break; }
+      A.a = si;
+      e = for_walk(p, plen, 2, n, A.offs[0]);
+      break;
     }
-  }
-  e = bcast_err(S, e);
-  if (e) return e;
-  uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
-  for (uint32_t k = 0; k < nsub; k++) {
-    uint32_t off = S.offs[k];
-    int ee = p[off], ff = p[off + 1];
-    uint32_t exc = ld_u16(p + off + 2);
-    int64_t mn = (int64_t)ld_u64(p + off + 4);
-    uint32_t w = p[off + 12];
-    uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-    uint64_t* o = dst + (size_t)k * kSub;
-    const uint8_t* words = p + off + 13;
-    int t = threadIdx.x, l = t & 31;
-    if (w == 0) {
-      uint64_t v = f64_bits(alp_decode_value(mn, ee, ff));
-      for (uint32_t i = t; i < cnt; i += kDecThreads) o[i] = v;
-    } else {
-      uint32_t mask = w == 32 ? 0xFFFFFFFFu : ((1u << w) - 1u);
-      for (int r = t >> 5; r < 32; r += kDecThreads / 32) {
-        uint32_t idx = (uint32_t)(r * 32 + l);
-        uint32_t bit = (uint32_t)r * w, word = bit >> 5, sh = bit & 31;
-        uint32_t v = ld_u32(words + 4u * (word * 32u + l)) >> sh;
-        if (sh + w > 32) v |= ld_u32(words + 4u * ((word + 1) * 32u + l)) << (32 - sh);
-        v &= mask;
-        int64_t d = (int64_t)((uint64_t)mn + (uint64_t)v);
-        if (idx < cnt) o[idx] = f64_bits(alp_decode_value(d, ee, ff));
-      }
-    }
-    if (exc) {
-      __syncthreads();
-      if (threadIdx.x == 0) {  // sequential patch keeps "last exception wins"
-        const uint8_t* xp = words + 128u * w;
-        for (uint32_t x = 0; x < exc; x++) o[ld_u16(xp + 10 * x)] = ld_u64(xp + 10 * x + 2);
-      }
-      __syncthreads();
-    }
-  }
-  return E_OK;
-}
-
-// ALP-RD with bit-packed code and right streams (reference codecs/alp_rd.rs:208-285).
-__device__ uint32_t dec_alprd(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, uint64_t* dst) {
-  uint32_t e = E_OK;
-  if (threadIdx.x == 0) {
-    uint64_t pos = 0;
-    do {
+    case M_ALP:
+      e = alp_walk(p, plen, n, A.offs[0]);
+      break;
+    case M_ALP_RD: {  // alp_rd.rs:208-285
+      uint64_t pos = 0;
       if (pos >= plen) { e = E_TRUNCATED; break; }
       uint32_t lbw = p[pos++];
       if (lbw < 1 || lbw > 63) { e = E_CORRUPT; break; }
@@ -254,7 +140,7 @@ __device__ uint32_t dec_alprd(DecSmem& S, const uint8_t* p, uint64_t plen, uint6
       if (dsz > 8) { e = E_CORRUPT; break; }
       for (uint32_t j = 0; j < dsz; j++) {
         if (plen < pos + 8) { e = E_TRUNCATED; break; }
-        S.dict8[j] = ld_u64(p + pos);
+        A.dict8[j] = ld_u64(p + pos);
         pos += 8;
       }
       if (e) break;
@@ -263,13 +149,13 @@ __device__ uint32_t dec_alprd(DecSmem& S, const uint8_t* p, uint64_t plen, uint6
       if (e) break;
       if (nexc > n) { e = E_CORRUPT; break; }
       uint64_t exc_start = pos;
-      for (uint64_t x = 0; x < nexc; x++) {
+      for (uint64_t x = 0; x < nexc && !e; x++) {
         uint64_t pp;
         e = rd_varint(p, plen, &pos, &pp);
         if (e) break;
         if (plen < pos + 8) { e = E_TRUNCATED; break; }
         pos += 8;
-        if (pp >= n) { e = E_CORRUPT; break; }
+        if (pp >= n) e = E_CORRUPT;
       }
       if (e) break;
       if (pos >= plen) { e = E_TRUNCATED; break; }
@@ -283,97 +169,26 @@ __device__ uint32_t dec_alprd(DecSmem& S, const uint8_t* p, uint64_t plen, uint6
       if (pos >= plen) { e = E_TRUNCATED; break; }
       uint32_t rtag = p[pos++];
       uint64_t rpos = pos;
-      if (ctag == 1 || rtag == 1) { e = ctag > 1 ? E_CORRUPT : E_UNSUPPORTED; break; }
+      if (ctag == 1) { e = E_UNSUPPORTED; break; }
       if (ctag != 0) { e = E_CORRUPT; break; }
-      e = for_walk(p + cpos, clen, 0, n, S.offs, nullptr);
+      e = for_walk(p, cpos + clen, cpos, n, A.offs[0]);
       if (e) break;
+      if (rtag == 1) { e = E_UNSUPPORTED; break; }
       if (rtag != 0) { e = E_CORRUPT; break; }
-      e = for_walk(p + rpos, plen - rpos, 0, n, S.offs2, nullptr);
-      if (e) break;
-      S.sc[0] = lbw;
-      S.sc[1] = dsz;
-      S.sc[2] = nexc;
-      S.sc[3] = exc_start;
-      S.sc[4] = cpos;
-      S.sc[5] = rpos;
-    } while (0);
-    S.flag = 0;
-  }
-  e = bcast_err(S, e);
-  if (e) return e;
-  uint32_t lbw = (uint32_t)S.sc[0], dsz = (uint32_t)S.sc[1], rbw = 64 - lbw;
-  const uint8_t* cp = p + S.sc[4];
-  const uint8_t* rp = p + S.sc[5];
-  uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
-  for (uint32_t k = 0; k < nsub; k++) {
-    uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-    for_unpack(cp, S.offs[k], cnt, [&](uint32_t i, uint64_t v) { S.buf[i] = v; });
-    __syncthreads();
-    uint64_t* o = dst + (size_t)k * kSub;
-    for_unpack(rp, S.offs2[k], cnt, [&](uint32_t i, uint64_t r) {
-      uint64_t c = S.buf[i];
-      if (c >= dsz) {
-        S.flag = 1;
-      } else {
-        o[i] = (S.dict8[c] << rbw) | r;
-      }
-    });
-    __syncthreads();
-  }
-  if (S.flag) return E_CORRUPT;
-  if (threadIdx.x == 0 && S.sc[2]) {
-    uint64_t pos = S.sc[3], rmask = (1ull << rbw) - 1ull;
-    for (uint64_t x = 0; x < S.sc[2]; x++) {
-      uint64_t pp;
-      rd_varint(p, plen, &pos, &pp);
-      uint64_t l = ld_u64(p + pos);
-      pos += 8;
-      dst[pp] = (l << rbw) | (dst[pp] & rmask);
+      e = for_walk(p, plen, rpos, n, A.offs[1]);
+      A.a = lbw;
+      A.b = dsz;
+      A.c = exc_start;
+      A.d = nexc;
+      break;
     }
-  }
-  __syncthreads();
-  return E_OK;
-}
-
-// FLOAT_MULT with a bit-packed k stream (reference codecs/float_mult.rs:100-133).
-__device__ uint32_t dec_floatmult(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, uint64_t* dst) {
-  if (plen < 1) return E_TRUNCATED;
-  uint32_t tag = p[0];
-  if (plen < 2) return E_TRUNCATED;
-  uint32_t si = p[1];
-  if (si >= 7) return E_CORRUPT;
-  if (tag == 1) return E_UNSUPPORTED;
-  if (tag != 0) return E_CORRUPT;
-  double scale = kFmScales[si];
-  uint32_t e = E_OK;
-  const uint8_t* q = p + 2;
-  if (threadIdx.x == 0) e = for_walk(q, plen - 2, 0, n, S.offs, nullptr);
-  e = bcast_err(S, e);
-  if (e) return e;
-  uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
-  for (uint32_t k = 0; k < nsub; k++) {
-    uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-    uint64_t* o = dst + (size_t)k * kSub;
-    for_unpack(q, S.offs[k], cnt,
-               [&](uint32_t i, uint64_t v) { o[i] = f64_bits(__ddiv_rn(__ll2double_rn((long long)v), scale)); });
-  }
-  return E_OK;
-}
-
-// DICT with raw / delta values and bit-packed codes (reference codecs/dict.rs:154-207).
-__device__ uint32_t dec_dict(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, uint64_t* dst,
-                             uint64_t* scratch) {
-  uint32_t e = E_OK;
-  if (threadIdx.x == 0) {
-    uint64_t pos = 0;
-    do {
-      uint64_t card;
+    case M_DICT: {  // dict.rs:154-207
+      uint64_t pos = 0, card, vlen;
       e = rd_varint(p, plen, &pos, &card);
       if (e) break;
       if (card > n) { e = E_CORRUPT; break; }
       if (pos >= plen) { e = E_TRUNCATED; break; }
       uint32_t vtag = p[pos++];
-      uint64_t vlen;
       e = rd_varint(p, plen, &pos, &vlen);
       if (e) break;
       if (vlen > plen - pos) { e = E_TRUNCATED; break; }
@@ -382,7 +197,7 @@ __device__ uint32_t dec_dict(DecSmem& S, const uint8_t* p, uint64_t plen, uint64
         if (vlen != card * 8) { e = E_CORRUPT; break; }
       } else if (vtag == 1) {
         if (vlen < 8) { e = E_TRUNCATED; break; }
-        e = for_walk(p + vpos + 8, vlen - 8, 0, card, S.offs2, nullptr);
+        e = for_walk(p, vpos + vlen, vpos + 8, card, A.offs[1]);
         if (e) break;
       } else if (vtag == 2) {
         e = E_UNSUPPORTED;
@@ -396,136 +211,299 @@ __device__ uint32_t dec_dict(DecSmem& S, const uint8_t* p, uint64_t plen, uint64
       uint32_t ctag = p[pos++];
       if (ctag == 1) { e = E_UNSUPPORTED; break; }
       if (ctag != 0) { e = E_CORRUPT; break; }
-      e = for_walk(p, plen, pos, n, S.offs, nullptr);
-      if (e) break;
-      S.sc[0] = card;
-      S.sc[1] = vtag;
-      S.sc[2] = vpos;
-    } while (0);
-    S.flag = 0;
-  }
-  e = bcast_err(S, e);
-  if (e) return e;
-  uint64_t card = S.sc[0];
-  uint32_t vtag = (uint32_t)S.sc[1];
-  const uint8_t* vb = p + S.sc[2];
-  const uint64_t* dict = nullptr;
-  if (vtag == 1) {  // delta-decode the sorted dictionary into smem or scratch
-    uint64_t* dd = card <= kDictSmem ? S.dict : scratch;
-    uint64_t carry = ld_u64(vb);
-    const uint8_t* q = vb + 8;
-    uint32_t ns = (uint32_t)((card + kSub - 1) / kSub);
-    for (uint32_t k = 0; k < ns; k++) {
-      uint32_t cnt = (uint32_t)qmin(kSub, card - (uint64_t)k * kSub);
-      for_unpack(q, S.offs2[k], cnt, [&](uint32_t i, uint64_t v) { S.buf[i] = unzigzag64(v); });
-      __syncthreads();
-      uint64_t* o = dd + (size_t)k * kSub;
-      carry = chunk_prefix(S, cnt, carry, [&](uint32_t i, uint64_t v) { o[i] = v; });
+      e = for_walk(p, plen, pos, n, A.offs[0]);
+      A.a = card;
+      A.b = vtag;
+      A.c = vpos;
+      break;
     }
-    __syncthreads();
-    dict = dd;
-  }
-  uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
-  for (uint32_t k = 0; k < nsub; k++) {
-    uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-    uint64_t* o = dst + (size_t)k * kSub;
-    for_unpack(p, S.offs[k], cnt, [&](uint32_t i, uint64_t c) {
-      if (c >= card) {
-        S.flag = 1;
-      } else {
-        o[i] = dict ? dict[c] : ld_u64(vb + 8 * c);
-      }
-    });
-  }
-  __syncthreads();
-  return S.flag ? E_CORRUPT : E_OK;
-}
-
-// RLE (reference codecs/rle.rs:44-75).
-__device__ uint32_t dec_rle(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, uint64_t* dst) {
-  uint32_t e = E_OK;
-  if (threadIdx.x == 0) {
-    uint64_t pos = 0, nr;
-    do {
+    case M_RLE: {  // rle.rs:44-75
+      uint64_t pos = 0, nr;
       e = rd_varint(p, plen, &pos, &nr);
       if (e) break;
       if (nr > n) { e = E_CORRUPT; break; }
       if (plen - pos < nr * 8) { e = E_TRUNCATED; break; }
       uint64_t vpos = pos;
       pos += nr * 8;
-      e = for_walk(p, plen, pos, nr, S.offs, nullptr);
-      S.sc[0] = nr;
-      S.sc[1] = vpos;
-    } while (0);
-    S.flag = 0;
-  }
-  e = bcast_err(S, e);
-  if (e) return e;
-  uint64_t nr = S.sc[0];
-  const uint8_t* rv = p + S.sc[1];
-  uint32_t nsub = (uint32_t)((nr + kSub - 1) / kSub);
-  uint64_t carry = 0;
-  uint64_t* ends = S.dict;  // 1024 inclusive run ends of the current chunk
-  for (uint32_t k = 0; k < nsub; k++) {
-    uint32_t cnt = (uint32_t)qmin(kSub, nr - (uint64_t)k * kSub);
-    for_unpack(p, S.offs[k], cnt, [&](uint32_t i, uint64_t v) { S.buf[i] = v; });
-    __syncthreads();
-    uint64_t start = carry;
-    carry = chunk_prefix(S, cnt, carry, [&](uint32_t i, uint64_t v) {
-      ends[i] = v;
-      if (v > n || v < start) S.flag = 1;  // overrun (v < start: the prefix wrapped)
-    });
-    __syncthreads();
-    if (S.flag) return E_CORRUPT;
-    uint64_t hi = carry;  // <= n
-    for (uint64_t i = start + threadIdx.x; i < hi; i += kDecThreads) {
-      uint32_t lo = 0, up = cnt;  // first run with end > i
-      while (lo < up) {
-        uint32_t mid = (lo + up) >> 1;
-        if (ends[mid] > i) up = mid; else lo = mid + 1;
-      }
-      dst[i] = ld_u64(rv + 8ull * ((uint64_t)k * kSub + lo));
+      e = for_walk(p, plen, pos, nr, A.offs[0]);
+      A.a = nr;
+      A.b = vpos;
+      break;
     }
-    __syncthreads();
+    default:
+      e = E_UNSUPPORTED;
+      break;
   }
-  return carry != n ? E_LENGTH_MISMATCH : E_OK;
+  A.err = e;
+  if (e) atomicMin(err, ((unsigned long long)f << 8) | e);
 }
 
-// XORZ (reference codecs/xorz.rs:18-32): LEB128 XOR chain, decoded by one thread.
-__device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, uint64_t* dst) {
-  uint32_t e = E_OK;
+// ---------------------------------------------------------------------------
+// Warp-level FastLanes unpack of one sub-block: calls f(i, min + residual) for
+// every value index i < count.  For widths <= 32 lane l decodes FastLanes lane
+// l (rows 0..31); above 32 lane l decodes 64-bit lane l % 16, rows 32*(l/16)
+// .. +31.  Each row's words are consecutive across the warp.
+// ---------------------------------------------------------------------------
+template <class F>
+__device__ inline void warp_unpack(const uint8_t* p, uint32_t off, uint32_t count, F f) {
+  int l = threadIdx.x & 31;
+  uint32_t w = p[off];
+  uint64_t mn = ld_u64(p + off + 1);
+  const uint8_t* words = p + off + 9;
+  if (w == 0) {
+    for (uint32_t i = l; i < count; i += 32) f(i, mn);
+  } else if (w <= 32) {
+    uint32_t mask = w == 32 ? 0xFFFFFFFFu : ((1u << w) - 1u);
+#pragma unroll 4
+    for (uint32_t r = 0; r < 32; r++) {
+      uint32_t idx = r * 32 + l;
+      uint32_t bit = r * w, word = bit >> 5, sh = bit & 31;
+      uint32_t v = ld_u32(words + 4u * (word * 32u + l)) >> sh;
+      if (sh + w > 32) v |= ld_u32(words + 4u * ((word + 1) * 32u + l)) << (32 - sh);
+      v &= mask;
+      if (idx < count) f(idx, mn + (uint64_t)v);
+    }
+  } else {
+    uint64_t mask = w == 64 ? ~0ull : ((1ull << w) - 1ull);
+    uint32_t fl = l & 15, r0 = (l >> 4) * 32;
+#pragma unroll 4
+    for (uint32_t r = r0; r < r0 + 32; r++) {
+      uint32_t idx = r * 16 + fl;
+      uint32_t bit = r * w, word = bit >> 6, sh = bit & 63;
+      uint64_t v = ld_u64(words + 8u * (word * 16u + fl)) >> sh;
+      if (sh + w > 64) v |= ld_u64(words + 8u * ((word + 1) * 16u + fl)) << (64 - sh);
+      v &= mask;
+      if (idx < count) f(idx, mn + v);
+    }
+  }
+}
+
+// Warp inclusive prefix over buf[0..count) (u64, wrapping), starting from
+// `carry`; writes via out(i, v).
+template <class W>
+__device__ inline void warp_prefix_smem(const uint64_t* buf, uint32_t count, uint64_t carry, W out) {
+  int l = threadIdx.x & 31;
+  uint64_t run = carry;
+  for (uint32_t base = 0; base < count; base += 32) {
+    uint32_t i = base + l;
+    uint64_t v = i < count ? buf[i] : 0ull;
+    uint64_t inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+      if (l >= o) inc += u;
+    }
+    if (i < count) out(i, run + inc);
+    run += __shfl_sync(0xffffffffu, inc, 31);
+  }
+}
+
+struct DecSmem {
+  uint64_t subsum[kMaxSubs + 1];
+  uint64_t subcarry[kMaxSubs + 1];
+  uint32_t flag;
+  uint32_t wcnt[kDecWarps];
+  int64_t wmax[kDecWarps];
+  uint64_t wxor[kDecWarps];
+  uint64_t sc[4];
+  unsigned long long nth;
+  union {
+    uint64_t wbuf[kDecWarps][kSub];  // per-warp sub-block staging (64 KB)
+    struct {
+      uint64_t dict[kDictSmem];      // dictionary values (16 KB)
+      uint64_t stage[4][kSub];       // staging for the dictionary prefix pass
+    } d;
+    uint64_t xbuf[kXorzChunk];       // XORZ chunk values (16 KB)
+  } u;
+};
+
+// Sum of one sub-block's values after a per-value map g (warp-uniform result).
+template <class G>
+__device__ inline uint64_t warp_sub_sum(const uint8_t* p, uint32_t off, uint32_t count, G g) {
+  uint64_t s = 0;
+  warp_unpack(p, off, count, [&](uint32_t, uint64_t v) { s += g(v); });
+  return warp_sum(s);
+}
+
+// Two-phase prefix-sum decode of a FoR chain whose values are summed in index
+// order (DeltaBitpack deltas, dictionary deltas): per-sub-block sums, a carry
+// scan, then each warp stages its sub-block in smem and writes running values.
+// `nstage` warps take part in the second phase (one staging buffer each).
+template <class G, class W>
+__device__ void chain_prefix(DecSmem& S, const uint8_t* p, const uint32_t* offs, uint64_t n, uint64_t base_carry,
+                             uint64_t* stage, int nstage, G g, W out) {
+  int l = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
+  for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+    uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+    uint64_t s = warp_sub_sum(p, offs[k], cnt, g);
+    if (l == 0) S.subsum[k] = s;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    uint64_t pos = 0, prev = 0;
-    for (uint64_t i = 0; i < n; i++) {
-      uint64_t x;
-      e = rd_varint(p, plen, &pos, &x);
-      if (e) break;
-      prev ^= x;
-      dst[i] = prev;
+    uint64_t c = base_carry;
+    for (uint32_t k = 0; k < nsub; k++) {
+      S.subcarry[k] = c;
+      c += S.subsum[k];
     }
-    if (!e && pos != plen) e = E_CORRUPT;
   }
-  return bcast_err(S, e);
+  __syncthreads();
+  if (warp < nstage) {
+    uint64_t* buf = stage + (size_t)warp * kSub;
+    for (uint32_t k = warp; k < nsub; k += nstage) {
+      uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+      warp_unpack(p, offs[k], cnt, [&](uint32_t i, uint64_t v) { buf[i] = g(v); });
+      __syncwarp();
+      warp_prefix_smem(buf, cnt, S.subcarry[k], [&](uint32_t i, uint64_t v) { out((uint64_t)k * kSub + i, v); });
+      __syncwarp();
+    }
+  }
+  __syncthreads();
 }
 
+// XORZ (reference codecs/xorz.rs:18-32): LEB128 of v_i ^ v_{i-1}.  Byte-parallel:
+// terminator bytes (bit 7 clear) end values; block scans number them and find
+// each value's first byte, the terminator's thread assembles the value, and a
+// block XOR-scan rebuilds v.  Error kinds follow the sequential reader.
+__device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, uint64_t* dst) {
+  int t = threadIdx.x, l = t & 31, warp = t >> 5;
+  if (n == 0) return plen ? E_CORRUPT : E_OK;
+  uint64_t vbase = 0;         // values completed before this chunk
+  uint64_t xcarry = 0;        // XOR of all values so far
+  int64_t last_term = -1;     // position of the last terminator before the chunk
+  bool saw_nth = false;
+  uint64_t nth_pos = 0;
+  if (t == 0) {
+    S.flag = 0;
+    S.nth = ~0ull;
+  }
+  __syncthreads();
+  for (uint64_t base = 0; base < plen && vbase < n; base += kXorzChunk) {
+    uint64_t b0 = base + (uint64_t)t * 8;
+    uint32_t tm = 0;  // terminator mask of this thread's 8 bytes
+    for (int j = 0; j < 8; j++)
+      if (b0 + j < plen && !(p[b0 + j] & 0x80)) tm |= 1u << j;
+    uint32_t cnt = __popc(tm);
+    int64_t mylast = tm ? (int64_t)(b0 + 31 - __clz(tm)) : -1;
+    uint32_t inc = cnt;
+    int64_t mx = mylast;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+      int64_t um = __shfl_up_sync(0xffffffffu, mx, o);
+      if (l >= o) {
+        inc += u;
+        mx = um > mx ? um : mx;
+      }
+    }
+    if (l == 31) {
+      S.wcnt[warp] = inc;
+      S.wmax[warp] = mx;
+    }
+    __syncthreads();
+    uint32_t woff = 0, total = 0;
+    int64_t wprev = last_term, chunk_last = last_term;
+    for (int w2 = 0; w2 < kDecWarps; w2++) {
+      if (w2 < warp) {
+        woff += S.wcnt[w2];
+        wprev = S.wmax[w2] > wprev ? S.wmax[w2] : wprev;
+      }
+      total += S.wcnt[w2];
+      chunk_last = S.wmax[w2] > chunk_last ? S.wmax[w2] : chunk_last;
+    }
+    int64_t mx_ex = __shfl_up_sync(0xffffffffu, mx, 1);
+    if (l == 0) mx_ex = -1;
+    int64_t prev = mx_ex > wprev ? mx_ex : wprev;  // last terminator before this thread's bytes
+    uint32_t k = woff + inc - cnt;
+    uint32_t m = tm;
+    while (m) {
+      int j = __ffs(m) - 1;
+      m &= m - 1;
+      uint64_t pos = b0 + j;
+      uint64_t start = (uint64_t)(prev + 1);
+      uint64_t len = pos - start + 1;
+      uint64_t vi = vbase + k;
+      if (vi < n) {
+        if (len > 10) {
+          S.flag = 1;
+        } else {
+          uint64_t x = 0;
+          for (uint64_t q = 0; q < len; q++) x |= (uint64_t)(p[start + q] & 0x7f) << (7 * q);
+          S.u.xbuf[k] = x;
+        }
+        if (vi == n - 1) {
+          saw_nth = true;
+          nth_pos = pos;
+        }
+      }
+      prev = (int64_t)pos;
+      k++;
+    }
+    __syncthreads();
+    uint32_t cv = (uint32_t)qmin(total, n - vbase);
+    uint32_t i0 = (uint32_t)t * 8;
+    uint64_t vals[8], xs = 0;
+    for (int j = 0; j < 8; j++) {
+      vals[j] = (i0 + j < cv) ? S.u.xbuf[i0 + j] : 0ull;
+      xs ^= vals[j];
+    }
+    uint64_t xi = xs;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t u = __shfl_up_sync(0xffffffffu, xi, o);
+      if (l >= o) xi ^= u;
+    }
+    if (l == 31) S.wxor[warp] = xi;
+    __syncthreads();
+    uint64_t wx = 0, tx = 0;
+    for (int w2 = 0; w2 < kDecWarps; w2++) {
+      if (w2 < warp) wx ^= S.wxor[w2];
+      tx ^= S.wxor[w2];
+    }
+    uint64_t run = xcarry ^ wx ^ xi ^ xs;
+    for (int j = 0; j < 8; j++) {
+      run ^= vals[j];
+      if (i0 + j < cv) dst[vbase + i0 + j] = run;
+    }
+    xcarry ^= tx;
+    vbase += total;
+    last_term = chunk_last;
+    __syncthreads();
+  }
+  if (saw_nth) atomicMin(&S.nth, (unsigned long long)nth_pos);
+  __syncthreads();
+  uint32_t e = E_OK;
+  if (S.flag) e = E_CORRUPT;
+  else if (vbase < n) e = (plen - (uint64_t)(last_term + 1) >= 10) ? E_CORRUPT : E_TRUNCATED;
+  else if (S.nth != plen - 1) e = E_CORRUPT;
+  __syncthreads();
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// The decode kernel
+// ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __restrict__ stream,
                                                               const FrameDesc* __restrict__ frames, int nf,
-                                                              int dtype, uint64_t* __restrict__ lane,
+                                                              int dtype, const FrameAux* __restrict__ aux,
+                                                              uint64_t* __restrict__ lane,
                                                               uint64_t* __restrict__ scratch,
                                                               unsigned long long* __restrict__ err) {
-  __shared__ DecSmem S;
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  DecSmem& S = *reinterpret_cast<DecSmem*>(smem_raw);
   int f = blockIdx.x;
   if (f >= nf) return;
+  const FrameAux& A = aux[f];
+  if (A.err) return;
   FrameDesc d = frames[f];
   const uint8_t* p = stream + d.payload_off;
   uint64_t plen = d.plen, n = d.n;
   uint64_t* out = lane + d.value_off;
+  int t = threadIdx.x, l = t & 31, warp = t >> 5;
+  uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
   uint32_t e = E_OK;
-  int t = threadIdx.x;
+  if (t == 0) S.flag = 0;
+  __syncthreads();
   switch (d.mode) {
     case M_RAW: {
       uint32_t lb = lane_bytes(dtype);
-      if (plen != n * lb) { e = E_CORRUPT; break; }
       if (dtype == DT_F32) {
         for (uint64_t i = t; i < n; i += kDecThreads) out[i] = f32bits_to_f64bits(ld_u32(p + 4 * i));
       } else if (lb == 4) {
@@ -536,26 +514,192 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
       break;
     }
     case M_CONST: {
-      if (plen != 8) { e = E_CORRUPT; break; }
       uint64_t v = ld_u64(p);
       for (uint64_t i = t; i < n; i += kDecThreads) out[i] = v;
       break;
     }
     case M_STRIDE: {
-      if (plen != 16) { e = E_CORRUPT; break; }
       uint64_t first = ld_u64(p), stride = ld_u64(p + 8);
       for (uint64_t i = t; i < n; i += kDecThreads) out[i] = first + i * stride;
       break;
     }
-    case M_XORZ: e = dec_xorz(S, p, plen, n, out); break;
-    case M_FOR_BITPACK: e = dec_for(S, p, plen, 0, n, out); break;
-    case M_DELTA_BITPACK: e = dec_delta(S, p, plen, n, out); break;
-    case M_ALP: e = dec_alp(S, p, plen, n, out); break;
-    case M_ALP_RD: e = dec_alprd(S, p, plen, n, out); break;
-    case M_FLOAT_MULT: e = dec_floatmult(S, p, plen, n, out); break;
-    case M_DICT: e = dec_dict(S, p, plen, n, out, scratch ? scratch + d.value_off : nullptr); break;
-    case M_RLE: e = dec_rle(S, p, plen, n, out); break;
-    default: e = E_UNSUPPORTED; break;
+    case M_XORZ:
+      e = dec_xorz(S, p, plen, n, out);
+      break;
+    case M_FOR_BITPACK:
+      for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+        uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+        uint64_t* o = out + (size_t)k * kSub;
+        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) { o[i] = v; });
+      }
+      break;
+    case M_DELTA_BITPACK:
+      chain_prefix(S, p, A.offs[0], n, ld_u64(p), &S.u.wbuf[0][0], kDecWarps,
+                   [](uint64_t v) { return unzigzag64(v); }, [&](uint64_t i, uint64_t v) { out[i] = v; });
+      break;
+    case M_FLOAT_MULT: {
+      double scale = kFmScales[A.a];
+      for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+        uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+        uint64_t* o = out + (size_t)k * kSub;
+        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) {
+          o[i] = f64_bits(__ddiv_rn(__ll2double_rn((long long)v), scale));
+        });
+      }
+      break;
+    }
+    case M_ALP:
+      for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+        uint32_t off = A.offs[0][k];
+        int ee = p[off], ff = p[off + 1];
+        uint32_t exc = ld_u16(p + off + 2);
+        int64_t mn = (int64_t)ld_u64(p + off + 4);
+        uint32_t w = p[off + 12];
+        uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+        uint64_t* o = out + (size_t)k * kSub;
+        const uint8_t* words = p + off + 13;
+        if (w == 0) {
+          uint64_t v = f64_bits(alp_decode_value(mn, ee, ff));
+          for (uint32_t i = l; i < cnt; i += 32) o[i] = v;
+        } else {
+          uint32_t mask = w == 32 ? 0xFFFFFFFFu : ((1u << w) - 1u);
+          for (uint32_t r = 0; r < 32; r++) {
+            uint32_t idx = r * 32 + l;
+            uint32_t bit = r * w, word = bit >> 5, sh = bit & 31;
+            uint32_t v = ld_u32(words + 4u * (word * 32u + l)) >> sh;
+            if (sh + w > 32) v |= ld_u32(words + 4u * ((word + 1) * 32u + l)) << (32 - sh);
+            v &= mask;
+            if (idx < cnt) o[idx] = f64_bits(alp_decode_value((int64_t)((uint64_t)mn + v), ee, ff));
+          }
+        }
+        __syncwarp();
+        if (exc && l == 0) {  // in order, so a repeated position keeps the last exception
+          const uint8_t* xp = words + 128u * w;
+          for (uint32_t x = 0; x < exc; x++) o[ld_u16(xp + 10 * x)] = ld_u64(xp + 10 * x + 2);
+        }
+        __syncwarp();
+      }
+      break;
+    case M_ALP_RD: {
+      uint32_t lbw = (uint32_t)A.a, dsz = (uint32_t)A.b, rbw = 64 - lbw;
+      uint64_t* cb = &S.u.wbuf[warp][0];
+      for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+        uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) { cb[i] = v; });
+        __syncwarp();
+        uint64_t* o = out + (size_t)k * kSub;
+        warp_unpack(p, A.offs[1][k], cnt, [&](uint32_t i, uint64_t r) {
+          uint64_t c = cb[i];
+          if (c >= dsz) S.flag = 1;
+          else o[i] = (A.dict8[c] << rbw) | r;
+        });
+        __syncwarp();
+      }
+      __syncthreads();
+      if (S.flag) {
+        e = E_CORRUPT;
+        break;
+      }
+      if (t == 0 && A.d) {  // exceptions in order (alp_rd.rs:281-283)
+        uint64_t pos = A.c, rmask = (1ull << rbw) - 1ull;
+        for (uint64_t x = 0; x < A.d; x++) {
+          uint64_t pp = 0;
+          rd_varint(p, plen, &pos, &pp);
+          uint64_t lv = ld_u64(p + pos);
+          pos += 8;
+          out[pp] = (lv << rbw) | (out[pp] & rmask);
+        }
+      }
+      break;
+    }
+    case M_DICT: {
+      uint64_t card = A.a;
+      const uint8_t* vb = p + A.c;
+      const uint64_t* dict = nullptr;
+      if (A.b == 1) {  // delta-coded sorted dictionary -> smem or scratch
+        uint64_t* dd = card <= kDictSmem ? S.u.d.dict : scratch;
+        if (!dd) {
+          e = E_UNSUPPORTED;
+          break;
+        }
+        chain_prefix(S, p, A.offs[1], card, ld_u64(vb), &S.u.d.stage[0][0], 4,
+                     [](uint64_t v) { return unzigzag64(v); }, [&](uint64_t i, uint64_t v) { dd[i] = v; });
+        dict = dd;
+      } else if (card <= kDictSmem) {
+        for (uint64_t i = t; i < card; i += kDecThreads) S.u.d.dict[i] = ld_u64(vb + 8 * i);
+        __syncthreads();
+        dict = S.u.d.dict;
+      }
+      for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+        uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+        uint64_t* o = out + (size_t)k * kSub;
+        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t c) {
+          if (c >= card) S.flag = 1;
+          else o[i] = dict ? dict[c] : ld_u64(vb + 8 * c);
+        });
+      }
+      __syncthreads();
+      if (S.flag) e = E_CORRUPT;
+      break;
+    }
+    case M_RLE: {
+      uint64_t nr = A.a;
+      const uint8_t* rv = p + A.b;
+      uint32_t nrs = (uint32_t)((nr + kSub - 1) / kSub);
+      // phase 1: run-length sums per chunk (saturating at n+1 to catch overruns)
+      for (uint32_t k = warp; k < nrs; k += kDecWarps) {
+        uint32_t cnt = (uint32_t)qmin(kSub, nr - (uint64_t)k * kSub);
+        uint64_t s = 0;
+        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t, uint64_t v) { s = qmin(s + qmin(v, n + 1), n + 1); });
+        for (int o = 16; o; o >>= 1) s = qmin(s + __shfl_xor_sync(0xffffffffu, s, o), n + 1);
+        if (l == 0) S.subsum[k] = s;
+      }
+      __syncthreads();
+      if (t == 0) {
+        uint64_t c = 0;
+        uint32_t bad = 0;
+        for (uint32_t k = 0; k < nrs; k++) {
+          S.subcarry[k] = c;
+          c += S.subsum[k];
+          if (c > n) bad = 1;
+        }
+        S.sc[0] = bad ? 1ull : (c != n ? 2ull : 0ull);
+      }
+      __syncthreads();
+      if (S.sc[0] == 1) { e = E_CORRUPT; break; }
+      if (S.sc[0] == 2) { e = E_LENGTH_MISMATCH; break; }
+      // phase 2: per chunk, run ends in smem, then a warp-striped expand
+      uint64_t* ends = &S.u.wbuf[warp][0];
+      for (uint32_t k = warp; k < nrs; k += kDecWarps) {
+        uint32_t cnt = (uint32_t)qmin(kSub, nr - (uint64_t)k * kSub);
+        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) { ends[i] = v; });
+        __syncwarp();
+        uint64_t start = S.subcarry[k];
+        warp_prefix_smem(ends, cnt, start, [&](uint32_t i, uint64_t v) { ends[i] = v; });
+        __syncwarp();
+        uint64_t stop = start + S.subsum[k];
+        uint32_t r = 0;
+        bool init = false;
+        for (uint64_t i = start + l; i < stop; i += 32) {
+          if (!init) {
+            uint32_t lo = 0, hi = cnt;
+            while (lo < hi) {
+              uint32_t mid = (lo + hi) >> 1;
+              if (ends[mid] > i) hi = mid; else lo = mid + 1;
+            }
+            r = lo;
+            init = true;
+          }
+          while (ends[r] <= i) r++;
+          out[i] = ld_u64(rv + 8ull * ((uint64_t)k * kSub + r));
+        }
+        __syncwarp();
+      }
+      break;
+    }
+    default:
+      e = E_UNSUPPORTED;
+      break;
   }
   if (e && t == 0) atomicMin(err, ((unsigned long long)f << 8) | e);
 }
@@ -651,10 +795,16 @@ __global__ void k_decimal_combine(const uint64_t* __restrict__ limbs, uint64_t l
 // ---------------------------------------------------------------------------
 // Host launchers.
 // ---------------------------------------------------------------------------
+uint64_t decode_aux_bytes(int nf) { return (uint64_t)(nf > 0 ? nf : 1) * sizeof(FrameAux); }
+
 void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, uint64_t* lane,
-                          uint64_t* scratch, unsigned long long* err, cudaStream_t st) {
-  if (nf > 0) k_decode_frames<<<nf, kDecThreads, 0, st>>>(stream, frames, nf, dtype, lane, scratch, err);
-  count_launches(nf > 0 ? 1 : 0);
+                          uint64_t* scratch, void* aux, unsigned long long* err, cudaStream_t st) {
+  if (nf <= 0) return;
+  FrameAux* A = reinterpret_cast<FrameAux*>(aux);
+  k_walk_frames<<<(nf + 127) / 128, 128, 0, st>>>(stream, frames, nf, dtype, A, err);
+  cudaFuncSetAttribute(k_decode_frames, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecSmem));
+  k_decode_frames<<<nf, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, nf, dtype, A, lane, scratch, err);
+  count_launches(2);
 }
 
 void launch_word_popcount(const uint8_t* bm, uint64_t n, uint64_t* cnt, cudaStream_t st) {

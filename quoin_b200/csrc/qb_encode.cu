@@ -1541,22 +1541,39 @@ __global__ void k_plan(const uint8_t* __restrict__ grow, uint64_t n, uint64_t fi
     if (blockIdx.x == 0 && threadIdx.x == 0) *nb = (uint32_t)nblk;
     return;
   }
-  if (blockIdx.x || threadIdx.x) return;
+  // Adaptive: the block starts form a chain over the 32768-value windows
+  // (grow -> +4 windows, else +1).  Stage the flags in shared memory so the
+  // sequential walk runs at shared-memory latency.
+  if (blockIdx.x) return;
+  __shared__ uint8_t s_grow[16384];
+  __shared__ uint32_t s_count;
+  uint64_t nwin = (n + kBaseQuantum - 1) / kBaseQuantum;
+  if (threadIdx.x == 0) s_count = 0;
   uint64_t s = 0;
-  uint32_t c = 0;
-  while (s < n) {
-    uint64_t end = grow[s / kBaseQuantum] ? qmin(s + kMaxBlock, n) : qmin(s + kBaseQuantum, n);
-    FrameDesc f;
-    f.value_off = s;
-    f.n = (uint32_t)(end - s);
-    f.payload_off = 0;
-    f.plen = 0;
-    f.mode = 0;
-    f.aux = 0;
-    frames[c++] = f;
-    s = end;
+  for (uint64_t w0 = 0; w0 < nwin; w0 += 16384) {
+    uint64_t wn = qmin(16384, nwin - w0);
+    __syncthreads();
+    for (uint64_t i = threadIdx.x; i < wn; i += blockDim.x) s_grow[i] = grow[w0 + i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t c = s_count;
+      while (s < n && s / kBaseQuantum < w0 + wn) {
+        uint64_t end = s_grow[s / kBaseQuantum - w0] ? qmin(s + kMaxBlock, n) : qmin(s + kBaseQuantum, n);
+        FrameDesc f;
+        f.value_off = s;
+        f.n = (uint32_t)(end - s);
+        f.payload_off = 0;
+        f.plen = 0;
+        f.mode = 0;
+        f.aux = 0;
+        frames[c++] = f;
+        s = end;
+      }
+      s_count = c;
+    }
   }
-  *nb = c;
+  __syncthreads();
+  if (threadIdx.x == 0) *nb = s_count;
 }
 
 __global__ void k_frame_sizes(const FrameDesc* __restrict__ frames, const uint32_t* __restrict__ nbp, uint32_t maxb,

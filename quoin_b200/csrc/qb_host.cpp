@@ -25,6 +25,72 @@ uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
 
 using namespace qb;
 
+// ---------------------------------------------------------------------------
+// Optional per-kernel-class CUDA-event timing (recorded on the launching
+// stream, resolved after the call's final synchronisation).
+// ---------------------------------------------------------------------------
+namespace {
+enum TimerClass { T_COMPETE = 0, T_EMIT, T_DECODE, T_FINALIZE, T_LOWER, T_PLAN, T_VALIDITY, T_OTHER, T_COUNT };
+struct Timing {
+  std::atomic<bool> on{false};
+  std::mutex mu;
+  double ms[T_COUNT] = {};
+  uint64_t calls[T_COUNT] = {};
+  std::vector<cudaEvent_t> pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+};
+Timing g_timing;
+
+cudaEvent_t take_event() {
+  if (!g_timing.pool.empty()) {
+    cudaEvent_t e = g_timing.pool.back();
+    g_timing.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct TimedRegion {
+  int cls;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr, b = nullptr;
+  TimedRegion(int c, cudaStream_t s) : cls(c), st(s) {
+    if (!g_timing.on.load()) return;
+    std::lock_guard<std::mutex> l(g_timing.mu);
+    a = take_event();
+    b = take_event();
+    cudaEventRecord(a, st);
+  }
+  ~TimedRegion() {
+    if (!a) return;
+    cudaEventRecord(b, st);
+    std::lock_guard<std::mutex> l(g_timing.mu);
+    g_timing.pending.push_back({cls, {a, b}});
+  }
+};
+
+// Called after a stream synchronisation: folds finished event pairs in.
+void resolve_timing() {
+  if (!g_timing.on.load()) return;
+  std::lock_guard<std::mutex> l(g_timing.mu);
+  for (auto& p : g_timing.pending) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(p.second.second) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess) {
+      g_timing.ms[p.first] += ms;
+      g_timing.calls[p.first] += 1;
+    } else {
+      cudaGetLastError();
+    }
+    g_timing.pool.push_back(p.second.first);
+    g_timing.pool.push_back(p.second.second);
+  }
+  g_timing.pending.clear();
+}
+}  // namespace
+
 namespace {
 
 enum { WT_F64 = 0, WT_I64, WT_U64, WT_I32, WT_U32, WT_F32, WT_DEC128, WT_DEC256 };
@@ -33,6 +99,9 @@ enum { K_OK = 0, K_BAD_MAGIC = 1, K_VERSION = 2, K_TRUNC = 3, K_UNKNOWN_MODE = 4
 constexpr uint64_t kMaxBlockValues = 131072;
 constexpr uint64_t kBaseQuantumH = 32768;
 constexpr uint64_t kMaxBitmapBytes = 1ull << 36;
+// Columns longer than this cannot be allocated on any host the reference runs
+// on; its decoder reports the failed allocation as CorruptPayload.
+constexpr uint64_t kMaxLogicalValues = 1ull << 36;
 
 inline uint32_t lane_bytes_h(int dt) { return (dt == WT_I32 || dt == WT_U32 || dt == WT_F32) ? 4u : 8u; }
 inline uint32_t native_width(int dt) {
@@ -125,7 +194,7 @@ inline int plain_code(int ext) {
 // ---------------------------------------------------------------------------
 enum Slot {
   S_IN, S_BM, S_RANK, S_LANE, S_GROW, S_FRAMES, S_NB, S_SIZES, S_TILE, S_SCRATCH, S_OUT, S_VTMP, S_VBLOB,
-  S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_COUNT
+  S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_DAUX, S_COUNT
 };
 
 struct QuoinCtx {
@@ -264,6 +333,7 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
     CK(c->ensure(S_VBLOB, blob_cap));
     uint64_t* vtmp = c->p<uint64_t>(S_VTMP);
     uint64_t* vtile = vtmp + validity_tmp_words(ln);
+    TimedRegion tr(T_VALIDITY, st);
     launch_validity_blob(j.d_bm, ln, vtmp, vtile, c->p<uint8_t>(S_VBLOB), d_misc + 2, st);
     launch_put_validity(d_dst + 16, 16, c->p<uint8_t>(S_VBLOB), d_misc + 2, d_misc, st);
   }
@@ -282,20 +352,33 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
   CK(c->ensure(S_GROW, (n + kBaseQuantumH - 1) / kBaseQuantumH + 16));
   FrameDesc* fr = c->p<FrameDesc>(S_FRAMES);
   uint32_t* nb = c->p<uint32_t>(S_NB);
-  if (!bs) launch_probe_windows(j.lane, n, c->p<uint8_t>(S_GROW), st);
-  launch_plan(c->p<uint8_t>(S_GROW), n, bs, fr, nb, st);
-  launch_compete(j.lane, fr, nb, (uint32_t)maxb, j.dtype, j.level, c->p<uint8_t>(S_SCRATCH), nullptr, st);
-  launch_frame_offsets(fr, nb, (uint32_t)maxb, d_misc, c->p<uint64_t>(S_SIZES), c->p<uint64_t>(S_TILE), d_misc + 1,
-                       st);
+  {
+    TimedRegion tr(T_PLAN, st);
+    if (!bs) launch_probe_windows(j.lane, n, c->p<uint8_t>(S_GROW), st);
+    launch_plan(c->p<uint8_t>(S_GROW), n, bs, fr, nb, st);
+  }
+  {
+    TimedRegion tr(T_COMPETE, st);
+    launch_compete(j.lane, fr, nb, (uint32_t)maxb, j.dtype, j.level, c->p<uint8_t>(S_SCRATCH), nullptr, st);
+  }
+  {
+    TimedRegion tr(T_OTHER, st);
+    launch_frame_offsets(fr, nb, (uint32_t)maxb, d_misc, c->p<uint64_t>(S_SIZES), c->p<uint64_t>(S_TILE),
+                         d_misc + 1, st);
+  }
   uint64_t hm[2] = {0, 0};
   CK(cudaMemcpyAsync(hm, d_misc, 16, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   uint64_t total = hm[0] + hm[1];
   *out_len = total;
   if (total > dst_cap) return QUOIN_ERR_BUFFER_TOO_SMALL;
-  launch_emit(j.lane, fr, nb, (uint32_t)maxb, j.dtype, c->p<uint8_t>(S_SCRATCH), d_dst, st);
+  {
+    TimedRegion tr(T_EMIT, st);
+    launch_emit(j.lane, fr, nb, (uint32_t)maxb, j.dtype, c->p<uint8_t>(S_SCRATCH), d_dst, st);
+  }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));
+  resolve_timing();
   return QUOIN_OK;
 }
 
@@ -318,8 +401,11 @@ int device_valid_count(QuoinCtx* c, cudaStream_t st, const uint8_t* d_bm, uint64
   CK(c->ensure(S_TILE, (scan_tile_count(nw) + 16) * 8));
   CK(c->ensure(S_MISC, 64 * 8));
   uint64_t* rank = c->p<uint64_t>(S_RANK);
-  launch_word_popcount(d_bm, n, rank, st);
-  launch_scan_sum(rank, rank, nw, c->p<uint64_t>(S_TILE), c->p<uint64_t>(S_MISC) + 8, st);
+  {
+    TimedRegion tr(T_VALIDITY, st);
+    launch_word_popcount(d_bm, n, rank, st);
+    launch_scan_sum(rank, rank, nw, c->p<uint64_t>(S_TILE), c->p<uint64_t>(S_MISC) + 8, st);
+  }
   CK(cudaMemcpyAsync(n_valid, c->p<uint64_t>(S_MISC) + 8, 8, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return QUOIN_OK;
@@ -441,6 +527,7 @@ int compress_column_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, c
     lane = (const uint64_t*)d_values;
   } else {
     CK(c->ensure(S_LANE, n_valid * 8 + 64));
+    TimedRegion tr(T_LOWER, st);
     launch_lower(d_values, wire, d_bm, d_bm ? c->p<uint64_t>(S_RANK) : nullptr, n, c->p<uint64_t>(S_LANE), st);
     lane = c->p<uint64_t>(S_LANE);
   }
@@ -514,6 +601,7 @@ int parse_lane(const uint8_t* src, uint64_t base, uint64_t len, LaneIdx& L) {
   L.dtype = s[7];
   L.has_validity = s[5] & 1;
   L.logical_n = rd64(s + 8);
+  if (L.logical_n > kMaxLogicalValues) return K_CORRUPT;  // decoder.rs:105-106 / validity.rs:135-136 allocation
   uint64_t pos = 16;
   L.n_total = L.logical_n;
   if (L.has_validity) {
@@ -589,6 +677,7 @@ int parse_stream(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
     X.wire = expect;
     X.has_validity = src[5] & 1;
     X.n = rd64(src + 8);
+    if (X.n > kMaxLogicalValues) return K_CORRUPT;
     X.scale = (int8_t)src[16];
     X.precision = src[17];
     int nl = src[18];
@@ -674,6 +763,10 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
   unsigned long long* d_err = c->p<unsigned long long>(S_ERR);
   CK(cudaMemsetAsync(d_err, 0xFF, 8, st));
   const uint8_t* bm = X.has_validity ? dbm : nullptr;
+  uint64_t max_nf = 1;
+  for (auto& L : X.lanes) max_nf = L.frames.size() > max_nf ? L.frames.size() : max_nf;
+  CK(c->ensure(S_DAUX, decode_aux_bytes((int)max_nf)));
+  void* daux = c->p<void>(S_DAUX);
   if (!X.decimal) {
     const LaneIdx& L = X.lanes[0];
     bool direct = !X.has_validity && lane_bytes_h(X.wire) == 8 && ((uintptr_t)d_out & 7) == 0;
@@ -689,8 +782,14 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
       CK(c->ensure(S_DSCR, L.n_total * 8 + 64));
       scr = c->p<uint64_t>(S_DSCR);
     }
-    launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, lane_out, scr, d_err, st);
-    if (!direct && X.n) launch_finalize(lane_out, bm, drank, X.n, X.wire, d_out, st);
+    {
+      TimedRegion tr(T_DECODE, st);
+      launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, lane_out, scr, daux, d_err, st);
+    }
+    if (!direct && X.n) {
+      TimedRegion tr(T_FINALIZE, st);
+      launch_finalize(lane_out, bm, drank, X.n, X.wire, d_out, st);
+    }
   } else {
     CK(c->ensure(S_LIMBS, (uint64_t)X.nl * X.n_valid * 8 + 64));
     uint64_t* limbs = c->p<uint64_t>(S_LIMBS);
@@ -704,10 +803,14 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
     }
     for (int k = 0; k < X.nl; k++) {
       const LaneIdx& L = X.lanes[k];
+      TimedRegion tr(T_DECODE, st);
       launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), WT_U64, limbs + (uint64_t)k * X.n_valid,
-                           scr, d_err, st);
+                           scr, daux, d_err, st);
     }
-    if (X.n) launch_decimal_combine(limbs, X.n_valid, X.nl, dvmin, bm, drank, X.n, (uint8_t*)d_out, st);
+    if (X.n) {
+      TimedRegion tr(T_FINALIZE, st);
+      launch_decimal_combine(limbs, X.n_valid, X.nl, dvmin, bm, drank, X.n, (uint8_t*)d_out, st);
+    }
   }
   if (d_valid_out && X.has_validity && X.n)
     CK(cudaMemcpyAsync(d_valid_out, dbm, (X.n + 7) / 8, cudaMemcpyDeviceToDevice, st));
@@ -715,6 +818,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
   CK(cudaMemcpyAsync(&herr, d_err, 8, cudaMemcpyDeviceToHost, st));
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));
+  resolve_timing();
   if (herr != ~0ull) return kind_to_code((int)(herr & 0xFF));
   return QUOIN_OK;
 }
@@ -1083,6 +1187,21 @@ int quoin_b200_stream_info(const uint8_t* src, size_t len, int32_t* wire, uint64
   return QUOIN_OK;
 }
 
+int quoin_b200_parse(const uint8_t* src, size_t len, int32_t* wire, uint64_t* n, int32_t* has_validity) {
+  if (!src || !wire || !n || !has_validity) return QUOIN_ERR_NULL;
+  try {
+    QuoinDecodeIndex X;
+    int k = parse_stream(src, len, X);
+    if (k) return kind_to_code(k);
+    *wire = X.wire;
+    *n = X.n;
+    *has_validity = X.has_validity;
+    return QUOIN_OK;
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
 int quoin_b200_decompress_column(QuoinCtx* ctx, const uint8_t* src, size_t len, void* values_out,
                                  uint8_t* validity_out) {
   if (!src || !values_out) return QUOIN_ERR_NULL;
@@ -1205,5 +1324,25 @@ void quoin_b200_reset_mode_win_counts(void) {
 }
 
 uint64_t quoin_b200_kernel_launches(void) { return launches_total(); }
+
+void quoin_b200_timing_enable(int on) {
+  std::lock_guard<std::mutex> l(g_timing.mu);
+  for (int k = 0; k < T_COUNT; k++) {
+    g_timing.ms[k] = 0;
+    g_timing.calls[k] = 0;
+  }
+  g_timing.on.store(on != 0);
+}
+
+int quoin_b200_timing_read(double* ms_out, uint64_t* calls_out, int n) {
+  if (!ms_out || !calls_out) return QUOIN_ERR_NULL;
+  resolve_timing();
+  std::lock_guard<std::mutex> l(g_timing.mu);
+  for (int k = 0; k < n && k < T_COUNT; k++) {
+    ms_out[k] = g_timing.ms[k];
+    calls_out[k] = g_timing.calls[k];
+  }
+  return T_COUNT;
+}
 
 }  // extern "C"

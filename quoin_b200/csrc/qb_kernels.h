@@ -9,8 +9,11 @@
 namespace qb {
 
 // ---- decoder (qb_decode.cu) ----
+// Walk (validation + sub-block offsets) and decode of nf frames.  `aux` is
+// device scratch of decode_aux_bytes(nf) bytes.
+uint64_t decode_aux_bytes(int nf);
 void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, uint64_t* lane,
-                          uint64_t* scratch, unsigned long long* err, cudaStream_t st);
+                          uint64_t* scratch, void* aux, unsigned long long* err, cudaStream_t st);
 void launch_word_popcount(const uint8_t* bm, uint64_t n, uint64_t* cnt, cudaStream_t st);
 void launch_finalize(const uint64_t* lane, const uint8_t* bm, const uint64_t* word_rank, uint64_t n, int dtype,
                      void* out, cudaStream_t st);
