@@ -160,6 +160,7 @@ struct EncSmem {
   uint32_t neq_k[kSubsMax];
   uint32_t subsz[kSubsMax + 1];
   uint64_t submin[kSubsMax];
+  uint64_t item_min[kSubsMax], item_max[kSubsMax];
   unsigned long long xor_bytes, umin, umax, e_vmin, e_vmax, e_dmax, acc64;
   uint32_t neq, stride_bad, fm_mask, alp_fail, flag, ovf, card, has_max, max_rank, cnt32, dl;
   uint32_t distinct_bits[512];
@@ -286,115 +287,6 @@ __device__ uint64_t block_for(EncSmem& S, uint8_t* dst, uint32_t M, bool sgn, V 
   return total;
 }
 
-// ---------------------------------------------------------------------------
-// Block features (reference encoder.rs:705-750) and the integer early-out
-// (encoder.rs:655-683).  Requires S.neq from the stats pass.
-// ---------------------------------------------------------------------------
-__device__ void sample_features(EncSmem& S, const uint64_t* v, uint32_t n) {
-  for (uint32_t i = threadIdx.x; i < 512; i += blockDim.x) S.distinct_bits[i] = 0;
-  if (threadIdx.x == 0) {
-    S.e_vmin = v[0];
-    S.e_vmax = v[0];
-    S.e_dmax = 0;
-  }
-  __syncthreads();
-  uint32_t dstride = max(n / 4096u, 1u);
-  for (uint32_t i = threadIdx.x; (uint64_t)i * dstride < n; i += blockDim.x) {
-    uint64_t h = v[(uint64_t)i * dstride] * 0x9E3779B97F4A7C15ull;
-    uint32_t b = (uint32_t)((h >> 50) & 0x3FFF);
-    atomicOr(&S.distinct_bits[b >> 5], 1u << (b & 31));
-  }
-  uint32_t estep = max(n / 2048u, 1u);
-  for (uint32_t i = threadIdx.x; (uint64_t)i * estep < n; i += blockDim.x) {
-    uint32_t idx = i * estep;
-    uint64_t x = v[idx];
-    atomic_min_u64(&S.e_vmin, x);
-    atomic_max_u64(&S.e_vmax, x);
-    if (idx >= estep) atomic_max_u64(&S.e_dmax, zigzag64(x - v[idx - 1]));
-  }
-  __syncthreads();
-}
-
-// ---------------------------------------------------------------------------
-// Stats pass: one warp per 1024-value sub-block.
-// ---------------------------------------------------------------------------
-__device__ void stats_pass(EncSmem& S, const uint64_t* v, uint32_t n, int dtype, bool do_fm) {
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t nsub = (n + kSub - 1) / kSub;
-  uint64_t v0 = v[0], stride = n > 1 ? v[1] - v[0] : 0;
-  bool sgn = dtype_signed(dtype);
-  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
-    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
-    uint64_t carry = base ? v[base - 1] : v0;
-    uint64_t umn = kEmpty64, umx = 0, dzmn = kEmpty64, dzmx = 0, xb = 0;
-    int64_t smn = INT64_MAX, smx = INT64_MIN;
-    uint32_t nq = 0, sbad = 0, fmfail = 0;
-    uint32_t alive = do_fm ? *(volatile uint32_t*)&S.fm_mask : 0u;
-#pragma unroll 4
-    for (uint32_t j = 0; j < 32; j++) {
-      uint32_t li = j * 32 + lane;
-      bool ok = li < cnt;
-      uint32_t idx = base + li;
-      uint64_t x = ok ? v[idx] : 0;
-      uint64_t up = __shfl_up_sync(0xffffffffu, x, 1);
-      uint64_t pv = lane ? up : carry;
-      carry = __shfl_sync(0xffffffffu, x, 31);
-      if (ok) {
-        umn = u64min(umn, x);
-        umx = u64max(umx, x);
-        int64_t sx = (int64_t)x;
-        smn = sx < smn ? sx : smn;
-        smx = sx > smx ? sx : smx;
-        uint64_t dz = zigzag64(x - (idx ? pv : x));
-        dzmn = u64min(dzmn, dz);
-        dzmx = u64max(dzmx, dz);
-        xb += varint_len(x ^ (idx ? pv : 0ull));
-        nq += (idx && x != pv) ? 1u : 0u;
-        sbad |= (x != v0 + (uint64_t)idx * stride) ? 1u : 0u;
-        if (alive) fmfail |= fm_fail_bits(x, alive);
-      }
-      if (do_fm && (j & 7) == 7) {
-        uint32_t f = warp_or(fmfail);
-        if (f && lane == 0) atomicAnd(&S.fm_mask, ~f);
-        alive = *(volatile uint32_t*)&S.fm_mask & ~f;
-        fmfail = 0;
-      }
-    }
-    umn = warp_min(umn);
-    umx = warp_max(umx);
-    smn = warp_min_i64(smn);
-    smx = warp_max_i64(smx);
-    dzmn = warp_min(dzmn);
-    dzmx = warp_max(dzmx);
-    xb = warp_sum(xb);
-    nq = warp_sum(nq);
-    sbad = warp_or(sbad);
-    if (lane == 0) {
-      S.w_a[k] = (uint8_t)(sgn ? bit_width64((uint64_t)smx - (uint64_t)smn) : bit_width64(umx - umn));
-      S.w_b[k] = (uint8_t)bit_width64(dzmx - dzmn);
-      S.neq_k[k] = nq;
-      atomicAdd(&S.xor_bytes, (unsigned long long)xb);
-      atomicAdd(&S.neq, nq);
-      atomicOr(&S.stride_bad, sbad);
-      atomic_min_u64(&S.umin, umn);
-      atomic_max_u64(&S.umax, umx);
-    }
-  }
-}
-
-// FLOAT_MULT k widths for the chosen scale (signed FoR of k).
-__device__ void fm_widths(EncSmem& S, const uint64_t* v, uint32_t n, int s) {
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t nsub = (n + kSub - 1) / kSub;
-  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
-    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
-    uint64_t mn;
-    uint32_t w;
-    warp_minmax(cnt, true, [&](uint32_t i) { return (uint64_t)fm_k(v[base + i], s); }, &mn, &w);
-    if (lane == 0) S.w_d[k] = (uint8_t)w;
-  }
-}
-
 // ALP for one sub-block (reference alp.rs:49-166): find_ef on the 32-value
 // sample, then the full encode statistics.  Warp-cooperative; returns false
 // when the sub-block (hence the block) bails.
@@ -510,17 +402,20 @@ __device__ inline uint32_t rd_code_bits(uint32_t dl) {
   return b ? b : 1;
 }
 
-// Returns the chosen left bit width, or 0 when ALP-RD does not apply.
-__device__ uint32_t rd_choose_cut(EncSmem& S, const uint64_t* v, uint32_t n) {
+// Returns the chosen left bit width, or 0 when ALP-RD does not apply.  The
+// sample is block[0], block[step], ... (step = max(n/2048, 1)); when `pre` is
+// given it holds those values at pre[i * pre_stride].
+__device__ uint32_t rd_choose_cut(EncSmem& S, const uint64_t* v, uint32_t n, const uint64_t* pre, uint32_t pre_stride) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t step = max(n / 2048u, 1u);
   uint32_t sn = (n + step - 1) / step;
   uint32_t P = pow2_at_least(sn);
   uint64_t* smp = S.big.rd.smp;
-  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) smp[i] = i < sn ? v[(uint64_t)i * step] : kEmpty64;
+  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
+    smp[i] = i < sn ? (pre ? pre[(uint64_t)i * pre_stride] : v[(uint64_t)i * step]) : kEmpty64;
   __syncthreads();
   block_bitonic_sort(smp, P);
-  for (uint32_t lbw = warp + 1; lbw <= 24; lbw += kEncWarps) {
+  for (uint32_t lbw = warp + 1; lbw <= 24; lbw += blockDim.x / 32) {
     uint32_t rbw = 64 - lbw;
     uint32_t t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     uint32_t last_start = 0, G = 0;
@@ -929,31 +824,250 @@ __device__ uint32_t* rle_starts(EncSmem& S, const uint64_t* v, uint32_t n, uint3
   return st;
 }
 
-// ---------------------------------------------------------------------------
-// The competition kernel.
-// ---------------------------------------------------------------------------
 struct Cand {
   uint64_t len;
   bool ok;
 };
 
-__device__ void init_smem(EncSmem& S, const uint64_t* v) {
-  if (threadIdx.x == 0) {
-    S.xor_bytes = 0;
-    S.umin = kEmpty64;
-    S.umax = 0;
-    S.neq = 0;
-    S.stride_bad = 0;
-    S.fm_mask = 0x7F;
-    S.alp_fail = 0;
-    S.flag = 0;
+// ---------------------------------------------------------------------------
+// Competition, part 1: per-sub-block statistics.  One warp per 1024-value
+// sub-block, one pass over the lane.  Quantities that depend on whether the
+// sub-block opens a block (its first value's delta / XOR / equality with the
+// previous value) are kept out of the internal sums and folded in by k_decide,
+// so the statistics are computed before the block plan exists.
+// ---------------------------------------------------------------------------
+struct SubStats {
+  uint64_t umin, umax, first, last, d;  // d = v[1] - v[0] of the sub-block
+  int64_t smin, smax;
+  uint64_t dzmin, dzmax;                // zigzag deltas of internal pairs (j >= 1)
+  uint64_t e16min, e16max, e16dz;       // early-out samples j % 16 == 0
+  uint64_t e64min, e64max, e64dz;       // early-out samples j % 64 == 0
+  uint32_t xb, neq, cnt;                // internal XORZ bytes, internal transitions, values
+  uint8_t stride_ok, alp_ok, alp_w, fm_pass;
+  uint16_t alp_exc, pad16;
+  uint32_t pad32;
+};
+static_assert(sizeof(SubStats) == 144, "SubStats layout");
+struct FmStat {  // signed min / max of k = round(x * scale) per FLOAT_MULT scale
+  int64_t kmin[7], kmax[7];
+};
+
+constexpr int kStatsWarps = 32;  // one CTA per 32768-value window in adaptive mode
+
+template <bool FLOATS>
+__global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
+    const uint64_t* __restrict__ v, uint64_t n, uint64_t fixed_bs, int dtype, int level,
+    SubStats* __restrict__ ss, FmStat* __restrict__ fms, uint64_t* __restrict__ smp16, uint8_t* __restrict__ grow,
+    uint32_t* __restrict__ winbits) {
+  __shared__ uint32_t bitsA[512], bitsB[512];
+  __shared__ uint64_t s_first[kStatsWarps], s_last[kStatsWarps];
+  __shared__ uint32_t s_neq[kStatsWarps], s_cnt[kStatsWarps];
+  __shared__ uint64_t alp_smp[kStatsWarps][32];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool do_float = FLOATS && level >= 1;
+  uint64_t item = (uint64_t)blockIdx.x * kStatsWarps + warp;
+  uint64_t s, cnt64;
+  if (fixed_bs) {
+    uint64_t spb = (fixed_bs + kSub - 1) / kSub;
+    uint64_t b = item / spb, k = item % spb;
+    uint64_t bstart = b * fixed_bs, bend = qmin(bstart + fixed_bs, n);
+    s = bstart + k * kSub;
+    cnt64 = (bstart < n && s < bend) ? qmin(kSub, bend - s) : 0;
+  } else {
+    s = item * kSub;
+    cnt64 = s < n ? qmin(kSub, n - s) : 0;
   }
+  uint32_t cnt = (uint32_t)cnt64;
+  // window probe sampling (adaptive): window-relative stride max(len/4096, 1)
+  uint64_t wstart = (uint64_t)blockIdx.x * kBaseQuantum;
+  uint32_t wlen = fixed_bs ? 0u : (uint32_t)(wstart < n ? qmin(kBaseQuantum, n - wstart) : 0);
+  uint32_t wstride = max(wlen / 4096u, 1u);
+  if (!fixed_bs) {
+    for (int i = threadIdx.x; i < 512; i += blockDim.x) {
+      bitsA[i] = 0;
+      bitsB[i] = 0;
+    }
+    __syncthreads();
+  }
+  SubStats R;
+  uint64_t umn = kEmpty64, umx = 0, dzmn = kEmpty64, dzmx = 0, xb = 0;
+  int64_t smn = INT64_MAX, smx = INT64_MIN;
+  uint64_t a16mn = kEmpty64, a16mx = 0, a16dz = 0, a64mn = kEmpty64, a64mx = 0, a64dz = 0;
+  uint32_t nq = 0, sbad = 0, fmfail = 0;
+  int64_t kmn[7], kmx[7];
+#pragma unroll
+  for (int q = 0; q < 7; q++) {
+    kmn[q] = INT64_MAX;
+    kmx[q] = INT64_MIN;
+  }
+  const uint64_t* sv = v + s;
+  uint64_t d = cnt >= 2 ? sv[1] - sv[0] : 0;
+  uint32_t alive = do_float ? 0x7Fu : 0u;
+  uint64_t carry = 0;
+  for (uint32_t r = 0; r < 32; r++) {
+    uint32_t j = r * 32 + lane;
+    bool ok = j < cnt;
+    uint64_t x = ok ? sv[j] : 0;
+    uint64_t up = __shfl_up_sync(0xffffffffu, x, 1);
+    uint64_t pv = lane ? up : carry;
+    carry = __shfl_sync(0xffffffffu, x, 31);
+    if (ok) {
+      umn = u64min(umn, x);
+      umx = u64max(umx, x);
+      int64_t sx = (int64_t)x;
+      smn = sx < smn ? sx : smn;
+      smx = sx > smx ? sx : smx;
+      if (j > 0) {
+        uint64_t dz = zigzag64(x - pv);
+        dzmn = u64min(dzmn, dz);
+        dzmx = u64max(dzmx, dz);
+        xb += varint_len(x ^ pv);
+        nq += x != pv ? 1u : 0u;
+        sbad |= (x - pv != d) ? 1u : 0u;
+      }
+      if ((j & 15) == 0) {
+        a16mn = u64min(a16mn, x);
+        a16mx = u64max(a16mx, x);
+        if (j > 0) a16dz = u64max(a16dz, zigzag64(x - pv));
+        if (smp16 && !fixed_bs) smp16[(s + j) >> 4] = x;
+      }
+      if ((j & 63) == 0) {
+        a64mn = u64min(a64mn, x);
+        a64mx = u64max(a64mx, x);
+        if (j > 0) a64dz = u64max(a64dz, zigzag64(x - pv));
+      }
+      if (!fixed_bs) {
+        uint32_t wj = (uint32_t)(s - wstart) + j;
+        if (wj % wstride == 0) {
+          uint32_t bk = (uint32_t)(((x * 0x9E3779B97F4A7C15ull) >> 50) & 0x3FFF);
+          atomicOr(&bitsA[bk >> 5], 1u << (bk & 31));
+        }
+        if ((wj & 31) == 0) {
+          uint32_t bk = (uint32_t)(((x * 0x9E3779B97F4A7C15ull) >> 50) & 0x3FFF);
+          atomicOr(&bitsB[bk >> 5], 1u << (bk & 31));
+        }
+      }
+      if (FLOATS && alive) {
+        double xd = as_f64(x);
+        uint32_t a2 = alive;
+        while (a2) {
+          int q = __ffs(a2) - 1;
+          a2 &= a2 - 1;
+          double sc = kFmScales[q];
+          double k = round_half_away(__dmul_rn(xd, sc));
+          bool good = is_finite_f64(k) && fabs(k) < 9.0e18 && f64_bits(__ddiv_rn(k, sc)) == x;
+          if (!good) {
+            fmfail |= 1u << q;
+          } else {
+            int64_t ki = __double2ll_rz(k);
+            kmn[q] = ki < kmn[q] ? ki : kmn[q];
+            kmx[q] = ki > kmx[q] ? ki : kmx[q];
+          }
+        }
+      }
+    }
+    if (do_float && (r & 7) == 7) alive &= ~warp_or(fmfail);
+  }
+  R.umin = warp_min(umn);
+  R.umax = warp_max(umx);
+  R.smin = warp_min_i64(smn);
+  R.smax = warp_max_i64(smx);
+  R.dzmin = warp_min(dzmn);
+  R.dzmax = warp_max(dzmx);
+  R.e16min = warp_min(a16mn);
+  R.e16max = warp_max(a16mx);
+  R.e16dz = warp_max(a16dz);
+  R.e64min = warp_min(a64mn);
+  R.e64max = warp_max(a64mx);
+  R.e64dz = warp_max(a64dz);
+  R.xb = (uint32_t)warp_sum(xb);
+  R.neq = warp_sum(nq);
+  R.stride_ok = warp_or(sbad) ? 0 : 1;
+  R.cnt = cnt;
+  R.first = cnt ? sv[0] : 0;
+  R.last = cnt ? sv[cnt - 1] : 0;
+  R.d = d;
+  R.fm_pass = do_float ? (uint8_t)(0x7Fu & ~warp_or(fmfail)) : 0;
+  R.alp_ok = 0;
+  R.alp_w = 0;
+  R.alp_exc = 0;
+  R.pad16 = 0;
+  R.pad32 = 0;
+  if (FLOATS && do_float && cnt) {
+    AlpSub a;
+    bool ok = alp_subblock(sv, cnt, alp_smp[warp], &a);
+    R.alp_ok = ok ? 1 : 0;
+    R.alp_w = ok ? (uint8_t)a.w : 0;
+    R.alp_exc = ok ? (uint16_t)a.exc : 0;
+  }
+  if (FLOATS && do_float) {
+#pragma unroll
+    for (int q = 0; q < 7; q++) {
+      int64_t a = warp_min_i64(kmn[q]), b = warp_max_i64(kmx[q]);
+      if (lane == 0) {
+        fms[item].kmin[q] = a;
+        fms[item].kmax[q] = b;
+      }
+    }
+  }
+  if (lane == 0) {
+    ss[item] = R;
+    s_first[warp] = R.first;
+    s_last[warp] = R.last;
+    s_neq[warp] = R.neq;
+    s_cnt[warp] = cnt;
+  }
+  if (fixed_bs) return;
+  // Window probe (reference encoder.rs:166-176, 705-750): grow the block at
+  // this window when the sampled distinct count is low or most consecutive
+  // values repeat.  consec_eq = len - transitions (the first element counts
+  // against itself).
   __syncthreads();
+  if (warp == 0 && wlen) {
+    uint32_t dc = 0;
+    for (int i = lane; i < 512; i += 32) dc += __popc(bitsA[i]);
+    dc = warp_sum(dc);
+    uint32_t tr = 0;
+    if (lane < kStatsWarps && s_cnt[lane]) {
+      tr = s_neq[lane];
+      if (lane > 0 && s_first[lane] != s_last[lane - 1]) tr++;
+    }
+    tr = warp_sum(tr);
+    if (lane == 0) {
+      uint32_t consec = wlen - tr;
+      grow[blockIdx.x] = (dc < 2048 || (uint64_t)consec * 2 > wlen) ? 1 : 0;
+    }
+    for (int i = lane; i < 512; i += 32) {
+      winbits[(uint64_t)blockIdx.x * 1024 + i] = bitsA[i];
+      winbits[(uint64_t)blockIdx.x * 1024 + 512 + i] = bitsB[i];
+    }
+  }
 }
 
-__global__ void __launch_bounds__(kEncThreads) k_compete(const uint64_t* __restrict__ lane, FrameDesc* frames,
-                                                         const uint32_t* __restrict__ nbp, int dtype, int level,
-                                                         uint8_t* __restrict__ scratch) {
+// ---------------------------------------------------------------------------
+// Competition, part 2: one CTA per block.  Candidate sizes in closed form
+// from the sub-block statistics, the integer early-out, the ALP-RD cut search,
+// and the DICT / RLE passes for compressible blocks (encoder.rs:275-469).
+// ---------------------------------------------------------------------------
+__device__ uint32_t popc_bits_block(EncSmem& S, const uint32_t* bits) {
+  uint32_t c = 0;
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) c += __popc(bits[i]);
+  c = warp_sum(c);
+  if ((threadIdx.x & 31) == 0) S.red32[threadIdx.x >> 5] = c;
+  __syncthreads();
+  uint32_t t = 0;
+  for (int w = 0; w < kEncWarps; w++) t += S.red32[w];
+  __syncthreads();
+  return t;
+}
+
+__global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restrict__ lane, FrameDesc* frames,
+                                                        const uint32_t* __restrict__ nbp, uint64_t fixed_bs,
+                                                        int dtype, int level, const SubStats* __restrict__ ss,
+                                                        const FmStat* __restrict__ fms,
+                                                        const uint64_t* __restrict__ smp16,
+                                                        const uint32_t* __restrict__ winbits,
+                                                        uint8_t* __restrict__ scratch) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   EncSmem& S = *reinterpret_cast<EncSmem*>(smem_raw);
   uint32_t b = blockIdx.x;
@@ -964,34 +1078,131 @@ __global__ void __launch_bounds__(kEncThreads) k_compete(const uint64_t* __restr
   uint8_t* scr = scratch + fd.value_off * kEncScratchPerValue;
   bool fam_float = dtype_float(dtype);
   bool reduced = level == 0;
+  bool sgn = dtype_signed(dtype);
   uint64_t lambda = level_lambda(level);
   uint64_t lb = lane_bytes(dtype);
   uint64_t decoded_bytes = (uint64_t)n * lb, raw_bytes = (uint64_t)n * 8;
   uint32_t nsub = (n + kSub - 1) / kSub;
-
-  init_smem(S, v);
-  stats_pass(S, v, n, dtype, fam_float && !reduced);
+  uint64_t g0 = fixed_bs ? (uint64_t)b * ((fixed_bs + kSub - 1) / kSub) : fd.value_off / kSub;
+  int t = threadIdx.x, lane_id = t & 31, warp = t >> 5;
+  uint32_t step = max(n / 2048u, 1u);
+  // Early-out samples from the statistics when the block is a full adaptive block.
+  bool pre_e = !fixed_bs && (step == 16 || step == 64) && (fd.value_off % kBaseQuantum) == 0;
+  if (t == 0) {
+    S.xor_bytes = 0;
+    S.umin = kEmpty64;
+    S.umax = 0;
+    S.e_vmin = kEmpty64;
+    S.e_vmax = 0;
+    S.e_dmax = 0;
+    S.neq = 0;
+    S.stride_bad = 0;
+    S.fm_mask = 0x7F;
+    S.alp_fail = 0;
+    S.acc64 = 0;
+    S.sc[1] = 0;
+    S.sc[2] = 0;
+    S.sc[4] = 0;
+  }
   __syncthreads();
-  sample_features(S, v, n);
+  uint64_t D = n >= 2 ? v[1] - v[0] : 0;
+  uint64_t my_for = 0, my_delta = 0, my_alp = 0;
+  for (uint32_t k = t; k < nsub; k += blockDim.x) {
+    SubStats R = ss[g0 + k];
+    uint64_t pl = k ? ss[g0 + k - 1].last : 0;
+    uint32_t wf = sgn ? bit_width64((uint64_t)R.smax - (uint64_t)R.smin) : bit_width64(R.umax - R.umin);
+    uint64_t dzf = k ? zigzag64(R.first - pl) : 0;
+    uint64_t dmn = R.cnt > 1 ? u64min(R.dzmin, dzf) : dzf, dmx = R.cnt > 1 ? u64max(R.dzmax, dzf) : dzf;
+    my_for += 9 + 128ull * wf;
+    my_delta += 9 + 128ull * bit_width64(dmx - dmn);
+    uint32_t nq = R.neq + ((k && R.first != pl) ? 1u : 0u);
+    S.neq_k[k] = nq;
+    S.item_min[k] = R.umin;
+    S.item_max[k] = R.umax;
+    atomicAdd(&S.neq, nq);
+    atomicAdd(&S.xor_bytes, (unsigned long long)(R.xb + varint_len(R.first ^ pl)));
+    atomic_min_u64(&S.umin, R.umin);
+    atomic_max_u64(&S.umax, R.umax);
+    bool sok = R.stride_ok && (R.cnt < 2 || R.d == D) && (k == 0 || R.first - pl == D);
+    if (!sok) atomicOr(&S.stride_bad, 1u);
+    if (pre_e) {
+      uint64_t emn = step == 16 ? R.e16min : R.e64min, emx = step == 16 ? R.e16max : R.e64max;
+      uint64_t edz = step == 16 ? R.e16dz : R.e64dz;
+      if (k) edz = u64max(edz, dzf);
+      atomic_min_u64(&S.e_vmin, emn);
+      atomic_max_u64(&S.e_vmax, emx);
+      atomic_max_u64(&S.e_dmax, edz);
+    }
+    if (fam_float && !reduced) {
+      atomicAnd(&S.fm_mask, (uint32_t)R.fm_pass);
+      if (!R.alp_ok) atomicOr(&S.alp_fail, 1u);
+      my_alp += 13 + 128ull * R.alp_w + 10ull * R.alp_exc;
+    }
+  }
+  my_for = warp_sum(my_for);
+  my_delta = warp_sum(my_delta);
+  my_alp = warp_sum(my_alp);
+  if (lane_id == 0) {
+    atomicAdd((unsigned long long*)&S.sc[1], (unsigned long long)my_for);
+    atomicAdd((unsigned long long*)&S.sc[2], (unsigned long long)my_delta);
+    atomicAdd((unsigned long long*)&S.sc[4], (unsigned long long)my_alp);
+  }
+  __syncthreads();
+  uint64_t vl = varint_len(n);
+  uint64_t sz_for = vl + S.sc[1], sz_delta = 8 + vl + S.sc[2], sz_alp = vl + S.sc[4];
 
-  // Integer early-out (reference encoder.rs:295-298,655-683).
-  if (threadIdx.x == 0) {
-    uint32_t distinct = 0;
-    for (int i = 0; i < 512; i++) distinct += __popc(S.distinct_bits[i]);
-    bool distinct_low = distinct < 2048;
+  // Integer early-out (encoder.rs:295-298, 655-683) with the block's features.
+  bool eo = false;
+  if (!fam_float) {
     uint32_t consec_eq = n - S.neq;
     bool repeats = (uint64_t)consec_eq * 2 > (uint64_t)n;
-    bool eo = false;
-    if (!fam_float && !(distinct_low || repeats || n < 256)) {
+    uint32_t dstride = max(n / 4096u, 1u);
+    uint32_t distinct;
+    uint64_t wi = fd.value_off / kBaseQuantum;
+    if (!fixed_bs && dstride == 8 && n == (uint32_t)kBaseQuantum) {
+      distinct = popc_bits_block(S, winbits + wi * 1024);
+    } else if (!fixed_bs && dstride == 32 && n == (uint32_t)kMaxBlock) {
+      for (int i = t; i < 512; i += blockDim.x)
+        S.distinct_bits[i] = winbits[wi * 1024 + 512 + i] | winbits[(wi + 1) * 1024 + 512 + i] |
+                             winbits[(wi + 2) * 1024 + 512 + i] | winbits[(wi + 3) * 1024 + 512 + i];
+      __syncthreads();
+      distinct = popc_bits_block(S, S.distinct_bits);
+    } else {
+      for (int i = t; i < 512; i += blockDim.x) S.distinct_bits[i] = 0;
+      __syncthreads();
+      for (uint32_t i = t; (uint64_t)i * dstride < n; i += blockDim.x) {
+        uint64_t h = v[(uint64_t)i * dstride] * 0x9E3779B97F4A7C15ull;
+        uint32_t bk = (uint32_t)((h >> 50) & 0x3FFF);
+        atomicOr(&S.distinct_bits[bk >> 5], 1u << (bk & 31));
+      }
+      __syncthreads();
+      distinct = popc_bits_block(S, S.distinct_bits);
+    }
+    bool distinct_low = distinct < 2048;
+    if (!(distinct_low || repeats || n < 256)) {
+      if (!pre_e) {
+        if (t == 0) {
+          S.e_vmin = v[0];
+          S.e_vmax = v[0];
+          S.e_dmax = 0;
+        }
+        __syncthreads();
+        for (uint32_t i = t; (uint64_t)i * step < n; i += blockDim.x) {
+          uint32_t idx = i * step;
+          uint64_t x = v[idx];
+          atomic_min_u64(&S.e_vmin, x);
+          atomic_max_u64(&S.e_vmax, x);
+          if (idx >= step) atomic_max_u64(&S.e_dmax, zigzag64(x - v[idx - 1]));
+        }
+        __syncthreads();
+      }
       uint32_t thr = (uint32_t)(lb * 8) - 4;
       uint32_t vw = bit_width64(S.e_vmax - S.e_vmin), dw = bit_width64(S.e_dmax);
       eo = vw >= thr && dw >= thr;
     }
-    S.flag = eo ? 1u : 0u;
   }
-  __syncthreads();
-  if (S.flag) {
-    if (threadIdx.x == 0) {
+  if (eo) {
+    if (t == 0) {
       frames[b].mode = M_RAW;
       frames[b].plen = (uint32_t)decoded_bytes;
       frames[b].aux = 0;
@@ -1000,77 +1211,40 @@ __global__ void __launch_bounds__(kEncThreads) k_compete(const uint64_t* __restr
     return;
   }
 
-  // Candidates in the reference's consideration order (encoder.rs:301-344).
-  uint64_t vl = varint_len(n);
-  uint64_t sz_for = vl, sz_delta = 8 + vl;
-  if (threadIdx.x == 0) {
-    for (uint32_t k = 0; k < nsub; k++) {
-      sz_for += 9 + 128ull * S.w_a[k];
-      sz_delta += 9 + 128ull * S.w_b[k];
-    }
-    S.sc[1] = sz_for;
-    S.sc[2] = sz_delta;
-  }
-  __syncthreads();
-  sz_for = S.sc[1];
-  sz_delta = S.sc[2];
-
   Cand c_fm = {0, false}, c_alp = {0, false}, c_rd = {0, false};
   uint32_t fm_scale = 0, rd_lbw = 0;
   if (fam_float && !reduced) {
-    // FLOAT_MULT (float_mult.rs:66-98, bit-packed k)
     uint32_t mask = S.fm_mask;
-    if (mask) {
+    if (mask) {  // FLOAT_MULT (float_mult.rs:66-98, bit-packed k)
       fm_scale = __ffs(mask) - 1;
-      fm_widths(S, v, n, (int)fm_scale);
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        uint64_t s = 2 + vl;
-        for (uint32_t k = 0; k < nsub; k++) s += 9 + 128ull * S.w_d[k];
-        S.sc[3] = s;
+      uint64_t my = 0;
+      for (uint32_t k = t; k < nsub; k += blockDim.x) {
+        const FmStat& F = fms[g0 + k];
+        my += 9 + 128ull * bit_width64((uint64_t)F.kmax[fm_scale] - (uint64_t)F.kmin[fm_scale]);
       }
+      my = warp_sum(my);
+      if (lane_id == 0) S.red[warp] = my;
+      __syncthreads();
+      uint64_t tot = 0;
+      for (int w = 0; w < kEncWarps; w++) tot += S.red[w];
       __syncthreads();
       c_fm.ok = true;
-      c_fm.len = S.sc[3];
+      c_fm.len = 2 + vl + tot;
     }
-    // ALP (alp.rs:93-166)
-    {
-      int lane_id = threadIdx.x & 31, warp = threadIdx.x >> 5;
-      for (uint32_t k = warp; k < nsub; k += kEncWarps) {
-        if (__shfl_sync(0xffffffffu, *(volatile uint32_t*)&S.alp_fail, 0)) break;
-        uint32_t cnt = min((uint32_t)kSub, n - k * kSub);
-        AlpSub a;
-        bool ok = alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], &a);
-        if (lane_id == 0) {
-          if (!ok) S.alp_fail = 1;
-          else {
-            S.w_c[k] = (uint8_t)a.w;
-            S.alp_exc[k] = (uint16_t)a.exc;
-          }
-        }
-      }
-      __syncthreads();
-      if (threadIdx.x == 0 && !S.alp_fail) {
-        uint64_t s = vl;
-        for (uint32_t k = 0; k < nsub; k++) s += 13 + 128ull * S.w_c[k] + 10ull * S.alp_exc[k];
-        S.sc[4] = s;
-      }
-      __syncthreads();
-      c_alp.ok = !S.alp_fail;
-      c_alp.len = S.sc[4];
-    }
+    c_alp.ok = !S.alp_fail;  // ALP (alp.rs:93-166)
+    c_alp.len = sz_alp;
     // ALP-RD (alp_rd.rs:132-206, bit-packed streams)
-    rd_lbw = rd_choose_cut(S, v, n);
+    bool pre_s = smp16 && !fixed_bs && (step == 16 || step == 64) && (fd.value_off % kBaseQuantum) == 0;
+    rd_lbw = rd_choose_cut(S, v, n, pre_s ? smp16 + fd.value_off / 16 : nullptr, step / 16);
     if (rd_lbw) {
       rd_top8(S, v, n, rd_lbw, scr);
       uint32_t rbw = 64 - rd_lbw;
       uint64_t rmask = (1ull << rbw) - 1ull;
-      if (threadIdx.x == 0) {
+      if (t == 0) {
         S.acc64 = 0;
         S.cnt32 = 0;
       }
       __syncthreads();
-      int lane_id = threadIdx.x & 31, warp = threadIdx.x >> 5;
       for (uint32_t k = warp; k < nsub; k += kEncWarps) {
         uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
         uint64_t cmx = 0, rmn = kEmpty64, rmx = 0, cmn = kEmpty64, eb = 0;
@@ -1102,7 +1276,7 @@ __global__ void __launch_bounds__(kEncThreads) k_compete(const uint64_t* __restr
         }
       }
       __syncthreads();
-      if (threadIdx.x == 0) {
+      if (t == 0) {
         uint64_t nexc = S.cnt32;
         uint64_t clen = vl, rlen = vl;
         for (uint32_t k = 0; k < nsub; k++) {
@@ -1123,9 +1297,9 @@ __global__ void __launch_bounds__(kEncThreads) k_compete(const uint64_t* __restr
   uint64_t best_len = decoded_bytes;
   uint64_t best_score = best_len + ((lambda * decode_weight(M_RAW) * decoded_bytes) >> 8);
   auto consider = [&](int m, uint64_t len) {
-    uint64_t s = len + ((lambda * decode_weight(m) * decoded_bytes) >> 8);
-    if (s < best_score) {
-      best_score = s;
+    uint64_t sc = len + ((lambda * decode_weight(m) * decoded_bytes) >> 8);
+    if (sc < best_score) {
+      best_score = sc;
       best_mode = m;
       best_len = len;
     }
@@ -1141,12 +1315,23 @@ __global__ void __launch_bounds__(kEncThreads) k_compete(const uint64_t* __restr
   bool block_compressible = best_len * 20 < raw_bytes * 19;  // encoder.rs:394,644-646
 
   if (block_compressible && !reduced) {
-    // DICT (dict.rs:87-152, bit-packed codes)
+    // DICT (dict.rs:87-152, bit-packed codes).  The dictionary is sorted, so
+    // a sub-block's code range is [rank(min), rank(max)].
     DictView dv = dict_prepare(S, v, n, scr);
     if (!S.flag) {
       uint32_t vtag;
       uint64_t vlen = dict_values_len(S, dv, &vtag);
-      uint64_t clen = block_for(S, nullptr, n, false, [&](uint32_t i) { return (uint64_t)dict_rank(S, dv, v[i]); });
+      uint64_t my = 0;
+      for (uint32_t k = t; k < nsub; k += blockDim.x) {
+        uint32_t r0 = dict_rank(S, dv, S.item_min[k]), r1 = dict_rank(S, dv, S.item_max[k]);
+        my += 9 + 128ull * bit_width64((uint64_t)(r1 - r0));
+      }
+      my = warp_sum(my);
+      if (lane_id == 0) S.red[warp] = my;
+      __syncthreads();
+      uint64_t clen = vl;
+      for (int w = 0; w < kEncWarps; w++) clen += S.red[w];
+      __syncthreads();
       consider(M_DICT, varint_len(dv.card) + 1 + varint_len(vlen) + vlen + 1 + clen);
     }
     __syncthreads();
@@ -1161,7 +1346,7 @@ __global__ void __launch_bounds__(kEncThreads) k_compete(const uint64_t* __restr
       consider(M_RLE, varint_len(runs) + 8ull * runs + lens);
     }
   }
-  if (threadIdx.x == 0) {
+  if (t == 0) {
     frames[b].mode = (uint32_t)best_mode;
     frames[b].plen = (uint32_t)best_len;
     frames[b].aux = best_mode == M_FLOAT_MULT ? fm_scale : best_mode == M_ALP_RD ? rd_lbw : 0;
@@ -1493,36 +1678,6 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
 // Window probe, block planning and frame offsets.
 // ---------------------------------------------------------------------------
 
-// One CTA per 32768-value window: grow flag = distinct_low || repeats
-// (reference encoder.rs:166-176, 705-750).
-__global__ void k_probe_windows(const uint64_t* __restrict__ v, uint64_t n, uint8_t* __restrict__ grow) {
-  __shared__ uint32_t bits[512];
-  __shared__ uint32_t s_neq;
-  uint64_t s = (uint64_t)blockIdx.x * kBaseQuantum;
-  uint32_t len = (uint32_t)qmin(kBaseQuantum, n - s);
-  const uint64_t* w = v + s;
-  for (int i = threadIdx.x; i < 512; i += blockDim.x) bits[i] = 0;
-  if (threadIdx.x == 0) s_neq = 0;
-  __syncthreads();
-  uint32_t nq = 0;
-  for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) nq += (i && w[i] != w[i - 1]) ? 1u : 0u;
-  nq = warp_sum(nq);
-  if ((threadIdx.x & 31) == 0) atomicAdd(&s_neq, nq);
-  uint32_t stride = max(len / 4096u, 1u);
-  for (uint32_t i = threadIdx.x; (uint64_t)i * stride < len; i += blockDim.x) {
-    uint64_t h = w[(uint64_t)i * stride] * 0x9E3779B97F4A7C15ull;
-    uint32_t b = (uint32_t)((h >> 50) & 0x3FFF);
-    atomicOr(&bits[b >> 5], 1u << (b & 31));
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t d = 0;
-    for (int i = 0; i < 512; i++) d += __popc(bits[i]);
-    uint32_t consec = len - s_neq;
-    grow[blockIdx.x] = (d < 2048 || (uint64_t)consec * 2 > len) ? 1 : 0;
-  }
-}
-
 // Block plan (reference encoder.rs:154-178): fills frames[].value_off / .n.
 __global__ void k_plan(const uint8_t* __restrict__ grow, uint64_t n, uint64_t fixed_bs, FrameDesc* frames,
                        uint32_t* nb) {
@@ -1595,12 +1750,6 @@ __global__ void k_frame_apply(FrameDesc* frames, const uint32_t* __restrict__ nb
 // ---------------------------------------------------------------------------
 static size_t enc_smem_bytes() { return sizeof(EncSmem); }
 
-void launch_probe_windows(const uint64_t* lane, uint64_t n, uint8_t* grow, cudaStream_t st) {
-  uint64_t nw = (n + kBaseQuantum - 1) / kBaseQuantum;
-  if (nw) k_probe_windows<<<(unsigned)nw, 256, 0, st>>>(lane, n, grow);
-  count_launches(nw ? 1 : 0);
-}
-
 void launch_plan(const uint8_t* grow, uint64_t n, uint64_t fixed_bs, FrameDesc* frames, uint32_t* nb,
                  cudaStream_t st) {
   unsigned g = 1;
@@ -1610,12 +1759,36 @@ void launch_plan(const uint8_t* grow, uint64_t n, uint64_t fixed_bs, FrameDesc* 
   count_launches(1);
 }
 
-void launch_compete(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, int dtype,
-                    int level, uint8_t* scratch, unsigned long long* wins, cudaStream_t st) {
-  (void)wins;
-  cudaFuncSetAttribute(k_compete, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)enc_smem_bytes());
+uint64_t sub_stats_items(uint64_t n, uint64_t fixed_bs) {
+  if (fixed_bs) return ((n + fixed_bs - 1) / fixed_bs) * ((fixed_bs + kSub - 1) / kSub);
+  return ((n + kBaseQuantum - 1) / kBaseQuantum) * (uint64_t)kStatsWarps;
+}
+uint64_t sub_stats_bytes() { return sizeof(SubStats); }
+uint64_t fm_stats_bytes() { return sizeof(FmStat); }
+
+void launch_sub_stats(const uint64_t* lane, uint64_t n, uint64_t fixed_bs, int dtype, int level, void* ss, void* fms,
+                      uint64_t* smp16, uint8_t* grow, uint32_t* winbits, cudaStream_t st) {
+  uint64_t items = sub_stats_items(n, fixed_bs);
+  unsigned g = (unsigned)((items + kStatsWarps - 1) / kStatsWarps);
+  if (!g) return;
+  if (dtype_float(dtype))
+    k_sub_stats<true><<<g, kStatsWarps * 32, 0, st>>>(lane, n, fixed_bs, dtype, level, (SubStats*)ss, (FmStat*)fms,
+                                                       smp16, grow, winbits);
+  else
+    k_sub_stats<false><<<g, kStatsWarps * 32, 0, st>>>(lane, n, fixed_bs, dtype, level, (SubStats*)ss,
+                                                        (FmStat*)fms, nullptr, grow, winbits);
+  count_launches(1);
+}
+
+void launch_decide(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, uint64_t fixed_bs,
+                   int dtype, int level, const void* ss, const void* fms, const uint64_t* smp16,
+                   const uint32_t* winbits, uint8_t* scratch, cudaStream_t st) {
+  cudaFuncSetAttribute(k_decide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)enc_smem_bytes());
   cudaFuncSetAttribute(k_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)enc_smem_bytes());
-  if (max_blocks) k_compete<<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, dtype, level, scratch);
+  if (max_blocks)
+    k_decide<<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, fixed_bs, dtype, level,
+                                                                (const SubStats*)ss, (const FmStat*)fms, smp16,
+                                                                winbits, scratch);
   count_launches(max_blocks ? 1 : 0);
 }
 

@@ -194,7 +194,8 @@ inline int plain_code(int ext) {
 // ---------------------------------------------------------------------------
 enum Slot {
   S_IN, S_BM, S_RANK, S_LANE, S_GROW, S_FRAMES, S_NB, S_SIZES, S_TILE, S_SCRATCH, S_OUT, S_VTMP, S_VBLOB,
-  S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_DAUX, S_COUNT
+  S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_DAUX, S_SUBST, S_FMST,
+  S_SMP16, S_WINBITS, S_COUNT
 };
 
 struct QuoinCtx {
@@ -349,17 +350,29 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
   CK(c->ensure(S_SIZES, maxb * 8));
   CK(c->ensure(S_TILE, (scan_tile_count(maxb) + 16) * 8));
   CK(c->ensure(S_SCRATCH, n * kEncScratchPerValue + 256));
-  CK(c->ensure(S_GROW, (n + kBaseQuantumH - 1) / kBaseQuantumH + 16));
+  uint64_t nwin = (n + kBaseQuantumH - 1) / kBaseQuantumH;
+  uint64_t items = sub_stats_items(n, bs);
+  bool fl = j.dtype == WT_F64 || j.dtype == WT_F32;
+  CK(c->ensure(S_GROW, nwin + 16));
+  CK(c->ensure(S_SUBST, (items + 1) * sub_stats_bytes()));
+  CK(c->ensure(S_WINBITS, (nwin + 1) * 1024 * 4));
+  if (fl) {
+    CK(c->ensure(S_FMST, (items + 1) * fm_stats_bytes()));
+    CK(c->ensure(S_SMP16, (n / 16 + 2) * 8));
+  }
   FrameDesc* fr = c->p<FrameDesc>(S_FRAMES);
   uint32_t* nb = c->p<uint32_t>(S_NB);
   {
     TimedRegion tr(T_PLAN, st);
-    if (!bs) launch_probe_windows(j.lane, n, c->p<uint8_t>(S_GROW), st);
+    launch_sub_stats(j.lane, n, bs, j.dtype, j.level, c->p<void>(S_SUBST), fl ? c->p<void>(S_FMST) : nullptr,
+                     fl ? c->p<uint64_t>(S_SMP16) : nullptr, c->p<uint8_t>(S_GROW), c->p<uint32_t>(S_WINBITS), st);
     launch_plan(c->p<uint8_t>(S_GROW), n, bs, fr, nb, st);
   }
   {
     TimedRegion tr(T_COMPETE, st);
-    launch_compete(j.lane, fr, nb, (uint32_t)maxb, j.dtype, j.level, c->p<uint8_t>(S_SCRATCH), nullptr, st);
+    launch_decide(j.lane, fr, nb, (uint32_t)maxb, bs, j.dtype, j.level, c->p<void>(S_SUBST),
+                  fl ? c->p<void>(S_FMST) : nullptr, fl ? c->p<uint64_t>(S_SMP16) : nullptr,
+                  c->p<uint32_t>(S_WINBITS), c->p<uint8_t>(S_SCRATCH), st);
   }
   {
     TimedRegion tr(T_OTHER, st);

@@ -24,11 +24,22 @@ void launch_decimal_combine(const uint64_t* limbs, uint64_t limb_stride, int nli
 // Per-block scratch the competition may use: 32 bytes per lane value.
 constexpr uint64_t kEncScratchPerValue = 32;
 
-void launch_probe_windows(const uint64_t* lane, uint64_t n, uint8_t* grow, cudaStream_t st);
+// Competition part 1: per-sub-block statistics (and, for adaptive blocks, the
+// window grow flags and probe bitsets).  Sizes: sub_stats_items(n, bs) records
+// of sub_stats_bytes(); FLOAT_MULT records of fm_stats_bytes() for float
+// columns; smp16 holds n/16 + 1 values (float columns); grow one byte per
+// 32768-value window and winbits 1024 words per window.
+uint64_t sub_stats_items(uint64_t n, uint64_t fixed_bs);
+uint64_t sub_stats_bytes();
+uint64_t fm_stats_bytes();
+void launch_sub_stats(const uint64_t* lane, uint64_t n, uint64_t fixed_bs, int dtype, int level, void* ss, void* fms,
+                      uint64_t* smp16, uint8_t* grow, uint32_t* winbits, cudaStream_t st);
 void launch_plan(const uint8_t* grow, uint64_t n, uint64_t fixed_bs, FrameDesc* frames, uint32_t* nb,
                  cudaStream_t st);
-void launch_compete(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, int dtype,
-                    int level, uint8_t* scratch, unsigned long long* wins, cudaStream_t st);
+// Competition part 2: one CTA per planned block; writes mode / plen / aux.
+void launch_decide(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, uint64_t fixed_bs,
+                   int dtype, int level, const void* ss, const void* fms, const uint64_t* smp16,
+                   const uint32_t* winbits, uint8_t* scratch, cudaStream_t st);
 // `base` (device) holds the byte offset at which the first frame starts.
 void launch_frame_offsets(FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, const uint64_t* base,
                           uint64_t* sizes_tmp, uint64_t* tile_tmp, uint64_t* total, cudaStream_t st);
