@@ -279,7 +279,6 @@ def run_gpu(args, rank, world, local):
     ms_arr = (ctypes.c_double * 8)()
     calls_arr = (ctypes.c_uint64 * 8)()
     L.quoin_b200_timing_read(ms_arr, calls_arr, 8)
-    L.quoin_b200_timing_enable(0)
     enc_ms = sum(ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps))
     dec_ms = sum(ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps))
     total_ms = ev[0].elapsed_time(ev[-1])
@@ -300,6 +299,28 @@ def run_gpu(args, rank, world, local):
     }
     per_class = {TIMER_NAMES[i]: (ms_arr[i], int(calls_arr[i])) for i in range(8)}
     dom = max(alg, key=lambda k: per_class[k][0])
+
+    # Per-column kernel-class breakdown (one untimed extra pass per column).
+    per_column = {}
+    for c in gcols:
+        L.quoin_b200_timing_enable(1)
+        with torch.cuda.stream(stream):
+            olen = ctypes.c_size_t()
+            rc = L.quoin_b200_compress_column_device(
+                ctx, c["wire"], n, P(c["d_vals"].data_ptr()), P(c["d_bm"].data_ptr()) if c["d_bm"] is not None else None,
+                0, 0, ctypes.byref(cfg), P(c["d_dst"].data_ptr()), c["cap"], ctypes.byref(olen), P(stream.cuda_stream))
+            if rc:
+                raise Q.Error(rc)
+            rc = L.quoin_b200_decompress_indexed_device(ctx, c["idx"], P(c["d_dst"].data_ptr()),
+                                                        P(c["d_out"].data_ptr()), P(c["d_vout"].data_ptr()),
+                                                        P(stream.cuda_stream))
+            if rc:
+                raise Q.Error(rc)
+        torch.cuda.synchronize()
+        L.quoin_b200_timing_read(ms_arr, calls_arr, 8)
+        per_column[c["name"]] = {TIMER_NAMES[i]: round(ms_arr[i], 4) for i in range(8) if ms_arr[i] > 0}
+        per_column[c["name"]]["stream_bytes"] = c["len"]
+    L.quoin_b200_timing_enable(0)
     dom_ms, dom_calls = per_class[dom]
     achieved = alg[dom] * args.steps / (dom_ms / 1e3) / 1e9 if dom_ms else 0.0
 
@@ -369,6 +390,7 @@ def run_gpu(args, rank, world, local):
             "decode_gbs": round(raw_bytes * world * args.steps / (dec_ms / 1e3) / 1e9, 3),
             "ratio": round(raw_bytes / stream_bytes, 4), "bit_exact": bit_exact,
             "kernel_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in per_class.items()},
+            "per_column_ms": per_column,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": None, "launches_per_step": dom_calls // max(args.steps, 1)},

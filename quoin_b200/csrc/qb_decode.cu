@@ -254,7 +254,7 @@ __device__ inline void warp_unpack(const uint8_t* p, uint32_t off, uint32_t coun
     for (uint32_t i = l; i < count; i += 32) f(i, mn);
   } else if (w <= 32) {
     uint32_t mask = w == 32 ? 0xFFFFFFFFu : ((1u << w) - 1u);
-#pragma unroll 4
+#pragma unroll 8
     for (uint32_t r = 0; r < 32; r++) {
       uint32_t idx = r * 32 + l;
       uint32_t bit = r * w, word = bit >> 5, sh = bit & 31;
@@ -266,7 +266,7 @@ __device__ inline void warp_unpack(const uint8_t* p, uint32_t off, uint32_t coun
   } else {
     uint64_t mask = w == 64 ? ~0ull : ((1ull << w) - 1ull);
     uint32_t fl = l & 15, r0 = (l >> 4) * 32;
-#pragma unroll 4
+#pragma unroll 8
     for (uint32_t r = r0; r < r0 + 32; r++) {
       uint32_t idx = r * 16 + fl;
       uint32_t bit = r * w, word = bit >> 6, sh = bit & 63;

@@ -181,13 +181,23 @@ __device__ inline void warp_minmax(uint32_t cnt, bool sgn, V val, uint64_t* mn_o
   int lane = threadIdx.x & 31;
   uint64_t umn = kEmpty64, umx = 0;
   int64_t smn = INT64_MAX, smx = INT64_MIN;
-  for (uint32_t i = lane; i < cnt; i += 32) {
-    uint64_t x = val(i);
+  for (uint32_t i0 = lane; i0 < cnt; i0 += 32 * 8) {
+   uint64_t xs[8];
+#pragma unroll
+   for (int q = 0; q < 8; q++) {
+     uint32_t iq = i0 + 32 * q;
+     xs[q] = iq < cnt ? val(iq) : 0ull;
+   }
+#pragma unroll
+   for (int q = 0; q < 8; q++) {
+    if (i0 + 32 * q >= cnt) break;
+    uint64_t x = xs[q];
     umn = u64min(umn, x);
     umx = u64max(umx, x);
     int64_t s = (int64_t)x;
     smn = s < smn ? s : smn;
     smx = s > smx ? s : smx;
+   }
   }
   if (sgn) {
     smn = warp_min_i64(smn);
@@ -217,9 +227,16 @@ __device__ inline void warp_for_pack(uint8_t* dst, uint32_t cnt, uint64_t mn, ui
   if (w <= 32) {
     uint64_t acc = 0;
     uint32_t nb = 0, wd = 0;
-    for (uint32_t r = 0; r < 32; r++) {
-      uint32_t i = r * 32 + lane;
-      uint32_t res = i < cnt ? (uint32_t)(val(i) - mn) : 0u;
+    for (uint32_t r0 = 0; r0 < 32; r0 += 8) {
+     uint32_t rs[8];
+#pragma unroll
+     for (int q = 0; q < 8; q++) {
+       uint32_t iq = (r0 + q) * 32 + lane;
+       rs[q] = iq < cnt ? (uint32_t)(val(iq) - mn) : 0u;
+     }
+#pragma unroll
+     for (int q = 0; q < 8; q++) {
+      uint32_t res = rs[q];
       if (w < 32) res &= (1u << w) - 1u;
       acc |= (uint64_t)res << nb;
       nb += w;
@@ -229,13 +246,21 @@ __device__ inline void warp_for_pack(uint8_t* dst, uint32_t cnt, uint64_t mn, ui
         acc >>= 32;
         nb -= 32;
       }
+     }
     }
   } else if (lane < 16) {
     unsigned __int128 acc = 0;
     uint32_t nb = 0, wd = 0;
-    for (uint32_t r = 0; r < 64; r++) {
-      uint32_t i = r * 16 + lane;
-      uint64_t res = i < cnt ? (val(i) - mn) : 0ull;
+    for (uint32_t r0 = 0; r0 < 64; r0 += 8) {
+     uint64_t rs[8];
+#pragma unroll
+     for (int q = 0; q < 8; q++) {
+       uint32_t iq = (r0 + q) * 16 + lane;
+       rs[q] = iq < cnt ? (val(iq) - mn) : 0ull;
+     }
+#pragma unroll
+     for (int q = 0; q < 8; q++) {
+      uint64_t res = rs[q];
       if (w < 64) res &= (1ull << w) - 1ull;
       acc |= (unsigned __int128)res << nb;
       nb += w;
@@ -245,6 +270,7 @@ __device__ inline void warp_for_pack(uint8_t* dst, uint32_t cnt, uint64_t mn, ui
         acc >>= 64;
         nb -= 64;
       }
+     }
     }
   }
 }
@@ -642,8 +668,18 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
     S.flag = 0;
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    uint64_t x = v[i];
+  for (uint32_t base = 0; base < n; base += blockDim.x * 8) {
+   uint64_t xs[8];
+#pragma unroll
+   for (int q = 0; q < 8; q++) {
+     uint32_t iq = base + q * blockDim.x + threadIdx.x;
+     xs[q] = iq < n ? v[iq] : 0ull;
+   }
+#pragma unroll 1
+   for (int q = 0; q < 8; q++) {
+    uint32_t i = base + q * blockDim.x + threadIdx.x;
+    if (i >= n) break;
+    uint64_t x = xs[q];
     uint32_t b = (uint32_t)((x * 0xD6E8FEB86659FD93ull) >> (64 - 17));
     atomicOr(&D.lb[b >> 5], 1u << (b & 31));
     if (*(volatile uint32_t*)&S.ovf) continue;
@@ -668,6 +704,7 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
       else h = (h + 1) & (kHashCap - 1);
     }
     if (!done) S.ovf = 1;
+   }
   }
   __syncthreads();
   DictView dv;
@@ -806,11 +843,20 @@ __device__ uint32_t* rle_starts(EncSmem& S, const uint64_t* v, uint32_t n, uint3
     uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
     uint64_t carry = base ? v[base - 1] : v[0];
     uint32_t before = S.subsz[k];
-    for (uint32_t j = 0; j < 32; j++) {
+    for (uint32_t j0 = 0; j0 < 32; j0 += 8) {
+     uint64_t xs[8];
+#pragma unroll
+     for (int q = 0; q < 8; q++) {
+       uint32_t lq = (j0 + q) * 32 + lane;
+       xs[q] = lq < cnt ? v[base + lq] : 0ull;
+     }
+#pragma unroll
+     for (int q = 0; q < 8; q++) {
+      uint32_t j = j0 + q;
       uint32_t li = j * 32 + lane;
       bool ok = li < cnt;
       uint32_t idx = base + li;
-      uint64_t x = ok ? v[idx] : 0;
+      uint64_t x = xs[q];
       uint64_t up = __shfl_up_sync(0xffffffffu, x, 1);
       uint64_t pv = lane ? up : carry;
       carry = __shfl_sync(0xffffffffu, x, 31);
@@ -818,6 +864,7 @@ __device__ uint32_t* rle_starts(EncSmem& S, const uint64_t* v, uint32_t n, uint3
       uint32_t m = __ballot_sync(0xffffffffu, tr);
       if (tr) st[1 + before + __popc(m & ((1u << lane) - 1u))] = idx;
       before += __popc(m);
+     }
     }
   }
   __syncthreads();
@@ -904,10 +951,19 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
   uint64_t d = cnt >= 2 ? sv[1] - sv[0] : 0;
   uint32_t alive = do_float ? 0x7Fu : 0u;
   uint64_t carry = 0;
-  for (uint32_t r = 0; r < 32; r++) {
+  for (uint32_t r0 = 0; r0 < 32; r0 += 8) {
+    uint64_t xs[8];  // eight independent loads in flight per lane
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      uint32_t jq = (r0 + q) * 32 + lane;
+      xs[q] = jq < cnt ? sv[jq] : 0ull;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+    uint32_t r = r0 + q;
     uint32_t j = r * 32 + lane;
     bool ok = j < cnt;
-    uint64_t x = ok ? sv[j] : 0;
+    uint64_t x = xs[q];
     uint64_t up = __shfl_up_sync(0xffffffffu, x, 1);
     uint64_t pv = lane ? up : carry;
     carry = __shfl_sync(0xffffffffu, x, 31);
@@ -966,7 +1022,8 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
         }
       }
     }
-    if (do_float && (r & 7) == 7) alive &= ~warp_or(fmfail);
+    }
+    if (do_float) alive &= ~warp_or(fmfail);
   }
   R.umin = warp_min(umn);
   R.umax = warp_max(umx);
@@ -1359,6 +1416,7 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
 // ---------------------------------------------------------------------------
 __device__ void emit_raw(const uint64_t* v, uint32_t n, int dtype, uint8_t* out) {
   uint32_t lb = lane_bytes(dtype);
+#pragma unroll 8
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
     uint64_t x = v[i];
     if (dtype == DT_F32) put_u32(out + 4ull * i, f64bits_to_f32bits(x));
