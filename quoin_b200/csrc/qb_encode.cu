@@ -19,6 +19,12 @@ constexpr uint32_t kHashCap = 2048;         // smem hash slots (dict / ALP-RD le
 constexpr uint32_t kHashLimit = 1536;       // distinct keys before falling back to scratch
 constexpr uint32_t kLbBits = 1u << 17;      // dict cardinality lower-bound bitset
 constexpr uint32_t kRunsSmem = 4096;
+constexpr uint32_t kNoLb = 0xFFFFFFFFu;
+
+// 17-bit bucket of the dictionary cardinality lower-bound bitset.
+__device__ __forceinline__ uint32_t dict_lb_bucket(uint64_t x) {
+  return (uint32_t)((x * 0xD6E8FEB86659FD93ull) >> (64 - 17));
+}
 constexpr uint64_t kEmpty64 = ~0ull;
 constexpr uint32_t kEmpty32 = 0xFFFFFFFFu;
 
@@ -653,14 +659,51 @@ __device__ inline uint32_t dict_rank(const EncSmem& S, const DictView& dv, uint6
   return lo;
 }
 
-__device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scratch) {
+// Insert x into the smem hash (no-op once the table has overflowed).
+__device__ __forceinline__ void dict_insert(DictArea& D, EncSmem& S, uint64_t x) {
+  if (*(volatile uint32_t*)&S.ovf) return;
+  if (x == kEmpty64) {
+    if (atomicExch(&S.has_max, 1u) == 0) atomicAdd(&S.card, 1u);
+    return;
+  }
+  uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 53);
+  for (uint32_t probe = 0; probe < kHashCap; probe++) {
+    uint64_t cur = D.hkey[h];
+    if (cur == kEmpty64) {
+      unsigned long long old = atomicCAS((unsigned long long*)&D.hkey[h], kEmpty64, x);
+      if (old == kEmpty64) {
+        if (atomicAdd(&S.card, 1u) >= kHashLimit) S.ovf = 1;
+        return;
+      }
+      cur = old;
+    }
+    if (cur == x) return;
+    h = (h + 1) & (kHashCap - 1);
+  }
+  S.ovf = 1;
+}
+
+// lb_pre: the block's 17-bit bucket count when the statistics pass computed it
+// (block == one adaptive window), else kNoLb.
+__device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scratch, uint32_t lb_pre) {
   DictArea& D = S.big.dict;
   uint32_t max_card = n / 2 + 1;
+  bool have_lb = lb_pre != kNoLb;
+  if (have_lb && lb_pre > max_card) {  // the lower bound alone proves the bail
+    if (threadIdx.x == 0) S.flag = 1;
+    __syncthreads();
+    DictView dv;
+    dv.smem = false;
+    dv.sorted = nullptr;
+    dv.card = lb_pre;
+    return dv;
+  }
   for (uint32_t i = threadIdx.x; i < kHashCap; i += blockDim.x) {
     D.hkey[i] = kEmpty64;
     D.hval[i] = 0;
   }
-  for (uint32_t i = threadIdx.x; i < kLbBits / 32; i += blockDim.x) D.lb[i] = 0;
+  if (!have_lb)
+    for (uint32_t i = threadIdx.x; i < kLbBits / 32; i += blockDim.x) D.lb[i] = 0;
   if (threadIdx.x == 0) {
     S.ovf = 0;
     S.card = 0;
@@ -669,42 +712,26 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
   }
   __syncthreads();
   for (uint32_t base = 0; base < n; base += blockDim.x * 8) {
-   uint64_t xs[8];
+    uint64_t xs[8];
 #pragma unroll
-   for (int q = 0; q < 8; q++) {
-     uint32_t iq = base + q * blockDim.x + threadIdx.x;
-     xs[q] = iq < n ? v[iq] : 0ull;
-   }
-#pragma unroll 1
-   for (int q = 0; q < 8; q++) {
-    uint32_t i = base + q * blockDim.x + threadIdx.x;
-    if (i >= n) break;
-    uint64_t x = xs[q];
-    uint32_t b = (uint32_t)((x * 0xD6E8FEB86659FD93ull) >> (64 - 17));
-    atomicOr(&D.lb[b >> 5], 1u << (b & 31));
-    if (*(volatile uint32_t*)&S.ovf) continue;
-    if (x == kEmpty64) {
-      if (atomicExch(&S.has_max, 1u) == 0) atomicAdd(&S.card, 1u);
-      continue;
+    for (int q = 0; q < 8; q++) {
+      uint32_t iq = base + q * blockDim.x + threadIdx.x;
+      xs[q] = iq < n ? v[iq] : 0ull;
     }
-    uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 53);
-    bool done = false;
-    for (uint32_t probe = 0; probe < kHashCap && !done; probe++) {
-      uint64_t cur = D.hkey[h];
-      if (cur == kEmpty64) {
-        unsigned long long old = atomicCAS((unsigned long long*)&D.hkey[h], kEmpty64, x);
-        if (old == kEmpty64) {
-          if (atomicAdd(&S.card, 1u) >= kHashLimit) S.ovf = 1;
-          done = true;
-          break;
+    if (!have_lb) {
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        if (base + q * blockDim.x + threadIdx.x < n) {
+          uint32_t b = dict_lb_bucket(xs[q]);
+          atomicOr(&D.lb[b >> 5], 1u << (b & 31));
         }
-        cur = old;
       }
-      if (cur == x) done = true;
-      else h = (h + 1) & (kHashCap - 1);
+    } else if (*(volatile uint32_t*)&S.ovf) {
+      break;
     }
-    if (!done) S.ovf = 1;
-   }
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+      if (base + q * blockDim.x + threadIdx.x < n) dict_insert(D, S, xs[q]);
   }
   __syncthreads();
   DictView dv;
@@ -739,17 +766,22 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
     return dv;
   }
   // Overflow: the lower-bound bitset may prove the bail outright.
-  uint32_t lbc = 0;
-  for (uint32_t i = threadIdx.x; i < kLbBits / 32; i += blockDim.x) lbc += __popc(D.lb[i]);
-  lbc = warp_sum(lbc);
-  if ((threadIdx.x & 31) == 0) S.red32[threadIdx.x >> 5] = lbc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t t = 0;
-    for (int w = 0; w < kEncWarps; w++) t += S.red32[w];
-    S.cnt32 = t;
+  if (have_lb) {
+    if (threadIdx.x == 0) S.cnt32 = lb_pre;
+    __syncthreads();
+  } else {
+    uint32_t lbc = 0;
+    for (uint32_t i = threadIdx.x; i < kLbBits / 32; i += blockDim.x) lbc += __popc(D.lb[i]);
+    lbc = warp_sum(lbc);
+    if ((threadIdx.x & 31) == 0) S.red32[threadIdx.x >> 5] = lbc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < kEncWarps; w++) t += S.red32[w];
+      S.cnt32 = t;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   if (S.cnt32 > max_card) {
     if (threadIdx.x == 0) S.flag = 1;
     __syncthreads();
@@ -907,6 +939,8 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
     SubStats* __restrict__ ss, FmStat* __restrict__ fms, uint64_t* __restrict__ smp16, uint8_t* __restrict__ grow,
     uint32_t* __restrict__ winbits) {
   __shared__ uint32_t bitsA[512], bitsB[512];
+  __shared__ uint32_t lbits[kLbBits / 32];  // dictionary cardinality lower bound (window)
+  __shared__ uint32_t s_lbc;
   __shared__ uint64_t s_first[kStatsWarps], s_last[kStatsWarps];
   __shared__ uint32_t s_neq[kStatsWarps], s_cnt[kStatsWarps];
   __shared__ uint64_t alp_smp[kStatsWarps][32];
@@ -934,6 +968,8 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
       bitsA[i] = 0;
       bitsB[i] = 0;
     }
+    for (int i = threadIdx.x; i < (int)(kLbBits / 32); i += blockDim.x) lbits[i] = 0;
+    if (threadIdx.x == 0) s_lbc = 0;
     __syncthreads();
   }
   SubStats R;
@@ -1002,6 +1038,8 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
           uint32_t bk = (uint32_t)(((x * 0x9E3779B97F4A7C15ull) >> 50) & 0x3FFF);
           atomicOr(&bitsB[bk >> 5], 1u << (bk & 31));
         }
+        uint32_t lb17 = dict_lb_bucket(x);
+        atomicOr(&lbits[lb17 >> 5], 1u << (lb17 & 31));
       }
       if (FLOATS && alive) {
         double xd = as_f64(x);
@@ -1080,6 +1118,14 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
   // values repeat.  consec_eq = len - transitions (the first element counts
   // against itself).
   __syncthreads();
+  {
+    uint32_t c = 0;
+    for (int i = threadIdx.x; i < (int)(kLbBits / 32); i += blockDim.x) c += __popc(lbits[i]);
+    c = warp_sum(c);
+    if (lane == 0 && c) atomicAdd(&s_lbc, c);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) winbits[(uint64_t)blockIdx.x * kWinWords + 1024] = s_lbc;
   if (warp == 0 && wlen) {
     uint32_t dc = 0;
     for (int i = lane; i < 512; i += 32) dc += __popc(bitsA[i]);
@@ -1095,8 +1141,8 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
       grow[blockIdx.x] = (dc < 2048 || (uint64_t)consec * 2 > wlen) ? 1 : 0;
     }
     for (int i = lane; i < 512; i += 32) {
-      winbits[(uint64_t)blockIdx.x * 1024 + i] = bitsA[i];
-      winbits[(uint64_t)blockIdx.x * 1024 + 512 + i] = bitsB[i];
+      winbits[(uint64_t)blockIdx.x * kWinWords + i] = bitsA[i];
+      winbits[(uint64_t)blockIdx.x * kWinWords + 512 + i] = bitsB[i];
     }
   }
 }
@@ -1217,11 +1263,11 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
     uint32_t distinct;
     uint64_t wi = fd.value_off / kBaseQuantum;
     if (!fixed_bs && dstride == 8 && n == (uint32_t)kBaseQuantum) {
-      distinct = popc_bits_block(S, winbits + wi * 1024);
+      distinct = popc_bits_block(S, winbits + wi * kWinWords);
     } else if (!fixed_bs && dstride == 32 && n == (uint32_t)kMaxBlock) {
       for (int i = t; i < 512; i += blockDim.x)
-        S.distinct_bits[i] = winbits[wi * 1024 + 512 + i] | winbits[(wi + 1) * 1024 + 512 + i] |
-                             winbits[(wi + 2) * 1024 + 512 + i] | winbits[(wi + 3) * 1024 + 512 + i];
+        S.distinct_bits[i] = winbits[wi * kWinWords + 512 + i] | winbits[(wi + 1) * kWinWords + 512 + i] |
+                             winbits[(wi + 2) * kWinWords + 512 + i] | winbits[(wi + 3) * kWinWords + 512 + i];
       __syncthreads();
       distinct = popc_bits_block(S, S.distinct_bits);
     } else {
@@ -1374,7 +1420,9 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
   if (block_compressible && !reduced) {
     // DICT (dict.rs:87-152, bit-packed codes).  The dictionary is sorted, so
     // a sub-block's code range is [rank(min), rank(max)].
-    DictView dv = dict_prepare(S, v, n, scr);
+    bool one_win = !fixed_bs && (fd.value_off % kBaseQuantum) == 0 && n <= (uint32_t)kBaseQuantum;
+    uint32_t lb_pre = one_win ? winbits[(fd.value_off / kBaseQuantum) * kWinWords + 1024] : kNoLb;
+    DictView dv = dict_prepare(S, v, n, scr, lb_pre);
     if (!S.flag) {
       uint32_t vtag;
       uint64_t vlen = dict_values_len(S, dv, &vtag);
@@ -1623,7 +1671,7 @@ __device__ void emit_alprd(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t l
 }
 
 __device__ void emit_dict(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scr, uint8_t* out) {
-  DictView dv = dict_prepare(S, v, n, scr);
+  DictView dv = dict_prepare(S, v, n, scr, kNoLb);
   uint32_t vtag;
   uint64_t vlen = dict_values_len(S, dv, &vtag);
   uint64_t pos = 0;

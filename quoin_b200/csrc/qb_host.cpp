@@ -355,7 +355,7 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
   bool fl = j.dtype == WT_F64 || j.dtype == WT_F32;
   CK(c->ensure(S_GROW, nwin + 16));
   CK(c->ensure(S_SUBST, (items + 1) * sub_stats_bytes()));
-  CK(c->ensure(S_WINBITS, (nwin + 1) * 1024 * 4));
+  CK(c->ensure(S_WINBITS, (nwin + 1) * kWinWords * 4));
   if (fl) {
     CK(c->ensure(S_FMST, (items + 1) * fm_stats_bytes()));
     CK(c->ensure(S_SMP16, (n / 16 + 2) * 8));

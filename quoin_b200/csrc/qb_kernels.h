@@ -28,7 +28,11 @@ constexpr uint64_t kEncScratchPerValue = 32;
 // window grow flags and probe bitsets).  Sizes: sub_stats_items(n, bs) records
 // of sub_stats_bytes(); FLOAT_MULT records of fm_stats_bytes() for float
 // columns; smp16 holds n/16 + 1 values (float columns); grow one byte per
-// 32768-value window and winbits 1024 words per window.
+// 32768-value window and winbits kWinWords words per window: the 14-bit probe
+// bucket bitsets at stride max(len/4096,1) ([0,512)) and stride 32
+// ([512,1024)), then word 1024 = the number of distinct 17-bit dictionary
+// hash buckets over the whole window (a lower bound of its cardinality).
+constexpr uint64_t kWinWords = 1028;
 uint64_t sub_stats_items(uint64_t n, uint64_t fixed_bs);
 uint64_t sub_stats_bytes();
 uint64_t fm_stats_bytes();
