@@ -73,6 +73,10 @@ __device__ inline uint32_t warp_or(uint32_t v) {
   for (int o = 16; o; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+__device__ inline uint64_t warp_or64(uint64_t v) {
+  for (int o = 16; o; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
 __device__ inline int64_t warp_min_i64(int64_t v) {
   for (int o = 16; o; o >>= 1) { int64_t u = __shfl_xor_sync(0xffffffffu, v, o); v = u < v ? u : v; }
   return v;
@@ -630,10 +634,86 @@ __device__ inline int rd_code(const EncSmem& S, uint64_t left) {
 // scratch hash + scratch bitonic sort + binary-search ranks.  Sets S.card and
 // S.flag (1 = dictionary bails: cardinality > n/2+1).
 // ---------------------------------------------------------------------------
+// Stable LSD radix sort (8-bit digits) of m u64 keys in a, using b as the
+// second buffer; digits on which every key agrees are skipped.  Returns the
+// buffer that holds the sorted keys.  All threads of a kEncThreads CTA; the
+// per-warp digit counters live in the dictionary smem area.
+__device__ uint64_t* block_radix_sort(EncSmem& S, uint64_t* a, uint64_t* b, uint32_t m) {
+  static_assert(kEncThreads == 256, "one thread per digit in the offset scan");
+  uint32_t* hist = reinterpret_cast<uint32_t*>(S.big.dict.sorted);  // [kEncWarps][256]
+  int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  uint64_t k0 = m ? a[0] : 0ull, diff = 0;
+  for (uint32_t i = t; i < m; i += blockDim.x) diff |= a[i] ^ k0;
+  diff = warp_or64(diff);
+  if (lane == 0) S.red[warp] = diff;
+  __syncthreads();
+  diff = 0;
+  for (int w = 0; w < kEncWarps; w++) diff |= S.red[w];
+  __syncthreads();
+  uint32_t seg = ((m + kEncWarps - 1) / kEncWarps + 31u) & ~31u;
+  uint32_t s0 = min(warp * seg, m), s1 = min(s0 + seg, m);
+  for (int shift = 0; shift < 64; shift += 8) {
+    if (((diff >> shift) & 0xFFull) == 0) continue;
+    for (int i = t; i < kEncWarps * 256; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (uint32_t i = s0 + lane; i < s1; i += 32) atomicAdd(&hist[warp * 256 + (uint32_t)((a[i] >> shift) & 0xFF)], 1u);
+    __syncthreads();
+    {  // offsets: digit-major, then warp order (stability)
+      uint32_t tot = 0;
+      for (int w = 0; w < kEncWarps; w++) tot += hist[w * 256 + t];
+      uint32_t inc = tot;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+      }
+      if (lane == 31) S.red32[warp] = inc;
+      __syncthreads();
+      uint32_t run = inc - tot;
+      for (int w = 0; w < warp; w++) run += S.red32[w];
+      for (int w = 0; w < kEncWarps; w++) {
+        uint32_t c = hist[w * 256 + t];
+        hist[w * 256 + t] = run;
+        run += c;
+      }
+    }
+    __syncthreads();
+    for (uint32_t base = s0; base < s1; base += 32 * 8) {
+      uint64_t ks[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        uint32_t i = base + q * 32 + lane;
+        ks[q] = i < s1 ? a[i] : 0ull;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        uint32_t i = base + q * 32 + lane;
+        uint32_t act = __ballot_sync(0xffffffffu, i < s1);
+        if (i < s1) {
+          uint32_t dg = (uint32_t)((ks[q] >> shift) & 0xFF);
+          uint32_t peers = __match_any_sync(act, dg);
+          uint32_t r = __popc(peers & ((1u << lane) - 1u));
+          b[hist[warp * 256 + dg] + r] = ks[q];
+          __syncwarp(act);
+          if (r == 0) hist[warp * 256 + dg] += __popc(peers);
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    uint64_t* tmp = a;
+    a = b;
+    b = tmp;
+  }
+  return a;
+}
+
 struct DictView {
   bool smem;
   const uint64_t* sorted;  // card values ascending
   uint32_t card;
+  const uint64_t* tkey = nullptr;  // scratch hash table (keys) and ranks, 2^lg slots
+  const uint32_t* trank = nullptr;
+  uint32_t lg = 0;
 };
 
 __device__ inline uint32_t dict_hash_slot(const uint64_t* hk, uint64_t x) {
@@ -651,12 +731,11 @@ __device__ inline uint32_t dict_rank(const EncSmem& S, const DictView& dv, uint6
     if (x == kEmpty64) return S.max_rank;
     return S.big.dict.hval[dict_hash_slot(S.big.dict.hkey, x)];
   }
-  uint32_t lo = 0, hi = dv.card;  // first index with sorted[i] >= x
-  while (lo < hi) {
-    uint32_t mid = (lo + hi) >> 1;
-    if (dv.sorted[mid] < x) lo = mid + 1; else hi = mid;
-  }
-  return lo;
+  if (x == kEmpty64) return S.max_rank;
+  uint32_t cap = 1u << dv.lg;
+  uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> (64 - dv.lg));
+  for (uint32_t probe = 0; probe < cap && dv.tkey[h] != x; probe++) h = (h + 1) & (cap - 1);
+  return dv.trank[h];
 }
 
 // Insert x into the smem hash (no-op once the table has overflowed).
@@ -790,50 +869,81 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
     dv.card = S.cnt32;
     return dv;
   }
-  // Scratch path: u32 table of (first index + 1), capacity >= 2n; then sort.
-  uint32_t cap = pow2_at_least(2 * n), lg = 31 - __clz(cap);
-  uint32_t* T = reinterpret_cast<uint32_t*>(scratch);
-  uint64_t* srt = reinterpret_cast<uint64_t*>(scratch + 4ull * cap);
-  for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) T[i] = 0;
+  // Scratch path (more than kHashLimit distinct values): a u64 key hash table
+  // T[cap] in scratch (cap = pow2 >= n, so the table stays at most about half
+  // full for a dictionary that does not bail), the distinct keys compacted and
+  // radix-sorted, and a rank table R[cap] beside T for the code lookups.
+  // Scratch use: 12*cap + 16*max_card bytes <= 32*n.
+  uint32_t cap = pow2_at_least(n), lg = 31 - __clz(cap);
+  uint64_t* T = reinterpret_cast<uint64_t*>(scratch);
+  uint32_t* R = reinterpret_cast<uint32_t*>(scratch + 8ull * cap);
+  uint64_t* A = reinterpret_cast<uint64_t*>(scratch + 12ull * cap);
+  uint64_t* B = A + max_card;
+  for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) T[i] = kEmpty64;
   if (threadIdx.x == 0) {
     S.card = 0;
     S.cnt32 = 0;
+    S.has_max = 0;
+    S.flag = 0;
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    uint64_t x = v[i];
-    uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> (64 - lg));
-    for (uint32_t probe = 0; probe < cap; probe++) {
-      uint32_t cur = T[h];
-      if (cur == 0) {
-        uint32_t old = atomicCAS(&T[h], 0u, i + 1);
-        if (old == 0) {
-          atomicAdd(&S.card, 1u);
-          break;
-        }
-        cur = old;
+  for (uint32_t base = 0; base < n; base += blockDim.x * 8) {
+    if (*(volatile uint32_t*)&S.flag) break;
+    uint64_t xs[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      uint32_t iq = base + q * blockDim.x + threadIdx.x;
+      xs[q] = iq < n ? v[iq] : 0ull;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      if (base + q * blockDim.x + threadIdx.x >= n) break;
+      uint64_t x = xs[q];
+      if (x == kEmpty64) {
+        if (atomicExch(&S.has_max, 1u) == 0 && atomicAdd(&S.card, 1u) >= max_card) S.flag = 1;
+        continue;
       }
-      if (v[cur - 1] == x) break;
-      h = (h + 1) & (cap - 1);
+      uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> (64 - lg));
+      for (uint32_t probe = 0; probe < cap; probe++) {
+        uint64_t cur = T[h];
+        if (cur == kEmpty64) {
+          cur = atomicCAS((unsigned long long*)&T[h], kEmpty64, x);
+          if (cur == kEmpty64) {
+            if (atomicAdd(&S.card, 1u) >= max_card) S.flag = 1;
+            break;
+          }
+        }
+        if (cur == x) break;
+        h = (h + 1) & (cap - 1);
+      }
     }
   }
   __syncthreads();
-  uint32_t card = S.card;
   dv.smem = false;
-  dv.card = card;
-  if (card > max_card) {
-    if (threadIdx.x == 0) S.flag = 1;
-    __syncthreads();
+  dv.tkey = T;
+  dv.trank = R;
+  dv.lg = lg;
+  if (S.flag) {  // cardinality > n/2 + 1
+    dv.card = S.card;
     dv.sorted = nullptr;
     return dv;
   }
-  uint32_t P = pow2_at_least(max(card, 1u));
-  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) srt[i] = kEmpty64;
-  __syncthreads();
+  uint32_t card = S.card, has_max = S.has_max;
   for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x)
-    if (T[i]) srt[atomicAdd(&S.cnt32, 1u)] = v[T[i] - 1];
+    if (T[i] != kEmpty64) A[atomicAdd(&S.cnt32, 1u)] = T[i];
   __syncthreads();
-  block_bitonic_sort(srt, P);
+  uint64_t* srt = block_radix_sort(S, A, B, card - has_max);
+  if (has_max && threadIdx.x == 0) srt[card - 1] = kEmpty64;
+  if (threadIdx.x == 0) S.max_rank = card - 1;
+  __syncthreads();
+  for (uint32_t r = threadIdx.x; r + has_max < card; r += blockDim.x) {
+    uint64_t x = srt[r];
+    uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> (64 - lg));
+    for (uint32_t probe = 0; probe < cap && T[h] != x; probe++) h = (h + 1) & (cap - 1);
+    R[h] = r;
+  }
+  __syncthreads();
+  dv.card = card;
   dv.sorted = srt;
   return dv;
 }

@@ -100,6 +100,22 @@ def shape_cases():
         ("lead_trail_nulls", np.arange(3000, dtype=np.int64), I64,
          bitmap_from_bools([100 <= i < 2900 for i in range(3000)])),
     ]
+    # Dictionaries beyond the shared-memory hash (more than 1536 distinct
+    # values): the scratch hash, radix sort and rank table.
+    pool = lcg_seq(31, 3000) >> np.uint64(8)  # 56-bit: FoR compresses a little, so DICT is tried
+    c.append(("dict_scratch_wide_u64", pool[(lcg1_seq(32, 40000) >> np.uint64(40)) % 1800], U64, None))
+    pool_max = pool.copy()
+    pool_max[17] = np.uint64(2**64 - 1)
+    c.append(("dict_scratch_with_max", pool_max[(lcg1_seq(33, 70000) >> np.uint64(40)) % 1800], U64, None))
+    c.append(("dict_scratch_i32", (pool[(lcg1_seq(34, 50000) >> np.uint64(40)) % 2500] >> np.uint64(32))
+              .astype(np.uint32).view(np.int32), I32, None))
+    c.append(("dict_scratch_big", (lcg_seq(35, 17000) >> np.uint64(8))[(lcg1_seq(36, 32768) >> np.uint64(40)) % 17000],
+              U64, None))
+    p17 = lcg_seq(38, 17500) >> np.uint64(8)  # 17500 distinct > 32768/2+1, bucket lower bound below it
+    c.append(("dict_scratch_bail", np.concatenate([p17, p17[:32768 - 17500]])[np.argsort(lcg_seq(39, 32768))],
+              U64, None))
+    c.append(("dict_scratch_grown", np.repeat(pool[(lcg1_seq(37, 60000) >> np.uint64(40)) % 2800], 3)[:170000],
+              U64, None))
     vb = rng.random(300000) > 0.1
     c.append(("nullable_ts_300k", (np.cumsum(1_000_000 + rng.poisson(5000, 300000)) + 1_700_000_000_000_000_000)
               .astype(np.int64), I64, bitmap_from_bools(vb)))
