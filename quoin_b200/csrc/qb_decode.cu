@@ -617,7 +617,9 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
       const uint8_t* vb = p + A.c;
       const uint64_t* dict = nullptr;
       if (A.b == 1) {  // delta-coded sorted dictionary -> smem or scratch
-        uint64_t* dd = card <= kDictSmem ? S.u.d.dict : scratch;
+        // scratch holds one u64 per lane value; a frame's dictionary (card <= n)
+        // uses the frame's own range
+        uint64_t* dd = card <= kDictSmem ? S.u.d.dict : (scratch ? scratch + d.value_off : nullptr);
         if (!dd) {
           e = E_UNSUPPORTED;
           break;

@@ -285,23 +285,13 @@ __device__ inline void warp_for_pack(uint8_t* dst, uint32_t cnt, uint64_t mn, ui
   }
 }
 
-// Whole-CTA FoR stream writer: varint(M) + sub-blocks of val(0..M).  When
-// dst is null only the size is computed.  Returns the byte length (all threads).
+// Second half of the FoR stream writer: with S.w_a[k] / S.submin[k] set for
+// every sub-block, lays out varint(M) + sub-blocks and (dst non-null) packs
+// val(0..M).  Returns the byte length (all threads).
 template <class V>
-__device__ uint64_t block_for(EncSmem& S, uint8_t* dst, uint32_t M, bool sgn, V val) {
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+__device__ uint64_t block_for_write(EncSmem& S, uint8_t* dst, uint32_t M, V val) {
+  int warp = threadIdx.x >> 5;
   uint32_t nsub = (M + kSub - 1) / kSub;
-  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
-    uint32_t cnt = min((uint32_t)kSub, M - k * kSub);
-    uint64_t mn;
-    uint32_t w;
-    warp_minmax(cnt, sgn, [&](uint32_t i) { return val(k * kSub + i); }, &mn, &w);
-    if (lane == 0) {
-      S.w_a[k] = (uint8_t)w;
-      S.submin[k] = mn;
-    }
-  }
-  __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t off = varint_len(M);
     for (uint32_t k = 0; k < nsub; k++) {
@@ -321,6 +311,26 @@ __device__ uint64_t block_for(EncSmem& S, uint8_t* dst, uint32_t M, bool sgn, V 
   }
   __syncthreads();
   return total;
+}
+
+// Whole-CTA FoR stream writer: varint(M) + sub-blocks of val(0..M).  When
+// dst is null only the size is computed.  Returns the byte length (all threads).
+template <class V>
+__device__ uint64_t block_for(EncSmem& S, uint8_t* dst, uint32_t M, bool sgn, V val) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nsub = (M + kSub - 1) / kSub;
+  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+    uint32_t cnt = min((uint32_t)kSub, M - k * kSub);
+    uint64_t mn;
+    uint32_t w;
+    warp_minmax(cnt, sgn, [&](uint32_t i) { return val(k * kSub + i); }, &mn, &w);
+    if (lane == 0) {
+      S.w_a[k] = (uint8_t)w;
+      S.submin[k] = mn;
+    }
+  }
+  __syncthreads();
+  return block_for_write(S, dst, M, val);
 }
 
 // ALP for one sub-block (reference alp.rs:49-166): find_ef on the 32-value
@@ -1073,6 +1083,8 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
   uint64_t wstart = (uint64_t)blockIdx.x * kBaseQuantum;
   uint32_t wlen = fixed_bs ? 0u : (uint32_t)(wstart < n ? qmin(kBaseQuantum, n - wstart) : 0);
   uint32_t wstride = max(wlen / 4096u, 1u);
+  const bool wpow2 = (wstride & (wstride - 1u)) == 0;  // full windows: stride 8
+  const bool sgn = dtype_signed(dtype);
   if (!fixed_bs) {
     for (int i = threadIdx.x; i < 512; i += blockDim.x) {
       bitsA[i] = 0;
@@ -1116,9 +1128,11 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
     if (ok) {
       umn = u64min(umn, x);
       umx = u64max(umx, x);
-      int64_t sx = (int64_t)x;
-      smn = sx < smn ? sx : smn;
-      smx = sx > smx ? sx : smx;
+      if (sgn) {
+        int64_t sx = (int64_t)x;
+        smn = sx < smn ? sx : smn;
+        smx = sx > smx ? sx : smx;
+      }
       if (j > 0) {
         uint64_t dz = zigzag64(x - pv);
         dzmn = u64min(dzmn, dz);
@@ -1140,7 +1154,7 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
       }
       if (!fixed_bs) {
         uint32_t wj = (uint32_t)(s - wstart) + j;
-        if (wj % wstride == 0) {
+        if (wpow2 ? (wj & (wstride - 1u)) == 0 : wj % wstride == 0) {
           uint32_t bk = (uint32_t)(((x * 0x9E3779B97F4A7C15ull) >> 50) & 0x3FFF);
           atomicOr(&bitsA[bk >> 5], 1u << (bk & 31));
         }
@@ -1148,8 +1162,10 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
           uint32_t bk = (uint32_t)(((x * 0x9E3779B97F4A7C15ull) >> 50) & 0x3FFF);
           atomicOr(&bitsB[bk >> 5], 1u << (bk & 31));
         }
-        uint32_t lb17 = dict_lb_bucket(x);
-        atomicOr(&lbits[lb17 >> 5], 1u << (lb17 & 31));
+        if (j == 0 || x != pv) {  // a repeat's bucket is already set
+          uint32_t lb17 = dict_lb_bucket(x);
+          atomicOr(&lbits[lb17 >> 5], 1u << (lb17 & 31));
+        }
       }
       if (FLOATS && alive) {
         double xd = as_f64(x);
@@ -1583,20 +1599,10 @@ __device__ void emit_raw(const uint64_t* v, uint32_t n, int dtype, uint8_t* out)
   }
 }
 
+// S.subsz[k] holds each sub-block's LEB128 byte count on entry.
 __device__ void emit_xorz(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* out) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t nsub = (n + kSub - 1) / kSub;
-  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
-    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
-    uint32_t tot = 0;
-    for (uint32_t i = lane; i < cnt; i += 32) {
-      uint32_t idx = base + i;
-      tot += varint_len(v[idx] ^ (idx ? v[idx - 1] : 0ull));
-    }
-    tot = warp_sum(tot);
-    if (lane == 0) S.subsz[k] = tot;
-  }
-  __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
     for (uint32_t k = 0; k < nsub; k++) {
@@ -1609,15 +1615,26 @@ __device__ void emit_xorz(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* ou
   for (uint32_t k = warp; k < nsub; k += kEncWarps) {
     uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
     uint32_t off = S.subsz[k];
-    for (uint32_t j = 0; j < 32; j++) {
-      uint32_t li = j * 32 + lane;
-      bool ok = li < cnt;
-      uint32_t idx = base + li;
-      uint64_t x = ok ? v[idx] ^ (idx ? v[idx - 1] : 0ull) : 0ull;
-      uint32_t sz = ok ? varint_len(x) : 0u;
-      uint32_t inc = warp_incl_scan(sz);
-      if (ok) put_varint(out + off + inc - sz, x);
-      off += __shfl_sync(0xffffffffu, inc, 31);
+    uint64_t carry = base ? v[base - 1] : 0ull;
+    for (uint32_t j0 = 0; j0 < 32; j0 += 8) {
+      uint64_t xs[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        uint32_t li = (j0 + q) * 32 + lane;
+        xs[q] = li < cnt ? v[base + li] : 0ull;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        uint32_t li = (j0 + q) * 32 + lane;
+        bool ok = li < cnt;
+        uint64_t up = __shfl_up_sync(0xffffffffu, xs[q], 1);
+        uint64_t x = ok ? xs[q] ^ (lane ? up : carry) : 0ull;
+        carry = __shfl_sync(0xffffffffu, xs[q], 31);
+        uint32_t sz = ok ? varint_len(x) : 0u;
+        uint32_t inc = warp_incl_scan(sz);
+        if (ok) put_varint(out + off + inc - sz, x);
+        off += __shfl_sync(0xffffffffu, inc, 31);
+      }
     }
   }
 }
@@ -1838,7 +1855,9 @@ __device__ void emit_rle(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scr
 
 __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict__ lane,
                                                       const FrameDesc* __restrict__ frames,
-                                                      const uint32_t* __restrict__ nbp, int dtype,
+                                                      const uint32_t* __restrict__ nbp, uint64_t fixed_bs, int dtype,
+                                                      const SubStats* __restrict__ ss,
+                                                      const FmStat* __restrict__ fms,
                                                       uint8_t* __restrict__ scratch, uint8_t* __restrict__ outbuf) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   EncSmem& S = *reinterpret_cast<EncSmem*>(smem_raw);
@@ -1856,6 +1875,37 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
     put_u32(hdr + 5, fd.plen);
   }
   bool sgn = dtype_signed(dtype);
+  // FoR / DELTA / FLOAT_MULT / XORZ sub-block layouts come from the statistics
+  // pass (the same numbers the competition sized the frame with).
+  uint32_t nsub = (n + kSub - 1) / kSub;
+  uint64_t g0 = fixed_bs ? (uint64_t)b * ((fixed_bs + kSub - 1) / kSub) : fd.value_off / kSub;
+  int m = (int)fd.mode;
+  if (m == M_FOR_BITPACK || m == M_DELTA_BITPACK || m == M_FLOAT_MULT || m == M_XORZ) {
+    for (uint32_t k = threadIdx.x; k < nsub; k += blockDim.x) {
+      const SubStats& R = ss[g0 + k];
+      uint64_t pl = k ? ss[g0 + k - 1].last : 0;
+      uint32_t w = 0;
+      uint64_t mn = 0;
+      if (m == M_FOR_BITPACK) {
+        w = sgn ? bit_width64((uint64_t)R.smax - (uint64_t)R.smin) : bit_width64(R.umax - R.umin);
+        mn = sgn ? (uint64_t)R.smin : R.umin;
+      } else if (m == M_DELTA_BITPACK) {
+        uint64_t dzf = k ? zigzag64(R.first - pl) : 0;
+        uint64_t dmn = R.cnt > 1 ? u64min(R.dzmin, dzf) : dzf, dmx = R.cnt > 1 ? u64max(R.dzmax, dzf) : dzf;
+        w = bit_width64(dmx - dmn);
+        mn = dmn;
+      } else if (m == M_FLOAT_MULT) {
+        const FmStat& F = fms[g0 + k];
+        w = bit_width64((uint64_t)F.kmax[fd.aux] - (uint64_t)F.kmin[fd.aux]);
+        mn = (uint64_t)F.kmin[fd.aux];
+      } else {
+        S.subsz[k] = R.xb + varint_len(R.first ^ pl);
+      }
+      S.w_a[k] = (uint8_t)w;
+      S.submin[k] = mn;
+    }
+    __syncthreads();
+  }
   switch (fd.mode) {
     case M_RAW: emit_raw(v, n, dtype, out); break;
     case M_CONST:
@@ -1868,10 +1918,10 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
       }
       break;
     case M_XORZ: emit_xorz(S, v, n, out); break;
-    case M_FOR_BITPACK: block_for(S, out, n, sgn, [&](uint32_t i) { return v[i]; }); break;
+    case M_FOR_BITPACK: block_for_write(S, out, n, [&](uint32_t i) { return v[i]; }); break;
     case M_DELTA_BITPACK:
       if (threadIdx.x == 0) put_u64(out, v[0]);
-      block_for(S, out + 8, n, false, [&](uint32_t i) { return zigzag64(v[i] - (i ? v[i - 1] : v[0])); });
+      block_for_write(S, out + 8, n, [&](uint32_t i) { return zigzag64(v[i] - (i ? v[i - 1] : v[0])); });
       break;
     case M_FLOAT_MULT: {
       int s = (int)fd.aux;
@@ -1879,7 +1929,7 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
         put_u8(out, 0);
         put_u8(out + 1, s);
       }
-      block_for(S, out + 2, n, true, [&](uint32_t i) { return (uint64_t)fm_k(v[i], s); });
+      block_for_write(S, out + 2, n, [&](uint32_t i) { return (uint64_t)fm_k(v[i], s); });
       break;
     }
     case M_ALP: emit_alp(S, v, n, out); break;
@@ -2008,9 +2058,12 @@ void launch_decide(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, 
   count_launches(max_blocks ? 1 : 0);
 }
 
-void launch_emit(const uint64_t* lane, const FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, int dtype,
-                 uint8_t* scratch, uint8_t* out, cudaStream_t st) {
-  if (max_blocks) k_emit<<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, dtype, scratch, out);
+void launch_emit(const uint64_t* lane, const FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks,
+                 uint64_t fixed_bs, int dtype, const void* ss, const void* fms, uint8_t* scratch, uint8_t* out,
+                 cudaStream_t st) {
+  if (max_blocks)
+    k_emit<<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, fixed_bs, dtype, (const SubStats*)ss,
+                                                              (const FmStat*)fms, scratch, out);
   count_launches(max_blocks ? 1 : 0);
 }
 

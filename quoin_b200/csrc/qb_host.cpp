@@ -387,7 +387,8 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
   if (total > dst_cap) return QUOIN_ERR_BUFFER_TOO_SMALL;
   {
     TimedRegion tr(T_EMIT, st);
-    launch_emit(j.lane, fr, nb, (uint32_t)maxb, j.dtype, c->p<uint8_t>(S_SCRATCH), d_dst, st);
+    launch_emit(j.lane, fr, nb, (uint32_t)maxb, bs, j.dtype, c->p<void>(S_SUBST), fl ? c->p<void>(S_FMST) : nullptr,
+                c->p<uint8_t>(S_SCRATCH), d_dst, st);
   }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));
