@@ -54,6 +54,7 @@ extern "C" {
 #define QUOIN_ERR_UNSUPPORTED         (-18) /* mode / entropy tag / level outside the pool */
 #define QUOIN_ERR_CUDA                (-19) /* a CUDA call failed (no device, OOM, ...)   */
 #define QUOIN_ERR_BAD_ARG             (-20)
+#define QUOIN_ERR_NOALLOC_LIMIT       (-21) /* stream outside quoin_b200_decompress_device_noalloc's limits */
 
 /* ---------------- reference ABI (capi/include/quoin.h:35-142) ---------------- */
 
@@ -201,6 +202,24 @@ int quoin_b200_index_info(const QuoinDecodeIndex *idx, int32_t *wire_dtype, uint
 int quoin_b200_decompress_indexed_device(QuoinCtx *ctx, const QuoinDecodeIndex *idx,
                                          const uint8_t *d_src, void *d_values_out,
                                          uint8_t *d_validity_out, void *stream);
+
+/* No counterpart in the reference.  Allocation-free device decode for callers
+ * that cannot let the library allocate device memory (an engine that owns all
+ * device memory through its own pool, or a process that must keep a fixed
+ * footprint): decodes the device-resident stream d_src[0 .. src_len) into
+ * d_values_out (8-byte aligned, room for out_cap_values values) using only a
+ * fixed scratch arena compiled into the library (about 2.5 MB per device), and
+ * writes the value count to *n_out.  Limits: at most 262,144 values and 256
+ * frames, dtype f64/i64/u64, no validity bitmap; other streams are rejected
+ * with QUOIN_ERR_NOALLOC_LIMIT (QUOIN_ERR_BUFFER_TOO_SMALL when n exceeds
+ * out_cap_values).  The caller zeroes nothing: each call resets the arena.
+ * Calls on one device share the arena, so calls that overlap in time race and
+ * must be serialised by the caller.  The first call on each device looks the
+ * arena up (and may load the module); make it before any stream capture.
+ * `stream` is a cudaStream_t (NULL = the default stream); the call returns
+ * after the work on it has completed. */
+int quoin_b200_decompress_device_noalloc(const uint8_t *d_src, size_t src_len, void *d_values_out,
+                                         size_t out_cap_values, uint64_t *n_out, void *stream);
 
 /* Per-mode win counts of the GPU competition since the last reset, indexed by
  * mode id (src/lib.rs:540-547, src/diag.rs). */

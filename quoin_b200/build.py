@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libquoin_b200.so")
 
-SOURCES = ["qb_decode.cu", "qb_encode.cu", "qb_lower.cu", "qb_host.cpp"]
+SOURCES = ["qb_decode.cu", "qb_encode.cu", "qb_lower.cu", "qb_noalloc.cu", "qb_host.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
