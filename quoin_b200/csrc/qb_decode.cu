@@ -21,6 +21,7 @@ constexpr int kDecWarps = kDecThreads / 32;
 constexpr int kMaxSubs = kMaxBlock / kSub;  // 128
 constexpr int kDictSmem = 2048;
 constexpr int kXorzChunk = kDecThreads * 8;  // payload bytes per XORZ step
+constexpr int kXorzRing = 4096;              // decoded XORZ values awaiting their store
 
 // Per-frame results of the walk (device memory, one per frame).
 struct FrameAux {
@@ -312,9 +313,99 @@ struct DecSmem {
       uint64_t dict[kDictSmem];      // dictionary values (16 KB)
       uint64_t stage[4][kSub];       // staging for the dictionary prefix pass
     } d;
-    uint64_t xbuf[kXorzChunk];       // XORZ chunk values (16 KB)
+    struct {
+      uint64_t xbuf[kXorzChunk];     // XORZ chunk values (16 KB)
+      uint64_t ring[kXorzRing];      // decoded values not yet stored (32 KB)
+    } x;
   } u;
 };
+
+// ---------------------------------------------------------------------------
+// Output stores.  Every decoded run of values [c0, c0 + cnt) (c0 = lane index
+// of the first value) is written straight to its final place: the lane (u64),
+// or the typed column, narrowed to the native width and scattered through the
+// validity bitmap with nulls as 0 (reference lib.rs:492-506, validity.rs:130-146).
+// With a bitmap, c0 is a multiple of 1024 and c0 + cnt is too, or the end of
+// the lane; the run then owns the positions [sel(c0), sel(c0 + cnt)), where
+// sel(c) is the position of the c-th valid value (0 for c = 0, n at the end),
+// so the nulls between runs are written exactly once.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void put_out(const DecodeOut& O, uint64_t pos, uint64_t v) {
+  if (O.dtype == DT_I32 || O.dtype == DT_U32) {
+    reinterpret_cast<uint32_t*>(O.out)[pos] = (uint32_t)v;
+  } else if (O.dtype == DT_F32) {
+    reinterpret_cast<uint32_t*>(O.out)[pos] = v ? f64bits_to_f32bits(v) : 0u;
+  } else {
+    reinterpret_cast<uint64_t*>(O.out)[pos] = v;
+  }
+}
+
+__device__ __forceinline__ void run_positions(const DecodeOut& O, uint64_t c0, uint64_t c1, uint64_t* p0,
+                                              uint64_t* p1) {
+  *p0 = c0 == 0 ? 0 : O.sel[c0 >> 10];
+  *p1 = c1 >= O.nvalid ? O.n : O.sel[c1 >> 10];
+}
+
+// Positions [32*w0, 32*w1) of the run [p0, p1) by one warp, relative ranks
+// counted from `rel` (the number of the run's values before position 32*w0).
+// The bitmap words are fetched 32 at a time, one per lane, and broadcast.
+template <class V>
+__device__ __forceinline__ void warp_store_words(const DecodeOut& O, uint64_t w0, uint64_t w1, uint64_t p0,
+                                                 uint64_t p1, uint32_t rel, V& val) {
+  int l = threadIdx.x & 31;
+  uint32_t below = (1u << l) - 1u;
+  for (uint64_t wb = w0; wb < w1; wb += 32) {
+    uint32_t mine = wb + l < w1 ? O.bm32[wb + l] : 0u;
+    uint32_t nw = (uint32_t)qmin(32, w1 - wb);
+    for (uint32_t j = 0; j < nw; j++) {
+      uint32_t bits = __shfl_sync(0xffffffffu, mine, j);
+      uint64_t base = (wb + j) << 5;
+      uint32_t in = 0xFFFFFFFFu;  // positions of this word inside [p0, p1)
+      if (base < p0) in &= 0xFFFFFFFFu << (uint32_t)(p0 - base);
+      if (base + 32 > p1) in &= 0xFFFFFFFFu >> (uint32_t)(base + 32 - p1);
+      bits &= in;
+      if ((in >> l) & 1u) {
+        uint64_t v = 0;
+        if ((bits >> l) & 1u) v = val(rel + __popc(bits & below));
+        put_out(O, base + l, v);
+      }
+      rel += __popc(bits);
+    }
+  }
+}
+
+// One warp stores one run; val(q) is called with increasing q per lane.
+template <class V>
+__device__ void warp_store(const DecodeOut& O, uint64_t c0, uint32_t cnt, V val) {
+  int l = threadIdx.x & 31;
+  if (!O.bm32) {
+    for (uint32_t q = l; q < cnt; q += 32) put_out(O, c0 + q, val(q));
+    return;
+  }
+  uint64_t p0, p1;
+  run_positions(O, c0, c0 + cnt, &p0, &p1);
+  if (p1 > p0) warp_store_words(O, p0 >> 5, (p1 + 31) >> 5, p0, p1, 0u, val);
+}
+
+// All warps of the CTA store one run: warp w takes the w-th contiguous slice of
+// the run's bitmap words and starts from the word's global rank.
+template <class V>
+__device__ void cta_store(const DecodeOut& O, uint64_t c0, uint32_t cnt, V val) {
+  int warp = threadIdx.x >> 5;
+  if (!O.bm32) {
+    for (uint32_t q = threadIdx.x; q < cnt; q += kDecThreads) put_out(O, c0 + q, val(q));
+    return;
+  }
+  uint64_t p0, p1;
+  run_positions(O, c0, c0 + cnt, &p0, &p1);
+  if (p1 <= p0) return;
+  uint64_t wb = p0 >> 5, we = (p1 + 31) >> 5;
+  uint64_t per = (we - wb + kDecWarps - 1) / kDecWarps;
+  uint64_t w0 = wb + (uint64_t)warp * per, w1 = qmin(w0 + per, we);
+  if (w0 >= w1) return;
+  uint32_t rel = w0 == wb ? 0u : (uint32_t)(O.wrank[w0] - c0);
+  warp_store_words(O, w0, w1, p0, p1, rel, val);
+}
 
 // Sum of one sub-block's values after a per-value map g (warp-uniform result).
 template <class G>
@@ -326,11 +417,12 @@ __device__ inline uint64_t warp_sub_sum(const uint8_t* p, uint32_t off, uint32_t
 
 // Two-phase prefix-sum decode of a FoR chain whose values are summed in index
 // order (DeltaBitpack deltas, dictionary deltas): per-sub-block sums, a carry
-// scan, then each warp stages its sub-block in smem and writes running values.
-// `nstage` warps take part in the second phase (one staging buffer each).
-template <class G, class W>
+// scan, then each warp stages its sub-block in smem, turns it into running
+// values in place and hands it to done(k, buf, cnt).  `nstage` warps take part
+// in the second phase (one staging buffer each).
+template <class G, class D>
 __device__ void chain_prefix(DecSmem& S, const uint8_t* p, const uint32_t* offs, uint64_t n, uint64_t base_carry,
-                             uint64_t* stage, int nstage, G g, W out) {
+                             uint64_t* stage, int nstage, G g, D done) {
   int l = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
   for (uint32_t k = warp; k < nsub; k += kDecWarps) {
@@ -353,7 +445,9 @@ __device__ void chain_prefix(DecSmem& S, const uint8_t* p, const uint32_t* offs,
       uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
       warp_unpack(p, offs[k], cnt, [&](uint32_t i, uint64_t v) { buf[i] = g(v); });
       __syncwarp();
-      warp_prefix_smem(buf, cnt, S.subcarry[k], [&](uint32_t i, uint64_t v) { out((uint64_t)k * kSub + i, v); });
+      warp_prefix_smem(buf, cnt, S.subcarry[k], [&](uint32_t i, uint64_t v) { buf[i] = v; });
+      __syncwarp();
+      done(k, buf, cnt);
       __syncwarp();
     }
   }
@@ -363,11 +457,15 @@ __device__ void chain_prefix(DecSmem& S, const uint8_t* p, const uint32_t* offs,
 // XORZ (reference codecs/xorz.rs:18-32): LEB128 of v_i ^ v_{i-1}.  Byte-parallel:
 // terminator bytes (bit 7 clear) end values; block scans number them and find
 // each value's first byte, the terminator's thread assembles the value, and a
-// block XOR-scan rebuilds v.  Error kinds follow the sequential reader.
-__device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, uint64_t* dst) {
+// block XOR-scan rebuilds v.  Values collect in a ring and leave it in runs of
+// 1024 (the last run shorter).  Error kinds follow the sequential reader.
+__device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, const DecodeOut& O,
+                             uint64_t c0) {
   int t = threadIdx.x, l = t & 31, warp = t >> 5;
   if (n == 0) return plen ? E_CORRUPT : E_OK;
+  uint64_t* ring = S.u.x.ring;
   uint64_t vbase = 0;         // values completed before this chunk
+  uint64_t flushed = 0;       // values already stored
   uint64_t xcarry = 0;        // XOR of all values so far
   int64_t last_term = -1;     // position of the last terminator before the chunk
   bool saw_nth = false;
@@ -380,6 +478,7 @@ __device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64
   for (uint64_t base = 0; base < plen && vbase < n; base += kXorzChunk) {
     uint64_t b0 = base + (uint64_t)t * 8;
     uint32_t tm = 0;  // terminator mask of this thread's 8 bytes
+#pragma unroll
     for (int j = 0; j < 8; j++)
       if (b0 + j < plen && !(p[b0 + j] & 0x80)) tm |= 1u << j;
     uint32_t cnt = __popc(tm);
@@ -427,7 +526,7 @@ __device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64
         } else {
           uint64_t x = 0;
           for (uint64_t q = 0; q < len; q++) x |= (uint64_t)(p[start + q] & 0x7f) << (7 * q);
-          S.u.xbuf[k] = x;
+          S.u.x.xbuf[k] = x;
         }
         if (vi == n - 1) {
           saw_nth = true;
@@ -442,7 +541,7 @@ __device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64
     uint32_t i0 = (uint32_t)t * 8;
     uint64_t vals[8], xs = 0;
     for (int j = 0; j < 8; j++) {
-      vals[j] = (i0 + j < cv) ? S.u.xbuf[i0 + j] : 0ull;
+      vals[j] = (i0 + j < cv) ? S.u.x.xbuf[i0 + j] : 0ull;
       xs ^= vals[j];
     }
     uint64_t xi = xs;
@@ -460,12 +559,25 @@ __device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64
     uint64_t run = xcarry ^ wx ^ xi ^ xs;
     for (int j = 0; j < 8; j++) {
       run ^= vals[j];
-      if (i0 + j < cv) dst[vbase + i0 + j] = run;
+      if (i0 + j < cv) ring[(vbase + i0 + j) & (kXorzRing - 1)] = run;
     }
     xcarry ^= tx;
     vbase += total;
     last_term = chunk_last;
     __syncthreads();
+    uint64_t have = qmin(vbase, n);
+    bool stored = false;
+    while (flushed + kSub <= have) {  // at most 3071 values wait in the ring
+      uint64_t f0 = flushed;
+      cta_store(O, c0 + f0, kSub, [&](uint32_t q) { return ring[(f0 + q) & (kXorzRing - 1)]; });
+      flushed += kSub;
+      stored = true;
+    }
+    if (stored) __syncthreads();
+  }
+  if (flushed < qmin(vbase, n)) {
+    uint64_t f0 = flushed;
+    cta_store(O, c0 + f0, (uint32_t)(qmin(vbase, n) - f0), [&](uint32_t q) { return ring[(f0 + q) & (kXorzRing - 1)]; });
   }
   if (saw_nth) atomicMin(&S.nth, (unsigned long long)nth_pos);
   __syncthreads();
@@ -483,8 +595,7 @@ __device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64
 __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __restrict__ stream,
                                                               const FrameDesc* __restrict__ frames, int nf,
                                                               int dtype, const FrameAux* __restrict__ aux,
-                                                              uint64_t* __restrict__ lane,
-                                                              uint64_t* __restrict__ scratch,
+                                                              DecodeOut O, uint64_t* __restrict__ scratch,
                                                               unsigned long long* __restrict__ err) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   DecSmem& S = *reinterpret_cast<DecSmem*>(smem_raw);
@@ -495,56 +606,72 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
   FrameDesc d = frames[f];
   const uint8_t* p = stream + d.payload_off;
   uint64_t plen = d.plen, n = d.n;
-  uint64_t* out = lane + d.value_off;
+  uint64_t c0 = d.value_off;
   int t = threadIdx.x, l = t & 31, warp = t >> 5;
   uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
+  uint64_t* stg = &S.u.wbuf[warp][0];
   uint32_t e = E_OK;
   if (t == 0) S.flag = 0;
   __syncthreads();
   switch (d.mode) {
     case M_RAW: {
       uint32_t lb = lane_bytes(dtype);
-      if (dtype == DT_F32) {
-        for (uint64_t i = t; i < n; i += kDecThreads) out[i] = f32bits_to_f64bits(ld_u32(p + 4 * i));
-      } else if (lb == 4) {
-        for (uint64_t i = t; i < n; i += kDecThreads) out[i] = ld_u32(p + 4 * i);
-      } else {
-        for (uint64_t i = t; i < n; i += kDecThreads) out[i] = ld_u64(p + 8 * i);
+      for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+        uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+        const uint8_t* q0 = p + (uint64_t)k * kSub * lb;
+        if (dtype == DT_F32) {
+          warp_store(O, c0 + (uint64_t)k * kSub, cnt, [&](uint32_t q) { return f32bits_to_f64bits(ld_u32(q0 + 4 * q)); });
+        } else if (lb == 4) {
+          warp_store(O, c0 + (uint64_t)k * kSub, cnt, [&](uint32_t q) { return (uint64_t)ld_u32(q0 + 4 * q); });
+        } else {
+          warp_store(O, c0 + (uint64_t)k * kSub, cnt, [&](uint32_t q) { return ld_u64(q0 + 8 * q); });
+        }
       }
       break;
     }
     case M_CONST: {
       uint64_t v = ld_u64(p);
-      for (uint64_t i = t; i < n; i += kDecThreads) out[i] = v;
+      for (uint32_t k = warp; k < nsub; k += kDecWarps)
+        warp_store(O, c0 + (uint64_t)k * kSub, (uint32_t)qmin(kSub, n - (uint64_t)k * kSub), [&](uint32_t) { return v; });
       break;
     }
     case M_STRIDE: {
       uint64_t first = ld_u64(p), stride = ld_u64(p + 8);
-      for (uint64_t i = t; i < n; i += kDecThreads) out[i] = first + i * stride;
+      for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+        uint64_t i0 = (uint64_t)k * kSub;
+        warp_store(O, c0 + i0, (uint32_t)qmin(kSub, n - i0), [&](uint32_t q) { return first + (i0 + q) * stride; });
+      }
       break;
     }
     case M_XORZ:
-      e = dec_xorz(S, p, plen, n, out);
+      e = dec_xorz(S, p, plen, n, O, c0);
       break;
     case M_FOR_BITPACK:
       for (uint32_t k = warp; k < nsub; k += kDecWarps) {
         uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-        uint64_t* o = out + (size_t)k * kSub;
-        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) { o[i] = v; });
+        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) { stg[i] = v; });
+        __syncwarp();
+        warp_store(O, c0 + (uint64_t)k * kSub, cnt, [&](uint32_t q) { return stg[q]; });
+        __syncwarp();
       }
       break;
     case M_DELTA_BITPACK:
       chain_prefix(S, p, A.offs[0], n, ld_u64(p), &S.u.wbuf[0][0], kDecWarps,
-                   [](uint64_t v) { return unzigzag64(v); }, [&](uint64_t i, uint64_t v) { out[i] = v; });
+                   [](uint64_t v) { return unzigzag64(v); },
+                   [&](uint32_t k, const uint64_t* buf, uint32_t cnt) {
+                     warp_store(O, c0 + (uint64_t)k * kSub, cnt, [&](uint32_t q) { return buf[q]; });
+                   });
       break;
     case M_FLOAT_MULT: {
       double scale = kFmScales[A.a];
       for (uint32_t k = warp; k < nsub; k += kDecWarps) {
         uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-        uint64_t* o = out + (size_t)k * kSub;
         warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) {
-          o[i] = f64_bits(__ddiv_rn(__ll2double_rn((long long)v), scale));
+          stg[i] = f64_bits(__ddiv_rn(__ll2double_rn((long long)v), scale));
         });
+        __syncwarp();
+        warp_store(O, c0 + (uint64_t)k * kSub, cnt, [&](uint32_t q) { return stg[q]; });
+        __syncwarp();
       }
       break;
     }
@@ -556,11 +683,10 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
         int64_t mn = (int64_t)ld_u64(p + off + 4);
         uint32_t w = p[off + 12];
         uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-        uint64_t* o = out + (size_t)k * kSub;
         const uint8_t* words = p + off + 13;
         if (w == 0) {
           uint64_t v = f64_bits(alp_decode_value(mn, ee, ff));
-          for (uint32_t i = l; i < cnt; i += 32) o[i] = v;
+          for (uint32_t i = l; i < cnt; i += 32) stg[i] = v;
         } else {
           uint32_t mask = w == 32 ? 0xFFFFFFFFu : ((1u << w) - 1u);
           for (uint32_t r = 0; r < 32; r++) {
@@ -569,30 +695,36 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
             uint32_t v = ld_u32(words + 4u * (word * 32u + l)) >> sh;
             if (sh + w > 32) v |= ld_u32(words + 4u * ((word + 1) * 32u + l)) << (32 - sh);
             v &= mask;
-            if (idx < cnt) o[idx] = f64_bits(alp_decode_value((int64_t)((uint64_t)mn + v), ee, ff));
+            if (idx < cnt) stg[idx] = f64_bits(alp_decode_value((int64_t)((uint64_t)mn + v), ee, ff));
           }
         }
         __syncwarp();
         if (exc && l == 0) {  // in order, so a repeated position keeps the last exception
           const uint8_t* xp = words + 128u * w;
-          for (uint32_t x = 0; x < exc; x++) o[ld_u16(xp + 10 * x)] = ld_u64(xp + 10 * x + 2);
+          for (uint32_t x = 0; x < exc; x++) stg[ld_u16(xp + 10 * x)] = ld_u64(xp + 10 * x + 2);
         }
+        __syncwarp();
+        warp_store(O, c0 + (uint64_t)k * kSub, cnt, [&](uint32_t q) { return stg[q]; });
         __syncwarp();
       }
       break;
     case M_ALP_RD: {
       uint32_t lbw = (uint32_t)A.a, dsz = (uint32_t)A.b, rbw = 64 - lbw;
-      uint64_t* cb = &S.u.wbuf[warp][0];
+      // With exceptions the values are assembled in the frame's scratch range
+      // first (the exception list is one sequential stream over the frame).
+      uint64_t* fo = A.d ? scratch + d.value_off : nullptr;
       for (uint32_t k = warp; k < nsub; k += kDecWarps) {
         uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) { cb[i] = v; });
+        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) { stg[i] = v; });
         __syncwarp();
-        uint64_t* o = out + (size_t)k * kSub;
+        uint64_t* o = fo ? fo + (size_t)k * kSub : stg;
         warp_unpack(p, A.offs[1][k], cnt, [&](uint32_t i, uint64_t r) {
-          uint64_t c = cb[i];
+          uint64_t c = stg[i];
           if (c >= dsz) S.flag = 1;
           else o[i] = (A.dict8[c] << rbw) | r;
         });
+        __syncwarp();
+        if (!fo) warp_store(O, c0 + (uint64_t)k * kSub, cnt, [&](uint32_t q) { return stg[q]; });
         __syncwarp();
       }
       __syncthreads();
@@ -600,15 +732,19 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
         e = E_CORRUPT;
         break;
       }
-      if (t == 0 && A.d) {  // exceptions in order (alp_rd.rs:281-283)
-        uint64_t pos = A.c, rmask = (1ull << rbw) - 1ull;
-        for (uint64_t x = 0; x < A.d; x++) {
-          uint64_t pp = 0;
-          rd_varint(p, plen, &pos, &pp);
-          uint64_t lv = ld_u64(p + pos);
-          pos += 8;
-          out[pp] = (lv << rbw) | (out[pp] & rmask);
+      if (fo) {
+        if (t == 0) {  // exceptions in order (alp_rd.rs:281-283)
+          uint64_t pos = A.c, rmask = (1ull << rbw) - 1ull;
+          for (uint64_t x = 0; x < A.d; x++) {
+            uint64_t pp = 0;
+            rd_varint(p, plen, &pos, &pp);
+            uint64_t lv = ld_u64(p + pos);
+            pos += 8;
+            fo[pp] = (lv << rbw) | (fo[pp] & rmask);
+          }
         }
+        __syncthreads();
+        cta_store(O, c0, (uint32_t)n, [&](uint32_t q) { return fo[q]; });
       }
       break;
     }
@@ -625,20 +761,40 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
           break;
         }
         chain_prefix(S, p, A.offs[1], card, ld_u64(vb), &S.u.d.stage[0][0], 4,
-                     [](uint64_t v) { return unzigzag64(v); }, [&](uint64_t i, uint64_t v) { dd[i] = v; });
+                     [](uint64_t v) { return unzigzag64(v); },
+                     [&](uint32_t k, const uint64_t* buf, uint32_t cnt) {
+                       for (uint32_t q = l; q < cnt; q += 32) dd[(uint64_t)k * kSub + q] = buf[q];
+                     });
         dict = dd;
       } else if (card <= kDictSmem) {
         for (uint64_t i = t; i < card; i += kDecThreads) S.u.d.dict[i] = ld_u64(vb + 8 * i);
         __syncthreads();
         dict = S.u.d.dict;
       }
+      // codes -> values, per warp and sub-block: with the dictionary in smem the
+      // codes are staged as u16 beside it, else the values in the warp's buffer
       for (uint32_t k = warp; k < nsub; k += kDecWarps) {
         uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
-        uint64_t* o = out + (size_t)k * kSub;
-        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t c) {
-          if (c >= card) S.flag = 1;
-          else o[i] = dict ? dict[c] : ld_u64(vb + 8 * c);
-        });
+        if (dict == S.u.d.dict) {
+          uint16_t* cb = reinterpret_cast<uint16_t*>(&S.u.d.stage[0][0]) + (size_t)warp * kSub;
+          warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t c) {
+            if (c >= card) {
+              S.flag = 1;
+              c = 0;
+            }
+            cb[i] = (uint16_t)c;
+          });
+          __syncwarp();
+          warp_store(O, c0 + (uint64_t)k * kSub, cnt, [&](uint32_t q) { return dict[cb[q]]; });
+        } else {
+          warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t c) {
+            if (c >= card) S.flag = 1;
+            else stg[i] = dict ? dict[c] : ld_u64(vb + 8 * c);
+          });
+          __syncwarp();
+          warp_store(O, c0 + (uint64_t)k * kSub, cnt, [&](uint32_t q) { return stg[q]; });
+        }
+        __syncwarp();
       }
       __syncthreads();
       if (S.flag) e = E_CORRUPT;
@@ -670,32 +826,32 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
       __syncthreads();
       if (S.sc[0] == 1) { e = E_CORRUPT; break; }
       if (S.sc[0] == 2) { e = E_LENGTH_MISMATCH; break; }
-      // phase 2: per chunk, run ends in smem, then a warp-striped expand
-      uint64_t* ends = &S.u.wbuf[warp][0];
+      if (!scratch) { e = E_UNSUPPORTED; break; }
+      // phase 2: run ends (u32, the frame's scratch range) ...
+      uint32_t* ends = reinterpret_cast<uint32_t*>(scratch + d.value_off);
       for (uint32_t k = warp; k < nrs; k += kDecWarps) {
         uint32_t cnt = (uint32_t)qmin(kSub, nr - (uint64_t)k * kSub);
-        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) { ends[i] = v; });
+        warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) { stg[i] = v; });
         __syncwarp();
-        uint64_t start = S.subcarry[k];
-        warp_prefix_smem(ends, cnt, start, [&](uint32_t i, uint64_t v) { ends[i] = v; });
+        warp_prefix_smem(stg, cnt, S.subcarry[k], [&](uint32_t i, uint64_t v) { ends[(uint64_t)k * kSub + i] = (uint32_t)v; });
         __syncwarp();
-        uint64_t stop = start + S.subsum[k];
-        uint32_t r = 0;
-        bool init = false;
-        for (uint64_t i = start + l; i < stop; i += 32) {
-          if (!init) {
-            uint32_t lo = 0, hi = cnt;
-            while (lo < hi) {
-              uint32_t mid = (lo + hi) >> 1;
-              if (ends[mid] > i) hi = mid; else lo = mid + 1;
-            }
-            r = lo;
-            init = true;
-          }
-          while (ends[r] <= i) r++;
-          out[i] = ld_u64(rv + 8ull * ((uint64_t)k * kSub + r));
+      }
+      __syncthreads();
+      // ... phase 3: each warp expands whole output sub-blocks from a cursor
+      // found by binary search over the run ends
+      for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+        uint32_t lo = k * kSub, cnt = (uint32_t)qmin(kSub, n - lo);
+        uint32_t a = 0, b = (uint32_t)nr;
+        while (a < b) {
+          uint32_t mid = (a + b) >> 1;
+          if (ends[mid] > lo) b = mid; else a = mid + 1;
         }
-        __syncwarp();
+        uint32_t cur = a;
+        warp_store(O, c0 + lo, cnt, [&](uint32_t q) {
+          uint32_t i = lo + q;
+          while (ends[cur] <= i) cur++;
+          return ld_u64(rv + 8ull * cur);
+        });
       }
       break;
     }
@@ -721,6 +877,26 @@ __global__ void k_word_popcount(const uint8_t* __restrict__ bm, uint64_t n, uint
     uint64_t rem = n - w * 32;
     if (rem < 32) bits &= (1u << rem) - 1u;
     cnt[w] = (uint64_t)__popc(bits);
+  }
+}
+
+// sel[m] = position of the (1024*m)-th valid value: the owner of every 1024th
+// rank is the one bitmap word whose rank range contains it.
+__global__ void k_select_table(const uint8_t* __restrict__ bm, uint64_t n, const uint64_t* __restrict__ word_rank,
+                               uint64_t nvalid, uint64_t* __restrict__ sel) {
+  uint64_t nw = (n + 31) / 32, nbytes = (n + 7) / 8;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t bits = 0;
+    for (int k = 0; k < 4; k++)
+      if (w * 4 + k < nbytes) bits |= (uint32_t)bm[w * 4 + k] << (8 * k);
+    uint64_t rem = n - w * 32;
+    if (rem < 32) bits &= (1u << rem) - 1u;
+    uint64_t r = word_rank[w], c = (uint64_t)__popc(bits);
+    uint64_t m = (r + kSub - 1) / kSub * kSub;
+    if (m < r + c && m < nvalid) {
+      for (uint64_t k = m - r; k; k--) bits &= bits - 1u;  // drop the lower set bits
+      sel[m / kSub] = w * 32 + (uint64_t)(__ffs(bits) - 1);
+    }
   }
 }
 
@@ -799,14 +975,23 @@ __global__ void k_decimal_combine(const uint64_t* __restrict__ limbs, uint64_t l
 // ---------------------------------------------------------------------------
 uint64_t decode_aux_bytes(int nf) { return (uint64_t)(nf > 0 ? nf : 1) * sizeof(FrameAux); }
 
-void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, uint64_t* lane,
+void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
                           uint64_t* scratch, void* aux, unsigned long long* err, cudaStream_t st) {
   if (nf <= 0) return;
   FrameAux* A = reinterpret_cast<FrameAux*>(aux);
   k_walk_frames<<<(nf + 127) / 128, 128, 0, st>>>(stream, frames, nf, dtype, A, err);
   cudaFuncSetAttribute(k_decode_frames, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecSmem));
-  k_decode_frames<<<nf, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, nf, dtype, A, lane, scratch, err);
+  k_decode_frames<<<nf, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, nf, dtype, A, out, scratch, err);
   count_launches(2);
+}
+
+void launch_select_table(const uint8_t* bm, uint64_t n, const uint64_t* word_rank, uint64_t nvalid, uint64_t* sel,
+                         cudaStream_t st) {
+  uint64_t nw = (n + 31) / 32;
+  if (nw == 0) return;
+  unsigned g = (unsigned)qmin((nw + 255) / 256, 148ull * 16);
+  k_select_table<<<g, 256, 0, st>>>(bm, n, word_rank, nvalid, sel);
+  count_launches(1);
 }
 
 void launch_word_popcount(const uint8_t* bm, uint64_t n, uint64_t* cnt, cudaStream_t st) {

@@ -195,7 +195,7 @@ inline int plain_code(int ext) {
 enum Slot {
   S_IN, S_BM, S_RANK, S_LANE, S_GROW, S_FRAMES, S_NB, S_SIZES, S_TILE, S_SCRATCH, S_OUT, S_VTMP, S_VBLOB,
   S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_DAUX, S_SUBST, S_FMST,
-  S_SMP16, S_WINBITS, S_COUNT
+  S_SMP16, S_WINBITS, S_DSEL, S_COUNT
 };
 
 struct QuoinCtx {
@@ -559,7 +559,8 @@ struct LaneIdx {
   bool has_validity = false;
   std::vector<uint8_t> bitmap;  // ceil(n/8), trailing bits cleared
   std::vector<FrameDesc> frames;
-  bool any_dict = false;
+  bool any_dict = false;  // frames that need the decode scratch range (DICT, RLE, ALP-RD)
+  bool aligned = true;    // every frame but the last holds a multiple of 1024 values
   uint64_t frame_base = 0;  // index of the first frame in the device table
 };
 
@@ -645,7 +646,8 @@ int parse_lane(const uint8_t* src, uint64_t base, uint64_t len, LaneIdx& L) {
     f.mode = (uint32_t)mode;
     f.aux = 0;
     L.frames.push_back(f);
-    if (mode == 19) L.any_dict = true;
+    if (mode == 19 || mode == 53 || mode == 52) L.any_dict = true;
+    if (!L.frames.empty() && (L.frames.back().value_off % 1024) != 0) L.aligned = false;
     pos += plen;
     counted += fn;
     if (counted > L.n_total) return K_CORRUPT;
@@ -672,6 +674,7 @@ struct QuoinDecodeIndex {
   FrameDesc* d_frames = nullptr;
   uint8_t* d_bm = nullptr;
   uint64_t* d_rank = nullptr;
+  uint64_t* d_sel = nullptr;
   uint64_t* d_vmin = nullptr;
 };
 
@@ -748,8 +751,13 @@ uint64_t total_frames(const QuoinDecodeIndex& X) {
 
 // Upload the index tables into device buffers (dfr, dbm, drank, dvmin) and
 // compute the validity word ranks on the device.
+uint64_t sel_bytes(const QuoinDecodeIndex& X) {
+  uint64_t nv = X.decimal || X.lanes.empty() ? 0 : X.lanes[0].n_total;
+  return (nv / 1024 + 2) * 8;
+}
+
 int upload_index(QuoinCtx* c, cudaStream_t st, QuoinDecodeIndex& X, FrameDesc* dfr, uint8_t* dbm, uint64_t* drank,
-                 uint64_t* dvmin) {
+                 uint64_t* dsel, uint64_t* dvmin) {
   uint64_t fb = 0;
   for (auto& L : X.lanes) {
     L.frame_base = fb;
@@ -763,6 +771,7 @@ int upload_index(QuoinCtx* c, cudaStream_t st, QuoinDecodeIndex& X, FrameDesc* d
     CK(c->ensure(S_TILE, (scan_tile_count(nw) + 16) * 8));
     launch_word_popcount(dbm, X.n, drank, st);
     launch_scan_sum(drank, drank, nw, c->p<uint64_t>(S_TILE), nullptr, st);
+    if (!X.decimal) launch_select_table(dbm, X.n, drank, X.lanes[0].n_total, dsel, st);
   }
   if (X.decimal) CK(cudaMemcpyAsync(dvmin, X.vmin, 32, cudaMemcpyHostToDevice, st));
   CK(cudaStreamSynchronize(st));
@@ -771,8 +780,8 @@ int upload_index(QuoinCtx* c, cudaStream_t st, QuoinDecodeIndex& X, FrameDesc* d
 
 // Decode the lanes of an uploaded index from the device stream d_src.
 int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, const FrameDesc* dfr, const uint8_t* dbm,
-                   const uint64_t* drank, const uint64_t* dvmin, const uint8_t* d_src, void* d_out,
-                   uint8_t* d_valid_out) {
+                   const uint64_t* drank, const uint64_t* dsel, const uint64_t* dvmin, const uint8_t* d_src,
+                   void* d_out, uint8_t* d_valid_out) {
   CK(c->ensure(S_ERR, 64));
   unsigned long long* d_err = c->p<unsigned long long>(S_ERR);
   CK(cudaMemsetAsync(d_err, 0xFF, 8, st));
@@ -783,26 +792,35 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
   void* daux = c->p<void>(S_DAUX);
   if (!X.decimal) {
     const LaneIdx& L = X.lanes[0];
-    bool direct = !X.has_validity && lane_bytes_h(X.wire) == 8 && ((uintptr_t)d_out & 7) == 0;
-    uint64_t* lane_out;
-    if (direct) {
-      lane_out = (uint64_t*)d_out;
-    } else {
-      CK(c->ensure(S_LANE, L.n_total * 8 + 64));
-      lane_out = c->p<uint64_t>(S_LANE);
-    }
+    uint32_t w = native_width(X.wire);
     uint64_t* scr = nullptr;
     if (L.any_dict) {
       CK(c->ensure(S_DSCR, L.n_total * 8 + 64));
       scr = c->p<uint64_t>(S_DSCR);
     }
-    {
-      TimedRegion tr(T_DECODE, st);
-      launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, lane_out, scr, daux, d_err, st);
-    }
-    if (!direct && X.n) {
-      TimedRegion tr(T_FINALIZE, st);
-      launch_finalize(lane_out, bm, drank, X.n, X.wire, d_out, st);
+    // Fused: decoded values go straight to the typed column (narrowed, and
+    // scattered through the bitmap when there is one).
+    bool fused = (!X.has_validity || L.aligned) && ((uintptr_t)d_out % w) == 0;
+    if (fused) {
+      DecodeOut O{d_out, X.wire, X.has_validity ? reinterpret_cast<const uint32_t*>(dbm) : nullptr, drank, dsel, X.n,
+                  L.n_total};
+      {
+        TimedRegion tr(T_DECODE, st);
+        launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, scr, daux, d_err, st);
+      }
+      if (L.n_total == 0 && X.n) CK(cudaMemsetAsync(d_out, 0, X.n * w, st));  // all null
+    } else {
+      CK(c->ensure(S_LANE, L.n_total * 8 + 64));
+      uint64_t* lane_out = c->p<uint64_t>(S_LANE);
+      DecodeOut O{lane_out, WT_U64, nullptr, nullptr, nullptr, L.n_total, L.n_total};
+      {
+        TimedRegion tr(T_DECODE, st);
+        launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, scr, daux, d_err, st);
+      }
+      if (X.n) {
+        TimedRegion tr(T_FINALIZE, st);
+        launch_finalize(lane_out, bm, drank, X.n, X.wire, d_out, st);
+      }
     }
   } else {
     CK(c->ensure(S_LIMBS, (uint64_t)X.nl * X.n_valid * 8 + 64));
@@ -817,9 +835,9 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
     }
     for (int k = 0; k < X.nl; k++) {
       const LaneIdx& L = X.lanes[k];
+      DecodeOut O{limbs + (uint64_t)k * X.n_valid, WT_U64, nullptr, nullptr, nullptr, X.n_valid, X.n_valid};
       TimedRegion tr(T_DECODE, st);
-      launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), WT_U64, limbs + (uint64_t)k * X.n_valid,
-                           scr, daux, d_err, st);
+      launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), WT_U64, O, scr, daux, d_err, st);
     }
     if (X.n) {
       TimedRegion tr(T_FINALIZE, st);
@@ -850,14 +868,16 @@ int decompress_host(QuoinCtx* c, const uint8_t* src, uint64_t len, void* values_
   CK(c->ensure(S_DRANK, ((X->n + 31) / 32 + 1) * 8));
   CK(c->ensure(S_MISC, 64 * 8));
   uint64_t* dvmin = c->p<uint64_t>(S_MISC) + 32;
-  int rc = upload_index(c, st, *X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK), dvmin);
+  CK(c->ensure(S_DSEL, sel_bytes(*X)));
+  int rc = upload_index(c, st, *X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK),
+                        c->p<uint64_t>(S_DSEL), dvmin);
   if (rc) return rc;
   CK(c->ensure(S_SRC, len + 64));
   if (len) CK(cudaMemcpyAsync(c->p<uint8_t>(S_SRC), src, len, cudaMemcpyHostToDevice, st));
   uint64_t out_bytes = X->n * native_width(X->wire);
   CK(c->ensure(S_OUTVALS, out_bytes + 64));
-  rc = decode_indexed(c, st, *X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK), dvmin,
-                      c->p<uint8_t>(S_SRC), c->p<void>(S_OUTVALS), nullptr);
+  rc = decode_indexed(c, st, *X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK),
+                      c->p<uint64_t>(S_DSEL), dvmin, c->p<uint8_t>(S_SRC), c->p<void>(S_OUTVALS), nullptr);
   if (rc) return rc;
   if (out_bytes) CK(cudaMemcpyAsync(values_out, c->p<void>(S_OUTVALS), out_bytes, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -1268,13 +1288,14 @@ int quoin_b200_index_create(QuoinCtx* ctx, const uint8_t* src, size_t len, Quoin
     bool ok = cudaMalloc(&X->d_frames, (nf + 1) * sizeof(FrameDesc)) == cudaSuccess &&
               cudaMalloc(&X->d_bm, X->bitmap.size() + 16) == cudaSuccess &&
               cudaMalloc(&X->d_rank, ((X->n + 31) / 32 + 1) * 8) == cudaSuccess &&
+              cudaMalloc(&X->d_sel, sel_bytes(*X)) == cudaSuccess &&
               cudaMalloc(&X->d_vmin, 64) == cudaSuccess;
     if (!ok) {
       cudaGetLastError();
       quoin_b200_index_free(X);
       return QUOIN_ERR_CUDA;
     }
-    int rc = upload_index(c, c->stream, *X, X->d_frames, X->d_bm, X->d_rank, X->d_vmin);
+    int rc = upload_index(c, c->stream, *X, X->d_frames, X->d_bm, X->d_rank, X->d_sel, X->d_vmin);
     if (rc) {
       quoin_b200_index_free(X);
       return rc;
@@ -1293,6 +1314,7 @@ void quoin_b200_index_free(QuoinDecodeIndex* X) {
     if (X->d_frames) cudaFree(X->d_frames);
     if (X->d_bm) cudaFree(X->d_bm);
     if (X->d_rank) cudaFree(X->d_rank);
+    if (X->d_sel) cudaFree(X->d_sel);
     if (X->d_vmin) cudaFree(X->d_vmin);
   }
   delete X;
@@ -1315,7 +1337,8 @@ int quoin_b200_decompress_indexed_device(QuoinCtx* ctx, const QuoinDecodeIndex* 
     std::lock_guard<std::mutex> l(c->mu);
     DeviceScope ds(c->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-    return decode_indexed(c, st, *X, X->d_frames, X->d_bm, X->d_rank, X->d_vmin, d_src, d_values_out, d_validity_out);
+    return decode_indexed(c, st, *X, X->d_frames, X->d_bm, X->d_rank, X->d_sel, X->d_vmin, d_src, d_values_out,
+                          d_validity_out);
   } catch (...) {
     return QUOIN_ERR_PANIC;
   }

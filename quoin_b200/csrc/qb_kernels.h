@@ -12,8 +12,25 @@ namespace qb {
 // Walk (validation + sub-block offsets) and decode of nf frames.  `aux` is
 // device scratch of decode_aux_bytes(nf) bytes.
 uint64_t decode_aux_bytes(int nf);
-void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, uint64_t* lane,
+// Where decoded values go: the lane (out = u64 per lane value, bm32 null,
+// dtype DT_U64) or the typed column (narrowed to dtype's native width and,
+// with bm32, scattered through the validity words with nulls as 0; wrank =
+// exclusive popcount prefix per 32-bit word, sel from launch_select_table).
+// With a bitmap every frame but the last must hold a multiple of 1024 values.
+struct DecodeOut {
+  void* out;
+  int dtype;
+  const uint32_t* bm32;
+  const uint64_t* wrank;
+  const uint64_t* sel;
+  uint64_t n;       // logical values (positions)
+  uint64_t nvalid;  // lane values
+};
+void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
                           uint64_t* scratch, void* aux, unsigned long long* err, cudaStream_t st);
+// sel[m] = position of the (1024*m)-th valid value, m < ceil(nvalid / 1024).
+void launch_select_table(const uint8_t* bm, uint64_t n, const uint64_t* word_rank, uint64_t nvalid, uint64_t* sel,
+                         cudaStream_t st);
 void launch_word_popcount(const uint8_t* bm, uint64_t n, uint64_t* cnt, cudaStream_t st);
 void launch_finalize(const uint64_t* lane, const uint8_t* bm, const uint64_t* word_rank, uint64_t n, int dtype,
                      void* out, cudaStream_t st);

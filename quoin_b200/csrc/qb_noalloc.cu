@@ -47,7 +47,7 @@ struct NoAllocArena {
   NoAllocStatus st;
   FrameDesc frames[kNoAllocMaxFrames];
   uint8_t aux[kNoAllocMaxFrames * kNoAllocAuxBytes];
-  uint64_t dict[kNoAllocMaxValues];  // large delta-coded dictionaries, one slot per value
+  uint64_t dict[kNoAllocMaxValues];  // decode scratch (large dictionaries, RLE run ends, ALP-RD), one slot per value
 };
 
 static __device__ __align__(256) NoAllocArena g_noalloc_arena;
@@ -177,8 +177,8 @@ extern "C" int quoin_b200_decompress_device_noalloc(const uint8_t* d_src, size_t
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     k_noalloc_parse<<<1, 32, 0, st>>>(d_src, src_len, out_cap_values, A);
     count_launches(1);
-    launch_decode_frames(d_src, A->frames, (int)kNoAllocMaxFrames, DT_U64, static_cast<uint64_t*>(d_values_out),
-                         A->dict, A->aux, &A->st.err, st);
+    DecodeOut O{d_values_out, DT_U64, nullptr, nullptr, nullptr, 0, 0};
+    launch_decode_frames(d_src, A->frames, (int)kNoAllocMaxFrames, DT_U64, O, A->dict, A->aux, &A->st.err, st);
     NoAllocStatus hs;
     if (cudaMemcpyAsync(&hs, &A->st, sizeof(hs), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {

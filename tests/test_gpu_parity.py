@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 from conftest import bitmap_from_bools, lcg1_seq, lcg_seq
+from quoin_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
@@ -116,6 +117,22 @@ def shape_cases():
               U64, None))
     c.append(("dict_scratch_grown", np.repeat(pool[(lcg1_seq(37, 60000) >> np.uint64(40)) % 2800], 3)[:170000],
               U64, None))
+    # Nullable columns of every decode shape: values are scattered through the
+    # bitmap straight from the block decoder.
+    vb2 = rng.random(150000) > 0.2
+    cats = (lcg_seq(41, 64) >> np.uint64(33)).astype(np.int64) - (1 << 30)
+    c.append(("nullable_i32_rle", np.repeat(cats[rng.integers(0, 64, 10000)], 15)[:150000].astype(np.int32), I32,
+              bitmap_from_bools(vb2)))
+    c.append(("nullable_u64_xorz", synth.runs_u64(150000, np.random.default_rng(5)), U64, bitmap_from_bools(vb2)))
+    c.append(("nullable_f32", (np.round(rng.normal(25, 5, 150000) * 10) / 10).astype(np.float32), F32,
+              bitmap_from_bools(vb2)))
+    c.append(("nullable_f64_walk", 20.0 + np.cumsum(rng.normal(0, 1e-3, 150000)), F64, bitmap_from_bools(vb2)))
+    u12 = rng.random(150000) + 1.0
+    u12[rng.integers(0, 150000, 1500)] = rng.random(1500) * 1e6
+    c.append(("nullable_f64_alprd", u12, F64, bitmap_from_bools(vb2)))
+    c.append(("nullable_f64_alp", np.floor(rng.random(150000) * 1_000_000 + 0.5) / 100.0, F64, bitmap_from_bools(vb2)))
+    c.append(("nullable_dict_scratch", pool[(lcg1_seq(43, 150000) >> np.uint64(40)) % 2500], U64,
+              bitmap_from_bools(vb2)))
     vb = rng.random(300000) > 0.1
     c.append(("nullable_ts_300k", (np.cumsum(1_000_000 + rng.poisson(5000, 300000)) + 1_700_000_000_000_000_000)
               .astype(np.int64), I64, bitmap_from_bools(vb)))
@@ -141,6 +158,22 @@ def test_shapes_match_oracle(qb, oracle, case, level):
 def test_fixed_block_sizes(qb, oracle, bs):
     vals = (1000 + np.arange(40_000) % 777).astype(np.int64)
     assert gpu_compress(qb, vals, I64, block_size=bs) == oracle.compress_column(vals, I64, block_size=bs)
+
+
+@pytest.mark.parametrize("bs", [1000, 2048, 5000])
+def test_fixed_block_sizes_with_nulls(qb, oracle, bs):
+    """Block sizes that are and are not multiples of 1024, with a bitmap."""
+    rng = np.random.default_rng(bs)
+    vals = (1_000_000 + np.cumsum(rng.poisson(40, 30_000))).astype(np.int64)
+    bm = bitmap_from_bools(rng.random(30_000) > 0.3)
+    want = oracle.compress_column(vals, I64, bm, block_size=bs)
+    assert gpu_compress(qb, vals, I64, bm, block_size=bs) == want
+    d = qb.decompress_column(want)
+    assert dec_bytes(d) == expected_values(vals, I64, bm)
+    vals32 = (vals % 1000).astype(np.int32)
+    want32 = oracle.compress_column(vals32, I32, bm, block_size=bs)
+    assert gpu_compress(qb, vals32, I32, bm, block_size=bs) == want32
+    assert dec_bytes(qb.decompress_column(want32)) == expected_values(vals32, I32, bm)
 
 
 def test_predictor_log2_is_recorded(qb, oracle):
