@@ -360,6 +360,11 @@ __device__ __forceinline__ void warp_store_words(const DecodeOut& O, uint64_t w0
     for (uint32_t j = 0; j < nw; j++) {
       uint32_t bits = __shfl_sync(0xffffffffu, mine, j);
       uint64_t base = (wb + j) << 5;
+      if (bits == 0xFFFFFFFFu && base >= p0 && base + 32 <= p1) {  // 32 valid values in a row
+        put_out(O, base + l, val(rel + (uint32_t)l));
+        rel += 32;
+        continue;
+      }
       uint32_t in = 0xFFFFFFFFu;  // positions of this word inside [p0, p1)
       if (base < p0) in &= 0xFFFFFFFFu << (uint32_t)(p0 - base);
       if (base + 32 > p1) in &= 0xFFFFFFFFu >> (uint32_t)(base + 32 - p1);
@@ -596,11 +601,12 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
                                                               const FrameDesc* __restrict__ frames, int nf,
                                                               int dtype, const FrameAux* __restrict__ aux,
                                                               DecodeOut O, uint64_t* __restrict__ scratch,
-                                                              unsigned long long* __restrict__ err) {
+                                                              unsigned long long* __restrict__ err,
+                                                              const uint32_t* __restrict__ list) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   DecSmem& S = *reinterpret_cast<DecSmem*>(smem_raw);
-  int f = blockIdx.x;
-  if (f >= nf) return;
+  if ((int)blockIdx.x >= nf) return;
+  int f = list ? (int)list[blockIdx.x] : (int)blockIdx.x;
   const FrameAux& A = aux[f];
   if (A.err) return;
   FrameDesc d = frames[f];
@@ -862,6 +868,584 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
   if (e && t == 0) atomicMin(err, ((unsigned long long)f << 8) | e);
 }
 
+// ===========================================================================
+// Warp-item decoder.  The frame table is cut into warp-sized items of at most
+// 512 values (half a FastLanes sub-block) or 512 XORZ payload bytes, so every
+// warp of the grid has the same amount of work whatever the frame sizes.
+// Modes whose values depend on everything before them in the frame carry
+// state across items through a prepass:
+//   DELTA  item sums of the deltas      -> carry = base + sums before
+//   RLE    run-chunk (1024 runs) sums   -> start value of each chunk
+//   XORZ   per item value count, XOR of the values ending in it, last
+//          terminator, over-long flag   -> value base and XOR carry
+// and a per-frame scan (one warp per frame) that also performs the frame-level
+// checks in the sequential decoder's order.  DICT frames and ALP-RD frames
+// with exceptions are decoded by k_decode_frames from a frame list.
+// ===========================================================================
+constexpr int kItemVals = 512;
+constexpr int kItemBytes = 512;          // XORZ payload bytes per item
+constexpr int kItemStage = kItemVals + kItemVals / 16;  // u64 staging with one pad per 16
+constexpr int kItemWarps = 8;
+
+struct PreRec {
+  uint64_t a;     // DELTA/RLE: sum; XORZ: XOR of values ending in the item.  After the scan: carry / start / XOR carry
+  uint64_t b;     // XORZ: value count.  After the scan: value base
+  int64_t last;   // XORZ: last terminator (payload-relative), -1 if none
+  uint32_t flag;  // XORZ: a value longer than 10 bytes ends in the item
+  uint32_t pad;
+};
+static_assert(sizeof(PreRec) == 32, "PreRec layout");
+
+__device__ __forceinline__ uint32_t skew(uint32_t i) { return i + (i >> 4); }
+
+// Half h (values [512h, 512h+512) of a sub-block holding `count` values) of a
+// FastLanes FoR sub-block; f(i, v) with i relative to the sub-block.
+template <class F>
+__device__ inline void warp_unpack_half(const uint8_t* p, uint32_t off, uint32_t h, uint32_t count, F f) {
+  int l = threadIdx.x & 31;
+  uint32_t w = p[off];
+  uint64_t mn = ld_u64(p + off + 1);
+  const uint8_t* words = p + off + 9;
+  if (w == 0) {
+    uint32_t e = min(count, (h + 1) * kItemVals);
+    for (uint32_t i = h * kItemVals + l; i < e; i += 32) f(i, mn);
+  } else if (w <= 32) {
+    // lane l's bit stream: rows 16h .. 16h+15 start at bit 16h*w; words are
+    // read once each into a 64-bit buffer
+    uint32_t mask = w == 32 ? 0xFFFFFFFFu : ((1u << w) - 1u);
+    uint32_t bit0 = h * 16 * w, wd = bit0 >> 5;
+    const uint8_t* lw = words + 4u * l;
+    uint64_t buf = ld_u32(lw + 128u * wd) >> (bit0 & 31);
+    uint32_t nb = 32 - (bit0 & 31);
+    wd++;
+#pragma unroll 4
+    for (uint32_t r = h * 16; r < h * 16 + 16; r++) {
+      if (nb < w) {
+        buf |= (uint64_t)ld_u32(lw + 128u * wd) << nb;
+        wd++;
+        nb += 32;
+      }
+      uint32_t v = (uint32_t)buf & mask;
+      buf >>= w;
+      nb -= w;
+      uint32_t idx = r * 32 + l;
+      if (idx < count) f(idx, mn + (uint64_t)v);
+    }
+  } else {
+    uint64_t mask = w == 64 ? ~0ull : ((1ull << w) - 1ull);
+    uint32_t fl = l & 15, r0 = h * 32 + (l >> 4) * 16;
+#pragma unroll 8
+    for (uint32_t r = r0; r < r0 + 16; r++) {
+      uint32_t idx = r * 16 + fl;
+      uint32_t bit = r * w, word = bit >> 6, sh = bit & 63;
+      uint64_t v = ld_u64(words + 8u * (word * 16u + fl)) >> sh;
+      if (sh + w > 64) v |= ld_u64(words + 8u * ((word + 1) * 16u + fl)) << (64 - sh);
+      v &= mask;
+      if (idx < count) f(idx, mn + v);
+    }
+  }
+}
+
+// Position of the c-th valid value (c < nvalid): from the 1024-granular table,
+// the owning bitmap word is found 32 words at a time.
+__device__ uint64_t warp_select(const DecodeOut& O, uint64_t c) {
+  if (!O.bm32) return c;
+  if (c >= O.nvalid) return O.n;
+  uint64_t s = O.sel[c >> 10];
+  if ((c & 1023) == 0) return s;
+  int l = threadIdx.x & 31;
+  uint64_t nw = (O.n + 31) >> 5;
+  uint32_t tail = (uint32_t)(O.n & 31);
+  for (uint64_t w0 = s >> 5; w0 < nw; w0 += 32) {
+    uint64_t w = w0 + l;
+    uint32_t bits = 0;
+    uint64_t r = 0;
+    bool hit = false;
+    if (w < nw) {
+      bits = O.bm32[w];
+      if (w == nw - 1 && tail) bits &= (1u << tail) - 1u;
+      r = O.wrank[w];
+      hit = r <= c && c < r + (uint64_t)__popc(bits);
+    }
+    uint32_t m = __ballot_sync(0xffffffffu, hit);
+    if (m) {
+      int src = __ffs(m) - 1;
+      bits = __shfl_sync(0xffffffffu, bits, src);
+      r = __shfl_sync(0xffffffffu, r, src);
+      for (uint64_t k = c - r; k; k--) bits &= bits - 1u;
+      return ((w0 + (uint64_t)src) << 5) + (uint64_t)(__ffs(bits) - 1);
+    }
+  }
+  return O.n;
+}
+
+// Store the run [c0, c0 + cnt) of lane values (any c0): it owns the positions
+// from the c0-th valid value (0 for c0 = 0) to the (c0+cnt)-th (n at the end).
+template <class V>
+__device__ void warp_store_any(const DecodeOut& O, uint64_t c0, uint32_t cnt, V val) {
+  if (cnt == 0) return;
+  if (!O.bm32) {
+    for (uint32_t q = threadIdx.x & 31; q < cnt; q += 32) put_out(O, c0 + q, val(q));
+    return;
+  }
+  uint64_t p0 = c0 == 0 ? 0 : warp_select(O, c0);
+  uint64_t p1 = c0 + cnt >= O.nvalid ? O.n : warp_select(O, c0 + cnt);
+  if (p1 > p0) warp_store_words(O, p0 >> 5, (p1 + 31) >> 5, p0, p1, 0u, val);
+}
+
+// In-place inclusive prefix sum (wrapping u64) of stg[skew(0 .. cnt)), cnt <=
+// 512, starting from `carry`: each lane sums 16 consecutive entries.
+__device__ inline void warp_prefix_skewed(uint64_t* stg, uint32_t cnt, uint64_t carry) {
+  int l = threadIdx.x & 31;
+  uint32_t b0 = (uint32_t)l * 16;
+  uint64_t s = 0;
+#pragma unroll
+  for (int j = 0; j < 16; j++)
+    if (b0 + j < cnt) s += stg[skew(b0 + j)];
+  uint64_t inc = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (l >= o) inc += u;
+  }
+  uint64_t run = carry + inc - s;
+#pragma unroll
+  for (int j = 0; j < 16; j++)
+    if (b0 + j < cnt) {
+      run += stg[skew(b0 + j)];
+      stg[skew(b0 + j)] = run;
+    }
+  __syncwarp();
+}
+
+// One XORZ item: payload bytes [s, s + 512) of a frame with plen bytes.  Lane l
+// owns bytes [s + 16l, s + 16l + 16).  XOR is linear, so the value v_i = x_1 ^
+// ... ^ x_i is the XOR of every byte's contribution (b & 0x7f) << 7j (j = the
+// byte's index inside its LEB128 value) up to value i's terminator: each lane
+// folds its bytes into a running state and a terminator emits the state.
+// Pass 1 (xorz_lane_scan) gives per lane its values, contribution XOR and the
+// terminator bookkeeping; pass 2 (xorz_lane_emit) re-runs the bytes from the
+// lane's starting state.  Bytes at or beyond a value's 11th are ignored and
+// a terminator there marks the value over-long (xorz.rs / varint.rs limits).
+struct XSlice {
+  uint32_t cnt, before, total;  // lane values, values in lanes before, item values
+  uint64_t xo;                  // XOR of the lane's byte contributions
+  int64_t lastt;                // item's last terminator (-1 none)
+  uint32_t bad;                 // lane ended an over-long value
+  uint32_t first_bad;           // lane-local index of the first such value (~0 none)
+  uint32_t tm;                  // lane's terminator mask over its 16 bytes
+  uint64_t b0;                  // lane's first byte
+  uint32_t j0;                  // index inside its value of the lane's first byte (capped at 10)
+  uint32_t nb;                  // lane's bytes inside the payload
+  uint64_t w0, w1;              // the lane's 16 bytes
+};
+
+__device__ __forceinline__ uint32_t term_mask8(uint64_t w) {
+  uint64_t t = (~w & 0x8080808080808080ull) >> 7;
+  return (uint32_t)((t * 0x0102040810204080ull) >> 56);
+}
+
+template <bool EMIT>
+__device__ __forceinline__ uint64_t xorz_lane_bytes(XSlice& X, uint64_t state, uint64_t* stg, uint32_t k) {
+  uint32_t j = X.j0;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    if ((uint32_t)q < X.nb) {
+      uint32_t b = (uint32_t)(((q < 8) ? (X.w0 >> (8 * q)) : (X.w1 >> (8 * (q - 8)))) & 0xFFu);
+      if (j < 10) state ^= (uint64_t)(b & 0x7Fu) << (7 * j);
+      if (!(b & 0x80u)) {
+        if (!EMIT && j >= 10) {
+          if (!X.bad) X.first_bad = k;
+          X.bad = 1;
+        }
+        if (EMIT) stg[skew(X.before + k)] = state;
+        k++;
+        j = 0;
+      } else {
+        j = j < 10 ? j + 1 : 10;
+      }
+    }
+  }
+  return state;
+}
+
+__device__ XSlice xorz_lane_scan(const uint8_t* p, uint64_t plen, uint64_t s) {
+  int l = threadIdx.x & 31;
+  XSlice X;
+  X.b0 = s + (uint64_t)l * 16;
+  X.nb = X.b0 < plen ? (uint32_t)qmin(16, plen - X.b0) : 0u;
+  if (X.nb == 16) {
+    X.w0 = ld_u64(p + X.b0);
+    X.w1 = ld_u64(p + X.b0 + 8);
+  } else {
+    X.w0 = 0;
+    X.w1 = 0;
+    for (uint32_t q = 0; q < X.nb; q++) {
+      uint64_t b = p[X.b0 + q];
+      if (q < 8) X.w0 |= b << (8 * q); else X.w1 |= b << (8 * (q - 8));
+    }
+  }
+  uint32_t tm = term_mask8(X.w0) | (term_mask8(X.w1) << 8);
+  if (X.nb < 16) tm &= (1u << X.nb) - 1u;
+  X.tm = tm;
+  X.cnt = __popc(tm);
+  int64_t mylast = tm ? (int64_t)(X.b0 + 31 - __clz(tm)) : -1;
+  // the terminator before the item: look back at most 10 bytes
+  int64_t found = -1;
+  if (s > 0 && l < 10 && (uint64_t)l < s) {
+    uint64_t q = s - 1 - (uint64_t)l;
+    if (!(p[q] & 0x80)) found = (int64_t)q;
+  }
+  for (int o = 16; o; o >>= 1) {
+    int64_t u = __shfl_xor_sync(0xffffffffu, found, o);
+    found = u > found ? u : found;
+  }
+  int64_t item_prev = s == 0 ? -1 : (found >= 0 ? found : (s >= 11 ? (int64_t)s - 11 : -1));
+  uint32_t inc = X.cnt;
+  int64_t mx = mylast;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+    int64_t um = __shfl_up_sync(0xffffffffu, mx, o);
+    if (l >= o) {
+      inc += u;
+      mx = um > mx ? um : mx;
+    }
+  }
+  X.before = inc - X.cnt;
+  X.total = __shfl_sync(0xffffffffu, inc, 31);
+  X.lastt = __shfl_sync(0xffffffffu, mx, 31);
+  int64_t prev = __shfl_up_sync(0xffffffffu, mx, 1);  // last terminator in the lanes before
+  if (l == 0 || prev < item_prev) prev = item_prev;
+  uint64_t dist = X.b0 - (uint64_t)(prev + 1);
+  X.j0 = (uint32_t)qmin(dist, 10);
+  X.bad = 0;
+  X.first_bad = ~0u;
+  X.xo = xorz_lane_bytes<false>(X, 0ull, nullptr, 0);
+  return X;
+}
+
+__device__ inline uint32_t warp_or_u32(uint32_t v) {
+  for (int o = 16; o; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Prepass: one warp per prepass item.
+__global__ void __launch_bounds__(kItemWarps * 32) k_prepass(const uint8_t* __restrict__ stream,
+                                                           const FrameDesc* __restrict__ frames,
+                                                           const FrameAux* __restrict__ aux,
+                                                           const ItemRef* __restrict__ items, uint32_t nitems,
+                                                           PreRec* __restrict__ pre, uint64_t* __restrict__ scratch) {
+  __shared__ uint32_t rle_stage[kItemWarps][kSub];
+  uint32_t g = blockIdx.x * kItemWarps + (threadIdx.x >> 5);
+  int l = threadIdx.x & 31;
+  if (g >= nitems) return;
+  ItemRef it = items[g];
+  const FrameAux& A = aux[it.frame];
+  if (A.err) return;
+  FrameDesc d = frames[it.frame];
+  const uint8_t* p = stream + d.payload_off;
+  uint64_t n = d.n;
+  PreRec R;
+  R.a = 0;
+  R.b = 0;
+  R.last = -1;
+  R.flag = 0;
+  R.pad = 0;
+  if (d.mode == M_DELTA_BITPACK) {
+    uint32_t k = it.local >> 1, h = it.local & 1;
+    uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+    uint64_t s = 0;
+    warp_unpack_half(p, A.offs[0][k], h, cnt, [&](uint32_t, uint64_t v) { s += unzigzag64(v); });
+    R.a = warp_sum(s);
+  } else if (d.mode == M_RLE) {
+    // run chunk k: the saturating length sum (validation) and the chunk-local
+    // run ends (u32, the frame's scratch range) for the output items
+    uint64_t nr = A.a;
+    uint32_t k = it.local;
+    uint32_t cnt = (uint32_t)qmin(kSub, nr - (uint64_t)k * kSub);
+    uint32_t* ends = reinterpret_cast<uint32_t*>(scratch + d.value_off) + (uint64_t)k * kSub;
+    uint32_t* buf = rle_stage[threadIdx.x >> 5];
+    uint64_t s = 0;
+    warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t v) {
+      s = qmin(s + qmin(v, n + 1), n + 1);
+      buf[i] = (uint32_t)v;
+    });
+    __syncwarp();
+    uint32_t run = 0;
+    for (uint32_t base = 0; base < cnt; base += 32) {  // every lane takes every step
+      uint32_t i = base + l;
+      uint32_t inc = i < cnt ? buf[i] : 0u;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (l >= o) inc += u;
+      }
+      if (i < cnt) ends[i] = run + inc;
+      run += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    for (int o = 16; o; o >>= 1) s = qmin(s + __shfl_xor_sync(0xffffffffu, s, o), n + 1);
+    R.a = s;
+  } else if (d.mode == M_XORZ) {
+    XSlice X = xorz_lane_scan(p, d.plen, (uint64_t)it.local * kItemBytes);
+    uint64_t xo = X.xo;
+    for (int o = 16; o; o >>= 1) xo ^= __shfl_xor_sync(0xffffffffu, xo, o);
+    R.a = xo;
+    R.b = X.total;
+    R.last = X.lastt;
+    R.flag = warp_or_u32(X.bad);
+  }
+  if (l == 0) pre[g] = R;
+}
+
+// Per frame (one warp): exclusive scan of its prepass records and the
+// frame-level checks.  frame_pre[f] = (first prepass record, count).
+__global__ void k_prepass_scan(const uint8_t* __restrict__ stream, const FrameDesc* __restrict__ frames, int nf,
+                               FrameAux* __restrict__ aux, const uint2* __restrict__ frame_pre,
+                               PreRec* __restrict__ pre, unsigned long long* __restrict__ err) {
+  int f = blockIdx.x * kItemWarps + (threadIdx.x >> 5);
+  int l = threadIdx.x & 31;
+  if (f >= nf) return;
+  FrameDesc d = frames[f];
+  if (d.mode != M_DELTA_BITPACK && d.mode != M_RLE && d.mode != M_XORZ) return;
+  if (aux[f].err) return;
+  uint2 fp = frame_pre[f];
+  PreRec* R = pre + fp.x;
+  const uint8_t* p = stream + d.payload_off;
+  uint64_t n = d.n;
+  uint64_t carry_a = d.mode == M_DELTA_BITPACK ? ld_u64(p) : 0ull;
+  uint64_t carry_b = 0;
+  int64_t last = -1;
+  uint32_t flag = 0;
+  for (uint32_t b = 0; b < fp.y; b += 32) {
+    uint32_t i = b + l;
+    PreRec r;
+    r.a = 0;
+    r.b = 0;
+    r.last = -1;
+    r.flag = 0;
+    if (i < fp.y) r = R[i];
+    uint64_t ia = r.a, ib = r.b;
+    int64_t im = r.last;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t ua = __shfl_up_sync(0xffffffffu, ia, o);
+      uint64_t ub = __shfl_up_sync(0xffffffffu, ib, o);
+      int64_t um = __shfl_up_sync(0xffffffffu, im, o);
+      if (l >= o) {
+        ia = d.mode == M_XORZ ? (ia ^ ua) : (ia + ua);
+        ib += ub;
+        im = um > im ? um : im;
+      }
+    }
+    if (i < fp.y) {
+      R[i].a = d.mode == M_XORZ ? (carry_a ^ ia ^ r.a) : (carry_a + ia - r.a);
+      R[i].b = carry_b + ib - r.b;
+    }
+    carry_a = d.mode == M_XORZ ? (carry_a ^ __shfl_sync(0xffffffffu, ia, 31)) : (carry_a + __shfl_sync(0xffffffffu, ia, 31));
+    carry_b += __shfl_sync(0xffffffffu, ib, 31);
+    int64_t bm = __shfl_sync(0xffffffffu, im, 31);
+    last = bm > last ? bm : last;
+    flag |= warp_or_u32(r.flag);
+  }
+  if (l != 0) return;
+  uint32_t e = E_OK;
+  if (d.mode == M_RLE) {  // rle.rs:58-71 (sums saturate at n + 1)
+    if (carry_a > n) e = E_CORRUPT;
+    else if (carry_a != n) e = E_LENGTH_MISMATCH;
+  } else if (d.mode == M_XORZ) {  // xorz.rs:18-32 read sequentially
+    if (n == 0) e = d.plen ? E_CORRUPT : E_OK;
+    else if (carry_b < n) e = flag ? E_CORRUPT : ((d.plen - (uint64_t)(last + 1) >= 10) ? E_CORRUPT : E_TRUNCATED);
+  }
+  if (e) {
+    aux[f].err = e;
+    atomicMin(err, ((unsigned long long)f << 8) | e);
+  }
+}
+
+// Main items: one warp per item.
+__global__ void __launch_bounds__(kItemWarps * 32) k_decode_items(const uint8_t* __restrict__ stream,
+                                                                const FrameDesc* __restrict__ frames,
+                                                                int dtype, const FrameAux* __restrict__ aux,
+                                                                const ItemRef* __restrict__ items, uint32_t nitems,
+                                                                const uint2* __restrict__ frame_pre,
+                                                                const PreRec* __restrict__ pre, DecodeOut O,
+                                                                const uint64_t* __restrict__ scratch,
+                                                                unsigned long long* __restrict__ err) {
+  __shared__ __align__(16) uint64_t stage_all[kItemWarps][kItemStage];
+  int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+  uint32_t g = blockIdx.x * kItemWarps + warp;
+  if (g >= nitems) return;
+  ItemRef it = items[g];
+  const FrameAux& A = aux[it.frame];
+  if (A.err) return;
+  FrameDesc d = frames[it.frame];
+  const uint8_t* p = stream + d.payload_off;
+  uint64_t n = d.n;
+  uint64_t* stg = stage_all[warp];
+  uint32_t e = E_OK;
+  switch (d.mode) {
+    case M_RAW: case M_CONST: case M_STRIDE: {
+      uint64_t i0 = (uint64_t)it.local * kItemVals;
+      uint32_t cnt = (uint32_t)qmin(kItemVals, n - i0);
+      uint64_t c0 = d.value_off + i0;
+      if (d.mode == M_CONST) {
+        uint64_t v = ld_u64(p);
+        warp_store_any(O, c0, cnt, [&](uint32_t) { return v; });
+      } else if (d.mode == M_STRIDE) {
+        uint64_t first = ld_u64(p), stride = ld_u64(p + 8);
+        warp_store_any(O, c0, cnt, [&](uint32_t q) { return first + (i0 + q) * stride; });
+      } else if (dtype == DT_F32) {
+        warp_store_any(O, c0, cnt, [&](uint32_t q) { return f32bits_to_f64bits(ld_u32(p + 4 * (i0 + q))); });
+      } else if (lane_bytes(dtype) == 4) {
+        warp_store_any(O, c0, cnt, [&](uint32_t q) { return (uint64_t)ld_u32(p + 4 * (i0 + q)); });
+      } else {
+        warp_store_any(O, c0, cnt, [&](uint32_t q) { return ld_u64(p + 8 * (i0 + q)); });
+      }
+      break;
+    }
+    case M_FOR_BITPACK: case M_FLOAT_MULT: case M_DELTA_BITPACK: {
+      uint32_t k = it.local >> 1, h = it.local & 1;
+      uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+      uint32_t hb = h * kItemVals, hc = cnt > hb ? min((uint32_t)kItemVals, cnt - hb) : 0u;
+      if (d.mode == M_FLOAT_MULT) {
+        double scale = kFmScales[A.a];
+        warp_unpack_half(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t v) {
+          stg[skew(i - hb)] = f64_bits(__ddiv_rn(__ll2double_rn((long long)v), scale));
+        });
+      } else if (d.mode == M_DELTA_BITPACK) {
+        warp_unpack_half(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t v) { stg[skew(i - hb)] = unzigzag64(v); });
+      } else {
+        warp_unpack_half(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t v) { stg[skew(i - hb)] = v; });
+      }
+      __syncwarp();
+      if (d.mode == M_DELTA_BITPACK) warp_prefix_skewed(stg, hc, pre[frame_pre[it.frame].x + it.local].a);
+      warp_store_any(O, d.value_off + (uint64_t)k * kSub + hb, hc, [&](uint32_t q) { return stg[skew(q)]; });
+      break;
+    }
+    case M_ALP: {
+      uint32_t k = it.local >> 1, h = it.local & 1;
+      uint32_t off = A.offs[0][k];
+      int ee = p[off], ff = p[off + 1];
+      uint32_t exc = ld_u16(p + off + 2);
+      int64_t mn = (int64_t)ld_u64(p + off + 4);
+      uint32_t w = p[off + 12];
+      uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+      uint32_t hb = h * kItemVals, hc = cnt > hb ? min((uint32_t)kItemVals, cnt - hb) : 0u;
+      const uint8_t* words = p + off + 13;
+      if (w == 0) {
+        uint64_t v = f64_bits(alp_decode_value(mn, ee, ff));
+        for (uint32_t q = l; q < hc; q += 32) stg[skew(q)] = v;
+      } else {
+        uint32_t mask = w == 32 ? 0xFFFFFFFFu : ((1u << w) - 1u);
+        for (uint32_t r = h * 16; r < h * 16 + 16; r++) {
+          uint32_t idx = r * 32 + l;
+          uint32_t bit = r * w, word = bit >> 5, sh = bit & 31;
+          uint32_t v = ld_u32(words + 4u * (word * 32u + l)) >> sh;
+          if (sh + w > 32) v |= ld_u32(words + 4u * ((word + 1) * 32u + l)) << (32 - sh);
+          v &= mask;
+          if (idx < cnt) stg[skew(idx - hb)] = f64_bits(alp_decode_value((int64_t)((uint64_t)mn + v), ee, ff));
+        }
+      }
+      __syncwarp();
+      if (exc && l == 0) {  // in order, so a repeated position keeps the last exception
+        const uint8_t* xp = words + 128u * w;
+        for (uint32_t x = 0; x < exc; x++) {
+          uint32_t pos = ld_u16(xp + 10 * x);
+          if (pos >= hb && pos < hb + kItemVals) stg[skew(pos - hb)] = ld_u64(xp + 10 * x + 2);
+        }
+      }
+      __syncwarp();
+      warp_store_any(O, d.value_off + (uint64_t)k * kSub + hb, hc, [&](uint32_t q) { return stg[skew(q)]; });
+      break;
+    }
+    case M_ALP_RD: {  // frames without exceptions only
+      uint32_t k = it.local >> 1, h = it.local & 1;
+      uint32_t lbw = (uint32_t)A.a, dsz = (uint32_t)A.b, rbw = 64 - lbw;
+      uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+      uint32_t hb = h * kItemVals, hc = cnt > hb ? min((uint32_t)kItemVals, cnt - hb) : 0u;
+      uint32_t bad = 0;
+      warp_unpack_half(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t c) { stg[skew(i - hb)] = c; });
+      __syncwarp();
+      warp_unpack_half(p, A.offs[1][k], h, cnt, [&](uint32_t i, uint64_t r) {
+        uint64_t c = stg[skew(i - hb)];
+        if (c >= dsz) bad = 1;
+        else stg[skew(i - hb)] = (A.dict8[c] << rbw) | r;
+      });
+      __syncwarp();
+      if (warp_or_u32(bad)) {
+        e = E_CORRUPT;
+        break;
+      }
+      warp_store_any(O, d.value_off + (uint64_t)k * kSub + hb, hc, [&](uint32_t q) { return stg[skew(q)]; });
+      break;
+    }
+    case M_RLE: {
+      uint64_t nr = A.a;
+      const uint8_t* rv = p + A.b;
+      uint32_t nrs = (uint32_t)((nr + kSub - 1) / kSub);
+      const PreRec* R = pre + frame_pre[it.frame].x;  // .a = first value of each run chunk
+      const uint32_t* ends = reinterpret_cast<const uint32_t*>(scratch + d.value_off);  // chunk-local run ends
+      uint64_t lo = (uint64_t)it.local * kItemVals, hi = qmin(lo + kItemVals, n);
+      uint32_t kc = 0;  // last chunk starting at or before lo
+      for (uint32_t b = 0; b < nrs; b += 32) {
+        bool ok = b + l < nrs && R[b + l].a <= lo;
+        uint32_t m = __ballot_sync(0xffffffffu, ok);
+        if (m) kc = b + 31 - __clz(m);
+        if (m != 0xffffffffu) break;
+      }
+      uint64_t cs = R[kc].a;
+      uint32_t ck = (uint32_t)qmin(kSub, nr - (uint64_t)kc * kSub);
+      uint32_t a = 0, bb = ck;  // first run of the chunk ending after lo
+      while (a < bb) {
+        uint32_t mid = (a + bb) >> 1;
+        if (cs + ends[(uint64_t)kc * kSub + mid] > lo) bb = mid; else a = mid + 1;
+      }
+      uint64_t rc = (uint64_t)kc * kSub + a;
+      warp_store_any(O, d.value_off + lo, (uint32_t)(hi - lo), [&](uint32_t q) {
+        uint64_t i = lo + q;
+        while (cs + ends[rc] <= i) {
+          rc++;
+          if ((rc & (kSub - 1)) == 0) cs = R[rc / kSub].a;
+        }
+        return ld_u64(rv + 8ull * rc);
+      });
+      break;
+    }
+    case M_XORZ: {
+      const PreRec& R = pre[frame_pre[it.frame].x + it.local];
+      uint64_t vbase = R.b;
+      XSlice X = xorz_lane_scan(p, d.plen, (uint64_t)it.local * kItemBytes);
+      uint64_t inc = X.xo;  // contributions of the lanes before, then the lane's bytes
+      for (int o = 1; o < 32; o <<= 1) {
+        uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (l >= o) inc ^= u;
+      }
+      xorz_lane_bytes<true>(X, R.a ^ inc ^ X.xo, stg, 0);
+      __syncwarp();
+      // checks on the values that exist (index < n): length, and the n-th
+      // value's terminator must be the payload's last byte
+      uint32_t bad = 0;
+      uint64_t lane0 = vbase + X.before;
+      if (X.first_bad != ~0u && lane0 + X.first_bad < n) bad = 1;
+      if (n && lane0 <= n - 1 && n - 1 < lane0 + X.cnt) {
+        uint32_t m = X.tm;
+        for (uint64_t q = n - 1 - lane0; q; q--) m &= m - 1u;
+        if ((int64_t)(X.b0 + (uint64_t)(__ffs(m) - 1)) != (int64_t)d.plen - 1) bad = 1;
+      }
+      if (warp_or_u32(bad)) {
+        e = E_CORRUPT;
+        break;
+      }
+      if (vbase < n) {
+        uint32_t cnt = (uint32_t)qmin((uint64_t)X.total, n - vbase);
+        warp_store_any(O, d.value_off + vbase, cnt, [&](uint32_t q) { return stg[skew(q)]; });
+      }
+      break;
+    }
+    default:
+      e = E_UNSUPPORTED;
+      break;
+  }
+  if (e && l == 0) atomicMin(err, ((unsigned long long)it.frame << 8) | e);
+}
+
 // ---------------------------------------------------------------------------
 // Validity ranks and the final typed write.
 // ---------------------------------------------------------------------------
@@ -981,9 +1565,44 @@ void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf
   FrameAux* A = reinterpret_cast<FrameAux*>(aux);
   k_walk_frames<<<(nf + 127) / 128, 128, 0, st>>>(stream, frames, nf, dtype, A, err);
   cudaFuncSetAttribute(k_decode_frames, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecSmem));
-  k_decode_frames<<<nf, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, nf, dtype, A, out, scratch, err);
+  k_decode_frames<<<nf, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, nf, dtype, A, out, scratch, err, nullptr);
   count_launches(2);
 }
+
+void launch_decode_items(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
+                         const ItemPlan& plan, void* pre, uint64_t* scratch, void* aux, unsigned long long* err,
+                         cudaStream_t st) {
+  if (nf <= 0) return;
+  FrameAux* A = reinterpret_cast<FrameAux*>(aux);
+  PreRec* P = reinterpret_cast<PreRec*>(pre);
+  k_walk_frames<<<(nf + 127) / 128, 128, 0, st>>>(stream, frames, nf, dtype, A, err);
+  int launches = 1;
+  if (plan.npre) {
+    k_prepass<<<(plan.npre + kItemWarps - 1) / kItemWarps, kItemWarps * 32, 0, st>>>(stream, frames, A,
+                                                                                   plan.pre_items, plan.npre, P,
+                                                                                   scratch);
+    launches++;
+  }
+  if (plan.need_scan) {
+    k_prepass_scan<<<(nf + kItemWarps - 1) / kItemWarps, kItemWarps * 32, 0, st>>>(stream, frames, nf, A,
+                                                                                 plan.frame_pre, P, err);
+    launches++;
+  }
+  if (plan.nmain) {
+    k_decode_items<<<(plan.nmain + kItemWarps - 1) / kItemWarps, kItemWarps * 32, 0, st>>>(
+        stream, frames, dtype, A, plan.main_items, plan.nmain, plan.frame_pre, P, out, scratch, err);
+    launches++;
+  }
+  if (plan.nlist) {
+    cudaFuncSetAttribute(k_decode_frames, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecSmem));
+    k_decode_frames<<<plan.nlist, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, (int)plan.nlist, dtype, A, out,
+                                                                       scratch, err, plan.list);
+    launches++;
+  }
+  count_launches(launches);
+}
+
+uint64_t prepass_rec_bytes() { return sizeof(PreRec); }
 
 void launch_select_table(const uint8_t* bm, uint64_t n, const uint64_t* word_rank, uint64_t nvalid, uint64_t* sel,
                          cudaStream_t st) {

@@ -195,7 +195,7 @@ inline int plain_code(int ext) {
 enum Slot {
   S_IN, S_BM, S_RANK, S_LANE, S_GROW, S_FRAMES, S_NB, S_SIZES, S_TILE, S_SCRATCH, S_OUT, S_VTMP, S_VBLOB,
   S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_DAUX, S_SUBST, S_FMST,
-  S_SMP16, S_WINBITS, S_DSEL, S_COUNT
+  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_COUNT
 };
 
 struct QuoinCtx {
@@ -561,7 +561,14 @@ struct LaneIdx {
   std::vector<FrameDesc> frames;
   bool any_dict = false;  // frames that need the decode scratch range (DICT, RLE, ALP-RD)
   bool aligned = true;    // every frame but the last holds a multiple of 1024 values
-  uint64_t frame_base = 0;  // index of the first frame in the device table
+  uint64_t frame_base = 0;
+  // warp-item decode tables (launch_decode_items) and their offsets in the
+  // index-wide device table
+  std::vector<ItemRef> pre_items, main_items;
+  std::vector<uint2> frame_pre;
+  std::vector<uint32_t> list;
+  bool need_scan = false;
+  uint64_t main_base = 0, pre_base = 0, fp_base = 0, list_base = 0;  // index of the first frame in the device table
 };
 
 // Reference validity.rs:73-119.
@@ -655,6 +662,89 @@ int parse_lane(const uint8_t* src, uint64_t base, uint64_t len, LaneIdx& L) {
   return K_OK;
 }
 
+// Warp items of every frame (512 values, or 512 payload bytes for XORZ).
+// Frames the items do not cover, or whose header cannot be read here, go to
+// the frame list; the device walk reports their errors.
+void build_items(const uint8_t* src, LaneIdx& L) {
+  const uint32_t V = 512, B = 512;
+  for (uint32_t f = 0; f < (uint32_t)L.frames.size(); f++) {
+    const FrameDesc& d = L.frames[f];
+    const uint8_t* p = src + d.payload_off;
+    uint64_t n = d.n, plen = d.plen;
+    uint32_t pre0 = (uint32_t)L.pre_items.size();
+    uint32_t nv = (uint32_t)((n + V - 1) / V);
+    auto add_main = [&](uint32_t cnt) {
+      for (uint32_t j = 0; j < cnt; j++) L.main_items.push_back(ItemRef{f, j});
+    };
+    auto add_pre = [&](uint32_t cnt) {
+      for (uint32_t j = 0; j < cnt; j++) L.pre_items.push_back(ItemRef{f, j});
+    };
+    switch (d.mode) {
+      case 5: case 1: case 2: case 50: case 17: case 9:  // RAW CONST STRIDE FOR FLOAT_MULT ALP
+        add_main(nv);
+        break;
+      case 51:  // DELTA
+        add_pre(nv);
+        add_main(nv);
+        L.need_scan = true;
+        break;
+      case 3: {  // XORZ
+        uint32_t nb = (uint32_t)((plen + B - 1) / B);
+        add_pre(nb);
+        add_main(nb);
+        L.need_scan = true;
+        break;
+      }
+      case 53: {  // RLE: varint(nruns) first
+        uint64_t pos = 0, nr = 0;
+        if (rd_varint_h(p, plen, &pos, &nr) != K_OK || nr > n) {
+          L.list.push_back(f);
+          break;
+        }
+        add_pre((uint32_t)((nr + 1023) / 1024));
+        add_main(nv);
+        L.need_scan = true;
+        break;
+      }
+      case 52: {  // ALP-RD: items only without exceptions
+        uint64_t nexc = 1;
+        if (plen >= 2 && p[1] <= 8) {
+          uint64_t pos = 2 + 8ull * p[1];
+          if (pos > plen || rd_varint_h(p, plen, &pos, &nexc) != K_OK) nexc = 1;
+        }
+        if (nexc == 0) add_main(nv);
+        else L.list.push_back(f);
+        break;
+      }
+      default:
+        L.list.push_back(f);
+        break;
+    }
+    L.frame_pre.push_back(make_uint2(pre0, (uint32_t)L.pre_items.size() - pre0));
+  }
+}
+
+// Bytes of the index-wide item table; assigns each lane's offsets.
+uint64_t layout_items(std::vector<LaneIdx>& lanes) {
+  uint64_t m = 0, pr = 0, fp = 0, li = 0;
+  for (auto& L : lanes) {
+    L.main_base = m;
+    L.pre_base = pr;
+    L.fp_base = fp;
+    L.list_base = li;
+    m += L.main_items.size();
+    pr += L.pre_items.size();
+    fp += L.frame_pre.size();
+    li += L.list.size();
+  }
+  for (auto& L : lanes) {
+    L.pre_base += m;
+    L.fp_base = m + pr + L.fp_base;
+    L.list_base = m + pr + fp + L.list_base;
+  }
+  return (m + pr + fp + li) * 8 + 64;  // ItemRef / uint2 are 8 bytes, list entries padded to 8
+}
+
 }  // namespace
 
 struct QuoinDecodeIndex {
@@ -676,12 +766,28 @@ struct QuoinDecodeIndex {
   uint64_t* d_rank = nullptr;
   uint64_t* d_sel = nullptr;
   uint64_t* d_vmin = nullptr;
+  uint64_t* d_items = nullptr;  // item tables of every lane (layout_items)
+  uint64_t items_bytes = 0;
+  uint64_t max_pre = 0;
 };
 
 namespace {
 
-// Reference lib.rs:462-490 + decimal.rs:100-168: parse a whole stream.
+int parse_stream_lanes(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X);
+
+// Reference lib.rs:462-490 + decimal.rs:100-168: parse a whole stream, then lay
+// out the warp-item tables of its lanes.
 int parse_stream(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
+  int k = parse_stream_lanes(src, len, X);
+  if (k) return k;
+  X.items_bytes = layout_items(X.lanes);
+  X.max_pre = 0;
+  for (auto& L : X.lanes) X.max_pre = L.pre_items.size() > X.max_pre ? L.pre_items.size() : X.max_pre;
+  return K_OK;
+}
+
+// The header, validity and frame tables of the stream's lane(s).
+int parse_stream_lanes(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
   if (len > 5 && (src[5] & 2)) {  // decimal container (decimal.rs:39-41)
     if (len < 8) return K_TRUNC;
     if (src[7] > 7) return K_DTYPE;
@@ -720,6 +826,7 @@ int parse_stream(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
       LaneIdx L;
       r = parse_lane(src, pos, sl, L);
       if (r) return r;
+      build_items(src, L);
       if (L.logical_n != X.n_valid) return K_CORRUPT;
       X.lanes.push_back(std::move(L));
       pos += sl;
@@ -733,6 +840,7 @@ int parse_stream(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
   LaneIdx L;
   int r = parse_lane(src, 0, len, L);
   if (r) return r;
+  build_items(src, L);
   if (L.dtype == WT_DEC128 || L.dtype == WT_DEC256) return K_CORRUPT;  // lib.rs:503-505
   X.wire = L.dtype;
   X.n = L.logical_n;
@@ -757,7 +865,7 @@ uint64_t sel_bytes(const QuoinDecodeIndex& X) {
 }
 
 int upload_index(QuoinCtx* c, cudaStream_t st, QuoinDecodeIndex& X, FrameDesc* dfr, uint8_t* dbm, uint64_t* drank,
-                 uint64_t* dsel, uint64_t* dvmin) {
+                 uint64_t* dsel, uint64_t* dvmin, uint64_t* ditems) {
   uint64_t fb = 0;
   for (auto& L : X.lanes) {
     L.frame_base = fb;
@@ -765,6 +873,14 @@ int upload_index(QuoinCtx* c, cudaStream_t st, QuoinDecodeIndex& X, FrameDesc* d
       CK(cudaMemcpyAsync(dfr + fb, L.frames.data(), L.frames.size() * sizeof(FrameDesc), cudaMemcpyHostToDevice, st));
     fb += L.frames.size();
   }
+  std::vector<uint64_t> tab(X.items_bytes / 8, 0);
+  for (auto& L : X.lanes) {
+    if (!L.main_items.empty()) memcpy(tab.data() + L.main_base, L.main_items.data(), L.main_items.size() * 8);
+    if (!L.pre_items.empty()) memcpy(tab.data() + L.pre_base, L.pre_items.data(), L.pre_items.size() * 8);
+    if (!L.frame_pre.empty()) memcpy(tab.data() + L.fp_base, L.frame_pre.data(), L.frame_pre.size() * 8);
+    if (!L.list.empty()) memcpy(tab.data() + L.list_base, L.list.data(), L.list.size() * 4);
+  }
+  if (!tab.empty()) CK(cudaMemcpyAsync(ditems, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, st));
   if (X.has_validity && X.n) {
     uint64_t nw = (X.n + 31) / 32;
     CK(cudaMemcpyAsync(dbm, X.bitmap.data(), X.bitmap.size(), cudaMemcpyHostToDevice, st));
@@ -779,9 +895,22 @@ int upload_index(QuoinCtx* c, cudaStream_t st, QuoinDecodeIndex& X, FrameDesc* d
 }
 
 // Decode the lanes of an uploaded index from the device stream d_src.
+ItemPlan lane_plan(const LaneIdx& L, const uint64_t* ditems) {
+  ItemPlan P;
+  P.main_items = reinterpret_cast<const ItemRef*>(ditems + L.main_base);
+  P.nmain = (uint32_t)L.main_items.size();
+  P.pre_items = reinterpret_cast<const ItemRef*>(ditems + L.pre_base);
+  P.npre = (uint32_t)L.pre_items.size();
+  P.frame_pre = reinterpret_cast<const uint2*>(ditems + L.fp_base);
+  P.list = reinterpret_cast<const uint32_t*>(ditems + L.list_base);
+  P.nlist = (uint32_t)L.list.size();
+  P.need_scan = L.need_scan;
+  return P;
+}
+
 int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, const FrameDesc* dfr, const uint8_t* dbm,
-                   const uint64_t* drank, const uint64_t* dsel, const uint64_t* dvmin, const uint8_t* d_src,
-                   void* d_out, uint8_t* d_valid_out) {
+                   const uint64_t* drank, const uint64_t* dsel, const uint64_t* dvmin, const uint64_t* ditems,
+                   const uint8_t* d_src, void* d_out, uint8_t* d_valid_out) {
   CK(c->ensure(S_ERR, 64));
   unsigned long long* d_err = c->p<unsigned long long>(S_ERR);
   CK(cudaMemsetAsync(d_err, 0xFF, 8, st));
@@ -790,6 +919,8 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
   for (auto& L : X.lanes) max_nf = L.frames.size() > max_nf ? L.frames.size() : max_nf;
   CK(c->ensure(S_DAUX, decode_aux_bytes((int)max_nf)));
   void* daux = c->p<void>(S_DAUX);
+  CK(c->ensure(S_PRE, (X.max_pre + 1) * prepass_rec_bytes()));
+  void* dpre = c->p<void>(S_PRE);
   if (!X.decimal) {
     const LaneIdx& L = X.lanes[0];
     uint32_t w = native_width(X.wire);
@@ -806,7 +937,8 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
                   L.n_total};
       {
         TimedRegion tr(T_DECODE, st);
-        launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, scr, daux, d_err, st);
+        launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, lane_plan(L, ditems), dpre,
+                            scr, daux, d_err, st);
       }
       if (L.n_total == 0 && X.n) CK(cudaMemsetAsync(d_out, 0, X.n * w, st));  // all null
     } else {
@@ -815,7 +947,8 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
       DecodeOut O{lane_out, WT_U64, nullptr, nullptr, nullptr, L.n_total, L.n_total};
       {
         TimedRegion tr(T_DECODE, st);
-        launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, scr, daux, d_err, st);
+        launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, lane_plan(L, ditems), dpre,
+                            scr, daux, d_err, st);
       }
       if (X.n) {
         TimedRegion tr(T_FINALIZE, st);
@@ -837,7 +970,8 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
       const LaneIdx& L = X.lanes[k];
       DecodeOut O{limbs + (uint64_t)k * X.n_valid, WT_U64, nullptr, nullptr, nullptr, X.n_valid, X.n_valid};
       TimedRegion tr(T_DECODE, st);
-      launch_decode_frames(d_src, dfr + L.frame_base, (int)L.frames.size(), WT_U64, O, scr, daux, d_err, st);
+      launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), WT_U64, O, lane_plan(L, ditems), dpre, scr,
+                          daux, d_err, st);
     }
     if (X.n) {
       TimedRegion tr(T_FINALIZE, st);
@@ -869,15 +1003,17 @@ int decompress_host(QuoinCtx* c, const uint8_t* src, uint64_t len, void* values_
   CK(c->ensure(S_MISC, 64 * 8));
   uint64_t* dvmin = c->p<uint64_t>(S_MISC) + 32;
   CK(c->ensure(S_DSEL, sel_bytes(*X)));
+  CK(c->ensure(S_DITEMS, X->items_bytes));
   int rc = upload_index(c, st, *X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK),
-                        c->p<uint64_t>(S_DSEL), dvmin);
+                        c->p<uint64_t>(S_DSEL), dvmin, c->p<uint64_t>(S_DITEMS));
   if (rc) return rc;
   CK(c->ensure(S_SRC, len + 64));
   if (len) CK(cudaMemcpyAsync(c->p<uint8_t>(S_SRC), src, len, cudaMemcpyHostToDevice, st));
   uint64_t out_bytes = X->n * native_width(X->wire);
   CK(c->ensure(S_OUTVALS, out_bytes + 64));
   rc = decode_indexed(c, st, *X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK),
-                      c->p<uint64_t>(S_DSEL), dvmin, c->p<uint8_t>(S_SRC), c->p<void>(S_OUTVALS), nullptr);
+                      c->p<uint64_t>(S_DSEL), dvmin, c->p<uint64_t>(S_DITEMS), c->p<uint8_t>(S_SRC),
+                      c->p<void>(S_OUTVALS), nullptr);
   if (rc) return rc;
   if (out_bytes) CK(cudaMemcpyAsync(values_out, c->p<void>(S_OUTVALS), out_bytes, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -1289,13 +1425,14 @@ int quoin_b200_index_create(QuoinCtx* ctx, const uint8_t* src, size_t len, Quoin
               cudaMalloc(&X->d_bm, X->bitmap.size() + 16) == cudaSuccess &&
               cudaMalloc(&X->d_rank, ((X->n + 31) / 32 + 1) * 8) == cudaSuccess &&
               cudaMalloc(&X->d_sel, sel_bytes(*X)) == cudaSuccess &&
+              cudaMalloc(&X->d_items, X->items_bytes) == cudaSuccess &&
               cudaMalloc(&X->d_vmin, 64) == cudaSuccess;
     if (!ok) {
       cudaGetLastError();
       quoin_b200_index_free(X);
       return QUOIN_ERR_CUDA;
     }
-    int rc = upload_index(c, c->stream, *X, X->d_frames, X->d_bm, X->d_rank, X->d_sel, X->d_vmin);
+    int rc = upload_index(c, c->stream, *X, X->d_frames, X->d_bm, X->d_rank, X->d_sel, X->d_vmin, X->d_items);
     if (rc) {
       quoin_b200_index_free(X);
       return rc;
@@ -1315,6 +1452,7 @@ void quoin_b200_index_free(QuoinDecodeIndex* X) {
     if (X->d_bm) cudaFree(X->d_bm);
     if (X->d_rank) cudaFree(X->d_rank);
     if (X->d_sel) cudaFree(X->d_sel);
+    if (X->d_items) cudaFree(X->d_items);
     if (X->d_vmin) cudaFree(X->d_vmin);
   }
   delete X;
@@ -1337,8 +1475,8 @@ int quoin_b200_decompress_indexed_device(QuoinCtx* ctx, const QuoinDecodeIndex* 
     std::lock_guard<std::mutex> l(c->mu);
     DeviceScope ds(c->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-    return decode_indexed(c, st, *X, X->d_frames, X->d_bm, X->d_rank, X->d_sel, X->d_vmin, d_src, d_values_out,
-                          d_validity_out);
+    return decode_indexed(c, st, *X, X->d_frames, X->d_bm, X->d_rank, X->d_sel, X->d_vmin, X->d_items, d_src,
+                          d_values_out, d_validity_out);
   } catch (...) {
     return QUOIN_ERR_PANIC;
   }

@@ -28,6 +28,29 @@ struct DecodeOut {
 };
 void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
                           uint64_t* scratch, void* aux, unsigned long long* err, cudaStream_t st);
+// Warp-item decode of one lane (every item covers at most 512 values or 512
+// XORZ payload bytes).  The host builds the tables from the frame table:
+// pre_items / main_items name (frame, item index within the frame);
+// frame_pre[f] = (first prepass item of frame f, count); list = frames decoded
+// whole by one CTA (DICT, ALP-RD with exceptions, modes outside the items).
+// `pre` holds npre records of prepass_rec_bytes().
+struct ItemRef {
+  uint32_t frame, local;
+};
+struct ItemPlan {
+  const ItemRef* pre_items;
+  uint32_t npre;
+  const ItemRef* main_items;
+  uint32_t nmain;
+  const uint2* frame_pre;
+  const uint32_t* list;
+  uint32_t nlist;
+  bool need_scan;
+};
+uint64_t prepass_rec_bytes();
+void launch_decode_items(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
+                         const ItemPlan& plan, void* pre, uint64_t* scratch, void* aux, unsigned long long* err,
+                         cudaStream_t st);
 // sel[m] = position of the (1024*m)-th valid value, m < ceil(nvalid / 1024).
 void launch_select_table(const uint8_t* bm, uint64_t n, const uint64_t* word_rank, uint64_t nvalid, uint64_t* sel,
                          cudaStream_t st);
