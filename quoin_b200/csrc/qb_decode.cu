@@ -22,6 +22,7 @@ constexpr int kMaxSubs = kMaxBlock / kSub;  // 128
 constexpr int kDictSmem = 2048;
 constexpr int kXorzChunk = kDecThreads * 8;  // payload bytes per XORZ step
 constexpr int kXorzRing = 4096;              // decoded XORZ values awaiting their store
+constexpr uint64_t kSelStep = 512;           // select-table granularity (valid values)
 
 // Per-frame results of the walk (device memory, one per frame).
 struct FrameAux {
@@ -325,10 +326,10 @@ struct DecSmem {
 // of the first value) is written straight to its final place: the lane (u64),
 // or the typed column, narrowed to the native width and scattered through the
 // validity bitmap with nulls as 0 (reference lib.rs:492-506, validity.rs:130-146).
-// With a bitmap, c0 is a multiple of 1024 and c0 + cnt is too, or the end of
-// the lane; the run then owns the positions [sel(c0), sel(c0 + cnt)), where
+// With a bitmap the run owns the positions [sel(c0), sel(c0 + cnt)), where
 // sel(c) is the position of the c-th valid value (0 for c = 0, n at the end),
-// so the nulls between runs are written exactly once.
+// so the nulls between runs are written exactly once.  Every lane of the
+// warp takes part (run_positions is warp-cooperative).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void put_out(const DecodeOut& O, uint64_t pos, uint64_t v) {
   if (O.dtype == DT_I32 || O.dtype == DT_U32) {
@@ -340,51 +341,120 @@ __device__ __forceinline__ void put_out(const DecodeOut& O, uint64_t pos, uint64
   }
 }
 
+// Position of the c-th valid value (c < nvalid): from the 512-granular table,
+// the owning bitmap word is found 32 words at a time.
+__device__ uint64_t warp_select(const DecodeOut& O, uint64_t c) {
+  if (!O.bm32) return c;
+  if (c >= O.nvalid) return O.n;
+  uint64_t s = O.sel[c >> 9];
+  if ((c & 511) == 0) return s;
+  int l = threadIdx.x & 31;
+  uint64_t nw = (O.n + 31) >> 5;
+  uint32_t tail = (uint32_t)(O.n & 31);
+  for (uint64_t w0 = s >> 5; w0 < nw; w0 += 32) {
+    uint64_t w = w0 + l;
+    uint32_t bits = 0;
+    uint64_t r = 0;
+    bool hit = false;
+    if (w < nw) {
+      bits = O.bm32[w];
+      if (w == nw - 1 && tail) bits &= (1u << tail) - 1u;
+      r = O.wrank[w];
+      hit = r <= c && c < r + (uint64_t)__popc(bits);
+    }
+    uint32_t m = __ballot_sync(0xffffffffu, hit);
+    if (m) {
+      int src = __ffs(m) - 1;
+      bits = __shfl_sync(0xffffffffu, bits, src);
+      r = __shfl_sync(0xffffffffu, r, src);
+      for (uint64_t k = c - r; k; k--) bits &= bits - 1u;
+      return ((w0 + (uint64_t)src) << 5) + (uint64_t)(__ffs(bits) - 1);
+    }
+  }
+  return O.n;
+}
+
 __device__ __forceinline__ void run_positions(const DecodeOut& O, uint64_t c0, uint64_t c1, uint64_t* p0,
                                               uint64_t* p1) {
-  *p0 = c0 == 0 ? 0 : O.sel[c0 >> 10];
-  *p1 = c1 >= O.nvalid ? O.n : O.sel[c1 >> 10];
+  *p0 = c0 == 0 ? 0 : warp_select(O, c0);
+  *p1 = c1 >= O.nvalid ? O.n : warp_select(O, c1);
+}
+
+// Output element writers: 0 = u64 lane value, 1 = low 32 bits (i32 / u32),
+// 2 = f64 bits narrowed to f32 (nulls stay 0).
+template <int KIND>
+__device__ __forceinline__ void put_kind(void* base, uint64_t i, uint64_t v) {
+  if (KIND == 0) reinterpret_cast<uint64_t*>(base)[i] = v;
+  else if (KIND == 1) reinterpret_cast<uint32_t*>(base)[i] = (uint32_t)v;
+  else reinterpret_cast<uint32_t*>(base)[i] = v ? f64bits_to_f32bits(v) : 0u;
+}
+__device__ __forceinline__ int out_kind(int dtype) {
+  return (dtype == DT_I32 || dtype == DT_U32) ? 1 : dtype == DT_F32 ? 2 : 0;
 }
 
 // Positions [32*w0, 32*w1) of the run [p0, p1) by one warp, relative ranks
 // counted from `rel` (the number of the run's values before position 32*w0).
-// The bitmap words are fetched 32 at a time, one per lane, and broadcast.
-template <class V>
-__device__ __forceinline__ void warp_store_words(const DecodeOut& O, uint64_t w0, uint64_t w1, uint64_t p0,
-                                                 uint64_t p1, uint32_t rel, V& val) {
+// The bitmap words are fetched 32 at a time, one per lane, and broadcast; the
+// lanes of a word write 32 consecutive positions.
+template <int KIND, class V>
+__device__ __forceinline__ void store_words_k(const DecodeOut& O, uint64_t w0, uint64_t nwords, uint32_t first_in,
+                                              uint32_t last_in, uint32_t rel, V& val) {
   int l = threadIdx.x & 31;
   uint32_t below = (1u << l) - 1u;
-  for (uint64_t wb = w0; wb < w1; wb += 32) {
-    uint32_t mine = wb + l < w1 ? O.bm32[wb + l] : 0u;
-    uint32_t nw = (uint32_t)qmin(32, w1 - wb);
+  uint8_t* ow = reinterpret_cast<uint8_t*>(O.out) + (w0 << 5) * (KIND == 0 ? 8u : 4u);
+  const uint32_t* bw = O.bm32 + w0;
+  for (uint64_t wb = 0; wb < nwords; wb += 32) {
+    uint32_t mine = wb + l < nwords ? bw[wb + l] : 0u;
+    uint32_t nw = (uint32_t)qmin(32, nwords - wb);
     for (uint32_t j = 0; j < nw; j++) {
-      uint32_t bits = __shfl_sync(0xffffffffu, mine, j);
-      uint64_t base = (wb + j) << 5;
-      if (bits == 0xFFFFFFFFu && base >= p0 && base + 32 <= p1) {  // 32 valid values in a row
-        put_out(O, base + l, val(rel + (uint32_t)l));
-        rel += 32;
-        continue;
-      }
-      uint32_t in = 0xFFFFFFFFu;  // positions of this word inside [p0, p1)
-      if (base < p0) in &= 0xFFFFFFFFu << (uint32_t)(p0 - base);
-      if (base + 32 > p1) in &= 0xFFFFFFFFu >> (uint32_t)(base + 32 - p1);
-      bits &= in;
+      uint32_t in = (wb + j == 0 ? first_in : 0xFFFFFFFFu) & (wb + j + 1 == nwords ? last_in : 0xFFFFFFFFu);
+      uint32_t bits = __shfl_sync(0xffffffffu, mine, j) & in;
       if ((in >> l) & 1u) {
         uint64_t v = 0;
         if ((bits >> l) & 1u) v = val(rel + __popc(bits & below));
-        put_out(O, base + l, v);
+        put_kind<KIND>(ow, (uint64_t)l, v);
       }
       rel += __popc(bits);
+      ow += 32u * (KIND == 0 ? 8u : 4u);
     }
+  }
+}
+
+template <class V>
+__device__ __forceinline__ void warp_store_words(const DecodeOut& O, uint64_t w0, uint64_t w1, uint64_t p0,
+                                                 uint64_t p1, uint32_t rel, V& val) {
+  uint64_t lo = w0 << 5, hi = w1 << 5;
+  uint32_t first_in = p0 > lo ? (0xFFFFFFFFu << (uint32_t)(p0 - lo)) : 0xFFFFFFFFu;
+  uint32_t last_in = p1 < hi ? (0xFFFFFFFFu >> (uint32_t)(hi - p1)) : 0xFFFFFFFFu;
+  switch (out_kind(O.dtype)) {
+    case 1: store_words_k<1>(O, w0, w1 - w0, first_in, last_in, rel, val); break;
+    case 2: store_words_k<2>(O, w0, w1 - w0, first_in, last_in, rel, val); break;
+    default: store_words_k<0>(O, w0, w1 - w0, first_in, last_in, rel, val); break;
+  }
+}
+
+// Lanes store values c0 .. c0+cnt-1 of a run without a bitmap.
+template <class V>
+__device__ __forceinline__ void warp_store_dense(const DecodeOut& O, uint64_t c0, uint32_t cnt, V& val) {
+  int l = threadIdx.x & 31;
+  switch (out_kind(O.dtype)) {
+    case 1:
+      for (uint32_t q = l; q < cnt; q += 32) put_kind<1>(O.out, c0 + q, val(q));
+      break;
+    case 2:
+      for (uint32_t q = l; q < cnt; q += 32) put_kind<2>(O.out, c0 + q, val(q));
+      break;
+    default:
+      for (uint32_t q = l; q < cnt; q += 32) put_kind<0>(O.out, c0 + q, val(q));
+      break;
   }
 }
 
 // One warp stores one run; val(q) is called with increasing q per lane.
 template <class V>
 __device__ void warp_store(const DecodeOut& O, uint64_t c0, uint32_t cnt, V val) {
-  int l = threadIdx.x & 31;
   if (!O.bm32) {
-    for (uint32_t q = l; q < cnt; q += 32) put_out(O, c0 + q, val(q));
+    warp_store_dense(O, c0, cnt, val);
     return;
   }
   uint64_t p0, p1;
@@ -946,50 +1016,17 @@ __device__ inline void warp_unpack_half(const uint8_t* p, uint32_t off, uint32_t
   }
 }
 
-// Position of the c-th valid value (c < nvalid): from the 1024-granular table,
-// the owning bitmap word is found 32 words at a time.
-__device__ uint64_t warp_select(const DecodeOut& O, uint64_t c) {
-  if (!O.bm32) return c;
-  if (c >= O.nvalid) return O.n;
-  uint64_t s = O.sel[c >> 10];
-  if ((c & 1023) == 0) return s;
-  int l = threadIdx.x & 31;
-  uint64_t nw = (O.n + 31) >> 5;
-  uint32_t tail = (uint32_t)(O.n & 31);
-  for (uint64_t w0 = s >> 5; w0 < nw; w0 += 32) {
-    uint64_t w = w0 + l;
-    uint32_t bits = 0;
-    uint64_t r = 0;
-    bool hit = false;
-    if (w < nw) {
-      bits = O.bm32[w];
-      if (w == nw - 1 && tail) bits &= (1u << tail) - 1u;
-      r = O.wrank[w];
-      hit = r <= c && c < r + (uint64_t)__popc(bits);
-    }
-    uint32_t m = __ballot_sync(0xffffffffu, hit);
-    if (m) {
-      int src = __ffs(m) - 1;
-      bits = __shfl_sync(0xffffffffu, bits, src);
-      r = __shfl_sync(0xffffffffu, r, src);
-      for (uint64_t k = c - r; k; k--) bits &= bits - 1u;
-      return ((w0 + (uint64_t)src) << 5) + (uint64_t)(__ffs(bits) - 1);
-    }
-  }
-  return O.n;
-}
-
 // Store the run [c0, c0 + cnt) of lane values (any c0): it owns the positions
 // from the c0-th valid value (0 for c0 = 0) to the (c0+cnt)-th (n at the end).
 template <class V>
 __device__ void warp_store_any(const DecodeOut& O, uint64_t c0, uint32_t cnt, V val) {
   if (cnt == 0) return;
   if (!O.bm32) {
-    for (uint32_t q = threadIdx.x & 31; q < cnt; q += 32) put_out(O, c0 + q, val(q));
+    warp_store_dense(O, c0, cnt, val);
     return;
   }
-  uint64_t p0 = c0 == 0 ? 0 : warp_select(O, c0);
-  uint64_t p1 = c0 + cnt >= O.nvalid ? O.n : warp_select(O, c0 + cnt);
+  uint64_t p0, p1;
+  run_positions(O, c0, c0 + cnt, &p0, &p1);
   if (p1 > p0) warp_store_words(O, p0 >> 5, (p1 + 31) >> 5, p0, p1, 0u, val);
 }
 
@@ -1397,15 +1434,29 @@ __global__ void __launch_bounds__(kItemWarps * 32) k_decode_items(const uint8_t*
         uint32_t mid = (a + bb) >> 1;
         if (cs + ends[(uint64_t)kc * kSub + mid] > lo) bb = mid; else a = mid + 1;
       }
-      uint64_t rc = (uint64_t)kc * kSub + a;
-      warp_store_any(O, d.value_off + lo, (uint32_t)(hi - lo), [&](uint32_t q) {
-        uint64_t i = lo + q;
-        while (cs + ends[rc] <= i) {
-          rc++;
-          if ((rc & (kSub - 1)) == 0) cs = R[rc / kSub].a;
+      // expand the runs overlapping [lo, hi) into the staging buffer, one run
+      // per lane at a time, then store
+      uint64_t r = (uint64_t)kc * kSub + a;  // first run ending after lo
+      for (;;) {
+        uint64_t rr = r + (uint64_t)l;
+        uint64_t st = hi, en = hi;
+        if (rr < nr) {
+          uint64_t kk = rr / kSub;
+          uint64_t cbase = R[kk].a;
+          en = cbase + ends[rr];
+          st = (rr % kSub) ? cbase + ends[rr - 1] : cbase;
+          if (st < lo) st = lo;
+          if (en > hi) en = hi;
+          uint64_t v = ld_u64(rv + 8ull * rr);
+          for (uint64_t i = st; i < en; i++) stg[skew((uint32_t)(i - lo))] = v;
         }
-        return ld_u64(rv + 8ull * rc);
-      });
+        // stop once a lane's run reached hi (runs are in order)
+        bool done = rr >= nr || en >= hi;
+        if (__ballot_sync(0xffffffffu, done)) break;
+        r += 32;
+      }
+      __syncwarp();
+      warp_store_any(O, d.value_off + lo, (uint32_t)(hi - lo), [&](uint32_t q) { return stg[skew(q)]; });
       break;
     }
     case M_XORZ: {
@@ -1464,7 +1515,7 @@ __global__ void k_word_popcount(const uint8_t* __restrict__ bm, uint64_t n, uint
   }
 }
 
-// sel[m] = position of the (1024*m)-th valid value: the owner of every 1024th
+// sel[m] = position of the (512*m)-th valid value: the owner of every 512th
 // rank is the one bitmap word whose rank range contains it.
 __global__ void k_select_table(const uint8_t* __restrict__ bm, uint64_t n, const uint64_t* __restrict__ word_rank,
                                uint64_t nvalid, uint64_t* __restrict__ sel) {
@@ -1476,10 +1527,10 @@ __global__ void k_select_table(const uint8_t* __restrict__ bm, uint64_t n, const
     uint64_t rem = n - w * 32;
     if (rem < 32) bits &= (1u << rem) - 1u;
     uint64_t r = word_rank[w], c = (uint64_t)__popc(bits);
-    uint64_t m = (r + kSub - 1) / kSub * kSub;
+    uint64_t m = (r + kSelStep - 1) / kSelStep * kSelStep;
     if (m < r + c && m < nvalid) {
       for (uint64_t k = m - r; k; k--) bits &= bits - 1u;  // drop the lower set bits
-      sel[m / kSub] = w * 32 + (uint64_t)(__ffs(bits) - 1);
+      sel[m / kSelStep] = w * 32 + (uint64_t)(__ffs(bits) - 1);
     }
   }
 }

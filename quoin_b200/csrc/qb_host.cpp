@@ -560,7 +560,6 @@ struct LaneIdx {
   std::vector<uint8_t> bitmap;  // ceil(n/8), trailing bits cleared
   std::vector<FrameDesc> frames;
   bool any_dict = false;  // frames that need the decode scratch range (DICT, RLE, ALP-RD)
-  bool aligned = true;    // every frame but the last holds a multiple of 1024 values
   uint64_t frame_base = 0;
   // warp-item decode tables (launch_decode_items) and their offsets in the
   // index-wide device table
@@ -654,7 +653,6 @@ int parse_lane(const uint8_t* src, uint64_t base, uint64_t len, LaneIdx& L) {
     f.aux = 0;
     L.frames.push_back(f);
     if (mode == 19 || mode == 53 || mode == 52) L.any_dict = true;
-    if (!L.frames.empty() && (L.frames.back().value_off % 1024) != 0) L.aligned = false;
     pos += plen;
     counted += fn;
     if (counted > L.n_total) return K_CORRUPT;
@@ -861,7 +859,7 @@ uint64_t total_frames(const QuoinDecodeIndex& X) {
 // compute the validity word ranks on the device.
 uint64_t sel_bytes(const QuoinDecodeIndex& X) {
   uint64_t nv = X.decimal || X.lanes.empty() ? 0 : X.lanes[0].n_total;
-  return (nv / 1024 + 2) * 8;
+  return (nv / 512 + 2) * 8;
 }
 
 int upload_index(QuoinCtx* c, cudaStream_t st, QuoinDecodeIndex& X, FrameDesc* dfr, uint8_t* dbm, uint64_t* drank,
@@ -931,7 +929,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
     }
     // Fused: decoded values go straight to the typed column (narrowed, and
     // scattered through the bitmap when there is one).
-    bool fused = (!X.has_validity || L.aligned) && ((uintptr_t)d_out % w) == 0;
+    bool fused = ((uintptr_t)d_out % w) == 0;
     if (fused) {
       DecodeOut O{d_out, X.wire, X.has_validity ? reinterpret_cast<const uint32_t*>(dbm) : nullptr, drank, dsel, X.n,
                   L.n_total};

@@ -16,7 +16,6 @@ uint64_t decode_aux_bytes(int nf);
 // dtype DT_U64) or the typed column (narrowed to dtype's native width and,
 // with bm32, scattered through the validity words with nulls as 0; wrank =
 // exclusive popcount prefix per 32-bit word, sel from launch_select_table).
-// With a bitmap every frame but the last must hold a multiple of 1024 values.
 struct DecodeOut {
   void* out;
   int dtype;
@@ -51,7 +50,7 @@ uint64_t prepass_rec_bytes();
 void launch_decode_items(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
                          const ItemPlan& plan, void* pre, uint64_t* scratch, void* aux, unsigned long long* err,
                          cudaStream_t st);
-// sel[m] = position of the (1024*m)-th valid value, m < ceil(nvalid / 1024).
+// sel[m] = position of the (512*m)-th valid value, m < ceil(nvalid / 512).
 void launch_select_table(const uint8_t* bm, uint64_t n, const uint64_t* word_rank, uint64_t nvalid, uint64_t* sel,
                          cudaStream_t st);
 void launch_word_popcount(const uint8_t* bm, uint64_t n, uint64_t* cnt, cudaStream_t st);
