@@ -653,7 +653,13 @@ __device__ uint64_t* block_radix_sort(EncSmem& S, uint64_t* a, uint64_t* b, uint
   uint32_t* hist = reinterpret_cast<uint32_t*>(S.big.dict.sorted);  // [kEncWarps][256]
   int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   uint64_t k0 = m ? a[0] : 0ull, diff = 0;
-  for (uint32_t i = t; i < m; i += blockDim.x) diff |= a[i] ^ k0;
+  for (uint32_t i0 = t; i0 < m; i0 += blockDim.x * 8) {
+    uint64_t ks[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) ks[q] = i0 + q * blockDim.x < m ? a[i0 + q * blockDim.x] : k0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) diff |= ks[q] ^ k0;
+  }
   diff = warp_or64(diff);
   if (lane == 0) S.red[warp] = diff;
   __syncthreads();
@@ -666,7 +672,14 @@ __device__ uint64_t* block_radix_sort(EncSmem& S, uint64_t* a, uint64_t* b, uint
     if (((diff >> shift) & 0xFFull) == 0) continue;
     for (int i = t; i < kEncWarps * 256; i += blockDim.x) hist[i] = 0;
     __syncthreads();
-    for (uint32_t i = s0 + lane; i < s1; i += 32) atomicAdd(&hist[warp * 256 + (uint32_t)((a[i] >> shift) & 0xFF)], 1u);
+    for (uint32_t i0 = s0 + lane; i0 < s1; i0 += 32 * 8) {
+      uint64_t ks[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) ks[q] = i0 + 32 * q < s1 ? a[i0 + 32 * q] : 0ull;
+#pragma unroll
+      for (int q = 0; q < 8; q++)
+        if (i0 + 32 * q < s1) atomicAdd(&hist[warp * 256 + (uint32_t)((ks[q] >> shift) & 0xFF)], 1u);
+    }
     __syncthreads();
     {  // offsets: digit-major, then warp order (stability)
       uint32_t tot = 0;
@@ -905,6 +918,21 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
       uint32_t iq = base + q * blockDim.x + threadIdx.x;
       xs[q] = iq < n ? v[iq] : 0ull;
     }
+    // first probes of the eight values in flight together, then the CASes
+    uint32_t hs[8];
+    uint64_t cur0[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      hs[q] = (uint32_t)((xs[q] * 0x9E3779B97F4A7C15ull) >> (64 - lg));
+      cur0[q] = base + q * blockDim.x + threadIdx.x < n ? T[hs[q]] : 0ull;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      if (base + q * blockDim.x + threadIdx.x < n && xs[q] != kEmpty64 && cur0[q] == kEmpty64)
+        cur0[q] = atomicCAS((unsigned long long*)&T[hs[q]], kEmpty64, xs[q]);
+      else
+        cur0[q] = cur0[q] == kEmpty64 ? 1ull : cur0[q];  // (not used: 1 never equals kEmpty64)
+    }
 #pragma unroll
     for (int q = 0; q < 8; q++) {
       if (base + q * blockDim.x + threadIdx.x >= n) break;
@@ -913,8 +941,13 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
         if (atomicExch(&S.has_max, 1u) == 0 && atomicAdd(&S.card, 1u) >= max_card) S.flag = 1;
         continue;
       }
-      uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> (64 - lg));
-      for (uint32_t probe = 0; probe < cap; probe++) {
+      if (cur0[q] == kEmpty64) {  // the first-probe CAS inserted x
+        if (atomicAdd(&S.card, 1u) >= max_card) S.flag = 1;
+        continue;
+      }
+      if (cur0[q] == x) continue;
+      uint32_t h = (hs[q] + 1) & (cap - 1);
+      for (uint32_t probe = 1; probe < cap; probe++) {
         uint64_t cur = T[h];
         if (cur == kEmpty64) {
           cur = atomicCAS((unsigned long long*)&T[h], kEmpty64, x);
@@ -939,18 +972,41 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
     return dv;
   }
   uint32_t card = S.card, has_max = S.has_max;
-  for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x)
-    if (T[i] != kEmpty64) A[atomicAdd(&S.cnt32, 1u)] = T[i];
+  for (uint32_t i0 = threadIdx.x; i0 < cap; i0 += blockDim.x * 8) {
+    uint64_t ks[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) ks[q] = i0 + q * blockDim.x < cap ? T[i0 + q * blockDim.x] : kEmpty64;
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+      if (ks[q] != kEmpty64) A[atomicAdd(&S.cnt32, 1u)] = ks[q];
+  }
   __syncthreads();
   uint64_t* srt = block_radix_sort(S, A, B, card - has_max);
   if (has_max && threadIdx.x == 0) srt[card - 1] = kEmpty64;
   if (threadIdx.x == 0) S.max_rank = card - 1;
   __syncthreads();
-  for (uint32_t r = threadIdx.x; r + has_max < card; r += blockDim.x) {
-    uint64_t x = srt[r];
-    uint32_t h = (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> (64 - lg));
-    for (uint32_t probe = 0; probe < cap && T[h] != x; probe++) h = (h + 1) & (cap - 1);
-    R[h] = r;
+  for (uint32_t r0 = threadIdx.x; r0 + has_max < card; r0 += blockDim.x * 8) {
+    uint64_t xs[8];
+    uint32_t hs[8];
+    uint64_t cur[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) xs[q] = r0 + q * blockDim.x + has_max < card ? srt[r0 + q * blockDim.x] : 0ull;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      hs[q] = (uint32_t)((xs[q] * 0x9E3779B97F4A7C15ull) >> (64 - lg));
+      cur[q] = r0 + q * blockDim.x + has_max < card ? T[hs[q]] : 0ull;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      uint32_t r = r0 + q * blockDim.x;
+      if (r + has_max >= card) break;
+      uint32_t h = hs[q];
+      if (cur[q] != xs[q]) {
+        h = (h + 1) & (cap - 1);
+        for (uint32_t probe = 1; probe < cap && T[h] != xs[q]; probe++) h = (h + 1) & (cap - 1);
+      }
+      R[h] = r;
+    }
   }
   __syncthreads();
   dv.card = card;

@@ -287,6 +287,7 @@ struct LaneJob {
   int level;
   uint64_t block_size;  // 0 = adaptive, else clamped to [1, 131072]
   uint8_t plog2;
+  bool vb_raw = false;  // the bitmap's transition count proves the RAW validity blob
 };
 
 uint64_t max_blocks_for(uint64_t n, uint64_t bs) {
@@ -330,13 +331,17 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
       *out_len = lane_bound(n, ln, j.dtype, true, bs);
       return QUOIN_ERR_BUFFER_TOO_SMALL;
     }
-    CK(c->ensure(S_VTMP, (validity_tmp_words(ln) + scan_tile_count(nw) + 16) * 8));
-    CK(c->ensure(S_VBLOB, blob_cap));
-    uint64_t* vtmp = c->p<uint64_t>(S_VTMP);
-    uint64_t* vtile = vtmp + validity_tmp_words(ln);
     TimedRegion tr(T_VALIDITY, st);
-    launch_validity_blob(j.d_bm, ln, vtmp, vtile, c->p<uint8_t>(S_VBLOB), d_misc + 2, st);
-    launch_put_validity(d_dst + 16, 16, c->p<uint8_t>(S_VBLOB), d_misc + 2, d_misc, st);
+    if (j.vb_raw) {
+      launch_put_validity_raw(d_dst + 16, 16, j.d_bm, ln, d_misc, st);
+    } else {
+      CK(c->ensure(S_VTMP, (validity_tmp_words(ln) + scan_tile_count(nw) + 16) * 8));
+      CK(c->ensure(S_VBLOB, blob_cap));
+      uint64_t* vtmp = c->p<uint64_t>(S_VTMP);
+      uint64_t* vtile = vtmp + validity_tmp_words(ln);
+      launch_validity_blob(j.d_bm, ln, vtmp, vtile, c->p<uint8_t>(S_VBLOB), d_misc + 2, st);
+      launch_put_validity(d_dst + 16, 16, c->p<uint8_t>(S_VBLOB), d_misc + 2, d_misc, st);
+    }
   }
   if (maxb == 0) {
     uint64_t base = 0;
@@ -409,19 +414,28 @@ int check_level(const QuoinConfig* cfg, int* level, uint64_t* bs, uint8_t* plog2
 }
 
 // Count the valid bits of a device bitmap; fills S_RANK with per-word ranks.
-int device_valid_count(QuoinCtx* c, cudaStream_t st, const uint8_t* d_bm, uint64_t n, uint64_t* n_valid) {
+// Valid count and word ranks of a device bitmap; *vb_raw tells whether the
+// bitmap's transitions already prove the RAW validity blob (validity.rs:40-70).
+int device_valid_count(QuoinCtx* c, cudaStream_t st, const uint8_t* d_bm, uint64_t n, uint64_t* n_valid,
+                       bool* vb_raw) {
   uint64_t nw = (n + 31) / 32;
   CK(c->ensure(S_RANK, nw * 8 + 64));
   CK(c->ensure(S_TILE, (scan_tile_count(nw) + 16) * 8));
   CK(c->ensure(S_MISC, 64 * 8));
   uint64_t* rank = c->p<uint64_t>(S_RANK);
+  uint64_t* misc = c->p<uint64_t>(S_MISC);
   {
     TimedRegion tr(T_VALIDITY, st);
+    CK(cudaMemsetAsync(misc + 9, 0, 8, st));
     launch_word_popcount(d_bm, n, rank, st);
-    launch_scan_sum(rank, rank, nw, c->p<uint64_t>(S_TILE), c->p<uint64_t>(S_MISC) + 8, st);
+    launch_scan_sum(rank, rank, nw, c->p<uint64_t>(S_TILE), misc + 8, st);
+    launch_bitmap_transitions(d_bm, n, reinterpret_cast<unsigned long long*>(misc + 9), st);
   }
-  CK(cudaMemcpyAsync(n_valid, c->p<uint64_t>(S_MISC) + 8, 8, cudaMemcpyDeviceToHost, st));
+  uint64_t h[2] = {0, 0};
+  CK(cudaMemcpyAsync(h, misc + 8, 16, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  *n_valid = h[0];
+  *vb_raw = h[1] + 1 >= (n + 7) / 8;
   return QUOIN_OK;
 }
 
@@ -440,8 +454,9 @@ int compress_decimal_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, 
   int nl = wire == WT_DEC128 ? 2 : 4;
   uint64_t n_valid = n;
   const uint8_t* d_bm = nullptr;
+  bool vb_raw = false;
   if (d_validity && n) {
-    int rc = device_valid_count(c, st, d_validity, n, &n_valid);
+    int rc = device_valid_count(c, st, d_validity, n, &n_valid, &vb_raw);
     if (rc) return rc;
     if (n_valid < n) d_bm = d_validity;
   }
@@ -482,12 +497,16 @@ int compress_decimal_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, 
       *out_len = need_bound;
       return QUOIN_ERR_BUFFER_TOO_SMALL;
     }
-    CK(c->ensure(S_VTMP, (validity_tmp_words(n) + scan_tile_count(nw) + 16) * 8));
-    CK(c->ensure(S_VBLOB, blob_cap));
-    uint64_t* vtmp = c->p<uint64_t>(S_VTMP);
     uint64_t* d_misc = c->p<uint64_t>(S_MISC);
-    launch_validity_blob(d_bm, n, vtmp, vtmp + validity_tmp_words(n), c->p<uint8_t>(S_VBLOB), d_misc + 2, st);
-    launch_put_validity(d_dst + pos, pos, c->p<uint8_t>(S_VBLOB), d_misc + 2, d_misc + 3, st);
+    if (vb_raw) {
+      launch_put_validity_raw(d_dst + pos, pos, d_bm, n, d_misc + 3, st);
+    } else {
+      CK(c->ensure(S_VTMP, (validity_tmp_words(n) + scan_tile_count(nw) + 16) * 8));
+      CK(c->ensure(S_VBLOB, blob_cap));
+      uint64_t* vtmp = c->p<uint64_t>(S_VTMP);
+      launch_validity_blob(d_bm, n, vtmp, vtmp + validity_tmp_words(n), c->p<uint8_t>(S_VBLOB), d_misc + 2, st);
+      launch_put_validity(d_dst + pos, pos, c->p<uint8_t>(S_VBLOB), d_misc + 2, d_misc + 3, st);
+    }
     uint64_t np = 0;
     CK(cudaMemcpyAsync(&np, d_misc + 3, 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -530,8 +549,9 @@ int compress_column_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, c
                                    plog2, d_dst, dst_cap, out_len);
   uint64_t n_valid = n;
   const uint8_t* d_bm = nullptr;
+  bool vb_raw = false;
   if (d_validity && n) {
-    rc = device_valid_count(c, st, d_validity, n, &n_valid);
+    rc = device_valid_count(c, st, d_validity, n, &n_valid, &vb_raw);
     if (rc) return rc;
     if (n_valid < n) d_bm = d_validity;
   }
@@ -545,7 +565,7 @@ int compress_column_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, c
     launch_lower(d_values, wire, d_bm, d_bm ? c->p<uint64_t>(S_RANK) : nullptr, n, c->p<uint64_t>(S_LANE), st);
     lane = c->p<uint64_t>(S_LANE);
   }
-  LaneJob j{lane, n_valid, wire, n, d_bm, level, bs, plog2};
+  LaneJob j{lane, n_valid, wire, n, d_bm, level, bs, plog2, vb_raw};
   return encode_lane(c, st, j, d_dst, dst_cap, out_len);
 }
 

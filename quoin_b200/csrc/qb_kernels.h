@@ -107,6 +107,12 @@ void launch_decimal_split(const uint8_t* values, int nlimbs, const uint8_t* bm, 
 void launch_validity_blob(const uint8_t* bm, uint64_t n, uint64_t* tmp, uint64_t* tile_tmp, uint8_t* out,
                           uint64_t* blob_len, cudaStream_t st);
 uint64_t validity_tmp_words(uint64_t n);
+// Adds the bitmap's bit-transition count to *count (zero it first).
+void launch_bitmap_transitions(const uint8_t* bm, uint64_t n, unsigned long long* count, cudaStream_t st);
+// Writes varint(len) + the RAW validity blob of an n-bit bitmap at dst and the
+// stream offset after it (dst_off + its length) to *d_base.
+void launch_put_validity_raw(uint8_t* dst, uint64_t dst_off, const uint8_t* bm, uint64_t n, uint64_t* d_base,
+                             cudaStream_t st);
 void launch_write_bytes(uint8_t* dst, const uint8_t* src_dev, uint64_t len, cudaStream_t st);
 
 // Mode win counters (reference src/diag.rs).

@@ -17,22 +17,47 @@ __device__ inline uint64_t lower_one(const uint8_t* base, uint64_t i, int dtype)
   }
 }
 
-// Warp w handles bitmap word w; lane l position 32w + l.
+__device__ inline uint32_t bm_word_at(const uint8_t* bm, uint64_t w, uint64_t n) {
+  uint64_t nbytes = (n + 7) / 8;
+  uint32_t bits = 0;
+  for (int k = 0; k < 4; k++)
+    if (w * 4 + k < nbytes) bits |= (uint32_t)bm[w * 4 + k] << (8 * k);
+  uint64_t rem = n - w * 32;
+  if (rem < 32) bits &= (1u << rem) - 1u;
+  return bits;
+}
+
+// A warp lowers 8 bitmap words (256 positions) per step: lanes 0-7 fetch the
+// words and their ranks, every lane loads its 8 values up front, then each
+// valid value goes to lane[rank].
 __global__ void k_lower(const uint8_t* __restrict__ values, int dtype, const uint8_t* __restrict__ bm,
                         const uint64_t* __restrict__ word_rank, uint64_t n, uint64_t* __restrict__ lane) {
-  uint64_t nw = (n + 31) / 32, nbytes = (n + 7) / 8;
+  uint64_t nw = (n + 31) / 32;
   int l = threadIdx.x & 31;
+  uint32_t below = (1u << l) - 1u;
   uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t w = warp; w < nw; w += nwarps) {
-    uint64_t i = w * 32 + l;
-    if (bm) {
-      uint32_t byte = (w * 4 + (l >> 3) < nbytes) ? bm[w * 4 + (l >> 3)] : 0u;
-      uint32_t bits = 0;
-      for (int k = 0; k < 4; k++) bits |= __shfl_sync(0xffffffffu, byte, k * 8) << (8 * k);
-      if (i < n && ((bits >> l) & 1u)) lane[word_rank[w] + __popc(bits & ((1u << l) - 1u))] = lower_one(values, i, dtype);
-    } else if (i < n) {
-      lane[i] = lower_one(values, i, dtype);
+  for (uint64_t w0 = warp * 8; w0 < nw; w0 += nwarps * 8) {
+    uint32_t mybits = 0;
+    uint64_t myrank = 0;
+    if (bm && l < 8 && w0 + l < nw) {
+      mybits = bm_word_at(bm, w0 + l, n);
+      myrank = word_rank[w0 + l];
+    }
+    uint64_t vals[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      uint64_t i = (w0 + q) * 32 + l;
+      vals[q] = i < n ? lower_one(values, i, dtype) : 0ull;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      uint64_t i = (w0 + q) * 32 + l;
+      uint32_t bits = __shfl_sync(0xffffffffu, mybits, q);
+      uint64_t rank = __shfl_sync(0xffffffffu, myrank, q);
+      if (i >= n) continue;
+      if (!bm) lane[i] = vals[q];
+      else if ((bits >> l) & 1u) lane[rank + __popc(bits & below)] = vals[q];
     }
   }
 }
@@ -43,10 +68,16 @@ static unsigned grid_for_words(uint64_t n) {
   if (g > 148ull * 32) g = 148ull * 32;
   return g ? (unsigned)g : 1u;
 }
+static unsigned grid_for_lower(uint64_t n) {
+  uint64_t nw = (n + 31) / 32;
+  uint64_t g = (nw + 63) / 64;  // 8 warps x 8 words per block step
+  if (g > 148ull * 32) g = 148ull * 32;
+  return g ? (unsigned)g : 1u;
+}
 
 void launch_lower(const void* values, int dtype, const uint8_t* bm, const uint64_t* word_rank, uint64_t n,
                   uint64_t* lane, cudaStream_t st) {
-  if (n) k_lower<<<grid_for_words(n), 256, 0, st>>>((const uint8_t*)values, dtype, bm, word_rank, n, lane);
+  if (n) k_lower<<<grid_for_lower(n), 256, 0, st>>>((const uint8_t*)values, dtype, bm, word_rank, n, lane);
   count_launches(n ? 1 : 0);
 }
 
@@ -251,6 +282,58 @@ __global__ void k_vb_write(const uint8_t* __restrict__ bm, uint64_t n, const uin
   } else {
     for (uint64_t i = gtid; i < raw_len; i += gsz) out[1 + i] = bm[i];
   }
+}
+
+// Number of bit transitions of the bitmap (added to *count).  The RLE blob
+// holds one LEB128 run length per transition plus the final run, each at least
+// a byte, so transitions + 1 >= ceil(n/8) proves the RAW blob is chosen.
+__global__ void k_bitmap_transitions(const uint8_t* __restrict__ bm, uint64_t n, unsigned long long* count) {
+  uint64_t nw = (n + 31) / 32;
+  uint32_t c = 0;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (uint64_t)gridDim.x * blockDim.x)
+    c += __popc(trans_mask(bm, w, n));
+  c = warp_sum(c);
+  __shared__ uint32_t part[8];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += part[k];
+    if (t) atomicAdd(count, t);
+  }
+}
+void launch_bitmap_transitions(const uint8_t* bm, uint64_t n, unsigned long long* count, cudaStream_t st) {
+  uint64_t nw = (n + 31) / 32;
+  unsigned g = (unsigned)qmin((nw + 255) / 256, 148ull * 8);
+  if (g == 0) g = 1;
+  k_bitmap_transitions<<<g, 256, 0, st>>>(bm, n, count);
+  count_launches(1);
+}
+
+// The RAW validity blob straight into the stream: varint(1 + ceil(n/8)), tag
+// 0, the bitmap bytes (validity.rs:40-70); *d_base = the stream offset after it.
+__global__ void k_put_validity_raw(uint8_t* dst, uint64_t dst_off, const uint8_t* __restrict__ bm, uint64_t raw_len,
+                                   uint64_t* d_base) {
+  uint64_t len = 1 + raw_len;
+  uint32_t vl = varint_len(len);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    uint64_t v = len;
+    uint32_t k = 0;
+    do {
+      uint8_t b = (uint8_t)(v & 0x7f);
+      v >>= 7;
+      dst[k++] = v ? (b | 0x80) : b;
+    } while (v);
+    dst[vl] = 0;
+    *d_base = dst_off + vl + len;
+  }
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < raw_len; i += (uint64_t)gridDim.x * blockDim.x)
+    dst[vl + 1 + i] = bm[i];
+}
+void launch_put_validity_raw(uint8_t* dst, uint64_t dst_off, const uint8_t* bm, uint64_t n, uint64_t* d_base,
+                             cudaStream_t st) {
+  k_put_validity_raw<<<148 * 4, 256, 0, st>>>(dst, dst_off, bm, (n + 7) / 8, d_base);
+  count_launches(1);
 }
 
 uint64_t validity_tmp_words(uint64_t n) {
