@@ -911,7 +911,7 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
   }
   __syncthreads();
   for (uint32_t base = 0; base < n; base += blockDim.x * 8) {
-    if (*(volatile uint32_t*)&S.flag) break;
+    if (__any_sync(0xffffffffu, *(volatile uint32_t*)&S.flag)) break;  // warp-uniform exit
     uint64_t xs[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -933,16 +933,17 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
       else
         cur0[q] = cur0[q] == kEmpty64 ? 1ull : cur0[q];  // (not used: 1 never equals kEmpty64)
     }
+    uint32_t mine = 0;  // distinct keys this lane added (counted once per warp below)
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-      if (base + q * blockDim.x + threadIdx.x >= n) break;
+      if (base + q * blockDim.x + threadIdx.x >= n) continue;
       uint64_t x = xs[q];
       if (x == kEmpty64) {
-        if (atomicExch(&S.has_max, 1u) == 0 && atomicAdd(&S.card, 1u) >= max_card) S.flag = 1;
+        if (atomicExch(&S.has_max, 1u) == 0) mine++;
         continue;
       }
       if (cur0[q] == kEmpty64) {  // the first-probe CAS inserted x
-        if (atomicAdd(&S.card, 1u) >= max_card) S.flag = 1;
+        mine++;
         continue;
       }
       if (cur0[q] == x) continue;
@@ -952,7 +953,7 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
         if (cur == kEmpty64) {
           cur = atomicCAS((unsigned long long*)&T[h], kEmpty64, x);
           if (cur == kEmpty64) {
-            if (atomicAdd(&S.card, 1u) >= max_card) S.flag = 1;
+            mine++;
             break;
           }
         }
@@ -960,6 +961,8 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
         h = (h + 1) & (cap - 1);
       }
     }
+    mine = warp_sum(mine);
+    if ((threadIdx.x & 31) == 0 && mine && atomicAdd(&S.card, mine) + mine > max_card) S.flag = 1;
   }
   __syncthreads();
   dv.smem = false;
@@ -977,8 +980,14 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
 #pragma unroll
     for (int q = 0; q < 8; q++) ks[q] = i0 + q * blockDim.x < cap ? T[i0 + q * blockDim.x] : kEmpty64;
 #pragma unroll
-    for (int q = 0; q < 8; q++)
-      if (ks[q] != kEmpty64) A[atomicAdd(&S.cnt32, 1u)] = ks[q];
+    for (int q = 0; q < 8; q++) {  // one counter update per warp and step
+      bool ok = ks[q] != kEmpty64;
+      uint32_t m = __ballot_sync(0xffffffffu, ok);
+      uint32_t base_i = 0;
+      if ((threadIdx.x & 31) == 0 && m) base_i = atomicAdd(&S.cnt32, (uint32_t)__popc(m));
+      base_i = __shfl_sync(0xffffffffu, base_i, 0);
+      if (ok) A[base_i + __popc(m & ((1u << (threadIdx.x & 31)) - 1u))] = ks[q];
+    }
   }
   __syncthreads();
   uint64_t* srt = block_radix_sort(S, A, B, card - has_max);
