@@ -1148,7 +1148,6 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
   uint64_t wstart = (uint64_t)blockIdx.x * kBaseQuantum;
   uint32_t wlen = fixed_bs ? 0u : (uint32_t)(wstart < n ? qmin(kBaseQuantum, n - wstart) : 0);
   uint32_t wstride = max(wlen / 4096u, 1u);
-  const bool wpow2 = (wstride & (wstride - 1u)) == 0;  // full windows: stride 8
   const bool sgn = dtype_signed(dtype);
   if (!fixed_bs) {
     for (int i = threadIdx.x; i < 512; i += blockDim.x) {
@@ -1206,27 +1205,7 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
         nq += x != pv ? 1u : 0u;
         sbad |= (x - pv != d) ? 1u : 0u;
       }
-      if ((j & 15) == 0) {
-        a16mn = u64min(a16mn, x);
-        a16mx = u64max(a16mx, x);
-        if (j > 0) a16dz = u64max(a16dz, zigzag64(x - pv));
-        if (smp16 && !fixed_bs) smp16[(s + j) >> 4] = x;
-      }
-      if ((j & 63) == 0) {
-        a64mn = u64min(a64mn, x);
-        a64mx = u64max(a64mx, x);
-        if (j > 0) a64dz = u64max(a64dz, zigzag64(x - pv));
-      }
       if (!fixed_bs) {
-        uint32_t wj = (uint32_t)(s - wstart) + j;
-        if (wpow2 ? (wj & (wstride - 1u)) == 0 : wj % wstride == 0) {
-          uint32_t bk = (uint32_t)(((x * 0x9E3779B97F4A7C15ull) >> 50) & 0x3FFF);
-          atomicOr(&bitsA[bk >> 5], 1u << (bk & 31));
-        }
-        if ((wj & 31) == 0) {
-          uint32_t bk = (uint32_t)(((x * 0x9E3779B97F4A7C15ull) >> 50) & 0x3FFF);
-          atomicOr(&bitsB[bk >> 5], 1u << (bk & 31));
-        }
         if (j == 0 || x != pv) {  // a repeat's bucket is already set
           uint32_t lb17 = dict_lb_bucket(x);
           atomicOr(&lbits[lb17 >> 5], 1u << (lb17 & 31));
@@ -1253,6 +1232,33 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
     }
     }
     if (do_float) alive &= ~warp_or(fmfail);
+  }
+  // Sampled statistics, kept out of the per-value loop (only a few lanes of a
+  // row would take them): early-out samples at j % 16 / j % 64 == 0 and the
+  // window probe samples (stride wstride, and stride 32).
+  for (uint32_t j = 16u * lane; j < cnt; j += 512) {
+    uint64_t x = sv[j], pv = j ? sv[j - 1] : 0ull;
+    a16mn = u64min(a16mn, x);
+    a16mx = u64max(a16mx, x);
+    if (j > 0) a16dz = u64max(a16dz, zigzag64(x - pv));
+    if (smp16 && !fixed_bs) smp16[(s + j) >> 4] = x;
+    if ((j & 63) == 0) {
+      a64mn = u64min(a64mn, x);
+      a64mx = u64max(a64mx, x);
+      if (j > 0) a64dz = u64max(a64dz, zigzag64(x - pv));
+    }
+  }
+  if (!fixed_bs && cnt) {
+    uint32_t off = (uint32_t)(s - wstart) % wstride;
+    for (uint32_t j = (off ? wstride - off : 0u) + wstride * lane; j < cnt; j += wstride * 32) {
+      uint32_t bk = (uint32_t)(((sv[j] * 0x9E3779B97F4A7C15ull) >> 50) & 0x3FFF);
+      atomicOr(&bitsA[bk >> 5], 1u << (bk & 31));
+    }
+    uint32_t jb = 32u * lane;  // window offset of the sub-block is a multiple of 1024
+    if (jb < cnt) {
+      uint32_t bk = (uint32_t)(((sv[jb] * 0x9E3779B97F4A7C15ull) >> 50) & 0x3FFF);
+      atomicOr(&bitsB[bk >> 5], 1u << (bk & 31));
+    }
   }
   R.umin = warp_min(umn);
   R.umax = warp_max(umx);
