@@ -12,7 +12,7 @@
 
 namespace qb {
 
-constexpr int kEncThreads = 256;
+constexpr int kEncThreads = 512;
 constexpr int kEncWarps = kEncThreads / 32;
 constexpr int kSubsMax = kMaxBlock / kSub;  // 128
 constexpr uint32_t kHashCap = 2048;         // smem hash slots (dict / ALP-RD left parts)
@@ -649,8 +649,11 @@ __device__ inline int rd_code(const EncSmem& S, uint64_t left) {
 // buffer that holds the sorted keys.  All threads of a kEncThreads CTA; the
 // per-warp digit counters live in the dictionary smem area.
 __device__ uint64_t* block_radix_sort(EncSmem& S, uint64_t* a, uint64_t* b, uint32_t m) {
-  static_assert(kEncThreads == 256, "one thread per digit in the offset scan");
-  uint32_t* hist = reinterpret_cast<uint32_t*>(S.big.dict.sorted);  // [kEncWarps][256]
+  static_assert(kEncThreads >= 256 && kEncWarps * 256 * 4 <= sizeof(S.big.dict.sorted) + sizeof(S.big.dict.lb),
+                "one thread per digit in the offset scan; per-warp digit counters fit the dictionary area");
+  // per-warp digit counters [kEncWarps][256] over the sorted-keys and
+  // lower-bound arrays of the dictionary area (neither is in use here)
+  uint32_t* hist = reinterpret_cast<uint32_t*>(S.big.dict.sorted);
   int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   uint64_t k0 = m ? a[0] : 0ull, diff = 0;
   for (uint32_t i0 = t; i0 < m; i0 += blockDim.x * 8) {
@@ -681,22 +684,26 @@ __device__ uint64_t* block_radix_sort(EncSmem& S, uint64_t* a, uint64_t* b, uint
         if (i0 + 32 * q < s1) atomicAdd(&hist[warp * 256 + (uint32_t)((ks[q] >> shift) & 0xFF)], 1u);
     }
     __syncthreads();
-    {  // offsets: digit-major, then warp order (stability)
-      uint32_t tot = 0;
-      for (int w = 0; w < kEncWarps; w++) tot += hist[w * 256 + t];
-      uint32_t inc = tot;
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += u;
+    {  // offsets: digit-major, then warp order (stability); thread t < 256 owns digit t
+      uint32_t tot = 0, inc = 0;
+      if (t < 256) {
+        for (int w = 0; w < kEncWarps; w++) tot += hist[w * 256 + t];
+        inc = tot;
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += u;
+        }
+        if (lane == 31) S.red32[warp] = inc;
       }
-      if (lane == 31) S.red32[warp] = inc;
       __syncthreads();
-      uint32_t run = inc - tot;
-      for (int w = 0; w < warp; w++) run += S.red32[w];
-      for (int w = 0; w < kEncWarps; w++) {
-        uint32_t c = hist[w * 256 + t];
-        hist[w * 256 + t] = run;
-        run += c;
+      if (t < 256) {
+        uint32_t run = inc - tot;
+        for (int w = 0; w < warp; w++) run += S.red32[w];
+        for (int w = 0; w < kEncWarps; w++) {
+          uint32_t c = hist[w * 256 + t];
+          hist[w * 256 + t] = run;
+          run += c;
+        }
       }
     }
     __syncthreads();
