@@ -1166,7 +1166,7 @@ __device__ inline uint32_t warp_or_u32(uint32_t v) {
 }
 
 // Prepass: one warp per prepass item.
-__global__ void __launch_bounds__(kItemWarps * 32) k_prepass(const uint8_t* __restrict__ stream,
+__global__ void __launch_bounds__(kItemWarps * 32, 6) k_prepass(const uint8_t* __restrict__ stream,
                                                            const FrameDesc* __restrict__ frames,
                                                            const FrameAux* __restrict__ aux,
                                                            const ItemRef* __restrict__ items, uint32_t nitems,
@@ -1297,7 +1297,7 @@ __global__ void k_prepass_scan(const uint8_t* __restrict__ stream, const FrameDe
 }
 
 // Main items: one warp per item.
-__global__ void __launch_bounds__(kItemWarps * 32) k_decode_items(const uint8_t* __restrict__ stream,
+__global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8_t* __restrict__ stream,
                                                                 const FrameDesc* __restrict__ frames,
                                                                 int dtype, const FrameAux* __restrict__ aux,
                                                                 const ItemRef* __restrict__ items, uint32_t nitems,
