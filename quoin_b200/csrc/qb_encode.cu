@@ -1936,12 +1936,14 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
                                                       const uint32_t* __restrict__ nbp, uint64_t fixed_bs, int dtype,
                                                       const SubStats* __restrict__ ss,
                                                       const FmStat* __restrict__ fms,
-                                                      uint8_t* __restrict__ scratch, uint8_t* __restrict__ outbuf) {
+                                                      uint8_t* __restrict__ scratch, uint8_t* __restrict__ outbuf,
+                                                      uint64_t out_cap) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   EncSmem& S = *reinterpret_cast<EncSmem*>(smem_raw);
   uint32_t b = blockIdx.x;
   if (b >= *nbp) return;
   FrameDesc fd = frames[b];
+  if (fd.payload_off + fd.plen > out_cap) return;  // the caller sees the total and reports the shortfall
   const uint64_t* v = lane + fd.value_off;
   uint32_t n = fd.n;
   uint8_t* scr = scratch + fd.value_off * kEncScratchPerValue;
@@ -2138,10 +2140,10 @@ void launch_decide(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, 
 
 void launch_emit(const uint64_t* lane, const FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks,
                  uint64_t fixed_bs, int dtype, const void* ss, const void* fms, uint8_t* scratch, uint8_t* out,
-                 cudaStream_t st) {
+                 uint64_t out_cap, cudaStream_t st) {
   if (max_blocks)
     k_emit<<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, fixed_bs, dtype, (const SubStats*)ss,
-                                                              (const FmStat*)fms, scratch, out);
+                                                              (const FmStat*)fms, scratch, out, out_cap);
   count_launches(max_blocks ? 1 : 0);
 }
 

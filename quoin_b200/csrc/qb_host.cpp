@@ -384,20 +384,19 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
     launch_frame_offsets(fr, nb, (uint32_t)maxb, d_misc, c->p<uint64_t>(S_SIZES), c->p<uint64_t>(S_TILE),
                          d_misc + 1, st);
   }
-  uint64_t hm[2] = {0, 0};
-  CK(cudaMemcpyAsync(hm, d_misc, 16, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  uint64_t total = hm[0] + hm[1];
-  *out_len = total;
-  if (total > dst_cap) return QUOIN_ERR_BUFFER_TOO_SMALL;
-  {
+  {  // frames past dst_cap are skipped on the device; the total decides afterwards
     TimedRegion tr(T_EMIT, st);
     launch_emit(j.lane, fr, nb, (uint32_t)maxb, bs, j.dtype, c->p<void>(S_SUBST), fl ? c->p<void>(S_FMST) : nullptr,
-                c->p<uint8_t>(S_SCRATCH), d_dst, st);
+                c->p<uint8_t>(S_SCRATCH), d_dst, dst_cap, st);
   }
+  uint64_t hm[2] = {0, 0};
+  CK(cudaMemcpyAsync(hm, d_misc, 16, cudaMemcpyDeviceToHost, st));
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));
   resolve_timing();
+  uint64_t total = hm[0] + hm[1];
+  *out_len = total;
+  if (total > dst_cap) return QUOIN_ERR_BUFFER_TOO_SMALL;
   return QUOIN_OK;
 }
 

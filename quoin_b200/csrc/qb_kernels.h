@@ -87,10 +87,11 @@ void launch_decide(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, 
 void launch_frame_offsets(FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, const uint64_t* base,
                           uint64_t* sizes_tmp, uint64_t* tile_tmp, uint64_t* total, cudaStream_t st);
 // Emission: one CTA per frame; FoR / DELTA / FLOAT_MULT / XORZ layouts are read
-// from the statistics records of launch_sub_stats.
+// from the statistics records of launch_sub_stats.  Frames that would end past
+// out_cap bytes are not written.
 void launch_emit(const uint64_t* lane, const FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks,
                  uint64_t fixed_bs, int dtype, const void* ss, const void* fms, uint8_t* scratch, uint8_t* out,
-                 cudaStream_t st);
+                 uint64_t out_cap, cudaStream_t st);
 
 // ---- lowering / validity (qb_lower.cu) ----
 // Lower n native values (dtype width) to the u64 lane, keeping only positions
