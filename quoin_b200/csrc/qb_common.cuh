@@ -24,7 +24,8 @@ enum DType : int { DT_F64 = 0, DT_I64 = 1, DT_U64 = 2, DT_I32 = 3, DT_U32 = 4,
 enum Err : uint32_t { E_OK = 0, E_BAD_MAGIC = 1, E_UNSUPPORTED_VERSION = 2,
                       E_TRUNCATED = 3, E_UNKNOWN_MODE = 4, E_CORRUPT = 5,
                       E_LENGTH_MISMATCH = 6, E_UNSUPPORTED_DTYPE = 7,
-                      E_DTYPE_MISMATCH = 8, E_UNSUPPORTED = 9 };
+                      E_DTYPE_MISMATCH = 8, E_UNSUPPORTED = 9,
+                      E_NO_ENTROPY_AREA = 10 };  // entropy-coded part, no device area given
 
 constexpr int kSub = 1024;              // FastLanes sub-block (reference bitpack.rs:22)
 constexpr int kMaxBlock = 131072;       // reference format.rs:44

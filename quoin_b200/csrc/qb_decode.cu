@@ -27,8 +27,10 @@ constexpr uint64_t kSelStep = 512;           // select-table granularity (valid 
 // Per-frame results of the walk (device memory, one per frame).
 struct FrameAux {
   uint32_t err;
-  uint32_t pad;
+  uint32_t ent;         // 1: an entropy-coded part is decoded by the frame kernel
   uint64_t a, b, c, d;  // mode-specific scalars
+  uint64_t e0, e1, e2;  // entropy-coded parts: payload positions
+  uint32_t t0, t1;      // and their tags
   uint64_t dict8[8];    // ALP-RD dictionary
   uint32_t offs[2][kMaxSubs + 1];  // chain 0 / chain 1 sub-block header offsets (payload-relative)
 };
@@ -99,6 +101,7 @@ __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDes
   const uint8_t* p = stream + d.payload_off;
   uint64_t plen = d.plen, n = d.n;
   FrameAux& A = aux[f];
+  A.ent = 0;
   uint32_t e = E_OK;
   switch (d.mode) {
     case M_RAW:
@@ -119,11 +122,18 @@ __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDes
       if (plen < 8) { e = E_TRUNCATED; break; }
       e = for_walk(p, plen, 8, n, A.offs[0]);
       break;
+    case M_BYTE_TRANSPOSE:  // transpose.rs:10-32: the whole payload is entropy-coded
+      A.ent = 1;
+      break;
     case M_FLOAT_MULT: {  // float_mult.rs:100-133
       if (plen < 1 || plen < 2) { e = E_TRUNCATED; break; }
       uint32_t tag = p[0], si = p[1];
       if (si >= 7) { e = E_CORRUPT; break; }
-      if (tag == 1) { e = E_UNSUPPORTED; break; }
+      if (tag == 1) {  // FM_ENTROPY: rANS over LEB128 zigzag deltas of k
+        A.a = si;
+        A.ent = 1;
+        break;
+      }
       if (tag != 0) { e = E_CORRUPT; break; }
       A.a = si;
       e = for_walk(p, plen, 2, n, A.offs[0]);
@@ -171,17 +181,28 @@ __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDes
       if (pos >= plen) { e = E_TRUNCATED; break; }
       uint32_t rtag = p[pos++];
       uint64_t rpos = pos;
-      if (ctag == 1) { e = E_UNSUPPORTED; break; }
-      if (ctag != 0) { e = E_CORRUPT; break; }
-      e = for_walk(p, cpos + clen, cpos, n, A.offs[0]);
-      if (e) break;
-      if (rtag == 1) { e = E_UNSUPPORTED; break; }
-      if (rtag != 0) { e = E_CORRUPT; break; }
-      e = for_walk(p, plen, rpos, n, A.offs[1]);
       A.a = lbw;
       A.b = dsz;
       A.c = exc_start;
       A.d = nexc;
+      A.e0 = cpos;
+      A.e1 = clen;
+      A.e2 = rpos;
+      A.t0 = ctag;
+      A.t1 = rtag;
+      if (ctag == 1) {  // codes entropy-coded: the frame kernel decodes the rest in order
+        A.ent = 1;
+        break;
+      }
+      if (ctag != 0) { e = E_CORRUPT; break; }
+      e = for_walk(p, cpos + clen, cpos, n, A.offs[0]);
+      if (e) break;
+      if (rtag == 1) {  // rights entropy-coded (bit-packed rights bytes)
+        A.ent = 1;
+        break;
+      }
+      if (rtag != 0) { e = E_CORRUPT; break; }
+      e = for_walk(p, plen, rpos, n, A.offs[1]);
       break;
     }
     case M_DICT: {  // dict.rs:154-207
@@ -201,8 +222,12 @@ __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDes
         if (vlen < 8) { e = E_TRUNCATED; break; }
         e = for_walk(p, vpos + vlen, vpos + 8, card, A.offs[1]);
         if (e) break;
-      } else if (vtag == 2) {
-        e = E_UNSUPPORTED;
+      } else if (vtag == 2) {  // TRANSPOSE values: the frame kernel decodes the rest in order
+        A.a = card;
+        A.b = vtag;
+        A.c = vpos;
+        A.d = vlen;
+        A.ent = 1;
         break;
       } else {
         e = E_CORRUPT;
@@ -211,12 +236,17 @@ __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDes
       pos += vlen;
       if (pos >= plen) { e = E_TRUNCATED; break; }
       uint32_t ctag = p[pos++];
-      if (ctag == 1) { e = E_UNSUPPORTED; break; }
-      if (ctag != 0) { e = E_CORRUPT; break; }
-      e = for_walk(p, plen, pos, n, A.offs[0]);
       A.a = card;
       A.b = vtag;
       A.c = vpos;
+      A.d = vlen;
+      if (ctag == 1) {  // CODES_ENTROPY byte planes
+        A.e0 = pos;
+        A.ent = 1;
+        break;
+      }
+      if (ctag != 0) { e = E_CORRUPT; break; }
+      e = for_walk(p, plen, pos, n, A.offs[0]);
       break;
     }
     case M_RLE: {  // rle.rs:44-75
@@ -280,6 +310,26 @@ __device__ inline void warp_unpack(const uint8_t* p, uint32_t off, uint32_t coun
   }
 }
 
+// One value of a FastLanes sub-block (the same layout as warp_unpack): value
+// index i sits in lane i % 32, row i / 32 for widths <= 32, and in 64-bit lane
+// i % 16, row i / 16 above.
+__device__ inline uint64_t for_value_at(const uint8_t* p, uint32_t off, uint32_t i) {
+  uint32_t w = p[off];
+  uint64_t mn = ld_u64(p + off + 1);
+  const uint8_t* words = p + off + 9;
+  if (w == 0) return mn;
+  if (w <= 32) {
+    uint32_t l = i & 31, r = i >> 5, bit = r * w, word = bit >> 5, sh = bit & 31;
+    uint32_t v = ld_u32(words + 4u * (word * 32u + l)) >> sh;
+    if (sh + w > 32) v |= ld_u32(words + 4u * ((word + 1) * 32u + l)) << (32 - sh);
+    return mn + (uint64_t)(v & (w == 32 ? 0xFFFFFFFFu : ((1u << w) - 1u)));
+  }
+  uint32_t fl = i & 15, r = i >> 4, bit = r * w, word = bit >> 6, sh = bit & 63;
+  uint64_t v = ld_u64(words + 8u * (word * 16u + fl)) >> sh;
+  if (sh + w > 64) v |= ld_u64(words + 8u * ((word + 1) * 16u + fl)) << (64 - sh);
+  return mn + (v & (w == 64 ? ~0ull : ((1ull << w) - 1ull)));
+}
+
 // Warp inclusive prefix over buf[0..count) (u64, wrapping), starting from
 // `carry`; writes via out(i, v).
 template <class W>
@@ -308,6 +358,7 @@ struct DecSmem {
   uint64_t wxor[kDecWarps];
   uint64_t sc[4];
   unsigned long long nth;
+  uint32_t eoffs[kMaxSubs + 1];      // FoR chain sub-block offsets found by the frame kernel
   union {
     uint64_t wbuf[kDecWarps][kSub];  // per-warp sub-block staging (64 KB)
     struct {
@@ -318,6 +369,12 @@ struct DecSmem {
       uint64_t xbuf[kXorzChunk];     // XORZ chunk values (16 KB)
       uint64_t ring[kXorzRing];      // decoded values not yet stored (32 KB)
     } x;
+    struct {                         // rANS tables (rans.rs:110-175)
+      uint32_t freq[256];
+      uint32_t cum[257];
+      uint8_t sym[4096];
+      uint64_t sc[4];
+    } r;
   } u;
 };
 
@@ -665,6 +722,352 @@ __device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64
 }
 
 // ---------------------------------------------------------------------------
+// Entropy-coded parts (Balanced and above): the 4-state rANS blocks of
+// rans.rs:110-175 behind the entropy tag of entropy/mod.rs:152-178.
+// ---------------------------------------------------------------------------
+
+// One rANS block decoded by the CTA: thread 0 reads the header and runs the
+// decoder (four states share one byte stream, so it is sequential); all
+// threads build the slot -> symbol table.  Writes the first min(len, cap)
+// symbols to out and the decoded length to *len_out.  Error kinds and their
+// order follow rans.rs.
+__device__ __noinline__ uint32_t rans_decode_cta(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t max_len, uint8_t* out,
+                                   uint64_t cap, uint64_t* len_out) {
+  int t = threadIdx.x;
+  for (int i = t; i < 256; i += blockDim.x) S.u.r.freq[i] = 0;
+  for (int i = t; i < 4096; i += blockDim.x) S.u.r.sym[i] = 0;
+  __syncthreads();
+  if (t == 0) {
+    uint32_t e = E_OK;
+    uint64_t pos = 0, n64 = 0, ns = 0;
+    do {
+      e = rd_varint(p, plen, &pos, &n64);
+      if (e) break;
+      if (n64 > max_len) { e = E_CORRUPT; break; }
+      e = rd_varint(p, plen, &pos, &ns);
+      if (e) break;
+      if (ns == 0 || ns > 256) { e = E_CORRUPT; break; }
+      uint32_t sum = 0;
+      for (uint64_t k = 0; k < ns; k++) {
+        if (pos >= plen) { e = E_TRUNCATED; break; }
+        uint32_t sy = p[pos++];
+        uint64_t f64v;
+        e = rd_varint(p, plen, &pos, &f64v);
+        if (e) break;
+        uint32_t f = (uint32_t)f64v;  // the reference reads the frequency as a u32 (`as u32`)
+        if (f == 0 || f > 4096) { e = E_CORRUPT; break; }
+        S.u.r.freq[sy] = f;
+        sum += f;
+      }
+      if (e) break;
+      if (sum != 4096) { e = E_CORRUPT; break; }
+      uint32_t c = 0;
+      for (int sy = 0; sy < 256; sy++) {
+        S.u.r.cum[sy] = c;
+        c += S.u.r.freq[sy];
+      }
+      S.u.r.cum[256] = c;
+    } while (false);
+    S.u.r.sc[0] = e;
+    S.u.r.sc[1] = pos;
+    S.u.r.sc[2] = n64;
+  }
+  __syncthreads();
+  uint32_t e = (uint32_t)S.u.r.sc[0];
+  if (e) {
+    *len_out = 0;
+    __syncthreads();
+    return e;
+  }
+  for (int sy = t; sy < 256; sy += blockDim.x)
+    for (uint32_t slot = S.u.r.cum[sy]; slot < S.u.r.cum[sy + 1] && slot < 4096; slot++) S.u.r.sym[slot] = (uint8_t)sy;
+  __syncthreads();
+  if (t == 0) {
+    uint64_t pos = S.u.r.sc[1], n64 = S.u.r.sc[2];
+    uint32_t x[4] = {0, 0, 0, 0};
+    uint32_t ee = E_OK;
+    for (int k = 0; k < 4 && !ee; k++) {
+      if (plen < pos + 4) {
+        ee = E_TRUNCATED;
+      } else {
+        x[k] = ld_u32(p + pos);
+        pos += 4;
+      }
+    }
+    for (uint64_t i = 0; i < n64 && !ee; i++) {
+      uint32_t idx = (uint32_t)(i & 3), xi = x[idx], slot = xi & 4095u;
+      uint32_t sy = S.u.r.sym[slot];
+      if (i < cap) out[i] = (uint8_t)sy;
+      uint32_t xn = S.u.r.freq[sy] * (xi >> 12) + slot - S.u.r.cum[sy];
+      while (xn < (1u << 23)) {
+        if (pos >= plen) {
+          ee = E_TRUNCATED;
+          break;
+        }
+        xn = (xn << 8) | p[pos++];
+      }
+      x[idx] = xn;
+    }
+    S.u.r.sc[0] = ee;
+  }
+  __syncthreads();
+  e = (uint32_t)S.u.r.sc[0];
+  *len_out = S.u.r.sc[2];
+  __syncthreads();
+  return e;
+}
+
+// entropy/mod.rs:152-178: a tag byte, then rANS (the range coder, legacy tANS
+// and the LZ cascade tags are outside the pool).
+__device__ uint32_t residuals_cta(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t max_len, uint8_t* out,
+                                 uint64_t cap, uint64_t* len_out) {
+  *len_out = 0;
+  if (plen == 0) return E_TRUNCATED;
+  uint32_t tag = p[0];
+  if (tag == 2) return rans_decode_cta(S, p + 1, plen - 1, max_len, out, cap, len_out);
+  if (tag == 0 || tag == 1 || tag == 3) return E_UNSUPPORTED;
+  return E_CORRUPT;
+}
+
+// Thread 0 computes a status, every thread gets it.
+__device__ __forceinline__ uint32_t cta_bcast(DecSmem& S, uint32_t v) {
+  if (threadIdx.x == 0) S.sc[3] = v;
+  __syncthreads();
+  uint32_t r = (uint32_t)S.sc[3];
+  __syncthreads();
+  return r;
+}
+
+// A frame with an entropy-coded part, decoded whole by the CTA into the
+// frame's entropy area (24 bytes per value + 128) and stored.  Without an
+// area the frame is not decoded (E_NO_ENTROPY_AREA).
+__device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDesc& d, const FrameAux& A, const uint8_t* p,
+                                         uint8_t* ent, const DecodeOut& O) {
+  int t = threadIdx.x, l = t & 31, warp = t >> 5;
+  uint64_t plen = d.plen, n = d.n, c0 = d.value_off, len = 0;
+  uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
+  uint32_t e = E_OK;
+  if (!ent) return E_NO_ENTROPY_AREA;
+  switch (d.mode) {
+    case M_BYTE_TRANSPOSE: {  // transpose.rs:10-32, transform.rs:24-47
+      uint8_t* bt = ent;
+      e = residuals_cta(S, p, plen, n * 8 + 16, bt, n * 8 + 16, &len);
+      if (e) return e;
+      if (len != n * 8) return E_CORRUPT;
+      cta_store(O, c0, (uint32_t)n, [&](uint32_t q) {
+        uint64_t w = 0;
+        for (int pl = 0; pl < 8; pl++) w |= (uint64_t)bt[(uint64_t)pl * n + q] << (8 * pl);
+        return w;
+      });
+      return E_OK;
+    }
+    case M_FLOAT_MULT: {  // float_mult.rs:100-133, FM_ENTROPY
+      uint64_t cap = n * 10 + 16;
+      uint8_t* res = ent;
+      e = residuals_cta(S, p + 2, plen - 2, cap, res, cap, &len);
+      if (e) return e;
+      uint64_t* vals = reinterpret_cast<uint64_t*>(ent + ((cap + 15) & ~15ull));
+      uint32_t ee = E_OK;
+      if (t == 0) {
+        uint64_t pos = 0;
+        int64_t prev = 0;
+        for (uint64_t i = 0; i < n && !ee; i++) {
+          uint64_t z = 0;
+          ee = rd_varint(res, len, &pos, &z);
+          if (ee) break;
+          prev = (int64_t)((uint64_t)prev + unzigzag64(z));
+          vals[i] = (uint64_t)prev;
+        }
+        if (!ee && pos != len) ee = E_CORRUPT;
+      }
+      e = cta_bcast(S, ee);
+      if (e) return e;
+      double scale = kFmScales[A.a];
+      cta_store(O, c0, (uint32_t)n,
+                [&](uint32_t q) { return f64_bits(__ddiv_rn(__ll2double_rn((long long)vals[q]), scale)); });
+      return E_OK;
+    }
+    case M_ALP_RD: {  // alp_rd.rs:208-285 with entropy-coded codes and/or rights
+      uint32_t lbw = (uint32_t)A.a, dsz = (uint32_t)A.b, rbw = 64 - lbw;
+      uint8_t* codes = ent;                                   // n bytes
+      uint8_t* rb = ent + ((n + 15) & ~15ull);                // rights bytes, <= 8n + 64
+      uint64_t* vals = reinterpret_cast<uint64_t*>(rb + ((n * 8 + 64 + 15) & ~15ull));
+      if (A.t0 == 1) {
+        e = residuals_cta(S, p + A.e0, A.e1, n, codes, n, &len);
+        if (e) return e;
+        if (len != n) return E_CORRUPT;
+      }
+      const uint8_t* rsrc = p;
+      uint32_t ee = E_OK;
+      if (A.t1 == 0) {
+        if (t == 0) ee = for_walk(p, plen, A.e2, n, S.eoffs);
+      } else if (A.t1 == 1) {
+        e = residuals_cta(S, p + A.e2, plen - A.e2, n * 8 + 64, rb, n * 8 + 64, &len);
+        if (e) return e;
+        rsrc = rb;
+        if (t == 0) ee = for_walk(rb, len, 0, n, S.eoffs);
+      } else {
+        ee = E_CORRUPT;
+      }
+      e = cta_bcast(S, ee);
+      if (e) return e;
+      if (t == 0) S.flag = 0;
+      __syncthreads();
+      uint64_t* cbuf = &S.u.wbuf[warp][0];
+      for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+        uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+        if (A.t0 == 1) {
+          for (uint32_t i = l; i < cnt; i += 32) cbuf[i] = codes[(uint64_t)k * kSub + i];
+        } else {
+          warp_unpack(p, A.offs[0][k], cnt, [&](uint32_t i, uint64_t c) { cbuf[i] = c; });
+        }
+        __syncwarp();
+        uint64_t* o = vals + (uint64_t)k * kSub;
+        warp_unpack(rsrc, S.eoffs[k], cnt, [&](uint32_t i, uint64_t r) {
+          uint64_t c = cbuf[i];
+          if (c >= dsz) S.flag = 1;
+          else o[i] = (A.dict8[c] << rbw) | r;
+        });
+        __syncwarp();
+      }
+      __syncthreads();
+      if (S.flag) return E_CORRUPT;
+      if (t == 0 && A.d) {  // exceptions in order (alp_rd.rs:281-283): (left << rbw) | rights[p]
+        uint64_t pos = A.c;
+        for (uint64_t x = 0; x < A.d; x++) {
+          uint64_t pp = 0;
+          rd_varint(p, plen, &pos, &pp);
+          uint64_t lv = ld_u64(p + pos);
+          pos += 8;
+          vals[pp] = (lv << rbw) | for_value_at(rsrc, S.eoffs[pp / kSub], (uint32_t)(pp % kSub));
+        }
+      }
+      __syncthreads();
+      cta_store(O, c0, (uint32_t)n, [&](uint32_t q) { return vals[q]; });
+      return E_OK;
+    }
+    case M_DICT: {  // dict.rs:154-207 with TRANSPOSE values and/or CODES_ENTROPY
+      uint64_t card = A.a, vtag = A.b, vpos = A.c, vlen = A.d;
+      uint64_t* dv = reinterpret_cast<uint64_t*>(ent);                      // card values (card <= n)
+      uint64_t* vals = reinterpret_cast<uint64_t*>(ent + 8 * n);            // also the byte-plane buffer
+      uint16_t* codes = reinterpret_cast<uint16_t*>(ent + 16 * n);
+      if (vtag == 0) {
+        for (uint64_t i = t; i < card; i += kDecThreads) dv[i] = ld_u64(p + vpos + 8 * i);
+      } else if (vtag == 1) {
+        chain_prefix(S, p, A.offs[1], card, ld_u64(p + vpos), &S.u.d.stage[0][0], 4,
+                     [](uint64_t v) { return unzigzag64(v); },
+                     [&](uint32_t k, const uint64_t* buf, uint32_t cnt) {
+                       for (uint32_t q = l; q < cnt; q += 32) dv[(uint64_t)k * kSub + q] = buf[q];
+                     });
+      } else {
+        uint8_t* tb = reinterpret_cast<uint8_t*>(vals);
+        e = residuals_cta(S, p + vpos, vlen, card * 8, tb, card * 8, &len);
+        if (e) return e;
+        if (len != card * 8) return E_CORRUPT;
+        for (uint64_t i = t; i < card; i += kDecThreads) {
+          uint64_t w = 0;
+          for (int pl = 0; pl < 8; pl++) w |= (uint64_t)tb[(uint64_t)pl * card + i] << (8 * pl);
+          dv[i] = w;
+        }
+      }
+      __syncthreads();
+      // codes: the tag byte follows the values (already read by the walk for
+      // values tags 0 and 1, where only CODES_ENTROPY lands here)
+      uint32_t ctag = 1;
+      uint64_t pos = A.e0;
+      if (vtag == 2) {
+        uint32_t ee = E_OK;
+        if (t == 0) {
+          uint64_t q = vpos + vlen;
+          if (q >= plen) {
+            ee = E_TRUNCATED;
+          } else {
+            ctag = p[q];
+            S.sc[2] = q + 1;
+            if (ctag == 0) ee = for_walk(p, plen, q + 1, n, S.eoffs);
+            else if (ctag != 1) ee = E_CORRUPT;
+            S.sc[1] = ctag;
+          }
+        }
+        e = cta_bcast(S, ee);
+        if (e) return e;
+        ctag = (uint32_t)S.sc[1];
+        pos = S.sc[2];
+        __syncthreads();
+      }
+      if (ctag == 0) {
+        if (t == 0) S.flag = 0;
+        __syncthreads();
+        for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+          uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
+          uint64_t* o = vals + (uint64_t)k * kSub;
+          warp_unpack(p, S.eoffs[k], cnt, [&](uint32_t i, uint64_t c) {
+            if (c >= card) S.flag = 1;
+            else o[i] = dv[c];
+          });
+        }
+        __syncthreads();
+        if (S.flag) return E_CORRUPT;
+      } else {
+        for (uint64_t i = t; i < n; i += kDecThreads) codes[i] = 0;
+        uint32_t ee = E_OK;
+        uint64_t nb = 0;
+        if (t == 0) {
+          if (pos >= plen) {
+            ee = E_TRUNCATED;
+          } else {
+            nb = p[pos++];
+            if (nb < 1 || nb > 2) ee = E_CORRUPT;
+          }
+          S.sc[1] = nb;
+          S.sc[2] = pos;
+        }
+        e = cta_bcast(S, ee);
+        if (e) return e;
+        nb = S.sc[1];
+        pos = S.sc[2];
+        __syncthreads();
+        uint8_t* plane = reinterpret_cast<uint8_t*>(vals);
+        for (uint64_t k = 0; k < nb; k++) {
+          uint64_t ln = 0;
+          ee = E_OK;
+          if (t == 0) {
+            ee = rd_varint(p, plen, &pos, &ln);
+            if (!ee && ln > plen - pos) ee = E_TRUNCATED;
+            S.sc[1] = ln;
+            S.sc[2] = pos;
+          }
+          e = cta_bcast(S, ee);
+          if (e) return e;
+          ln = S.sc[1];
+          pos = S.sc[2];
+          __syncthreads();
+          e = residuals_cta(S, p + pos, ln, n, plane, n, &len);
+          if (e) return e;
+          pos += ln;
+          if (len != n) return E_CORRUPT;
+          for (uint64_t i = t; i < n; i += kDecThreads) codes[i] |= (uint16_t)((uint32_t)plane[i] << (8 * k));
+          __syncthreads();
+        }
+        if (t == 0) S.flag = 0;
+        __syncthreads();
+        for (uint64_t i = t; i < n; i += kDecThreads) {
+          uint32_t c = codes[i];
+          if (c >= card) S.flag = 1;
+          else vals[i] = dv[c];
+        }
+        __syncthreads();
+        if (S.flag) return E_CORRUPT;
+      }
+      cta_store(O, c0, (uint32_t)n, [&](uint32_t q) { return vals[q]; });
+      return E_OK;
+    }
+    default:
+      return E_UNSUPPORTED;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // The decode kernel
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __restrict__ stream,
@@ -672,7 +1075,8 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
                                                               int dtype, const FrameAux* __restrict__ aux,
                                                               DecodeOut O, uint64_t* __restrict__ scratch,
                                                               unsigned long long* __restrict__ err,
-                                                              const uint32_t* __restrict__ list) {
+                                                              const uint32_t* __restrict__ list,
+                                                              uint8_t* __restrict__ ent) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   DecSmem& S = *reinterpret_cast<DecSmem*>(smem_raw);
   if ((int)blockIdx.x >= nf) return;
@@ -681,6 +1085,12 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
   if (A.err) return;
   FrameDesc d = frames[f];
   const uint8_t* p = stream + d.payload_off;
+  if (A.ent) {  // entropy-coded parts, in the frame's area (FrameDesc::aux = 1 + offset / 128)
+    uint8_t* area = ent && d.aux ? ent + 128ull * (d.aux - 1) : nullptr;
+    uint32_t ee = decode_entropy_frame(S, d, A, p, area, O);
+    if (ee && threadIdx.x == 0) atomicMin(err, ((unsigned long long)f << 8) | ee);
+    return;
+  }
   uint64_t plen = d.plen, n = d.n;
   uint64_t c0 = d.value_off;
   int t = threadIdx.x, l = t & 31, warp = t >> 5;
@@ -809,14 +1219,14 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
         break;
       }
       if (fo) {
-        if (t == 0) {  // exceptions in order (alp_rd.rs:281-283)
-          uint64_t pos = A.c, rmask = (1ull << rbw) - 1ull;
+        if (t == 0) {  // exceptions in order (alp_rd.rs:281-283): (left << rbw) | rights[p]
+          uint64_t pos = A.c;
           for (uint64_t x = 0; x < A.d; x++) {
             uint64_t pp = 0;
             rd_varint(p, plen, &pos, &pp);
             uint64_t lv = ld_u64(p + pos);
             pos += 8;
-            fo[pp] = (lv << rbw) | (fo[pp] & rmask);
+            fo[pp] = (lv << rbw) | for_value_at(p, A.offs[1][pp / kSub], (uint32_t)(pp % kSub));
           }
         }
         __syncthreads();
@@ -1616,7 +2026,8 @@ void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf
   FrameAux* A = reinterpret_cast<FrameAux*>(aux);
   k_walk_frames<<<(nf + 127) / 128, 128, 0, st>>>(stream, frames, nf, dtype, A, err);
   cudaFuncSetAttribute(k_decode_frames, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecSmem));
-  k_decode_frames<<<nf, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, nf, dtype, A, out, scratch, err, nullptr);
+  k_decode_frames<<<nf, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, nf, dtype, A, out, scratch, err, nullptr,
+                                                            nullptr);
   count_launches(2);
 }
 
@@ -1647,7 +2058,7 @@ void launch_decode_items(const uint8_t* stream, const FrameDesc* frames, int nf,
   if (plan.nlist) {
     cudaFuncSetAttribute(k_decode_frames, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecSmem));
     k_decode_frames<<<plan.nlist, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, (int)plan.nlist, dtype, A, out,
-                                                                       scratch, err, plan.list);
+                                                                       scratch, err, plan.list, plan.ent);
     launches++;
   }
   count_launches(launches);

@@ -195,7 +195,7 @@ inline int plain_code(int ext) {
 enum Slot {
   S_IN, S_BM, S_RANK, S_LANE, S_GROW, S_FRAMES, S_NB, S_SIZES, S_TILE, S_SCRATCH, S_OUT, S_VTMP, S_VBLOB,
   S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_DAUX, S_SUBST, S_FMST,
-  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_COUNT
+  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_ENT, S_COUNT
 };
 
 struct QuoinCtx {
@@ -586,6 +586,7 @@ struct LaneIdx {
   std::vector<uint2> frame_pre;
   std::vector<uint32_t> list;
   bool need_scan = false;
+  uint64_t ent_bytes = 0;  // device area for the entropy-coded parts of listed frames
   uint64_t main_base = 0, pre_base = 0, fp_base = 0, list_base = 0;  // index of the first frame in the device table
 };
 
@@ -679,9 +680,63 @@ int parse_lane(const uint8_t* src, uint64_t base, uint64_t len, LaneIdx& L) {
   return K_OK;
 }
 
+// ALP-RD header up to the rights tag (reference alp_rd.rs:208-250): the
+// exception count and the two part tags; false when it does not parse here
+// (the device walk then reports the error).
+bool alprd_tags_h(const uint8_t* p, uint64_t plen, uint64_t* nexc, uint32_t* ctag, uint32_t* rtag) {
+  if (plen < 2 || p[1] > 8) return false;
+  uint64_t pos = 2 + 8ull * p[1], clen = 0;
+  if (pos > plen || rd_varint_h(p, plen, &pos, nexc) != K_OK) return false;
+  for (uint64_t x = 0; x < *nexc; x++) {
+    uint64_t pp;
+    if (rd_varint_h(p, plen, &pos, &pp) != K_OK || plen - pos < 8) return false;
+    pos += 8;
+  }
+  if (pos >= plen) return false;
+  *ctag = p[pos++];
+  if (rd_varint_h(p, plen, &pos, &clen) != K_OK || clen > plen - pos) return false;
+  pos += clen;
+  if (pos >= plen) return false;
+  *rtag = p[pos];
+  return true;
+}
+
+// Whether a frame may hold an entropy-coded part (Balanced and above: the
+// rANS stage of entropy/mod.rs:152-178), decoded by the frame kernel in a
+// device area of its own.  Errs on the side of yes when the header does not
+// parse: BYTE_TRANSPOSE always; FLOAT_MULT tag 1 (float_mult.rs:100-133);
+// ALP-RD codes or rights tag 1; DICT values tag 2 or codes tag 1
+// (dict.rs:154-207).
+bool entropy_frame_h(const uint8_t* p, uint64_t plen, uint32_t mode) {
+  switch (mode) {
+    case 11:
+      return true;
+    case 17:
+      return plen < 2 || p[0] == 1;
+    case 52: {
+      uint64_t nexc = 0;
+      uint32_t ct = 0, rt = 0;
+      return !alprd_tags_h(p, plen, &nexc, &ct, &rt) || ct == 1 || rt == 1;
+    }
+    case 19: {
+      uint64_t pos = 0, card = 0, vlen = 0;
+      if (rd_varint_h(p, plen, &pos, &card) != K_OK || pos >= plen) return true;
+      uint32_t vtag = p[pos++];
+      if (vtag == 2) return true;
+      if (rd_varint_h(p, plen, &pos, &vlen) != K_OK || vlen > plen - pos) return true;
+      pos += vlen;
+      return pos >= plen || p[pos] == 1;
+    }
+    default:
+      return false;
+  }
+}
+
 // Warp items of every frame (512 values, or 512 payload bytes for XORZ).
 // Frames the items do not cover, or whose header cannot be read here, go to
-// the frame list; the device walk reports their errors.
+// the frame list; the device walk reports their errors.  Listed frames with
+// an entropy-coded part get a device area of 24 bytes per value + 128
+// (128-byte units, 1 + its offset in FrameDesc::aux; 0 = none).
 void build_items(const uint8_t* src, LaneIdx& L) {
   const uint32_t V = 512, B = 512;
   for (uint32_t f = 0; f < (uint32_t)L.frames.size(); f++) {
@@ -697,8 +752,12 @@ void build_items(const uint8_t* src, LaneIdx& L) {
       for (uint32_t j = 0; j < cnt; j++) L.pre_items.push_back(ItemRef{f, j});
     };
     switch (d.mode) {
-      case 5: case 1: case 2: case 50: case 17: case 9:  // RAW CONST STRIDE FOR FLOAT_MULT ALP
+      case 5: case 1: case 2: case 50: case 9:  // RAW CONST STRIDE FOR ALP
         add_main(nv);
+        break;
+      case 17:  // FLOAT_MULT: items for the bit-packed form (tag 0)
+        if (plen >= 2 && p[0] == 0) add_main(nv);
+        else L.list.push_back(f);
         break;
       case 51:  // DELTA
         add_pre(nv);
@@ -723,13 +782,10 @@ void build_items(const uint8_t* src, LaneIdx& L) {
         L.need_scan = true;
         break;
       }
-      case 52: {  // ALP-RD: items only without exceptions
+      case 52: {  // ALP-RD: items only without exceptions and with both parts bit-packed
         uint64_t nexc = 1;
-        if (plen >= 2 && p[1] <= 8) {
-          uint64_t pos = 2 + 8ull * p[1];
-          if (pos > plen || rd_varint_h(p, plen, &pos, &nexc) != K_OK) nexc = 1;
-        }
-        if (nexc == 0) add_main(nv);
+        uint32_t ct = 1, rt = 1;
+        if (alprd_tags_h(p, plen, &nexc, &ct, &rt) && nexc == 0 && ct == 0 && rt == 0) add_main(nv);
         else L.list.push_back(f);
         break;
       }
@@ -738,6 +794,12 @@ void build_items(const uint8_t* src, LaneIdx& L) {
         break;
     }
     L.frame_pre.push_back(make_uint2(pre0, (uint32_t)L.pre_items.size() - pre0));
+  }
+  for (uint32_t f : L.list) {
+    FrameDesc& d = L.frames[f];
+    if (!entropy_frame_h(src + d.payload_off, d.plen, d.mode)) continue;
+    d.aux = (uint32_t)(1 + L.ent_bytes / 128);
+    L.ent_bytes += (24ull * d.n + 128 + 127) & ~127ull;
   }
 }
 
@@ -922,6 +984,7 @@ ItemPlan lane_plan(const LaneIdx& L, const uint64_t* ditems) {
   P.list = reinterpret_cast<const uint32_t*>(ditems + L.list_base);
   P.nlist = (uint32_t)L.list.size();
   P.need_scan = L.need_scan;
+  P.ent = nullptr;
   return P;
 }
 
@@ -938,6 +1001,18 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
   void* daux = c->p<void>(S_DAUX);
   CK(c->ensure(S_PRE, (X.max_pre + 1) * prepass_rec_bytes()));
   void* dpre = c->p<void>(S_PRE);
+  uint64_t ent_bytes = 0;  // lanes decode one after another on the stream: one area serves all
+  for (auto& L : X.lanes) ent_bytes = L.ent_bytes > ent_bytes ? L.ent_bytes : ent_bytes;
+  uint8_t* dent = nullptr;
+  if (ent_bytes) {
+    CK(c->ensure(S_ENT, ent_bytes));
+    dent = c->p<uint8_t>(S_ENT);
+  }
+  auto plan_of = [&](const LaneIdx& L) {
+    ItemPlan P = lane_plan(L, ditems);
+    P.ent = L.ent_bytes ? dent : nullptr;
+    return P;
+  };
   if (!X.decimal) {
     const LaneIdx& L = X.lanes[0];
     uint32_t w = native_width(X.wire);
@@ -954,7 +1029,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
                   L.n_total};
       {
         TimedRegion tr(T_DECODE, st);
-        launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, lane_plan(L, ditems), dpre,
+        launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, plan_of(L), dpre,
                             scr, daux, d_err, st);
       }
       if (L.n_total == 0 && X.n) CK(cudaMemsetAsync(d_out, 0, X.n * w, st));  // all null
@@ -964,7 +1039,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
       DecodeOut O{lane_out, WT_U64, nullptr, nullptr, nullptr, L.n_total, L.n_total};
       {
         TimedRegion tr(T_DECODE, st);
-        launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, lane_plan(L, ditems), dpre,
+        launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, plan_of(L), dpre,
                             scr, daux, d_err, st);
       }
       if (X.n) {
@@ -987,7 +1062,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
       const LaneIdx& L = X.lanes[k];
       DecodeOut O{limbs + (uint64_t)k * X.n_valid, WT_U64, nullptr, nullptr, nullptr, X.n_valid, X.n_valid};
       TimedRegion tr(T_DECODE, st);
-      launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), WT_U64, O, lane_plan(L, ditems), dpre, scr,
+      launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), WT_U64, O, plan_of(L), dpre, scr,
                           daux, d_err, st);
     }
     if (X.n) {

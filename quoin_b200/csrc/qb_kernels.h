@@ -45,6 +45,7 @@ struct ItemPlan {
   const uint32_t* list;
   uint32_t nlist;
   bool need_scan;
+  uint8_t* ent;  // entropy areas of the listed frames (FrameDesc::aux), or null
 };
 uint64_t prepass_rec_bytes();
 void launch_decode_items(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,

@@ -10,7 +10,9 @@
 // Limits (the arena is sized for them, larger streams are rejected with
 // QUOIN_ERR_NOALLOC_LIMIT before any decode work): at most
 // kNoAllocMaxValues values and kNoAllocMaxFrames frames; 8-byte dtypes
-// (f64 / i64 / u64) without a validity bitmap.
+// (f64 / i64 / u64) without a validity bitmap.  Frames with an entropy-coded
+// part (levels above Fast) need a decode area the arena does not hold: the
+// decode reports them with QUOIN_ERR_NOALLOC_LIMIT.
 //
 // Nothing in the arena has to start at zero: every call's first kernel resets
 // the status words and the frame table before the decode kernels read them.
@@ -31,7 +33,7 @@ namespace {
 
 constexpr uint32_t kNoAllocMaxFrames = 256;
 constexpr uint64_t kNoAllocMaxValues = 262144;
-constexpr uint64_t kNoAllocAuxBytes = 1152;  // per frame, >= the decoder's per-frame record
+constexpr uint64_t kNoAllocAuxBytes = 1280;  // per frame, >= the decoder's per-frame record
 constexpr uint64_t kMaxLogicalValuesD = 1ull << 36;
 constexpr int kMaxDevices = 64;
 
@@ -136,7 +138,8 @@ int kind_code(uint32_t kind) {
     case E_LENGTH_MISMATCH: return QUOIN_ERR_LENGTH_MISMATCH;
     case E_UNSUPPORTED_DTYPE: return QUOIN_ERR_UNSUPPORTED_DTYPE;
     case E_DTYPE_MISMATCH: return QUOIN_ERR_DTYPE_MISMATCH;
-    case kLimit: return QUOIN_ERR_NOALLOC_LIMIT;
+    case kLimit:
+    case E_NO_ENTROPY_AREA: return QUOIN_ERR_NOALLOC_LIMIT;
     case kLimit + 1: return QUOIN_ERR_BUFFER_TOO_SMALL;
     default: return QUOIN_ERR_UNSUPPORTED;
   }

@@ -199,17 +199,13 @@ def test_config_columns_match_oracle(qb, oracle, config):
 
 
 # ---------------------------------------------------------------------------
-# Decode of streams the GPU encoder never produces (Balanced-level tags are
-# outside the GPU decode pool today; they must be rejected, not mis-decoded).
+# Decode of a stream the GPU encoder never produces: Balanced level, with
+# rANS-coded ALP-RD codes (tests/test_entropy_decode.py covers every tag).
 # ---------------------------------------------------------------------------
-def test_unsupported_entropy_tags_are_rejected(qb, oracle):
+def test_balanced_stream_decodes(qb, oracle):
     vals = np.sin(np.arange(40000) * 0.01)
     s = oracle.compress_column(vals, F64, level=2)
-    try:
-        d = qb.decompress_column(s)
-        assert dec_bytes(d) == vals.view(np.uint8).tobytes()
-    except qb.Error as e:
-        assert e.kind in ("Unsupported", "CorruptPayload")
+    assert dec_bytes(qb.decompress_column(s)) == vals.view(np.uint8).tobytes()
 
 
 # ---------------------------------------------------------------------------
