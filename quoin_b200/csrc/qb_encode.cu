@@ -2025,8 +2025,9 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
 // ---------------------------------------------------------------------------
 
 // Block plan (reference encoder.rs:154-178): fills frames[].value_off / .n.
-__global__ void k_plan(const uint8_t* __restrict__ grow, uint64_t n, uint64_t fixed_bs, FrameDesc* frames,
-                       uint32_t* nb) {
+constexpr int kPlanThreads = 1024;
+__global__ void __launch_bounds__(kPlanThreads)
+    k_plan(const uint8_t* __restrict__ grow, uint64_t n, uint64_t fixed_bs, FrameDesc* frames, uint32_t* nb) {
   if (fixed_bs) {
     uint64_t nblk = (n + fixed_bs - 1) / fixed_bs;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nblk; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -2043,38 +2044,93 @@ __global__ void k_plan(const uint8_t* __restrict__ grow, uint64_t n, uint64_t fi
     return;
   }
   // Adaptive: the block starts form a chain over the 32768-value windows
-  // (grow -> +4 windows, else +1).  Stage the flags in shared memory so the
-  // sequential walk runs at shared-memory latency.
+  // (grow -> +4 windows, else +1).  As a scan: the state before window w is
+  // the number of windows still covered by the current block (0 = w starts a
+  // block), and window w maps it by f_w(s) = s ? s - 1 : (grow[w] ? 3 : 0).
+  // The maps compose (4 entries of 2 bits), so one CTA scans them in chunks
+  // of 4096 windows, then compacts the starts into the frame table.
   if (blockIdx.x) return;
-  __shared__ uint8_t s_grow[16384];
-  __shared__ uint32_t s_count;
+  constexpr int kPer = 4, kWarps = kPlanThreads / 32;
+  __shared__ uint32_t s_wmap[kWarps], s_wcnt[kWarps];
+  __shared__ uint32_t s_state, s_count;
+  int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   uint64_t nwin = (n + kBaseQuantum - 1) / kBaseQuantum;
-  if (threadIdx.x == 0) s_count = 0;
-  uint64_t s = 0;
-  for (uint64_t w0 = 0; w0 < nwin; w0 += 16384) {
-    uint64_t wn = qmin(16384, nwin - w0);
-    __syncthreads();
-    for (uint64_t i = threadIdx.x; i < wn; i += blockDim.x) s_grow[i] = grow[w0 + i];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t c = s_count;
-      while (s < n && s / kBaseQuantum < w0 + wn) {
-        uint64_t end = s_grow[s / kBaseQuantum - w0] ? qmin(s + kMaxBlock, n) : qmin(s + kBaseQuantum, n);
-        FrameDesc f;
-        f.value_off = s;
-        f.n = (uint32_t)(end - s);
-        f.payload_off = 0;
-        f.plen = 0;
-        f.mode = 0;
-        f.aux = 0;
-        frames[c++] = f;
-        s = end;
-      }
-      s_count = c;
-    }
+  if (t == 0) {
+    s_state = 0;
+    s_count = 0;
   }
   __syncthreads();
-  if (threadIdx.x == 0) *nb = s_count;
+  auto apply = [](uint32_t m, uint32_t st) { return (m >> (2 * st)) & 3u; };
+  auto compose = [&](uint32_t g, uint32_t f) {  // g after f
+    uint32_t r = 0;
+#pragma unroll
+    for (uint32_t st = 0; st < 4; st++) r |= apply(g, apply(f, st)) << (2 * st);
+    return r;
+  };
+  const uint32_t kId = 0u | (1u << 2) | (2u << 4) | (3u << 6);
+  for (uint64_t w0 = 0; w0 < nwin; w0 += (uint64_t)kPlanThreads * kPer) {
+    uint64_t wb = w0 + (uint64_t)t * kPer;
+    uint8_t g[kPer];
+    uint32_t m = kId;
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+      g[q] = wb + q < nwin ? grow[wb + q] : 0;
+      uint32_t f = wb + q < nwin ? ((g[q] ? 3u : 0u) | (0u << 2) | (1u << 4) | (2u << 6)) : kId;
+      m = compose(f, m);
+    }
+    // inclusive scan of the maps in window order
+    uint32_t inc = m;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc = compose(inc, u);
+    }
+    if (lane == 31) s_wmap[warp] = inc;
+    __syncthreads();
+    uint32_t pre = kId;  // maps of the warps before this one
+    for (int k = 0; k < warp; k++) pre = compose(s_wmap[k], pre);
+    uint32_t ex = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) ex = kId;
+    uint32_t st = apply(compose(ex, pre), s_state);  // state before window wb
+    uint32_t starts = 0;
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+      if (wb + q < nwin && st == 0) starts |= 1u << q;
+      if (wb + q < nwin) st = st ? st - 1 : (g[q] ? 3u : 0u);
+    }
+    uint32_t c = __popc(starts), ci = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t u = __shfl_up_sync(0xffffffffu, ci, o);
+      if (lane >= o) ci += u;
+    }
+    if (lane == 31) s_wcnt[warp] = ci;
+    __syncthreads();
+    uint32_t base = s_count;
+    for (int k = 0; k < warp; k++) base += s_wcnt[k];
+    base += ci - c;
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+      if (!(starts >> q & 1u)) continue;
+      uint64_t s0 = (wb + q) * (uint64_t)kBaseQuantum;
+      uint64_t end = g[q] ? qmin(s0 + kMaxBlock, n) : qmin(s0 + kBaseQuantum, n);
+      FrameDesc f;
+      f.value_off = s0;
+      f.n = (uint32_t)(end - s0);
+      f.payload_off = 0;
+      f.plen = 0;
+      f.mode = 0;
+      f.aux = 0;
+      frames[base++] = f;
+    }
+    __syncthreads();
+    if (t == kPlanThreads - 1) {  // the last thread holds the chunk's final state
+      s_state = st;
+      uint32_t tot = 0;
+      for (int k = 0; k < kWarps; k++) tot += s_wcnt[k];
+      s_count += tot;
+    }
+    __syncthreads();
+  }
+  if (t == 0) *nb = s_count;
 }
 
 __global__ void k_frame_sizes(const FrameDesc* __restrict__ frames, const uint32_t* __restrict__ nbp, uint32_t maxb,
@@ -2099,9 +2155,9 @@ static size_t enc_smem_bytes() { return sizeof(EncSmem); }
 void launch_plan(const uint8_t* grow, uint64_t n, uint64_t fixed_bs, FrameDesc* frames, uint32_t* nb,
                  cudaStream_t st) {
   unsigned g = 1;
-  if (fixed_bs) g = (unsigned)qmin(((n + fixed_bs - 1) / fixed_bs + 255) / 256, 4096);
+  if (fixed_bs) g = (unsigned)qmin(((n + fixed_bs - 1) / fixed_bs + kPlanThreads - 1) / kPlanThreads, 4096);
   if (g == 0) g = 1;
-  k_plan<<<g, 256, 0, st>>>(grow, n, fixed_bs, frames, nb);
+  k_plan<<<g, kPlanThreads, 0, st>>>(grow, n, fixed_bs, frames, nb);
   count_launches(1);
 }
 
