@@ -123,12 +123,18 @@ int quoin_typed_decompress(int32_t dtype, size_t n, const uint8_t *src,
 /* ---------------- B200 extensions ---------------- */
 
 /* Speed/ratio levels (src/lib.rs:93-119).  The GPU competition covers
- * FASTEST and FAST; higher levels return QUOIN_ERR_UNSUPPORTED. */
+ * FASTEST and FAST; higher levels return QUOIN_ERR_UNSUPPORTED.
+ * QUOIN_B200_LEVEL_BALANCED_INPOOL runs Balanced's competition (lambda 2,
+ * rANS-coded FLOAT_MULT / ALP-RD / DICT parts, BYTE_TRANSPOSE; encoder.rs:
+ * 275-469) without its Lz and Pco candidates: its streams are reference
+ * streams (any quoin decoder reads them) and equal Level::Balanced's bytes
+ * wherever neither Lz nor Pco would win a block. */
 #define QUOIN_LEVEL_FASTEST  0
 #define QUOIN_LEVEL_FAST     1
 #define QUOIN_LEVEL_BALANCED 2
 #define QUOIN_LEVEL_HIGH     3
 #define QUOIN_LEVEL_MAX      4
+#define QUOIN_B200_LEVEL_BALANCED_INPOOL 258
 
 /* Stream dtype wire ids (src/dtype.rs:68-78). */
 #define QUOIN_WIRE_F64 0

@@ -41,12 +41,16 @@ class Error(Exception):
 
 
 class Level(enum.IntEnum):
-    """Speed/ratio ladder (reference src/lib.rs:93-119)."""
+    """Speed/ratio ladder (reference src/lib.rs:93-119).  BALANCED_INPOOL is
+    Balanced's competition without its Lz and Pco candidates (lambda 2, the
+    rANS-coded FLOAT_MULT / ALP-RD / DICT parts and BYTE_TRANSPOSE): reference
+    streams, equal to Level.BALANCED's wherever neither Lz nor Pco would win."""
     FASTEST = 0
     FAST = 1
     BALANCED = 2
     HIGH = 3
     MAX = 4
+    BALANCED_INPOOL = 258
 
 
 class Selection(enum.Enum):
@@ -56,7 +60,8 @@ class Selection(enum.Enum):
 @dataclass
 class Config:
     """Encoder configuration (reference src/lib.rs:195-245).  The GPU covers
-    Level.FASTEST and Level.FAST; ``block_size=None`` selects adaptive blocks."""
+    Level.FASTEST, Level.FAST and Level.BALANCED_INPOOL; ``block_size=None``
+    selects adaptive blocks."""
     level: Level = Level.FAST
     block_size: Optional[int] = None
     predictor_log2: int = 16

@@ -159,6 +159,13 @@ union BigArea {
   DictArea dict;
   RleArea rle;
 };
+constexpr uint32_t kRansChunk = 4096;  // bytes staged per step of the serial rANS encoder
+struct RansArea {
+  uint32_t hist[256];
+  uint2 fc[256];                    // (frequency, cumulative frequency) per symbol
+  uint8_t buf[2][kRansChunk];       // double-buffered input bytes
+  uint32_t hdr, emitted;
+};
 
 struct EncSmem {
   uint8_t w_a[kSubsMax];   // FoR widths (also ALP widths in emit)
@@ -180,7 +187,9 @@ struct EncSmem {
   uint64_t red[kEncWarps];
   uint32_t red32[kEncWarps];
   uint64_t sc[8];
+  uint32_t exp_lo, exp_hi;
   BigArea big;
+  RansArea ra;
 };
 
 // ---------------------------------------------------------------------------
@@ -1095,6 +1104,240 @@ __device__ uint32_t* rle_starts(EncSmem& S, const uint64_t* v, uint32_t n, uint3
   return st;
 }
 
+// ---------------------------------------------------------------------------
+// Entropy stage of the Balanced candidate pool (reference entropy/rans.rs:25-108
+// behind the rANS tag of entropy/mod.rs:49-60): static 12-bit frequencies,
+// four interleaved states sharing one byte stream, L = 2^23.  A coded part is
+// [2][varint(m)][varint(symbols)][(symbol, varint(freq))...][4 x u32 states]
+// [bytes].  The encoder runs backward over the input and its state chains
+// are sequential, so thread 0 runs them while the other warps stage the next
+// 4096 input bytes in shared memory.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kRansM = 4096, kRansL = 1u << 23;
+
+// Histogram of byte_at(0 .. m) and the normalised frequencies (rans.rs:25-48:
+// f = max(1, c * 4096 / m); while the sum exceeds 4096 the largest f > 1 loses
+// one, ties to the highest symbol; a short sum goes to the largest f, ties to
+// the highest symbol).  Returns the header length after the tag byte.
+template <class B>
+__device__ uint32_t rans_plan(RansArea& R, uint32_t m, B byte_at) {
+  int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int i = t; i < 256; i += blockDim.x) R.hist[i] = 0;
+  __syncthreads();
+  for (uint32_t base = (uint32_t)warp * 32; base < m; base += blockDim.x) {
+    uint32_t i = base + lane;
+    uint32_t sym = i < m ? (uint32_t)byte_at(i) : 256u;
+    uint32_t peers = __match_any_sync(0xffffffffu, sym);
+    if (sym < 256 && lane == __ffs(peers) - 1) atomicAdd(&R.hist[sym], (uint32_t)__popc(peers));
+  }
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t f[8], sum = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      uint32_t c = R.hist[lane + 32 * j];
+      uint32_t q = (uint32_t)(((uint64_t)c * kRansM) / m);
+      f[j] = c ? (q ? q : 1u) : 0u;
+      sum += f[j];
+    }
+    sum = warp_sum(sum);
+    while (sum > kRansM) {
+      uint32_t key = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        if (f[j] > 1) key = max(key, (f[j] << 8) | (uint32_t)(lane + 32 * j));
+      key = warp_max(key);
+      uint32_t sym = key & 255u;
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        if ((uint32_t)(lane + 32 * j) == sym) f[j]--;
+      sum--;
+    }
+    if (sum < kRansM) {
+      uint32_t key = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) key = max(key, (f[j] << 8) | (uint32_t)(lane + 32 * j));
+      key = warp_max(key);
+      uint32_t sym = key & 255u;
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        if ((uint32_t)(lane + 32 * j) == sym) f[j] += kRansM - sum;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; j++) R.fc[lane + 32 * j].x = f[j];
+    __syncwarp();
+    if (lane == 0) {
+      uint32_t c = 0, present = 0, h = 0;
+      for (int sym = 0; sym < 256; sym++) {
+        uint32_t fs = R.fc[sym].x;
+        R.fc[sym].y = c;
+        c += fs;
+        if (fs) {
+          present++;
+          h += 1 + varint_len(fs);
+        }
+      }
+      R.hdr = varint_len(m) + varint_len(present) + h;
+    }
+  }
+  __syncthreads();
+  uint32_t hdr = R.hdr;
+  __syncthreads();
+  return hdr;
+}
+
+// Header of a coded part (after its tag byte), from the planned frequencies.
+__device__ void rans_put_header(const RansArea& R, uint32_t m, uint8_t* out) {
+  uint32_t present = 0;
+  for (int sym = 0; sym < 256; sym++) present += R.fc[sym].x ? 1u : 0u;
+  uint32_t pos = put_varint(out, m);
+  pos += put_varint(out + pos, present);
+  for (int sym = 0; sym < 256; sym++)
+    if (R.fc[sym].x) {
+      out[pos++] = (uint8_t)sym;
+      pos += put_varint(out + pos, R.fc[sym].x);
+    }
+}
+
+// Renormalisation of one state before coding a symbol of frequency f: bytes
+// leave from the low end while x >= f * 2^19 ((L >> 12) << 8 = 2^19).
+template <bool WRITE>
+__device__ __forceinline__ void rans_renorm(uint32_t& x, uint32_t f, uint32_t& e, uint8_t*& p) {
+  uint32_t xm = f << 19;
+  while (x >= xm) {
+    if (WRITE) *--p = (uint8_t)x;
+    x >>= 8;
+    e++;
+  }
+}
+__device__ __forceinline__ uint32_t rans_code(uint32_t x, uint2 fc) {
+  return ((x / fc.x) << 12) + (x % fc.x) + fc.y;
+}
+
+// The encoder pass over byte_at(m - 1 .. 0) with the planned frequencies.
+// Returns the number of stream bytes; WRITE stores them ending at `wend` and
+// the four final states in the 16 bytes before the first of them.
+template <bool WRITE, class B>
+__device__ uint32_t rans_run(RansArea& R, uint32_t m, B byte_at, uint8_t* wend) {
+  int t = threadIdx.x, warp = t >> 5;
+  uint32_t nch = (m + kRansChunk - 1) / kRansChunk;
+  auto fill = [&](uint32_t c, int slot) {  // warps 1.. stage chunk c
+    uint32_t lo = c * kRansChunk, hi = min(lo + kRansChunk, m);
+    for (uint32_t i = lo + (uint32_t)(t - 32); i < hi; i += blockDim.x - 32) R.buf[slot][i - lo] = (uint8_t)byte_at(i);
+  };
+  if (warp && nch) fill(nch - 1, 0);
+  __syncthreads();
+  uint32_t x0 = kRansL, x1 = kRansL, x2 = kRansL, x3 = kRansL, e = 0;
+  uint8_t* p = wend;
+  for (uint32_t k = 0; k < nch; k++) {
+    uint32_t c = nch - 1 - k;
+    if (warp && c > 0) fill(c - 1, (int)((k + 1) & 1));
+    if (t == 0) {
+      const uint8_t* bb = R.buf[k & 1];
+      uint32_t lo = c * kRansChunk, i = min(lo + kRansChunk, m);
+      while (i > lo && (i & 3)) {  // the top of the input, one step at a time
+        i--;
+        uint2 fc = R.fc[bb[i - lo]];
+        uint32_t& x = (i & 3) == 3 ? x3 : (i & 3) == 2 ? x2 : (i & 3) == 1 ? x1 : x0;
+        rans_renorm<WRITE>(x, fc.x, e, p);
+        x = rans_code(x, fc);
+      }
+      while (i > lo) {  // steps i-1 .. i-4 code with states 3, 2, 1, 0
+        i -= 4;
+        uint2 f3 = R.fc[bb[i + 3 - lo]], f2 = R.fc[bb[i + 2 - lo]], f1 = R.fc[bb[i + 1 - lo]],
+              f0 = R.fc[bb[i - lo]];
+        rans_renorm<WRITE>(x3, f3.x, e, p);
+        rans_renorm<WRITE>(x2, f2.x, e, p);
+        rans_renorm<WRITE>(x1, f1.x, e, p);
+        rans_renorm<WRITE>(x0, f0.x, e, p);
+        x3 = rans_code(x3, f3);
+        x2 = rans_code(x2, f2);
+        x1 = rans_code(x1, f1);
+        x0 = rans_code(x0, f0);
+      }
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    if (WRITE) {
+      put_u32(p - 16, x0);
+      put_u32(p - 12, x1);
+      put_u32(p - 8, x2);
+      put_u32(p - 4, x3);
+    }
+    R.emitted = e;
+  }
+  __syncthreads();
+  uint32_t r = R.emitted;
+  __syncthreads();
+  return r;
+}
+
+// Length of code_residuals(byte_at(0 .. m)) with the rANS tag: the coded part
+// entropy_pick keeps at lambda >= 2 (m > 0).
+template <class B>
+__device__ uint32_t coded_len(RansArea& R, uint32_t m, B byte_at) {
+  uint32_t h = rans_plan(R, m, byte_at);
+  return 1 + h + 16 + rans_run<false>(R, m, byte_at, nullptr);
+}
+
+// Writes the coded part of byte_at(0 .. m) whose length (tag included) is len.
+template <class B>
+__device__ void coded_write(RansArea& R, uint32_t m, B byte_at, uint8_t* out, uint32_t len) {
+  rans_plan(R, m, byte_at);
+  if (threadIdx.x == 0) {
+    out[0] = 2;
+    rans_put_header(R, m, out + 1);
+  }
+  rans_run<true>(R, m, byte_at, out + len);
+}
+
+// FLOAT_MULT's entropy form (float_mult.rs:66-98): LEB128(zigzag(k_i - k_{i-1}))
+// with k_{-1} = 0, written to dst; returns the byte count.  Thread t writes a
+// contiguous run of values at offsets from a block scan of their lengths.
+__device__ uint32_t fm_delta_bytes(EncSmem& S, const uint64_t* v, uint32_t n, int sc, uint8_t* dst) {
+  int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  uint32_t seg = (n + blockDim.x - 1) / blockDim.x;
+  uint32_t i0 = min((uint32_t)t * seg, n), i1 = min(i0 + seg, n);
+  uint32_t len = 0;
+  int64_t prev = i0 ? fm_k(v[i0 - 1], sc) : 0;
+  for (uint32_t i = i0; i < i1; i++) {
+    int64_t k = fm_k(v[i], sc);
+    len += varint_len(zigzag64((uint64_t)k - (uint64_t)prev));
+    prev = k;
+  }
+  uint32_t inc = warp_incl_scan(len);
+  if (lane == 31) S.red32[warp] = inc;
+  __syncthreads();
+  uint32_t off = inc - len, tot = 0;
+  for (int w = 0; w < kEncWarps; w++) {
+    if (w < warp) off += S.red32[w];
+    tot += S.red32[w];
+  }
+  prev = i0 ? fm_k(v[i0 - 1], sc) : 0;
+  for (uint32_t i = i0; i < i1; i++) {
+    int64_t k = fm_k(v[i], sc);
+    off += put_varint(dst + off, zigzag64((uint64_t)k - (uint64_t)prev));
+    prev = k;
+  }
+  __syncthreads();
+  return tot;
+}
+
+// The entropy parts chosen for a block (Balanced in-pool), read by k_emit.
+// Lengths include the rANS tag byte.
+constexpr uint32_t kEntFm = 1, kEntRdCodes = 2, kEntRdRights = 4, kEntDictVals = 8, kEntDictCodes = 16;
+struct EntRec {
+  uint32_t flags;
+  uint32_t fm;      // FLOAT_MULT coded deltas
+  uint32_t rdc;     // ALP-RD coded codes
+  uint32_t rdr;     // ALP-RD coded rights (the bit-packed rights bytes)
+  uint32_t bt;      // BYTE_TRANSPOSE payload
+  uint32_t dv;      // DICT coded transposed values
+  uint32_t dc[2];   // DICT coded code planes
+};
+static_assert(sizeof(EntRec) == 32, "EntRec layout");
+
 struct Cand {
   uint64_t len;
   bool ok;
@@ -1368,13 +1611,17 @@ __device__ uint32_t popc_bits_block(EncSmem& S, const uint32_t* bits) {
   return t;
 }
 
+// ENT: the Balanced in-pool competition, with the rANS-coded forms of
+// FLOAT_MULT, ALP-RD and DICT and the BYTE_TRANSPOSE candidate; the chosen
+// coded parts go to ent[b] for the emission.
+template <bool ENT>
 __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restrict__ lane, FrameDesc* frames,
                                                         const uint32_t* __restrict__ nbp, uint64_t fixed_bs,
                                                         int dtype, int level, const SubStats* __restrict__ ss,
                                                         const FmStat* __restrict__ fms,
                                                         const uint64_t* __restrict__ smp16,
                                                         const uint32_t* __restrict__ winbits,
-                                                        uint8_t* __restrict__ scratch) {
+                                                        uint8_t* __restrict__ scratch, EntRec* __restrict__ ent) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   EncSmem& S = *reinterpret_cast<EncSmem*>(smem_raw);
   uint32_t b = blockIdx.x;
@@ -1393,6 +1640,7 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
   uint64_t g0 = fixed_bs ? (uint64_t)b * ((fixed_bs + kSub - 1) / kSub) : fd.value_off / kSub;
   int t = threadIdx.x, lane_id = t & 31, warp = t >> 5;
   uint32_t step = max(n / 2048u, 1u);
+  EntRec er = {0, 0, 0, 0, 0, 0, {0, 0}};
   // Early-out samples from the statistics when the block is a full adaptive block.
   bool pre_e = !fixed_bs && (step == 16 || step == 64) && (fd.value_off % kBaseQuantum) == 0;
   if (t == 0) {
@@ -1537,6 +1785,15 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
       __syncthreads();
       c_fm.ok = true;
       c_fm.len = 2 + vl + tot;
+      if (ENT) {  // FM_ENTROPY, kept when strictly smaller (float_mult.rs:80-92)
+        uint32_t m = fm_delta_bytes(S, v, n, (int)fm_scale, scr);
+        uint32_t el = coded_len(S.ra, m, [&](uint32_t i) { return (uint32_t)scr[i]; });
+        if (el < c_fm.len - 2) {
+          c_fm.len = 2 + el;
+          er.flags |= kEntFm;
+          er.fm = el;
+        }
+      }
     }
     c_alp.ok = !S.alp_fail;  // ALP (alp.rs:93-166)
     c_alp.len = sz_alp;
@@ -1583,19 +1840,32 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
         }
       }
       __syncthreads();
-      if (t == 0) {
-        uint64_t nexc = S.cnt32;
-        uint64_t clen = vl, rlen = vl;
-        for (uint32_t k = 0; k < nsub; k++) {
-          clen += 9 + 128ull * S.w_a[k];
-          rlen += 9 + 128ull * S.w_b[k];
-        }
-        S.sc[5] = (nexc * 4 > n) ? 0ull
-                                 : 2 + 8ull * S.dl + varint_len(nexc) + S.acc64 + 1 + varint_len(clen) + clen + 1 + rlen;
+      uint64_t nexc = S.cnt32, excb = S.acc64, clen = vl, rlen = vl;
+      for (uint32_t k = 0; k < nsub; k++) {
+        clen += 9 + 128ull * S.w_a[k];
+        rlen += 9 + 128ull * S.w_b[k];
       }
+      c_rd.ok = nexc * 4 <= n;
+      if (ENT && c_rd.ok) {  // T_ENT codes / rights, kept when strictly smaller (alp_rd.rs:176-200)
+        uint32_t cl = coded_len(S.ra, n, [&](uint32_t i) {
+          int c = rd_code(S, v[i] >> rbw);
+          return (uint32_t)(c < 0 ? 0 : c);
+        });
+        if (cl < clen) {
+          clen = cl;
+          er.flags |= kEntRdCodes;
+          er.rdc = cl;
+        }
+        uint32_t rb = (uint32_t)block_for(S, scr, n, false, [&](uint32_t i) { return v[i] & rmask; });
+        uint32_t rl = coded_len(S.ra, rb, [&](uint32_t i) { return (uint32_t)scr[i]; });
+        if (rl < rlen) {
+          rlen = rl;
+          er.flags |= kEntRdRights;
+          er.rdr = rl;
+        }
+      }
+      c_rd.len = 2 + 8ull * S.dl + varint_len(nexc) + excb + 1 + varint_len(clen) + clen + 1 + rlen;
       __syncthreads();
-      c_rd.ok = S.sc[5] != 0;
-      c_rd.len = S.sc[5];
     }
   }
 
@@ -1621,6 +1891,38 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
   if (c_rd.ok) consider(M_ALP_RD, c_rd.len);
   bool block_compressible = best_len * 20 < raw_bytes * 19;  // encoder.rs:394,644-646
 
+  if (ENT && block_compressible) {
+    // BYTE_TRANSPOSE (encoder.rs:414-420) when the exponent-field range is at
+    // most 64 or most consecutive values repeat (encoder.rs:705-750)
+    if (t == 0) {
+      S.exp_lo = 0x7FF;
+      S.exp_hi = 0;
+    }
+    __syncthreads();
+    uint32_t elo = 0x7FF, ehi = 0;
+    for (uint32_t i = t; i < n; i += blockDim.x) {
+      uint32_t ex = (uint32_t)(v[i] >> 52) & 0x7FFu;
+      elo = min(elo, ex);
+      ehi = max(ehi, ex);
+    }
+    elo = warp_min(elo);
+    ehi = warp_max(ehi);
+    if (lane_id == 0) {
+      atomicMin(&S.exp_lo, elo);
+      atomicMax(&S.exp_hi, ehi);
+    }
+    __syncthreads();
+    bool repeats = (uint64_t)(n - S.neq) * 2 > (uint64_t)n;
+    if (S.exp_hi - S.exp_lo <= 64 || repeats) {
+      uint32_t bl = coded_len(S.ra, 8 * n, [&](uint32_t i) {
+        uint32_t pl = i / n;
+        return (uint32_t)(v[i - pl * n] >> (8 * pl)) & 255u;
+      });
+      er.bt = bl;
+      consider(M_BYTE_TRANSPOSE, bl);
+    }
+  }
+
   if (block_compressible && !reduced) {
     // DICT (dict.rs:87-152, bit-packed codes).  The dictionary is sorted, so
     // a sub-block's code range is [rank(min), rank(max)].
@@ -1630,6 +1932,20 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
     if (!S.flag) {
       uint32_t vtag;
       uint64_t vlen = dict_values_len(S, dv, &vtag);
+      if (ENT) {  // TRANSPOSE values, kept when strictly smaller (dict.rs:52-59)
+        const uint64_t* sv = dv.sorted;
+        uint32_t card = dv.card;
+        uint32_t tl = coded_len(S.ra, 8 * card, [&](uint32_t i) {
+          uint32_t pl = i / card;
+          return (uint32_t)(sv[i - pl * card] >> (8 * pl)) & 255u;
+        });
+        if (tl < vlen) {
+          vlen = tl;
+          vtag = 2;
+          er.flags |= kEntDictVals;
+          er.dv = tl;
+        }
+      }
       uint64_t my = 0;
       for (uint32_t k = t; k < nsub; k += blockDim.x) {
         uint32_t r0 = dict_rank(S, dv, S.item_min[k]), r1 = dict_rank(S, dv, S.item_max[k]);
@@ -1641,6 +1957,21 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
       uint64_t clen = vl;
       for (int w = 0; w < kEncWarps; w++) clen += S.red[w];
       __syncthreads();
+      if (ENT && dv.card <= 65536u) {  // CODES_ENTROPY byte planes, kept when strictly smaller (dict.rs:128-145)
+        uint32_t nb = dv.card <= 256u ? 1u : 2u;
+        uint64_t el = 1;
+        uint32_t pls[2] = {0, 0};
+        for (uint32_t pl = 0; pl < nb; pl++) {
+          pls[pl] = coded_len(S.ra, n, [&](uint32_t i) { return (dict_rank(S, dv, v[i]) >> (8 * pl)) & 255u; });
+          el += varint_len(pls[pl]) + pls[pl];
+        }
+        if (el < clen) {
+          clen = el;
+          er.flags |= kEntDictCodes;
+          er.dc[0] = pls[0];
+          er.dc[1] = pls[1];
+        }
+      }
       consider(M_DICT, varint_len(dv.card) + 1 + varint_len(vlen) + vlen + 1 + clen);
     }
     __syncthreads();
@@ -1660,6 +1991,7 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
     frames[b].plen = (uint32_t)best_len;
     frames[b].aux = best_mode == M_FLOAT_MULT ? fm_scale : best_mode == M_ALP_RD ? rd_lbw : 0;
     atomicAdd(&g_wins[best_mode], 1ull);
+    if (ENT) ent[b] = er;
   }
 }
 
@@ -1799,7 +2131,8 @@ __device__ void emit_alp(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* out
   }
 }
 
-__device__ void emit_alprd(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t lbw, uint8_t* scr, uint8_t* out) {
+__device__ void emit_alprd(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t lbw, uint8_t* scr, uint8_t* out,
+                           const EntRec* er) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t nsub = (n + kSub - 1) / kSub;
   rd_top8(S, v, n, lbw, scr);
@@ -1863,22 +2196,44 @@ __device__ void emit_alprd(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t l
     int c = rd_code(S, v[i] >> rbw);
     return c < 0 ? 0ull : (uint64_t)c;
   };
-  uint64_t clen = block_for(S, nullptr, n, false, code_of);
-  uint32_t cvl = varint_len(clen);
-  if (threadIdx.x == 0) {
-    put_u8(out + pos, 0);
-    put_varint(out + pos + 1, clen);
+  uint64_t rpos;
+  if (er && (er->flags & kEntRdCodes)) {
+    uint32_t clen = er->rdc, cvl = varint_len(clen);
+    if (threadIdx.x == 0) {
+      put_u8(out + pos, 1);
+      put_varint(out + pos + 1, clen);
+    }
+    coded_write(S.ra, n, [&](uint32_t i) { return (uint32_t)code_of(i); }, out + pos + 1 + cvl, clen);
+    rpos = pos + 1 + cvl + clen;
+  } else {
+    uint64_t clen = block_for(S, nullptr, n, false, code_of);
+    uint32_t cvl = varint_len(clen);
+    if (threadIdx.x == 0) {
+      put_u8(out + pos, 0);
+      put_varint(out + pos + 1, clen);
+    }
+    block_for(S, out + pos + 1 + cvl, n, false, code_of);
+    rpos = pos + 1 + cvl + clen;
   }
-  block_for(S, out + pos + 1 + cvl, n, false, code_of);
-  uint64_t rpos = pos + 1 + cvl + clen;
-  if (threadIdx.x == 0) put_u8(out + rpos, 0);
-  block_for(S, out + rpos + 1, n, false, [&](uint32_t i) { return v[i] & rmask; });
+  auto right_of = [&](uint32_t i) { return v[i] & rmask; };
+  if (er && (er->flags & kEntRdRights)) {  // the bit-packed rights, coded
+    uint32_t rb = (uint32_t)block_for(S, scr, n, false, right_of);
+    if (threadIdx.x == 0) put_u8(out + rpos, 1);
+    coded_write(S.ra, rb, [&](uint32_t i) { return (uint32_t)scr[i]; }, out + rpos + 1, er->rdr);
+  } else {
+    if (threadIdx.x == 0) put_u8(out + rpos, 0);
+    block_for(S, out + rpos + 1, n, false, right_of);
+  }
 }
 
-__device__ void emit_dict(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scr, uint8_t* out) {
+__device__ void emit_dict(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scr, uint8_t* out, const EntRec* er) {
   DictView dv = dict_prepare(S, v, n, scr, kNoLb);
   uint32_t vtag;
   uint64_t vlen = dict_values_len(S, dv, &vtag);
+  if (er && (er->flags & kEntDictVals)) {
+    vtag = 2;
+    vlen = er->dv;
+  }
   uint64_t pos = 0;
   if (threadIdx.x == 0) {
     pos = put_varint(out, dv.card);
@@ -1889,14 +2244,36 @@ __device__ void emit_dict(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* sc
   __syncthreads();
   pos = S.sc[6];
   const uint64_t* s = dv.sorted;
+  uint32_t card = dv.card;
   if (vtag == 0) {
-    for (uint32_t i = threadIdx.x; i < dv.card; i += blockDim.x) put_u64(out + pos + 8ull * i, s[i]);
-  } else {
+    for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) put_u64(out + pos + 8ull * i, s[i]);
+  } else if (vtag == 1) {
     if (threadIdx.x == 0) put_u64(out + pos, s[0]);
-    block_for(S, out + pos + 8, dv.card, false, [&](uint32_t i) { return zigzag64(s[i] - (i ? s[i - 1] : s[0])); });
+    block_for(S, out + pos + 8, card, false, [&](uint32_t i) { return zigzag64(s[i] - (i ? s[i - 1] : s[0])); });
+  } else {
+    coded_write(S.ra, 8 * card, [&](uint32_t i) {
+      uint32_t pl = i / card;
+      return (uint32_t)(s[i - pl * card] >> (8 * pl)) & 255u;
+    }, out + pos, (uint32_t)vlen);
   }
   __syncthreads();
   pos += vlen;
+  if (er && (er->flags & kEntDictCodes)) {  // nplanes, then varint(len) + coded plane each
+    uint32_t nb = card <= 256u ? 1u : 2u;
+    if (threadIdx.x == 0) {
+      put_u8(out + pos, 1);
+      put_u8(out + pos + 1, nb);
+    }
+    pos += 2;
+    for (uint32_t pl = 0; pl < nb; pl++) {
+      uint32_t len = er->dc[pl];
+      if (threadIdx.x == 0) put_varint(out + pos, len);
+      pos += varint_len(len);
+      coded_write(S.ra, n, [&](uint32_t i) { return (dict_rank(S, dv, v[i]) >> (8 * pl)) & 255u; }, out + pos, len);
+      pos += len;
+    }
+    return;
+  }
   if (threadIdx.x == 0) put_u8(out + pos, 0);
   block_for(S, out + pos + 1, n, false, [&](uint32_t i) { return (uint64_t)dict_rank(S, dv, v[i]); });
 }
@@ -1931,13 +2308,14 @@ __device__ void emit_rle(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scr
             [&](uint32_t r) { return (uint64_t)((r + 1 < runs ? st[r + 1] : n) - st[r]); });
 }
 
+template <bool ENT>
 __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict__ lane,
                                                       const FrameDesc* __restrict__ frames,
                                                       const uint32_t* __restrict__ nbp, uint64_t fixed_bs, int dtype,
                                                       const SubStats* __restrict__ ss,
                                                       const FmStat* __restrict__ fms,
                                                       uint8_t* __restrict__ scratch, uint8_t* __restrict__ outbuf,
-                                                      uint64_t out_cap) {
+                                                      uint64_t out_cap, const EntRec* __restrict__ ent) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   EncSmem& S = *reinterpret_cast<EncSmem*>(smem_raw);
   uint32_t b = blockIdx.x;
@@ -1960,6 +2338,9 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
   uint32_t nsub = (n + kSub - 1) / kSub;
   uint64_t g0 = fixed_bs ? (uint64_t)b * ((fixed_bs + kSub - 1) / kSub) : fd.value_off / kSub;
   int m = (int)fd.mode;
+  EntRec er = {0, 0, 0, 0, 0, 0, {0, 0}};
+  if (ENT) er = ent[b];
+  const EntRec* erp = ENT ? &er : nullptr;
   if (m == M_FOR_BITPACK || m == M_DELTA_BITPACK || m == M_FLOAT_MULT || m == M_XORZ) {
     for (uint32_t k = threadIdx.x; k < nsub; k += blockDim.x) {
       const SubStats& R = ss[g0 + k];
@@ -2005,16 +2386,29 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
       break;
     case M_FLOAT_MULT: {
       int s = (int)fd.aux;
+      bool coded = ENT && (er.flags & kEntFm);
       if (threadIdx.x == 0) {
-        put_u8(out, 0);
+        put_u8(out, coded ? 1 : 0);
         put_u8(out + 1, s);
       }
-      block_for_write(S, out + 2, n, [&](uint32_t i) { return (uint64_t)fm_k(v[i], s); });
+      if (coded) {
+        uint32_t mb = fm_delta_bytes(S, v, n, s, scr);
+        coded_write(S.ra, mb, [&](uint32_t i) { return (uint32_t)scr[i]; }, out + 2, er.fm);
+      } else {
+        block_for_write(S, out + 2, n, [&](uint32_t i) { return (uint64_t)fm_k(v[i], s); });
+      }
       break;
     }
+    case M_BYTE_TRANSPOSE:  // transpose.rs:10-32 (Balanced in-pool only)
+      if (ENT)
+        coded_write(S.ra, 8 * n, [&](uint32_t i) {
+          uint32_t pl = i / n;
+          return (uint32_t)(v[i - pl * n] >> (8 * pl)) & 255u;
+        }, out, fd.plen);
+      break;
     case M_ALP: emit_alp(S, v, n, out); break;
-    case M_ALP_RD: emit_alprd(S, v, n, fd.aux, scr, out); break;
-    case M_DICT: emit_dict(S, v, n, scr, out); break;
+    case M_ALP_RD: emit_alprd(S, v, n, fd.aux, scr, out, erp); break;
+    case M_DICT: emit_dict(S, v, n, scr, out, erp); break;
     case M_RLE: emit_rle(S, v, n, scr, out); break;
     default: break;
   }
@@ -2184,24 +2578,42 @@ void launch_sub_stats(const uint64_t* lane, uint64_t n, uint64_t fixed_bs, int d
 
 void launch_decide(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, uint64_t fixed_bs,
                    int dtype, int level, const void* ss, const void* fms, const uint64_t* smp16,
-                   const uint32_t* winbits, uint8_t* scratch, cudaStream_t st) {
-  cudaFuncSetAttribute(k_decide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)enc_smem_bytes());
-  cudaFuncSetAttribute(k_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)enc_smem_bytes());
-  if (max_blocks)
-    k_decide<<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, fixed_bs, dtype, level,
-                                                                (const SubStats*)ss, (const FmStat*)fms, smp16,
-                                                                winbits, scratch);
+                   const uint32_t* winbits, uint8_t* scratch, void* ent, cudaStream_t st) {
+  int sm = (int)enc_smem_bytes();
+  cudaFuncSetAttribute(k_decide<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_decide<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_emit<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_emit<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (max_blocks) {
+    if (ent)
+      k_decide<true><<<max_blocks, kEncThreads, sm, st>>>(lane, frames, nb, fixed_bs, dtype, level,
+                                                          (const SubStats*)ss, (const FmStat*)fms, smp16, winbits,
+                                                          scratch, (EntRec*)ent);
+    else
+      k_decide<false><<<max_blocks, kEncThreads, sm, st>>>(lane, frames, nb, fixed_bs, dtype, level,
+                                                           (const SubStats*)ss, (const FmStat*)fms, smp16, winbits,
+                                                           scratch, nullptr);
+  }
   count_launches(max_blocks ? 1 : 0);
 }
 
 void launch_emit(const uint64_t* lane, const FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks,
                  uint64_t fixed_bs, int dtype, const void* ss, const void* fms, uint8_t* scratch, uint8_t* out,
-                 uint64_t out_cap, cudaStream_t st) {
-  if (max_blocks)
-    k_emit<<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, fixed_bs, dtype, (const SubStats*)ss,
-                                                              (const FmStat*)fms, scratch, out, out_cap);
+                 uint64_t out_cap, const void* ent, cudaStream_t st) {
+  if (max_blocks) {
+    if (ent)
+      k_emit<true><<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, fixed_bs, dtype,
+                                                                      (const SubStats*)ss, (const FmStat*)fms,
+                                                                      scratch, out, out_cap, (const EntRec*)ent);
+    else
+      k_emit<false><<<max_blocks, kEncThreads, enc_smem_bytes(), st>>>(lane, frames, nb, fixed_bs, dtype,
+                                                                       (const SubStats*)ss, (const FmStat*)fms,
+                                                                       scratch, out, out_cap, nullptr);
+  }
   count_launches(max_blocks ? 1 : 0);
 }
+
+uint64_t ent_rec_bytes() { return sizeof(EntRec); }
 
 unsigned long long* device_win_counters() {
   void* p = nullptr;

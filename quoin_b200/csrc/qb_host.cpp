@@ -195,7 +195,7 @@ inline int plain_code(int ext) {
 enum Slot {
   S_IN, S_BM, S_RANK, S_LANE, S_GROW, S_FRAMES, S_NB, S_SIZES, S_TILE, S_SCRATCH, S_OUT, S_VTMP, S_VBLOB,
   S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_DAUX, S_SUBST, S_FMST,
-  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_ENT, S_COUNT
+  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_ENT, S_ENTREC, S_COUNT
 };
 
 struct QuoinCtx {
@@ -365,6 +365,11 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
     CK(c->ensure(S_FMST, (items + 1) * fm_stats_bytes()));
     CK(c->ensure(S_SMP16, (n / 16 + 2) * 8));
   }
+  void* ent = nullptr;  // Balanced in-pool: the chosen rANS-coded parts per block
+  if (j.level >= 2) {
+    CK(c->ensure(S_ENTREC, maxb * ent_rec_bytes()));
+    ent = c->p<void>(S_ENTREC);
+  }
   FrameDesc* fr = c->p<FrameDesc>(S_FRAMES);
   uint32_t* nb = c->p<uint32_t>(S_NB);
   {
@@ -377,7 +382,7 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
     TimedRegion tr(T_COMPETE, st);
     launch_decide(j.lane, fr, nb, (uint32_t)maxb, bs, j.dtype, j.level, c->p<void>(S_SUBST),
                   fl ? c->p<void>(S_FMST) : nullptr, fl ? c->p<uint64_t>(S_SMP16) : nullptr,
-                  c->p<uint32_t>(S_WINBITS), c->p<uint8_t>(S_SCRATCH), st);
+                  c->p<uint32_t>(S_WINBITS), c->p<uint8_t>(S_SCRATCH), ent, st);
   }
   {
     TimedRegion tr(T_OTHER, st);
@@ -387,7 +392,7 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
   {  // frames past dst_cap are skipped on the device; the total decides afterwards
     TimedRegion tr(T_EMIT, st);
     launch_emit(j.lane, fr, nb, (uint32_t)maxb, bs, j.dtype, c->p<void>(S_SUBST), fl ? c->p<void>(S_FMST) : nullptr,
-                c->p<uint8_t>(S_SCRATCH), d_dst, dst_cap, st);
+                c->p<uint8_t>(S_SCRATCH), d_dst, dst_cap, ent, st);
   }
   uint64_t hm[2] = {0, 0};
   CK(cudaMemcpyAsync(hm, d_misc, 16, cudaMemcpyDeviceToHost, st));
@@ -402,8 +407,12 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
 
 int check_level(const QuoinConfig* cfg, int* level, uint64_t* bs, uint8_t* plog2) {
   int lv = cfg ? cfg->level : QUOIN_LEVEL_FAST;
-  if (lv < 0 || lv > 4) return QUOIN_ERR_BAD_ARG;
-  if (lv >= QUOIN_LEVEL_BALANCED) return QUOIN_ERR_UNSUPPORTED;
+  if (lv == QUOIN_B200_LEVEL_BALANCED_INPOOL) {
+    lv = QUOIN_LEVEL_BALANCED;  // Balanced's candidate pool without Lz and Pco
+  } else {
+    if (lv < 0 || lv > 4) return QUOIN_ERR_BAD_ARG;
+    if (lv >= QUOIN_LEVEL_BALANCED) return QUOIN_ERR_UNSUPPORTED;
+  }
   int64_t b = cfg ? cfg->block_size : 0;
   int32_t p = cfg ? cfg->predictor_log2 : 16;
   *level = lv;

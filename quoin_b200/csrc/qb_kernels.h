@@ -81,9 +81,13 @@ void launch_sub_stats(const uint64_t* lane, uint64_t n, uint64_t fixed_bs, int d
 void launch_plan(const uint8_t* grow, uint64_t n, uint64_t fixed_bs, FrameDesc* frames, uint32_t* nb,
                  cudaStream_t st);
 // Competition part 2: one CTA per planned block; writes mode / plen / aux.
+// With `ent` (max_blocks records of ent_rec_bytes()) the Balanced in-pool
+// candidates run too (rANS-coded parts, BYTE_TRANSPOSE) and their choices
+// are recorded there for the emission.
 void launch_decide(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, uint64_t fixed_bs,
                    int dtype, int level, const void* ss, const void* fms, const uint64_t* smp16,
-                   const uint32_t* winbits, uint8_t* scratch, cudaStream_t st);
+                   const uint32_t* winbits, uint8_t* scratch, void* ent, cudaStream_t st);
+uint64_t ent_rec_bytes();
 // `base` (device) holds the byte offset at which the first frame starts.
 void launch_frame_offsets(FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, const uint64_t* base,
                           uint64_t* sizes_tmp, uint64_t* tile_tmp, uint64_t* total, cudaStream_t st);
@@ -92,7 +96,7 @@ void launch_frame_offsets(FrameDesc* frames, const uint32_t* nb, uint32_t max_bl
 // out_cap bytes are not written.
 void launch_emit(const uint64_t* lane, const FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks,
                  uint64_t fixed_bs, int dtype, const void* ss, const void* fms, uint8_t* scratch, uint8_t* out,
-                 uint64_t out_cap, cudaStream_t st);
+                 uint64_t out_cap, const void* ent, cudaStream_t st);
 
 // ---- lowering / validity (qb_lower.cu) ----
 // Lower n native values (dtype width) to the u64 lane, keeping only positions
