@@ -1201,9 +1201,11 @@ __device__ void rans_put_header(const RansArea& R, uint32_t m, uint8_t* out) {
 
 // Renormalisation of one state before coding a symbol of frequency f: bytes
 // leave from the low end while x >= f * 2^19 ((L >> 12) << 8 = 2^19).
+// (f >= 1 for every symbol the histogram saw; the max keeps the loop finite
+// whatever the input.)
 template <bool WRITE>
 __device__ __forceinline__ void rans_renorm(uint32_t& x, uint32_t f, uint32_t& e, uint8_t*& p) {
-  uint32_t xm = f << 19;
+  uint32_t xm = max(f, 1u) << 19;
   while (x >= xm) {
     if (WRITE) *--p = (uint8_t)x;
     x >>= 8;
@@ -1211,8 +1213,19 @@ __device__ __forceinline__ void rans_renorm(uint32_t& x, uint32_t f, uint32_t& e
   }
 }
 __device__ __forceinline__ uint32_t rans_code(uint32_t x, uint2 fc) {
-  return ((x / fc.x) << 12) + (x % fc.x) + fc.y;
+  uint32_t f = max(fc.x, 1u);
+  return ((x / f) << 12) + (x % f) + fc.y;
 }
+
+// Destination of a bit-packed stream of `len` bytes that a block stages for
+// rANS: its scratch range (32 B per value) when it fits, else the shared
+// big area, free once the ALP-RD dictionary is in S.dict8 (a sub-block pads
+// to 1024 values, so a block of fewer than 257 values can exceed its range;
+// such a stream is at most varint(n) + 9 + 128 * 64 bytes).
+__device__ __forceinline__ uint8_t* stage_dst(EncSmem& S, uint8_t* scr, uint32_t n, uint64_t len) {
+  return len <= 32ull * n ? scr : reinterpret_cast<uint8_t*>(&S.big);
+}
+static_assert(sizeof(BigArea) >= 3 + 9 + 128 * 64, "staged bit-packed stream of a short block");
 
 // The encoder pass over byte_at(m - 1 .. 0) with the planned frequencies.
 // Returns the number of stream bytes; WRITE stores them ending at `wend` and
@@ -1856,8 +1869,9 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
           er.flags |= kEntRdCodes;
           er.rdc = cl;
         }
-        uint32_t rb = (uint32_t)block_for(S, scr, n, false, [&](uint32_t i) { return v[i] & rmask; });
-        uint32_t rl = coded_len(S.ra, rb, [&](uint32_t i) { return (uint32_t)scr[i]; });
+        uint8_t* rdst = stage_dst(S, scr, n, rlen);
+        uint32_t rb = (uint32_t)block_for(S, rdst, n, false, [&](uint32_t i) { return v[i] & rmask; });
+        uint32_t rl = coded_len(S.ra, rb, [&](uint32_t i) { return (uint32_t)rdst[i]; });
         if (rl < rlen) {
           rlen = rl;
           er.flags |= kEntRdRights;
@@ -2217,9 +2231,10 @@ __device__ void emit_alprd(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t l
   }
   auto right_of = [&](uint32_t i) { return v[i] & rmask; };
   if (er && (er->flags & kEntRdRights)) {  // the bit-packed rights, coded
-    uint32_t rb = (uint32_t)block_for(S, scr, n, false, right_of);
+    uint8_t* rdst = stage_dst(S, scr, n, block_for(S, nullptr, n, false, right_of));
+    uint32_t rb = (uint32_t)block_for(S, rdst, n, false, right_of);
     if (threadIdx.x == 0) put_u8(out + rpos, 1);
-    coded_write(S.ra, rb, [&](uint32_t i) { return (uint32_t)scr[i]; }, out + rpos + 1, er->rdr);
+    coded_write(S.ra, rb, [&](uint32_t i) { return (uint32_t)rdst[i]; }, out + rpos + 1, er->rdr);
   } else {
     if (threadIdx.x == 0) put_u8(out + rpos, 0);
     block_for(S, out + rpos + 1, n, false, right_of);
