@@ -18,8 +18,10 @@ LIB = os.path.join(HERE, "libquoin_b200.so")
 SOURCES = ["qb_decode.cu", "qb_encode.cu", "qb_lower.cu", "qb_noalloc.cu", "qb_host.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Host code: POPCNT for the validity counts (every x86-64 server CPU of the
+# B200 generation has it).
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-         "-Xcompiler", "-Wall"]
+         "-Xcompiler", "-Wall", "-Xcompiler", "-mpopcnt"]
 
 
 def _newer(target: str, deps) -> bool:

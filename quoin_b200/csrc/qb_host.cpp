@@ -204,6 +204,7 @@ struct QuoinCtx {
   void* buf[S_COUNT] = {};
   size_t cap[S_COUNT] = {};
   std::mutex mu;
+  QuoinDecodeIndex* hidx = nullptr;  // host-side parsed index reused by the host-buffer decodes
 
   cudaError_t ensure(int s, size_t bytes) {
     if (bytes == 0) bytes = 16;
@@ -597,6 +598,25 @@ struct LaneIdx {
   bool need_scan = false;
   uint64_t ent_bytes = 0;  // device area for the entropy-coded parts of listed frames
   uint64_t main_base = 0, pre_base = 0, fp_base = 0, list_base = 0;  // index of the first frame in the device table
+
+  // Back to the empty state, keeping every buffer's capacity (a context
+  // reuses its parsed index, so repeated decodes touch no fresh pages).
+  void reset() {
+    dtype = 0;
+    logical_n = n_total = 0;
+    has_validity = false;
+    bitmap.clear();
+    frames.clear();
+    any_dict = false;
+    frame_base = 0;
+    pre_items.clear();
+    main_items.clear();
+    frame_pre.clear();
+    list.clear();
+    need_scan = false;
+    ent_bytes = 0;
+    main_base = pre_base = fp_base = list_base = 0;
+  }
 };
 
 // Reference validity.rs:73-119.
@@ -748,6 +768,13 @@ bool entropy_frame_h(const uint8_t* p, uint64_t plen, uint32_t mode) {
 // (128-byte units, 1 + its offset in FrameDesc::aux; 0 = none).
 void build_items(const uint8_t* src, LaneIdx& L) {
   const uint32_t V = 512, B = 512;
+  {  // one reservation (items of 512 values or 512 XORZ bytes, prepass items at most as many)
+    uint64_t est = 0;
+    for (const FrameDesc& d : L.frames) est += (d.n + V - 1) / V + (d.plen + B - 1) / B;
+    L.main_items.reserve(est);
+    L.pre_items.reserve(est);
+    L.frame_pre.reserve(L.frames.size());
+  }
   for (uint32_t f = 0; f < (uint32_t)L.frames.size(); f++) {
     const FrameDesc& d = L.frames[f];
     const uint8_t* p = src + d.payload_off;
@@ -874,8 +901,36 @@ int parse_stream(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
   return K_OK;
 }
 
-// The header, validity and frame tables of the stream's lane(s).
+// Lane k of X, emptied (its buffers keep their capacity).
+LaneIdx& lane_slot(QuoinDecodeIndex& X, size_t k) {
+  if (X.lanes.size() <= k) X.lanes.resize(k + 1);
+  X.lanes[k].reset();
+  return X.lanes[k];
+}
+
+// The header, validity and frame tables of the stream's lane(s).  X may be a
+// reused host index: every field is set again.
 int parse_stream_lanes(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
+  X.wire = 0;
+  X.n = 0;
+  X.has_validity = false;
+  X.decimal = false;
+  X.scale = 0;
+  X.precision = 0;
+  X.nl = 0;
+  for (auto& m : X.vmin) m = 0;
+  X.n_valid = 0;
+  X.bitmap.clear();
+  X.items_bytes = 0;
+  X.max_pre = 0;
+  size_t nlanes = 0;
+  struct Trim {  // lanes beyond the parsed ones are dropped on every return
+    QuoinDecodeIndex& X;
+    size_t& n;
+    ~Trim() {
+      if (X.lanes.size() > n) X.lanes.resize(n);
+    }
+  } trim{X, nlanes};
   if (len > 5 && (src[5] & 2)) {  // decimal container (decimal.rs:39-41)
     if (len < 8) return K_TRUNC;
     if (src[7] > 7) return K_DTYPE;
@@ -911,12 +966,11 @@ int parse_stream_lanes(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
       int r = rd_varint_h(src, len, &pos, &sl);
       if (r) return r;
       if (sl > len - pos) return K_TRUNC;
-      LaneIdx L;
+      LaneIdx& L = lane_slot(X, nlanes++);
       r = parse_lane(src, pos, sl, L);
       if (r) return r;
       build_items(src, L);
       if (L.logical_n != X.n_valid) return K_CORRUPT;
-      X.lanes.push_back(std::move(L));
       pos += sl;
     }
     int want = expect == WT_DEC128 ? 2 : 4;
@@ -925,7 +979,7 @@ int parse_stream_lanes(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
     for (int k = 0; k < nl; k++) X.vmin[k] = rd64(src + vmin_off + 8 * k);
     return K_OK;
   }
-  LaneIdx L;
+  LaneIdx& L = lane_slot(X, nlanes++);
   int r = parse_lane(src, 0, len, L);
   if (r) return r;
   build_items(src, L);
@@ -933,9 +987,8 @@ int parse_stream_lanes(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
   X.wire = L.dtype;
   X.n = L.logical_n;
   X.has_validity = L.has_validity;
-  X.bitmap = L.bitmap;
+  X.bitmap.swap(L.bitmap);  // the stream's bitmap is the column's
   X.n_valid = L.n_total;
-  X.lanes.push_back(std::move(L));
   return K_OK;
 }
 
@@ -1092,10 +1145,30 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
 
 // Decode a host stream into host buffers (values_out: n native values;
 // validity_out: ceil(n/8) bytes or null).  *X_out receives the parsed index.
-int decompress_host(QuoinCtx* c, const uint8_t* src, uint64_t len, void* values_out, uint8_t* validity_out,
-                    QuoinDecodeIndex* X) {
-  int k = parse_stream(src, len, *X);
-  if (k) return kind_to_code(k);
+// The context's reusable host index (its buffers keep their capacity).
+QuoinDecodeIndex& host_index(QuoinCtx* c) {
+  if (!c->hidx) c->hidx = new QuoinDecodeIndex();
+  return *c->hidx;
+}
+
+// First half of a host-buffer decode: the stream's copy to the device (S_SRC)
+// starts, and the host parses the stream meanwhile.  After a parse error the
+// copy is waited for (the caller owns src) and the error returned.
+int begin_decode(QuoinCtx* c, const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
+  cudaStream_t st = c->stream;
+  CK(c->ensure(S_SRC, len + 64));
+  if (len) CK(cudaMemcpyAsync(c->p<uint8_t>(S_SRC), src, len, cudaMemcpyHostToDevice, st));
+  int k = parse_stream(src, len, X);
+  if (k) {
+    cudaStreamSynchronize(st);
+    return kind_to_code(k);
+  }
+  return QUOIN_OK;
+}
+
+// Second half: uploads the index, decodes, copies the values (and the
+// validity bitmap) out.  Every return waits for the stream's work.
+int finish_decode(QuoinCtx* c, QuoinDecodeIndex* X, void* values_out, uint8_t* validity_out) {
   cudaStream_t st = c->stream;
   uint64_t nf = total_frames(*X);
   CK(c->ensure(S_DFRAMES, (nf + 1) * sizeof(FrameDesc)));
@@ -1107,9 +1180,10 @@ int decompress_host(QuoinCtx* c, const uint8_t* src, uint64_t len, void* values_
   CK(c->ensure(S_DITEMS, X->items_bytes));
   int rc = upload_index(c, st, *X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK),
                         c->p<uint64_t>(S_DSEL), dvmin, c->p<uint64_t>(S_DITEMS));
-  if (rc) return rc;
-  CK(c->ensure(S_SRC, len + 64));
-  if (len) CK(cudaMemcpyAsync(c->p<uint8_t>(S_SRC), src, len, cudaMemcpyHostToDevice, st));
+  if (rc) {
+    cudaStreamSynchronize(st);
+    return rc;
+  }
   uint64_t out_bytes = X->n * native_width(X->wire);
   CK(c->ensure(S_OUTVALS, out_bytes + 64));
   rc = decode_indexed(c, st, *X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK),
@@ -1120,6 +1194,13 @@ int decompress_host(QuoinCtx* c, const uint8_t* src, uint64_t len, void* values_
   CK(cudaStreamSynchronize(st));
   if (validity_out && X->has_validity && X->n) memcpy(validity_out, X->bitmap.data(), X->bitmap.size());
   return QUOIN_OK;
+}
+
+int decompress_host(QuoinCtx* c, const uint8_t* src, uint64_t len, void* values_out, uint8_t* validity_out,
+                    QuoinDecodeIndex* X) {
+  int rc = begin_decode(c, src, len, *X);
+  if (rc) return rc;
+  return finish_decode(c, X, values_out, validity_out);
 }
 
 // Host-buffer compress of a typed column (wire dtype, native little-endian values).
@@ -1195,18 +1276,19 @@ static int decompress_f64(const QuoinCtx* cc, const uint8_t* src, size_t len, do
     if (!c) return QUOIN_ERR_PANIC;
     std::lock_guard<std::mutex> l(c->mu);
     DeviceScope ds(c->device);
-    QuoinDecodeIndex X;
-    int k = parse_stream(src, len, X);
-    if (k) return QUOIN_ERR_CORRUPT;
-    if (X.wire != WT_F64) return QUOIN_ERR_CORRUPT;  // DTypeMismatch (lib.rs:522-527)
+    QuoinDecodeIndex& X = host_index(c);
+    if (begin_decode(c, src, len, X)) return QUOIN_ERR_CORRUPT;
+    if (X.wire != WT_F64) {  // DTypeMismatch (lib.rs:522-527)
+      cudaStreamSynchronize(c->stream);
+      return QUOIN_ERR_CORRUPT;
+    }
     std::vector<double> tmp;
     double* out = dst;
     if (X.n > cap) {
       tmp.resize(X.n ? X.n : 1);
       out = tmp.data();
     }
-    QuoinDecodeIndex Y;
-    int rc = decompress_host(c, src, len, out, nullptr, &Y);
+    int rc = finish_decode(c, &X, out, nullptr);
     if (rc) return plain_code(rc);
     *out_values = X.n;
     if (X.n > cap) return QUOIN_ERR_BUFFER_TOO_SMALL;
@@ -1259,6 +1341,7 @@ void quoin_ctx_free(QuoinCtx* ctx) {
       if (ctx->buf[s]) cudaFree(ctx->buf[s]);
     cudaStreamDestroy(ctx->stream);
   }
+  delete ctx->hidx;
   delete ctx;
 }
 
@@ -1360,9 +1443,8 @@ int quoin_typed_decompress(int32_t dtype, size_t n, const uint8_t* src, size_t s
     if (!c) return QUOIN_ERR_PANIC;
     std::lock_guard<std::mutex> l(c->mu);
     DeviceScope ds(c->device);
-    QuoinDecodeIndex X;
-    int k = parse_stream(src, src_len, X);
-    if (k) return QUOIN_ERR_CORRUPT;
+    QuoinDecodeIndex& X = host_index(c);
+    if (begin_decode(c, src, src_len, X)) return QUOIN_ERR_CORRUPT;
     // (Arrow dtype, decoded column) pairs accepted by scatter_values (typed.rs:256-273)
     int narrow_to = 0;  // bytes when narrowing
     bool sgn = false;
@@ -1385,16 +1467,16 @@ int quoin_typed_decompress(int32_t dtype, size_t n, const uint8_t* src, size_t s
       default: ok = false;
     }
     (void)sgn;
-    std::vector<uint8_t> full(X.n * native_width(X.wire) + 8);
-    QuoinDecodeIndex Y;
-    int rc = decompress_host(c, src, src_len, full.data(), nullptr, &Y);
-    if (rc) return plain_code(rc);
-    if (!ok || X.n != n) return QUOIN_ERR_CORRUPT;
     uint32_t w = native_width(X.wire);
     uint8_t* out = (uint8_t*)values_out;
-    if (!narrow_to) {
+    bool direct = ok && X.n == n && !narrow_to;  // decode straight into the caller's buffer
+    std::vector<uint8_t> full(direct ? 0 : X.n * w + 8);
+    int rc = finish_decode(c, &X, direct ? values_out : (void*)full.data(), nullptr);
+    if (rc) return plain_code(rc);
+    if (!ok || X.n != n) return QUOIN_ERR_CORRUPT;
+    if (!direct && !narrow_to) {
       memcpy(out, full.data(), n * w);
-    } else {
+    } else if (!direct) {
       for (size_t i = 0; i < n; i++) memcpy(out + i * narrow_to, full.data() + i * w, narrow_to);  // `as` truncation
     }
     if (validity_out) {  // typed.rs:280-300
@@ -1481,8 +1563,7 @@ int quoin_b200_decompress_column(QuoinCtx* ctx, const uint8_t* src, size_t len, 
     if (!c) return QUOIN_ERR_CUDA;
     std::lock_guard<std::mutex> l(c->mu);
     DeviceScope ds(c->device);
-    QuoinDecodeIndex X;
-    return decompress_host(c, src, len, values_out, validity_out, &X);
+    return decompress_host(c, src, len, values_out, validity_out, &host_index(c));
   } catch (...) {
     return QUOIN_ERR_PANIC;
   }
