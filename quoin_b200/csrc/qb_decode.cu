@@ -1491,7 +1491,7 @@ __device__ __forceinline__ uint32_t term_mask8(uint64_t w) {
   return (uint32_t)((t * 0x0102040810204080ull) >> 56);
 }
 
-template <bool EMIT>
+template <bool EMIT, bool CHECK>
 __device__ __forceinline__ uint64_t xorz_lane_bytes(XSlice& X, uint64_t state, uint64_t* stg, uint32_t k) {
   uint32_t j = X.j0;
 #pragma unroll
@@ -1500,7 +1500,7 @@ __device__ __forceinline__ uint64_t xorz_lane_bytes(XSlice& X, uint64_t state, u
       uint32_t b = (uint32_t)(((q < 8) ? (X.w0 >> (8 * q)) : (X.w1 >> (8 * (q - 8)))) & 0xFFu);
       if (j < 10) state ^= (uint64_t)(b & 0x7Fu) << (7 * j);
       if (!(b & 0x80u)) {
-        if (!EMIT && j >= 10) {
+        if (CHECK && j >= 10) {
           if (!X.bad) X.first_bad = k;
           X.bad = 1;
         }
@@ -1515,6 +1515,10 @@ __device__ __forceinline__ uint64_t xorz_lane_bytes(XSlice& X, uint64_t state, u
   return state;
 }
 
+// BYTES: also run the lane's bytes once for their contribution XOR (xo) and
+// the over-long flags (the prepass); the item kernel folds that into its
+// emitting pass.
+template <bool BYTES>
 __device__ XSlice xorz_lane_scan(const uint8_t* p, uint64_t plen, uint64_t s) {
   int l = threadIdx.x & 31;
   XSlice X;
@@ -1566,7 +1570,7 @@ __device__ XSlice xorz_lane_scan(const uint8_t* p, uint64_t plen, uint64_t s) {
   X.j0 = (uint32_t)qmin(dist, 10);
   X.bad = 0;
   X.first_bad = ~0u;
-  X.xo = xorz_lane_bytes<false>(X, 0ull, nullptr, 0);
+  X.xo = BYTES ? xorz_lane_bytes<false, true>(X, 0ull, nullptr, 0) : 0ull;
   return X;
 }
 
@@ -1631,7 +1635,7 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_prepass(const uint8_t* _
     for (int o = 16; o; o >>= 1) s = qmin(s + __shfl_xor_sync(0xffffffffu, s, o), n + 1);
     R.a = s;
   } else if (d.mode == M_XORZ) {
-    XSlice X = xorz_lane_scan(p, d.plen, (uint64_t)it.local * kItemBytes);
+    XSlice X = xorz_lane_scan<true>(p, d.plen, (uint64_t)it.local * kItemBytes);
     uint64_t xo = X.xo;
     for (int o = 16; o; o >>= 1) xo ^= __shfl_xor_sync(0xffffffffu, xo, o);
     R.a = xo;
@@ -1872,13 +1876,17 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
     case M_XORZ: {
       const PreRec& R = pre[frame_pre[it.frame].x + it.local];
       uint64_t vbase = R.b;
-      XSlice X = xorz_lane_scan(p, d.plen, (uint64_t)it.local * kItemBytes);
-      uint64_t inc = X.xo;  // contributions of the lanes before, then the lane's bytes
+      XSlice X = xorz_lane_scan<false>(p, d.plen, (uint64_t)it.local * kItemBytes);
+      // one pass from a zero state (values relative to the lane's start), then
+      // the lane's carry: the item's carry and the lanes before
+      uint64_t own = xorz_lane_bytes<true, true>(X, 0ull, stg, 0);
+      uint64_t inc = own;
       for (int o = 1; o < 32; o <<= 1) {
         uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
         if (l >= o) inc ^= u;
       }
-      xorz_lane_bytes<true>(X, R.a ^ inc ^ X.xo, stg, 0);
+      uint64_t base = R.a ^ inc ^ own;
+      for (uint32_t q = 0; q < X.cnt; q++) stg[skew(X.before + q)] ^= base;
       __syncwarp();
       // checks on the values that exist (index < n): length, and the n-th
       // value's terminator must be the payload's last byte
