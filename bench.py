@@ -243,10 +243,18 @@ def run_gpu(args, rank, world, local):
             raise Q.Error(rc)
 
     def compress_all():
-        list(pool.map(compress_one, gcols))
+        if args.serial_columns:
+            for c in gcols:
+                compress_one(c)
+        else:
+            list(pool.map(compress_one, gcols))
 
     def decompress_all():
-        list(pool.map(decompress_one, gcols))
+        if args.serial_columns:
+            for c in gcols:
+                decompress_one(c)
+        else:
+            list(pool.map(decompress_one, gcols))
 
     def mark():
         """A timing event on stream 0 ordered after the work queued on every column stream."""
@@ -372,7 +380,10 @@ def run_gpu(args, rank, world, local):
                 olen.value + hout.numel() + (hvout.numel() if hb is not None else 0))
 
     def e2e_step():  # the columns' host copies overlap in both directions
-        r = list(pool.map(e2e_one, zip(gcols, pinned)))
+        if args.serial_columns:
+            r = [e2e_one(cp) for cp in zip(gcols, pinned)]
+        else:
+            r = list(pool.map(e2e_one, zip(gcols, pinned)))
         return sum(a for a, _ in r), sum(b for _, b in r)
 
     e2e_step()
@@ -407,8 +418,10 @@ def run_gpu(args, rank, world, local):
                                    "Level::Fast", "values_per_column": n, "columns": 3, "global_values": n * 3 * world,
                        "l2": "inputs (1.25 GiB per rank) exceed the 126 MB L2; no flush needed",
                        "parallelism": f"replicas x{world} (each rank encodes and decodes its own copy of the columns)",
-                       "concurrency": "the three columns run on three CUDA streams (one context and host thread "
-                                      "each); every step compresses all three, then decompresses all three"},
+                       "concurrency": ("the three columns run one after another (--serial-columns)" if args.serial_columns
+                                       else "the three columns run on three CUDA streams (one context and host "
+                                            "thread each); every step compresses all three, then decompresses "
+                                            "all three")},
             "encode_gbs": round(raw_bytes * world * args.steps / (enc_ms / 1e3) / 1e9, 3),
             "decode_gbs": round(raw_bytes * world * args.steps / (dec_ms / 1e3) / 1e9, 3),
             "ratio": round(raw_bytes / stream_bytes, 4), "bit_exact": bit_exact,
@@ -444,6 +457,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="values per column")
     ap.add_argument("--cpu-sample", type=int, default=1 << 24)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serial-columns", action="store_true",
+                    help="one host thread runs the columns one after another (for profilers)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":

@@ -1422,10 +1422,10 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
     __syncthreads();
   }
   SubStats R;
-  uint64_t umn = kEmpty64, umx = 0, dzmn = kEmpty64, dzmx = 0, xb = 0;
+  uint64_t umn = kEmpty64, umx = 0, dzmn = kEmpty64, dzmx = 0;
   int64_t smn = INT64_MAX, smx = INT64_MIN;
   uint64_t a16mn = kEmpty64, a16mx = 0, a16dz = 0, a64mn = kEmpty64, a64mx = 0, a64dz = 0;
-  uint32_t nq = 0, sbad = 0, fmfail = 0;
+  uint32_t nq = 0, xb = 0, fmfail = 0;
   int64_t kmn[7], kmx[7];
 #pragma unroll
   for (int q = 0; q < 7; q++) {
@@ -1449,9 +1449,11 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
     uint32_t j = r * 32 + lane;
     bool ok = j < cnt;
     uint64_t x = xs[q];
-    uint64_t up = __shfl_up_sync(0xffffffffu, x, 1);
-    uint64_t pv = lane ? up : carry;
-    carry = __shfl_sync(0xffffffffu, x, 31);
+    // one rotation gives every lane its predecessor; lane 0's is the previous
+    // row's last value, which the rotation hands it for the next row
+    uint64_t rot = __shfl_sync(0xffffffffu, x, (lane + 31) & 31);
+    uint64_t pv = lane ? rot : carry;
+    carry = rot;
     if (ok) {
       umn = u64min(umn, x);
       umx = u64max(umx, x);
@@ -1466,7 +1468,6 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
         dzmx = u64max(dzmx, dz);
         xb += varint_len(x ^ pv);
         nq += x != pv ? 1u : 0u;
-        sbad |= (x - pv != d) ? 1u : 0u;
       }
       if (!fixed_bs) {
         if (j == 0 || x != pv) {  // a repeat's bucket is already set
@@ -1535,9 +1536,10 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
   R.e64min = warp_min(a64mn);
   R.e64max = warp_max(a64mx);
   R.e64dz = warp_max(a64dz);
-  R.xb = (uint32_t)warp_sum(xb);
+  R.xb = warp_sum(xb);
   R.neq = warp_sum(nq);
-  R.stride_ok = warp_or(sbad) ? 0 : 1;
+  // every internal delta equals d exactly when the zigzag deltas are all zigzag(d)
+  R.stride_ok = (cnt < 2 || (R.dzmin == R.dzmax && R.dzmax == zigzag64(d))) ? 1 : 0;
   R.cnt = cnt;
   R.first = cnt ? sv[0] : 0;
   R.last = cnt ? sv[cnt - 1] : 0;
