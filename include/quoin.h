@@ -146,13 +146,20 @@ int quoin_typed_decompress(int32_t dtype, size_t n, const uint8_t *src,
 #define QUOIN_WIRE_DECIMAL128 6
 #define QUOIN_WIRE_DECIMAL256 7
 
+/* Mode selection (src/lib.rs:65-73): FULL sizes every candidate on the whole
+ * block; SAMPLE sizes them on a stratified sample of the block and encodes
+ * only the winner in full (src/encoder.rs:470-620), at FASTEST and FAST. */
+#define QUOIN_B200_SELECTION_FULL   0
+#define QUOIN_B200_SELECTION_SAMPLE 1
+
 /* Encoder configuration (src/lib.rs:195-245): predictor_log2 (clamped 10..16,
  * recorded in the header), level, block_size (0 = adaptive; else clamped to
- * [1, 131072]). */
+ * [1, 131072]), selection (QUOIN_B200_SELECTION_*). */
 typedef struct {
     int32_t level;
     int64_t block_size;
     int32_t predictor_log2;
+    int32_t selection;
 } QuoinConfig;
 
 /* Replaces compress_column(ColumnRef, Option<&[u8]>, Config) (src/lib.rs:429-455)

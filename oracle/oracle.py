@@ -27,6 +27,7 @@ ERR_NAMES = {1: "BadMagic", 2: "UnsupportedVersion", 3: "Truncated", 4: "Unknown
              8: "DTypeMismatch", 9: "Unsupported", 10: "BadArg"}
 
 LEVEL_FASTEST, LEVEL_FAST, LEVEL_BALANCED_INPOOL = 0, 1, 2
+SELECT_SAMPLE = 0x100  # added to a level: Selection::Sample (reference src/encoder.rs:470-620)
 
 
 class OracleError(Exception):
@@ -97,8 +98,10 @@ def _ptr(a):
 
 def compress_column(values: np.ndarray, dtype: int, validity=None, level: int = LEVEL_FAST,
                     block_size=None, scale: int = 0, precision: int = 0, predictor_log2: int = 16,
-                    threads: int = 1) -> bytes:
+                    threads: int = 1, sample: bool = False) -> bytes:
     values = np.ascontiguousarray(values)
+    if sample:
+        level |= SELECT_SAMPLE
     n = values.nbytes // NATIVE_WIDTH[dtype]
     vb = None if validity is None else np.ascontiguousarray(validity, dtype=np.uint8)
     out = ctypes.POINTER(ctypes.c_uint8)()

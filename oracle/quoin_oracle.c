@@ -1771,6 +1771,101 @@ static void encode_block_full(const uint64_t *b, size_t n, int dtype, int level,
     b_free(&best.payload);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Selection::Sample — encoder.rs:470-620, mode gates encoder.rs:24-60        */
+/* ------------------------------------------------------------------------ */
+
+/* The in-pool members of SAMPLE_MODES (encoder.rs:479-495), in its order; the
+ * predictor modes between Xorz and FloatMult run only at High/Max. */
+static const int SAMPLE_POOL[] = {M_XORZ, M_FLOAT_MULT, M_BYTE_TRANSPOSE, M_FOR_BITPACK, M_DELTA_BITPACK,
+                                  M_ALP, M_ALP_RD, M_DICT, M_RLE};
+#define SAMPLE_RUNS 8
+#define SAMPLE_RUN_LEN 64
+
+/* mode_runs (encoder.rs:50-60): float-only modes, and the entropy modes at
+ * Balanced and above. */
+static bool sample_mode_runs(int mode, bool fam_float, int level) {
+    if ((mode == M_FLOAT_MULT || mode == M_ALP || mode == M_ALP_RD) && !fam_float) return false;
+    if ((mode == M_FLOAT_MULT || mode == M_BYTE_TRANSPOSE) && level < 2) return false;
+    return true;
+}
+
+/* encode_mode (encoder.rs:543-572) for the in-pool modes; false when the mode
+ * does not apply. */
+static bool sample_encode_mode(int mode, const uint64_t *b, size_t n, int dtype, int level, buf_t *out) {
+    bool entropy = level >= 2;
+    switch (mode) {
+        case M_XORZ: xorz_encode(b, n, out); return true;
+        case M_FOR_BITPACK: for_encode(b, n, dtype_signed(dtype), out); return true;
+        case M_DELTA_BITPACK: delta_encode(b, n, out); return true;
+        case M_FLOAT_MULT: return fm_encode(b, n, entropy, out);
+        case M_ALP: return alp_encode(b, n, out);
+        case M_ALP_RD: return alprd_encode(b, n, entropy, out);
+        case M_DICT: return dict_encode(b, n, entropy, out);
+        case M_RLE: return rle_encode(b, n, out);
+        case M_BYTE_TRANSPOSE: {
+            if (n == 0) return false;
+            uint8_t *tr = transpose_encode(b, n);
+            code_residuals(tr, n * 8, out);
+            free(tr);
+            return true;
+        }
+        default: return false;
+    }
+}
+
+/* encoder.rs:574-620 for the in-pool modes (Lz and Pco, which Balanced would
+ * try on the full block, are outside the pool): RAW, then CONST and STRIDE on
+ * the full block, then the winner of the sample estimates encoded in full. */
+static void encode_block_sampled(const uint64_t *b, size_t n, int dtype, int level, buf_t *out) {
+    bool fam_float = dtype_float(dtype);
+    best_t best = {0};
+    best.lambda = level_lambda(level);
+    best.decoded_bytes = (uint64_t)n * lane_bytes(dtype);
+    best.mode = M_RAW;
+    raw_encode(b, n, dtype, &best.payload);
+    best.score = best.payload.len + penalty(M_RAW, best.lambda, best.decoded_bytes);
+    buf_t p = {0};
+    if (const_encode(b, n, &p)) consider(&best, M_CONST, &p); else b_free(&p);
+    if (stride_encode(b, n, &p)) consider(&best, M_STRIDE, &p); else b_free(&p);
+    /* build_sample (encoder.rs:503-516): 8 runs of 64 spread over the block */
+    size_t total = SAMPLE_RUNS * SAMPLE_RUN_LEN, m = n;
+    uint64_t *smp = (uint64_t *)malloc((n < total ? n : total) * 8 + 8);
+    if (n <= total) {
+        memcpy(smp, b, n * 8);
+    } else {
+        m = total;
+        for (size_t r = 0; r < SAMPLE_RUNS; r++) {
+            size_t start = r * (n - SAMPLE_RUN_LEN) / (SAMPLE_RUNS - 1);
+            memcpy(smp + r * SAMPLE_RUN_LEN, b + start, SAMPLE_RUN_LEN * 8);
+        }
+    }
+    int win = -1;
+    size_t win_est = SIZE_MAX;
+    for (size_t k = 0; k < sizeof SAMPLE_POOL / sizeof SAMPLE_POOL[0]; k++) {
+        int mode = SAMPLE_POOL[k];
+        if (!sample_mode_runs(mode, fam_float, level)) continue;
+        buf_t e = {0};
+        if (sample_encode_mode(mode, smp, m, dtype, level, &e) && e.len < win_est) {
+            win_est = e.len;
+            win = mode;
+        }
+        b_free(&e);
+    }
+    free(smp);
+    if (win >= 0 && sample_encode_mode(win, b, n, dtype, level, &p)) consider(&best, win, &p); else b_free(&p);
+    atomic_fetch_add(&g_wins[best.mode], 1);
+    frame_bytes(best.mode, n, &best.payload, out);
+    b_free(&best.payload);
+}
+
+/* encoder.rs:244-256: the level argument carries OQ_SELECT_SAMPLE for
+ * Selection::Sample. */
+static void encode_block(const uint64_t *b, size_t n, int dtype, int level, buf_t *out) {
+    if (level & OQ_SELECT_SAMPLE) encode_block_sampled(b, n, dtype, level & 0xFF, out);
+    else encode_block_full(b, n, dtype, level, out);
+}
+
 /* encoder.rs:154-178 */
 static size_t plan_blocks(const uint64_t *v, size_t n, long block_size, size_t **starts_out) {
     size_t cap = n / 32768 + 2, nb = 0;
@@ -1817,8 +1912,7 @@ static void *enc_worker(void *arg) {
     for (;;) {
         size_t k = atomic_fetch_add(&j->next, 1);
         if (k >= j->nb) break;
-        encode_block_full(j->vals + j->starts[k], j->starts[k + 1] - j->starts[k], j->dtype, j->level,
-                          &j->frames[k]);
+        encode_block(j->vals + j->starts[k], j->starts[k + 1] - j->starts[k], j->dtype, j->level, &j->frames[k]);
     }
     return NULL;
 }
@@ -2277,7 +2371,8 @@ static uint64_t *to_lane(int dtype, size_t n, const void *values) {
 static int compress_column_impl(int dtype, size_t n, const void *values, const uint8_t *validity, int8_t scale,
                                 uint8_t precision, int level, long block_size, int plog2, int threads,
                                 uint8_t **out, size_t *out_len) {
-    if (level < 0 || level > 2 || dtype < 0 || dtype > 7) return OQ_BAD_ARG;
+    if (level < 0 || (level & ~(OQ_SELECT_SAMPLE | 0xFF)) || (level & 0xFF) > 2 || dtype < 0 || dtype > 7)
+        return OQ_BAD_ARG;
     buf_t b = {0};
     if (dtype == OQ_DEC128 || dtype == OQ_DEC256) { /* lib.rs:431-443 */
         decimal_compress(dtype, n, (const uint8_t *)values, validity, scale, precision, level, block_size, plog2,
@@ -2315,7 +2410,7 @@ int oq_compress_column_mt(int dtype, size_t n, const void *values, const uint8_t
 
 int oq_compress_lane(const uint64_t *vals, size_t n_valid, int dtype, size_t logical_n, const uint8_t *validity,
                      int level, long block_size, int plog2, uint8_t **out, size_t *out_len) {
-    if (level < 0 || level > 2) return OQ_BAD_ARG;
+    if (level < 0 || (level & ~(OQ_SELECT_SAMPLE | 0xFF)) || (level & 0xFF) > 2) return OQ_BAD_ARG;
     buf_t b = {0};
     compress_lane_buf(vals, n_valid, dtype, logical_n, validity, level, block_size, plog2, 1, &b);
     *out = b.p ? b.p : (uint8_t *)malloc(1);

@@ -49,6 +49,10 @@ enum {
 enum { OQ_F64 = 0, OQ_I64 = 1, OQ_U64 = 2, OQ_I32 = 3, OQ_U32 = 4, OQ_F32 = 5,
        OQ_DEC128 = 6, OQ_DEC256 = 7 };
 
+/* Added to a level: Selection::Sample instead of Selection::Full (reference
+ * src/lib.rs:65-73, src/encoder.rs:470-620). */
+#define OQ_SELECT_SAMPLE 0x100
+
 /* Compress a typed column.  `values` holds n native values (8 B for
  * f64/i64/u64, 4 B for i32/u32/f32, 16 B for dec128, 32 B for dec256).
  * `validity` is an Arrow bitmap of ceil(n/8) bytes or NULL.  `block_size` <= 0

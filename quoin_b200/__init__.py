@@ -54,7 +54,11 @@ class Level(enum.IntEnum):
 
 
 class Selection(enum.Enum):
-    FULL = "full"  # the GPU competition always encodes every candidate's exact size
+    """Mode selection (reference src/lib.rs:65-73): FULL sizes every candidate
+    on the whole block; SAMPLE sizes them on a stratified sample and encodes
+    only the winner in full (Level.FASTEST and Level.FAST)."""
+    FULL = "full"
+    SAMPLE = "sample"
 
 
 @dataclass
@@ -70,7 +74,8 @@ class Config:
 
 
 class _QuoinConfig(ctypes.Structure):
-    _fields_ = [("level", ctypes.c_int32), ("block_size", ctypes.c_int64), ("predictor_log2", ctypes.c_int32)]
+    _fields_ = [("level", ctypes.c_int32), ("block_size", ctypes.c_int64), ("predictor_log2", ctypes.c_int32),
+                ("selection", ctypes.c_int32)]
 
 
 # Stream dtype wire ids (reference src/dtype.rs:68-78).
@@ -140,7 +145,8 @@ VERSION = lib.quoin_version().decode()
 
 def _cfg(cfg: Optional[Config]) -> _QuoinConfig:
     cfg = cfg or Config()
-    return _QuoinConfig(int(cfg.level), int(cfg.block_size or 0), int(cfg.predictor_log2))
+    return _QuoinConfig(int(cfg.level), int(cfg.block_size or 0), int(cfg.predictor_log2),
+                        1 if cfg.selection == Selection.SAMPLE else 0)
 
 
 def _check(rc: int) -> None:

@@ -1626,10 +1626,206 @@ __device__ uint32_t popc_bits_block(EncSmem& S, const uint32_t* bits) {
   return t;
 }
 
+// ---------------------------------------------------------------------------
+// Selection::Sample (reference encoder.rs:470-620) at Fastest and Fast: the
+// candidate modes are sized on a stratified sample of the block (8 runs of 64
+// values spread over it, or the whole block up to 512 values) and the
+// smallest estimate, first in SAMPLE_MODES order on ties, is the one encoded
+// in full.  The in-pool members at these levels: Xorz, ForBitpack,
+// DeltaBitpack, Alp and AlpRd (float columns), Dict, Rle; FloatMult and
+// ByteTranspose are entropy modes (Balanced and above).
+// ---------------------------------------------------------------------------
+__device__ __noinline__ int sample_winner(EncSmem& S, const uint64_t* v, uint32_t n, int dtype, uint8_t* scr) {
+  int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  uint64_t* smp = reinterpret_cast<uint64_t*>(&S.ra.buf[0][0]);  // 512 values (the rANS staging is idle)
+  uint32_t m = n <= 512u ? n : 512u;
+  for (uint32_t i = t; i < m; i += blockDim.x) {
+    uint32_t src = i;
+    if (n > 512u) {  // build_sample: run r starts at r * (n - 64) / 7
+      uint32_t r = i >> 6;
+      src = (uint32_t)((uint64_t)r * (n - 64u) / 7u) + (i & 63u);
+    }
+    smp[i] = v[src];
+  }
+  if (t == 0) {
+    S.sc[0] = 0;            // XORZ bytes
+    S.sc[1] = kEmpty64;     // unsigned min
+    S.sc[2] = 0;            // unsigned max
+    S.sc[3] = kEmpty64;     // signed min, as x ^ 2^63 (signed order in unsigned compares)
+    S.sc[4] = 0;            // signed max, likewise
+    S.sc[5] = kEmpty64;     // zigzag delta min
+    S.sc[6] = 0;            // zigzag delta max
+    S.cnt32 = 0;            // transitions
+  }
+  __syncthreads();
+  const bool fl = dtype_float(dtype), sgn = dtype_signed(dtype);
+  const uint64_t kBias = 0x8000000000000000ull;  // signed order as unsigned order
+  {
+    uint64_t xb = 0, umn = kEmpty64, umx = 0, bmn = kEmpty64, bmx = 0, dmn = kEmpty64, dmx = 0;
+    uint32_t tr = 0;
+    for (uint32_t i = t; i < m; i += blockDim.x) {
+      uint64_t x = smp[i], pv = i ? smp[i - 1] : 0ull;
+      xb += varint_len(x ^ pv);
+      umn = u64min(umn, x);
+      umx = u64max(umx, x);
+      bmn = u64min(bmn, x ^ kBias);
+      bmx = u64max(bmx, x ^ kBias);
+      uint64_t dz = i ? zigzag64(x - pv) : 0ull;  // delta_bitpack: d_0 = 0
+      dmn = u64min(dmn, dz);
+      dmx = u64max(dmx, dz);
+      tr += (i && x != pv) ? 1u : 0u;
+    }
+    xb = warp_sum(xb);
+    umn = warp_min(umn);
+    umx = warp_max(umx);
+    bmn = warp_min(bmn);
+    bmx = warp_max(bmx);
+    dmn = warp_min(dmn);
+    dmx = warp_max(dmx);
+    tr = warp_sum(tr);
+    if (lane == 0) {
+      atomicAdd((unsigned long long*)&S.sc[0], (unsigned long long)xb);
+      atomic_min_u64((unsigned long long*)&S.sc[1], umn);
+      atomic_max_u64((unsigned long long*)&S.sc[2], umx);
+      atomic_min_u64((unsigned long long*)&S.sc[3], bmn);
+      atomic_max_u64((unsigned long long*)&S.sc[4], bmx);
+      atomic_min_u64((unsigned long long*)&S.sc[5], dmn);
+      atomic_max_u64((unsigned long long*)&S.sc[6], dmx);
+      atomicAdd(&S.cnt32, tr);
+    }
+  }
+  __syncthreads();
+  uint64_t vl = varint_len(m);
+  uint64_t est_xorz = S.sc[0];
+  uint64_t est_for = vl + 9 + 128ull * bit_width64(sgn ? S.sc[4] - S.sc[3] : S.sc[2] - S.sc[1]);
+  uint64_t est_delta = 8 + vl + 9 + 128ull * bit_width64(S.sc[6] - S.sc[5]);
+  uint32_t transitions = S.cnt32;
+  __syncthreads();
+  int win = M_XORZ;
+  uint64_t win_est = est_xorz;
+  auto take = [&](int mode, uint64_t est) {
+    if (est < win_est) {
+      win_est = est;
+      win = mode;
+    }
+  };
+  take(M_FOR_BITPACK, est_for);
+  take(M_DELTA_BITPACK, est_delta);
+  if (fl) {
+    // ALP (alp.rs:93-166): one sub-block
+    if (warp == 0) {
+      AlpSub a;
+      bool ok = alp_subblock(smp, m, S.alp_smp[0], &a);
+      if (lane == 0) S.sc[7] = ok ? vl + 13 + 128ull * a.w + 10ull * a.exc : kEmpty64;
+    }
+    __syncthreads();
+    uint64_t est_alp = S.sc[7];
+    __syncthreads();
+    if (est_alp != kEmpty64) take(M_ALP, est_alp);
+    // ALP-RD (alp_rd.rs:132-206), bit-packed streams
+    uint32_t lbw = rd_choose_cut(S, smp, m, nullptr, 0);
+    if (lbw) {
+      rd_top8(S, smp, m, lbw, scr);
+      uint32_t rbw = 64 - lbw;
+      uint64_t rmask = (1ull << rbw) - 1ull;
+      if (t == 0) {
+        S.sc[0] = 0;         // exception bytes
+        S.sc[1] = kEmpty64;  // code min
+        S.sc[2] = 0;         // code max
+        S.sc[3] = kEmpty64;  // right min
+        S.sc[4] = 0;         // right max
+        S.cnt32 = 0;         // exceptions
+      }
+      __syncthreads();
+      uint64_t eb = 0, cmn = kEmpty64, cmx = 0, rmn = kEmpty64, rmx = 0;
+      uint32_t ne = 0;
+      for (uint32_t i = t; i < m; i += blockDim.x) {
+        uint64_t x = smp[i];
+        int c = rd_code(S, x >> rbw);
+        uint64_t code = c < 0 ? 0ull : (uint64_t)c;
+        if (c < 0) {
+          ne++;
+          eb += varint_len(i) + 8;
+        }
+        cmn = u64min(cmn, code);
+        cmx = u64max(cmx, code);
+        rmn = u64min(rmn, x & rmask);
+        rmx = u64max(rmx, x & rmask);
+      }
+      eb = warp_sum(eb);
+      ne = warp_sum(ne);
+      cmn = warp_min(cmn);
+      cmx = warp_max(cmx);
+      rmn = warp_min(rmn);
+      rmx = warp_max(rmx);
+      if (lane == 0) {
+        atomicAdd((unsigned long long*)&S.sc[0], (unsigned long long)eb);
+        atomic_min_u64((unsigned long long*)&S.sc[1], cmn);
+        atomic_max_u64((unsigned long long*)&S.sc[2], cmx);
+        atomic_min_u64((unsigned long long*)&S.sc[3], rmn);
+        atomic_max_u64((unsigned long long*)&S.sc[4], rmx);
+        atomicAdd(&S.cnt32, ne);
+      }
+      __syncthreads();
+      uint64_t nexc = S.cnt32;
+      uint64_t clen = vl + 9 + 128ull * bit_width64(S.sc[2] - S.sc[1]);
+      uint64_t rlen = vl + 9 + 128ull * bit_width64(S.sc[4] - S.sc[3]);
+      if (nexc * 4 <= m)
+        take(M_ALP_RD, 2 + 8ull * S.dl + varint_len(nexc) + S.sc[0] + 1 + varint_len(clen) + clen + 1 + rlen);
+      __syncthreads();
+    }
+  }
+  // DICT (dict.rs:87-152), bit-packed codes
+  DictView dv = dict_prepare(S, smp, m, scr, kNoLb);
+  if (!S.flag) {
+    uint32_t vtag;
+    uint64_t vlen = dict_values_len(S, dv, &vtag);
+    if (t == 0) {
+      S.sc[1] = kEmpty64;
+      S.sc[2] = 0;
+    }
+    __syncthreads();
+    uint64_t rmn = kEmpty64, rmx = 0;
+    for (uint32_t i = t; i < m; i += blockDim.x) {
+      uint64_t r = dict_rank(S, dv, smp[i]);
+      rmn = u64min(rmn, r);
+      rmx = u64max(rmx, r);
+    }
+    rmn = warp_min(rmn);
+    rmx = warp_max(rmx);
+    if (lane == 0) {
+      atomic_min_u64((unsigned long long*)&S.sc[1], rmn);
+      atomic_max_u64((unsigned long long*)&S.sc[2], rmx);
+    }
+    __syncthreads();
+    uint64_t clen = vl + 9 + 128ull * bit_width64(S.sc[2] - S.sc[1]);
+    take(M_DICT, varint_len(dv.card) + 1 + varint_len(vlen) + vlen + 1 + clen);
+  }
+  __syncthreads();
+  // RLE (rle.rs:10-42): completed runs beyond m/2 + 1 bail
+  if (transitions <= m / 2 + 1) {
+    if (t == 0) {
+      uint32_t runs = transitions + 1, start = 0, lmn = 0xFFFFFFFFu, lmx = 0;
+      for (uint32_t i = 1; i <= m; i++)
+        if (i == m || smp[i] != smp[i - 1]) {
+          uint32_t len = i - start;
+          lmn = min(lmn, len);
+          lmx = max(lmx, len);
+          start = i;
+        }
+      S.sc[0] = varint_len(runs) + 8ull * runs + varint_len(runs) + 9 + 128ull * bit_width64((uint64_t)(lmx - lmn));
+    }
+    __syncthreads();
+    take(M_RLE, S.sc[0]);
+  }
+  __syncthreads();
+  return win;
+}
+
 // ENT: the Balanced in-pool competition, with the rANS-coded forms of
 // FLOAT_MULT, ALP-RD and DICT and the BYTE_TRANSPOSE candidate; the chosen
 // coded parts go to ent[b] for the emission.
-template <bool ENT>
+template <bool ENT, bool SAMPLE>
 __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restrict__ lane, FrameDesc* frames,
                                                         const uint32_t* __restrict__ nbp, uint64_t fixed_bs,
                                                         int dtype, int level, const SubStats* __restrict__ ss,
@@ -1720,10 +1916,15 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
   __syncthreads();
   uint64_t vl = varint_len(n);
   uint64_t sz_for = vl + S.sc[1], sz_delta = 8 + vl + S.sc[2], sz_alp = vl + S.sc[4];
+  // Selection::Sample: the mode whose estimate on the block's sample is the
+  // smallest; it alone is sized in full below (encoder.rs:574-620).
+  int win = -1;
+  if (SAMPLE) win = sample_winner(S, v, n, dtype, scr);
 
-  // Integer early-out (encoder.rs:295-298, 655-683) with the block's features.
+  // Integer early-out (encoder.rs:295-298, 655-683) with the block's features
+  // (the sampled selection has none).
   bool eo = false;
-  if (!fam_float) {
+  if (!SAMPLE && !fam_float) {
     uint32_t consec_eq = n - S.neq;
     bool repeats = (uint64_t)consec_eq * 2 > (uint64_t)n;
     uint32_t dstride = max(n / 4096u, 1u);
@@ -1783,8 +1984,8 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
 
   Cand c_fm = {0, false}, c_alp = {0, false}, c_rd = {0, false};
   uint32_t fm_scale = 0, rd_lbw = 0;
-  if (fam_float && !reduced) {
-    uint32_t mask = S.fm_mask;
+  if (fam_float && (SAMPLE ? (win == M_ALP || win == M_ALP_RD) : !reduced)) {
+    uint32_t mask = SAMPLE ? 0u : S.fm_mask;  // FLOAT_MULT is an entropy mode for the sampled pool
     if (mask) {  // FLOAT_MULT (float_mult.rs:66-98, bit-packed k)
       fm_scale = __ffs(mask) - 1;
       uint64_t my = 0;
@@ -1812,9 +2013,30 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
     }
     c_alp.ok = !S.alp_fail;  // ALP (alp.rs:93-166)
     c_alp.len = sz_alp;
+    if (SAMPLE && win == M_ALP && reduced) {  // Fastest gathered no ALP statistics: size it here
+      if (t == 0) {
+        S.acc64 = 0;
+        S.alp_fail = 0;
+      }
+      __syncthreads();
+      for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+        uint32_t cnt = min((uint32_t)kSub, n - k * kSub);
+        AlpSub a;
+        bool ok = alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], &a);
+        if (lane_id == 0) {
+          if (ok) atomicAdd(&S.acc64, (unsigned long long)(13 + 128ull * a.w + 10ull * a.exc));
+          else atomicOr(&S.alp_fail, 1u);
+        }
+      }
+      __syncthreads();
+      c_alp.ok = !S.alp_fail;
+      c_alp.len = vl + S.acc64;
+    }
     // ALP-RD (alp_rd.rs:132-206, bit-packed streams)
     bool pre_s = smp16 && !fixed_bs && (step == 16 || step == 64) && (fd.value_off % kBaseQuantum) == 0;
-    rd_lbw = rd_choose_cut(S, v, n, pre_s ? smp16 + fd.value_off / 16 : nullptr, step / 16);
+    rd_lbw = (SAMPLE && win != M_ALP_RD) ? 0u
+                                         : rd_choose_cut(S, v, n, pre_s ? smp16 + fd.value_off / 16 : nullptr,
+                                                         step / 16);
     if (rd_lbw) {
       rd_top8(S, v, n, rd_lbw, scr);
       uint32_t rbw = 64 - rd_lbw;
@@ -1899,12 +2121,20 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
   };
   if (S.umin == S.umax) consider(M_CONST, 8);
   if (n >= 2 && !S.stride_bad) consider(M_STRIDE, 16);
-  if (!reduced) consider(M_XORZ, S.xor_bytes);
-  consider(M_FOR_BITPACK, sz_for);
-  consider(M_DELTA_BITPACK, sz_delta);
-  if (c_fm.ok) consider(M_FLOAT_MULT, c_fm.len);
-  if (c_alp.ok) consider(M_ALP, c_alp.len);
-  if (c_rd.ok) consider(M_ALP_RD, c_rd.len);
+  if (SAMPLE) {  // the sample's winner, sized in full (DICT / RLE below)
+    if (win == M_XORZ) consider(M_XORZ, S.xor_bytes);
+    if (win == M_FOR_BITPACK) consider(M_FOR_BITPACK, sz_for);
+    if (win == M_DELTA_BITPACK) consider(M_DELTA_BITPACK, sz_delta);
+    if (win == M_ALP && c_alp.ok) consider(M_ALP, c_alp.len);
+    if (win == M_ALP_RD && c_rd.ok) consider(M_ALP_RD, c_rd.len);
+  } else {
+    if (!reduced) consider(M_XORZ, S.xor_bytes);
+    consider(M_FOR_BITPACK, sz_for);
+    consider(M_DELTA_BITPACK, sz_delta);
+    if (c_fm.ok) consider(M_FLOAT_MULT, c_fm.len);
+    if (c_alp.ok) consider(M_ALP, c_alp.len);
+    if (c_rd.ok) consider(M_ALP_RD, c_rd.len);
+  }
   bool block_compressible = best_len * 20 < raw_bytes * 19;  // encoder.rs:394,644-646
 
   if (ENT && block_compressible) {
@@ -1939,13 +2169,15 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
     }
   }
 
-  if (block_compressible && !reduced) {
+  if (SAMPLE ? (win == M_DICT || win == M_RLE) : (block_compressible && !reduced)) {
     // DICT (dict.rs:87-152, bit-packed codes).  The dictionary is sorted, so
     // a sub-block's code range is [rank(min), rank(max)].
     bool one_win = !fixed_bs && (fd.value_off % kBaseQuantum) == 0 && n <= (uint32_t)kBaseQuantum;
     uint32_t lb_pre = one_win ? winbits[(fd.value_off / kBaseQuantum) * kWinWords + 1024] : kNoLb;
-    DictView dv = dict_prepare(S, v, n, scr, lb_pre);
-    if (!S.flag) {
+    bool want_dict = !SAMPLE || win == M_DICT;
+    DictView dv;
+    if (want_dict) dv = dict_prepare(S, v, n, scr, lb_pre);
+    if (want_dict && !S.flag) {
       uint32_t vtag;
       uint64_t vlen = dict_values_len(S, dv, &vtag);
       if (ENT) {  // TRANSPOSE values, kept when strictly smaller (dict.rs:52-59)
@@ -1993,7 +2225,7 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
     __syncthreads();
     // RLE (rle.rs:10-42)
     uint32_t neq = S.neq;
-    if (neq <= n / 2 + 1) {
+    if ((!SAMPLE || win == M_RLE) && neq <= n / 2 + 1) {
       uint32_t runs = neq + 1;
       uint32_t* st = rle_starts(S, v, n, runs, scr);
       uint64_t lens = block_for(S, nullptr, runs, false, [&](uint32_t r) {
@@ -2595,21 +2827,26 @@ void launch_sub_stats(const uint64_t* lane, uint64_t n, uint64_t fixed_bs, int d
 
 void launch_decide(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, uint64_t fixed_bs,
                    int dtype, int level, const void* ss, const void* fms, const uint64_t* smp16,
-                   const uint32_t* winbits, uint8_t* scratch, void* ent, cudaStream_t st) {
+                   const uint32_t* winbits, uint8_t* scratch, void* ent, bool sample, cudaStream_t st) {
   int sm = (int)enc_smem_bytes();
-  cudaFuncSetAttribute(k_decide<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_decide<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_decide<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_decide<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_decide<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   cudaFuncSetAttribute(k_emit<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   cudaFuncSetAttribute(k_emit<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (max_blocks) {
     if (ent)
-      k_decide<true><<<max_blocks, kEncThreads, sm, st>>>(lane, frames, nb, fixed_bs, dtype, level,
+      k_decide<true, false><<<max_blocks, kEncThreads, sm, st>>>(lane, frames, nb, fixed_bs, dtype, level,
                                                           (const SubStats*)ss, (const FmStat*)fms, smp16, winbits,
                                                           scratch, (EntRec*)ent);
+    else if (sample)
+      k_decide<false, true><<<max_blocks, kEncThreads, sm, st>>>(lane, frames, nb, fixed_bs, dtype, level,
+                                                                 (const SubStats*)ss, (const FmStat*)fms, smp16,
+                                                                 winbits, scratch, nullptr);
     else
-      k_decide<false><<<max_blocks, kEncThreads, sm, st>>>(lane, frames, nb, fixed_bs, dtype, level,
-                                                           (const SubStats*)ss, (const FmStat*)fms, smp16, winbits,
-                                                           scratch, nullptr);
+      k_decide<false, false><<<max_blocks, kEncThreads, sm, st>>>(lane, frames, nb, fixed_bs, dtype, level,
+                                                                  (const SubStats*)ss, (const FmStat*)fms, smp16,
+                                                                  winbits, scratch, nullptr);
   }
   count_launches(max_blocks ? 1 : 0);
 }

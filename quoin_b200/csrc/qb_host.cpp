@@ -307,7 +307,12 @@ uint64_t lane_bound(uint64_t n_valid, uint64_t logical_n, int dtype, bool validi
 
 // Runs the GPU competition and emission for one lane (reference
 // encoder.rs:184-214).  Writes the stream at d_dst and its length to *out_len.
+// LaneJob::level carries Selection::Sample as kSelectSample beside the level.
+constexpr int kSelectSample = 0x100;
+
 int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, size_t dst_cap, size_t* out_len) {
+  const int level = j.level & 0xFF;
+  const bool sample = (j.level & kSelectSample) != 0;
   uint64_t n = j.n_valid;
   uint64_t bs = j.block_size ? (j.block_size > kMaxBlockValues ? kMaxBlockValues : j.block_size) : 0;
   uint64_t maxb = max_blocks_for(n, bs);
@@ -367,7 +372,7 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
     CK(c->ensure(S_SMP16, (n / 16 + 2) * 8));
   }
   void* ent = nullptr;  // Balanced in-pool: the chosen rANS-coded parts per block
-  if (j.level >= 2) {
+  if (level >= 2) {
     CK(c->ensure(S_ENTREC, maxb * ent_rec_bytes()));
     ent = c->p<void>(S_ENTREC);
   }
@@ -375,15 +380,15 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
   uint32_t* nb = c->p<uint32_t>(S_NB);
   {
     TimedRegion tr(T_PLAN, st);
-    launch_sub_stats(j.lane, n, bs, j.dtype, j.level, c->p<void>(S_SUBST), fl ? c->p<void>(S_FMST) : nullptr,
+    launch_sub_stats(j.lane, n, bs, j.dtype, level, c->p<void>(S_SUBST), fl ? c->p<void>(S_FMST) : nullptr,
                      fl ? c->p<uint64_t>(S_SMP16) : nullptr, c->p<uint8_t>(S_GROW), c->p<uint32_t>(S_WINBITS), st);
     launch_plan(c->p<uint8_t>(S_GROW), n, bs, fr, nb, st);
   }
   {
     TimedRegion tr(T_COMPETE, st);
-    launch_decide(j.lane, fr, nb, (uint32_t)maxb, bs, j.dtype, j.level, c->p<void>(S_SUBST),
+    launch_decide(j.lane, fr, nb, (uint32_t)maxb, bs, j.dtype, level, c->p<void>(S_SUBST),
                   fl ? c->p<void>(S_FMST) : nullptr, fl ? c->p<uint64_t>(S_SMP16) : nullptr,
-                  c->p<uint32_t>(S_WINBITS), c->p<uint8_t>(S_SCRATCH), ent, st);
+                  c->p<uint32_t>(S_WINBITS), c->p<uint8_t>(S_SCRATCH), ent, sample, st);
   }
   {
     TimedRegion tr(T_OTHER, st);
@@ -406,14 +411,19 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
   return QUOIN_OK;
 }
 
+// *level gets kSelectSample added for Selection::Sample (Fastest and Fast).
 int check_level(const QuoinConfig* cfg, int* level, uint64_t* bs, uint8_t* plog2) {
   int lv = cfg ? cfg->level : QUOIN_LEVEL_FAST;
+  int32_t sel = cfg ? cfg->selection : QUOIN_B200_SELECTION_FULL;
+  if (sel != QUOIN_B200_SELECTION_FULL && sel != QUOIN_B200_SELECTION_SAMPLE) return QUOIN_ERR_BAD_ARG;
   if (lv == QUOIN_B200_LEVEL_BALANCED_INPOOL) {
     lv = QUOIN_LEVEL_BALANCED;  // Balanced's candidate pool without Lz and Pco
+    if (sel == QUOIN_B200_SELECTION_SAMPLE) return QUOIN_ERR_UNSUPPORTED;
   } else {
     if (lv < 0 || lv > 4) return QUOIN_ERR_BAD_ARG;
     if (lv >= QUOIN_LEVEL_BALANCED) return QUOIN_ERR_UNSUPPORTED;
   }
+  if (sel == QUOIN_B200_SELECTION_SAMPLE) lv |= kSelectSample;
   int64_t b = cfg ? cfg->block_size : 0;
   int32_t p = cfg ? cfg->predictor_log2 : 16;
   *level = lv;

@@ -83,10 +83,11 @@ void launch_plan(const uint8_t* grow, uint64_t n, uint64_t fixed_bs, FrameDesc* 
 // Competition part 2: one CTA per planned block; writes mode / plen / aux.
 // With `ent` (max_blocks records of ent_rec_bytes()) the Balanced in-pool
 // candidates run too (rANS-coded parts, BYTE_TRANSPOSE) and their choices
-// are recorded there for the emission.
+// are recorded there for the emission.  `sample`: Selection::Sample (levels
+// Fastest and Fast; not with `ent`).
 void launch_decide(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, uint64_t fixed_bs,
                    int dtype, int level, const void* ss, const void* fms, const uint64_t* smp16,
-                   const uint32_t* winbits, uint8_t* scratch, void* ent, cudaStream_t st);
+                   const uint32_t* winbits, uint8_t* scratch, void* ent, bool sample, cudaStream_t st);
 uint64_t ent_rec_bytes();
 // `base` (device) holds the byte offset at which the first frame starts.
 void launch_frame_offsets(FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, const uint64_t* base,
