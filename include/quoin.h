@@ -55,6 +55,7 @@ extern "C" {
 #define QUOIN_ERR_CUDA                (-19) /* a CUDA call failed (no device, OOM, ...)   */
 #define QUOIN_ERR_BAD_ARG             (-20)
 #define QUOIN_ERR_NOALLOC_LIMIT       (-21) /* stream outside quoin_b200_decompress_device_noalloc's limits */
+#define QUOIN_ERR_UNSUPPORTED_ARROW_TYPE (-22) /* Error::UnsupportedArrowType (src/error.rs) */
 
 /* ---------------- reference ABI (capi/include/quoin.h:35-142) ---------------- */
 
@@ -249,6 +250,57 @@ uint64_t quoin_b200_kernel_launches(void);
  * of classes written (ms totals and call counts). */
 void quoin_b200_timing_enable(int on);
 int quoin_b200_timing_read(double *ms_out, uint64_t *calls_out, int n);
+
+/* ---------------- Arrow C Data Interface ---------------- */
+
+/* The standard Arrow C Data Interface structs (declared here unless the
+ * caller's Arrow headers already did). */
+#ifndef ARROW_C_DATA_INTERFACE
+#define ARROW_C_DATA_INTERFACE
+#define ARROW_FLAG_DICTIONARY_ORDERED 1
+#define ARROW_FLAG_NULLABLE 2
+#define ARROW_FLAG_MAP_KEYS_SORTED 4
+struct ArrowSchema {
+    const char *format;
+    const char *name;
+    const char *metadata;
+    int64_t flags;
+    int64_t n_children;
+    struct ArrowSchema **children;
+    struct ArrowSchema *dictionary;
+    void (*release)(struct ArrowSchema *);
+    void *private_data;
+};
+struct ArrowArray {
+    int64_t length;
+    int64_t null_count;
+    int64_t offset;
+    int64_t n_buffers;
+    int64_t n_children;
+    const void **buffers;
+    struct ArrowArray **children;
+    struct ArrowArray *dictionary;
+    void (*release)(struct ArrowArray *);
+    void *private_data;
+};
+#endif
+typedef struct ArrowSchema ArrowSchema;
+typedef struct ArrowArray ArrowArray;
+
+/* Replaces compress_array(&dyn Array, Config) (src/arrow.rs:61-123): compresses
+ * a primitive Arrow array (Float64 "g", Float32 "f", Int64 "l", UInt64 "L",
+ * Int32 "i", UInt32 "I", Decimal128 "d:P,S", Decimal256 "d:P,S,256") with its
+ * validity; the array's offset is honoured (a sliced bitmap is re-packed).
+ * Other types: QUOIN_ERR_UNSUPPORTED_ARROW_TYPE.  The array is only read. */
+int quoin_b200_compress_arrow(QuoinCtx *ctx, const struct ArrowSchema *schema,
+                              const struct ArrowArray *array, const QuoinConfig *cfg, uint8_t *dst,
+                              size_t dst_cap, size_t *out_len);
+
+/* Replaces decompress_array(&[u8]) (src/arrow.rs:129-160): fills *schema_out and
+ * *array_out with a new array of the stream's type (null slots hold 0); the
+ * caller owns both and frees them through their release callbacks. */
+int quoin_b200_decompress_arrow(QuoinCtx *ctx, const uint8_t *src, size_t src_len,
+                                struct ArrowSchema *schema_out, struct ArrowArray *array_out);
 
 #ifdef __cplusplus
 } /* extern "C" */
