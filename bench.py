@@ -354,45 +354,104 @@ def run_gpu(args, rank, world, local):
         per_column[c["name"]]["stream_bytes"] = c["len"]
     L.quoin_b200_timing_enable(0)
 
-    # e2e through the host-buffer C ABI with pinned host memory.
+    # e2e through the host-buffer C ABI with pinned host memory.  Each column
+    # is a two-stage stream: one host thread compresses step after step (its
+    # context), another decompresses each step's stream as it arrives (a
+    # second context), with two stream buffers between them, so one step's
+    # decompress (mostly device -> host) overlaps the next step's compress
+    # (mostly host -> device).  --serial-columns runs compress then
+    # decompress of one column at a time from one thread.
+    import queue
+    import threading
+
+    dctxs = [ctypes.c_void_p(L.quoin_ctx_create(0)) for _ in gcols]
     pinned = []
     for c in gcols:
         hv = torch.from_numpy(np.ascontiguousarray(c["v"]).view(np.uint8).copy()).pin_memory()
         hb = torch.from_numpy(c["bm"].copy()).pin_memory() if c["bm"] is not None else None
-        hdst = torch.empty(c["len"] + (1 << 20), dtype=torch.uint8).pin_memory()
+        hdst = [torch.empty(c["len"] + (1 << 20), dtype=torch.uint8).pin_memory() for _ in range(2)]
         hout = torch.empty(n * c["w"], dtype=torch.uint8).pin_memory()
         hvout = torch.empty((n + 7) // 8, dtype=torch.uint8).pin_memory()
         pinned.append((hv, hb, hdst, hout, hvout))
 
-    def e2e_one(cp):  # compress then decompress one column through the host-buffer API
-        c, (hv, hb, hdst, hout, hvout) = cp
+    def e2e_compress(c, pin, slot):
+        hv, hb, hdst, _, _ = pin
         olen = ctypes.c_size_t()
         rc = L.quoin_b200_compress_column(c["ctx"], c["wire"], n, P(hv.data_ptr()),
-                                          P(hb.data_ptr()) if hb is not None else None, 0, 0,
-                                          ctypes.byref(cfg), P(hdst.data_ptr()), hdst.numel(), ctypes.byref(olen))
+                                          P(hb.data_ptr()) if hb is not None else None, 0, 0, ctypes.byref(cfg),
+                                          P(hdst[slot].data_ptr()), hdst[slot].numel(), ctypes.byref(olen))
         if rc:
             raise Q.Error(rc)
-        rc = L.quoin_b200_decompress_column(c["ctx"], P(hdst.data_ptr()), olen.value, P(hout.data_ptr()),
+        return olen.value
+
+    def e2e_decompress(ci, pin, slot, olen):
+        _, _, hdst, hout, hvout = pin
+        rc = L.quoin_b200_decompress_column(dctxs[ci], P(hdst[slot].data_ptr()), olen, P(hout.data_ptr()),
                                             P(hvout.data_ptr()))
         if rc:
             raise Q.Error(rc)
-        return (hv.numel() + (hb.numel() if hb is not None else 0) + olen.value,
-                olen.value + hout.numel() + (hvout.numel() if hb is not None else 0))
 
-    def e2e_step():  # the columns' host copies overlap in both directions
+    def e2e_bytes():
+        h2d = d2h = 0
+        for c, (hv, hb, hdst, hout, hvout) in zip(gcols, pinned):
+            h2d += hv.numel() + (hb.numel() if hb is not None else 0) + c["len"]
+            d2h += c["len"] + hout.numel() + (hvout.numel() if hb is not None else 0)
+        return h2d, d2h
+
+    def e2e_run(steps):
         if args.serial_columns:
-            r = [e2e_one(cp) for cp in zip(gcols, pinned)]
-        else:
-            r = list(pool.map(e2e_one, zip(gcols, pinned)))
-        return sum(a for a, _ in r), sum(b for _, b in r)
+            for _ in range(steps):
+                for ci, (c, pin) in enumerate(zip(gcols, pinned)):
+                    e2e_decompress(ci, pin, 0, e2e_compress(c, pin, 0))
+            return
+        errors = []
 
-    e2e_step()
+        def column(ci):
+            c, pin = gcols[ci], pinned[ci]
+            q = queue.Queue()
+            free = threading.Semaphore(2)
+
+            def produce():
+                try:
+                    for k in range(steps):
+                        free.acquire()
+                        q.put((k % 2, e2e_compress(c, pin, k % 2)))
+                except Exception as e:  # noqa: BLE001 - reported after the join
+                    errors.append(e)
+                q.put(None)
+
+            prod = threading.Thread(target=produce)
+            prod.start()
+            try:
+                while True:
+                    item = q.get()
+                    if item is None:
+                        break
+                    e2e_decompress(ci, pin, item[0], item[1])
+                    free.release()
+            except Exception as e:  # noqa: BLE001
+                errors.append(e)
+                while prod.is_alive():  # let the producer finish its queued work
+                    free.release()
+                    if q.get() is None:
+                        break
+            prod.join()
+
+        threads = [threading.Thread(target=column, args=(ci,)) for ci in range(len(gcols))]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        if errors:
+            raise errors[0]
+
+    e2e_run(1)
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        h2d, d2h = e2e_step()
+    e2e_run(args.steps)
     e2e_s = time.perf_counter() - t0
+    h2d, d2h = e2e_bytes()
     e2e_s = max_over_ranks([e2e_s], world, dev)[0]
     e2e_gbs = whole_job_gbs(raw_bytes, world, args.steps, e2e_s)
 
@@ -434,14 +493,16 @@ def run_gpu(args, rank, world, local):
                          "traffic": None, "decode_calls_per_step": per_class["decode"][1] // max(args.steps, 1)},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "timing": "wall clock around synchronous host-buffer C-ABI calls (one host thread and "
-                              "context per column), pinned host memory"},
+                    "timing": ("wall clock around synchronous host-buffer C-ABI calls, pinned host memory; "
+                               + ("one column at a time" if args.serial_columns else
+                                  "per column one thread compresses step after step and another decompresses "
+                                  "each step's stream (two stream buffers), so the two copy directions overlap"))},
             "gpu_launches": int(launches // max(args.steps, 1) * args.steps),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     pool.shutdown()
-    for cx in ctxs:
+    for cx in ctxs + dctxs:
         L.quoin_ctx_free(cx)
     if world > 1:
         dist.destroy_process_group()
