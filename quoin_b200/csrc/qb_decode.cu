@@ -722,6 +722,50 @@ __device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64
 }
 
 // ---------------------------------------------------------------------------
+// ALP-RD exceptions (alp_rd.rs:281-283): vals[p] = (left << rbw) | rights[p]
+// for each (varint p, u64 left) record, in list order.  The list is read by
+// thread 0 (its byte layout is sequential) in chunks into shared memory; a
+// chunk whose positions strictly increase (every list the encoder writes) is
+// then applied by the whole CTA, whose random reads of the rights and the
+// values overlap; otherwise thread 0 applies it in order.  The records were
+// validated by the frame walk (positions < n, no truncation).
+// ---------------------------------------------------------------------------
+constexpr uint32_t kExcChunk = 4096;
+__device__ void alprd_exceptions(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t pos, uint64_t nexc,
+                                 const uint8_t* rsrc, const uint32_t* roffs, uint32_t rbw, uint64_t* vals) {
+  uint32_t* epos = reinterpret_cast<uint32_t*>(&S.u.wbuf[0][0]);  // 16 KB
+  uint64_t* elv = &S.u.wbuf[0][0] + kExcChunk / 2;                  // 32 KB
+  int t = threadIdx.x;
+  __syncthreads();  // every thread has read S.flag and left the staging buffers
+  for (uint64_t x0 = 0; x0 < nexc; x0 += kExcChunk) {
+    uint32_t cnt = (uint32_t)qmin(kExcChunk, nexc - x0);
+    if (t == 0) {
+      uint32_t inc = 1;
+      for (uint32_t k = 0; k < cnt; k++) {
+        uint64_t pp = 0;
+        rd_varint(p, plen, &pos, &pp);
+        elv[k] = ld_u64(p + pos);
+        pos += 8;
+        epos[k] = (uint32_t)pp;
+        if (k && pp <= epos[k - 1]) inc = 0;
+      }
+      S.flag = inc;
+    }
+    __syncthreads();
+    auto apply = [&](uint32_t k) {
+      uint32_t pp = epos[k];
+      vals[pp] = (elv[k] << rbw) | for_value_at(rsrc, roffs[pp / kSub], pp % kSub);
+    };
+    if (S.flag) {
+      for (uint32_t k = t; k < cnt; k += blockDim.x) apply(k);
+    } else if (t == 0) {
+      for (uint32_t k = 0; k < cnt; k++) apply(k);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Entropy-coded parts (Balanced and above): the 4-state rANS blocks of
 // rans.rs:110-175 behind the entropy tag of entropy/mod.rs:152-178.
 // ---------------------------------------------------------------------------
@@ -932,16 +976,7 @@ __device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDes
       }
       __syncthreads();
       if (S.flag) return E_CORRUPT;
-      if (t == 0 && A.d) {  // exceptions in order (alp_rd.rs:281-283): (left << rbw) | rights[p]
-        uint64_t pos = A.c;
-        for (uint64_t x = 0; x < A.d; x++) {
-          uint64_t pp = 0;
-          rd_varint(p, plen, &pos, &pp);
-          uint64_t lv = ld_u64(p + pos);
-          pos += 8;
-          vals[pp] = (lv << rbw) | for_value_at(rsrc, S.eoffs[pp / kSub], (uint32_t)(pp % kSub));
-        }
-      }
+      if (A.d) alprd_exceptions(S, p, plen, A.c, A.d, rsrc, S.eoffs, rbw, vals);
       __syncthreads();
       cta_store(O, c0, (uint32_t)n, [&](uint32_t q) { return vals[q]; });
       return E_OK;
@@ -1219,17 +1254,7 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
         break;
       }
       if (fo) {
-        if (t == 0) {  // exceptions in order (alp_rd.rs:281-283): (left << rbw) | rights[p]
-          uint64_t pos = A.c;
-          for (uint64_t x = 0; x < A.d; x++) {
-            uint64_t pp = 0;
-            rd_varint(p, plen, &pos, &pp);
-            uint64_t lv = ld_u64(p + pos);
-            pos += 8;
-            fo[pp] = (lv << rbw) | for_value_at(p, A.offs[1][pp / kSub], (uint32_t)(pp % kSub));
-          }
-        }
-        __syncthreads();
+        alprd_exceptions(S, p, plen, A.c, A.d, p, A.offs[1], rbw, fo);
         cta_store(O, c0, (uint32_t)n, [&](uint32_t q) { return fo[q]; });
       }
       break;
