@@ -509,6 +509,158 @@ def run_gpu(args, rank, world, local):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Batched configuration (--workload config3): many columns of uneven length
+# and mixed dtype, plain per-column calls on one context vs batch calls over
+# a pool of contexts (quoin_b200_*_batch_device).
+# ---------------------------------------------------------------------------
+def run_gpu_config3(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    import quoin_b200 as Q
+    from quoin_b200 import synth
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    L = Q.lib
+    P, S = ctypes.c_void_p, ctypes.c_size_t
+
+    class CompressJob(ctypes.Structure):
+        _fields_ = [("wire_dtype", ctypes.c_int32), ("scale", ctypes.c_int8), ("precision", ctypes.c_uint8),
+                    ("n", S), ("d_values", P), ("d_validity", P), ("d_dst", P), ("dst_cap", S), ("out_len", S),
+                    ("status", ctypes.c_int32)]
+
+    class DecompressJob(ctypes.Structure):
+        _fields_ = [("idx", P), ("d_src", P), ("d_values_out", P), ("d_validity_out", P),
+                    ("status", ctypes.c_int32)]
+
+    L.quoin_b200_batch_create.restype = P
+    L.quoin_b200_batch_create.argtypes = [ctypes.c_int]
+    L.quoin_b200_batch_free.argtypes = [P]
+    L.quoin_b200_compress_batch_device.argtypes = [P, ctypes.POINTER(CompressJob), S,
+                                                   ctypes.POINTER(Q._QuoinConfig)]
+    L.quoin_b200_decompress_batch_device.argtypes = [P, ctypes.POINTER(DecompressJob), S]
+    cfg = Q._QuoinConfig(int(Q.Level.FAST), 0, 16, 0)
+    cols = synth.config3_columns(args.columns, args.max_len)
+    ctx = P(L.quoin_ctx_create(0))
+    batch = P(L.quoin_b200_batch_create(args.workers))
+    raw_bytes = 0
+    gc = []
+    for name, dt, v, bm in cols:
+        nb = np.ascontiguousarray(v).nbytes
+        raw_bytes += nb
+        dv = torch.from_numpy(np.ascontiguousarray(v).view(np.uint8).reshape(-1).copy()).to(dev)
+        db = torch.from_numpy(bm.copy()).to(dev) if bm is not None else None
+        cap = Q._stream_bound(dt, len(v), bm is not None)
+        gc.append(dict(dt=dt, n=len(v), sc=4 if dt == Q.DECIMAL128 else 0, pr=18 if dt == Q.DECIMAL128 else 0,
+                       dv=dv, db=db, cap=cap, dd=torch.empty(cap, dtype=torch.uint8, device=dev),
+                       dout=torch.empty(max(nb, 8), dtype=torch.uint8, device=dev),
+                       dvb=torch.empty(max((len(v) + 7) // 8, 1), dtype=torch.uint8, device=dev), v=v, bm=bm))
+    cjobs = (CompressJob * len(gc))()
+    for j, c in enumerate(gc):
+        cjobs[j] = CompressJob(c["dt"], c["sc"], c["pr"], c["n"], c["dv"].data_ptr(),
+                               c["db"].data_ptr() if c["db"] is not None else None, c["dd"].data_ptr(), c["cap"],
+                               0, 0)
+    torch.cuda.synchronize()
+    # first pass: batched compress, then indices, bit-exact round trip
+    if L.quoin_b200_compress_batch_device(batch, cjobs, len(gc), ctypes.byref(cfg)):
+        raise Q.Error(next(cjobs[j].status for j in range(len(gc)) if cjobs[j].status))
+    stream_bytes = 0
+    djobs = (DecompressJob * len(gc))()
+    for j, c in enumerate(gc):
+        c["len"] = cjobs[j].out_len
+        stream_bytes += c["len"]
+        hs = c["dd"][: c["len"]].cpu().numpy().tobytes()
+        idx = P()
+        if L.quoin_b200_index_create(ctx, hs, len(hs), ctypes.byref(idx)):
+            raise Q.Error(-14)
+        c["idx"] = idx
+        djobs[j] = DecompressJob(idx, c["dd"].data_ptr(), c["dout"].data_ptr(), c["dvb"].data_ptr(), 0)
+    if L.quoin_b200_decompress_batch_device(batch, djobs, len(gc)):
+        raise Q.Error(-14)
+    torch.cuda.synchronize()
+    bit_exact = True
+    for c in gc:
+        raw = np.ascontiguousarray(c["v"]).view(np.uint8).reshape(c["n"], -1).copy()
+        if c["bm"] is not None:
+            raw[~np.unpackbits(c["bm"], bitorder="little")[: c["n"]].astype(bool)] = 0
+        if c["dout"][: raw.size].cpu().numpy().tobytes() != raw.tobytes():
+            bit_exact = False
+
+    def plain():
+        for c in gc:
+            olen = ctypes.c_size_t()
+            rc = L.quoin_b200_compress_column_device(
+                ctx, c["dt"], c["n"], P(c["dv"].data_ptr()), P(c["db"].data_ptr()) if c["db"] is not None else None,
+                c["sc"], c["pr"], ctypes.byref(cfg), P(c["dd"].data_ptr()), c["cap"], ctypes.byref(olen), None)
+            if rc:
+                raise Q.Error(rc)
+        for c in gc:
+            rc = L.quoin_b200_decompress_indexed_device(ctx, c["idx"], P(c["dd"].data_ptr()), P(c["dout"].data_ptr()),
+                                                        P(c["dvb"].data_ptr()), None)
+            if rc:
+                raise Q.Error(rc)
+
+    def batched():
+        if L.quoin_b200_compress_batch_device(batch, cjobs, len(gc), ctypes.byref(cfg)):
+            raise Q.Error(-14)
+        if L.quoin_b200_decompress_batch_device(batch, djobs, len(gc)):
+            raise Q.Error(-14)
+
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()  # every call returns after its columns' device work completed
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks([e0.elapsed_time(e1)], world, dev)[0]
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    batched_ms = timed(batched)
+    clocks = sampler.stop()
+    plain_ms = timed(plain)
+    value = whole_job_gbs(raw_bytes, world, args.steps, batched_ms / 1e3)
+    plain_gbs = whole_job_gbs(raw_bytes, world, args.steps, plain_ms / 1e3)
+    for c in gc:
+        L.quoin_b200_index_free(c["idx"])
+    L.quoin_b200_batch_free(batch)
+    L.quoin_ctx_free(ctx)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(batched_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "mixed (f64/f32/i64/u64/i32/u32/decimal128)",
+            "data": "synthetic",
+            "config": {"workload": f"config3: {len(gc)} columns, lengths floor(exp(U[ln 1024, ln {args.max_len}])), "
+                                   "dtype uniform over 7, null rate U(0,0.2); Level::Fast",
+                       "columns": len(gc), "global_values": int(sum(c["n"] for c in gc)) * world,
+                       "uncompressed_bytes": raw_bytes, "workers": args.workers,
+                       "parallelism": f"replicas x{world}"},
+            "plain_gbs": round(plain_gbs, 3), "batched_over_plain": round(value / plain_gbs, 3) if plain_gbs else None,
+            "ratio": round(raw_bytes / stream_bytes, 4), "bit_exact": bit_exact,
+            "cpu_baseline": None, "clocks": clocks,
+            "note": "plain = per-column compress_column_device / decompress_indexed_device calls on one context; "
+                    "value = the same columns through the batch calls",
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -520,10 +672,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serial-columns", action="store_true",
                     help="one host thread runs the columns one after another (for profilers)")
+    ap.add_argument("--workload", default="config1", choices=["config1", "config3"],
+                    help="config3: the batched configuration (plain vs batch calls)")
+    ap.add_argument("--columns", type=int, default=256, help="config3: number of columns")
+    ap.add_argument("--max-len", type=int, default=1 << 21, help="config3: longest column")
+    ap.add_argument("--workers", type=int, default=8, help="config3: contexts in the batch")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "config3":
+        return run_gpu_config3(args, rank, world, local)
     return run_gpu(args, rank, world, local)
 
 

@@ -251,6 +251,49 @@ uint64_t quoin_b200_kernel_launches(void);
 void quoin_b200_timing_enable(int on);
 int quoin_b200_timing_read(double *ms_out, uint64_t *calls_out, int n);
 
+/* ---------------- batches of columns ---------------- */
+
+/* No reference counterpart (the batched configuration: many columns of uneven
+ * length and mixed dtype).  A batch holds `workers` contexts (1..64) on the
+ * current device; a batch call hands its columns, longest first, to one host
+ * worker per context, so short columns' launch and synchronisation latencies
+ * overlap.  Every column's stream is byte-identical to the single-column
+ * call's.  One batch call at a time per batch. */
+typedef struct QuoinBatch QuoinBatch;
+QuoinBatch *quoin_b200_batch_create(int workers);
+void quoin_b200_batch_free(QuoinBatch *batch);
+
+/* One column of quoin_b200_compress_batch_device: the arguments of
+ * quoin_b200_compress_column_device (device pointers) and its results. */
+typedef struct {
+    int32_t wire_dtype;
+    int8_t scale;
+    uint8_t precision;
+    size_t n;
+    const void *d_values;
+    const uint8_t *d_validity;
+    uint8_t *d_dst;
+    size_t dst_cap;
+    size_t out_len; /* out: stream length (the needed size on BUFFER_TOO_SMALL) */
+    int32_t status; /* out: the column's return code */
+} QuoinB200CompressJob;
+
+/* One column of quoin_b200_decompress_batch_device: the arguments of
+ * quoin_b200_decompress_indexed_device and its return code. */
+typedef struct {
+    const QuoinDecodeIndex *idx;
+    const uint8_t *d_src;
+    void *d_values_out;
+    uint8_t *d_validity_out;
+    int32_t status; /* out */
+} QuoinB200DecompressJob;
+
+/* Every job is attempted; returns QUOIN_OK, or the status of the first failing
+ * job in job order (each job's own status is in its record). */
+int quoin_b200_compress_batch_device(QuoinBatch *batch, QuoinB200CompressJob *jobs, size_t njobs,
+                                     const QuoinConfig *cfg);
+int quoin_b200_decompress_batch_device(QuoinBatch *batch, QuoinB200DecompressJob *jobs, size_t njobs);
+
 /* ---------------- Arrow C Data Interface ---------------- */
 
 /* The standard Arrow C Data Interface structs (declared here unless the

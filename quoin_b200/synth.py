@@ -9,7 +9,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import DECIMAL128, F32, F64, I32, I64, U64
+from . import DECIMAL128, F32, F64, I32, I64, U32, U64
 
 BASE_SEED = 20261203
 
@@ -114,3 +114,34 @@ def config_columns(config: str, n: int):
             ("decimal128", DECIMAL128, decimal128_uniform(n, r[2]), None),
         ]
     raise ValueError(config)
+
+
+def config3_columns(ncols: int, max_len: int = 1 << 21, min_len: int = 1024):
+    """The batched configuration: `ncols` columns with lengths floor(exp(U[ln min_len,
+    ln max_len])), dtype uniform over f64/f32/i64/u64/i32/u32/decimal128, the
+    per-dtype generators of configs 0-2, and a null rate U(0, 0.2) each.
+    [(name, wire dtype, values, validity bitmap or None)]."""
+    dtypes = [F64, F32, I64, U64, I32, U32, DECIMAL128]
+    out = []
+    for c in range(ncols):
+        r = rng_for(3, c)
+        n = int(np.floor(np.exp(r.uniform(np.log(min_len), np.log(max_len)))))
+        dt = dtypes[int(r.integers(0, len(dtypes)))]
+        null_rate = float(r.uniform(0.0, 0.2))
+        if dt == F64:
+            v = prices_f64(n, r) if c % 2 == 0 else random_walk_f64(n, r)
+        elif dt == F32:
+            v = sensor_f32(n, r)
+        elif dt == I64:
+            v = timestamps_i64(n, r)
+        elif dt == U64:
+            v = runs_u64(n, r)
+        elif dt == I32:
+            v = categories_i32(n, r)
+        elif dt == U32:
+            v = categories_i32(n, r).view(np.uint32)
+        else:
+            v = decimal128_uniform(n, r)
+        bm = bernoulli_bitmap(r, n, 1.0 - null_rate) if null_rate > 0 else None
+        out.append((f"col{c}", dt, v, bm))
+    return out
