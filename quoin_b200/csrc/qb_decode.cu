@@ -31,6 +31,8 @@ struct FrameAux {
   uint64_t a, b, c, d;  // mode-specific scalars
   uint64_t e0, e1, e2;  // entropy-coded parts: payload positions
   uint32_t t0, t1;      // and their tags
+  uint32_t defer;       // 1: an ALP-RD exception list left to the frame kernel's walk
+  uint32_t pad_;
   uint64_t dict8[8];    // ALP-RD dictionary
   uint32_t offs[2][kMaxSubs + 1];  // chain 0 / chain 1 sub-block header offsets (payload-relative)
 };
@@ -92,6 +94,41 @@ __device__ uint32_t alp_walk(const uint8_t* p, uint64_t plen, uint64_t n, uint32
   return E_OK;
 }
 
+// ALP-RD payload after the exception list (alp_rd.rs:208-285): codes tag,
+// varint(codes_len), codes, rights tag, rights.  Bit-packed parts get their
+// FoR sub-block offsets; an entropy-coded part (tag 1) leaves the rest to the
+// frame kernel's entropy path.
+__device__ uint32_t alprd_walk_tail(const uint8_t* p, uint64_t plen, uint64_t n, uint64_t pos, FrameAux& A) {
+  if (pos >= plen) return E_TRUNCATED;
+  uint32_t ctag = p[pos++];
+  uint64_t clen;
+  uint32_t e = rd_varint(p, plen, &pos, &clen);
+  if (e) return e;
+  if (clen > plen - pos) return E_TRUNCATED;
+  uint64_t cpos = pos;
+  pos += clen;
+  if (pos >= plen) return E_TRUNCATED;
+  uint32_t rtag = p[pos++];
+  A.e0 = cpos;
+  A.e1 = clen;
+  A.e2 = pos;
+  A.t0 = ctag;
+  A.t1 = rtag;
+  if (ctag == 1) {  // codes entropy-coded: the frame kernel decodes the rest in order
+    A.ent = 1;
+    return E_OK;
+  }
+  if (ctag != 0) return E_CORRUPT;
+  e = for_walk(p, cpos + clen, cpos, n, A.offs[0]);
+  if (e) return e;
+  if (rtag == 1) {  // rights entropy-coded (bit-packed rights bytes)
+    A.ent = 1;
+    return E_OK;
+  }
+  if (rtag != 0) return E_CORRUPT;
+  return for_walk(p, plen, pos, n, A.offs[1]);
+}
+
 // One thread per frame.
 __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDesc* __restrict__ frames, int nf,
                               int dtype, FrameAux* __restrict__ aux, unsigned long long* __restrict__ err) {
@@ -102,6 +139,7 @@ __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDes
   uint64_t plen = d.plen, n = d.n;
   FrameAux& A = aux[f];
   A.ent = 0;
+  A.defer = 0;
   uint32_t e = E_OK;
   switch (d.mode) {
     case M_RAW:
@@ -160,49 +198,15 @@ __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDes
       e = rd_varint(p, plen, &pos, &nexc);
       if (e) break;
       if (nexc > n) { e = E_CORRUPT; break; }
-      uint64_t exc_start = pos;
-      for (uint64_t x = 0; x < nexc && !e; x++) {
-        uint64_t pp;
-        e = rd_varint(p, plen, &pos, &pp);
-        if (e) break;
-        if (plen < pos + 8) { e = E_TRUNCATED; break; }
-        pos += 8;
-        if (pp >= n) e = E_CORRUPT;
-      }
-      if (e) break;
-      if (pos >= plen) { e = E_TRUNCATED; break; }
-      uint32_t ctag = p[pos++];
-      uint64_t clen;
-      e = rd_varint(p, plen, &pos, &clen);
-      if (e) break;
-      if (clen > plen - pos) { e = E_TRUNCATED; break; }
-      uint64_t cpos = pos;
-      pos += clen;
-      if (pos >= plen) { e = E_TRUNCATED; break; }
-      uint32_t rtag = p[pos++];
-      uint64_t rpos = pos;
       A.a = lbw;
       A.b = dsz;
-      A.c = exc_start;
+      A.c = pos;
       A.d = nexc;
-      A.e0 = cpos;
-      A.e1 = clen;
-      A.e2 = rpos;
-      A.t0 = ctag;
-      A.t1 = rtag;
-      if (ctag == 1) {  // codes entropy-coded: the frame kernel decodes the rest in order
-        A.ent = 1;
+      if (nexc) {  // the list and the rest of the walk: alprd_list_walk + alprd_walk_tail in the frame kernel
+        A.defer = 1;
         break;
       }
-      if (ctag != 0) { e = E_CORRUPT; break; }
-      e = for_walk(p, cpos + clen, cpos, n, A.offs[0]);
-      if (e) break;
-      if (rtag == 1) {  // rights entropy-coded (bit-packed rights bytes)
-        A.ent = 1;
-        break;
-      }
-      if (rtag != 0) { e = E_CORRUPT; break; }
-      e = for_walk(p, plen, rpos, n, A.offs[1]);
+      e = alprd_walk_tail(p, plen, n, pos, A);
       break;
     }
     case M_DICT: {  // dict.rs:154-207
@@ -539,6 +543,34 @@ __device__ void cta_store(const DecodeOut& O, uint64_t c0, uint32_t cnt, V val) 
   warp_store_words(O, w0, w1, p0, p1, rel, val);
 }
 
+// A whole frame's values f(0 .. n-1), typically reads of a global buffer,
+// stored by the CTA one 1024-value sub-block per warp: the warp reads its
+// sub-block into its staging buffer (eight reads in flight per lane) and
+// stores it as one run.  Uses the per-warp staging area.
+template <class F>
+__device__ void cta_store_staged(DecSmem& S, const DecodeOut& O, uint64_t c0, uint32_t n, F f) {
+  int l = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t* stg = &S.u.wbuf[warp][0];
+  uint32_t nsub = (n + kSub - 1) / kSub;
+  __syncthreads();  // the staging area is free
+  for (uint32_t k = warp; k < nsub; k += kDecWarps) {
+    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+    for (uint32_t j0 = 0; j0 < 32; j0 += 8) {
+      uint64_t r[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        uint32_t i = (j0 + j) * 32 + l;
+        r[j] = i < cnt ? f(base + i) : 0ull;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) stg[(j0 + j) * 32 + l] = r[j];
+    }
+    __syncwarp();
+    warp_store(O, c0 + base, cnt, [&](uint32_t q) { return stg[q]; });
+    __syncwarp();
+  }
+}
+
 // Sum of one sub-block's values after a per-value map g (warp-uniform result).
 template <class G>
 __device__ inline uint64_t warp_sub_sum(const uint8_t* p, uint32_t off, uint32_t count, G g) {
@@ -722,47 +754,245 @@ __device__ uint32_t dec_xorz(DecSmem& S, const uint8_t* p, uint64_t plen, uint64
 }
 
 // ---------------------------------------------------------------------------
-// ALP-RD exceptions (alp_rd.rs:281-283): vals[p] = (left << rbw) | rights[p]
-// for each (varint p, u64 left) record, in list order.  The list is read by
-// thread 0 (its byte layout is sequential) in chunks into shared memory; a
-// chunk whose positions strictly increase (every list the encoder writes) is
-// then applied by the whole CTA, whose random reads of the rights and the
-// values overlap; otherwise thread 0 applies it in order.  The records were
-// validated by the frame walk (positions < n, no truncation).
+// ALP-RD exception lists (alp_rd.rs:208-285): nexc records of (varint
+// position, u64 left part).  Records have variable length, so the start of
+// each depends on the previous one's varint.  The list is staged through
+// shared memory (at most 16 KB, and at most 18 bytes per remaining record, a
+// round) with a bitmap of its varint terminator bytes (high bit clear); the
+// CTA computes, for every staged offset, where a record starting there would
+// end (the first terminator within 10 bytes, then 8 bytes), and one thread
+// follows the chain through that table: one shared load per record.  The
+// records of a round are then decoded, checked and applied by the whole CTA.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kExcChunk = 4096;
+constexpr uint32_t kExcStage = 16384;  // staged list bytes per round
+constexpr uint32_t kExcRecs = 2048;    // records per round (a stage holds at most 16384 / 9 + 1)
+constexpr uint32_t kExcWords = (kExcStage + 32) / 32 + 7;  // 520: two words past the last staged byte
+constexpr uint16_t kNxBadVarint = 0xFFFF, kNxShort = 0xFFFE;
+
+struct ExcStage {
+  uint8_t* bytes;   // bytes[j] = the byte at the 16-byte aligned address below the round's position + j
+  uint16_t* nx;     // nx[j]: stage offset after a record starting at j, or kNxBadVarint / kNxShort
+  uint32_t* epos;   // record positions (over nx, once the chain has been followed)
+  uint64_t* left;   // record left parts (likewise)
+  uint32_t* term;   // terminator bitmap over the stage (bit j: byte j staged, high bit clear)
+  uint16_t* start;  // record starts (stage offsets)
+};
+
+// Carves the stage out of the per-warp staging area (64 KB): 16 KB + 32 of
+// bytes, the next-record table (its space reused for positions and left
+// parts), 520 bitmap words and the starts (55 KB).
+__device__ inline ExcStage exc_stage(DecSmem& S) {
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(&S.u.wbuf[0][0]) + 15) & ~(uintptr_t)15);
+  ExcStage X;
+  X.bytes = base;
+  X.nx = reinterpret_cast<uint16_t*>(base + kExcStage + 32);
+  X.left = reinterpret_cast<uint64_t*>(X.nx);
+  X.epos = reinterpret_cast<uint32_t*>(X.left + kExcRecs);
+  X.term = reinterpret_cast<uint32_t*>(X.nx + kExcStage + 32);
+  X.start = reinterpret_cast<uint16_t*>(X.term + kExcWords);
+  return X;
+}
+static_assert(8 * kExcRecs + 4 * kExcRecs <= 2 * (kExcStage + 32), "positions and left parts fit the table");
+static_assert(3 * (kExcStage + 32) + 4 * kExcWords + 2 * kExcRecs + 15 <= sizeof(uint64_t) * kDecWarps * kSub,
+              "exception stage fits the per-warp staging area");
+
+// The 4 bytes at byte offset o of a 4-byte aligned shared buffer (o + 8 within it).
+__device__ inline uint32_t lds_u32(const uint8_t* b, uint32_t o) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(b);
+  return __funnelshift_r(w[o >> 2], w[(o >> 2) + 1], (o & 3) * 8);
+}
+
+// Bits of the 10 bytes from stage offset o in the terminator bitmap.
+__device__ inline uint32_t term10(const uint32_t* term, uint32_t o) {
+  uint64_t win = ((uint64_t)term[o >> 5] | ((uint64_t)term[(o >> 5) + 1] << 32)) >> (o & 31);
+  return (uint32_t)win & 0x3FFu;
+}
+
+// Payload bytes [pos, send) into the stage by the whole CTA (16-byte loads for
+// the aligned middle, bytes at the edges; nothing outside the range is read),
+// the terminator bitmap and the next-record table (bounded by plen as the
+// record reads are).  Returns the stage offset of byte pos.
+__device__ uint32_t stage_list(const ExcStage& X, const uint8_t* p, uint64_t pos, uint64_t send, uint64_t plen) {
+  uintptr_t g0 = reinterpret_cast<uintptr_t>(p + pos), g1 = reinterpret_cast<uintptr_t>(p + send);
+  uintptr_t a0 = g0 & ~(uintptr_t)15, c0 = (g0 + 15) & ~(uintptr_t)15, a1 = g1 & ~(uintptr_t)15;
+  uint32_t head = (uint32_t)(g0 - a0), end = head + (uint32_t)(send - pos);
+  for (uintptr_t c = c0 + 16u * threadIdx.x; c < a1; c += 16u * blockDim.x)
+    *reinterpret_cast<uint4*>(X.bytes + (c - a0)) = __ldg(reinterpret_cast<const uint4*>(c));
+  uintptr_t e0 = c0 < g1 ? c0 : g1, t0 = a1 > c0 ? a1 : c0;
+  for (uintptr_t c = g0 + threadIdx.x; c < e0; c += blockDim.x) X.bytes[c - a0] = *reinterpret_cast<const uint8_t*>(c);
+  for (uintptr_t c = t0 + threadIdx.x; c < g1; c += blockDim.x) X.bytes[c - a0] = *reinterpret_cast<const uint8_t*>(c);
+  __syncthreads();
+  for (uint32_t w = threadIdx.x; w < kExcWords; w += blockDim.x) {
+    uint32_t bits = 0;
+    uint32_t j0 = 32 * w;
+    if (j0 < end && j0 + 32 > head) {
+      const uint32_t* q = reinterpret_cast<const uint32_t*>(X.bytes + j0);
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        uint32_t m = ~q[i] & 0x80808080u;
+        bits |= (((m >> 7) & 1u) | ((m >> 14) & 2u) | ((m >> 21) & 4u) | ((m >> 28) & 8u)) << (4 * i);
+      }
+      if (head > j0) bits &= ~0u << (head - j0);
+      if (end < j0 + 32) bits &= (1u << (end - j0)) - 1u;
+    }
+    X.term[w] = bits;
+  }
+  __syncthreads();
+  for (uint32_t j = head + threadIdx.x; j < end; j += blockDim.x) {
+    uint32_t m10 = term10(X.term, j);
+    uint16_t v = kNxBadVarint;
+    if (m10) {
+      uint32_t vl = (uint32_t)__ffs(m10);
+      v = plen - (pos + (j - head) + vl) < 8 ? kNxShort : (uint16_t)(j + vl + 8);
+    }
+    X.nx[j] = v;
+  }
+  __syncthreads();
+  return head;
+}
+
+__device__ __forceinline__ uint32_t lds_u16(const uint16_t* p) {
+  uint16_t v;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"((uint32_t)__cvta_generic_to_shared(p)));
+  return v;
+}
+__device__ __forceinline__ void sts_u16(uint16_t* p, uint32_t v) {
+  asm volatile("st.shared.u16 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(p)), "h"((uint16_t)v));
+}
+
+// Thread 0: the chain of records from stage offset `head` (list position
+// gpos) while records remain (at most kExcRecs) and each is wholly staged (its
+// start + 18 within the stage, or the stage reaching plen).  Fills X.start;
+// stops at the first record whose varint runs past 10 bytes (E_CORRUPT, as
+// rd_varint) or past plen, or whose 8-byte left part does not fit
+// (E_TRUNCATED).  Returns the records found; *err and *next describe the stop.
+__device__ __forceinline__ uint32_t exc_chain(const ExcStage& X, uint32_t head, uint32_t end, uint64_t gpos,
+                                              uint64_t plen, bool staged_to_plen, uint64_t want, uint32_t* err,
+                                              uint64_t* next) {
+  uint32_t k = 0, e = E_OK, o = head;
+  uint32_t lim = (uint32_t)qmin(want, (uint64_t)kExcRecs);
+  uint32_t last = staged_to_plen ? end : (end >= 18 ? end - 18 : 0);  // records may start at o <= last
+  while (k < lim && o <= last) {
+    if (!staged_to_plen || o < end) {
+      uint32_t nxt = lds_u16(X.nx + o);
+      if (nxt < kNxShort) {
+        sts_u16(X.start + k, o);
+        k++;
+        o = nxt;
+        continue;
+      }
+      e = nxt == kNxShort ? E_TRUNCATED : (plen - (gpos + (o - head)) >= 10 ? E_CORRUPT : E_TRUNCATED);
+    } else {
+      e = E_TRUNCATED;  // the list runs past plen
+    }
+    break;
+  }
+  *err = e;
+  *next = gpos + (o - head);
+  return k;
+}
+
+// Record r of the stage: its position and left part (rd_varint's value).
+__device__ inline void exc_decode(const ExcStage& X, uint32_t r, uint64_t* pp, uint64_t* lv) {
+  uint32_t o = X.start[r];
+  uint32_t vl = (uint32_t)__ffs(term10(X.term, o));
+  uint64_t v = 0;
+  for (uint32_t i = 0; i < vl; i++) v |= (uint64_t)(X.bytes[o + i] & 0x7Fu) << (7 * i);
+  *pp = v;
+  *lv = (uint64_t)lds_u32(X.bytes, o + vl) | ((uint64_t)lds_u32(X.bytes, o + vl + 4) << 32);
+}
+
+// The frame walk's pass over an exception list (alp_rd.rs:230-245): in list
+// order, each record's varint (rd_varint's errors), its 8 bytes (E_TRUNCATED),
+// then position < n (E_CORRUPT); the first failing record decides.  All
+// threads call it.  Returns the error and sets *end past the list.
+__device__ uint32_t alprd_list_walk(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t n, uint64_t pos,
+                                    uint64_t nexc, uint64_t* end) {
+  ExcStage X = exc_stage(S);
+  uint64_t x = 0;
+  uint32_t e = E_OK;
+  while (x < nexc) {
+    uint64_t send = pos + qmin(qmin((uint64_t)kExcStage, plen - pos), 18 * (nexc - x));
+    __syncthreads();  // the previous round's reads are done
+    uint32_t head = stage_list(X, p, pos, send, plen);
+    if (threadIdx.x == 0) {
+      uint32_t ee;
+      uint64_t q;
+      uint32_t k = exc_chain(X, head, head + (uint32_t)(send - pos), pos, plen, send == plen, nexc - x, &ee, &q);
+      S.sc[0] = q;
+      S.sc[1] = k;
+      S.flag = ee;
+    }
+    __syncthreads();
+    uint32_t k = (uint32_t)S.sc[1];
+    bool bad = false;
+    for (uint32_t r = threadIdx.x; r < k; r += blockDim.x) {
+      uint64_t pp, lv;
+      exc_decode(X, r, &pp, &lv);
+      bad |= pp >= n;
+    }
+    if (__syncthreads_or(bad)) {  // a record before any structural stop
+      e = E_CORRUPT;
+      break;
+    }
+    pos = S.sc[0];
+    x += k;
+    e = S.flag;
+    if (e || k == 0) break;  // k == 0 without an error is not reached: a stage holds a record
+  }
+  *end = pos;
+  return e;
+}
+
+// ALP-RD exceptions (alp_rd.rs:281-283): vals[p] = (left << rbw) | rights[p]
+// for each record, in list order.  A round whose positions strictly increase
+// (every list the encoder writes) is applied by the whole CTA, whose random
+// reads of the rights overlap; otherwise thread 0 applies it in order, so a
+// repeated position keeps its last record.  The list was validated by
+// alprd_list_walk (positions < n, no truncation).
 __device__ void alprd_exceptions(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t pos, uint64_t nexc,
                                  const uint8_t* rsrc, const uint32_t* roffs, uint32_t rbw, uint64_t* vals) {
-  uint32_t* epos = reinterpret_cast<uint32_t*>(&S.u.wbuf[0][0]);  // 16 KB
-  uint64_t* elv = &S.u.wbuf[0][0] + kExcChunk / 2;                  // 32 KB
+  ExcStage X = exc_stage(S);
   int t = threadIdx.x;
-  __syncthreads();  // every thread has read S.flag and left the staging buffers
-  for (uint64_t x0 = 0; x0 < nexc; x0 += kExcChunk) {
-    uint32_t cnt = (uint32_t)qmin(kExcChunk, nexc - x0);
+  uint64_t x = 0;
+  while (x < nexc) {
+    uint64_t send = pos + qmin(qmin((uint64_t)kExcStage, plen - pos), 18 * (nexc - x));
+    __syncthreads();  // every thread has left the staging area (and read S.flag)
+    uint32_t head = stage_list(X, p, pos, send, plen);
     if (t == 0) {
-      uint32_t inc = 1;
-      for (uint32_t k = 0; k < cnt; k++) {
-        uint64_t pp = 0;
-        rd_varint(p, plen, &pos, &pp);
-        elv[k] = ld_u64(p + pos);
-        pos += 8;
-        epos[k] = (uint32_t)pp;
-        if (k && pp <= epos[k - 1]) inc = 0;
-      }
-      S.flag = inc;
+      uint32_t ee;
+      uint64_t q;
+      uint32_t k = exc_chain(X, head, head + (uint32_t)(send - pos), pos, plen, send == plen, nexc - x, &ee, &q);
+      S.sc[0] = q;
+      S.sc[1] = k;
     }
     __syncthreads();
-    auto apply = [&](uint32_t k) {
-      uint32_t pp = epos[k];
-      vals[pp] = (elv[k] << rbw) | for_value_at(rsrc, roffs[pp / kSub], pp % kSub);
+    uint32_t k = (uint32_t)S.sc[1];
+    uint64_t q = S.sc[0];
+    for (uint32_t r = t; r < k; r += blockDim.x) {
+      uint64_t pp, lv;
+      exc_decode(X, r, &pp, &lv);
+      X.epos[r] = (uint32_t)pp;
+      X.left[r] = lv;
+    }
+    __syncthreads();
+    bool dis = false;
+    for (uint32_t r = t + 1; r < k; r += blockDim.x) dis |= X.epos[r] <= X.epos[r - 1];
+    bool inc = !__syncthreads_or(dis);
+    auto apply = [&](uint32_t r) {
+      uint32_t pp = X.epos[r];
+      vals[pp] = (X.left[r] << rbw) | for_value_at(rsrc, roffs[pp / kSub], pp % kSub);
     };
-    if (S.flag) {
-      for (uint32_t k = t; k < cnt; k += blockDim.x) apply(k);
+    if (inc) {
+      for (uint32_t r = t; r < k; r += blockDim.x) apply(r);
     } else if (t == 0) {
-      for (uint32_t k = 0; k < cnt; k++) apply(k);
+      for (uint32_t r = 0; r < k; r++) apply(r);
     }
-    __syncthreads();
+    if (k == 0) break;  // not reached for a walked list
+    x += k;
+    pos = q;
   }
+  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -898,7 +1128,7 @@ __device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDes
       e = residuals_cta(S, p, plen, n * 8 + 16, bt, n * 8 + 16, &len);
       if (e) return e;
       if (len != n * 8) return E_CORRUPT;
-      cta_store(O, c0, (uint32_t)n, [&](uint32_t q) {
+      cta_store_staged(S, O, c0, (uint32_t)n, [&](uint32_t q) {
         uint64_t w = 0;
         for (int pl = 0; pl < 8; pl++) w |= (uint64_t)bt[(uint64_t)pl * n + q] << (8 * pl);
         return w;
@@ -927,8 +1157,8 @@ __device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDes
       e = cta_bcast(S, ee);
       if (e) return e;
       double scale = kFmScales[A.a];
-      cta_store(O, c0, (uint32_t)n,
-                [&](uint32_t q) { return f64_bits(__ddiv_rn(__ll2double_rn((long long)vals[q]), scale)); });
+      cta_store_staged(S, O, c0, (uint32_t)n,
+                       [&](uint32_t q) { return f64_bits(__ddiv_rn(__ll2double_rn((long long)vals[q]), scale)); });
       return E_OK;
     }
     case M_ALP_RD: {  // alp_rd.rs:208-285 with entropy-coded codes and/or rights
@@ -977,8 +1207,7 @@ __device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDes
       __syncthreads();
       if (S.flag) return E_CORRUPT;
       if (A.d) alprd_exceptions(S, p, plen, A.c, A.d, rsrc, S.eoffs, rbw, vals);
-      __syncthreads();
-      cta_store(O, c0, (uint32_t)n, [&](uint32_t q) { return vals[q]; });
+      cta_store_staged(S, O, c0, (uint32_t)n, [&](uint32_t q) { return vals[q]; });
       return E_OK;
     }
     case M_DICT: {  // dict.rs:154-207 with TRANSPOSE values and/or CODES_ENTROPY
@@ -1094,7 +1323,7 @@ __device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDes
         __syncthreads();
         if (S.flag) return E_CORRUPT;
       }
-      cta_store(O, c0, (uint32_t)n, [&](uint32_t q) { return vals[q]; });
+      cta_store_staged(S, O, c0, (uint32_t)n, [&](uint32_t q) { return vals[q]; });
       return E_OK;
     }
     default:
@@ -1107,7 +1336,7 @@ __device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDes
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __restrict__ stream,
                                                               const FrameDesc* __restrict__ frames, int nf,
-                                                              int dtype, const FrameAux* __restrict__ aux,
+                                                              int dtype, FrameAux* aux,
                                                               DecodeOut O, uint64_t* __restrict__ scratch,
                                                               unsigned long long* __restrict__ err,
                                                               const uint32_t* __restrict__ list,
@@ -1116,10 +1345,22 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
   DecSmem& S = *reinterpret_cast<DecSmem*>(smem_raw);
   if ((int)blockIdx.x >= nf) return;
   int f = list ? (int)list[blockIdx.x] : (int)blockIdx.x;
-  const FrameAux& A = aux[f];
+  FrameAux& A = aux[f];  // written here only by thread 0 of a deferred walk, read after a barrier
   if (A.err) return;
   FrameDesc d = frames[f];
   const uint8_t* p = stream + d.payload_off;
+  if (A.defer) {  // an ALP-RD frame with exceptions: the rest of the frame walk
+    uint64_t end = 0;
+    uint32_t e = alprd_list_walk(S, p, d.plen, d.n, A.c, A.d, &end);
+    if (!e) e = cta_bcast(S, threadIdx.x == 0 ? alprd_walk_tail(p, d.plen, d.n, end, A) : 0u);
+    if (e) {
+      if (threadIdx.x == 0) {
+        A.err = e;
+        atomicMin(err, ((unsigned long long)f << 8) | e);
+      }
+      return;
+    }
+  }
   if (A.ent) {  // entropy-coded parts, in the frame's area (FrameDesc::aux = 1 + offset / 128)
     uint8_t* area = ent && d.aux ? ent + 128ull * (d.aux - 1) : nullptr;
     uint32_t ee = decode_entropy_frame(S, d, A, p, area, O);
@@ -1255,7 +1496,7 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
       }
       if (fo) {
         alprd_exceptions(S, p, plen, A.c, A.d, p, A.offs[1], rbw, fo);
-        cta_store(O, c0, (uint32_t)n, [&](uint32_t q) { return fo[q]; });
+        cta_store_staged(S, O, c0, (uint32_t)n, [&](uint32_t q) { return fo[q]; });
       }
       break;
     }

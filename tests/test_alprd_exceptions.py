@@ -69,3 +69,37 @@ def test_repeated_exception_position_later_record_wins(qb, oracle):
     want = oracle.decompress_column(s)[1]
     got = qb.decompress_column(s).values
     assert np.ascontiguousarray(got).view(np.uint8).tobytes() == np.ascontiguousarray(want).view(np.uint8).tobytes()
+
+
+def _rebuilt(p, offs, k, new_varint):
+    """The payload with record k's position varint replaced (the records after it shift)."""
+    end = _varint(p, offs[k])[1]
+    return p[:offs[k]] + bytes(new_varint) + p[end:]
+
+
+def test_damaged_exception_lists_match_oracle(qb, oracle):
+    from test_entropy_decode import _agree
+    n = 32768
+    bits, p = alprd_payload(oracle, n, 14)
+    offs = exception_records(p)
+    k = len(offs) // 2
+    pos_k = _varint(p, offs[k])[0]
+    cases = {
+        "position_n": _rebuilt(p, offs, k, [n & 0x7F | 0x80, (n >> 7) & 0x7F | 0x80, n >> 14]),
+        "position_last": _rebuilt(p, offs, k, [(n - 1) & 0x7F | 0x80, ((n - 1) >> 7) & 0x7F | 0x80, (n - 1) >> 14]),
+        "varint_4_bytes": _rebuilt(p, offs, k, [pos_k & 0x7F | 0x80, (pos_k >> 7) & 0x7F | 0x80,
+                                                (pos_k >> 14) | 0x80, 0]),
+        "varint_6_bytes": _rebuilt(p, offs, k, [pos_k & 0x7F | 0x80, (pos_k >> 7) & 0x7F | 0x80,
+                                                (pos_k >> 14) | 0x80, 0x80, 0x80, 0]),
+        "varint_11_bytes": _rebuilt(p, offs, k, [0x80] * 10 + [0]),
+        "cut_in_record": p[:offs[k] + 4],
+        "cut_at_record": p[:offs[k]],
+        "cut_last_record": p[:offs[-1] + 2],
+    }
+    kinds = {}
+    for name, q in cases.items():
+        kinds[name] = _agree(qb, oracle, one_frame_stream(q, n))
+    assert kinds["position_n"] == "CorruptPayload"
+    assert kinds["varint_4_bytes"] == "ok" and kinds["varint_6_bytes"] == "ok"
+    assert kinds["varint_11_bytes"] == "CorruptPayload"
+    assert kinds["cut_in_record"] == kinds["cut_at_record"] == "Truncated"
