@@ -18,6 +18,10 @@ compressed at Level::Fast (the byte-identical level) and decompressed again.
 C restatement in oracle/, since the Rust reference cannot be built here) on
 all host cores, on a bounded sample of the same columns.
 
+`--workload config2` runs the float-lane columns (f64 random walk, f32
+sensor readings, Decimal128) the same way; `--workload config3` compares
+plain per-column calls with the batch calls on many uneven columns.
+
 Run: python bench.py [--gpus N --steps K --warmup W] (torchrun for N > 1).
 """
 from __future__ import annotations
@@ -41,6 +45,21 @@ sys.path.insert(0, ROOT)
 METRIC = "encode+decode GB/s (uncompressed bytes; Level::Fast, bit-exact round trip)"
 N_DEFAULT = 67_108_864
 TIMER_NAMES = ["compete", "emit", "decode", "finalize", "lower", "plan", "validity", "other"]
+
+# Single-column workloads: (synth config, description, arithmetic types).
+WORKLOADS = {
+    "config1": ("1", "config1 integer lanes: i64 timestamps (1e6+Poisson(5000) steps), u64 base+U[0,2^k) runs, "
+                     "i32 Zipf(1.1) 64-category geometric runs; 10% nulls; Level::Fast", "int64/uint64/int32"),
+    "config2": ("2", "config2 float lanes: f64 random walk x+N(0,1e-3) from 20.0 at full precision, f32 "
+                     "round(N(25,5)*10)/10, Decimal128(18,4) uniform in [-1e14,1e14); no nulls; Level::Fast",
+                "f64/f32/decimal128"),
+}
+
+
+def decimal_args(wire):
+    """(scale, precision) of the benchmark's decimal columns; (0, 0) otherwise."""
+    from quoin_b200 import DECIMAL128
+    return (4, 18) if wire == DECIMAL128 else (0, 0)
 
 
 def dist_env():
@@ -139,7 +158,8 @@ def cpu_reference_run(cols, threads: int, sample: int):
         vs = v[:sample]
         bs = None if bm is None else bm[: (sample + 7) // 8]
         t0 = time.perf_counter()
-        s = O.compress_column(vs, dt, bs, level=O.LEVEL_FAST, threads=threads)
+        sc, pr = decimal_args(dt)
+        s = O.compress_column(vs, dt, bs, level=O.LEVEL_FAST, scale=sc, precision=pr, threads=threads)
         t1 = time.perf_counter()
         O.decompress_column(s, threads=threads)
         t2 = time.perf_counter()
@@ -155,7 +175,16 @@ def run_reference(args, rank, world):
     from quoin_b200 import synth
     threads = os.cpu_count() or 1
     sample = args.cpu_sample
-    cols = synth.config_columns("1", sample)
+    if args.workload == "config3":  # the batch's columns, each cut to an equal share of the sample
+        cols = synth.config3_columns(args.columns, args.max_len)
+        share = max(sample // len(cols), 1)
+        cols = [(nm, dt, v[:share], None if bm is None else bm[: (min(len(v), share) + 7) // 8])
+                for nm, dt, v, bm in cols]
+        wl = ("3", f"config3: {len(cols)} columns of the batched configuration, each cut to its first {share} "
+                   "values; Level::Fast", "mixed (f64/f32/i64/u64/i32/u32/decimal128)")
+    else:
+        wl = WORKLOADS[args.workload]
+        cols = synth.config_columns(wl[0], sample)
     for _ in range(args.warmup):
         cpu_reference_run(cols, threads, sample)
     tot_b = 0
@@ -171,13 +200,12 @@ def run_reference(args, rank, world):
     line = {
         "impl": "reference", "metric": METRIC, "value": round(gbs, 4), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot_s / args.steps * 1e3, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64/uint64/int32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl[2],
         "data": "synthetic",
-        "config": {"workload": "config1 integer lanes (i64 timestamps, u64 runs, i32 categories), 10% nulls, "
-                               "Level::Fast", "values_per_column": sample, "columns": 3},
+        "config": {"workload": wl[1], "values_per_column": sample, "columns": len(cols)},
         "encode_gbs": round(tot_b / e_s / 1e9, 4), "decode_gbs": round(tot_b / d_s / 1e9, 4),
         "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": f"first {sample} values of each config-1 column, oracle C restatement, "
+                         "sample": f"first {sample} values of each {args.workload} column, oracle C restatement, "
                                    f"{threads} threads over plan_blocks ranges / frames"},
         "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the Rust reference cannot be built here (no cargo, unvendored crates); its CPU path is timed "
@@ -202,7 +230,8 @@ def run_gpu(args, rank, world, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     dev = torch.device("cuda", local)
     n = args.n
-    cols = synth.config_columns("1", n)
+    wl = WORKLOADS[args.workload]
+    cols = synth.config_columns(wl[0], n)
     L = Q.lib
     # One context (CUDA stream + device arenas) and one host thread per column:
     # the columns' kernels overlap on the GPU, filling each other's tails.
@@ -222,15 +251,17 @@ def run_gpu(args, rank, world, local):
         d_dst = torch.empty(cap, dtype=torch.uint8, device=dev)
         d_out = torch.empty(n * w, dtype=torch.uint8, device=dev)
         d_vout = torch.empty((n + 7) // 8, dtype=torch.uint8, device=dev)
+        sc, pr = decimal_args(wire)
         gcols.append(dict(name=name, wire=wire, v=v, bm=bm, w=w, d_vals=d_vals, d_bm=d_bm, cap=cap, d_dst=d_dst,
-                          d_out=d_out, d_vout=d_vout, len=0, idx=None, ctx=ctxs[ci], st=streams[ci]))
+                          d_out=d_out, d_vout=d_vout, len=0, idx=None, ctx=ctxs[ci], st=streams[ci], sc=sc, pr=pr))
     torch.cuda.synchronize()
 
     def compress_one(c):
         olen = ctypes.c_size_t()
         rc = L.quoin_b200_compress_column_device(
             c["ctx"], c["wire"], n, P(c["d_vals"].data_ptr()), P(c["d_bm"].data_ptr()) if c["d_bm"] is not None else None,
-            0, 0, ctypes.byref(cfg), P(c["d_dst"].data_ptr()), c["cap"], ctypes.byref(olen), P(c["st"].cuda_stream))
+            c["sc"], c["pr"], ctypes.byref(cfg), P(c["d_dst"].data_ptr()), c["cap"], ctypes.byref(olen),
+            P(c["st"].cuda_stream))
         if rc:
             raise Q.Error(rc)
         c["len"] = olen.value
@@ -378,7 +409,8 @@ def run_gpu(args, rank, world, local):
         hv, hb, hdst, _, _ = pin
         olen = ctypes.c_size_t()
         rc = L.quoin_b200_compress_column(c["ctx"], c["wire"], n, P(hv.data_ptr()),
-                                          P(hb.data_ptr()) if hb is not None else None, 0, 0, ctypes.byref(cfg),
+                                          P(hb.data_ptr()) if hb is not None else None, c["sc"], c["pr"],
+                                          ctypes.byref(cfg),
                                           P(hdst[slot].data_ptr()), hdst[slot].numel(), ctypes.byref(olen))
         if rc:
             raise Q.Error(rc)
@@ -471,11 +503,10 @@ def run_gpu(args, rank, world, local):
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int64/uint64/int32", "data": "synthetic",
-            "config": {"workload": "config1 integer lanes: i64 timestamps (1e6+Poisson(5000) steps), u64 "
-                                   "base+U[0,2^k) runs, i32 Zipf(1.1) 64-category geometric runs; 10% nulls; "
-                                   "Level::Fast", "values_per_column": n, "columns": 3, "global_values": n * 3 * world,
-                       "l2": "inputs (1.25 GiB per rank) exceed the 126 MB L2; no flush needed",
+            "scaling": "weak", "vs_baseline": None, "dtype": wl[2], "data": "synthetic",
+            "config": {"workload": wl[1], "values_per_column": n, "columns": len(gcols),
+                       "global_values": n * len(gcols) * world,
+                       "l2": f"inputs ({raw_bytes / 2**30:.2f} GiB per rank) exceed the 126 MB L2; no flush needed",
                        "parallelism": f"replicas x{world} (each rank encodes and decodes its own copy of the columns)",
                        "concurrency": ("the three columns run one after another (--serial-columns)" if args.serial_columns
                                        else "the three columns run on three CUDA streams (one context and host "
@@ -672,7 +703,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serial-columns", action="store_true",
                     help="one host thread runs the columns one after another (for profilers)")
-    ap.add_argument("--workload", default="config1", choices=["config1", "config3"],
+    ap.add_argument("--workload", default="config1", choices=["config1", "config2", "config3"],
                     help="config3: the batched configuration (plain vs batch calls)")
     ap.add_argument("--columns", type=int, default=256, help="config3: number of columns")
     ap.add_argument("--max-len", type=int, default=1 << 21, help="config3: longest column")
