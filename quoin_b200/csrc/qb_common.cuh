@@ -135,6 +135,19 @@ __device__ inline bool alp_roundtrips(uint64_t bits, int e, int f, int64_t* d) {
   return alp_encode_value(as_f64(bits), e, f, d) && f64_bits(alp_decode_value(*d, e, f)) == bits;
 }
 
+// alp_roundtrips without the integer conversions: the digit is kept as the
+// integral double r it is cast from.  |r| <= 2^63, and (f64)(r as i64) == r
+// (r = 2^63 saturates to i64::MAX, whose f64 is 2^63 again), so decoding from
+// r equals decoding from the digit, and r orders like the digit.
+__device__ inline bool alp_roundtrips_r(uint64_t bits, int e, int f, double* r) {
+  double tmp = __dmul_rn(__dmul_rn(as_f64(bits), kExp10[e]), kFrac10[f]);
+  const double kUpper = 9.223372036854776e18, kMagic = 6755399441055744.0;
+  if (!is_finite_f64(tmp) || tmp >= kUpper || tmp <= -kUpper) return false;
+  double rr = __dadd_rn(__dadd_rn(tmp, kMagic), -kMagic);
+  *r = rr;
+  return f64_bits(__dmul_rn(__dmul_rn(rr, kExp10[f]), kFrac10[e])) == bits;
+}
+
 // f64::round (half away from zero), written from its definition: trunc, then
 // step away from zero when the discarded fraction is at least one half.  The
 // subtraction x - trunc(x) is exact for every finite double.

@@ -342,6 +342,17 @@ __device__ uint64_t block_for(EncSmem& S, uint8_t* dst, uint32_t M, bool sgn, V 
   return block_for_write(S, dst, M, val);
 }
 
+// alp_roundtrips_r with the four powers of ten of its (e, f) given:
+// pe = 10^e, pf = 10^-f (encode), qf = 10^f, qe = 10^-e (decode).
+__device__ __forceinline__ bool alp_rt_pow(uint64_t bits, double pe, double pf, double qf, double qe, double* r) {
+  double tmp = __dmul_rn(__dmul_rn(as_f64(bits), pe), pf);
+  const double kUpper = 9.223372036854776e18, kMagic = 6755399441055744.0;
+  if (!is_finite_f64(tmp) || tmp >= kUpper || tmp <= -kUpper) return false;
+  double rr = __dadd_rn(__dadd_rn(tmp, kMagic), -kMagic);
+  *r = rr;
+  return f64_bits(__dmul_rn(__dmul_rn(rr, qf), qe)) == bits;
+}
+
 // ALP for one sub-block (reference alp.rs:49-166): find_ef on the 32-value
 // sample, then the full encode statistics.  Warp-cooperative; returns false
 // when the sub-block (hence the block) bails.
@@ -350,7 +361,8 @@ struct AlpSub {
   uint32_t w, exc;
   int64_t mn, filler;
 };
-__device__ bool alp_subblock(const uint64_t* sv, uint32_t cnt, uint64_t* smp, AlpSub* out) {
+__device__ bool alp_subblock(const uint64_t* sv, uint32_t cnt, uint64_t* smp, const double* pexp, const double* pfrac,
+                             AlpSub* out) {
   int lane = threadIdx.x & 31;
   uint32_t st = max(cnt / 32u, 1u);
   uint32_t sl = min(32u, (cnt + st - 1) / st);
@@ -358,21 +370,24 @@ __device__ bool alp_subblock(const uint64_t* sv, uint32_t cnt, uint64_t* smp, Al
   __syncwarp();
   uint64_t best_cost = kEmpty64;
   uint32_t best_c = 0xFFFF, best_exc = 0;
+  const double kInf = __longlong_as_double(0x7FF0000000000000ll);
   for (uint32_t c = lane; c < 190; c += 32) {
     int e, f;
     alp_combo(c, &e, &f);
+    const double pe = pexp[e], pf = pfrac[f], qf = pexp[f], qe = pfrac[e];
     uint32_t ex = 0;
-    int64_t lo = INT64_MAX, hi = INT64_MIN;
+    double lo = kInf, hi = -kInf;  // digits as the integral doubles they are cast from
     for (uint32_t s = 0; s < sl; s++) {
-      int64_t d;
-      if (alp_roundtrips(smp[s], e, f, &d)) {
-        lo = d < lo ? d : lo;
-        hi = d > hi ? d : hi;
+      double r;
+      if (alp_rt_pow(smp[s], pe, pf, qf, qe, &r)) {
+        lo = r < lo ? r : lo;
+        hi = r > hi ? r : hi;
       } else {
         ex++;
       }
     }
-    uint32_t width = (ex == sl) ? 64u : (hi <= lo ? 0u : bit_width64((uint64_t)hi - (uint64_t)lo));
+    int64_t lo_i = ex == sl ? 0 : f64_as_i64(lo), hi_i = ex == sl ? 0 : f64_as_i64(hi);
+    uint32_t width = (ex == sl) ? 64u : (hi_i <= lo_i ? 0u : bit_width64((uint64_t)hi_i - (uint64_t)lo_i));
     uint64_t cost = (uint64_t)width * sl + (uint64_t)ex * 80;
     if (cost < best_cost) {
       best_cost = cost;
@@ -394,23 +409,26 @@ __device__ bool alp_subblock(const uint64_t* sv, uint32_t cnt, uint64_t* smp, Al
   if (best_exc * 2 > sl) return false;
   int e, f;
   alp_combo(best_c, &e, &f);
+  const double pe = pexp[e], pf = pfrac[f], qf = pexp[f], qe = pfrac[e];
   uint32_t exc = 0, first_li = 0xFFFFFFFFu;
-  int64_t dmn = INT64_MAX, dmx = INT64_MIN, first_d = 0;
+  double rmn = kInf, rmx = -kInf, first_r = 0.0;
   for (uint32_t j = 0; j < 32; j++) {
     uint32_t li = j * 32 + lane;
     bool ok = li < cnt;
-    int64_t d = 0;
-    bool rt = ok && alp_roundtrips(sv[li], e, f, &d);
+    double r = 0.0;
+    bool rt = ok && alp_rt_pow(sv[li], pe, pf, qf, qe, &r);
     if (rt) {
-      dmn = d < dmn ? d : dmn;
-      dmx = d > dmx ? d : dmx;
+      rmn = r < rmn ? r : rmn;
+      rmx = r > rmx ? r : rmx;
       if (li < first_li) {
         first_li = li;
-        first_d = d;
+        first_r = r;
       }
     }
     exc += __popc(__ballot_sync(0xffffffffu, ok && !rt));
   }
+  int64_t first_d = f64_as_i64(first_r);
+  int64_t dmn = rmn == kInf ? INT64_MAX : f64_as_i64(rmn), dmx = rmx == -kInf ? INT64_MIN : f64_as_i64(rmx);
   dmn = warp_min_i64(dmn);
   dmx = warp_max_i64(dmx);
   for (int o = 16; o; o >>= 1) {
@@ -1381,6 +1399,50 @@ struct FmStat {  // signed min / max of k = round(x * scale) per FLOAT_MULT scal
 
 constexpr int kStatsWarps = 32;  // one CTA per 32768-value window in adaptive mode
 
+// Start and length of statistics item `item` (one 1024-value sub-block): with
+// a fixed block size the sub-blocks restart at every block boundary.
+__device__ inline uint32_t sub_range(uint64_t item, uint64_t n, uint64_t fixed_bs, uint64_t* s) {
+  if (fixed_bs) {
+    uint64_t spb = (fixed_bs + kSub - 1) / kSub;
+    uint64_t b = item / spb, k = item % spb;
+    uint64_t bstart = b * fixed_bs, bend = qmin(bstart + fixed_bs, n);
+    *s = bstart + k * kSub;
+    return (bstart < n && *s < bend) ? (uint32_t)qmin(kSub, bend - *s) : 0u;
+  }
+  *s = item * kSub;
+  return *s < n ? (uint32_t)qmin(kSub, n - *s) : 0u;
+}
+
+// ALP statistics of every sub-block (alp.rs:49-166), for float lanes at Fast
+// and above: one warp per sub-block, after k_sub_stats (whose records it
+// completes).  The power-of-ten tables are copied to shared memory, since the
+// (e, f) search reads them at a different index in every lane.
+constexpr int kAlpWarps = 8;
+__global__ void __launch_bounds__(kAlpWarps * 32) k_alp_stats(const uint64_t* __restrict__ v, uint64_t n,
+                                                              uint64_t fixed_bs, uint64_t items,
+                                                              SubStats* __restrict__ ss) {
+  __shared__ uint64_t smp[kAlpWarps][32];
+  __shared__ double pexp[19], pfrac[19];
+  if (threadIdx.x < 19) {
+    pexp[threadIdx.x] = kExp10[threadIdx.x];
+    pfrac[threadIdx.x] = kFrac10[threadIdx.x];
+  }
+  __syncthreads();
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t item = (uint64_t)blockIdx.x * kAlpWarps + warp;
+  if (item >= items) return;
+  uint64_t s;
+  uint32_t cnt = sub_range(item, n, fixed_bs, &s);
+  if (!cnt) return;
+  AlpSub a;
+  bool ok = alp_subblock(v + s, cnt, smp[warp], pexp, pfrac, &a);
+  if (lane == 0) {
+    ss[item].alp_ok = ok ? 1 : 0;
+    ss[item].alp_w = ok ? (uint8_t)a.w : 0;
+    ss[item].alp_exc = ok ? (uint16_t)a.exc : 0;
+  }
+}
+
 template <bool FLOATS>
 __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
     const uint64_t* __restrict__ v, uint64_t n, uint64_t fixed_bs, int dtype, int level,
@@ -1391,22 +1453,11 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
   __shared__ uint32_t s_lbc;
   __shared__ uint64_t s_first[kStatsWarps], s_last[kStatsWarps];
   __shared__ uint32_t s_neq[kStatsWarps], s_cnt[kStatsWarps];
-  __shared__ uint64_t alp_smp[kStatsWarps][32];
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool do_float = FLOATS && level >= 1;
   uint64_t item = (uint64_t)blockIdx.x * kStatsWarps + warp;
-  uint64_t s, cnt64;
-  if (fixed_bs) {
-    uint64_t spb = (fixed_bs + kSub - 1) / kSub;
-    uint64_t b = item / spb, k = item % spb;
-    uint64_t bstart = b * fixed_bs, bend = qmin(bstart + fixed_bs, n);
-    s = bstart + k * kSub;
-    cnt64 = (bstart < n && s < bend) ? qmin(kSub, bend - s) : 0;
-  } else {
-    s = item * kSub;
-    cnt64 = s < n ? qmin(kSub, n - s) : 0;
-  }
-  uint32_t cnt = (uint32_t)cnt64;
+  uint64_t s;
+  uint32_t cnt = sub_range(item, n, fixed_bs, &s);
   // window probe sampling (adaptive): window-relative stride max(len/4096, 1)
   uint64_t wstart = (uint64_t)blockIdx.x * kBaseQuantum;
   uint32_t wlen = fixed_bs ? 0u : (uint32_t)(wstart < n ? qmin(kBaseQuantum, n - wstart) : 0);
@@ -1494,8 +1545,9 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
         }
       }
     }
+    // a scale that failed anywhere in the sub-block is out: stop trying it
+    if (FLOATS && alive) alive &= ~warp_or(fmfail);
     }
-    if (do_float) alive &= ~warp_or(fmfail);
   }
   // Sampled statistics, kept out of the per-value loop (only a few lanes of a
   // row would take them): early-out samples at j % 16 / j % 64 == 0 and the
@@ -1550,13 +1602,6 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_sub_stats(
   R.alp_exc = 0;
   R.pad16 = 0;
   R.pad32 = 0;
-  if (FLOATS && do_float && cnt) {
-    AlpSub a;
-    bool ok = alp_subblock(sv, cnt, alp_smp[warp], &a);
-    R.alp_ok = ok ? 1 : 0;
-    R.alp_w = ok ? (uint8_t)a.w : 0;
-    R.alp_exc = ok ? (uint16_t)a.exc : 0;
-  }
   if (FLOATS && do_float) {
 #pragma unroll
     for (int q = 0; q < 7; q++) {
@@ -1715,7 +1760,7 @@ __device__ __noinline__ int sample_winner(EncSmem& S, const uint64_t* v, uint32_
     // ALP (alp.rs:93-166): one sub-block
     if (warp == 0) {
       AlpSub a;
-      bool ok = alp_subblock(smp, m, S.alp_smp[0], &a);
+      bool ok = alp_subblock(smp, m, S.alp_smp[0], kExp10, kFrac10, &a);
       if (lane == 0) S.sc[7] = ok ? vl + 13 + 128ull * a.w + 10ull * a.exc : kEmpty64;
     }
     __syncthreads();
@@ -2022,7 +2067,7 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
       for (uint32_t k = warp; k < nsub; k += kEncWarps) {
         uint32_t cnt = min((uint32_t)kSub, n - k * kSub);
         AlpSub a;
-        bool ok = alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], &a);
+        bool ok = alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], kExp10, kFrac10, &a);
         if (lane_id == 0) {
           if (ok) atomicAdd(&S.acc64, (unsigned long long)(13 + 128ull * a.w + 10ull * a.exc));
           else atomicOr(&S.alp_fail, 1u);
@@ -2304,7 +2349,7 @@ __device__ void emit_alp(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* out
   for (uint32_t k = warp; k < nsub; k += kEncWarps) {
     uint32_t cnt = min((uint32_t)kSub, n - k * kSub);
     AlpSub a;
-    alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], &a);  // succeeded in the competition
+    alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], kExp10, kFrac10, &a);  // succeeded in the competition
     if (lane == 0) {
       S.alp_ef[k][0] = (uint8_t)a.e;
       S.alp_ef[k][1] = (uint8_t)a.f;
@@ -2816,10 +2861,15 @@ void launch_sub_stats(const uint64_t* lane, uint64_t n, uint64_t fixed_bs, int d
   uint64_t items = sub_stats_items(n, fixed_bs);
   unsigned g = (unsigned)((items + kStatsWarps - 1) / kStatsWarps);
   if (!g) return;
-  if (dtype_float(dtype))
+  if (dtype_float(dtype)) {
     k_sub_stats<true><<<g, kStatsWarps * 32, 0, st>>>(lane, n, fixed_bs, dtype, level, (SubStats*)ss, (FmStat*)fms,
                                                        smp16, grow, winbits);
-  else
+    if (level >= 1) {
+      k_alp_stats<<<(unsigned)((items + kAlpWarps - 1) / kAlpWarps), kAlpWarps * 32, 0, st>>>(lane, n, fixed_bs, items,
+                                                                                            (SubStats*)ss);
+      count_launches(1);
+    }
+  } else
     k_sub_stats<false><<<g, kStatsWarps * 32, 0, st>>>(lane, n, fixed_bs, dtype, level, (SubStats*)ss,
                                                         (FmStat*)fms, nullptr, grow, winbits);
   count_launches(1);
