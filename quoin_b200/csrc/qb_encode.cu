@@ -557,9 +557,16 @@ __device__ void rd_top8(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t lbw,
     S.cnt32 = 0;
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    if (*(volatile uint32_t*)&S.ovf) break;
-    uint32_t key = (uint32_t)(v[i] >> rbw);
+  // Counts are warp-aggregated: the lanes holding equal left parts (few
+  // distinct ones is the common case) add once, by their lowest lane.
+  int lane0 = threadIdx.x & 31;
+  for (uint32_t base = threadIdx.x & ~31u; base < n; base += blockDim.x) {
+    if (__any_sync(0xffffffffu, *(volatile uint32_t*)&S.ovf != 0)) break;
+    uint32_t i = base + lane0;
+    uint32_t key = i < n ? (uint32_t)(v[i] >> rbw) : kEmpty32;  // left parts are < 2^24
+    uint32_t peers = __match_any_sync(0xffffffffu, key);
+    if (key == kEmpty32 || lane0 != __ffs(peers) - 1) continue;
+    uint32_t add = __popc(peers);
     uint32_t h = (uint32_t)(((uint64_t)key * 0x9E3779B97F4A7C15ull) >> 53);  // 11 bits
     for (uint32_t probe = 0; probe < kHashCap; probe++) {
       uint32_t cur = hk[h];
@@ -573,7 +580,7 @@ __device__ void rd_top8(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t lbw,
         }
       }
       if (cur == key) {
-        atomicAdd(&hc[h], 1u);
+        atomicAdd(&hc[h], add);
         break;
       }
       h = (h + 1) & (kHashCap - 1);
@@ -593,8 +600,12 @@ __device__ void rd_top8(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t lbw,
       tc[i] = 0;
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-      uint32_t key = (uint32_t)(v[i] >> rbw);
+    for (uint32_t base = threadIdx.x & ~31u; base < n; base += blockDim.x) {
+      uint32_t i = base + lane0;
+      uint32_t key = i < n ? (uint32_t)(v[i] >> rbw) : kEmpty32;
+      uint32_t peers = __match_any_sync(0xffffffffu, key);
+      if (key == kEmpty32 || lane0 != __ffs(peers) - 1) continue;
+      uint32_t add = __popc(peers);
       uint32_t h = (uint32_t)(((uint64_t)key * 0x9E3779B97F4A7C15ull) >> (64 - lg));
       for (uint32_t probe = 0; probe < cap; probe++) {
         uint32_t cur = tk[h];
@@ -603,7 +614,7 @@ __device__ void rd_top8(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t lbw,
           cur = old == kEmpty32 ? key : old;
         }
         if (cur == key) {
-          atomicAdd(&tc[h], 1u);
+          atomicAdd(&tc[h], add);
           break;
         }
         h = (h + 1) & (cap - 1);
@@ -2346,10 +2357,16 @@ __device__ void emit_alp(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* out
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t nsub = (n + kSub - 1) / kSub;
   __shared__ int64_t s_fill[kSubsMax];
+  __shared__ double s_pexp[19], s_pfrac[19];  // the (e, f) search reads them at per-lane indices
+  if (threadIdx.x < 19) {
+    s_pexp[threadIdx.x] = kExp10[threadIdx.x];
+    s_pfrac[threadIdx.x] = kFrac10[threadIdx.x];
+  }
+  __syncthreads();
   for (uint32_t k = warp; k < nsub; k += kEncWarps) {
     uint32_t cnt = min((uint32_t)kSub, n - k * kSub);
     AlpSub a;
-    alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], kExp10, kFrac10, &a);  // succeeded in the competition
+    alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], s_pexp, s_pfrac, &a);  // succeeded in the competition
     if (lane == 0) {
       S.alp_ef[k][0] = (uint8_t)a.e;
       S.alp_ef[k][1] = (uint8_t)a.f;
