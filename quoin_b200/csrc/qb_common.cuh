@@ -3,6 +3,7 @@
 // float codecs need (no contraction; every product/sum is an explicit
 // round-to-nearest intrinsic so results equal the reference's IEEE doubles).
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -53,6 +54,19 @@ __host__ __device__ inline uint64_t unzigzag64(uint64_t z) { return (z >> 1) ^ (
 
 __device__ inline uint32_t bit_width64(uint64_t range) {
   return range == 0 ? 0u : 64u - (uint32_t)__clzll((long long)range);
+}
+
+// Runs f() once per device and process: kernel attributes belong to the
+// device's context, so each device is configured on first use, and the calls
+// (driver calls that take the context's lock) stay off the per-column path.
+template <class F>
+inline void once_per_device(std::atomic<unsigned long long>& done, F f) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return;
+  f();
+  done.fetch_or(bit, std::memory_order_release);
 }
 
 // ---------------------------------------------------------------------------

@@ -2292,6 +2292,13 @@ __global__ void k_decimal_combine(const uint64_t* __restrict__ limbs, uint64_t l
 // ---------------------------------------------------------------------------
 // Host launchers.
 // ---------------------------------------------------------------------------
+static void set_decode_frames_smem() {
+  static std::atomic<unsigned long long> done{0};
+  once_per_device(done, [] {
+    cudaFuncSetAttribute(k_decode_frames, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecSmem));
+  });
+}
+
 uint64_t decode_aux_bytes(int nf) { return (uint64_t)(nf > 0 ? nf : 1) * sizeof(FrameAux); }
 
 void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
@@ -2299,7 +2306,7 @@ void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf
   if (nf <= 0) return;
   FrameAux* A = reinterpret_cast<FrameAux*>(aux);
   k_walk_frames<<<(nf + 127) / 128, 128, 0, st>>>(stream, frames, nf, dtype, A, err);
-  cudaFuncSetAttribute(k_decode_frames, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecSmem));
+  set_decode_frames_smem();
   k_decode_frames<<<nf, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, nf, dtype, A, out, scratch, err, nullptr,
                                                             nullptr);
   count_launches(2);
@@ -2330,7 +2337,7 @@ void launch_decode_items(const uint8_t* stream, const FrameDesc* frames, int nf,
     launches++;
   }
   if (plan.nlist) {
-    cudaFuncSetAttribute(k_decode_frames, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecSmem));
+    set_decode_frames_smem();
     k_decode_frames<<<plan.nlist, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, (int)plan.nlist, dtype, A, out,
                                                                        scratch, err, plan.list, plan.ent);
     launches++;

@@ -2896,11 +2896,14 @@ void launch_decide(const uint64_t* lane, FrameDesc* frames, const uint32_t* nb, 
                    int dtype, int level, const void* ss, const void* fms, const uint64_t* smp16,
                    const uint32_t* winbits, uint8_t* scratch, void* ent, bool sample, cudaStream_t st) {
   int sm = (int)enc_smem_bytes();
-  cudaFuncSetAttribute(k_decide<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_decide<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_decide<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_emit<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_emit<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  static std::atomic<unsigned long long> smem_set{0};
+  once_per_device(smem_set, [sm] {
+    cudaFuncSetAttribute(k_decide<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_decide<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_decide<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_emit<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_emit<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  });
   if (max_blocks) {
     if (ent)
       k_decide<true, false><<<max_blocks, kEncThreads, sm, st>>>(lane, frames, nb, fixed_bs, dtype, level,
