@@ -205,6 +205,7 @@ struct QuoinCtx {
   size_t cap[S_COUNT] = {};
   std::mutex mu;
   QuoinDecodeIndex* hidx = nullptr;  // host-side parsed index reused by the host-buffer decodes
+  uint64_t* hbox = nullptr;          // 512 B of pinned host memory for the small device -> host reads
 
   cudaError_t ensure(int s, size_t bytes) {
     if (bytes == 0) bytes = 16;
@@ -241,7 +242,23 @@ QuoinCtx* ctx_new() {
     delete c;
     return nullptr;
   }
+  if (cudaHostAlloc(reinterpret_cast<void**>(&c->hbox), 512, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();  // reads then go to pageable memory
+    c->hbox = nullptr;
+  }
   return c;
+}
+
+// Reads `bytes` (at most 512) of device memory into host `out` and waits for
+// the stream.  Through the context's pinned mailbox the copy is a plain DMA
+// (a pageable destination takes the driver's staging path and its locks).
+cudaError_t read_small(QuoinCtx* c, cudaStream_t st, void* out, const void* d_src, size_t bytes) {
+  void* tgt = (c->hbox && bytes <= 512) ? static_cast<void*>(c->hbox) : out;
+  cudaError_t e = cudaMemcpyAsync(tgt, d_src, bytes, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && tgt != out) memcpy(out, tgt, bytes);
+  return e;
 }
 
 QuoinCtx* g_default = nullptr;
@@ -351,8 +368,7 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
   }
   if (maxb == 0) {
     uint64_t base = 0;
-    CK(cudaMemcpyAsync(&base, d_misc, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    CK(read_small(c, st, &base, d_misc, 8));
     *out_len = base;
     return QUOIN_OK;
   }
@@ -401,9 +417,7 @@ int encode_lane(QuoinCtx* c, cudaStream_t st, const LaneJob& j, uint8_t* d_dst, 
                 c->p<uint8_t>(S_SCRATCH), d_dst, dst_cap, ent, st);
   }
   uint64_t hm[2] = {0, 0};
-  CK(cudaMemcpyAsync(hm, d_misc, 16, cudaMemcpyDeviceToHost, st));
-  CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(st));
+  CK(read_small(c, st, hm, d_misc, 16));
   resolve_timing();
   uint64_t total = hm[0] + hm[1];
   *out_len = total;
@@ -451,8 +465,7 @@ int device_valid_count(QuoinCtx* c, cudaStream_t st, const uint8_t* d_bm, uint64
     launch_bitmap_transitions(d_bm, n, reinterpret_cast<unsigned long long*>(misc + 9), st);
   }
   uint64_t h[2] = {0, 0};
-  CK(cudaMemcpyAsync(h, misc + 8, 16, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  CK(read_small(c, st, h, misc + 8, 16));
   *n_valid = h[0];
   *vb_raw = h[1] + 1 >= (n + 7) / 8;
   return QUOIN_OK;
@@ -487,8 +500,7 @@ int compress_decimal_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, 
   uint64_t* limbs = c->p<uint64_t>(S_LIMBS);
   launch_decimal_split(d_values, nl, d_bm, d_bm ? c->p<uint64_t>(S_RANK) : nullptr, n, d_vmin, limbs, n_valid, st);
   uint64_t vmin[4] = {0, 0, 0, 0};
-  CK(cudaMemcpyAsync(vmin, d_vmin, 32, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  CK(read_small(c, st, vmin, d_vmin, 32));
   std::vector<uint8_t> hdr;
   const char* magic = "FCR1";
   hdr.insert(hdr.end(), magic, magic + 4);
@@ -527,8 +539,7 @@ int compress_decimal_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, 
       launch_put_validity(d_dst + pos, pos, c->p<uint8_t>(S_VBLOB), d_misc + 2, d_misc + 3, st);
     }
     uint64_t np = 0;
-    CK(cudaMemcpyAsync(&np, d_misc + 3, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    CK(read_small(c, st, &np, d_misc + 3, 8));
     pos = np;
   }
   uint64_t sub_cap = lane_bound(n_valid, n_valid, WT_U64, false, bs);
@@ -1145,9 +1156,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
   if (d_valid_out && X.has_validity && X.n)
     CK(cudaMemcpyAsync(d_valid_out, dbm, (X.n + 7) / 8, cudaMemcpyDeviceToDevice, st));
   unsigned long long herr = 0;
-  CK(cudaMemcpyAsync(&herr, d_err, 8, cudaMemcpyDeviceToHost, st));
-  CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(st));
+  CK(read_small(c, st, &herr, d_err, 8));
   resolve_timing();
   if (herr != ~0ull) return kind_to_code((int)(herr & 0xFF));
   return QUOIN_OK;
@@ -1350,6 +1359,7 @@ void quoin_ctx_free(QuoinCtx* ctx) {
     for (int s = 0; s < S_COUNT; s++)
       if (ctx->buf[s]) cudaFree(ctx->buf[s]);
     cudaStreamDestroy(ctx->stream);
+    if (ctx->hbox) cudaFreeHost(ctx->hbox);
   }
   delete ctx->hidx;
   delete ctx;
