@@ -175,13 +175,15 @@ def run_reference(args, rank, world):
     from quoin_b200 import synth
     threads = os.cpu_count() or 1
     sample = args.cpu_sample
-    if args.workload == "config3":  # the batch's columns, each cut to an equal share of the sample
-        cols = synth.config3_columns(args.columns, args.max_len)
+    if args.workload in ("config3", "config4"):  # the columns, each cut to an equal share of the sample
+        cols = (synth.config3_columns(args.columns, args.max_len) if args.workload == "config3"
+                else synth.config4_columns(args.columns4, args.max_bytes))
         share = max(sample // len(cols), 1)
         cols = [(nm, dt, v[:share], None if bm is None else bm[: (min(len(v), share) + 7) // 8])
                 for nm, dt, v, bm in cols]
-        wl = ("3", f"config3: {len(cols)} columns of the batched configuration, each cut to its first {share} "
-                   "values; Level::Fast", "mixed (f64/f32/i64/u64/i32/u32/decimal128)")
+        wl = (args.workload[-1], f"{args.workload}: {len(cols)} columns of the configuration, each cut to its "
+                                 f"first {share} values; compress then decompress each; Level::Fast",
+              "mixed (f64/f32/i64/u64/i32/u32/decimal128)")
     else:
         wl = WORKLOADS[args.workload]
         cols = synth.config_columns(wl[0], sample)
@@ -692,6 +694,167 @@ def run_gpu_config3(args, rank, world, local):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Serving configuration (--workload config4): an open-loop Poisson request
+# stream (70% decompress, 30% compress) over resident columns, served by the
+# request server (a pool of contexts, FIFO admission against a 120 GB device
+# budget) and by the plain per-request path (one context, one request at a
+# time), at offered loads from 10% to 100% of the server's measured peak.
+# ---------------------------------------------------------------------------
+def run_gpu_config4(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    import quoin_b200 as Q
+    from quoin_b200 import synth
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    L = Q.lib
+    P, S, U64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64
+
+    class Request(ctypes.Structure):
+        _fields_ = [("op", ctypes.c_int32), ("wire_dtype", ctypes.c_int32), ("scale", ctypes.c_int8),
+                    ("precision", ctypes.c_uint8), ("n", S), ("d_values", P), ("d_validity", P), ("d_dst", P),
+                    ("dst_cap", S), ("idx", P), ("d_src", P), ("d_values_out", P), ("d_validity_out", P),
+                    ("device_bytes", U64), ("out_len", S), ("status", ctypes.c_int32), ("done", ctypes.c_int32),
+                    ("t_submit_ns", U64), ("t_start_ns", U64), ("t_end_ns", U64)]
+
+    L.quoin_b200_server_create.restype = P
+    L.quoin_b200_server_create.argtypes = [ctypes.c_int, U64, ctypes.POINTER(Q._QuoinConfig)]
+    L.quoin_b200_server_submit.argtypes = [P, ctypes.POINTER(Request)]
+    L.quoin_b200_server_wait.argtypes = [P, ctypes.POINTER(Request), ctypes.c_int]
+    L.quoin_b200_server_peak_bytes.argtypes = [P]
+    L.quoin_b200_server_peak_bytes.restype = U64
+    L.quoin_b200_server_free.argtypes = [P]
+    cfg = Q._QuoinConfig(int(Q.Level.FAST), 0, 16, 0)
+    budget = 120 << 30
+
+    # Resident columns: values, a compressed copy (source of the decompress
+    # requests) with its decode index, and output buffers.  Concurrent requests
+    # on one column write the same bytes to its shared outputs.
+    cols = synth.config4_columns(args.columns4, args.max_bytes)
+    ctx = P(L.quoin_ctx_create(0))
+    tpl = []
+    resident = 0
+    for name, dt, v, bm in cols:
+        n = len(v)
+        nb = np.ascontiguousarray(v).nbytes
+        dv = torch.from_numpy(np.ascontiguousarray(v).view(np.uint8).reshape(-1).copy()).to(dev)
+        db = torch.from_numpy(bm.copy()).to(dev) if bm is not None else None
+        cap = Q._stream_bound(dt, n, bm is not None)
+        dd = torch.empty(cap, dtype=torch.uint8, device=dev)
+        sc, pr = (4, 18) if dt == Q.DECIMAL128 else (0, 0)
+        olen = ctypes.c_size_t()
+        rc = L.quoin_b200_compress_column_device(ctx, dt, n, P(dv.data_ptr()), P(db.data_ptr()) if db is not None else None,
+                                                 sc, pr, ctypes.byref(cfg), P(dd.data_ptr()), cap, ctypes.byref(olen), None)
+        if rc:
+            raise Q.Error(rc)
+        hs = dd[: olen.value].cpu().numpy().tobytes()
+        ds = torch.from_numpy(np.frombuffer(hs, np.uint8).copy()).to(dev)
+        idx = P()
+        if L.quoin_b200_index_create(ctx, hs, len(hs), ctypes.byref(idx)):
+            raise Q.Error(-14)
+        dout = torch.empty(max(nb, 8), dtype=torch.uint8, device=dev)
+        dvb = torch.empty(max((n + 7) // 8, 1), dtype=torch.uint8, device=dev)
+        resident += dv.numel() + cap + ds.numel() + dout.numel() + dvb.numel()
+        tpl.append(dict(dt=dt, n=n, nb=nb, sc=sc, pr=pr, dv=dv, db=db, dd=dd, cap=cap, ds=ds, slen=len(hs), idx=idx,
+                        dout=dout, dvb=dvb))
+    torch.cuda.synchronize()
+
+    def request(t, op):
+        c = tpl[t]
+        if op == 0:
+            return Request(op=0, wire_dtype=c["dt"], scale=c["sc"], precision=c["pr"], n=c["n"],
+                           d_values=c["dv"].data_ptr(), d_validity=c["db"].data_ptr() if c["db"] is not None else None,
+                           d_dst=c["dd"].data_ptr(), dst_cap=c["cap"], device_bytes=c["nb"] + c["cap"])
+        return Request(op=1, idx=c["idx"], d_src=c["ds"].data_ptr(), d_values_out=c["dout"].data_ptr(),
+                       d_validity_out=c["dvb"].data_ptr(), device_bytes=c["slen"] + c["nb"])
+
+    rng = np.random.default_rng(20261203 + 400)
+
+    def draw(k):
+        """k requests: (column, op) with 70% decompress."""
+        return [(int(rng.integers(0, len(tpl))), 0 if rng.random() < 0.3 else 1) for _ in range(k)]
+
+    def serve(srv, reqs, arrivals):
+        """Submits reqs at the arrival offsets (seconds; None = all at once), waits for all;
+        returns (GB/s, latencies in ms)."""
+        rs = [request(t, op) for t, op in reqs]
+        t0 = time.perf_counter()
+        for i, r in enumerate(rs):
+            if arrivals is not None:
+                d = t0 + arrivals[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+            rc = L.quoin_b200_server_submit(srv, ctypes.byref(r))
+            if rc:
+                raise Q.Error(rc)
+        for r in rs:
+            rc = L.quoin_b200_server_wait(srv, ctypes.byref(r), -1)
+            if rc:
+                raise Q.Error(rc)
+        nbytes = sum(tpl[t]["nb"] for t, _ in reqs)
+        span = (max(r.t_end_ns for r in rs) - min(r.t_submit_ns for r in rs)) / 1e9
+        lat = np.array([(r.t_end_ns - r.t_submit_ns) / 1e6 for r in rs])
+        return nbytes / span / 1e9, lat
+
+    pool = P(L.quoin_b200_server_create(args.workers, budget, ctypes.byref(cfg)))
+    plain = P(L.quoin_b200_server_create(1, budget, ctypes.byref(cfg)))
+    for _ in range(max(args.warmup, 1)):  # every context sees every column
+        serve(pool, [(t, op) for t in range(len(tpl)) for op in (0, 1)] * 2, None)
+        serve(plain, [(t, op) for t in range(len(tpl)) for op in (0, 1)], None)
+    peak_reqs = draw(args.requests)
+    peak_gbs, _ = serve(pool, peak_reqs, None)
+    mean_bytes = float(np.mean([tpl[t]["nb"] for t, _ in peak_reqs]))
+    sampler = ClockSampler(local)
+    sampler.start()
+    loads = []
+    for pct in range(10, 101, 10):
+        reqs = draw(args.requests)
+        rate = pct / 100.0 * peak_gbs * 1e9 / mean_bytes  # requests per second
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+        row = {"offered": pct / 100.0, "offered_gbs": round(pct / 100.0 * peak_gbs, 3)}
+        for key, srv in (("server", pool), ("plain", plain)):
+            gbs, lat = serve(srv, reqs, arrivals)
+            row[key] = {"gbs": round(gbs, 3), "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                        "p99_ms": round(float(np.percentile(lat, 99)), 3)}
+        loads.append(row)
+    clocks = sampler.stop()
+    peak_held = L.quoin_b200_server_peak_bytes(pool)
+    L.quoin_b200_server_free(pool)
+    L.quoin_b200_server_free(plain)
+    for c in tpl:
+        L.quoin_b200_index_free(c["idx"])
+    L.quoin_ctx_free(ctx)
+    top = loads[-1]
+    if rank == 0:
+        line = {
+            "metric": "served GB/s (uncompressed bytes; 70% decompress / 30% compress, Level::Fast, open-loop "
+                      "Poisson arrivals at 100% of the measured peak)",
+            "value": top["server"]["gbs"], "unit": "GB/s", "n_gpus": world, "steps": len(loads),
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed (f64/f32/i64/u64/i32/u32/decimal128)", "data": "synthetic",
+            "config": {"workload": f"config4: {len(tpl)} resident columns, sizes floor(exp(U[ln 64 KiB, "
+                                   f"ln {args.max_bytes >> 20} MiB])) bytes, dtypes and generators of config3; "
+                                   f"{args.requests} requests per offered load",
+                       "workers": args.workers, "budget_bytes": budget, "resident_bytes": resident,
+                       "mean_request_bytes": int(mean_bytes), "parallelism": f"replicas x{world}"},
+            "peak_gbs": round(peak_gbs, 3), "loads": loads, "peak_admitted_bytes": int(peak_held),
+            "server_over_plain_at_100pct": round(top["server"]["gbs"] / top["plain"]["gbs"], 3)
+            if top["plain"]["gbs"] else None,
+            "cpu_baseline": None, "clocks": clocks,
+            "note": "server = the request server over a pool of contexts; plain = the same arrivals served one "
+                    "request at a time on one context; latency = completion - submission (queueing included)",
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -703,17 +866,23 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serial-columns", action="store_true",
                     help="one host thread runs the columns one after another (for profilers)")
-    ap.add_argument("--workload", default="config1", choices=["config1", "config2", "config3"],
-                    help="config3: the batched configuration (plain vs batch calls)")
+    ap.add_argument("--workload", default="config1", choices=["config1", "config2", "config3", "config4"],
+                    help="config3: the batched configuration (plain vs batch calls); config4: the served "
+                         "request stream")
     ap.add_argument("--columns", type=int, default=256, help="config3: number of columns")
     ap.add_argument("--max-len", type=int, default=1 << 21, help="config3: longest column")
-    ap.add_argument("--workers", type=int, default=8, help="config3: contexts in the batch")
+    ap.add_argument("--workers", type=int, default=8, help="config3/config4: contexts in the batch / server")
+    ap.add_argument("--columns4", type=int, default=24, help="config4: resident columns")
+    ap.add_argument("--max-bytes", type=int, default=256 << 20, help="config4: largest column")
+    ap.add_argument("--requests", type=int, default=600, help="config4: requests per offered load")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.workload == "config3":
         return run_gpu_config3(args, rank, world, local)
+    if args.workload == "config4":
+        return run_gpu_config4(args, rank, world, local)
     return run_gpu(args, rank, world, local)
 
 

@@ -294,6 +294,59 @@ int quoin_b200_compress_batch_device(QuoinBatch *batch, QuoinB200CompressJob *jo
                                      const QuoinConfig *cfg);
 int quoin_b200_decompress_batch_device(QuoinBatch *batch, QuoinB200DecompressJob *jobs, size_t njobs);
 
+/* ---------------- Request server ---------------- */
+
+/* No counterpart in the reference.  A server runs compress and decompress
+ * requests on device-resident buffers for many callers: requests are queued
+ * in arrival order and admitted when the device memory they hold fits the
+ * server's budget beside the running ones (a request above the budget on its
+ * own is refused with QUOIN_ERR_OVER_BUDGET), then run on a pool of contexts.
+ * Each request's bytes are those of the single-column call. */
+#define QUOIN_ERR_OVER_BUDGET (-23) /* a request needs more device memory than the server's budget */
+#define QUOIN_ERR_TIMEOUT     (-24) /* quoin_b200_server_wait: the request has not finished yet */
+#define QUOIN_B200_OP_COMPRESS   0
+#define QUOIN_B200_OP_DECOMPRESS 1
+
+typedef struct QuoinServer QuoinServer;
+
+typedef struct {
+    int32_t op;                       /* QUOIN_B200_OP_COMPRESS or QUOIN_B200_OP_DECOMPRESS */
+    /* compress: the arguments of quoin_b200_compress_column_device */
+    int32_t wire_dtype;
+    int8_t scale;
+    uint8_t precision;
+    size_t n;
+    const void *d_values;
+    const uint8_t *d_validity;
+    uint8_t *d_dst;
+    size_t dst_cap;
+    /* decompress: the arguments of quoin_b200_decompress_indexed_device */
+    const QuoinDecodeIndex *idx;
+    const uint8_t *d_src;
+    void *d_values_out;
+    uint8_t *d_validity_out;
+    /* device memory the request's own buffers hold while it waits and runs */
+    uint64_t device_bytes;
+    /* out */
+    size_t out_len;                   /* compress: stream length */
+    int32_t status;                   /* the call's return code */
+    int32_t done;                     /* set when the request has finished */
+    uint64_t t_submit_ns, t_start_ns, t_end_ns; /* steady clock, ns since the server started */
+} QuoinB200Request;
+
+/* workers: 1..64 contexts; budget_bytes: device memory the admitted requests may hold. */
+QuoinServer *quoin_b200_server_create(int workers, uint64_t budget_bytes, const QuoinConfig *cfg);
+/* Queues `req` (which must stay valid until it is done) and returns at once. */
+int quoin_b200_server_submit(QuoinServer *server, QuoinB200Request *req);
+/* Waits up to timeout_ms (negative: without limit) for `req`; returns its
+ * status, or QUOIN_ERR_TIMEOUT. */
+int quoin_b200_server_wait(QuoinServer *server, QuoinB200Request *req, int timeout_ms);
+/* Peak device bytes held by admitted requests (budget accounting, including the
+ * server's estimate of each request's working memory). */
+uint64_t quoin_b200_server_peak_bytes(QuoinServer *server);
+/* Finishes the queued requests and frees the server. */
+void quoin_b200_server_free(QuoinServer *server);
+
 /* ---------------- Arrow C Data Interface ---------------- */
 
 /* The standard Arrow C Data Interface structs (declared here unless the

@@ -27,7 +27,7 @@ _ERRORS = {
     -10: "BadMagic", -11: "UnsupportedVersion", -12: "Truncated", -13: "UnknownMode",
     -14: "CorruptPayload", -15: "LengthMismatch", -16: "UnsupportedDType", -17: "DTypeMismatch",
     -18: "Unsupported", -19: "Cuda", -20: "BadArg", -1: "Null", -2: "BufferTooSmall", -3: "Corrupt",
-    -4: "Panic", -21: "NoAllocLimit", -22: "UnsupportedArrowType",
+    -4: "Panic", -21: "NoAllocLimit", -22: "UnsupportedArrowType", -23: "OverBudget", -24: "Timeout",
 }
 
 

@@ -116,17 +116,37 @@ def config_columns(config: str, n: int):
     raise ValueError(config)
 
 
+MIXED_DTYPES = [F64, F32, I64, U64, I32, U32, DECIMAL128]
+NATIVE_BYTES = {F64: 8, F32: 4, I64: 8, U64: 8, I32: 4, U32: 4, DECIMAL128: 16}
+
+
 def config3_columns(ncols: int, max_len: int = 1 << 21, min_len: int = 1024):
     """The batched configuration: `ncols` columns with lengths floor(exp(U[ln min_len,
     ln max_len])), dtype uniform over f64/f32/i64/u64/i32/u32/decimal128, the
     per-dtype generators of configs 0-2, and a null rate U(0, 0.2) each.
     [(name, wire dtype, values, validity bitmap or None)]."""
-    dtypes = [F64, F32, I64, U64, I32, U32, DECIMAL128]
+    return _mixed_columns(3, ncols, lambda r, dt: int(np.floor(np.exp(r.uniform(np.log(min_len), np.log(max_len))))))
+
+
+def config4_columns(ncols: int, max_bytes: int = 256 << 20, min_bytes: int = 64 << 10):
+    """Request columns of the serving configuration: sizes floor(exp(U[ln min_bytes,
+    ln max_bytes])) bytes of native values, dtypes and generators as config3."""
+    return _mixed_columns(4, ncols, lambda r, dt: max(
+        int(np.floor(np.exp(r.uniform(np.log(min_bytes), np.log(max_bytes))))) // NATIVE_BYTES[dt], 1),
+        size_first=False)
+
+
+def _mixed_columns(config: int, ncols: int, length, size_first: bool = True):
+    dtypes = MIXED_DTYPES
     out = []
     for c in range(ncols):
-        r = rng_for(3, c)
-        n = int(np.floor(np.exp(r.uniform(np.log(min_len), np.log(max_len)))))
-        dt = dtypes[int(r.integers(0, len(dtypes)))]
+        r = rng_for(config, c)
+        if size_first:
+            n = length(r, None)
+            dt = dtypes[int(r.integers(0, len(dtypes)))]
+        else:
+            dt = dtypes[int(r.integers(0, len(dtypes)))]
+            n = length(r, dt)
         null_rate = float(r.uniform(0.0, 0.2))
         if dt == F64:
             v = prices_f64(n, r) if c % 2 == 0 else random_walk_f64(n, r)
