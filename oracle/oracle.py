@@ -73,6 +73,11 @@ def lib():
         L.oq_encode_mode.argtypes = [ctypes.c_int, P, S, ctypes.c_int, ctypes.c_int,
                                      ctypes.POINTER(U8P), ctypes.POINTER(S)]
         L.oq_decode_mode.argtypes = [ctypes.c_int, P, S, S, ctypes.c_int, P]
+        L.oq_linear_payload.argtypes = [ctypes.c_int, P, S, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(U8P), ctypes.POINTER(S)]
+        L.oq_rc_compress.argtypes = [P, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
+        L.oq_linear_select_order.argtypes = [P, S]
+        L.oq_rc_decompress.argtypes = [P, S, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
         L.oq_pack32.argtypes = [P, ctypes.c_uint32, P]
         L.oq_unpack32.argtypes = [P, ctypes.c_uint32, P]
         L.oq_pack64.argtypes = [P, ctypes.c_uint32, P]
@@ -168,6 +173,48 @@ def rans_decompress(payload: bytes, max_len: int) -> bytes:
     if rc:
         raise OracleError(rc)
     return _take(ctypes.cast(out, ctypes.c_void_p).value, olen.value) or b""
+
+
+def rc_compress(data: bytes) -> bytes:
+    """The range coder (entropy/rc.rs): varint(len) ++ coded bytes."""
+    a = np.frombuffer(data, dtype=np.uint8) if data else np.zeros(1, np.uint8)
+    out = ctypes.POINTER(ctypes.c_uint8)()
+    olen = ctypes.c_size_t()
+    lib().oq_rc_compress(a.ctypes.data, len(data), ctypes.byref(out), ctypes.byref(olen))
+    return _take(ctypes.cast(out, ctypes.c_void_p).value, olen.value) or b""
+
+
+def rc_decompress(payload: bytes, max_len: int) -> bytes:
+    a = np.frombuffer(payload, dtype=np.uint8) if payload else np.zeros(1, np.uint8)
+    out = ctypes.POINTER(ctypes.c_uint8)()
+    olen = ctypes.c_size_t()
+    rc = lib().oq_rc_decompress(a.ctypes.data, len(payload), max_len, ctypes.byref(out), ctypes.byref(olen))
+    if rc:
+        raise OracleError(rc)
+    return _take(ctypes.cast(out, ctypes.c_void_p).value, olen.value) or b""
+
+
+TAG_RC, TAG_RANS = 0, 2
+M_ORDERED_DELTA, M_DELTA2, M_DELTA_DP = 7, 20, 45
+
+
+def linear_select_order(lane: np.ndarray) -> int:
+    lane = np.ascontiguousarray(lane, dtype=np.uint64)
+    return lib().oq_linear_select_order(lane.ctypes.data, lane.size)
+
+
+def linear_payload(mode: int, lane: np.ndarray, order: int = 0, tag: int = TAG_RC):
+    """A DELTA2 / DELTA_DP / ORDERED_DELTA frame payload (codecs/linear.rs) whose
+    residual bytes are coded by `tag`; None when DELTA_DP does not apply."""
+    lane = np.ascontiguousarray(lane, dtype=np.uint64)
+    out = ctypes.POINTER(ctypes.c_uint8)()
+    olen = ctypes.c_size_t()
+    rc = lib().oq_linear_payload(mode, lane.ctypes.data, lane.size, order, tag, ctypes.byref(out),
+                                 ctypes.byref(olen))
+    if rc:
+        raise OracleError(rc)
+    p = ctypes.cast(out, ctypes.c_void_p).value
+    return _take(p, olen.value) if p else None
 
 
 def encode_mode(mode: int, lane: np.ndarray, dtype: int = DT_U64, level: int = LEVEL_FAST):

@@ -848,13 +848,143 @@ static void code_residuals(const uint8_t *res, size_t n, buf_t *out) {
     b_push(out, TAG_RANS);
     rans_compress(res, n, out);
 }
-/* entropy/mod.rs:152-178.  The range coder, legacy tANS and LZ cascade tags
- * are outside the in-path pool. */
+/* ------------------------------------------------------------------------ */
+/* Range coder — src/entropy/rc.rs: a binary LZMA-style coder (11-bit         */
+/* probabilities adapted by shift 5, a 32-bit range renormalised a byte at a  */
+/* time, carries through a cached byte) under an order-1 byte model: 256      */
+/* contexts (the previous byte) x a 256-node bit tree, MSB first.             */
+/* ------------------------------------------------------------------------ */
+#define RC_PROB_BITS 11
+#define RC_PROB_INIT 1024
+#define RC_MOVE_BITS 5
+#define RC_TOP (1u << 24)
+
+typedef struct {
+    uint64_t low;
+    uint32_t range;
+    uint8_t cache;
+    uint64_t cache_size;
+    buf_t *out;
+} rc_enc_t;
+
+/* rc.rs:40-57 */
+static void rc_shift_low(rc_enc_t *e) {
+    if ((e->low >> 32) != 0 || e->low < 0xFF000000ull) {
+        uint8_t carry = (uint8_t)(e->low >> 32);
+        uint8_t temp = e->cache;
+        do {
+            b_push(e->out, (uint8_t)(temp + carry));
+            temp = 0xFF;
+        } while (--e->cache_size != 0);
+        e->cache = (uint8_t)((e->low >> 24) & 0xFF);
+    }
+    e->cache_size++;
+    e->low = (e->low & 0x00FFFFFFull) << 8;
+}
+
+/* rc.rs:59-79 (the branchless form selects exactly these updates) */
+static void rc_encode_bit(rc_enc_t *e, uint16_t *prob, uint32_t bit) {
+    uint32_t bound = (e->range >> RC_PROB_BITS) * (uint32_t)*prob;
+    uint32_t p = *prob;
+    if (bit) {
+        e->low += bound;
+        e->range -= bound;
+        *prob = (uint16_t)(p - (p >> RC_MOVE_BITS));
+    } else {
+        e->range = bound;
+        *prob = (uint16_t)(p + (((1u << RC_PROB_BITS) - p) >> RC_MOVE_BITS));
+    }
+    while (e->range < RC_TOP) {
+        e->range <<= 8;
+        rc_shift_low(e);
+    }
+}
+
+typedef struct {
+    uint32_t code, range;
+    const uint8_t *in;
+    size_t len, pos;
+} rc_dec_t;
+
+/* rc.rs:113-120: reads past the end give 0 */
+static uint32_t rc_next(rc_dec_t *d) {
+    uint32_t b = d->pos < d->len ? d->in[d->pos] : 0;
+    d->pos++;
+    return b;
+}
+
+/* rc.rs:122-142 */
+static uint32_t rc_decode_bit(rc_dec_t *d, uint16_t *prob) {
+    uint32_t bound = (d->range >> RC_PROB_BITS) * (uint32_t)*prob;
+    uint32_t p = *prob;
+    uint32_t bit = d->code >= bound;
+    if (bit) {
+        d->code -= bound;
+        d->range -= bound;
+        *prob = (uint16_t)(p - (p >> RC_MOVE_BITS));
+    } else {
+        d->range = bound;
+        *prob = (uint16_t)(p + (((1u << RC_PROB_BITS) - p) >> RC_MOVE_BITS));
+    }
+    while (d->range < RC_TOP) {
+        d->range <<= 8;
+        d->code = (d->code << 8) | rc_next(d);
+    }
+    return bit;
+}
+
+/* rc.rs:193-206: varint(len) ++ coded bytes */
+static void rc_compress(const uint8_t *src, size_t n, buf_t *out) {
+    b_varint(out, n);
+    rc_enc_t e = {0, 0xFFFFFFFFu, 0, 1, out};
+    uint16_t *probs = (uint16_t *)malloc(65536 * sizeof(uint16_t));
+    for (size_t i = 0; i < 65536; i++) probs[i] = RC_PROB_INIT;
+    size_t ctx = 0;
+    for (size_t i = 0; i < n; i++) {
+        uint32_t node = 1;
+        for (int k = 7; k >= 0; k--) {
+            uint32_t bit = (src[i] >> k) & 1u;
+            rc_encode_bit(&e, &probs[ctx * 256 + node], bit);
+            node = (node << 1) | bit;
+        }
+        ctx = src[i];
+    }
+    for (int k = 0; k < 5; k++) rc_shift_low(&e);
+    free(probs);
+}
+
+/* rc.rs:208-225 */
+static int rc_decompress(const uint8_t *p, size_t plen, size_t max_len, buf_t *out) {
+    size_t pos = 0;
+    uint64_t len = 0;
+    int rc = varint_read(p, plen, &pos, &len);
+    if (rc) return rc;
+    if (len > max_len) return OQ_CORRUPT;
+    rc_dec_t d = {0, 0xFFFFFFFFu, p + pos, plen - pos, 0};
+    rc_next(&d);  /* the encoder's leading cache byte */
+    for (int k = 0; k < 4; k++) d.code = (d.code << 8) | rc_next(&d);
+    uint16_t *probs = (uint16_t *)malloc(65536 * sizeof(uint16_t));
+    for (size_t i = 0; i < 65536; i++) probs[i] = RC_PROB_INIT;
+    b_reserve(out, (size_t)len);
+    size_t ctx = 0;
+    for (uint64_t i = 0; i < len; i++) {
+        uint32_t node = 1;
+        for (int k = 0; k < 8; k++) node = (node << 1) | rc_decode_bit(&d, &probs[ctx * 256 + node]);
+        uint8_t b = (uint8_t)(node & 0xFF);
+        b_push(out, b);
+        ctx = b;
+    }
+    free(probs);
+    return OQ_OK;
+}
+
+/* entropy/mod.rs:152-178.  The legacy tANS tag (decoded by the reference,
+ * never produced) and the LZ cascade tag (Max) are not restated. */
 static int decode_residuals(const uint8_t *p, size_t plen, size_t max_len, buf_t *out) {
     if (plen == 0) return OQ_TRUNCATED;
     switch (p[0]) {
         case TAG_RANS: return rans_decompress(p + 1, plen - 1, max_len, out);
-        case TAG_RC:
+        case TAG_RC: return rc_decompress(p + 1, plen - 1, max_len, out);
         case TAG_TANS:
         case TAG_LZ: return OQ_UNSUPPORTED;
         default: return OQ_CORRUPT;
@@ -1962,6 +2092,178 @@ static void compress_lane_buf(const uint64_t *vals, size_t n_valid, int dtype, s
 /* ------------------------------------------------------------------------ */
 
 /* decoder.rs:145-190 (in-path modes) */
+/* ------------------------------------------------------------------------ */
+/* Linear recurrences — src/codecs/linear.rs (High / Max modes): ORDERED_DELTA */
+/* (second difference of the u64 patterns, zigzag LEB128), DELTA2 (XOR with a */
+/* polynomial extrapolation in f64) and DELTA_DP (the f64 residual, verified  */
+/* invertible).  The frame payload is the entropy-coded residual bytes.        */
+/* ------------------------------------------------------------------------ */
+
+/* linear.rs:31-45 */
+static void idelta2_encode(const uint64_t *v, size_t n, buf_t *out) {
+    uint64_t p1 = 0, p2 = 0;
+    for (size_t i = 0; i < n; i++) {
+        uint64_t pred = i == 0 ? 0 : i == 1 ? p1 : p1 * 2 - p2;
+        b_varint(out, zigzag64(v[i] - pred));
+        p2 = p1;
+        p1 = v[i];
+    }
+}
+/* linear.rs:47-66 */
+static int idelta2_decode(const uint8_t *p, size_t len, size_t n, uint64_t *out) {
+    uint64_t p1 = 0, p2 = 0;
+    size_t pos = 0;
+    for (size_t i = 0; i < n; i++) {
+        uint64_t pred = i == 0 ? 0 : i == 1 ? p1 : p1 * 2 - p2, r;
+        int rc = varint_read(p, len, &pos, &r);
+        if (rc) return rc;
+        uint64_t v = pred + unzigzag64(r);
+        out[i] = v;
+        p2 = p1;
+        p1 = v;
+    }
+    return pos == len ? OQ_OK : OQ_CORRUPT;
+}
+
+static uint64_t f64_to_bits(double d);
+static double bits_to_f64(uint64_t b);
+/* f64 arithmetic with NaN operands propagated as x86 SSE does in source
+ * order (the first NaN operand, quieted; an invalid operation gives the
+ * default NaN 0xFFF8...), written out so the result does not depend on how a
+ * compiler orders the operands. */
+static double nan_op(double a, double b, double r) {
+    if (isnan(a)) return bits_to_f64(f64_to_bits(a) | 0x0008000000000000ull);
+    if (isnan(b)) return bits_to_f64(f64_to_bits(b) | 0x0008000000000000ull);
+    if (isnan(r)) return bits_to_f64(0xFFF8000000000000ull);
+    return r;
+}
+static double x_mul(double a, double b) { return nan_op(a, b, a * b); }
+static double x_add(double a, double b) { return nan_op(a, b, a + b); }
+static double x_sub(double a, double b) { return nan_op(a, b, a - b); }
+
+/* linear.rs:75-100: Newton extrapolation, most recent first; the effective
+ * order drops to the history available.  pred = 0.0 + c0*h0 + c1*h1 + ...,
+ * each product and sum rounded on its own (no FMA). */
+static double lin_predict(const double *h, size_t avail, int order) {
+    static const int coef[5][4] = {{0}, {1}, {2, -1}, {3, -3, 1}, {4, -6, 4, -1}};
+    int eff = (size_t)order < avail ? order : (int)avail;
+    if (eff == 0) return 0.0;
+    double pred = 0.0;
+    for (int k = 0; k < eff; k++) pred = x_add(pred, x_mul((double)coef[eff][k], h[k]));
+    return pred;
+}
+static void lin_push(double *h, double v) {
+    h[3] = h[2];
+    h[2] = h[1];
+    h[1] = h[0];
+    h[0] = v;
+}
+static uint64_t f64_to_bits(double d) {
+    uint64_t b;
+    memcpy(&b, &d, 8);
+    return b;
+}
+static double bits_to_f64(uint64_t b) {
+    double d;
+    memcpy(&d, &b, 8);
+    return d;
+}
+
+/* linear.rs:121-140: the order whose order-th difference of a 1,024-value
+ * window from the middle of the block has the smallest mean magnitude. */
+static int lin_select_order(const uint64_t *v, size_t n) {
+    if (n < 8) return 2;
+    size_t win = n < 1024 ? n : 1024, start = (n - win) / 2, len = win;
+    double *d = (double *)malloc(win * sizeof(double));
+    for (size_t i = 0; i < win; i++) d[i] = bits_to_f64(v[start + i]);
+    int best = 1;
+    double best_mag = INFINITY;
+    for (int order = 1; order <= 4; order++) {
+        for (size_t i = 0; i + 1 < len; i++) d[i] = d[i + 1] - d[i];
+        if (len) len--;
+        double mag = INFINITY;
+        if (len) {
+            double sum = -0.0;
+            for (size_t i = 0; i < len; i++) sum += fabs(d[i]);
+            mag = sum / (double)len;
+        }
+        if (isfinite(mag) && mag < best_mag) {
+            best_mag = mag;
+            best = order;
+        }
+    }
+    free(d);
+    return best;
+}
+
+/* linear.rs:146-157 */
+static void delta2_encode(const uint64_t *v, size_t n, int order, buf_t *out) {
+    b_push(out, (uint8_t)order);
+    double h[4] = {0, 0, 0, 0};
+    for (size_t i = 0; i < n; i++) {
+        uint64_t pred = f64_to_bits(lin_predict(h, i < 4 ? i : 4, order));
+        b_varint(out, v[i] ^ pred);
+        lin_push(h, bits_to_f64(v[i]));
+    }
+}
+/* linear.rs:159-179 */
+static int delta2_decode(const uint8_t *p, size_t len, size_t n, uint64_t *out) {
+    if (len == 0) return OQ_TRUNCATED;
+    int order = p[0];
+    if (order < 1 || order > 4) return OQ_CORRUPT;
+    double h[4] = {0, 0, 0, 0};
+    size_t pos = 1;
+    for (size_t i = 0; i < n; i++) {
+        uint64_t pred = f64_to_bits(lin_predict(h, i < 4 ? i : 4, order)), r;
+        int rc = varint_read(p, len, &pos, &r);
+        if (rc) return rc;
+        out[i] = r ^ pred;
+        lin_push(h, bits_to_f64(out[i]));
+    }
+    return pos == len ? OQ_OK : OQ_CORRUPT;
+}
+
+/* linear.rs:190-213: false when some value does not survive pred + (v - pred) */
+static bool dp_encode(const uint64_t *v, size_t n, int order, buf_t *out) {
+    if (n == 0) return false;
+    b_push(out, (uint8_t)order);
+    double h[4] = {0, 0, 0, 0};
+    uint64_t prev = 0;
+    for (size_t i = 0; i < n; i++) {
+        double x = bits_to_f64(v[i]), pred = lin_predict(h, i < 4 ? i : 4, order), r = x_sub(x, pred);
+        if (f64_to_bits(x_add(pred, r)) != v[i]) return false;
+        uint64_t rb = f64_to_bits(r);
+        b_varint(out, rb ^ prev);
+        prev = rb;
+        lin_push(h, x);
+    }
+    return true;
+}
+/* linear.rs:215-237 */
+static int dp_decode(const uint8_t *p, size_t len, size_t n, uint64_t *out) {
+    if (len == 0) return OQ_TRUNCATED;
+    int order = p[0];
+    if (order < 1 || order > 4) return OQ_CORRUPT;
+    double h[4] = {0, 0, 0, 0};
+    uint64_t prev = 0;
+    size_t pos = 1;
+    for (size_t i = 0; i < n; i++) {
+        double pred = lin_predict(h, i < 4 ? i : 4, order);
+        uint64_t r;
+        int rc = varint_read(p, len, &pos, &r);
+        if (rc) return rc;
+        uint64_t rb = r ^ prev;
+        double x = x_add(pred, bits_to_f64(rb));
+        out[i] = f64_to_bits(x);
+        prev = rb;
+        lin_push(h, x);
+    }
+    return pos == len ? OQ_OK : OQ_CORRUPT;
+}
+
+/* decoder.rs:150-171: entropy-coded residuals (bound 10n + 16), then the recurrence */
+static int linear_frame_decode(int mode, const uint8_t *p, size_t plen, size_t n, uint64_t *out);
+
 static int decode_frame(int mode, const uint8_t *p, size_t plen, size_t n, int dtype, uint64_t *out) {
     switch (mode) {
         case M_RAW: return raw_decode(p, plen, n, dtype, out);
@@ -1990,8 +2292,23 @@ static int decode_frame(int mode, const uint8_t *p, size_t plen, size_t n, int d
         case M_ALP_RD: return alprd_decode(p, plen, n, out);
         case M_DICT: return dict_decode(p, plen, n, out);
         case M_RLE: return rle_decode(p, plen, n, out);
+        case M_ORDERED_DELTA:
+        case M_DELTA2:
+        case M_DELTA_DP: return linear_frame_decode(mode, p, plen, n, out);
         default: return OQ_UNSUPPORTED;
     }
+}
+
+static int linear_frame_decode(int mode, const uint8_t *p, size_t plen, size_t n, uint64_t *out) {
+    buf_t b = {0};
+    int rc = decode_residuals(p, plen, n * 10 + 16, &b);
+    if (!rc) {
+        if (mode == M_ORDERED_DELTA) rc = idelta2_decode(b.p, b.len, n, out);
+        else if (mode == M_DELTA2) rc = delta2_decode(b.p, b.len, n, out);
+        else rc = dp_decode(b.p, b.len, n, out);
+    }
+    b_free(&b);
+    return rc;
 }
 
 typedef struct {
@@ -2564,6 +2881,61 @@ int oq_encode_mode(int mode, const uint64_t *v, size_t n, int dtype, int level, 
     *out = b.p ? b.p : (uint8_t *)malloc(1);
     *out_len = b.len;
     return OQ_OK;
+}
+
+/* A High / Max linear-mode payload (linear.rs) with the residual bytes coded
+ * by `tag` (TAG_RC or TAG_RANS, entropy/mod.rs:24-29); order 0 picks it as
+ * the reference's encoder does (linear.rs:121-140).  *out = NULL when
+ * DELTA_DP does not apply. */
+int oq_linear_payload(int mode, const uint64_t *v, size_t n, int order, int tag, uint8_t **out, size_t *out_len) {
+    buf_t r = {0}, b = {0};
+    *out = NULL;
+    *out_len = 0;
+    if (order == 0) order = lin_select_order(v, n);
+    if (mode == M_ORDERED_DELTA) {
+        idelta2_encode(v, n, &r);
+    } else if (mode == M_DELTA2) {
+        delta2_encode(v, n, order, &r);
+    } else if (mode == M_DELTA_DP) {
+        if (!dp_encode(v, n, order, &r)) {
+            b_free(&r);
+            return OQ_OK;
+        }
+    } else {
+        return OQ_UNSUPPORTED;
+    }
+    if (tag == TAG_RC) {
+        b_push(&b, TAG_RC);
+        rc_compress(r.p, r.len, &b);
+    } else if (tag == TAG_RANS && r.len) {
+        b_push(&b, TAG_RANS);
+        rans_compress(r.p, r.len, &b);
+    } else {
+        b_free(&r);
+        return OQ_UNSUPPORTED;
+    }
+    b_free(&r);
+    *out = b.p;
+    *out_len = b.len;
+    return OQ_OK;
+}
+
+int oq_linear_select_order(const uint64_t *v, size_t n) { return lin_select_order(v, n); }
+
+int oq_rc_compress(const uint8_t *data, size_t n, uint8_t **out, size_t *out_len) {
+    buf_t b = {0};
+    rc_compress(data, n, &b);
+    *out = b.p;
+    *out_len = b.len;
+    return OQ_OK;
+}
+
+int oq_rc_decompress(const uint8_t *payload, size_t len, size_t max_len, uint8_t **out, size_t *out_len) {
+    buf_t b = {0};
+    int rc = rc_decompress(payload, len, max_len, &b);
+    *out = b.p ? b.p : (uint8_t *)malloc(1);
+    *out_len = b.len;
+    return rc;
 }
 
 int oq_decode_mode(int mode, const uint8_t *payload, size_t plen, size_t n, int dtype, uint64_t *out) {

@@ -113,6 +113,19 @@ int oq_decompress_column_mt(const uint8_t *src, size_t len, int threads, int *dt
                             size_t *n, void **values, uint8_t **validity, int8_t *scale,
                             uint8_t *precision);
 
+/* High / Max linear modes (src/codecs/linear.rs): a frame payload of mode 7
+ * (ORDERED_DELTA), 20 (DELTA2) or 45 (DELTA_DP) with the residual bytes coded
+ * by tag 0 (range coder) or 2 (rANS); order 0 = the reference's choice.
+ * *out = NULL when DELTA_DP does not apply to the values. */
+int oq_linear_payload(int mode, const uint64_t *vals, size_t n, int order, int tag,
+                      uint8_t **out, size_t *out_len);
+/* linear.rs:121-140: the extrapolation order the reference's encoder picks. */
+int oq_linear_select_order(const uint64_t *vals, size_t n);
+/* The range coder (src/entropy/rc.rs): varint(len) ++ coded bytes. */
+int oq_rc_compress(const uint8_t *data, size_t n, uint8_t **out, size_t *out_len);
+int oq_rc_decompress(const uint8_t *payload, size_t len, size_t max_len, uint8_t **out,
+                     size_t *out_len);
+
 #ifdef __cplusplus
 }
 #endif

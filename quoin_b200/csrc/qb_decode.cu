@@ -161,6 +161,9 @@ __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDes
       e = for_walk(p, plen, 8, n, A.offs[0]);
       break;
     case M_BYTE_TRANSPOSE:  // transpose.rs:10-32: the whole payload is entropy-coded
+    case M_ORDERED_DELTA:   // linear.rs: entropy-coded residual bytes (decoder.rs:162-171)
+    case M_DELTA2:
+    case M_DELTA_DP:
       A.ent = 1;
       break;
     case M_FLOAT_MULT: {  // float_mult.rs:100-133
@@ -362,6 +365,7 @@ struct DecSmem {
   uint64_t wxor[kDecWarps];
   uint64_t sc[4];
   unsigned long long nth;
+  uint16_t* rcm;                     // range-coder model (256 x 256) of the frame, in its entropy area
   uint32_t eoffs[kMaxSubs + 1];      // FoR chain sub-block offsets found by the frame kernel
   union {
     uint64_t wbuf[kDecWarps][kSub];  // per-warp sub-block staging (64 KB)
@@ -1093,14 +1097,170 @@ __device__ __noinline__ uint32_t rans_decode_cta(DecSmem& S, const uint8_t* p, u
 
 // entropy/mod.rs:152-178: a tag byte, then rANS (the range coder, legacy tANS
 // and the LZ cascade tags are outside the pool).
+// The range coder (rc.rs:86-225): an LZMA-style binary decoder, 11-bit
+// probabilities adapted by shift 5, under an order-1 byte model (the previous
+// byte picks one of 256 bit trees of 256 nodes).  The bits are one dependent
+// chain, so thread 0 decodes; the CTA resets the 128 KB model (in the frame's
+// entropy area) first.  Reads past the end give 0, as in the reference, so
+// only the declared length can fail (E_CORRUPT above max_len).  Every
+// renormalisation loop ends: a probability stays in [1, 2047], so after a
+// bit the range is at least 2^13 and two byte shifts bring it back above 2^24.
+__device__ __noinline__ uint32_t rc_decode_cta(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t max_len,
+                                               uint8_t* out, uint64_t cap, uint64_t* len_out) {
+  uint16_t* probs = S.rcm;
+  if (!probs) return E_NO_ENTROPY_AREA;
+  for (uint32_t i = threadIdx.x; i < 65536u; i += blockDim.x) probs[i] = 1024;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t pos = 0, len = 0;
+    uint32_t e = rd_varint(p, plen, &pos, &len);
+    if (!e && (len > max_len || len > cap)) e = E_CORRUPT;
+    if (!e) {
+      const uint8_t* in = p + pos;
+      uint64_t inlen = plen - pos, ip = 0;
+      auto next = [&]() -> uint32_t {
+        uint32_t b = ip < inlen ? in[ip] : 0u;
+        ip++;
+        return b;
+      };
+      uint32_t code = 0, range = 0xFFFFFFFFu;
+      next();  // the encoder's leading cache byte
+      for (int k = 0; k < 4; k++) code = (code << 8) | next();
+      uint32_t ctx = 0;
+      for (uint64_t i = 0; i < len; i++) {
+        uint16_t* pr = probs + ctx * 256;
+        uint32_t node = 1;
+        for (int k = 0; k < 8; k++) {
+          uint32_t pv = pr[node];
+          uint32_t bound = (range >> 11) * pv;
+          if (code >= bound) {
+            code -= bound;
+            range -= bound;
+            pr[node] = (uint16_t)(pv - (pv >> 5));
+            node = (node << 1) | 1u;
+          } else {
+            range = bound;
+            pr[node] = (uint16_t)(pv + ((2048u - pv) >> 5));
+            node <<= 1;
+          }
+          while (range < (1u << 24)) {
+            range <<= 8;
+            code = (code << 8) | next();
+          }
+        }
+        uint8_t b = (uint8_t)(node & 0xFF);
+        out[i] = b;
+        ctx = b;
+      }
+    }
+    S.sc[2] = e ? 0 : len;
+    S.flag = e;
+  }
+  __syncthreads();
+  uint32_t e = S.flag;
+  *len_out = S.sc[2];
+  __syncthreads();
+  return e;
+}
+
+// entropy/mod.rs:152-178: tag 2 rANS, tag 0 the range coder; the legacy tANS
+// tag (decoded by the reference, never produced) and the LZ cascade (Max) are
+// not decoded here.
 __device__ uint32_t residuals_cta(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t max_len, uint8_t* out,
                                  uint64_t cap, uint64_t* len_out) {
   *len_out = 0;
   if (plen == 0) return E_TRUNCATED;
   uint32_t tag = p[0];
   if (tag == 2) return rans_decode_cta(S, p + 1, plen - 1, max_len, out, cap, len_out);
-  if (tag == 0 || tag == 1 || tag == 3) return E_UNSUPPORTED;
+  if (tag == 0) return rc_decode_cta(S, p + 1, plen - 1, max_len, out, cap, len_out);
+  if (tag == 1 || tag == 3) return E_UNSUPPORTED;
   return E_CORRUPT;
+}
+
+// ---------------------------------------------------------------------------
+// Linear recurrences (linear.rs, High / Max): thread 0 runs them over the
+// decoded residual bytes (each value depends on the previous ones).  The f64
+// arithmetic is the reference's, with no contraction; NaN operands propagate
+// as x86 SSE does in source order (the first NaN operand, quieted; an invalid
+// operation gives the default NaN), so encode and decode stay in lock-step.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double nan_op(double a, double b, double r) {
+  if (isnan(a)) return as_f64(f64_bits(a) | 0x0008000000000000ull);
+  if (isnan(b)) return as_f64(f64_bits(b) | 0x0008000000000000ull);
+  if (isnan(r)) return as_f64(0xFFF8000000000000ull);
+  return r;
+}
+__device__ __forceinline__ double x_mul(double a, double b) { return nan_op(a, b, __dmul_rn(a, b)); }
+__device__ __forceinline__ double x_add(double a, double b) { return nan_op(a, b, __dadd_rn(a, b)); }
+
+// linear.rs:75-100: the order-min(order, avail) Newton extrapolation from the
+// history h (most recent first): 0.0 + c0*h0 + c1*h1 + ...
+__device__ inline double lin_predict(const double* h, uint32_t avail, uint32_t order) {
+  uint32_t eff = order < avail ? order : avail;
+  double pred = 0.0;
+  if (eff == 1) {
+    pred = x_add(pred, x_mul(1.0, h[0]));
+  } else if (eff == 2) {
+    pred = x_add(pred, x_mul(2.0, h[0]));
+    pred = x_add(pred, x_mul(-1.0, h[1]));
+  } else if (eff == 3) {
+    pred = x_add(pred, x_mul(3.0, h[0]));
+    pred = x_add(pred, x_mul(-3.0, h[1]));
+    pred = x_add(pred, x_mul(1.0, h[2]));
+  } else if (eff == 4) {
+    pred = x_add(pred, x_mul(4.0, h[0]));
+    pred = x_add(pred, x_mul(-6.0, h[1]));
+    pred = x_add(pred, x_mul(4.0, h[2]));
+    pred = x_add(pred, x_mul(-1.0, h[3]));
+  }
+  return pred;
+}
+
+// One linear-mode frame's values from its residual bytes r[0 .. len):
+// ORDERED_DELTA (linear.rs:47-66), DELTA2 (159-179), DELTA_DP (215-237).
+// Thread 0 only; returns the error kind.
+__device__ uint32_t linear_values(uint32_t mode, const uint8_t* r, uint64_t len, uint64_t n, uint64_t* vals) {
+  uint64_t pos = 0;
+  if (mode == M_ORDERED_DELTA) {
+    uint64_t p1 = 0, p2 = 0;
+    for (uint64_t i = 0; i < n; i++) {
+      uint64_t pred = i == 0 ? 0 : i == 1 ? p1 : p1 * 2 - p2, z;
+      uint32_t e = rd_varint(r, len, &pos, &z);
+      if (e) return e;
+      uint64_t v = pred + unzigzag64(z);
+      vals[i] = v;
+      p2 = p1;
+      p1 = v;
+    }
+    return pos == len ? E_OK : E_CORRUPT;
+  }
+  if (len == 0) return E_TRUNCATED;
+  uint32_t order = r[0];
+  if (order < 1 || order > 4) return E_CORRUPT;
+  pos = 1;
+  double h[4] = {0.0, 0.0, 0.0, 0.0};
+  uint64_t prev = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    double pred = lin_predict(h, i < 4 ? (uint32_t)i : 4u, order);
+    uint64_t z;
+    uint32_t e = rd_varint(r, len, &pos, &z);
+    if (e) return e;
+    double x;
+    if (mode == M_DELTA2) {
+      vals[i] = z ^ f64_bits(pred);
+      x = as_f64(vals[i]);
+    } else {
+      uint64_t rb = z ^ prev;
+      x = x_add(pred, as_f64(rb));
+      vals[i] = f64_bits(x);
+      prev = rb;
+    }
+    h[3] = h[2];
+    h[2] = h[1];
+    h[1] = h[0];
+    h[0] = x;
+  }
+  return pos == len ? E_OK : E_CORRUPT;
 }
 
 // Thread 0 computes a status, every thread gets it.
@@ -1113,7 +1273,8 @@ __device__ __forceinline__ uint32_t cta_bcast(DecSmem& S, uint32_t v) {
 }
 
 // A frame with an entropy-coded part, decoded whole by the CTA into the
-// frame's entropy area (24 bytes per value + 128) and stored.  Without an
+// frame's entropy area (24 bytes per value + 128, then the range coder's
+// 128 KB model) and stored.  Without an
 // area the frame is not decoded (E_NO_ENTROPY_AREA).
 __device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDesc& d, const FrameAux& A, const uint8_t* p,
                                          uint8_t* ent, const DecodeOut& O) {
@@ -1122,7 +1283,21 @@ __device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDes
   uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
   uint32_t e = E_OK;
   if (!ent) return E_NO_ENTROPY_AREA;
+  if (t == 0) S.rcm = reinterpret_cast<uint16_t*>(ent + ((24 * n + 128 + 127) & ~127ull));  // 128 KB past the layout
+  __syncthreads();
   switch (d.mode) {
+    case M_ORDERED_DELTA:
+    case M_DELTA2:
+    case M_DELTA_DP: {  // decoder.rs:162-171: residuals (bound 10n + 16), then the recurrence
+      uint8_t* res = ent;                                               // <= 10n + 16 bytes
+      uint64_t* vals = reinterpret_cast<uint64_t*>(ent + ((n * 10 + 16 + 15) & ~15ull));  // 8n
+      e = residuals_cta(S, p, plen, n * 10 + 16, res, n * 10 + 16, &len);
+      if (e) return e;
+      e = cta_bcast(S, t == 0 ? linear_values(d.mode, res, len, n, vals) : 0u);
+      if (e) return e;
+      cta_store_staged(S, O, c0, (uint32_t)n, [&](uint32_t q) { return vals[q]; });
+      return E_OK;
+    }
     case M_BYTE_TRANSPOSE: {  // transpose.rs:10-32, transform.rs:24-47
       uint8_t* bt = ent;
       e = residuals_cta(S, p, plen, n * 8 + 16, bt, n * 8 + 16, &len);

@@ -759,7 +759,7 @@ bool alprd_tags_h(const uint8_t* p, uint64_t plen, uint64_t* nexc, uint32_t* cta
 // (dict.rs:154-207).
 bool entropy_frame_h(const uint8_t* p, uint64_t plen, uint32_t mode) {
   switch (mode) {
-    case 11:
+    case 11: case 7: case 20: case 45:  // BYTE_TRANSPOSE; ORDERED_DELTA, DELTA2, DELTA_DP (linear.rs)
       return true;
     case 17:
       return plen < 2 || p[0] == 1;
@@ -785,7 +785,8 @@ bool entropy_frame_h(const uint8_t* p, uint64_t plen, uint32_t mode) {
 // Warp items of every frame (512 values, or 512 payload bytes for XORZ).
 // Frames the items do not cover, or whose header cannot be read here, go to
 // the frame list; the device walk reports their errors.  Listed frames with
-// an entropy-coded part get a device area of 24 bytes per value + 128
+// an entropy-coded part get a device area of 24 bytes per value + 128, then
+// 128 KB for the range coder's model
 // (128-byte units, 1 + its offset in FrameDesc::aux; 0 = none).
 void build_items(const uint8_t* src, LaneIdx& L) {
   const uint32_t V = 512, B = 512;
@@ -856,7 +857,7 @@ void build_items(const uint8_t* src, LaneIdx& L) {
     FrameDesc& d = L.frames[f];
     if (!entropy_frame_h(src + d.payload_off, d.plen, d.mode)) continue;
     d.aux = (uint32_t)(1 + L.ent_bytes / 128);
-    L.ent_bytes += (24ull * d.n + 128 + 127) & ~127ull;
+    L.ent_bytes += ((24ull * d.n + 128 + 127) & ~127ull) + 131072;  // + the range coder's model
   }
 }
 

@@ -1,0 +1,148 @@
+"""High / Max residual modes: ORDERED_DELTA (7), DELTA2 (20) and DELTA_DP (45)
+from src/codecs/linear.rs, with residual bytes coded by the range coder
+(src/entropy/rc.rs, tag 0) or rANS (tag 2), and the range coder inside other
+entropy-coded parts.  The oracle restates the encoders and decoders (its CPU
+checks port the reference's tests: rc.rs roundtrip_random_bytes /
+roundtrip_skewed_bytes / empty, linear.rs float_delta_roundtrips_all_orders /
+idelta2_roundtrips / select_order_prefers_high_on_smooth_low_on_noise); the
+GPU decode must give the oracle's values, and the oracle's error kinds on
+damaged payloads.
+"""
+import numpy as np
+import pytest
+
+from conftest import lcg_seq
+
+F64, I64, U64 = 0, 1, 2
+M_OD, M_D2, M_DP, M_BT = 7, 20, 45, 11
+TAG_RC, TAG_RANS = 0, 2
+
+
+def stream(frames, dtype=F64):
+    """A stream around raw frame payloads: [(mode, n, payload)]."""
+    n = sum(f[1] for f in frames)
+    out = bytearray(b"FCR1" + bytes([2, 0, 16, dtype]) + n.to_bytes(8, "little"))
+    for mode, k, p in frames:
+        out += bytes([mode]) + k.to_bytes(4, "little") + len(p).to_bytes(4, "little") + p
+    return bytes(out)
+
+
+def lanes():
+    rng = np.random.default_rng(31)
+    i = np.arange(20000, dtype=np.float64)
+    walk = np.cumsum(rng.normal(0, 1e-3, 20000)) + 20.0
+    special = (i * 0.25).copy()
+    special[[5, 6, 700, 701, 702, 9000]] = [np.nan, np.inf, -np.inf, np.nan, -0.0, 1e308]
+    return {
+        "ramp_half": (i * 0.5).view(np.uint64),
+        "parabola": (0.5 * i * i).view(np.uint64),
+        "sine": (np.sin(i * 0.002) * 100.0 + i * 0.01).view(np.uint64),
+        "walk": walk.view(np.uint64),
+        "specials": special.view(np.uint64),
+        "int_wrap": (np.arange(20000, dtype=np.uint64) * np.uint64(3) - np.uint64(7)),
+        "random": lcg_seq(5, 20000),
+    }
+
+
+def test_oracle_range_coder_and_linear_round_trips(oracle):
+    data = bytes((lcg_seq(1, 50000) >> np.uint64(33)).astype(np.uint8))
+    assert oracle.rc_decompress(oracle.rc_compress(data), len(data)) == data
+    s = lcg_seq(7, 50000)
+    skew = np.where(s % np.uint64(16) == 0, (s >> np.uint64(40)).astype(np.uint8), 0).astype(np.uint8).tobytes()
+    packed = oracle.rc_compress(skew)
+    assert len(packed) < len(skew) and oracle.rc_decompress(packed, len(skew)) == skew
+    assert oracle.rc_decompress(oracle.rc_compress(b""), 0) == b""
+    lv = lanes()
+    for name, v in lv.items():
+        for mode in (M_OD, M_D2, M_DP):
+            for order in (0, 1, 2, 3, 4):
+                for tag in (TAG_RC, TAG_RANS):
+                    p = oracle.linear_payload(mode, v, order, tag)
+                    if p is None:
+                        assert mode == M_DP
+                        continue
+                    assert np.array_equal(oracle.decode_mode(mode, p, len(v)), v), (name, mode, order, tag)
+    assert oracle.linear_select_order(lv["sine"]) >= 3
+    assert oracle.linear_select_order(lv["random"]) <= 2
+
+
+def _agree(qb, oracle, s):
+    try:
+        want = ("ok", oracle.decompress_column(s))
+    except oracle.OracleError as e:
+        want = (e.kind, None)
+    try:
+        got = ("ok", qb.decompress_column(s))
+    except qb.Error as e:
+        got = (e.kind, None)
+    assert got[0] == want[0]
+    if got[0] == "ok":
+        assert np.ascontiguousarray(got[1].values).view(np.uint8).tobytes() == \
+            np.ascontiguousarray(want[1][1]).view(np.uint8).tobytes()
+    return got[0]
+
+
+@pytest.mark.gpu
+def test_linear_modes_decode_like_the_oracle(qb, oracle):
+    cases = 0
+    for name, v in lanes().items():
+        for mode in (M_OD, M_D2, M_DP):
+            for order, tag in ((0, TAG_RC), (1, TAG_RANS), (2, TAG_RC), (3, TAG_RANS), (4, TAG_RC)):
+                frames = []
+                for lo, hi in ((0, 1), (1, 4097), (4097, 20000)):  # warm-up edge, a mid frame, a long one
+                    p = oracle.linear_payload(mode, v[lo:hi], order, tag)
+                    if p is None:
+                        break
+                    frames.append((mode, hi - lo, p))
+                if len(frames) < 3:
+                    continue
+                dt = U64 if mode == M_OD else F64
+                s = stream(frames, dt)
+                assert _agree(qb, oracle, s) == "ok", (name, mode, order, tag)
+                d = qb.decompress_column(s)
+                assert np.ascontiguousarray(d.values).view(np.uint64).tobytes() == v.tobytes(), (name, mode)
+                cases += 1
+    assert cases >= 60
+
+
+@pytest.mark.gpu
+def test_range_coded_parts_of_other_modes(qb, oracle):
+    v = lanes()["walk"][:5000]
+    soa = np.ascontiguousarray(v).view(np.uint8).reshape(-1, 8).T.copy().tobytes()  # byte planes
+    p = bytes([TAG_RC]) + oracle.rc_compress(soa)
+    s = stream([(M_BT, len(v), p)])
+    assert _agree(qb, oracle, s) == "ok"
+    assert np.ascontiguousarray(qb.decompress_column(s).values).view(np.uint64).tobytes() == v.tobytes()
+
+
+@pytest.mark.gpu
+def test_damaged_linear_payloads_match_oracle(qb, oracle):
+    v = lanes()["sine"][:3000]
+    kinds = {}
+    for mode in (M_D2, M_DP, M_OD):
+        for tag in (TAG_RC, TAG_RANS):
+            good = oracle.linear_payload(mode, v, 2, tag)
+            res = (oracle.rc_decompress(good[1:], 10 * len(v) + 16) if tag == TAG_RC
+                   else oracle.rans_decompress(good[1:], 10 * len(v) + 16))
+            variants = {
+                "empty": b"",
+                "tag1": b"\x01" + good[1:],
+                "tag3": b"\x03" + good[1:],
+                "tag9": b"\x09" + good[1:],
+                "cut": good[: len(good) // 2],
+                "trailing": bytes([tag]) + (oracle.rc_compress(res + b"\x00") if tag == TAG_RC
+                                            else oracle.rans_compress(res + b"\x00")),
+                "short": bytes([tag]) + (oracle.rc_compress(res[:-3]) if tag == TAG_RC
+                                         else oracle.rans_compress(res[:-3])),
+            }
+            if mode != M_OD:
+                for o in (0, 5):
+                    r2 = bytes([o]) + res[1:]
+                    variants[f"order{o}"] = bytes([tag]) + (oracle.rc_compress(r2) if tag == TAG_RC
+                                                            else oracle.rans_compress(r2))
+            for k, p in variants.items():
+                kinds[(mode, tag, k)] = _agree(qb, oracle, stream([(mode, len(v), p)]))
+    assert kinds[(M_D2, TAG_RC, "order0")] == "CorruptPayload"
+    assert kinds[(M_D2, TAG_RC, "trailing")] == "CorruptPayload"
+    assert kinds[(M_DP, TAG_RANS, "tag1")] == "Unsupported"
+    assert kinds[(M_OD, TAG_RC, "empty")] == "Truncated"
