@@ -77,6 +77,10 @@ def lib():
                                         ctypes.POINTER(U8P), ctypes.POINTER(S)]
         L.oq_rc_compress.argtypes = [P, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
         L.oq_linear_select_order.argtypes = [P, S]
+        L.oq_pred_payload.argtypes = [ctypes.c_int, P, S, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(U8P), ctypes.POINTER(S)]
+        L.oq_crc32c_u64.argtypes = [ctypes.c_uint32, ctypes.c_uint64]
+        L.oq_crc32c_u64.restype = ctypes.c_uint32
         L.oq_rc_decompress.argtypes = [P, S, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
         L.oq_pack32.argtypes = [P, ctypes.c_uint32, P]
         L.oq_unpack32.argtypes = [P, ctypes.c_uint32, P]
@@ -196,6 +200,24 @@ def rc_decompress(payload: bytes, max_len: int) -> bytes:
 
 TAG_RC, TAG_RANS = 0, 2
 M_ORDERED_DELTA, M_DELTA2, M_DELTA_DP = 7, 20, 45
+
+
+M_PRED, M_PRED2, M_PRED_RC = 0, 25, 29
+
+
+def pred_payload(mode: int, lane: np.ndarray, plog2: int = 16, tag: int = TAG_RC) -> bytes:
+    """A PRED / PRED_RC / PRED2 frame payload (codecs/pred.rs)."""
+    lane = np.ascontiguousarray(lane, dtype=np.uint64)
+    out = ctypes.POINTER(ctypes.c_uint8)()
+    olen = ctypes.c_size_t()
+    rc = lib().oq_pred_payload(mode, lane.ctypes.data, lane.size, plog2, tag, ctypes.byref(out), ctypes.byref(olen))
+    if rc:
+        raise OracleError(rc)
+    return _take(ctypes.cast(out, ctypes.c_void_p).value, olen.value) or b""
+
+
+def crc32c_u64(crc: int, v: int) -> int:
+    return lib().oq_crc32c_u64(crc, v)
 
 
 def linear_select_order(lane: np.ndarray) -> int:

@@ -2261,10 +2261,94 @@ static int dp_decode(const uint8_t *p, size_t len, size_t n, uint64_t *out) {
     return pos == len ? OQ_OK : OQ_CORRUPT;
 }
 
+/* ------------------------------------------------------------------------ */
+/* FCM / DFCM predictors — src/codecs/pred.rs with src/hash.rs (High / Max):  */
+/* a 2^predictor_log2 table indexed by CRC32C(seed, context) predicts the    */
+/* value (FCM: the last value seen after the context value; DFCM: the last   */
+/* value + the last delta seen after the context delta); residuals are XORs, */
+/* LEB128.                                                                   */
+/* ------------------------------------------------------------------------ */
+#define HASH_SEED 0x9e3779b9u
+
+/* hash.rs:18-31: CRC32C (reflected 0x82F63B78) over the 8 bytes of v */
+static uint32_t crc32c_u64(uint32_t crc, uint64_t v) {
+    for (int i = 0; i < 8; i++) {
+        crc ^= (uint32_t)(v & 0xff);
+        v >>= 8;
+        for (int k = 0; k < 8; k++) crc = (crc >> 1) ^ (0x82F63B78u & (0u - (crc & 1u)));
+    }
+    return crc;
+}
+
+/* pred.rs:23-35 */
+static void fcm_encode(const uint64_t *v, size_t n, int plog2, buf_t *out) {
+    size_t mask = ((size_t)1 << plog2) - 1, ctx = 0;
+    uint64_t *table = (uint64_t *)calloc(mask + 1, 8);
+    for (size_t i = 0; i < n; i++) {
+        b_varint(out, v[i] ^ table[ctx]);
+        table[ctx] = v[i];
+        ctx = crc32c_u64(HASH_SEED, v[i]) & mask;
+    }
+    free(table);
+}
+/* pred.rs:37-58 */
+static int fcm_decode(const uint8_t *p, size_t len, size_t n, int plog2, uint64_t *out) {
+    size_t mask = ((size_t)1 << plog2) - 1, ctx = 0, pos = 0;
+    uint64_t *table = (uint64_t *)calloc(mask + 1, 8);
+    int rc = OQ_OK;
+    for (size_t i = 0; i < n && !rc; i++) {
+        uint64_t r;
+        rc = varint_read(p, len, &pos, &r);
+        if (rc) break;
+        uint64_t v = r ^ table[ctx];
+        out[i] = v;
+        table[ctx] = v;
+        ctx = crc32c_u64(HASH_SEED, v) & mask;
+    }
+    free(table);
+    if (rc) return rc;
+    return pos == len ? OQ_OK : OQ_CORRUPT;
+}
+/* pred.rs:60-76 */
+static void dfcm_encode(const uint64_t *v, size_t n, int plog2, buf_t *out) {
+    size_t mask = ((size_t)1 << plog2) - 1, dctx = 0;
+    uint64_t *table = (uint64_t *)calloc(mask + 1, 8), last = 0;
+    for (size_t i = 0; i < n; i++) {
+        b_varint(out, v[i] ^ (last + table[dctx]));
+        uint64_t delta = v[i] - last;
+        table[dctx] = delta;
+        dctx = crc32c_u64(HASH_SEED, delta) & mask;
+        last = v[i];
+    }
+    free(table);
+}
+/* pred.rs:78-98 */
+static int dfcm_decode(const uint8_t *p, size_t len, size_t n, int plog2, uint64_t *out) {
+    size_t mask = ((size_t)1 << plog2) - 1, dctx = 0, pos = 0;
+    uint64_t *table = (uint64_t *)calloc(mask + 1, 8), last = 0;
+    int rc = OQ_OK;
+    for (size_t i = 0; i < n; i++) {
+        uint64_t pred = last + table[dctx], r;
+        rc = varint_read(p, len, &pos, &r);
+        if (rc) break;
+        uint64_t v = r ^ pred;
+        out[i] = v;
+        uint64_t delta = v - last;
+        table[dctx] = delta;
+        dctx = crc32c_u64(HASH_SEED, delta) & mask;
+        last = v;
+    }
+    free(table);
+    if (rc) return rc;
+    return pos == len ? OQ_OK : OQ_CORRUPT;
+}
+
 /* decoder.rs:150-171: entropy-coded residuals (bound 10n + 16), then the recurrence */
 static int linear_frame_decode(int mode, const uint8_t *p, size_t plen, size_t n, uint64_t *out);
 
-static int decode_frame(int mode, const uint8_t *p, size_t plen, size_t n, int dtype, uint64_t *out) {
+static int pred_frame_decode(int mode, const uint8_t *p, size_t plen, size_t n, int plog2, uint64_t *out);
+
+static int decode_frame(int mode, const uint8_t *p, size_t plen, size_t n, int dtype, int plog2, uint64_t *out) {
     switch (mode) {
         case M_RAW: return raw_decode(p, plen, n, dtype, out);
         case M_CONST:
@@ -2295,8 +2379,22 @@ static int decode_frame(int mode, const uint8_t *p, size_t plen, size_t n, int d
         case M_ORDERED_DELTA:
         case M_DELTA2:
         case M_DELTA_DP: return linear_frame_decode(mode, p, plen, n, out);
+        case M_PRED:
+        case M_PRED_RC:
+        case M_PRED2: return pred_frame_decode(mode, p, plen, n, plog2, out);
         default: return OQ_UNSUPPORTED;
     }
+}
+
+/* decoder.rs:150-157: PRED reads LEB128 residuals directly, PRED_RC and
+ * PRED2 entropy-coded ones (bound 10n + 16) */
+static int pred_frame_decode(int mode, const uint8_t *p, size_t plen, size_t n, int plog2, uint64_t *out) {
+    if (mode == M_PRED) return fcm_decode(p, plen, n, plog2, out);
+    buf_t b = {0};
+    int rc = decode_residuals(p, plen, n * 10 + 16, &b);
+    if (!rc) rc = mode == M_PRED_RC ? fcm_decode(b.p, b.len, n, plog2, out) : dfcm_decode(b.p, b.len, n, plog2, out);
+    b_free(&b);
+    return rc;
 }
 
 static int linear_frame_decode(int mode, const uint8_t *p, size_t plen, size_t n, uint64_t *out) {
@@ -2322,6 +2420,7 @@ typedef struct {
     const frame_t *frames;
     size_t nf;
     int dtype;
+    int plog2; /* the header's predictor_log2 (format.rs:56-94) */
     uint64_t *lane;
     int *rcs;
     _Atomic size_t next;
@@ -2333,7 +2432,7 @@ static void *dec_worker(void *arg) {
         size_t k = atomic_fetch_add(&j->next, 1);
         if (k >= j->nf) break;
         const frame_t *f = &j->frames[k];
-        j->rcs[k] = decode_frame(f->mode, f->payload, f->plen, f->n, j->dtype, j->lane + f->off);
+        j->rcs[k] = decode_frame(f->mode, f->payload, f->plen, f->n, j->dtype, j->plog2, j->lane + f->off);
     }
     return NULL;
 }
@@ -2428,7 +2527,7 @@ static int decompress_lane(const uint8_t *src, size_t len, int threads, int *dty
     {
         uint64_t *vals = (uint64_t *)malloc(sizeof(uint64_t) * (n_total ? n_total : 1));
         int *rcs = (int *)calloc(nf ? nf : 1, sizeof(int));
-        dec_job_t job = {frames, nf, dtype, vals, rcs, 0};
+        dec_job_t job = {frames, nf, dtype, src[6], vals, rcs, 0};
         if (threads > 1 && nf > 1) {
             pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)threads);
             for (int i = 0; i < threads; i++) pthread_create(&th[i], NULL, dec_worker, &job);
@@ -2922,6 +3021,40 @@ int oq_linear_payload(int mode, const uint64_t *v, size_t n, int order, int tag,
 
 int oq_linear_select_order(const uint64_t *v, size_t n) { return lin_select_order(v, n); }
 
+/* A PRED (0, LEB128 residuals), PRED_RC (29) or PRED2 (25) frame payload
+ * (codecs/pred.rs) at predictor_log2 plog2; the residual bytes of 29 and 25
+ * are coded by `tag` (TAG_RC or TAG_RANS). */
+int oq_pred_payload(int mode, const uint64_t *v, size_t n, int plog2, int tag, uint8_t **out, size_t *out_len) {
+    buf_t r = {0}, b = {0};
+    *out = NULL;
+    *out_len = 0;
+    if (plog2 < 10 || plog2 > 16) return OQ_CORRUPT;
+    if (mode == M_PRED2) dfcm_encode(v, n, plog2, &r);
+    else if (mode == M_PRED || mode == M_PRED_RC) fcm_encode(v, n, plog2, &r);
+    else return OQ_UNSUPPORTED;
+    if (mode == M_PRED) {
+        *out = r.p ? r.p : (uint8_t *)malloc(1);
+        *out_len = r.len;
+        return OQ_OK;
+    }
+    if (tag == TAG_RC) {
+        b_push(&b, TAG_RC);
+        rc_compress(r.p, r.len, &b);
+    } else if (tag == TAG_RANS && r.len) {
+        b_push(&b, TAG_RANS);
+        rans_compress(r.p, r.len, &b);
+    } else {
+        b_free(&r);
+        return OQ_UNSUPPORTED;
+    }
+    b_free(&r);
+    *out = b.p;
+    *out_len = b.len;
+    return OQ_OK;
+}
+
+uint32_t oq_crc32c_u64(uint32_t crc, uint64_t v) { return crc32c_u64(crc, v); }
+
 int oq_rc_compress(const uint8_t *data, size_t n, uint8_t **out, size_t *out_len) {
     buf_t b = {0};
     rc_compress(data, n, &b);
@@ -2939,7 +3072,7 @@ int oq_rc_decompress(const uint8_t *payload, size_t len, size_t max_len, uint8_t
 }
 
 int oq_decode_mode(int mode, const uint8_t *payload, size_t plen, size_t n, int dtype, uint64_t *out) {
-    return decode_frame(mode, payload, plen, n, dtype, out);
+    return decode_frame(mode, payload, plen, n, dtype, 16, out);
 }
 
 int oq_validity_encode(const uint8_t *bitmap, size_t n, uint8_t **out, size_t *out_len) {

@@ -119,6 +119,12 @@ int oq_decompress_column_mt(const uint8_t *src, size_t len, int threads, int *dt
  * *out = NULL when DELTA_DP does not apply to the values. */
 int oq_linear_payload(int mode, const uint64_t *vals, size_t n, int order, int tag,
                       uint8_t **out, size_t *out_len);
+/* FCM / DFCM predictor payloads (src/codecs/pred.rs): mode 0 (PRED), 29
+ * (PRED_RC) or 25 (PRED2) at predictor_log2 plog2 (10..16); tag as above for
+ * 29 and 25.  And the predictor hash (src/hash.rs). */
+int oq_pred_payload(int mode, const uint64_t *vals, size_t n, int plog2, int tag,
+                    uint8_t **out, size_t *out_len);
+uint32_t oq_crc32c_u64(uint32_t crc, uint64_t v);
 /* linear.rs:121-140: the extrapolation order the reference's encoder picks. */
 int oq_linear_select_order(const uint64_t *vals, size_t n);
 /* The range coder (src/entropy/rc.rs): varint(len) ++ coded bytes. */

@@ -164,6 +164,9 @@ __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDes
     case M_ORDERED_DELTA:   // linear.rs: entropy-coded residual bytes (decoder.rs:162-171)
     case M_DELTA2:
     case M_DELTA_DP:
+    case M_PRED:            // pred.rs: a predictor table in the frame's area (decoder.rs:150-157)
+    case M_PRED_RC:
+    case M_PRED2:
       A.ent = 1;
       break;
     case M_FLOAT_MULT: {  // float_mult.rs:100-133
@@ -1216,6 +1219,54 @@ __device__ inline double lin_predict(const double* h, uint32_t avail, uint32_t o
   return pred;
 }
 
+// The predictor hash (hash.rs:18-31): CRC32C, reflected polynomial
+// 0x82F63B78, over the 8 bytes of v, by slicing: eight 256-entry tables
+// (t[k][b] = the CRC of byte b followed by k zero bytes) in shared memory.
+__device__ void crc_tables(uint32_t (*t)[256]) {
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
+    uint32_t c = i;
+    for (int k = 0; k < 8; k++) c = (c >> 1) ^ (0x82F63B78u & (0u - (c & 1u)));
+    t[0][i] = c;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x)
+    for (int k = 1; k < 8; k++) t[k][i] = (t[k - 1][i] >> 8) ^ t[0][t[k - 1][i] & 0xFF];
+  __syncthreads();
+}
+__device__ __forceinline__ uint32_t crc32c_u64(const uint32_t (*t)[256], uint32_t crc, uint64_t v) {
+  uint32_t x = crc ^ (uint32_t)v, hi = (uint32_t)(v >> 32);
+  return t[7][x & 0xFF] ^ t[6][(x >> 8) & 0xFF] ^ t[5][(x >> 16) & 0xFF] ^ t[4][x >> 24] ^ t[3][hi & 0xFF] ^
+         t[2][(hi >> 8) & 0xFF] ^ t[1][(hi >> 16) & 0xFF] ^ t[0][hi >> 24];
+}
+
+// FCM (pred.rs:37-58) or DFCM (pred.rs:78-98) values from LEB128 residuals
+// r[0 .. len) with a zeroed 2^plog2 table.  Thread 0 only.
+__device__ uint32_t pred_values(bool dfcm, const uint8_t* r, uint64_t len, uint64_t n, uint32_t plog2,
+                                const uint32_t (*crc)[256], uint64_t* table, uint64_t* vals) {
+  const uint32_t seed = 0x9e3779b9u, mask = (1u << plog2) - 1u;
+  uint64_t pos = 0, last = 0;
+  uint32_t ctx = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    uint64_t z;
+    uint32_t e = rd_varint(r, len, &pos, &z);
+    if (e) return e;
+    if (!dfcm) {
+      uint64_t v = z ^ table[ctx];
+      vals[i] = v;
+      table[ctx] = v;
+      ctx = crc32c_u64(crc, seed, v) & mask;
+    } else {
+      uint64_t v = z ^ (last + table[ctx]);
+      vals[i] = v;
+      uint64_t delta = v - last;
+      table[ctx] = delta;
+      ctx = crc32c_u64(crc, seed, delta) & mask;
+      last = v;
+    }
+  }
+  return pos == len ? E_OK : E_CORRUPT;
+}
+
 // One linear-mode frame's values from its residual bytes r[0 .. len):
 // ORDERED_DELTA (linear.rs:47-66), DELTA2 (159-179), DELTA_DP (215-237).
 // Thread 0 only; returns the error kind.
@@ -1286,6 +1337,28 @@ __device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDes
   if (t == 0) S.rcm = reinterpret_cast<uint16_t*>(ent + ((24 * n + 128 + 127) & ~127ull));  // 128 KB past the layout
   __syncthreads();
   switch (d.mode) {
+    case M_PRED:
+    case M_PRED_RC:
+    case M_PRED2: {  // decoder.rs:150-157: PRED's payload is the LEB128 residuals
+      uint8_t* res = ent;                                                               // <= 10n + 16 bytes
+      uint64_t* vals = reinterpret_cast<uint64_t*>(ent + ((n * 10 + 16 + 15) & ~15ull));  // 8n
+      uint64_t* table = reinterpret_cast<uint64_t*>(ent + ((24 * n + 128 + 127) & ~127ull) + 131072);
+      const uint8_t* r = p;
+      len = plen;
+      if (d.mode != M_PRED) {
+        e = residuals_cta(S, p, plen, n * 10 + 16, res, n * 10 + 16, &len);
+        if (e) return e;
+        r = res;
+      }
+      uint32_t plog2 = O.plog2 < 10 ? 10u : O.plog2 > 16 ? 16u : O.plog2;
+      for (uint32_t i = t; i < (1u << plog2); i += blockDim.x) table[i] = 0;
+      auto crc = reinterpret_cast<uint32_t(*)[256]>(&S.u.wbuf[0][0]);  // 8 KB of the staging area
+      crc_tables(crc);
+      e = cta_bcast(S, t == 0 ? pred_values(d.mode == M_PRED2, r, len, n, plog2, crc, table, vals) : 0u);
+      if (e) return e;
+      cta_store_staged(S, O, c0, (uint32_t)n, [&](uint32_t q) { return vals[q]; });
+      return E_OK;
+    }
     case M_ORDERED_DELTA:
     case M_DELTA2:
     case M_DELTA_DP: {  // decoder.rs:162-171: residuals (bound 10n + 16), then the recurrence

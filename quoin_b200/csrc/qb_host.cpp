@@ -605,6 +605,7 @@ int compress_column_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, c
 // ---------------------------------------------------------------------------
 struct LaneIdx {
   int dtype = 0;
+  uint32_t plog2 = 16;  // header byte 6 (format.rs:56-94): the FCM / DFCM table size
   uint64_t logical_n = 0, n_total = 0;
   bool has_validity = false;
   std::vector<uint8_t> bitmap;  // ceil(n/8), trailing bits cleared
@@ -624,6 +625,7 @@ struct LaneIdx {
   // reuses its parsed index, so repeated decodes touch no fresh pages).
   void reset() {
     dtype = 0;
+    plog2 = 16;
     logical_n = n_total = 0;
     has_validity = false;
     bitmap.clear();
@@ -690,6 +692,7 @@ int parse_lane(const uint8_t* src, uint64_t base, uint64_t len, LaneIdx& L) {
   if (s[6] < 10 || s[6] > 16) return K_CORRUPT;
   if (s[7] > 7) return K_DTYPE;
   L.dtype = s[7];
+  L.plog2 = s[6];
   L.has_validity = s[5] & 1;
   L.logical_n = rd64(s + 8);
   if (L.logical_n > kMaxLogicalValues) return K_CORRUPT;  // decoder.rs:105-106 / validity.rs:135-136 allocation
@@ -760,6 +763,7 @@ bool alprd_tags_h(const uint8_t* p, uint64_t plen, uint64_t* nexc, uint32_t* cta
 bool entropy_frame_h(const uint8_t* p, uint64_t plen, uint32_t mode) {
   switch (mode) {
     case 11: case 7: case 20: case 45:  // BYTE_TRANSPOSE; ORDERED_DELTA, DELTA2, DELTA_DP (linear.rs)
+    case 0: case 25: case 29:           // PRED, PRED2, PRED_RC (pred.rs; PRED needs only the table)
       return true;
     case 17:
       return plen < 2 || p[0] == 1;
@@ -858,6 +862,7 @@ void build_items(const uint8_t* src, LaneIdx& L) {
     if (!entropy_frame_h(src + d.payload_off, d.plen, d.mode)) continue;
     d.aux = (uint32_t)(1 + L.ent_bytes / 128);
     L.ent_bytes += ((24ull * d.n + 128 + 127) & ~127ull) + 131072;  // + the range coder's model
+    if (d.mode == 0 || d.mode == 25 || d.mode == 29) L.ent_bytes += 8ull << L.plog2;  // + the predictor table
   }
 }
 
@@ -1111,6 +1116,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
     if (fused) {
       DecodeOut O{d_out, X.wire, X.has_validity ? reinterpret_cast<const uint32_t*>(dbm) : nullptr, drank, dsel, X.n,
                   L.n_total};
+      O.plog2 = L.plog2;
       {
         TimedRegion tr(T_DECODE, st);
         launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, plan_of(L), dpre,
@@ -1121,6 +1127,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
       CK(c->ensure(S_LANE, L.n_total * 8 + 64));
       uint64_t* lane_out = c->p<uint64_t>(S_LANE);
       DecodeOut O{lane_out, WT_U64, nullptr, nullptr, nullptr, L.n_total, L.n_total};
+      O.plog2 = L.plog2;
       {
         TimedRegion tr(T_DECODE, st);
         launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, plan_of(L), dpre,
@@ -1145,6 +1152,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
     for (int k = 0; k < X.nl; k++) {
       const LaneIdx& L = X.lanes[k];
       DecodeOut O{limbs + (uint64_t)k * X.n_valid, WT_U64, nullptr, nullptr, nullptr, X.n_valid, X.n_valid};
+      O.plog2 = L.plog2;
       TimedRegion tr(T_DECODE, st);
       launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), WT_U64, O, plan_of(L), dpre, scr,
                           daux, d_err, st);

@@ -24,6 +24,7 @@ struct DecodeOut {
   const uint64_t* sel;
   uint64_t n;       // logical values (positions)
   uint64_t nvalid;  // lane values
+  uint32_t plog2 = 16;  // the stream header's predictor_log2 (FCM / DFCM table size)
 };
 void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
                           uint64_t* scratch, void* aux, unsigned long long* err, cudaStream_t st);

@@ -1,7 +1,8 @@
 """High / Max residual modes: ORDERED_DELTA (7), DELTA2 (20) and DELTA_DP (45)
-from src/codecs/linear.rs, with residual bytes coded by the range coder
-(src/entropy/rc.rs, tag 0) or rANS (tag 2), and the range coder inside other
-entropy-coded parts.  The oracle restates the encoders and decoders (its CPU
+from src/codecs/linear.rs, PRED (0), PRED_RC (29) and PRED2 (25) from
+src/codecs/pred.rs with the CRC32C predictor hash (src/hash.rs), with residual
+bytes coded by the range coder (src/entropy/rc.rs, tag 0) or rANS (tag 2), and
+the range coder inside other entropy-coded parts.  The oracle restates the encoders and decoders (its CPU
 checks port the reference's tests: rc.rs roundtrip_random_bytes /
 roundtrip_skewed_bytes / empty, linear.rs float_delta_roundtrips_all_orders /
 idelta2_roundtrips / select_order_prefers_high_on_smooth_low_on_noise); the
@@ -146,3 +147,55 @@ def test_damaged_linear_payloads_match_oracle(qb, oracle):
     assert kinds[(M_D2, TAG_RC, "trailing")] == "CorruptPayload"
     assert kinds[(M_DP, TAG_RANS, "tag1")] == "Unsupported"
     assert kinds[(M_OD, TAG_RC, "empty")] == "Truncated"
+
+
+M_PRED, M_PRED2, M_PRED_RC = 0, 25, 29
+
+
+def _crc32c_u64(crc, v):
+    for _ in range(8):
+        crc ^= v & 0xFF
+        v >>= 8
+        for _ in range(8):
+            crc = (crc >> 1) ^ (0x82F63B78 if crc & 1 else 0)
+    return crc
+
+
+def test_oracle_predictor_hash_and_round_trips(oracle):
+    for v in [0, 1, 42, 255, 256, 2**64 - 1, 0x0102030405060708] + [int(x) for x in lcg_seq(3, 50)]:
+        assert oracle.crc32c_u64(0x9E3779B9, v) == _crc32c_u64(0x9E3779B9, v)
+    for name, v in lanes().items():
+        for mode in (M_PRED, M_PRED_RC, M_PRED2):
+            for plog2 in (10, 16):
+                for tag in (TAG_RC, TAG_RANS):
+                    p = oracle.pred_payload(mode, v, plog2, tag)
+                    s = stream([(mode, len(v), p)], U64)
+                    s = s[:6] + bytes([plog2]) + s[7:]
+                    got = oracle.decompress_column(s)[1]
+                    assert np.ascontiguousarray(got).view(np.uint64).tobytes() == v.tobytes(), (name, mode)
+
+
+@pytest.mark.gpu
+def test_predictor_modes_decode_like_the_oracle(qb, oracle):
+    cases = 0
+    lv = lanes()
+    lv["repeats"] = np.tile(lcg_seq(9, 37), 600)[:20000]
+    for name, v in lv.items():
+        for mode, plog2, tag in ((M_PRED, 16, TAG_RC), (M_PRED, 10, TAG_RC), (M_PRED_RC, 16, TAG_RC),
+                                 (M_PRED_RC, 12, TAG_RANS), (M_PRED2, 16, TAG_RANS), (M_PRED2, 10, TAG_RC)):
+            frames = [(mode, hi - lo, oracle.pred_payload(mode, v[lo:hi], plog2, tag))
+                      for lo, hi in ((0, 1), (1, 4097), (4097, 20000))]
+            s = stream(frames, U64)
+            s = s[:6] + bytes([plog2]) + s[7:]
+            assert _agree(qb, oracle, s) == "ok", (name, mode, plog2, tag)
+            assert np.ascontiguousarray(qb.decompress_column(s).values).view(np.uint64).tobytes() == v.tobytes()
+            cases += 1
+    assert cases == 6 * len(lv)
+    # damage: trailing byte, cut residuals, bad tags
+    v = lv["sine"][:3000]
+    kinds = []
+    for mode in (M_PRED, M_PRED_RC, M_PRED2):
+        good = oracle.pred_payload(mode, v, 16, TAG_RC)
+        for bad in (good + b"\x00", good[:-5], b"\x05" + good[1:], b""):
+            kinds.append(_agree(qb, oracle, stream([(mode, len(v), bad)], U64)))
+    assert "CorruptPayload" in kinds and "Truncated" in kinds
