@@ -81,6 +81,8 @@ def lib():
                                       ctypes.POINTER(U8P), ctypes.POINTER(S)]
         L.oq_crc32c_u64.argtypes = [ctypes.c_uint32, ctypes.c_uint64]
         L.oq_crc32c_u64.restype = ctypes.c_uint32
+        L.oq_lz_compress.argtypes = [P, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
+        L.oq_lz_decompress.argtypes = [P, S, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
         L.oq_rc_decompress.argtypes = [P, S, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
         L.oq_pack32.argtypes = [P, ctypes.c_uint32, P]
         L.oq_unpack32.argtypes = [P, ctypes.c_uint32, P]
@@ -214,6 +216,28 @@ def pred_payload(mode: int, lane: np.ndarray, plog2: int = 16, tag: int = TAG_RC
     if rc:
         raise OracleError(rc)
     return _take(ctypes.cast(out, ctypes.c_void_p).value, olen.value) or b""
+
+
+def lz_compress(data: bytes) -> bytes:
+    """The LZ stream of codecs/lz.rs."""
+    a = np.frombuffer(data, dtype=np.uint8) if data else np.zeros(1, np.uint8)
+    out = ctypes.POINTER(ctypes.c_uint8)()
+    olen = ctypes.c_size_t()
+    lib().oq_lz_compress(a.ctypes.data, len(data), ctypes.byref(out), ctypes.byref(olen))
+    return _take(ctypes.cast(out, ctypes.c_void_p).value, olen.value) or b""
+
+
+def lz_decompress(stream: bytes, expected: int) -> bytes:
+    a = np.frombuffer(stream, dtype=np.uint8) if stream else np.zeros(1, np.uint8)
+    out = ctypes.POINTER(ctypes.c_uint8)()
+    olen = ctypes.c_size_t()
+    rc = lib().oq_lz_decompress(a.ctypes.data, len(stream), expected, ctypes.byref(out), ctypes.byref(olen))
+    if rc:
+        raise OracleError(rc)
+    return _take(ctypes.cast(out, ctypes.c_void_p).value, olen.value) or b""
+
+
+M_LZ, TAG_LZ = 4, 3
 
 
 def crc32c_u64(crc: int, v: int) -> int:

@@ -978,17 +978,153 @@ static int rc_decompress(const uint8_t *p, size_t plen, size_t max_len, buf_t *o
     return OQ_OK;
 }
 
-/* entropy/mod.rs:152-178.  The legacy tANS tag (decoded by the reference,
- * never produced) and the LZ cascade tag (Max) are not restated. */
-static int decode_residuals(const uint8_t *p, size_t plen, size_t max_len, buf_t *out) {
+/* ------------------------------------------------------------------------ */
+/* LZ — src/codecs/lz.rs: byte LZ77 with LZSS framing (a control byte of 8    */
+/* flags, MSB first; 1 = match (varint offset, varint length - 4), 0 = a     */
+/* literal byte) after varint(original length).  Mode LZ (4) codes a block's  */
+/* little-endian bytes; the Max cascade (entropy tag 3) codes residual bytes. */
+/* ------------------------------------------------------------------------ */
+#define LZ_MIN_MATCH 4
+#define LZ_HASH_BITS 17
+#define LZ_MAX_CHAIN 64
+
+/* lz.rs:19-23 */
+static size_t lz_hash4(const uint8_t *w) {
+    uint32_t v = (uint32_t)w[0] | ((uint32_t)w[1] << 8) | ((uint32_t)w[2] << 16) | ((uint32_t)w[3] << 24);
+    return (size_t)((uint32_t)(v * 2654435761u) >> (32 - LZ_HASH_BITS));
+}
+
+/* lz.rs:30-117: greedy matching over hash chains of at most 64 candidates */
+static void lz_compress(const uint8_t *in, size_t n, buf_t *out) {
+    int64_t *head = (int64_t *)malloc(((size_t)1 << LZ_HASH_BITS) * sizeof(int64_t));
+    int64_t *prev = (int64_t *)malloc((n ? n : 1) * sizeof(int64_t));
+    for (size_t i = 0; i < ((size_t)1 << LZ_HASH_BITS); i++) head[i] = -1;
+    for (size_t i = 0; i < n; i++) prev[i] = -1;
+    /* tokens: off = 0 marks a literal (matches always have off >= 1) */
+    uint32_t *toff = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
+    uint32_t *tval = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
+    size_t nt = 0, i = 0;
+    while (i < n) {
+        size_t best_len = 0, best_off = 0;
+        if (i + LZ_MIN_MATCH <= n) {
+            size_t h = lz_hash4(in + i), max_len = n - i;
+            int64_t cand = head[h];
+            int chain = LZ_MAX_CHAIN;
+            while (cand >= 0 && chain > 0) {
+                size_t c = (size_t)cand;
+                if (best_len == 0 || (c + best_len < n && in[c + best_len] == in[i + best_len])) {
+                    size_t l = 0;
+                    while (l < max_len && in[c + l] == in[i + l]) l++;
+                    if (l > best_len) {
+                        best_len = l;
+                        best_off = i - c;
+                        if (l == max_len) break;
+                    }
+                }
+                cand = prev[c];
+                chain--;
+            }
+        }
+        if (best_len >= LZ_MIN_MATCH) {
+            toff[nt] = (uint32_t)best_off;
+            tval[nt++] = (uint32_t)best_len;
+            size_t end = i + best_len;
+            for (; i < end; i++)
+                if (i + LZ_MIN_MATCH <= n) {
+                    size_t h = lz_hash4(in + i);
+                    prev[i] = head[h];
+                    head[h] = (int64_t)i;
+                }
+        } else {
+            toff[nt] = 0;
+            tval[nt++] = in[i];
+            if (i + LZ_MIN_MATCH <= n) {
+                size_t h = lz_hash4(in + i);
+                prev[i] = head[h];
+                head[h] = (int64_t)i;
+            }
+            i++;
+        }
+    }
+    b_varint(out, n);
+    for (size_t g = 0; g < nt; g += 8) {
+        uint8_t ctrl = 0;
+        size_t ge = g + 8 < nt ? g + 8 : nt;
+        for (size_t k = g; k < ge; k++)
+            if (toff[k]) ctrl |= (uint8_t)(1u << (7 - (k - g)));
+        b_push(out, ctrl);
+        for (size_t k = g; k < ge; k++) {
+            if (toff[k]) {
+                b_varint(out, toff[k]);
+                b_varint(out, tval[k] - LZ_MIN_MATCH);
+            } else {
+                b_push(out, (uint8_t)tval[k]);
+            }
+        }
+    }
+    free(head);
+    free(prev);
+    free(toff);
+    free(tval);
+}
+
+/* lz.rs:119-155 */
+static int lz_decompress(const uint8_t *p, size_t len, size_t expected, buf_t *out) {
+    size_t pos = 0;
+    uint64_t n;
+    int rc = varint_read(p, len, &pos, &n);
+    if (rc) return rc;
+    if (n != expected) return OQ_CORRUPT;
+    b_reserve(out, (size_t)n);
+    while (out->len < n) {
+        if (pos >= len) return OQ_TRUNCATED;
+        uint8_t ctrl = p[pos++];
+        for (int k = 0; k < 8 && out->len < n; k++) {
+            if ((ctrl >> (7 - k)) & 1) {
+                uint64_t off, ml;
+                if ((rc = varint_read(p, len, &pos, &off))) return rc;
+                if ((rc = varint_read(p, len, &pos, &ml))) return rc;
+                ml += LZ_MIN_MATCH;
+                if (off == 0 || off > out->len) return OQ_CORRUPT;
+                if (ml > n - out->len) return OQ_CORRUPT; /* out.len() + len > n, without wrapping */
+                size_t start = out->len - (size_t)off;
+                for (uint64_t j = 0; j < ml; j++) b_push(out, out->p[start + j]);
+            } else {
+                if (pos >= len) return OQ_TRUNCATED;
+                b_push(out, p[pos++]);
+            }
+        }
+    }
+    return OQ_OK;
+}
+
+/* entropy/mod.rs:152-163: tag 2 rANS, tag 0 the range coder; the legacy
+ * tANS tag (decoded by the reference, never produced) is not restated. */
+static int decode_entropy_only(const uint8_t *p, size_t plen, size_t max_len, buf_t *out) {
     if (plen == 0) return OQ_TRUNCATED;
     switch (p[0]) {
         case TAG_RANS: return rans_decompress(p + 1, plen - 1, max_len, out);
         case TAG_RC: return rc_decompress(p + 1, plen - 1, max_len, out);
-        case TAG_TANS:
-        case TAG_LZ: return OQ_UNSUPPORTED;
+        case TAG_TANS: return OQ_UNSUPPORTED;
         default: return OQ_CORRUPT;
     }
+}
+/* entropy/mod.rs:165-178: tag 3 is the LZ cascade (Max): varint(residual
+ * length) ++ an entropy-coded LZ stream of at most 2 * length + 64 bytes. */
+static int decode_residuals(const uint8_t *p, size_t plen, size_t max_len, buf_t *out) {
+    if (plen && p[0] == TAG_LZ) {
+        size_t pos = 0;
+        uint64_t orig;
+        int rc = varint_read(p + 1, plen - 1, &pos, &orig);
+        if (rc) return rc;
+        if (orig > max_len) return OQ_CORRUPT;
+        buf_t lzs = {0};
+        rc = decode_entropy_only(p + 1 + pos, plen - 1 - pos, (size_t)orig * 2 + 64, &lzs);
+        if (!rc) rc = lz_decompress(lzs.p, lzs.len, (size_t)orig, out);
+        b_free(&lzs);
+        return rc;
+    }
+    return decode_entropy_only(p, plen, max_len, out);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -2382,6 +2518,16 @@ static int decode_frame(int mode, const uint8_t *p, size_t plen, size_t n, int d
         case M_PRED:
         case M_PRED_RC:
         case M_PRED2: return pred_frame_decode(mode, p, plen, n, plog2, out);
+        case M_LZ: { /* decoder.rs:172-175, lz.rs:165-172 */
+            buf_t b = {0}, o = {0};
+            int rc = decode_residuals(p, plen, n * 16 + 1024, &b);
+            if (!rc) rc = lz_decompress(b.p, b.len, n * 8, &o);
+            if (!rc)
+                for (size_t i = 0; i < n; i++) out[i] = rd_u64(o.p + 8 * i);
+            b_free(&b);
+            b_free(&o);
+            return rc;
+        }
         default: return OQ_UNSUPPORTED;
     }
 }
@@ -3054,6 +3200,22 @@ int oq_pred_payload(int mode, const uint64_t *v, size_t n, int plog2, int tag, u
 }
 
 uint32_t oq_crc32c_u64(uint32_t crc, uint64_t v) { return crc32c_u64(crc, v); }
+
+/* lz.rs: the LZ stream of `data` (lz_compress) and its inverse */
+int oq_lz_compress(const uint8_t *data, size_t n, uint8_t **out, size_t *out_len) {
+    buf_t b = {0};
+    lz_compress(data, n, &b);
+    *out = b.p;
+    *out_len = b.len;
+    return OQ_OK;
+}
+int oq_lz_decompress(const uint8_t *stream, size_t len, size_t expected, uint8_t **out, size_t *out_len) {
+    buf_t b = {0};
+    int rc = lz_decompress(stream, len, expected, &b);
+    *out = b.p ? b.p : (uint8_t *)malloc(1);
+    *out_len = b.len;
+    return rc;
+}
 
 int oq_rc_compress(const uint8_t *data, size_t n, uint8_t **out, size_t *out_len) {
     buf_t b = {0};

@@ -125,6 +125,10 @@ int oq_linear_payload(int mode, const uint64_t *vals, size_t n, int order, int t
 int oq_pred_payload(int mode, const uint64_t *vals, size_t n, int plog2, int tag,
                     uint8_t **out, size_t *out_len);
 uint32_t oq_crc32c_u64(uint32_t crc, uint64_t v);
+/* The LZ stream of src/codecs/lz.rs (lz_compress / lz_decompress). */
+int oq_lz_compress(const uint8_t *data, size_t n, uint8_t **out, size_t *out_len);
+int oq_lz_decompress(const uint8_t *stream, size_t len, size_t expected, uint8_t **out,
+                     size_t *out_len);
 /* linear.rs:121-140: the extrapolation order the reference's encoder picks. */
 int oq_linear_select_order(const uint64_t *vals, size_t n);
 /* The range coder (src/entropy/rc.rs): varint(len) ++ coded bytes. */

@@ -167,6 +167,7 @@ __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDes
     case M_PRED:            // pred.rs: a predictor table in the frame's area (decoder.rs:150-157)
     case M_PRED_RC:
     case M_PRED2:
+    case M_LZ:              // lz.rs: entropy-coded LZ tokens (decoder.rs:172-175)
       A.ent = 1;
       break;
     case M_FLOAT_MULT: {  // float_mult.rs:100-133
@@ -369,6 +370,8 @@ struct DecSmem {
   uint64_t sc[4];
   unsigned long long nth;
   uint16_t* rcm;                     // range-coder model (256 x 256) of the frame, in its entropy area
+  uint8_t* lzs;                      // the LZ cascade's scratch (ent_lz_cap bytes), in the same area
+  uint64_t lzs_cap;
   uint32_t eoffs[kMaxSubs + 1];      // FoR chain sub-block offsets found by the frame kernel
   union {
     uint64_t wbuf[kDecWarps][kSub];  // per-warp sub-block staging (64 KB)
@@ -1100,6 +1103,15 @@ __device__ __noinline__ uint32_t rans_decode_cta(DecSmem& S, const uint8_t* p, u
 
 // entropy/mod.rs:152-178: a tag byte, then rANS (the range coder, legacy tANS
 // and the LZ cascade tags are outside the pool).
+// Thread 0 computes a status, every thread gets it.
+__device__ __forceinline__ uint32_t cta_bcast(DecSmem& S, uint32_t v) {
+  if (threadIdx.x == 0) S.sc[3] = v;
+  __syncthreads();
+  uint32_t r = (uint32_t)S.sc[3];
+  __syncthreads();
+  return r;
+}
+
 // The range coder (rc.rs:86-225): an LZMA-style binary decoder, 11-bit
 // probabilities adapted by shift 5, under an order-1 byte model (the previous
 // byte picks one of 256 bit trees of 256 nodes).  The bits are one dependent
@@ -1166,18 +1178,66 @@ __device__ __noinline__ uint32_t rc_decode_cta(DecSmem& S, const uint8_t* p, uin
   return e;
 }
 
-// entropy/mod.rs:152-178: tag 2 rANS, tag 0 the range coder; the legacy tANS
-// tag (decoded by the reference, never produced) and the LZ cascade (Max) are
-// not decoded here.
-__device__ uint32_t residuals_cta(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t max_len, uint8_t* out,
-                                 uint64_t cap, uint64_t* len_out) {
+// LZ tokens (lz.rs:119-155): varint(length) (== expected, else E_CORRUPT),
+// then groups of a control byte (8 flags, MSB first) and 8 tokens: a match
+// (varint offset, varint length - 4; overlapping copies allowed) or a
+// literal.  Thread 0; every loop is bounded by the expected length.
+__device__ uint32_t lz_decode(const uint8_t* p, uint64_t len, uint64_t expected, uint8_t* out, uint64_t cap) {
+  uint64_t pos = 0, n = 0, o = 0;
+  uint32_t e = rd_varint(p, len, &pos, &n);
+  if (e) return e;
+  if (n != expected || n > cap) return E_CORRUPT;
+  while (o < n) {
+    if (pos >= len) return E_TRUNCATED;
+    uint32_t ctrl = p[pos++];
+    for (int k = 0; k < 8 && o < n; k++) {
+      if ((ctrl >> (7 - k)) & 1u) {
+        uint64_t off, ml;
+        if ((e = rd_varint(p, len, &pos, &off))) return e;
+        if ((e = rd_varint(p, len, &pos, &ml))) return e;
+        ml += 4;
+        if (off == 0 || off > o) return E_CORRUPT;
+        if (ml > n - o) return E_CORRUPT;  // o + ml > n, without wrapping (o <= n)
+        for (uint64_t j = 0; j < ml; j++, o++) out[o] = out[o - off];
+      } else {
+        if (pos >= len) return E_TRUNCATED;
+        out[o++] = p[pos++];
+      }
+    }
+  }
+  return E_OK;
+}
+
+// entropy/mod.rs:152-163: tag 2 rANS, tag 0 the range coder; the legacy tANS
+// tag (decoded by the reference, never produced) is not decoded here.
+__device__ uint32_t entropy_only_cta(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t max_len, uint8_t* out,
+                                     uint64_t cap, uint64_t* len_out) {
   *len_out = 0;
   if (plen == 0) return E_TRUNCATED;
   uint32_t tag = p[0];
   if (tag == 2) return rans_decode_cta(S, p + 1, plen - 1, max_len, out, cap, len_out);
   if (tag == 0) return rc_decode_cta(S, p + 1, plen - 1, max_len, out, cap, len_out);
-  if (tag == 1 || tag == 3) return E_UNSUPPORTED;
+  if (tag == 1) return E_UNSUPPORTED;
   return E_CORRUPT;
+}
+
+// entropy/mod.rs:165-178: tag 3 is the LZ cascade (Max): varint(residual
+// length, at most max_len) ++ an entropy-coded LZ stream of at most twice that
+// + 64 bytes, decoded into the area's cascade scratch, then expanded.
+__device__ uint32_t residuals_cta(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t max_len, uint8_t* out,
+                                 uint64_t cap, uint64_t* len_out) {
+  *len_out = 0;
+  if (plen == 0 || p[0] != 3) return entropy_only_cta(S, p, plen, max_len, out, cap, len_out);
+  uint64_t pos = 1, orig = 0, lzl = 0;
+  uint32_t e = rd_varint(p, plen, &pos, &orig);
+  if (e) return e;
+  if (orig > max_len || orig > cap) return E_CORRUPT;
+  if (!S.lzs || 2 * orig + 64 > S.lzs_cap) return E_NO_ENTROPY_AREA;
+  e = entropy_only_cta(S, p + pos, plen - pos, 2 * orig + 64, S.lzs, S.lzs_cap, &lzl);
+  if (e) return e;
+  e = cta_bcast(S, threadIdx.x == 0 ? lz_decode(S.lzs, lzl, orig, out, cap) : 0u);
+  if (!e) *len_out = orig;
+  return e;
 }
 
 // ---------------------------------------------------------------------------
@@ -1314,14 +1374,6 @@ __device__ uint32_t linear_values(uint32_t mode, const uint8_t* r, uint64_t len,
   return pos == len ? E_OK : E_CORRUPT;
 }
 
-// Thread 0 computes a status, every thread gets it.
-__device__ __forceinline__ uint32_t cta_bcast(DecSmem& S, uint32_t v) {
-  if (threadIdx.x == 0) S.sc[3] = v;
-  __syncthreads();
-  uint32_t r = (uint32_t)S.sc[3];
-  __syncthreads();
-  return r;
-}
 
 // A frame with an entropy-coded part, decoded whole by the CTA into the
 // frame's entropy area (24 bytes per value + 128, then the range coder's
@@ -1334,15 +1386,29 @@ __device__ __noinline__ uint32_t decode_entropy_frame(DecSmem& S, const FrameDes
   uint32_t nsub = (uint32_t)((n + kSub - 1) / kSub);
   uint32_t e = E_OK;
   if (!ent) return E_NO_ENTROPY_AREA;
-  if (t == 0) S.rcm = reinterpret_cast<uint16_t*>(ent + ((24 * n + 128 + 127) & ~127ull));  // 128 KB past the layout
+  if (t == 0) {
+    S.rcm = reinterpret_cast<uint16_t*>(ent + ent_rc_off(n));
+    S.lzs = ent + ent_lz_off(n, d.mode, O.plog2);
+    S.lzs_cap = ent_lz_cap(n);
+  }
   __syncthreads();
   switch (d.mode) {
+    case M_LZ: {  // decoder.rs:172-175: LZ tokens (bound 16n + 1,024) over the block's bytes (lz.rs:165-172)
+      uint8_t* tok = ent;
+      uint64_t* vals = reinterpret_cast<uint64_t*>(ent + ((n * 16 + 1024 + 15) & ~15ull));  // 8n
+      e = residuals_cta(S, p, plen, n * 16 + 1024, tok, n * 16 + 1024, &len);
+      if (e) return e;
+      e = cta_bcast(S, t == 0 ? lz_decode(tok, len, n * 8, reinterpret_cast<uint8_t*>(vals), n * 8) : 0u);
+      if (e) return e;
+      cta_store_staged(S, O, c0, (uint32_t)n, [&](uint32_t q) { return vals[q]; });
+      return E_OK;
+    }
     case M_PRED:
     case M_PRED_RC:
     case M_PRED2: {  // decoder.rs:150-157: PRED's payload is the LEB128 residuals
       uint8_t* res = ent;                                                               // <= 10n + 16 bytes
       uint64_t* vals = reinterpret_cast<uint64_t*>(ent + ((n * 10 + 16 + 15) & ~15ull));  // 8n
-      uint64_t* table = reinterpret_cast<uint64_t*>(ent + ((24 * n + 128 + 127) & ~127ull) + 131072);
+      uint64_t* table = reinterpret_cast<uint64_t*>(ent + ent_table_off(n));
       const uint8_t* r = p;
       len = plen;
       if (d.mode != M_PRED) {

@@ -764,6 +764,7 @@ bool entropy_frame_h(const uint8_t* p, uint64_t plen, uint32_t mode) {
   switch (mode) {
     case 11: case 7: case 20: case 45:  // BYTE_TRANSPOSE; ORDERED_DELTA, DELTA2, DELTA_DP (linear.rs)
     case 0: case 25: case 29:           // PRED, PRED2, PRED_RC (pred.rs; PRED needs only the table)
+    case 4:                             // LZ (lz.rs)
       return true;
     case 17:
       return plen < 2 || p[0] == 1;
@@ -789,8 +790,8 @@ bool entropy_frame_h(const uint8_t* p, uint64_t plen, uint32_t mode) {
 // Warp items of every frame (512 values, or 512 payload bytes for XORZ).
 // Frames the items do not cover, or whose header cannot be read here, go to
 // the frame list; the device walk reports their errors.  Listed frames with
-// an entropy-coded part get a device area of 24 bytes per value + 128, then
-// 128 KB for the range coder's model
+// an entropy-coded part get a device area (ent_area_bytes: the mode's layout,
+// the range coder's model, a predictor table, the LZ cascade's scratch)
 // (128-byte units, 1 + its offset in FrameDesc::aux; 0 = none).
 void build_items(const uint8_t* src, LaneIdx& L) {
   const uint32_t V = 512, B = 512;
@@ -861,8 +862,7 @@ void build_items(const uint8_t* src, LaneIdx& L) {
     FrameDesc& d = L.frames[f];
     if (!entropy_frame_h(src + d.payload_off, d.plen, d.mode)) continue;
     d.aux = (uint32_t)(1 + L.ent_bytes / 128);
-    L.ent_bytes += ((24ull * d.n + 128 + 127) & ~127ull) + 131072;  // + the range coder's model
-    if (d.mode == 0 || d.mode == 25 || d.mode == 29) L.ent_bytes += 8ull << L.plog2;  // + the predictor table
+    L.ent_bytes += ent_area_bytes(d.n, d.mode, L.plog2);
   }
 }
 

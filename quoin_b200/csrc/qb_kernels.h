@@ -9,6 +9,22 @@
 namespace qb {
 
 // ---- decoder (qb_decode.cu) ----
+// The entropy area of a listed frame of n values (128-byte aligned pieces):
+// the mode's own layout (24 bytes per value + 1,152), the range coder's
+// 256 x 256 model (128 KB), the FCM / DFCM table of PRED, PRED_RC and PRED2
+// (8 << predictor_log2 bytes), and the LZ cascade's scratch for an inner LZ
+// stream of up to twice the largest residual bound (16n + 1,024) + 64.
+__host__ __device__ inline uint64_t ent_rc_off(uint64_t n) { return (24 * n + 1152 + 127) & ~127ull; }
+__host__ __device__ inline bool ent_has_table(uint32_t mode) { return mode == 0 || mode == 25 || mode == 29; }
+__host__ __device__ inline uint64_t ent_table_off(uint64_t n) { return ent_rc_off(n) + 131072; }
+__host__ __device__ inline uint64_t ent_lz_off(uint64_t n, uint32_t mode, uint32_t plog2) {
+  return ent_table_off(n) + (ent_has_table(mode) ? (8ull << plog2) : 0);
+}
+__host__ __device__ inline uint64_t ent_lz_cap(uint64_t n) { return 32 * n + 2112; }
+__host__ __device__ inline uint64_t ent_area_bytes(uint64_t n, uint32_t mode, uint32_t plog2) {
+  return ent_lz_off(n, mode, plog2) + ((ent_lz_cap(n) + 127) & ~127ull);
+}
+
 // Walk (validation + sub-block offsets) and decode of nf frames.  `aux` is
 // device scratch of decode_aux_bytes(nf) bytes.
 uint64_t decode_aux_bytes(int nf);

@@ -2,7 +2,8 @@
 from src/codecs/linear.rs, PRED (0), PRED_RC (29) and PRED2 (25) from
 src/codecs/pred.rs with the CRC32C predictor hash (src/hash.rs), with residual
 bytes coded by the range coder (src/entropy/rc.rs, tag 0) or rANS (tag 2), and
-the range coder inside other entropy-coded parts.  The oracle restates the encoders and decoders (its CPU
+the range coder inside other entropy-coded parts; LZ (4) and the Max LZ cascade
+(entropy tag 3) from src/codecs/lz.rs.  The oracle restates the encoders and decoders (its CPU
 checks port the reference's tests: rc.rs roundtrip_random_bytes /
 roundtrip_skewed_bytes / empty, linear.rs float_delta_roundtrips_all_orders /
 idelta2_roundtrips / select_order_prefers_high_on_smooth_low_on_noise); the
@@ -199,3 +200,77 @@ def test_predictor_modes_decode_like_the_oracle(qb, oracle):
         for bad in (good + b"\x00", good[:-5], b"\x05" + good[1:], b""):
             kinds.append(_agree(qb, oracle, stream([(mode, len(v), bad)], U64)))
     assert "CorruptPayload" in kinds and "Truncated" in kinds
+
+
+M_LZ, TAG_LZ = 4, 3
+
+
+def _varint_bytes(v):
+    out = bytearray()
+    while True:
+        b = v & 0x7F
+        v >>= 7
+        if v:
+            out.append(b | 0x80)
+        else:
+            out.append(b)
+            return bytes(out)
+
+
+def _coded(oracle, data, tag):
+    return bytes([tag]) + (oracle.rc_compress(data) if tag == TAG_RC else oracle.rans_compress(data))
+
+
+def _cascade(oracle, res, tag):
+    """entropy/mod.rs:124-146: the Max LZ cascade around residual bytes."""
+    return bytes([TAG_LZ]) + _varint_bytes(len(res)) + _coded(oracle, oracle.lz_compress(res), tag)
+
+
+def test_oracle_lz_round_trips(oracle):
+    # lz.rs tests roundtrip_repetitive / roundtrip_random_and_edges
+    rep = np.array([float(i & 15) for i in range(50000)]).view(np.uint64)
+    enc = oracle.lz_compress(rep.tobytes())
+    assert len(enc) < rep.nbytes // 4 and oracle.lz_decompress(enc, rep.nbytes) == rep.tobytes()
+    rnd = lcg_seq(1, 5000).tobytes()
+    assert oracle.lz_decompress(oracle.lz_compress(rnd), len(rnd)) == rnd
+    assert oracle.lz_decompress(oracle.lz_compress(b""), 0) == b""
+    one = np.array([42], np.uint64).tobytes()
+    assert oracle.lz_decompress(oracle.lz_compress(one), 8) == one
+
+
+@pytest.mark.gpu
+def test_lz_mode_and_cascade_decode_like_the_oracle(qb, oracle):
+    lv = lanes()
+    lv["dict16"] = np.array([float(i & 15) for i in range(20000)]).view(np.uint64)
+    lv["repeats"] = np.tile(lcg_seq(9, 37), 600)[:20000]
+    for name, v in lv.items():
+        for tag in (TAG_RC, TAG_RANS):
+            frames = [(M_LZ, hi - lo, _coded(oracle, oracle.lz_compress(v[lo:hi].tobytes()), tag))
+                      for lo, hi in ((0, 1), (1, 4097), (4097, 20000))]
+            s = stream(frames, U64)
+            assert _agree(qb, oracle, s) == "ok", (name, tag)
+            assert np.ascontiguousarray(qb.decompress_column(s).values).view(np.uint64).tobytes() == v.tobytes()
+    # the cascade around DELTA2, PRED2 and BYTE_TRANSPOSE residuals
+    v = lv["repeats"][:8000]
+    for mode, tag in ((M_D2, TAG_RC), (M_PRED2, TAG_RANS), (M_BT, TAG_RC)):
+        if mode == M_D2:
+            res = oracle.rc_decompress(oracle.linear_payload(M_D2, v, 2, TAG_RC)[1:], 10 * len(v) + 16)
+        elif mode == M_PRED2:
+            res = oracle.rc_decompress(oracle.pred_payload(M_PRED2, v, 16, TAG_RC)[1:], 10 * len(v) + 16)
+        else:
+            res = np.ascontiguousarray(v).view(np.uint8).reshape(-1, 8).T.copy().tobytes()
+        s = stream([(mode, len(v), _cascade(oracle, res, tag))], U64)
+        assert _agree(qb, oracle, s) == "ok", mode
+        assert np.ascontiguousarray(qb.decompress_column(s).values).view(np.uint64).tobytes() == v.tobytes()
+    # damage inside the LZ stream: bad offset, overrun, wrong length, cuts; cascade length above the bound
+    good = oracle.lz_compress(lv["dict16"][:4096].tobytes())
+    kinds = []
+    variants = [good[:len(good) // 2], good[:-1], _varint_bytes(4096 * 8 + 8) + good[len(_varint_bytes(4096 * 8)):]]
+    b = bytearray(good)
+    b[len(_varint_bytes(4096 * 8)) + 9:len(_varint_bytes(4096 * 8)) + 10] = b"\x7f"  # an offset byte of the first match
+    variants.append(bytes(b))
+    for bad in variants:
+        kinds.append(_agree(qb, oracle, stream([(M_LZ, 4096, _coded(oracle, bad, TAG_RANS))], U64)))
+    huge = bytes([TAG_LZ]) + _varint_bytes(10 ** 9) + _coded(oracle, good, TAG_RC)
+    kinds.append(_agree(qb, oracle, stream([(M_D2, 4096, huge)], U64)))
+    assert kinds[-1] == "CorruptPayload" and "Truncated" in kinds and "CorruptPayload" in kinds[:-1]
