@@ -211,6 +211,9 @@ void quoin_b200_index_free(QuoinDecodeIndex *idx);
 /* n and wire dtype of an indexed stream. */
 int quoin_b200_index_info(const QuoinDecodeIndex *idx, int32_t *wire_dtype, uint64_t *n,
                           int32_t *has_validity);
+/* Decimal scale and precision (0 for other dtypes) and the number of valid values. */
+int quoin_b200_index_decimal(const QuoinDecodeIndex *idx, int8_t *scale, uint8_t *precision,
+                             uint64_t *n_valid);
 /* Decode the device copy d_src of the indexed stream into d_values_out (and
  * d_validity_out when non-NULL and the stream has a bitmap). */
 int quoin_b200_decompress_indexed_device(QuoinCtx *ctx, const QuoinDecodeIndex *idx,
@@ -397,6 +400,47 @@ int quoin_b200_compress_arrow(QuoinCtx *ctx, const struct ArrowSchema *schema,
  * caller owns both and frees them through their release callbacks. */
 int quoin_b200_decompress_arrow(QuoinCtx *ctx, const uint8_t *src, size_t src_len,
                                 struct ArrowSchema *schema_out, struct ArrowArray *array_out);
+
+/* ---------------- Arrow C Device Data Interface ---------------- */
+
+/* The standard device-array struct (declared here unless the caller's Arrow
+ * headers already did). */
+#ifndef ARROW_C_DEVICE_DATA_INTERFACE
+#define ARROW_C_DEVICE_DATA_INTERFACE
+typedef int32_t ArrowDeviceType;
+#define ARROW_DEVICE_CPU 1
+#define ARROW_DEVICE_CUDA 2
+#define ARROW_DEVICE_CUDA_HOST 3
+#define ARROW_DEVICE_CUDA_MANAGED 13
+struct ArrowDeviceArray {
+    struct ArrowArray array;
+    int64_t device_id;
+    ArrowDeviceType device_type;
+    void *sync_event; /* for CUDA: a cudaEvent_t* to wait on before reading, or NULL */
+    int64_t reserved[3];
+};
+#endif
+typedef struct ArrowDeviceArray ArrowDeviceArray;
+
+/* Zero-copy compress of a device-resident Arrow array (device_type CUDA or
+ * CUDA_MANAGED, on the context's device): the values buffer (and validity
+ * bitmap) are read in place on `stream` (a cudaStream_t; NULL = the context's
+ * stream) after its sync_event; a bitmap whose offset is not a multiple of 8
+ * is re-packed on the device.  d_dst / out_len as in
+ * quoin_b200_compress_column_device.  Types and errors as
+ * quoin_b200_compress_arrow; QUOIN_ERR_BAD_ARG for a host device_type. */
+int quoin_b200_compress_arrow_device(QuoinCtx *ctx, const struct ArrowSchema *schema,
+                                     const struct ArrowDeviceArray *array, const QuoinConfig *cfg,
+                                     uint8_t *d_dst, size_t dst_cap, size_t *out_len, void *stream);
+
+/* Decodes the indexed stream (device copy d_src) into a new device-resident
+ * Arrow array (device_type CUDA, the context's device, sync_event NULL: the
+ * data is ready when the call returns); the caller owns *schema_out and
+ * *array_out and frees them (and the device buffers) through their release
+ * callbacks. */
+int quoin_b200_decompress_arrow_device(QuoinCtx *ctx, const QuoinDecodeIndex *idx, const uint8_t *d_src,
+                                       struct ArrowSchema *schema_out, struct ArrowDeviceArray *array_out,
+                                       void *stream);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -12,7 +12,10 @@
 #include <cstring>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "../../include/quoin.h"
+#include "qb_kernels.h"
 
 namespace {
 
@@ -191,6 +194,151 @@ extern "C" int quoin_b200_decompress_arrow(QuoinCtx* ctx, const uint8_t* src, si
     array_out->buffers = ap->buffers;
     array_out->release = release_array;
     array_out->private_data = ap;
+    return QUOIN_OK;
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Arrow C Device Data Interface: device-resident arrays, read and written in
+// place (no host copy of the values).
+// ---------------------------------------------------------------------------
+namespace {
+
+// The Arrow format of a stream's wire dtype (and decimal scale / precision).
+bool format_of(int32_t wire, int8_t scale, uint8_t precision, char* out, size_t cap, uint32_t* width) {
+  switch (wire) {
+    case QUOIN_WIRE_F64: snprintf(out, cap, "g"); *width = 8; return true;
+    case QUOIN_WIRE_F32: snprintf(out, cap, "f"); *width = 4; return true;
+    case QUOIN_WIRE_I64: snprintf(out, cap, "l"); *width = 8; return true;
+    case QUOIN_WIRE_U64: snprintf(out, cap, "L"); *width = 8; return true;
+    case QUOIN_WIRE_I32: snprintf(out, cap, "i"); *width = 4; return true;
+    case QUOIN_WIRE_U32: snprintf(out, cap, "I"); *width = 4; return true;
+    case QUOIN_WIRE_DECIMAL128: snprintf(out, cap, "d:%d,%d", precision, scale); *width = 16; return true;
+    case QUOIN_WIRE_DECIMAL256: snprintf(out, cap, "d:%d,%d,256", precision, scale); *width = 32; return true;
+    default: return false;
+  }
+}
+
+struct DeviceArrayPrivate {
+  void* values;
+  uint8_t* validity;
+  const void* buffers[2];
+};
+
+void release_device_array(ArrowArray* a) {
+  if (!a || !a->release) return;
+  DeviceArrayPrivate* p = static_cast<DeviceArrayPrivate*>(a->private_data);
+  cudaFree(p->values);
+  if (p->validity) cudaFree(p->validity);
+  delete p;
+  a->release = nullptr;
+}
+
+}  // namespace
+
+extern "C" int quoin_b200_compress_arrow_device(QuoinCtx* ctx, const ArrowSchema* schema, const ArrowDeviceArray* darr,
+                                                const QuoinConfig* cfg, uint8_t* d_dst, size_t dst_cap,
+                                                size_t* out_len, void* stream) {
+  if (!schema || !darr || !d_dst || !out_len) return QUOIN_ERR_NULL;
+  try {
+    ArrowType t;
+    if (!arrow_type(schema->format, &t) || schema->n_children != 0 || schema->dictionary) {
+      return QUOIN_ERR_UNSUPPORTED_ARROW_TYPE;
+    }
+    if (darr->device_type != ARROW_DEVICE_CUDA && darr->device_type != ARROW_DEVICE_CUDA_MANAGED) {
+      return QUOIN_ERR_BAD_ARG;
+    }
+    const ArrowArray* a = &darr->array;
+    if (a->length < 0 || a->offset < 0 || a->n_buffers < 2) return QUOIN_ERR_BAD_ARG;
+    uint64_t n = (uint64_t)a->length, off = (uint64_t)a->offset;
+    const uint8_t* base = static_cast<const uint8_t*>(a->buffers[1]);
+    if (!base && n) return QUOIN_ERR_NULL;
+    cudaStream_t st = qb::ctx_stream(ctx, stream);
+    if (darr->sync_event && cudaStreamWaitEvent(st, *static_cast<cudaEvent_t*>(darr->sync_event), 0) != cudaSuccess) {
+      cudaGetLastError();
+      return QUOIN_ERR_CUDA;
+    }
+    const uint8_t* values = base ? base + off * t.width : nullptr;
+    const uint8_t* src_bm = static_cast<const uint8_t*>(a->buffers[0]);
+    uint8_t* bm = nullptr;
+    if (src_bm && a->null_count != 0 && n) {  // re-packed from the array's offset, trailing bits clear
+      if (cudaMallocAsync(reinterpret_cast<void**>(&bm), (n + 7) / 8, st) != cudaSuccess) {
+        cudaGetLastError();
+        return QUOIN_ERR_CUDA;
+      }
+      qb::launch_bitmap_repack(src_bm, off, n, bm, st);
+    }
+    int rc = quoin_b200_compress_column_device(ctx, t.wire, n, values, bm, (int8_t)t.scale, (uint8_t)t.precision, cfg,
+                                               d_dst, dst_cap, out_len, st);
+    if (bm) cudaFreeAsync(bm, st);
+    return rc;
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+extern "C" int quoin_b200_decompress_arrow_device(QuoinCtx* ctx, const QuoinDecodeIndex* idx, const uint8_t* d_src,
+                                                  ArrowSchema* schema_out, ArrowDeviceArray* out, void* stream) {
+  if (!idx || !d_src || !schema_out || !out) return QUOIN_ERR_NULL;
+  try {
+    int32_t wire = 0, hv = 0;
+    uint64_t n = 0, n_valid = 0;
+    int8_t scale = 0;
+    uint8_t precision = 0;
+    int rc = quoin_b200_index_info(idx, &wire, &n, &hv);
+    if (!rc) rc = quoin_b200_index_decimal(idx, &scale, &precision, &n_valid);
+    if (rc) return rc;
+    SchemaPrivate* sp = new SchemaPrivate();
+    uint32_t width = 0;
+    if (!format_of(wire, scale, precision, sp->format, sizeof sp->format, &width)) {
+      delete sp;
+      return QUOIN_ERR_UNSUPPORTED_DTYPE;
+    }
+    // 64-byte aligned device buffers, as Arrow recommends (cudaMalloc aligns to 256)
+    void* values = nullptr;
+    uint8_t* validity = nullptr;
+    size_t vbytes = (size_t)n * width;
+    if (cudaMalloc(&values, vbytes ? vbytes : 64) != cudaSuccess ||
+        (hv && cudaMalloc(reinterpret_cast<void**>(&validity), (n + 7) / 8 ? (n + 7) / 8 : 64) != cudaSuccess)) {
+      cudaGetLastError();
+      cudaFree(values);
+      delete sp;
+      return QUOIN_ERR_CUDA;
+    }
+    rc = quoin_b200_decompress_indexed_device(ctx, idx, d_src, values, validity, stream);
+    if (rc) {
+      cudaFree(values);
+      if (validity) cudaFree(validity);
+      delete sp;
+      return rc;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    DeviceArrayPrivate* ap = new DeviceArrayPrivate();
+    ap->values = values;
+    ap->validity = validity;
+    ap->buffers[0] = validity;
+    ap->buffers[1] = values;
+
+    memset(schema_out, 0, sizeof *schema_out);
+    schema_out->format = sp->format;
+    schema_out->name = "";
+    schema_out->flags = ARROW_FLAG_NULLABLE;
+    schema_out->release = release_schema;
+    schema_out->private_data = sp;
+
+    memset(out, 0, sizeof *out);
+    out->array.length = (int64_t)n;
+    out->array.null_count = hv ? (int64_t)(n - n_valid) : 0;
+    out->array.n_buffers = 2;
+    out->array.buffers = ap->buffers;
+    out->array.release = release_device_array;
+    out->array.private_data = ap;
+    out->device_id = dev;
+    out->device_type = ARROW_DEVICE_CUDA;
+    out->sync_event = nullptr;  // the call returned after the decode completed
     return QUOIN_OK;
   } catch (...) {
     return QUOIN_ERR_PANIC;

@@ -889,6 +889,12 @@ uint64_t layout_items(std::vector<LaneIdx>& lanes) {
 
 }  // namespace
 
+cudaStream_t qb::ctx_stream(QuoinCtx* c, void* stream) {
+  if (stream) return static_cast<cudaStream_t>(stream);
+  QuoinCtx* x = pick(c);
+  return x ? x->stream : nullptr;
+}
+
 struct QuoinDecodeIndex {
   int wire = 0;
   uint64_t n = 0;
@@ -1667,6 +1673,14 @@ void quoin_b200_index_free(QuoinDecodeIndex* X) {
     if (X->d_vmin) cudaFree(X->d_vmin);
   }
   delete X;
+}
+
+int quoin_b200_index_decimal(const QuoinDecodeIndex* X, int8_t* scale, uint8_t* precision, uint64_t* n_valid) {
+  if (!X || !scale || !precision || !n_valid) return QUOIN_ERR_NULL;
+  *scale = X->scale;
+  *precision = X->precision;
+  *n_valid = X->has_validity ? X->n_valid : X->n;
+  return QUOIN_OK;
 }
 
 int quoin_b200_index_info(const QuoinDecodeIndex* X, int32_t* wire, uint64_t* n, int32_t* has_validity) {

@@ -6,6 +6,8 @@
 
 #include "qb_layout.h"
 
+struct QuoinCtx;
+
 namespace qb {
 
 // ---- decoder (qb_decode.cu) ----
@@ -133,6 +135,11 @@ void launch_validity_blob(const uint8_t* bm, uint64_t n, uint64_t* tmp, uint64_t
 uint64_t validity_tmp_words(uint64_t n);
 // Adds the bitmap's bit-transition count to *count (zero it first).
 void launch_bitmap_transitions(const uint8_t* bm, uint64_t n, unsigned long long* count, cudaStream_t st);
+// The stream a call on context c runs on: `stream` when given, else the
+// context's own (the default context when c is null).
+cudaStream_t ctx_stream(struct ::QuoinCtx* c, void* stream);
+// Bits [bit_off, bit_off + n) of src re-packed into dst from bit 0 (ceil(n/8) bytes, trailing bits clear).
+void launch_bitmap_repack(const uint8_t* src, uint64_t bit_off, uint64_t n, uint8_t* dst, cudaStream_t st);
 // Writes varint(len) + the RAW validity blob of an n-bit bitmap at dst and the
 // stream offset after it (dst_off + its length) to *d_base.
 void launch_put_validity_raw(uint8_t* dst, uint64_t dst_off, const uint8_t* bm, uint64_t n, uint64_t* d_base,

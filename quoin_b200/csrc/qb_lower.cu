@@ -302,6 +302,31 @@ __global__ void k_bitmap_transitions(const uint8_t* __restrict__ bm, uint64_t n,
     if (t) atomicAdd(count, t);
   }
 }
+// Bits [bit_off, bit_off + n) of a validity bitmap (LSB first) re-packed from
+// bit 0, trailing bits of the last byte cleared (the Arrow slice re-pack of
+// arrow.rs:29-52, on the device).  The source holds ceil((bit_off + n) / 8)
+// bytes; nothing past them is read.
+__global__ void k_bitmap_repack(const uint8_t* __restrict__ src, uint64_t bit_off, uint64_t n,
+                                uint8_t* __restrict__ dst) {
+  uint64_t nb = (n + 7) / 8, src_bytes = (bit_off + n + 7) / 8;
+  uint32_t sh = (uint32_t)(bit_off & 7);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nb; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t s0 = (bit_off >> 3) + i;
+    uint32_t v = src[s0] >> sh;
+    if (sh && s0 + 1 < src_bytes) v |= (uint32_t)src[s0 + 1] << (8 - sh);
+    if (i == nb - 1 && (n & 7)) v &= (1u << (n & 7)) - 1u;
+    dst[i] = (uint8_t)v;
+  }
+}
+
+void launch_bitmap_repack(const uint8_t* src, uint64_t bit_off, uint64_t n, uint8_t* dst, cudaStream_t st) {
+  uint64_t nb = (n + 7) / 8;
+  if (!nb) return;
+  unsigned g = (unsigned)((nb + 255) / 256 < 4096 ? (nb + 255) / 256 : 4096);
+  k_bitmap_repack<<<g, 256, 0, st>>>(src, bit_off, n, dst);
+  count_launches(1);
+}
+
 void launch_bitmap_transitions(const uint8_t* bm, uint64_t n, unsigned long long* count, cudaStream_t st) {
   uint64_t nw = (n + 31) / 32;
   unsigned g = (unsigned)qmin((nw + 255) / 256, 148ull * 8);
