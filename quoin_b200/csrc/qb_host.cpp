@@ -207,26 +207,37 @@ struct QuoinCtx {
   QuoinDecodeIndex* hidx = nullptr;  // host-side parsed index reused by the host-buffer decodes
   uint64_t* hbox = nullptr;          // 512 B of pinned host memory for the small device -> host reads
 
+  // Grows slot s to at least `bytes` (contents not kept).  The outgrown
+  // buffer is retired, not freed: cudaFree waits for the whole device, which
+  // would stall every other context's work (batches, the server); retired
+  // buffers are freed when the context is, or when an allocation fails.
+  // Growth at least doubles, so a slot's retired buffers stay below its size.
   cudaError_t ensure(int s, size_t bytes) {
     if (bytes == 0) bytes = 16;
     bytes = (bytes + 255) & ~(size_t)255;
     if (cap[s] >= bytes) return cudaSuccess;
-    if (buf[s]) {
-      cudaStreamSynchronize(stream);
-      cudaFree(buf[s]);
-      buf[s] = nullptr;
-      cap[s] = 0;
-    }
+    if (buf[s]) retired.push_back(buf[s]);
+    buf[s] = nullptr;
     size_t want = bytes + bytes / 4;
+    if (cap[s] && want < 2 * cap[s]) want = 2 * cap[s];
+    cap[s] = 0;
     cudaError_t e = cudaMalloc(&buf[s], want);
-    if (e != cudaSuccess) {
+    if (e != cudaSuccess) {  // free what was retired (after the device's work) and try the exact size
       cudaGetLastError();
+      free_retired();
       e = cudaMalloc(&buf[s], bytes);
       want = bytes;
     }
     if (e == cudaSuccess) cap[s] = want; else cudaGetLastError();
     return e;
   }
+  void free_retired() {
+    if (retired.empty()) return;
+    cudaDeviceSynchronize();
+    for (void* p : retired) cudaFree(p);
+    retired.clear();
+  }
+  std::vector<void*> retired;
   template <class T>
   T* p(int s) { return reinterpret_cast<T*>(buf[s]); }
 };
@@ -1373,6 +1384,8 @@ void quoin_ctx_free(QuoinCtx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (int s = 0; s < S_COUNT; s++)
       if (ctx->buf[s]) cudaFree(ctx->buf[s]);
+    for (void* p : ctx->retired) cudaFree(p);
+    ctx->retired.clear();
     cudaStreamDestroy(ctx->stream);
     if (ctx->hbox) cudaFreeHost(ctx->hbox);
   }
