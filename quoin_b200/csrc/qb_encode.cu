@@ -361,6 +361,8 @@ struct AlpSub {
   uint32_t w, exc;
   int64_t mn, filler;
 };
+__device__ bool alp_subblock_ef(const uint64_t* sv, uint32_t cnt, int e, int f, const double* pexp,
+                                const double* pfrac, AlpSub* out);
 __device__ bool alp_subblock(const uint64_t* sv, uint32_t cnt, uint64_t* smp, const double* pexp, const double* pfrac,
                              AlpSub* out) {
   int lane = threadIdx.x & 31;
@@ -409,6 +411,16 @@ __device__ bool alp_subblock(const uint64_t* sv, uint32_t cnt, uint64_t* smp, co
   if (best_exc * 2 > sl) return false;
   int e, f;
   alp_combo(best_c, &e, &f);
+  return alp_subblock_ef(sv, cnt, e, f, pexp, pfrac, out);
+}
+
+// The encode pass of one sub-block for a chosen (e, f) (alp.rs:109-166):
+// exceptions, digit range, the filler digit.  Warp-cooperative; false when
+// the digits need more than 32 bits.
+__device__ bool alp_subblock_ef(const uint64_t* sv, uint32_t cnt, int e, int f, const double* pexp,
+                                const double* pfrac, AlpSub* out) {
+  int lane = threadIdx.x & 31;
+  const double kInf = __longlong_as_double(0x7FF0000000000000ll);
   const double pe = pexp[e], pf = pfrac[f], qf = pexp[f], qe = pfrac[e];
   uint32_t exc = 0, first_li = 0xFFFFFFFFu;
   double rmn = kInf, rmx = -kInf, first_r = 0.0;
@@ -1429,6 +1441,7 @@ __device__ inline uint32_t sub_range(uint64_t item, uint64_t n, uint64_t fixed_b
 // completes).  The power-of-ten tables are copied to shared memory, since the
 // (e, f) search reads them at a different index in every lane.
 constexpr int kAlpWarps = 8;
+constexpr uint16_t kAlpEfKnown = 0x8000;  // SubStats::pad16 holds e | f << 8 of a sub-block that passed
 __global__ void __launch_bounds__(kAlpWarps * 32) k_alp_stats(const uint64_t* __restrict__ v, uint64_t n,
                                                               uint64_t fixed_bs, uint64_t items,
                                                               SubStats* __restrict__ ss) {
@@ -1451,6 +1464,7 @@ __global__ void __launch_bounds__(kAlpWarps * 32) k_alp_stats(const uint64_t* __
     ss[item].alp_ok = ok ? 1 : 0;
     ss[item].alp_w = ok ? (uint8_t)a.w : 0;
     ss[item].alp_exc = ok ? (uint16_t)a.exc : 0;
+    ss[item].pad16 = ok ? (uint16_t)(kAlpEfKnown | a.e | (a.f << 8)) : 0;  // the emitter reuses (e, f)
   }
 }
 
@@ -2353,7 +2367,7 @@ __device__ void emit_xorz(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* ou
   }
 }
 
-__device__ void emit_alp(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* out) {
+__device__ void emit_alp(EncSmem& S, const uint64_t* v, uint32_t n, const SubStats* ss, uint8_t* out) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t nsub = (n + kSub - 1) / kSub;
   __shared__ int64_t s_fill[kSubsMax];
@@ -2366,7 +2380,14 @@ __device__ void emit_alp(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* out
   for (uint32_t k = warp; k < nsub; k += kEncWarps) {
     uint32_t cnt = min((uint32_t)kSub, n - k * kSub);
     AlpSub a;
-    alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], s_pexp, s_pfrac, &a);  // succeeded in the competition
+    uint16_t ef = ss ? ss[k].pad16 : 0;  // the statistics' (e, f), or search again (Sample at Fastest)
+    if (ef & kAlpEfKnown) {
+      a.e = ef & 0xFF;
+      a.f = (ef >> 8) & 0x7F;
+      alp_subblock_ef(v + (uint64_t)k * kSub, cnt, a.e, a.f, s_pexp, s_pfrac, &a);
+    } else {
+      alp_subblock(v + (uint64_t)k * kSub, cnt, S.alp_smp[warp], s_pexp, s_pfrac, &a);  // succeeded in the competition
+    }
     if (lane == 0) {
       S.alp_ef[k][0] = (uint8_t)a.e;
       S.alp_ef[k][1] = (uint8_t)a.f;
@@ -2717,7 +2738,7 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
           return (uint32_t)(v[i - pl * n] >> (8 * pl)) & 255u;
         }, out, fd.plen);
       break;
-    case M_ALP: emit_alp(S, v, n, out); break;
+    case M_ALP: emit_alp(S, v, n, ss ? ss + g0 : nullptr, out); break;
     case M_ALP_RD: emit_alprd(S, v, n, fd.aux, scr, out, erp); break;
     case M_DICT: emit_dict(S, v, n, scr, out, erp); break;
     case M_RLE: emit_rle(S, v, n, scr, out); break;
