@@ -18,9 +18,11 @@ compressed at Level::Fast (the byte-identical level) and decompressed again.
 C restatement in oracle/, since the Rust reference cannot be built here) on
 all host cores, on a bounded sample of the same columns.
 
-`--workload config2` runs the float-lane columns (f64 random walk, f32
-sensor readings, Decimal128) the same way; `--workload config3` compares
-plain per-column calls with the batch calls on many uneven columns.
+`--workload float-lanes` runs the float-lane columns (f64 random walk, f32
+sensor readings, Decimal128) the same way; `--workload batched` compares
+plain per-column calls with the batch calls on many uneven columns, and
+`--workload served` drives the request server with an open-loop request
+stream.
 
 Run: python bench.py [--gpus N --steps K --warmup W] (torchrun for N > 1).
 """
@@ -48,9 +50,9 @@ TIMER_NAMES = ["compete", "emit", "decode", "finalize", "lower", "plan", "validi
 
 # Single-column workloads: (synth config, description, arithmetic types).
 WORKLOADS = {
-    "config1": ("1", "config1 integer lanes: i64 timestamps (1e6+Poisson(5000) steps), u64 base+U[0,2^k) runs, "
+    "integer-lanes": ("integer", "integer lanes: i64 timestamps (1e6+Poisson(5000) steps), u64 base+U[0,2^k) runs, "
                      "i32 Zipf(1.1) 64-category geometric runs; 10% nulls; Level::Fast", "int64/uint64/int32"),
-    "config2": ("2", "config2 float lanes: f64 random walk x+N(0,1e-3) from 20.0 at full precision, f32 "
+    "float-lanes": ("float", "float lanes: f64 random walk x+N(0,1e-3) from 20.0 at full precision, f32 "
                      "round(N(25,5)*10)/10, Decimal128(18,4) uniform in [-1e14,1e14); no nulls; Level::Fast",
                 "f64/f32/decimal128"),
 }
@@ -175,18 +177,18 @@ def run_reference(args, rank, world):
     from quoin_b200 import synth
     threads = os.cpu_count() or 1
     sample = args.cpu_sample
-    if args.workload in ("config3", "config4"):  # the columns, each cut to an equal share of the sample
-        cols = (synth.config3_columns(args.columns, args.max_len) if args.workload == "config3"
-                else synth.config4_columns(args.columns4, args.max_bytes))
+    if args.workload in ("batched", "served"):  # the columns, each cut to an equal share of the sample
+        cols = (synth.mixed_columns(args.columns, args.max_len) if args.workload == "batched"
+                else synth.request_columns(args.columns4, args.max_bytes))
         share = max(sample // len(cols), 1)
         cols = [(nm, dt, v[:share], None if bm is None else bm[: (min(len(v), share) + 7) // 8])
                 for nm, dt, v, bm in cols]
-        wl = (args.workload[-1], f"{args.workload}: {len(cols)} columns of the configuration, each cut to its "
+        wl = (args.workload, f"{args.workload}: {len(cols)} columns of the workload, each cut to its "
                                  f"first {share} values; compress then decompress each; Level::Fast",
               "mixed (f64/f32/i64/u64/i32/u32/decimal128)")
     else:
         wl = WORKLOADS[args.workload]
-        cols = synth.config_columns(wl[0], sample)
+        cols = synth.benchmark_columns(wl[0], sample)
     for _ in range(args.warmup):
         cpu_reference_run(cols, threads, sample)
     tot_b = 0
@@ -233,7 +235,7 @@ def run_gpu(args, rank, world, local):
     dev = torch.device("cuda", local)
     n = args.n
     wl = WORKLOADS[args.workload]
-    cols = synth.config_columns(wl[0], n)
+    cols = synth.benchmark_columns(wl[0], n)
     L = Q.lib
     # One context (CUDA stream + device arenas) and one host thread per column:
     # the columns' kernels overlap on the GPU, filling each other's tails.
@@ -543,11 +545,11 @@ def run_gpu(args, rank, world, local):
 
 
 # ---------------------------------------------------------------------------
-# Batched configuration (--workload config3): many columns of uneven length
+# Batched columns (--workload batched): many columns of uneven length
 # and mixed dtype, plain per-column calls on one context vs batch calls over
 # a pool of contexts (quoin_b200_*_batch_device).
 # ---------------------------------------------------------------------------
-def run_gpu_config3(args, rank, world, local):
+def run_gpu_batched(args, rank, world, local):
     import torch
     import torch.distributed as dist
     import quoin_b200 as Q
@@ -577,7 +579,7 @@ def run_gpu_config3(args, rank, world, local):
                                                    ctypes.POINTER(Q._QuoinConfig)]
     L.quoin_b200_decompress_batch_device.argtypes = [P, ctypes.POINTER(DecompressJob), S]
     cfg = Q._QuoinConfig(int(Q.Level.FAST), 0, 16, 0)
-    cols = synth.config3_columns(args.columns, args.max_len)
+    cols = synth.mixed_columns(args.columns, args.max_len)
     ctx = P(L.quoin_ctx_create(0))
     batch = P(L.quoin_b200_batch_create(args.workers))
     raw_bytes = 0
@@ -677,7 +679,7 @@ def run_gpu_config3(args, rank, world, local):
             "warmup": args.warmup, "ms_per_step": round(batched_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "mixed (f64/f32/i64/u64/i32/u32/decimal128)",
             "data": "synthetic",
-            "config": {"workload": f"config3: {len(gc)} columns, lengths floor(exp(U[ln 1024, ln {args.max_len}])), "
+            "config": {"workload": f"batched: {len(gc)} columns, lengths floor(exp(U[ln 1024, ln {args.max_len}])), "
                                    "dtype uniform over 7, null rate U(0,0.2); Level::Fast",
                        "columns": len(gc), "global_values": int(sum(c["n"] for c in gc)) * world,
                        "uncompressed_bytes": raw_bytes, "workers": args.workers,
@@ -695,13 +697,13 @@ def run_gpu_config3(args, rank, world, local):
 
 
 # ---------------------------------------------------------------------------
-# Serving configuration (--workload config4): an open-loop Poisson request
+# Served requests (--workload served): an open-loop Poisson request
 # stream (70% decompress, 30% compress) over resident columns, served by the
 # request server (a pool of contexts, FIFO admission against a 120 GB device
 # budget) and by the plain per-request path (one context, one request at a
 # time), at offered loads from 10% to 100% of the server's measured peak.
 # ---------------------------------------------------------------------------
-def run_gpu_config4(args, rank, world, local):
+def run_gpu_served(args, rank, world, local):
     import torch
     import torch.distributed as dist
     import quoin_b200 as Q
@@ -735,7 +737,7 @@ def run_gpu_config4(args, rank, world, local):
     # Resident columns: values, a compressed copy (source of the decompress
     # requests) with its decode index, and output buffers.  Concurrent requests
     # on one column write the same bytes to its shared outputs.
-    cols = synth.config4_columns(args.columns4, args.max_bytes)
+    cols = synth.request_columns(args.columns4, args.max_bytes)
     ctx = P(L.quoin_ctx_create(0))
     tpl = []
     resident = 0
@@ -843,8 +845,9 @@ def run_gpu_config4(args, rank, world, local):
             "value": top["server"]["gbs"], "unit": "GB/s", "n_gpus": world, "steps": len(loads),
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "mixed (f64/f32/i64/u64/i32/u32/decimal128)", "data": "synthetic",
-            "config": {"workload": f"config4: {len(tpl)} resident columns, sizes floor(exp(U[ln 64 KiB, "
-                                   f"ln {args.max_bytes >> 20} MiB])) bytes, dtypes and generators of config3; "
+            "config": {"workload": f"served: {len(tpl)} resident columns, sizes floor(exp(U[ln 64 KiB, "
+                                   f"ln {args.max_bytes >> 20} MiB])) bytes, dtypes and generators of the batched "
+                                   "columns; "
                                    f"{args.requests} requests per offered load",
                        "workers": args.workers, "budget_bytes": budget, "resident_bytes": resident,
                        "mean_request_bytes": int(mean_bytes), "parallelism": f"replicas x{world}"},
@@ -872,23 +875,23 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serial-columns", action="store_true",
                     help="one host thread runs the columns one after another (for profilers)")
-    ap.add_argument("--workload", default="config1", choices=["config1", "config2", "config3", "config4"],
-                    help="config3: the batched configuration (plain vs batch calls); config4: the served "
-                         "request stream")
-    ap.add_argument("--columns", type=int, default=256, help="config3: number of columns")
-    ap.add_argument("--max-len", type=int, default=1 << 21, help="config3: longest column")
-    ap.add_argument("--workers", type=int, default=8, help="config3/config4: contexts in the batch / server")
-    ap.add_argument("--columns4", type=int, default=24, help="config4: resident columns")
-    ap.add_argument("--max-bytes", type=int, default=256 << 20, help="config4: largest column")
-    ap.add_argument("--requests", type=int, default=600, help="config4: requests per offered load")
+    ap.add_argument("--workload", default="integer-lanes",
+                    choices=["integer-lanes", "float-lanes", "batched", "served"],
+                    help="batched: many uneven columns (plain vs batch calls); served: the request stream")
+    ap.add_argument("--columns", type=int, default=256, help="batched: number of columns")
+    ap.add_argument("--max-len", type=int, default=1 << 21, help="batched: longest column")
+    ap.add_argument("--workers", type=int, default=8, help="batched / served: contexts in the batch / server")
+    ap.add_argument("--columns4", type=int, default=24, help="served: resident columns")
+    ap.add_argument("--max-bytes", type=int, default=256 << 20, help="served: largest column")
+    ap.add_argument("--requests", type=int, default=600, help="served: requests per offered load")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
-    if args.workload == "config3":
-        return run_gpu_config3(args, rank, world, local)
-    if args.workload == "config4":
-        return run_gpu_config4(args, rank, world, local)
+    if args.workload == "batched":
+        return run_gpu_batched(args, rank, world, local)
+    if args.workload == "served":
+        return run_gpu_served(args, rank, world, local)
     return run_gpu(args, rank, world, local)
 
 

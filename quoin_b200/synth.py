@@ -1,9 +1,10 @@
-"""Seeded synthetic columns with the shapes of the benchmark configurations.
+"""Seeded synthetic columns with the shapes of the benchmark workloads.
 
 The published benchmarks run on datasets that are not available here (the
 ALP float corpus, ClickBench); these generators stand in for them with the
-value distributions each configuration names.  numpy PCG64, base seed
-20261203 + 100 * config + column index.
+value distributions each workload names.  numpy PCG64, base seed
+20261203 + 100 * column set + column index (column sets: 0 prices, 1 integer
+lanes, 2 float lanes, 3 mixed columns, 4 served requests).
 """
 from __future__ import annotations
 
@@ -14,8 +15,8 @@ from . import DECIMAL128, F32, F64, I32, I64, U32, U64
 BASE_SEED = 20261203
 
 
-def rng_for(config: int, column: int) -> np.random.Generator:
-    return np.random.default_rng(BASE_SEED + 100 * config + column)
+def rng_for(column_set: int, column: int) -> np.random.Generator:
+    return np.random.default_rng(BASE_SEED + 100 * column_set + column)
 
 
 def bernoulli_bitmap(rng: np.random.Generator, n: int, p_valid: float = 0.9) -> np.ndarray:
@@ -95,52 +96,55 @@ def decimal128_uniform(n: int, rng: np.random.Generator, lo: int = -10**14, hi: 
     return out
 
 
-def config_columns(config: str, n: int):
-    """[(name, wire dtype, values, validity bitmap or None)] for a benchmark config."""
-    if config == "1":
+def benchmark_columns(kind: str, n: int):
+    """[(name, wire dtype, values, validity bitmap or None)] of a benchmark column
+    set: "prices" (one f64 column of two-decimal prices with 3 % random-bit
+    values), "integer" (i64 timestamps, u64 runs, i32 categories, 10 % nulls) or
+    "float" (f64 random walk, f32 sensor readings, Decimal128)."""
+    if kind == "integer":
         r = [rng_for(1, c) for c in range(3)]
         return [
             ("timestamps_i64", I64, timestamps_i64(n, r[0]), bernoulli_bitmap(r[0], n)),
             ("runs_u64", U64, runs_u64(n, r[1]), bernoulli_bitmap(r[1], n)),
             ("categories_i32", I32, categories_i32(n, r[2]), bernoulli_bitmap(r[2], n)),
         ]
-    if config == "0":
+    if kind == "prices":
         return [("prices_f64", F64, prices_f64(n, rng_for(0, 0)), None)]
-    if config == "2":
+    if kind == "float":
         r = [rng_for(2, c) for c in range(3)]
         return [
             ("random_walk_f64", F64, random_walk_f64(n, r[0]), None),
             ("sensor_f32", F32, sensor_f32(n, r[1]), None),
             ("decimal128", DECIMAL128, decimal128_uniform(n, r[2]), None),
         ]
-    raise ValueError(config)
+    raise ValueError(kind)
 
 
 MIXED_DTYPES = [F64, F32, I64, U64, I32, U32, DECIMAL128]
 NATIVE_BYTES = {F64: 8, F32: 4, I64: 8, U64: 8, I32: 4, U32: 4, DECIMAL128: 16}
 
 
-def config3_columns(ncols: int, max_len: int = 1 << 21, min_len: int = 1024):
-    """The batched configuration: `ncols` columns with lengths floor(exp(U[ln min_len,
+def mixed_columns(ncols: int, max_len: int = 1 << 21, min_len: int = 1024):
+    """Many uneven columns: `ncols` columns with lengths floor(exp(U[ln min_len,
     ln max_len])), dtype uniform over f64/f32/i64/u64/i32/u32/decimal128, the
-    per-dtype generators of configs 0-2, and a null rate U(0, 0.2) each.
+    per-dtype generators of benchmark_columns, and a null rate U(0, 0.2) each.
     [(name, wire dtype, values, validity bitmap or None)]."""
     return _mixed_columns(3, ncols, lambda r, dt: int(np.floor(np.exp(r.uniform(np.log(min_len), np.log(max_len))))))
 
 
-def config4_columns(ncols: int, max_bytes: int = 256 << 20, min_bytes: int = 64 << 10):
-    """Request columns of the serving configuration: sizes floor(exp(U[ln min_bytes,
-    ln max_bytes])) bytes of native values, dtypes and generators as config3."""
+def request_columns(ncols: int, max_bytes: int = 256 << 20, min_bytes: int = 64 << 10):
+    """Columns of the served request stream: sizes floor(exp(U[ln min_bytes,
+    ln max_bytes])) bytes of native values, dtypes and generators as mixed_columns."""
     return _mixed_columns(4, ncols, lambda r, dt: max(
         int(np.floor(np.exp(r.uniform(np.log(min_bytes), np.log(max_bytes))))) // NATIVE_BYTES[dt], 1),
         size_first=False)
 
 
-def _mixed_columns(config: int, ncols: int, length, size_first: bool = True):
+def _mixed_columns(column_set: int, ncols: int, length, size_first: bool = True):
     dtypes = MIXED_DTYPES
     out = []
     for c in range(ncols):
-        r = rng_for(config, c)
+        r = rng_for(column_set, c)
         if size_first:
             n = length(r, None)
             dt = dtypes[int(r.integers(0, len(dtypes)))]

@@ -53,7 +53,7 @@ def test_batch_matches_single_column_calls(qb, batch_api):
     import torch
     L = batch_api
     torch.cuda.set_device(0)
-    cols = synth.config3_columns(48, 1 << 17)
+    cols = synth.mixed_columns(48, 1 << 17)
     cfg = qb._cfg(qb.Config(level=qb.Level.FAST))
     dev = []
     jobs = (CompressJob * len(cols))()

@@ -1,5 +1,5 @@
 """The benchmark columns at their full size (67,108,864 values each, seeded
-synthetic stand-ins for the integer-lane and float-lane configurations) at
+synthetic stand-ins for the integer-lane and float-lane workloads) at
 Level::Fast: the GPU stream must equal the oracle's byte for byte, and its
 decode must give back every value bit for bit (null slots as 0, the bitmap
 unchanged).
@@ -22,9 +22,9 @@ def _expected(v, bm, n):
     return raw.tobytes()
 
 
-@pytest.mark.parametrize("config", ["1", "2"])
-def test_full_size_columns_match_oracle_and_round_trip(qb, oracle, config):
-    for name, dt, v, bm in synth.config_columns(config, N_FULL):
+@pytest.mark.parametrize("kind", ["integer", "float"])
+def test_full_size_columns_match_oracle_and_round_trip(qb, oracle, kind):
+    for name, dt, v, bm in synth.benchmark_columns(kind, N_FULL):
         sc, pr = (4, 18) if dt == DEC128 else (0, 0)
         got = qb.compress_column(v, bm, qb.Config(level=qb.Level.FAST), dtype=dt, scale=sc, precision=pr)
         want = oracle.compress_column(v, dt, bm, level=1, scale=sc, precision=pr, threads=16)

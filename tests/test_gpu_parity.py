@@ -184,13 +184,13 @@ def test_predictor_log2_is_recorded(qb, oracle):
 
 
 # ---------------------------------------------------------------------------
-# Benchmark-config-shaped columns (seeded synthetic stand-ins), 1M values
+# Benchmark-shaped columns (seeded synthetic stand-ins), 1M values
 # ---------------------------------------------------------------------------
-@pytest.mark.parametrize("config", ["0", "1", "2"])
-def test_config_columns_match_oracle(qb, oracle, config):
+@pytest.mark.parametrize("kind", ["prices", "integer", "float"])
+def test_benchmark_columns_match_oracle(qb, oracle, kind):
     from quoin_b200 import synth
     n = 1 << 20
-    for name, dt, vals, bm in synth.config_columns(config, n):
+    for name, dt, vals, bm in synth.benchmark_columns(kind, n):
         sc, pr = (4, 18) if dt == DEC128 else (0, 0)
         want = oracle.compress_column(vals, dt, bm, level=1, scale=sc, precision=pr, threads=8)
         got = gpu_compress(qb, vals, dt, bm, 1, scale=sc, precision=pr)

@@ -107,13 +107,13 @@ def _run(qb, L, cols, workers, budget):
 
 
 def test_server_requests_match_single_calls(qb, server_api):
-    cols = synth.config3_columns(40, 1 << 17)
+    cols = synth.mixed_columns(40, 1 << 17)
     peak = _run(qb, server_api, cols, 6, 120 << 30)
     assert peak > 0
 
 
 def test_server_small_budget(qb, server_api):
-    cols = synth.config3_columns(12, 1 << 15, min_len=1 << 14)
+    cols = synth.mixed_columns(12, 1 << 15, min_len=1 << 14)
     budget = 6 << 20  # one or two of these requests at a time (48 B/value of working memory + buffers)
     peak = _run(qb, server_api, cols, 4, budget)
     assert 0 < peak <= budget
