@@ -118,3 +118,18 @@ def test_batch_matches_single_column_calls(qb, batch_api):
 def test_batch_create_rejects_bad_worker_counts(batch_api):
     assert not batch_api.quoin_b200_batch_create(0)
     assert not batch_api.quoin_b200_batch_create(65)
+
+
+def test_batch_edges(qb, batch_api):
+    L = batch_api
+    b = P(L.quoin_b200_batch_create(2))
+    try:
+        assert L.quoin_b200_compress_batch_device(b, None, 0, None) == 0  # no columns
+        assert L.quoin_b200_decompress_batch_device(b, None, 0) == 0
+        djobs = (DecompressJob * 1)()
+        djobs[0] = DecompressJob(None, None, None, None, 99)  # no index: this job alone fails
+        assert L.quoin_b200_decompress_batch_device(b, djobs, 1) == -1 and djobs[0].status == -1
+        assert L.quoin_b200_compress_batch_device(None, None, 0, None) == -1
+    finally:
+        L.quoin_b200_batch_free(b)
+    L.quoin_b200_batch_free(None)

@@ -133,3 +133,32 @@ def test_server_refuses_requests_above_budget(qb, server_api):
         L.quoin_b200_server_free(srv)
     assert not L.quoin_b200_server_create(0, 1 << 20, None)
     assert not L.quoin_b200_server_create(4, 0, None)
+
+
+def test_server_empty_column_and_free_with_queued_requests(qb, server_api):
+    import torch
+    L = server_api
+    cfg = qb._cfg(qb.Config(level=qb.Level.FAST))
+    srv = P(L.quoin_b200_server_create(2, 1 << 30, ctypes.byref(cfg)))
+    cap = qb._stream_bound(qb.I64, 0, False)
+    dd = torch.zeros(max(cap, 64), dtype=torch.uint8, device="cuda")
+    dv = torch.zeros(8, dtype=torch.uint8, device="cuda")
+    empty = Request(op=OP_COMPRESS, wire_dtype=qb.I64, n=0, d_values=dv.data_ptr(), d_dst=dd.data_ptr(),
+                    dst_cap=cap, device_bytes=64)
+    assert L.quoin_b200_server_submit(srv, ctypes.byref(empty)) == 0
+    assert L.quoin_b200_server_wait(srv, ctypes.byref(empty), -1) == 0
+    assert dd[: empty.out_len].cpu().numpy().tobytes() == qb.compress_column(np.zeros(0, np.int64))
+    # requests still queued when the server is freed are finished first
+    v = np.arange(1 << 16, dtype=np.int64)
+    dv2 = torch.from_numpy(v.view(np.uint8).copy()).cuda()
+    cap2 = qb._stream_bound(qb.I64, len(v), False)
+    outs = [torch.zeros(cap2, dtype=torch.uint8, device="cuda") for _ in range(8)]
+    reqs = [Request(op=OP_COMPRESS, wire_dtype=qb.I64, n=len(v), d_values=dv2.data_ptr(), d_dst=o.data_ptr(),
+                    dst_cap=cap2, device_bytes=v.nbytes + cap2) for o in outs]
+    for r in reqs:
+        assert L.quoin_b200_server_submit(srv, ctypes.byref(r)) == 0
+    L.quoin_b200_server_free(srv)
+    want = qb.compress_column(v)
+    for r, o in zip(reqs, outs):
+        assert r.done == 1 and r.status == 0
+        assert o[: r.out_len].cpu().numpy().tobytes() == want
