@@ -390,29 +390,39 @@ def run_gpu(args, rank, world, local):
     L.quoin_b200_timing_enable(0)
 
     # e2e through the host-buffer C ABI with pinned host memory.  Each column
-    # is a two-stage stream: one host thread compresses step after step (its
-    # context), another decompresses each step's stream as it arrives (a
-    # second context), with two stream buffers between them, so one step's
-    # decompress (mostly device -> host) overlaps the next step's compress
-    # (mostly host -> device).  --serial-columns runs compress then
+    # runs --e2e-lanes two-stage pipelines, lane li taking steps li, li +
+    # lanes, ...: one host thread compresses the lane's steps (its context),
+    # another decompresses each step's stream as it arrives (a second
+    # context), with two stream buffers between them, so decompresses (mostly
+    # device -> host) overlap compresses (mostly host -> device) and several
+    # copies are in flight per column.  --serial-columns runs compress then
     # decompress of one column at a time from one thread.
     import queue
     import threading
 
-    dctxs = [ctypes.c_void_p(L.quoin_ctx_create(0)) for _ in gcols]
+    lanes = 1 if args.serial_columns else max(args.e2e_lanes, 1)
+    # per column and lane: a compress context, a decompress context, two
+    # stream buffers and the output buffers; the inputs are shared
+    cctxs = [[c["ctx"]] + [ctypes.c_void_p(L.quoin_ctx_create(0)) for _ in range(lanes - 1)] for c in gcols]
+    dctxs = [[ctypes.c_void_p(L.quoin_ctx_create(0)) for _ in range(lanes)] for _ in gcols]
     pinned = []
     for c in gcols:
         hv = torch.from_numpy(np.ascontiguousarray(c["v"]).view(np.uint8).copy()).pin_memory()
         hb = torch.from_numpy(c["bm"].copy()).pin_memory() if c["bm"] is not None else None
-        hdst = [torch.empty(c["len"] + (1 << 20), dtype=torch.uint8).pin_memory() for _ in range(2)]
-        hout = torch.empty(n * c["w"], dtype=torch.uint8).pin_memory()
-        hvout = torch.empty((n + 7) // 8, dtype=torch.uint8).pin_memory()
-        pinned.append((hv, hb, hdst, hout, hvout))
+        per_lane = []
+        for _ in range(lanes):
+            hdst = [torch.empty(c["len"] + (1 << 20), dtype=torch.uint8).pin_memory() for _ in range(2)]
+            hout = torch.empty(n * c["w"], dtype=torch.uint8).pin_memory()
+            hvout = torch.empty((n + 7) // 8, dtype=torch.uint8).pin_memory()
+            per_lane.append((hdst, hout, hvout))
+        pinned.append((hv, hb, per_lane))
 
-    def e2e_compress(c, pin, slot):
-        hv, hb, hdst, _, _ = pin
+    def e2e_compress(ci, li, slot):
+        c = gcols[ci]
+        hv, hb, per_lane = pinned[ci]
+        hdst = per_lane[li][0]
         olen = ctypes.c_size_t()
-        rc = L.quoin_b200_compress_column(c["ctx"], c["wire"], n, P(hv.data_ptr()),
+        rc = L.quoin_b200_compress_column(cctxs[ci][li], c["wire"], n, P(hv.data_ptr()),
                                           P(hb.data_ptr()) if hb is not None else None, c["sc"], c["pr"],
                                           ctypes.byref(cfg),
                                           P(hdst[slot].data_ptr()), hdst[slot].numel(), ctypes.byref(olen))
@@ -420,16 +430,17 @@ def run_gpu(args, rank, world, local):
             raise Q.Error(rc)
         return olen.value
 
-    def e2e_decompress(ci, pin, slot, olen):
-        _, _, hdst, hout, hvout = pin
-        rc = L.quoin_b200_decompress_column(dctxs[ci], P(hdst[slot].data_ptr()), olen, P(hout.data_ptr()),
+    def e2e_decompress(ci, li, slot, olen):
+        hdst, hout, hvout = pinned[ci][2][li]
+        rc = L.quoin_b200_decompress_column(dctxs[ci][li], P(hdst[slot].data_ptr()), olen, P(hout.data_ptr()),
                                             P(hvout.data_ptr()))
         if rc:
             raise Q.Error(rc)
 
     def e2e_bytes():
         h2d = d2h = 0
-        for c, (hv, hb, hdst, hout, hvout) in zip(gcols, pinned):
+        for c, (hv, hb, per_lane) in zip(gcols, pinned):
+            hout, hvout = per_lane[0][1], per_lane[0][2]
             h2d += hv.numel() + (hb.numel() if hb is not None else 0) + c["len"]
             d2h += c["len"] + hout.numel() + (hvout.numel() if hb is not None else 0)
         return h2d, d2h
@@ -437,21 +448,20 @@ def run_gpu(args, rank, world, local):
     def e2e_run(steps):
         if args.serial_columns:
             for _ in range(steps):
-                for ci, (c, pin) in enumerate(zip(gcols, pinned)):
-                    e2e_decompress(ci, pin, 0, e2e_compress(c, pin, 0))
+                for ci in range(len(gcols)):
+                    e2e_decompress(ci, 0, 0, e2e_compress(ci, 0, 0))
             return
         errors = []
 
-        def column(ci):
-            c, pin = gcols[ci], pinned[ci]
+        def lane(ci, li, count):
             q = queue.Queue()
             free = threading.Semaphore(2)
 
             def produce():
                 try:
-                    for k in range(steps):
+                    for k in range(count):
                         free.acquire()
-                        q.put((k % 2, e2e_compress(c, pin, k % 2)))
+                        q.put((k % 2, e2e_compress(ci, li, k % 2)))
                 except Exception as e:  # noqa: BLE001 - reported after the join
                     errors.append(e)
                 q.put(None)
@@ -463,7 +473,7 @@ def run_gpu(args, rank, world, local):
                     item = q.get()
                     if item is None:
                         break
-                    e2e_decompress(ci, pin, item[0], item[1])
+                    e2e_decompress(ci, li, item[0], item[1])
                     free.release()
             except Exception as e:  # noqa: BLE001
                 errors.append(e)
@@ -473,7 +483,9 @@ def run_gpu(args, rank, world, local):
                         break
             prod.join()
 
-        threads = [threading.Thread(target=column, args=(ci,)) for ci in range(len(gcols))]
+        # lane li of a column takes steps li, li + lanes, ...
+        threads = [threading.Thread(target=lane, args=(ci, li, len(range(li, steps, lanes))))
+                   for ci in range(len(gcols)) for li in range(lanes)]
         for th in threads:
             th.start()
         for th in threads:
@@ -530,14 +542,15 @@ def run_gpu(args, rank, world, local):
             "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "timing": ("wall clock around synchronous host-buffer C-ABI calls, pinned host memory; "
                                + ("one column at a time" if args.serial_columns else
-                                  "per column one thread compresses step after step and another decompresses "
-                                  "each step's stream (two stream buffers), so the two copy directions overlap"))},
+                                  f"per column {lanes} pipeline(s), each one thread compressing its steps and "
+                                  "another decompressing each step's stream (two stream buffers), so the two copy "
+                                  "directions overlap"))},
             "gpu_launches": int(launches // max(args.steps, 1) * args.steps),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     pool.shutdown()
-    for cx in ctxs + dctxs:
+    for cx in ctxs + [x for row in cctxs for x in row[1:]] + [x for row in dctxs for x in row]:
         L.quoin_ctx_free(cx)
     if world > 1:
         dist.destroy_process_group()
@@ -873,6 +886,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="values per column")
     ap.add_argument("--cpu-sample", type=int, default=1 << 24)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--e2e-lanes", type=int, default=1,
+                    help="e2e: compress/decompress pipelines per column (each its own contexts and buffers)")
     ap.add_argument("--serial-columns", action="store_true",
                     help="one host thread runs the columns one after another (for profilers)")
     ap.add_argument("--workload", default="integer-lanes",
