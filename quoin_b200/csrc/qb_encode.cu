@@ -2971,8 +2971,54 @@ unsigned long long* device_win_counters() {
 #include "qb_scan.cuh"
 
 namespace qb {
+// At most kSmallWords frames in one CTA of 1,024 threads: k_frame_sizes, the
+// exclusive scan and k_frame_apply in one launch.
+__global__ void __launch_bounds__(1024) k_frame_offsets_small(FrameDesc* frames, const uint32_t* __restrict__ nbp,
+                                                              const uint64_t* __restrict__ base_p,
+                                                              uint64_t* __restrict__ total) {
+  __shared__ uint64_t wsum[32];
+  uint32_t nb = *nbp, t = threadIdx.x, l = t & 31, warp = t >> 5;
+  uint64_t base = *base_p;
+  uint64_t v[kSmallPer], s = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kSmallPer; k++) {
+    uint32_t i = t * kSmallPer + k;
+    v[k] = i < nb ? 9ull + frames[i].plen : 0ull;
+    s += v[k];
+  }
+  uint64_t inc = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+    if ((int)l >= o) inc += u;
+  }
+  if (l == 31) wsum[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t x = wsum[l];
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t u = __shfl_up_sync(0xffffffffu, x, o);
+      if ((int)l >= o) x += u;
+    }
+    wsum[l] = x;
+    if (l == 31) *total = x;
+  }
+  __syncthreads();
+  uint64_t run = (warp ? wsum[warp - 1] : 0ull) + inc - s;
+#pragma unroll
+  for (uint32_t k = 0; k < kSmallPer; k++) {
+    uint32_t i = t * kSmallPer + k;
+    if (i < nb) frames[i].payload_off = base + run + 9;
+    run += v[k];
+  }
+}
+
 void launch_frame_offsets(FrameDesc* frames, const uint32_t* nb, uint32_t max_blocks, const uint64_t* base,
                           uint64_t* sizes_tmp, uint64_t* tile_tmp, uint64_t* total, cudaStream_t st) {
+  if (max_blocks <= kSmallWords) {
+    k_frame_offsets_small<<<1, 1024, 0, st>>>(frames, nb, base, total);
+    count_launches(1);
+    return;
+  }
   unsigned g = (unsigned)qmin((max_blocks + 255) / 256, 1024);
   if (g == 0) g = 1;
   k_frame_sizes<<<g, 256, 0, st>>>(frames, nb, max_blocks, sizes_tmp);

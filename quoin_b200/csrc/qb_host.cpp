@@ -470,10 +470,14 @@ int device_valid_count(QuoinCtx* c, cudaStream_t st, const uint8_t* d_bm, uint64
   uint64_t* misc = c->p<uint64_t>(S_MISC);
   {
     TimedRegion tr(T_VALIDITY, st);
-    CK(cudaMemsetAsync(misc + 9, 0, 8, st));
-    launch_word_popcount(d_bm, n, rank, st);
-    launch_scan_sum(rank, rank, nw, c->p<uint64_t>(S_TILE), misc + 8, st);
-    launch_bitmap_transitions(d_bm, n, reinterpret_cast<unsigned long long*>(misc + 9), st);
+    if (nw <= kSmallWords) {  // one launch for a short column
+      launch_valid_small(d_bm, n, rank, misc + 8, reinterpret_cast<unsigned long long*>(misc + 9), st);
+    } else {
+      CK(cudaMemsetAsync(misc + 9, 0, 8, st));
+      launch_word_popcount(d_bm, n, rank, st);
+      launch_scan_sum(rank, rank, nw, c->p<uint64_t>(S_TILE), misc + 8, st);
+      launch_bitmap_transitions(d_bm, n, reinterpret_cast<unsigned long long*>(misc + 9), st);
+    }
   }
   uint64_t h[2] = {0, 0};
   CK(read_small(c, st, h, misc + 8, 16));

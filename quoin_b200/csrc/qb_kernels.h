@@ -135,6 +135,13 @@ void launch_validity_blob(const uint8_t* bm, uint64_t n, uint64_t* tmp, uint64_t
 uint64_t validity_tmp_words(uint64_t n);
 // Adds the bitmap's bit-transition count to *count (zero it first).
 void launch_bitmap_transitions(const uint8_t* bm, uint64_t n, unsigned long long* count, cudaStream_t st);
+// Short columns: a bitmap of at most kSmallWords words ranked, counted and its
+// transitions counted by one CTA (rank = exclusive word ranks, *total = the
+// valid count, *trans = 0/1 transitions); frame offsets of at most
+// kSmallWords blocks by one CTA.
+constexpr uint32_t kSmallPer = 8, kSmallWords = 1024 * kSmallPer;
+void launch_valid_small(const uint8_t* bm, uint64_t n, uint64_t* rank, uint64_t* total, unsigned long long* trans,
+                        cudaStream_t st);
 // The stream a call on context c runs on: `stream` when given, else the
 // context's own (the default context when c is null).
 cudaStream_t ctx_stream(struct ::QuoinCtx* c, void* stream);

@@ -302,6 +302,61 @@ __global__ void k_bitmap_transitions(const uint8_t* __restrict__ bm, uint64_t n,
     if (t) atomicAdd(count, t);
   }
 }
+// A short column's bitmap (at most kSmallWords 32-bit words) in one CTA of
+// 1,024 threads: every word's exclusive valid rank, the valid count and the
+// 0/1 transition count -- k_word_popcount, the rank scan and
+// k_bitmap_transitions in one launch, since short columns pay per launch.
+__global__ void __launch_bounds__(1024) k_valid_small(const uint8_t* __restrict__ bm, uint64_t n,
+                                                      uint64_t* __restrict__ rank, uint64_t* __restrict__ total,
+                                                      unsigned long long* __restrict__ trans) {
+  __shared__ uint64_t wsum[32];
+  __shared__ uint32_t wtr[32];
+  uint32_t nw = (uint32_t)((n + 31) / 32), t = threadIdx.x, l = t & 31, warp = t >> 5;
+  uint32_t c[kSmallPer];
+  uint32_t s = 0, tr = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kSmallPer; k++) {
+    uint32_t w = t * kSmallPer + k;
+    c[k] = w < nw ? (uint32_t)__popc(bm_word_at(bm, w, n)) : 0u;
+    s += c[k];
+    if (w < nw) tr += __popc(trans_mask(bm, w, n));
+  }
+  uint64_t inc = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+    if ((int)l >= o) inc += u;
+  }
+  tr = warp_sum(tr);
+  if (l == 31) wsum[warp] = inc;
+  if (l == 0) wtr[warp] = tr;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t x = wsum[l];
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t u = __shfl_up_sync(0xffffffffu, x, o);
+      if ((int)l >= o) x += u;
+    }
+    wsum[l] = x;  // inclusive over warps
+    uint32_t y = warp_sum(wtr[l]);
+    if (l == 31) *total = x;
+    if (l == 0) *trans = y;
+  }
+  __syncthreads();
+  uint64_t run = (warp ? wsum[warp - 1] : 0ull) + inc - s;
+#pragma unroll
+  for (uint32_t k = 0; k < kSmallPer; k++) {
+    uint32_t w = t * kSmallPer + k;
+    if (w < nw) rank[w] = run;
+    run += c[k];
+  }
+}
+
+void launch_valid_small(const uint8_t* bm, uint64_t n, uint64_t* rank, uint64_t* total, unsigned long long* trans,
+                        cudaStream_t st) {
+  k_valid_small<<<1, 1024, 0, st>>>(bm, n, rank, total, trans);
+  count_launches(1);
+}
+
 // Bits [bit_off, bit_off + n) of a validity bitmap (LSB first) re-packed from
 // bit 0, trailing bits of the last byte cleared (the Arrow slice re-pack of
 // arrow.rs:29-52, on the device).  The source holds ceil((bit_off + n) / 8)
