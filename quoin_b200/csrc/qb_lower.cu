@@ -421,9 +421,118 @@ uint64_t validity_tmp_words(uint64_t n) {
   return 3 * nw + scan_tiles(nw) + 8;
 }
 
+// The validity blob of a short column (at most kSmallWords words) in one CTA
+// of 1,024 threads: the three passes above (last transitions + max scan, run
+// bytes + sum scan, write) with block scans in place of the grid scans.
+__global__ void __launch_bounds__(1024) k_vb_small(const uint8_t* __restrict__ bm, uint64_t n,
+                                                   uint8_t* __restrict__ out, uint64_t* __restrict__ blob_len) {
+  __shared__ uint64_t wa[32], wb[32];
+  uint32_t nw = (uint32_t)((n + 31) / 32), t = threadIdx.x, l = t & 31, warp = t >> 5;
+  uint32_t tm[kSmallPer];
+  uint64_t mx = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kSmallPer; k++) {
+    uint32_t w = t * kSmallPer + k;
+    tm[k] = w < nw ? trans_mask(bm, w, n) : 0u;
+    if (tm[k]) mx = (uint64_t)w * 32 + (31 - __clz(tm[k]));  // words ascend: the thread's last transition
+  }
+  // exclusive max scan of the threads' last transitions (positions ascend, 0 = none yet)
+  uint64_t inc = mx;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+    if ((int)l >= o) inc = u > inc ? u : inc;
+  }
+  uint64_t ex = __shfl_up_sync(0xffffffffu, inc, 1);
+  if (l == 0) ex = 0;
+  if (l == 31) wa[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t x = wa[l];
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t u = __shfl_up_sync(0xffffffffu, x, o);
+      if ((int)l >= o) x = u > x ? u : x;
+    }
+    wa[l] = x;
+  }
+  __syncthreads();
+  uint64_t before = warp ? wa[warp - 1] : 0ull;
+  uint64_t prev0 = ex > before ? ex : before, t_last = wa[31];
+  // bytes of the runs that end at this thread's transitions, then their offsets
+  uint64_t prev = prev0, s = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kSmallPer; k++) {
+    uint32_t tt = tm[k];
+    uint32_t w = t * kSmallPer + k;
+    while (tt) {
+      uint64_t p = (uint64_t)w * 32 + (__ffs(tt) - 1);
+      tt &= tt - 1;
+      s += varint_len(p - prev);
+      prev = p;
+    }
+  }
+  uint64_t inc2 = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint64_t u = __shfl_up_sync(0xffffffffu, inc2, o);
+    if ((int)l >= o) inc2 += u;
+  }
+  if (l == 31) wb[warp] = inc2;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t x = wb[l];
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t u = __shfl_up_sync(0xffffffffu, x, o);
+      if ((int)l >= o) x += u;
+    }
+    wb[l] = x;
+  }
+  __syncthreads();
+  uint64_t run_bytes = wb[31], raw_len = (n + 7) / 8;
+  uint64_t rle_len = run_bytes + varint_len(n - t_last);
+  bool rle = rle_len < raw_len;
+  if (t == 0) {
+    out[0] = rle ? 1 : 0;
+    *blob_len = 1 + (rle ? rle_len : raw_len);
+  }
+  if (!rle) {
+    for (uint64_t i = t; i < raw_len; i += blockDim.x) out[1 + i] = bm[i];
+    return;
+  }
+  uint64_t pos = 1 + (warp ? wb[warp - 1] : 0ull) + inc2 - s;
+  prev = prev0;
+#pragma unroll
+  for (uint32_t k = 0; k < kSmallPer; k++) {
+    uint32_t tt = tm[k];
+    uint32_t w = t * kSmallPer + k;
+    while (tt) {
+      uint64_t p = (uint64_t)w * 32 + (__ffs(tt) - 1);
+      tt &= tt - 1;
+      uint64_t v = p - prev;
+      do {
+        uint8_t b = (uint8_t)(v & 0x7f);
+        v >>= 7;
+        out[pos++] = v ? (b | 0x80) : b;
+      } while (v);
+      prev = p;
+    }
+  }
+  if (t == 0) {
+    uint64_t v = n - t_last, q = 1 + run_bytes;
+    do {
+      uint8_t b = (uint8_t)(v & 0x7f);
+      v >>= 7;
+      out[q++] = v ? (b | 0x80) : b;
+    } while (v);
+  }
+}
+
 void launch_validity_blob(const uint8_t* bm, uint64_t n, uint64_t* tmp, uint64_t* tile_tmp, uint8_t* out,
                           uint64_t* blob_len, cudaStream_t st) {
   uint64_t nw = (n + 31) / 32;
+  if (nw <= kSmallWords) {
+    k_vb_small<<<1, 1024, 0, st>>>(bm, n, out, blob_len);
+    count_launches(1);
+    return;
+  }
   uint64_t* last = tmp;
   uint64_t* sizes = tmp + nw;
   uint64_t* state = tmp + 2 * nw;  // [0] t_last, [1] bytes
