@@ -58,6 +58,14 @@ WORKLOADS = {
 }
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture) of
+# one decode of the workload's three columns at 16,777,216 values each, summed
+# over k_walk_frames, k_prepass, k_prepass_scan and k_decode_items; reported
+# scaled by the values per column.  Lines still dirty in L2 when a launch ends
+# are not counted, so the figure is a lower bound on the written share.
+DECODE_TRAFFIC_16M = {"integer-lanes": 388_141_056}
+
+
 def decimal_args(wire):
     """(scale, precision) of the benchmark's decimal columns; (0, 0) otherwise."""
     from quoin_b200 import DECIMAL128
@@ -537,7 +545,12 @@ def run_gpu(args, rank, world, local):
                                                    "k_decode_items of the three columns in flight together)",
                          "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": None, "decode_calls_per_step": per_class["decode"][1] // max(args.steps, 1)},
+                         "traffic": (round(DECODE_TRAFFIC_16M[args.workload] * n / (1 << 24))
+                                     if args.workload in DECODE_TRAFFIC_16M else None),
+                         "traffic_note": ("DRAM bytes per decode phase (three decode calls), from an ncu capture "
+                                          "at 16,777,216 values per column scaled by the values processed"
+                                          if args.workload in DECODE_TRAFFIC_16M else "not captured"),
+                         "decode_calls_per_step": per_class["decode"][1] // max(args.steps, 1)},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "timing": ("wall clock around synchronous host-buffer C-ABI calls, pinned host memory; "
