@@ -79,6 +79,8 @@ def lib():
         L.oq_linear_select_order.argtypes = [P, S]
         L.oq_pred_payload.argtypes = [ctypes.c_int, P, S, ctypes.c_int, ctypes.c_int,
                                       ctypes.POINTER(U8P), ctypes.POINTER(S)]
+        L.oq_tans_compress.argtypes = [P, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
+        L.oq_tans_decompress.argtypes = [P, S, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
         L.oq_crc32c_u64.argtypes = [ctypes.c_uint32, ctypes.c_uint64]
         L.oq_crc32c_u64.restype = ctypes.c_uint32
         L.oq_lz_compress.argtypes = [P, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
@@ -200,7 +202,28 @@ def rc_decompress(payload: bytes, max_len: int) -> bytes:
     return _take(ctypes.cast(out, ctypes.c_void_p).value, olen.value) or b""
 
 
-TAG_RC, TAG_RANS = 0, 2
+TAG_RC, TAG_TANS, TAG_RANS = 0, 1, 2
+
+
+def tans_compress(data: bytes):
+    """tans.rs compress_bytes: the coded bytes (no tag), None where the coder declines."""
+    a = np.frombuffer(data, dtype=np.uint8) if data else np.zeros(1, np.uint8)
+    out = ctypes.POINTER(ctypes.c_uint8)()
+    olen = ctypes.c_size_t()
+    rc = lib().oq_tans_compress(a.ctypes.data, len(data), ctypes.byref(out), ctypes.byref(olen))
+    if rc:
+        return None
+    return _take(ctypes.cast(out, ctypes.c_void_p).value, olen.value)
+
+
+def tans_decompress(payload: bytes, max_len: int) -> bytes:
+    a = np.frombuffer(payload, dtype=np.uint8) if payload else np.zeros(1, np.uint8)
+    out = ctypes.POINTER(ctypes.c_uint8)()
+    olen = ctypes.c_size_t()
+    rc = lib().oq_tans_decompress(a.ctypes.data, len(payload), max_len, ctypes.byref(out), ctypes.byref(olen))
+    if rc:
+        raise OracleError(rc)
+    return _take(ctypes.cast(out, ctypes.c_void_p).value, olen.value) or b""
 M_ORDERED_DELTA, M_DELTA2, M_DELTA_DP = 7, 20, 45
 
 

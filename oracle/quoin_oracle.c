@@ -1098,14 +1098,208 @@ static int lz_decompress(const uint8_t *p, size_t len, size_t expected, buf_t *o
     return OQ_OK;
 }
 
-/* entropy/mod.rs:152-163: tag 2 rANS, tag 0 the range coder; the legacy
- * tANS tag (decoded by the reference, never produced) is not restated. */
+/* ------------------------------------------------------------------------ */
+/* tANS — src/entropy/tans.rs, src/bitio.rs (entropy tag 1: the reference    */
+/* still decodes it and no longer produces it; the encoder here only makes   */
+/* test streams)                                                             */
+/* ------------------------------------------------------------------------ */
+/* A 1,024-entry state table (states 1024..2047).  Wire: varint(len) ++
+ * u8(distinct - 1) ++ the distinct symbols ++ their u16 LE weights (sum 1024)
+ * ++ u32 LE final encoder state ++ the renormalisation bits, MSB first. */
+#define TANS_SIZE 1024u
+#define TANS_LOG 10u
+
+/* tans.rs:85-99: weight w of symbol s fills w table slots, visited with the
+ * odd stride 615 (3 * 1024 / 5 made odd), so every slot is written once. */
+static void tans_spread(const uint16_t *w, const uint8_t *syms, int num, uint8_t *table) {
+    uint32_t stride = (3u * TANS_SIZE) / 5u;
+    if (!(stride & 1u)) stride++;
+    uint32_t step = 0;
+    for (int s = 0; s < num; s++)
+        for (uint32_t k = 0; k < w[s]; k++, step++) table[(stride * step) & (TANS_SIZE - 1u)] = syms[s];
+}
+
+/* tans.rs:28-78: f32 weights, one extra table slot per symbol kept back and
+ * the rest shared by (count * 1024 / total - 1); then +-1 round-robin nudges
+ * (at most 8 * num + 16 each way) to a sum of exactly 1024, else no coder. */
+static int tans_quantize(const uint32_t *counts, const uint8_t *syms, int num, uint64_t total, uint16_t *w) {
+    if (num <= 0 || num > 256) return 0;
+    float mult = total ? (float)TANS_SIZE / (float)total : 0.0f;
+    float want[256], want_sum = 0.0f;
+    for (int i = 0; i < num; i++) {
+        float x = (float)counts[syms[i]] * mult - 1.0f;
+        if (x < 0.0f) x = 0.0f;
+        want[i] = x;
+        want_sum += x;
+    }
+    float share = want_sum > 0.0f ? ((float)TANS_SIZE - (float)num) / want_sum : 0.0f;
+    int64_t sum = 0;
+    for (int i = 0; i < num; i++) {
+        float x = 1.0f + want[i] * share + 0.5f;
+        uint16_t q = x >= 65535.0f ? 65535 : (uint16_t)x;
+        w[i] = q ? q : 1;
+        sum += w[i];
+    }
+    int guard = num * 8 + 16, i = 0;
+    for (; sum > (int64_t)TANS_SIZE && guard > 0; guard--, i = (i + 1) % num)
+        if (w[i] > 1) {
+            w[i]--;
+            sum--;
+        }
+    guard = num * 8 + 16;
+    i = 0;
+    for (; sum < (int64_t)TANS_SIZE && guard > 0; guard--, i = (i + 1) % num) {
+        w[i]++;
+        sum++;
+    }
+    return sum == (int64_t)TANS_SIZE;
+}
+
+/* tans.rs:108-191.  Returns 0 (no stream) for empty input or when the weights
+ * cannot be made to sum to 1024. */
+static int tans_compress(const uint8_t *src, size_t n, buf_t *out) {
+    if (n == 0) return 0;
+    uint32_t counts[256] = {0};
+    for (size_t i = 0; i < n; i++) counts[src[i]]++;
+    uint8_t syms[256];
+    int num = 0, slot[256];
+    for (int b = 0; b < 256; b++)
+        if (counts[b]) {
+            slot[b] = num;
+            syms[num++] = (uint8_t)b;
+        }
+    uint16_t w[256];
+    if (!tans_quantize(counts, syms, num, n, w)) return 0;
+    uint8_t table[TANS_SIZE];
+    tans_spread(w, syms, num, table);
+    /* per symbol: the renormalisation bit count (min_bits, +1 at or above
+     * cutoff) and the first of its next-state entries (start) */
+    uint32_t cutoff[256] = {0}, start[256] = {0}, fill[256];
+    uint8_t min_bits[256] = {0};
+    uint32_t cum = 0;
+    for (int s = 0; s < num; s++) {
+        uint32_t top = 2u * w[s] - 1u, lg = 0;
+        while ((top >> lg) > 1u) lg++;
+        min_bits[syms[s]] = (uint8_t)(TANS_LOG - lg);
+        cutoff[syms[s]] = (2u * w[s]) << (TANS_LOG - lg);
+        start[syms[s]] = cum;
+        fill[s] = cum;
+        cum += w[s];
+    }
+    uint32_t next[TANS_SIZE];
+    for (uint32_t i = 0; i < TANS_SIZE; i++) next[fill[slot[table[i]]]++] = TANS_SIZE + i;
+    /* encode last symbol first; the bits of symbol k go out in symbol order */
+    uint16_t *low = (uint16_t *)malloc(n * sizeof(uint16_t));
+    uint8_t *nb = (uint8_t *)malloc(n);
+    uint32_t state = TANS_SIZE;
+    for (size_t k = n; k-- > 0;) {
+        uint8_t c = src[k];
+        uint32_t bits = min_bits[c] + (state >= cutoff[c] ? 1u : 0u);
+        low[k] = (uint16_t)(bits ? (state & ((1u << bits) - 1u)) : 0u);
+        nb[k] = (uint8_t)bits;
+        state = next[start[c] + (state >> bits) - w[slot[c]]];
+    }
+    b_varint(out, n);
+    b_push(out, (uint8_t)(num - 1));
+    b_write(out, syms, (size_t)num);
+    for (int s = 0; s < num; s++) b_u16(out, w[s]);
+    b_u32(out, state);
+    uint64_t acc = 0;
+    unsigned have = 0;
+    for (size_t k = 0; k < n; k++) {
+        if (!nb[k]) continue;
+        acc = (acc << nb[k]) | low[k];
+        have += nb[k];
+        while (have >= 8) {
+            have -= 8;
+            b_push(out, (uint8_t)(acc >> have));
+        }
+        acc &= (1ull << have) - 1ull;
+    }
+    if (have) b_push(out, (uint8_t)(acc << (8 - have)));
+    free(low);
+    free(nb);
+    return 1;
+}
+
+/* tans.rs:193-283: header checks in the reference's order, then one table
+ * lookup and one MSB-first bit read per byte; reads past the end give 0. */
+static int tans_decompress(const uint8_t *p, size_t plen, size_t max_len, buf_t *out) {
+    size_t pos = 0;
+    uint64_t len;
+    int rc = varint_read(p, plen, &pos, &len);
+    if (rc) return rc;
+    if (len > max_len) return OQ_CORRUPT;
+    if (pos >= plen) return OQ_TRUNCATED;
+    int num = p[pos++] + 1;
+    if (plen - pos < (size_t)num) return OQ_TRUNCATED;
+    const uint8_t *syms = p + pos;
+    pos += (size_t)num;
+    uint16_t w[256];
+    for (int s = 0; s < num; s++) {
+        if (plen - pos < 2) return OQ_TRUNCATED;
+        w[s] = (uint16_t)(p[pos] | (p[pos + 1] << 8));
+        pos += 2;
+    }
+    if (plen - pos < 4) return OQ_TRUNCATED;
+    uint32_t state = (uint32_t)p[pos] | ((uint32_t)p[pos + 1] << 8) | ((uint32_t)p[pos + 2] << 16) |
+                     ((uint32_t)p[pos + 3] << 24);
+    pos += 4;
+    if (state < TANS_SIZE || state >= 2u * TANS_SIZE) return OQ_CORRUPT;
+    uint8_t seen[256] = {0};
+    uint32_t wsum = 0;
+    for (int s = 0; s < num; s++) {
+        if (!w[s] || seen[syms[s]]) return OQ_CORRUPT;
+        seen[syms[s]] = 1;
+        wsum += w[s];
+    }
+    if (wsum != TANS_SIZE) return OQ_CORRUPT;
+    uint8_t table[TANS_SIZE], bits_of[TANS_SIZE];
+    uint16_t base_of[TANS_SIZE];
+    tans_spread(w, syms, num, table);
+    /* the k-th slot of a symbol of weight w continues from x = w + k: it
+     * reads enough bits to bring x << bits into [1024, 2048) */
+    uint32_t x[256] = {0};
+    for (int s = 0; s < num; s++) x[syms[s]] = w[s];
+    for (uint32_t i = 0; i < TANS_SIZE; i++) {
+        uint32_t b = x[table[i]]++;
+        if (!b) return OQ_CORRUPT;
+        uint32_t bits = (uint32_t)(__builtin_clz(b) - __builtin_clz(TANS_SIZE));
+        base_of[i] = (uint16_t)((b << bits) - TANS_SIZE);
+        bits_of[i] = (uint8_t)bits;
+    }
+    const uint8_t *in = p + pos;
+    size_t inlen = plen - pos, ip = 0;
+    uint64_t acc = 0;
+    unsigned have = 0;
+    b_reserve(out, (size_t)len);
+    for (uint64_t k = 0; k < len; k++) {
+        uint32_t idx = state - TANS_SIZE;
+        if (idx >= TANS_SIZE) return OQ_CORRUPT;
+        uint32_t bits = bits_of[idx], extra = 0;
+        if (bits) {
+            while (have < bits) {
+                acc = (acc << 8) | (ip < inlen ? in[ip] : 0u);
+                ip++;
+                have += 8;
+            }
+            have -= bits;
+            extra = (uint32_t)(acc >> have) & ((1u << bits) - 1u);
+            acc &= (1ull << have) - 1ull;
+        }
+        out->p[out->len++] = table[idx];
+        state = TANS_SIZE + base_of[idx] + extra;
+    }
+    return OQ_OK;
+}
+
+/* entropy/mod.rs:152-163: tag 2 rANS, tag 0 the range coder, tag 1 tANS. */
 static int decode_entropy_only(const uint8_t *p, size_t plen, size_t max_len, buf_t *out) {
     if (plen == 0) return OQ_TRUNCATED;
     switch (p[0]) {
         case TAG_RANS: return rans_decompress(p + 1, plen - 1, max_len, out);
         case TAG_RC: return rc_decompress(p + 1, plen - 1, max_len, out);
-        case TAG_TANS: return OQ_UNSUPPORTED;
+        case TAG_TANS: return tans_decompress(p + 1, plen - 1, max_len, out);
         default: return OQ_CORRUPT;
     }
 }
@@ -3128,8 +3322,24 @@ int oq_encode_mode(int mode, const uint64_t *v, size_t n, int dtype, int level, 
     return OQ_OK;
 }
 
+/* `tag` ++ the bytes coded by the range coder (0), tANS (1) or rANS (2).
+ * 0 when that coder makes no stream for these bytes. */
+static int code_tagged(const uint8_t *r, size_t n, int tag, buf_t *b) {
+    b_push(b, (uint8_t)tag);
+    if (tag == TAG_RC) {
+        rc_compress(r, n, b);
+        return 1;
+    }
+    if (tag == TAG_TANS) return tans_compress(r, n, b);
+    if (tag == TAG_RANS && n) {
+        rans_compress(r, n, b);
+        return 1;
+    }
+    return 0;
+}
+
 /* A High / Max linear-mode payload (linear.rs) with the residual bytes coded
- * by `tag` (TAG_RC or TAG_RANS, entropy/mod.rs:24-29); order 0 picks it as
+ * by `tag` (TAG_RC, TAG_TANS or TAG_RANS, entropy/mod.rs:24-29); order 0 picks it as
  * the reference's encoder does (linear.rs:121-140).  *out = NULL when
  * DELTA_DP does not apply. */
 int oq_linear_payload(int mode, const uint64_t *v, size_t n, int order, int tag, uint8_t **out, size_t *out_len) {
@@ -3149,14 +3359,9 @@ int oq_linear_payload(int mode, const uint64_t *v, size_t n, int order, int tag,
     } else {
         return OQ_UNSUPPORTED;
     }
-    if (tag == TAG_RC) {
-        b_push(&b, TAG_RC);
-        rc_compress(r.p, r.len, &b);
-    } else if (tag == TAG_RANS && r.len) {
-        b_push(&b, TAG_RANS);
-        rans_compress(r.p, r.len, &b);
-    } else {
+    if (!code_tagged(r.p, r.len, tag, &b)) {
         b_free(&r);
+        b_free(&b);
         return OQ_UNSUPPORTED;
     }
     b_free(&r);
@@ -3169,7 +3374,7 @@ int oq_linear_select_order(const uint64_t *v, size_t n) { return lin_select_orde
 
 /* A PRED (0, LEB128 residuals), PRED_RC (29) or PRED2 (25) frame payload
  * (codecs/pred.rs) at predictor_log2 plog2; the residual bytes of 29 and 25
- * are coded by `tag` (TAG_RC or TAG_RANS). */
+ * are coded by `tag` (TAG_RC, TAG_TANS or TAG_RANS). */
 int oq_pred_payload(int mode, const uint64_t *v, size_t n, int plog2, int tag, uint8_t **out, size_t *out_len) {
     buf_t r = {0}, b = {0};
     *out = NULL;
@@ -3183,18 +3388,39 @@ int oq_pred_payload(int mode, const uint64_t *v, size_t n, int plog2, int tag, u
         *out_len = r.len;
         return OQ_OK;
     }
-    if (tag == TAG_RC) {
-        b_push(&b, TAG_RC);
-        rc_compress(r.p, r.len, &b);
-    } else if (tag == TAG_RANS && r.len) {
-        b_push(&b, TAG_RANS);
-        rans_compress(r.p, r.len, &b);
-    } else {
+    if (!code_tagged(r.p, r.len, tag, &b)) {
         b_free(&r);
+        b_free(&b);
         return OQ_UNSUPPORTED;
     }
     b_free(&r);
     *out = b.p;
+    *out_len = b.len;
+    return OQ_OK;
+}
+
+/* tans.rs compress_bytes / decompress_bytes (the coded bytes, no tag);
+ * oq_tans_compress gives OQ_UNSUPPORTED where the reference returns None. */
+int oq_tans_compress(const uint8_t *data, size_t n, uint8_t **out, size_t *out_len) {
+    buf_t b = {0};
+    *out = NULL;
+    *out_len = 0;
+    if (!tans_compress(data, n, &b)) {
+        b_free(&b);
+        return OQ_UNSUPPORTED;
+    }
+    *out = b.p;
+    *out_len = b.len;
+    return OQ_OK;
+}
+int oq_tans_decompress(const uint8_t *src, size_t len, size_t max_len, uint8_t **out, size_t *out_len) {
+    buf_t b = {0};
+    int rc = tans_decompress(src, len, max_len, &b);
+    if (rc) {
+        b_free(&b);
+        return rc;
+    }
+    *out = b.p ? b.p : (uint8_t *)malloc(1);
     *out_len = b.len;
     return OQ_OK;
 }

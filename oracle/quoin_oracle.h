@@ -115,7 +115,7 @@ int oq_decompress_column_mt(const uint8_t *src, size_t len, int threads, int *dt
 
 /* High / Max linear modes (src/codecs/linear.rs): a frame payload of mode 7
  * (ORDERED_DELTA), 20 (DELTA2) or 45 (DELTA_DP) with the residual bytes coded
- * by tag 0 (range coder) or 2 (rANS); order 0 = the reference's choice.
+ * by tag 0 (range coder), 1 (tANS) or 2 (rANS); order 0 = the reference's choice.
  * *out = NULL when DELTA_DP does not apply to the values. */
 int oq_linear_payload(int mode, const uint64_t *vals, size_t n, int order, int tag,
                       uint8_t **out, size_t *out_len);
@@ -125,6 +125,10 @@ int oq_linear_payload(int mode, const uint64_t *vals, size_t n, int order, int t
 int oq_pred_payload(int mode, const uint64_t *vals, size_t n, int plog2, int tag,
                     uint8_t **out, size_t *out_len);
 uint32_t oq_crc32c_u64(uint32_t crc, uint64_t v);
+/* tANS (src/entropy/tans.rs, entropy tag 1): the coded bytes without the tag. */
+int oq_tans_compress(const uint8_t *data, size_t n, uint8_t **out, size_t *out_len);
+int oq_tans_decompress(const uint8_t *src, size_t len, size_t max_len, uint8_t **out,
+                       size_t *out_len);
 /* The LZ stream of src/codecs/lz.rs (lz_compress / lz_decompress). */
 int oq_lz_compress(const uint8_t *data, size_t n, uint8_t **out, size_t *out_len);
 int oq_lz_decompress(const uint8_t *stream, size_t len, size_t expected, uint8_t **out,

@@ -1178,6 +1178,99 @@ __device__ __noinline__ uint32_t rc_decode_cta(DecSmem& S, const uint8_t* p, uin
   return e;
 }
 
+// tANS (tans.rs:193-283, entropy tag 1, still decoded by the reference):
+// varint(len) ++ u8(distinct - 1) ++ symbols ++ u16 LE weights (each >= 1,
+// symbols distinct, sum 1024) ++ u32 LE state in [1024, 2048) ++ MSB-first
+// renormalisation bits (reads past the end give 0).  Symbol s of weight w
+// takes w of the 1,024 table slots, visited with the odd stride 615; the k-th
+// slot of s continues from x = w + k and reads the bits that bring x << bits
+// into [1024, 2048).  A legacy tag, so thread 0 builds the table (in the
+// frame's range-coder model area) and decodes; every loop is bounded by 1024
+// or by the declared length.
+__device__ __noinline__ uint32_t tans_decode_cta(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t max_len,
+                                                 uint8_t* out, uint64_t cap, uint64_t* len_out) {
+  if (!S.rcm) return E_NO_ENTROPY_AREA;
+  if (threadIdx.x == 0) {
+    uint32_t* node = reinterpret_cast<uint32_t*>(S.rcm);  // base | bits << 16 | symbol << 24
+    uint8_t* table = reinterpret_cast<uint8_t*>(node + 1024);
+    uint32_t* x = reinterpret_cast<uint32_t*>(table + 1024);  // per symbol
+    uint64_t pos = 0, len = 0;
+    uint32_t e = rd_varint(p, plen, &pos, &len);
+    if (!e && (len > max_len || len > cap)) e = E_CORRUPT;
+    uint32_t num = 0, state = 0;
+    uint64_t syms = 0, wts = 0;
+    if (!e) {
+      if (pos >= plen) e = E_TRUNCATED;
+      else num = p[pos++] + 1u;
+    }
+    if (!e) {
+      if (plen - pos < num) e = E_TRUNCATED;
+      syms = pos;
+      pos += num;
+    }
+    if (!e) {
+      if (plen - pos < 2ull * num) e = E_TRUNCATED;
+      wts = pos;
+      pos += 2ull * num;
+    }
+    if (!e) {
+      if (plen - pos < 4) e = E_TRUNCATED;
+      else state = ld_u32(p + pos);
+      pos += 4;
+    }
+    if (!e && (state < 1024u || state >= 2048u)) e = E_CORRUPT;
+    if (!e) {
+      uint32_t seen[8] = {0, 0, 0, 0, 0, 0, 0, 0}, wsum = 0;
+      for (uint32_t s = 0; s < num && !e; s++) {
+        uint32_t sym = p[syms + s], w = p[wts + 2 * s] | ((uint32_t)p[wts + 2 * s + 1] << 8);
+        if (w == 0 || ((seen[sym >> 5] >> (sym & 31)) & 1u)) e = E_CORRUPT;
+        seen[sym >> 5] |= 1u << (sym & 31);
+        wsum += w;
+      }
+      if (!e && wsum != 1024u) e = E_CORRUPT;
+    }
+    if (!e) {
+      uint32_t step = 0;
+      for (uint32_t s = 0; s < num; s++) {
+        uint32_t sym = p[syms + s], w = p[wts + 2 * s] | ((uint32_t)p[wts + 2 * s + 1] << 8);
+        x[sym] = w;
+        for (uint32_t k = 0; k < w; k++, step++) table[(615u * step) & 1023u] = (uint8_t)sym;
+      }
+      for (uint32_t i = 0; i < 1024u; i++) {
+        uint32_t sym = table[i], b = x[sym]++;
+        uint32_t bits = (uint32_t)(__clz(b) - __clz(1024u));
+        node[i] = ((b << bits) - 1024u) | (bits << 16) | (sym << 24);
+      }
+      const uint8_t* in = p + pos;
+      uint64_t inlen = plen - pos, ip = 0, acc = 0;
+      uint32_t have = 0;
+      for (uint64_t k = 0; k < len; k++) {
+        uint32_t nd = node[state - 1024u];
+        uint32_t bits = (nd >> 16) & 0xFFu, extra = 0;
+        if (bits) {
+          while (have < bits) {
+            acc = (acc << 8) | (ip < inlen ? in[ip] : 0u);
+            ip++;
+            have += 8;
+          }
+          have -= bits;
+          extra = (uint32_t)(acc >> have) & ((1u << bits) - 1u);
+          acc &= (1ull << have) - 1ull;
+        }
+        out[k] = (uint8_t)(nd >> 24);
+        state = 1024u + (nd & 0xFFFFu) + extra;  // < 2048 for a table built from valid weights
+      }
+    }
+    S.sc[2] = e ? 0 : len;
+    S.flag = e;
+  }
+  __syncthreads();
+  uint32_t e = S.flag;
+  *len_out = S.sc[2];
+  __syncthreads();
+  return e;
+}
+
 // LZ tokens (lz.rs:119-155): varint(length) (== expected, else E_CORRUPT),
 // then groups of a control byte (8 flags, MSB first) and 8 tokens: a match
 // (varint offset, varint length - 4; overlapping copies allowed) or a
@@ -1208,8 +1301,7 @@ __device__ uint32_t lz_decode(const uint8_t* p, uint64_t len, uint64_t expected,
   return E_OK;
 }
 
-// entropy/mod.rs:152-163: tag 2 rANS, tag 0 the range coder; the legacy tANS
-// tag (decoded by the reference, never produced) is not decoded here.
+// entropy/mod.rs:152-163: tag 2 rANS, tag 0 the range coder, tag 1 tANS.
 __device__ uint32_t entropy_only_cta(DecSmem& S, const uint8_t* p, uint64_t plen, uint64_t max_len, uint8_t* out,
                                      uint64_t cap, uint64_t* len_out) {
   *len_out = 0;
@@ -1217,7 +1309,7 @@ __device__ uint32_t entropy_only_cta(DecSmem& S, const uint8_t* p, uint64_t plen
   uint32_t tag = p[0];
   if (tag == 2) return rans_decode_cta(S, p + 1, plen - 1, max_len, out, cap, len_out);
   if (tag == 0) return rc_decode_cta(S, p + 1, plen - 1, max_len, out, cap, len_out);
-  if (tag == 1) return E_UNSUPPORTED;
+  if (tag == 1) return tans_decode_cta(S, p + 1, plen - 1, max_len, out, cap, len_out);
   return E_CORRUPT;
 }
 

@@ -211,13 +211,14 @@ def test_rans_part_errors_match_oracle(qb, oracle):
     kinds = []
     # tag 0 re-reads the rANS bytes as range-coder input, which only fails on
     # its declared length (here the same n, so both decoders give the same
-    # garbage values); tANS -> Unsupported; tag 3 reads them as an LZ cascade,
-    # whose inner stream fails; others -> CorruptPayload
+    # garbage values); tag 1 reads them as a tANS header, whose weights do not
+    # sum to 1024; tag 3 reads them as an LZ cascade, whose inner stream fails;
+    # others -> CorruptPayload
     for tag in (0, 1, 3, 4, 255):
         b = bytearray(s)
         b[off] = tag
         kinds.append(_agree(qb, oracle, bytes(b)))
-    assert kinds == ["ok", "Unsupported"] + ["CorruptPayload"] * 3
+    assert kinds == ["ok"] + ["CorruptPayload"] * 4
     _, n_end = _varint(p, 1)  # payload offset of varint(number of symbols)
     b = bytearray(s)
     b[off + n_end] = 0  # zero symbols
