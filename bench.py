@@ -60,10 +60,11 @@ WORKLOADS = {
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture) of
 # one decode of the workload's three columns at 16,777,216 values each, summed
-# over k_walk_frames, k_prepass, k_prepass_scan and k_decode_items; reported
+# over k_walk_frames, k_prepass, k_prepass_scan, k_decode_items,
+# k_decode_frames and k_decimal_combine; reported
 # scaled by the values per column.  Lines still dirty in L2 when a launch ends
 # are not counted, so the figure is a lower bound on the written share.
-DECODE_TRAFFIC_16M = {"integer-lanes": 388_141_056}
+DECODE_TRAFFIC_16M = {"integer-lanes": 388_141_056, "float-lanes": 1_085_646_080}
 
 
 def decimal_args(wire):
@@ -542,7 +543,8 @@ def run_gpu(args, rank, world, local):
             "kernel_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in per_class.items()},
             "per_column_ms": per_column,
             "roofline": {"bound": "hbm", "kernel": "decode (k_walk_frames, k_prepass, k_prepass_scan, "
-                                                   "k_decode_items of the three columns in flight together)",
+                                                   "k_decode_items, k_decode_frames, k_decimal_combine of the "
+                                                   "three columns in flight together)",
                          "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": (round(DECODE_TRAFFIC_16M[args.workload] * n / (1 << 24))
