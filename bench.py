@@ -67,10 +67,34 @@ WORKLOADS = {
 DECODE_TRAFFIC_16M = {"integer-lanes": 388_141_056, "float-lanes": 1_085_646_080}
 
 
+DECIMAL128_WIRE = 6  # wire dtype id of Decimal128 (reference src/dtype.rs:68-93)
+
+
 def decimal_args(wire):
     """(scale, precision) of the benchmark's decimal columns; (0, 0) otherwise."""
-    from quoin_b200 import DECIMAL128
-    return (4, 18) if wire == DECIMAL128 else (0, 0)
+    return (4, 18) if wire == DECIMAL128_WIRE else (0, 0)
+
+
+def load_synth():
+    """The column generators (quoin_b200/synth.py), loaded by path: importing
+    the package would load the CUDA library, which the CPU reference arm must
+    not touch."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("qb_synth", os.path.join(ROOT, "quoin_b200", "synth.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def dist_env():
@@ -183,9 +207,11 @@ def cpu_reference_run(cols, threads: int, sample: int):
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    from quoin_b200 import synth
+    synth = load_synth()
     threads = os.cpu_count() or 1
-    sample = args.cpu_sample
+    # the GPU arm's workload: whole columns (batched / served: an equal share
+    # of --cpu-sample per column)
+    sample = args.cpu_sample if args.workload in ("batched", "served") else args.n
     if args.workload in ("batched", "served"):  # the columns, each cut to an equal share of the sample
         cols = (synth.mixed_columns(args.columns, args.max_len) if args.workload == "batched"
                 else synth.request_columns(args.columns4, args.max_bytes))
@@ -210,6 +236,11 @@ def run_reference(args, rank, world):
         e_s += e
         d_s += d
     gbs = tot_b / tot_s / 1e9
+    # one host thread on a bounded part of the same columns, beside the
+    # all-core figure
+    one = max(min(args.single_thread_sample, sample), 1)
+    cols1 = [(nm, dt, v[:one], None if bm is None else bm[: (min(len(v), one) + 7) // 8]) for nm, dt, v, bm in cols]
+    b1, e1, d1 = cpu_reference_run(cols1, 1, one)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(gbs, 4), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot_s / args.steps * 1e3, 3),
@@ -218,8 +249,14 @@ def run_reference(args, rank, world):
         "config": {"workload": wl[1], "values_per_column": sample, "columns": len(cols)},
         "encode_gbs": round(tot_b / e_s / 1e9, 4), "decode_gbs": round(tot_b / d_s / 1e9, 4),
         "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": f"first {sample} values of each {args.workload} column, oracle C restatement, "
-                                   f"{threads} threads over plan_blocks ranges / frames"},
+                         "sample": (f"the whole {args.workload} columns ({sample} values each)"
+                                    if sample == args.n and args.workload not in ("batched", "served") else
+                                    f"first {sample} values of each {args.workload} column")
+                                   + f", oracle C restatement, {threads} threads over plan_blocks ranges / frames",
+                         "cpu_model": cpu_model(),
+                         "single_thread": {"value": round(b1 / (e1 + d1) / 1e9, 4), "unit": "GB/s",
+                                           "encode_gbs": round(b1 / e1 / 1e9, 4), "decode_gbs": round(b1 / d1 / 1e9, 4),
+                                           "sample": f"first {one} values of each column, 1 thread"}},
         "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the Rust reference cannot be built here (no cargo, unvendored crates); its CPU path is timed "
                 "through the repository's C restatement of the same algorithm",
@@ -899,7 +936,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="values per column")
-    ap.add_argument("--cpu-sample", type=int, default=1 << 24)
+    ap.add_argument("--cpu-sample", type=int, default=1 << 24,
+                    help="values per column of the GPU arm's cpu_baseline leg (and of the batched / served "
+                         "reference arm)")
+    ap.add_argument("--single-thread-sample", type=int, default=1 << 21,
+                    help="reference arm: values per column of the one-thread run")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-lanes", type=int, default=1,
                     help="e2e: compress/decompress pipelines per column (each its own contexts and buffers)")

@@ -225,11 +225,15 @@ int quoin_b200_decompress_indexed_device(QuoinCtx *ctx, const QuoinDecodeIndex *
  * device memory through its own pool, or a process that must keep a fixed
  * footprint): decodes the device-resident stream d_src[0 .. src_len) into
  * d_values_out (8-byte aligned, room for out_cap_values values) using only a
- * fixed scratch arena compiled into the library (about 2.5 MB per device), and
- * writes the value count to *n_out.  Limits: at most 262,144 values and 256
- * frames, dtype f64/i64/u64, no validity bitmap; other streams are rejected
- * with QUOIN_ERR_NOALLOC_LIMIT (QUOIN_ERR_BUFFER_TOO_SMALL when n exceeds
- * out_cap_values).  The caller zeroes nothing: each call resets the arena.
+ * fixed scratch arena compiled into the library (2,433,088 bytes per device),
+ * and writes the value count to *n_out.  Limits: at most 262,144 values and
+ * 256 frames, dtype f64/i64/u64, no validity bitmap; other streams, and frames
+ * with an entropy-coded part (levels above Fast), are rejected with
+ * QUOIN_ERR_NOALLOC_LIMIT.  When n exceeds out_cap_values the call returns
+ * QUOIN_ERR_BUFFER_TOO_SMALL with the needed count in *n_out; on every other
+ * nonzero return *n_out is 0 and the contents of d_values_out are
+ * unspecified (frames before a corrupt one may have been written).  The
+ * caller zeroes nothing: each call resets the arena.
  * Calls on one device share the arena, so calls that overlap in time race and
  * must be serialised by the caller.  The first call on each device looks the
  * arena up (and may load the module); make it before any stream capture.

@@ -51,6 +51,9 @@ struct NoAllocArena {
   uint8_t aux[kNoAllocMaxFrames * kNoAllocAuxBytes];
   uint64_t dict[kNoAllocMaxValues];  // decode scratch (large dictionaries, RLE run ends, ALP-RD), one slot per value
 };
+// The arena's footprint on every device that loads the library (quoted in
+// include/quoin.h): 64 + 256 x 32 + 256 x 1,280 + 262,144 x 8 bytes.
+static_assert(sizeof(NoAllocArena) == 2433088, "documented arena size");
 
 static __device__ __align__(256) NoAllocArena g_noalloc_arena;
 
@@ -76,8 +79,8 @@ __global__ void k_noalloc_parse(const uint8_t* __restrict__ s, uint64_t len, uin
   A->st.err = ~0ull;
   do {
     if (len < 16) { kind = E_TRUNCATED; break; }
-    if (len > 5 && (s[5] & 2)) { kind = kLimit; break; }  // decimal container
     if (s[0] != 'F' || s[1] != 'C' || s[2] != 'R' || s[3] != '1') { kind = E_BAD_MAGIC; break; }
+    if (s[5] & 2) { kind = kLimit; break; }  // decimal container
     if (s[4] != 2) { kind = E_UNSUPPORTED_VERSION; break; }
     if (s[5] & ~1u) { kind = E_CORRUPT; break; }
     if (s[6] < 10 || s[6] > 16) { kind = E_CORRUPT; break; }
@@ -189,6 +192,7 @@ extern "C" int quoin_b200_decompress_device_noalloc(const uint8_t* d_src, size_t
       return QUOIN_ERR_CUDA;
     }
     if (cudaGetLastError() != cudaSuccess) return QUOIN_ERR_CUDA;
+    if (hs.kind == kLimit + 1) *n_out = hs.n;  // the count the buffer needs
     if (hs.kind) return kind_code(hs.kind);
     if (hs.err != ~0ull) return kind_code((uint32_t)(hs.err & 0xFF));
     *n_out = hs.n;

@@ -10,7 +10,11 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import DECIMAL128, F32, F64, I32, I64, U32, U64
+# Wire dtype ids of the stream header (reference src/dtype.rs:68-93), the same
+# values as the package's constants.  Defined here so the generators load
+# without the CUDA library (the CPU reference arm of the benchmark imports
+# this file by path).
+F64, I64, U64, I32, U32, F32, DECIMAL128, DECIMAL256 = range(8)
 
 BASE_SEED = 20261203
 

@@ -112,10 +112,35 @@ def test_noalloc_rejects_streams_outside_its_limits(qb, api):
     assert run(many_frames, 300) == ERR_NOALLOC_LIMIT
     ok = qb.compress_column(np.arange(1000, dtype=np.int64) * 3, None, qb.Config(), dtype=I64)
     assert run(ok, 999) == ERR_BUFFER_TOO_SMALL
+    d_ok = torch.from_numpy(np.frombuffer(ok, np.uint8).copy()).cuda()
+    assert noalloc(api, d_ok, len(ok), d_out, 999) == (ERR_BUFFER_TOO_SMALL, 1000)  # the count it needs
     assert run(b"XCR1" + ok[4:], 1000) == ERR_BAD_MAGIC
+    # not a stream, with the decimal-container bit set: the magic is checked first
+    assert run(b"ABCD\x02\x02" + ok[6:], 1000) == ERR_BAD_MAGIC
     assert run(ok[:20], 1000) == ERR_TRUNCATED
     # the arena is reset by every call: a good stream decodes after the errors
     d_src = torch.from_numpy(np.frombuffer(ok, np.uint8).copy()).cuda()
     rc, n = noalloc(api, d_src, len(ok), d_out, 1000)
     assert rc == 0 and n == 1000
     assert np.array_equal(d_out[:1000].cpu().numpy(), np.arange(1000, dtype=np.int64) * 3)
+
+
+def test_noalloc_rejects_entropy_coded_frames_while_decoding(qb, api):
+    """A stream inside the size limits whose frames carry an entropy-coded part
+    (Balanced: byte-transposed rANS planes) passes the frame-table check and
+    is refused by the decode kernels, which have no area for the coded part in
+    the fixed arena; the next call still decodes a good stream."""
+    _, torch = api
+    rng = np.random.default_rng(20240611)
+    b = np.minimum(rng.geometric(0.3, (60000, 6)) - 1, 255).astype(np.uint64)
+    vals = (b << (np.arange(6, dtype=np.uint64) * np.uint64(8))).sum(axis=1, dtype=np.uint64)
+    coded = qb.compress_column(vals, None, qb.Config(level=qb.Level.BALANCED_INPOOL), dtype=U64)
+    assert coded[16] == 11  # the first frame is BYTE_TRANSPOSE
+    d_out = torch.zeros(60000, dtype=torch.int64, device="cuda")
+    d_src = torch.from_numpy(np.frombuffer(coded, np.uint8).copy()).cuda()
+    assert noalloc(api, d_src, len(coded), d_out, 60000) == (ERR_NOALLOC_LIMIT, 0)
+    ok = qb.compress_column(vals, None, qb.Config(level=qb.Level.FAST), dtype=U64)
+    d_src = torch.from_numpy(np.frombuffer(ok, np.uint8).copy()).cuda()
+    rc, n = noalloc(api, d_src, len(ok), d_out, 60000)
+    assert rc == 0 and n == 60000
+    assert d_out.cpu().numpy().view(np.uint64).tobytes() == vals.tobytes()
