@@ -220,6 +220,24 @@ int quoin_b200_decompress_indexed_device(QuoinCtx *ctx, const QuoinDecodeIndex *
                                          const uint8_t *d_src, void *d_values_out,
                                          uint8_t *d_validity_out, void *stream);
 
+/* Decode a device-resident stream d_src[0 .. src_len) into device memory
+ * (replaces decompress_column, src/lib.rs:462-508, for a caller whose stream
+ * is already on the GPU; the reader is src/decoder.rs:43-118 and
+ * src/format.rs:65-94).  The header, the validity blob and the frame table
+ * are read on the device, so the host never copies the stream (streams the
+ * device reader does not take, such as damaged ones or an RLE validity blob,
+ * are read from a host copy by the host reader, with the same error codes).
+ * d_values_out receives n values of the stream's native width (nulls as 0),
+ * values_cap_bytes being its size; d_validity_out (optional) receives the
+ * ceil(n/8)-byte bitmap when the stream has one.  *wire_out and *n_out get
+ * the stream's dtype and value count (also with QUOIN_ERR_BUFFER_TOO_SMALL).
+ * `stream` is a cudaStream_t (NULL = the context's stream); the call returns
+ * after the decode completed. */
+int quoin_b200_decompress_column_device(QuoinCtx *ctx, const uint8_t *d_src, size_t src_len,
+                                        void *d_values_out, size_t values_cap_bytes,
+                                        uint8_t *d_validity_out, int32_t *wire_out, uint64_t *n_out,
+                                        void *stream);
+
 /* No counterpart in the reference.  Allocation-free device decode for callers
  * that cannot let the library allocate device memory (an engine that owns all
  * device memory through its own pool, or a process that must keep a fixed

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libquoin_b200.so")
 
-SOURCES = ["qb_decode.cu", "qb_encode.cu", "qb_lower.cu", "qb_noalloc.cu", "qb_host.cpp", "qb_arrow.cpp", "qb_batch.cpp",
+SOURCES = ["qb_decode.cu", "qb_dparse.cu", "qb_encode.cu", "qb_lower.cu", "qb_noalloc.cu", "qb_host.cpp", "qb_arrow.cpp", "qb_batch.cpp",
            "qb_serve.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

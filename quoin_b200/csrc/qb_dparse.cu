@@ -1,0 +1,571 @@
+// Device-side stream reader: the header, the validity blob and the frame
+// table of a device-resident stream (reference src/format.rs:65-94,
+// src/decoder.rs:43-118, src/decimal.rs:100-168), so a column decodes from
+// device memory without the host ever holding the stream.
+//
+// The frame table is a chain: frame k+1 starts 9 + plen_k bytes after frame
+// k, and the walk stops once the frames hold the lane's value count.  One
+// thread following it pays one memory latency per frame (thousands per
+// column), so the chain is resolved in parallel instead:
+//   1. every byte position of a lane whose 9 bytes could be a frame header
+//      (mode id known, 1 <= n <= 131072, plen < 2^24 and within the lane) is a
+//      candidate: one pass over the lane, with a zero-byte test on 8-byte
+//      words that rejects almost every position in a few instructions
+//      (k_dp_cand_count, a scan, k_dp_cand_write, in position order);
+//   2. each candidate's successor (the candidate at pos + 9 + plen) is found
+//      by binary search; marks spread from the lane's first frame along the
+//      successors by pointer doubling, so after log2(K) rounds exactly the
+//      frames on the chain are marked (every jump from a chain frame lands on
+//      a chain frame), and chain order is position order (k_dp_chain);
+//   3. the marked frames are cut where their values reach the lane's count,
+//      and each frame's warp items (512 values, or 512 XORZ payload bytes)
+//      are counted and laid out as the host reader's build_items does
+//      (k_dp_chain), then listed (k_dp_expand).
+// A stream the fast path cannot take (a header or validity error, an RLE
+// validity blob, a chain frame that is not a candidate, a count mismatch,
+// more candidates than the tables hold) is flagged, and the host reader
+// parses a host copy instead, so every error kind stays the reference's.
+#include "qb_common.cuh"
+#include "qb_kernels.h"
+#include "qb_layout.h"
+#include "qb_scan.cuh"
+
+namespace qb {
+namespace {
+
+constexpr int kDpThreads = 256;
+constexpr uint64_t kDpChunk = (uint64_t)kDpThreads * 16;  // positions per candidate CTA
+constexpr int kChainThreads = 1024;
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint64_t kMaxLogicalD = 1ull << 36;  // the host reader's allocation limit (decoder.rs:105-106)
+
+__device__ inline bool dp_mode_known(uint32_t id) {  // reference mode.rs:60-84
+  switch (id) {
+    case 0: case 1: case 2: case 3: case 4: case 5: case 7: case 9: case 11: case 17:
+    case 19: case 20: case 25: case 29: case 45: case 50: case 51: case 52: case 53: case 54:
+      return true;
+    default: return false;
+  }
+}
+
+// One bit per byte of w (bit k for byte k): set where the byte is zero.
+__device__ __forceinline__ uint32_t zero_bytes8(uint64_t w) {
+  uint64_t t = (w & 0x7F7F7F7F7F7F7F7Full) + 0x7F7F7F7F7F7F7F7Full;
+  t = ~(t | w | 0x7F7F7F7F7F7F7F7Full);  // 0x80 in every zero byte, nothing else
+  return (uint32_t)(((t >> 7) * 0x0102040810204080ull) >> 56);
+}
+
+// ---------------------------------------------------------------------------
+// Header (one thread).  Any error, or a form the device reader leaves to the
+// host (an RLE validity blob, a limb lane with its own bitmap), sets kind = 1.
+// ---------------------------------------------------------------------------
+__device__ bool dp_lane_header(const uint8_t* s, uint64_t base, uint64_t len, DpLane& L) {
+  const uint8_t* h = s + base;
+  if (len < 16) return false;
+  if (h[0] != 'F' || h[1] != 'C' || h[2] != 'R' || h[3] != '1') return false;
+  if (h[4] != 2 || (h[5] & ~1u) || h[6] < 10 || h[6] > 16 || h[7] > 7) return false;
+  L.base = base;
+  L.len = len;
+  L.dtype = h[7];
+  L.plog2 = h[6];
+  L.has_validity = h[5] & 1;
+  L.logical_n = ld_u64(h + 8);
+  L.fstart = base + 16;
+  return L.logical_n <= kMaxLogicalD;
+}
+
+// The RAW validity blob at s[pos .. pos + vlen) (validity.rs:73-90): tag 0
+// then ceil(n/8) bytes.
+__device__ bool dp_validity(const uint8_t* s, uint64_t len, uint64_t* pos, uint64_t n, DpHead& H) {
+  uint64_t vlen;
+  if (rd_varint(s, len, pos, &vlen) != E_OK || vlen > len - *pos || vlen == 0) return false;
+  if (s[*pos] != 0) return false;  // RLE blob: the host reader decodes it
+  uint64_t raw = (n + 7) / 8;
+  if (vlen - 1 < raw) return false;
+  H.vblob_off = *pos + 1;
+  H.vblob_len = raw;
+  *pos += vlen;
+  return true;
+}
+
+__global__ void k_dp_head(const uint8_t* __restrict__ s, uint64_t len, DpHead* __restrict__ out) {
+  if (threadIdx.x || blockIdx.x) return;
+  DpHead H;
+  memset(&H, 0, sizeof(H));
+  H.kind = 1;
+  do {
+    if (len > 5 && (s[5] & 2)) {  // decimal container (decimal.rs:39-41, 100-168)
+      if (len < 19) break;
+      if (s[0] != 'F' || s[1] != 'C' || s[2] != 'R' || s[3] != '1' || s[4] != 2) break;
+      if (s[7] != DT_DEC128 && s[7] != DT_DEC256) break;
+      H.decimal = 1;
+      H.wire = s[7];
+      H.has_validity = s[5] & 1;
+      H.n = ld_u64(s + 8);
+      if (H.n > kMaxLogicalD) break;
+      H.scale = (int8_t)s[16];
+      H.precision = s[17];
+      uint32_t nl = s[18];
+      if (nl != (H.wire == DT_DEC128 ? 2u : 4u)) break;
+      uint64_t pos = 19 + 8ull * nl;
+      if (pos > len) break;
+      for (uint32_t k = 0; k < nl; k++) H.vmin[k] = ld_u64(s + 19 + 8 * k);
+      if (H.has_validity && !dp_validity(s, len, &pos, H.n, H)) break;
+      bool ok = true;
+      for (uint32_t k = 0; k < nl && ok; k++) {
+        uint64_t sl;
+        if (rd_varint(s, len, &pos, &sl) != E_OK || sl > len - pos) { ok = false; break; }
+        ok = dp_lane_header(s, pos, sl, H.lanes[k]) && !H.lanes[k].has_validity;
+        pos += sl;
+      }
+      if (!ok) break;
+      H.nl = nl;
+      H.kind = 0;
+    } else {
+      DpLane& L = H.lanes[0];
+      if (!dp_lane_header(s, 0, len, L)) break;
+      if (L.dtype == DT_DEC128 || L.dtype == DT_DEC256) break;  // lib.rs:503-505
+      H.wire = L.dtype;
+      H.n = L.logical_n;
+      H.has_validity = L.has_validity;
+      uint64_t pos = 16;
+      if (H.has_validity && !dp_validity(s, len, &pos, H.n, H)) break;
+      L.fstart = pos;
+      H.nl = 1;
+      H.kind = 0;
+    }
+  } while (false);
+  *out = H;
+}
+
+// Bitmap bytes of the RAW blob with the bits past n cleared, and the bytes
+// after it zeroed up to the next 8 (the popcount reads whole words).
+__global__ void k_dp_bitmap(const uint8_t* __restrict__ s, const DpHead* __restrict__ H, uint8_t* __restrict__ bm) {
+  uint64_t off = H->vblob_off, nb = H->vblob_len, n = H->n;
+  uint64_t end = (nb + 7) & ~7ull;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint8_t b = 0;
+    if (i < nb) {
+      b = s[off + i];
+      if (i == nb - 1 && (n & 7)) b &= (uint8_t)((1u << (n & 7)) - 1u);
+    }
+    bm[i] = b;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Candidates.  CTA j covers positions [fstart + j*kDpChunk, +kDpChunk) of
+// lane `lane`; thread t the 16 positions from 16t.
+// ---------------------------------------------------------------------------
+__device__ inline uint32_t dp_thread_cands(const uint8_t* __restrict__ s, uint64_t buf_len, uint64_t a, uint64_t end) {
+  // a = first position; end = lane end; a header at p needs p + 9 <= end
+  if (a + 9 > end) return 0;
+  uint64_t w0, w1, w2;
+  if (a + 24 <= buf_len) {
+    w0 = ld_u64(s + a);
+    w1 = ld_u64(s + a + 8);
+    w2 = ld_u64(s + a + 16);
+  } else {
+    w0 = w1 = w2 = 0;
+#pragma unroll
+    for (int i = 0; i < 24; i++) {
+      uint64_t b = (a + i < buf_len) ? s[a + i] : 0xFF;  // past the buffer: never zero
+      if (i < 8) w0 |= b << (8 * i);
+      else if (i < 16) w1 |= b << (8 * (i - 8));
+      else w2 |= b << (8 * (i - 16));
+    }
+  }
+  uint32_t z = zero_bytes8(w0) | (zero_bytes8(w1) << 8) | (zero_bytes8(w2) << 16);
+  // byte i+4 (top byte of n) and byte i+8 (top byte of plen) zero
+  uint32_t m = (z >> 4) & (z >> 8) & 0xFFFFu;
+  uint64_t last = end - 9;  // last position that can hold a header (>= a here)
+  if (a + 15 > last) m &= (2u << (uint32_t)(last - a)) - 1u;
+  uint32_t out = 0;
+  while (m) {
+    uint32_t i = __ffs(m) - 1;
+    m &= m - 1;
+    uint64_t p = a + i;
+    uint32_t mode = s[p];
+    uint32_t n = ld_u32(s + p + 1), plen = ld_u32(s + p + 5);
+    if (dp_mode_known(mode) && n >= 1 && n <= (uint32_t)kMaxBlock && plen <= end - p - 9) out |= 1u << i;
+  }
+  return out;
+}
+
+__global__ void __launch_bounds__(kDpThreads) k_dp_cand_count(const uint8_t* __restrict__ s, uint64_t buf_len,
+                                                              const DpHead* __restrict__ H, int lane,
+                                                              uint64_t* __restrict__ cnt) {
+  __shared__ uint32_t red[kDpThreads / 32];
+  const DpLane& L = H->lanes[lane];
+  uint64_t end = L.base + L.len;
+  uint64_t a = L.fstart + (uint64_t)blockIdx.x * kDpChunk + 16ull * threadIdx.x;
+  uint32_t c = H->kind ? 0u : (uint32_t)__popc(dp_thread_cands(s, buf_len, a, end));
+  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kDpThreads / 32; w++) t += red[w];
+    cnt[blockIdx.x] = t;
+  }
+}
+
+// Writes chunk j's candidates at off[j] (off = exclusive scan of the counts
+// with one extra entry, so off[j + 1] - off[j] is chunk j's count).
+__global__ void __launch_bounds__(kDpThreads) k_dp_cand_write(const uint8_t* __restrict__ s, uint64_t buf_len,
+                                                              const DpHead* __restrict__ H, int lane,
+                                                              const uint64_t* __restrict__ off, uint64_t cap,
+                                                              DpCand* __restrict__ cand) {
+  __shared__ uint64_t s_warp[33];
+  uint64_t base = off[blockIdx.x];
+  if (off[blockIdx.x + 1] == base || H->kind) return;
+  const DpLane& L = H->lanes[lane];
+  uint64_t end = L.base + L.len;
+  uint64_t a = L.fstart + (uint64_t)blockIdx.x * kDpChunk + 16ull * threadIdx.x;
+  uint32_t m = dp_thread_cands(s, buf_len, a, end);
+  uint64_t at = base + block_excl_scan<ScanSum>((uint64_t)__popc(m), s_warp, nullptr);
+  while (m) {
+    uint32_t i = __ffs(m) - 1;
+    m &= m - 1;
+    uint64_t p = a + i;
+    if (at < cap) {
+      DpCand c;
+      c.pos = p;
+      c.n = ld_u32(s + p + 1);
+      c.plen_mode = (ld_u32(s + p + 5) << 8) | s[p];
+      cand[at] = c;
+    }
+    at++;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Chain resolution and item layout (one CTA per lane).
+// ---------------------------------------------------------------------------
+// ALP-RD header up to the rights tag (alp_rd.rs:208-250); false when it does
+// not parse (the frame is then listed and the frame kernel reports it).
+__device__ bool dp_alprd_tags(const uint8_t* p, uint64_t plen, uint64_t* nexc, uint32_t* ctag, uint32_t* rtag) {
+  if (plen < 2 || p[1] > 8) return false;
+  uint64_t pos = 2 + 8ull * p[1], clen = 0;
+  if (pos > plen || rd_varint(p, plen, &pos, nexc) != E_OK) return false;
+  for (uint64_t x = 0; x < *nexc; x++) {
+    uint64_t pp;
+    if (rd_varint(p, plen, &pos, &pp) != E_OK || plen - pos < 8) return false;
+    pos += 8;
+  }
+  if (pos >= plen) return false;
+  *ctag = p[pos++];
+  if (rd_varint(p, plen, &pos, &clen) != E_OK || clen > plen - pos) return false;
+  pos += clen;
+  if (pos >= plen) return false;
+  *rtag = p[pos];
+  return true;
+}
+
+// Whether a listed frame may hold an entropy-coded part and so needs a
+// device area (the host reader's entropy_frame_h, the same rules).
+__device__ bool dp_entropy_frame(const uint8_t* p, uint64_t plen, uint32_t mode) {
+  switch (mode) {
+    case 11: case 7: case 20: case 45: case 0: case 25: case 29: case 4:
+      return true;
+    case 17:
+      return plen < 2 || p[0] == 1;
+    case 52: {
+      uint64_t nexc = 0;
+      uint32_t ct = 0, rt = 0;
+      return !dp_alprd_tags(p, plen, &nexc, &ct, &rt) || ct == 1 || rt == 1;
+    }
+    case 19: {
+      uint64_t pos = 0, card = 0, vlen = 0;
+      if (rd_varint(p, plen, &pos, &card) != E_OK || pos >= plen) return true;
+      uint32_t vtag = p[pos++];
+      if (vtag == 2) return true;
+      if (rd_varint(p, plen, &pos, &vlen) != E_OK || vlen > plen - pos) return true;
+      pos += vlen;
+      return pos >= plen || p[pos] == 1;
+    }
+    default:
+      return false;
+  }
+}
+
+struct FrameItems {
+  uint32_t nmain, npre;
+  bool list, scan, dict;
+  uint64_t ent;
+};
+
+// The host reader's build_items for one frame.
+__device__ FrameItems dp_frame_items(const uint8_t* p, uint64_t n, uint64_t plen, uint32_t mode, uint32_t plog2) {
+  FrameItems r{0, 0, false, false, false, 0};
+  uint32_t nv = (uint32_t)((n + 511) / 512);
+  switch (mode) {
+    case 5: case 1: case 2: case 50: case 9:
+      r.nmain = nv;
+      break;
+    case 17:
+      if (plen >= 2 && p[0] == 0) r.nmain = nv; else r.list = true;
+      break;
+    case 51:
+      r.npre = r.nmain = nv;
+      r.scan = true;
+      break;
+    case 3:
+      r.npre = r.nmain = (uint32_t)((plen + 511) / 512);
+      r.scan = true;
+      break;
+    case 53: {
+      uint64_t pos = 0, nr = 0;
+      if (rd_varint(p, plen, &pos, &nr) != E_OK || nr > n) {
+        r.list = true;
+        break;
+      }
+      r.npre = (uint32_t)((nr + 1023) / 1024);
+      r.nmain = nv;
+      r.scan = true;
+      break;
+    }
+    case 52: {
+      uint64_t nexc = 1;
+      uint32_t ct = 1, rt = 1;
+      if (dp_alprd_tags(p, plen, &nexc, &ct, &rt) && nexc == 0 && ct == 0 && rt == 0) r.nmain = nv;
+      else r.list = true;
+      break;
+    }
+    default:
+      r.list = true;
+      break;
+  }
+  r.dict = mode == 19 || mode == 53 || mode == 52;
+  if (r.list && dp_entropy_frame(p, plen, mode)) r.ent = ent_area_bytes(n, mode, plog2);
+  return r;
+}
+
+__global__ void __launch_bounds__(kChainThreads) k_dp_chain(const uint8_t* __restrict__ s, const DpHead* __restrict__ H,
+                                                            int lane, const uint64_t* __restrict__ d_nvalid,
+                                                            const DpCand* __restrict__ cand,
+                                                            const uint64_t* __restrict__ d_ncand, uint64_t cap,
+                                                            uint32_t* __restrict__ gJ, uint8_t* __restrict__ gmarks,
+                                                            DpTables T, DpLaneOut* __restrict__ out) {
+  extern __shared__ __align__(16) uint8_t dsm[];
+  __shared__ uint64_t s_warp[33];
+  __shared__ uint64_t s_i0;
+  __shared__ int s_fail;
+  const int tid = threadIdx.x;
+  DpLaneOut R;
+  memset(&R, 0, sizeof(R));
+  R.status = 1;
+  if (H->kind) {
+    if (tid == 0) *out = R;
+    return;
+  }
+  const DpLane& L = H->lanes[lane];
+  uint64_t K = *d_ncand;
+  R.ncand = K;
+  // values the lane's frames hold: the valid count (a plain stream with a
+  // bitmap), else the lane header's n, which a decimal limb must match
+  uint64_t n_total = L.logical_n;
+  if (H->decimal) {
+    uint64_t nv = H->has_validity ? *d_nvalid : H->n;
+    if (n_total != nv) {
+      if (tid == 0) *out = R;
+      return;
+    }
+  } else if (L.has_validity) {
+    n_total = *d_nvalid;
+  }
+  if (n_total == 0) {  // no frame is read (decoder.rs: the walk runs while counted < n)
+    R.status = 0;
+    if (tid == 0) {
+      T.main_off[0] = 0;
+      *out = R;
+    }
+    return;
+  }
+  if (K > cap || K == 0) {
+    if (tid == 0) *out = R;
+    return;
+  }
+  // the first frame: binary search for fstart
+  if (tid == 0) {
+    uint64_t lo = 0, hi = K;
+    while (lo < hi) {
+      uint64_t mid = (lo + hi) >> 1;
+      if (cand[mid].pos < L.fstart) lo = mid + 1; else hi = mid;
+    }
+    s_i0 = lo;
+    s_fail = (lo == K || cand[lo].pos != L.fstart);
+  }
+  __syncthreads();
+  if (s_fail) {
+    if (tid == 0) *out = R;
+    return;
+  }
+  const uint64_t i0 = s_i0;
+  const uint32_t M = (uint32_t)(K - i0);
+  const DpCand* C = cand + i0;
+  // successor tables (two, for the doubling) and marks: in shared memory when
+  // they fit, else in the global scratch
+  uint32_t *J0, *J1;
+  uint8_t* marks;
+  if ((uint64_t)M * 9 + 16 <= kDpChainSmem) {
+    J0 = reinterpret_cast<uint32_t*>(dsm);
+    J1 = J0 + M;
+    marks = reinterpret_cast<uint8_t*>(J1 + M);
+  } else {
+    J0 = gJ;
+    J1 = gJ + M;
+    marks = gmarks;
+  }
+  for (uint32_t i = tid; i < M; i += kChainThreads) {
+    uint64_t target = C[i].pos + 9 + (C[i].plen_mode >> 8);
+    uint32_t lo = i + 1, hi = M;
+    while (lo < hi) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (C[mid].pos < target) lo = mid + 1; else hi = mid;
+    }
+    J0[i] = (lo < M && C[lo].pos == target) ? lo : kNone;
+    marks[i] = i == 0;
+  }
+  __syncthreads();
+  // pointer doubling: after round r every chain frame within 2^(r+1) - 1
+  // jumps of the first is marked (a mark set during a round may be used in
+  // the same round: it is a chain frame too)
+  uint32_t rounds = 1;
+  while ((1ull << rounds) <= M) rounds++;
+  for (uint32_t r = 0; r < rounds; r++) {
+    for (uint32_t i = tid; i < M; i += kChainThreads) {
+      uint32_t j = J0[i];
+      if (j != kNone && marks[i]) marks[j] = 1;
+      J1[i] = j == kNone ? kNone : J0[j];
+    }
+    __syncthreads();
+    uint32_t* t = J0;
+    J0 = J1;
+    J1 = t;
+  }
+  // the marked frames in position order, cut at the lane's value count: the
+  // values before a marked frame only grow along the chain, so the kept
+  // frames (those starting below the count) are a prefix of the marked ones
+  uint64_t carry_f = 0, carry_v = 0, carry_main = 0, carry_pre = 0, carry_list = 0, carry_ent = 0;
+  bool scan = false, dict = false, stop = false, fail = false;
+  for (uint32_t t0 = 0; t0 < M && !stop; t0 += kChainThreads) {
+    uint32_t i = t0 + tid;
+    bool marked = i < M && marks[i];
+    DpCand c;
+    c.pos = 0;
+    c.n = 0;
+    c.plen_mode = 0;
+    if (marked) c = C[i];
+    uint64_t vx = block_excl_scan<ScanSum>(marked ? (uint64_t)c.n : 0ull, s_warp, nullptr);
+    uint64_t voff = carry_v + vx;
+    bool keep = marked && voff < n_total;
+    FrameItems it{0, 0, false, false, false, 0};
+    uint32_t mode = c.plen_mode & 0xFF, plen = c.plen_mode >> 8;
+    if (keep) it = dp_frame_items(s + c.pos + 9, c.n, plen, mode, L.plog2);
+    bool last = keep && voff + c.n >= n_total;
+    stop = __syncthreads_or(last) != 0;
+    // past the count: CorruptPayload, which the host reader reports
+    fail = (__syncthreads_or(last && voff + c.n > n_total) != 0) || fail;
+    uint64_t tf, tv, tp, tl, te;
+    uint64_t fx = block_excl_scan<ScanSum>(keep ? 1ull : 0ull, s_warp, &tf);
+    block_excl_scan<ScanSum>(keep ? (uint64_t)c.n : 0ull, s_warp, &tv);
+    uint64_t packed = keep ? ((uint64_t)it.npre << 32 | it.nmain) : 0ull;
+    uint64_t px = block_excl_scan<ScanSum>(packed, s_warp, &tp);
+    uint64_t lx = block_excl_scan<ScanSum>(keep && it.list ? 1ull : 0ull, s_warp, &tl);
+    uint64_t ex = block_excl_scan<ScanSum>(keep ? it.ent : 0ull, s_warp, &te);
+    if (keep) {
+      uint64_t f = carry_f + fx;
+      FrameDesc d;
+      d.payload_off = c.pos + 9;
+      d.value_off = voff;
+      d.n = c.n;
+      d.plen = plen;
+      d.mode = mode;
+      d.aux = it.ent ? (uint32_t)(1 + (carry_ent + ex) / 128) : 0u;
+      T.frames[f] = d;
+      T.frame_pre[f] = make_uint2((uint32_t)(carry_pre + (px >> 32)), it.npre);
+      T.main_off[f] = carry_main + (px & 0xFFFFFFFFull);
+      if (it.list) T.list[carry_list + lx] = (uint32_t)f;
+    }
+    scan = (__syncthreads_or(keep && it.scan) != 0) || scan;
+    dict = (__syncthreads_or(keep && it.dict) != 0) || dict;
+    carry_f += tf;
+    carry_v += tv;
+    carry_main += tp & 0xFFFFFFFFull;
+    carry_pre += tp >> 32;
+    carry_list += tl;
+    carry_ent += te;
+  }
+  if (tid == 0) {
+    R.status = (fail || !stop || carry_v != n_total) ? 1u : 0u;
+    R.nframes = (uint32_t)carry_f;
+    R.nmain = (uint32_t)carry_main;
+    R.npre = (uint32_t)carry_pre;
+    R.nlist = (uint32_t)carry_list;
+    R.need_scan = scan;
+    R.any_dict = dict;
+    R.ent_bytes = carry_ent;
+    T.main_off[carry_f] = carry_main;
+    *out = R;
+  }
+}
+
+// Warp items of every frame: main items (frame, k) for k < its count, and the
+// prepass items likewise (launch_decode_items' tables).
+__global__ void k_dp_expand(const DpLaneOut* __restrict__ out, DpTables T) {
+  uint32_t nf = out->status ? 0u : out->nframes;
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t f = warp; f < nf; f += nwarps) {
+    uint64_t m0 = T.main_off[f], m1 = T.main_off[f + 1];
+    for (uint64_t k = m0 + lane; k < m1; k += 32) T.main_items[k] = ItemRef{f, (uint32_t)(k - m0)};
+    uint2 fp = T.frame_pre[f];
+    for (uint32_t k = lane; k < fp.y; k += 32) T.pre_items[fp.x + k] = ItemRef{f, k};
+  }
+}
+
+std::atomic<unsigned long long> g_chain_attr{0};
+
+}  // namespace
+
+void launch_dp_head(const uint8_t* s, uint64_t len, DpHead* H, cudaStream_t st) {
+  k_dp_head<<<1, 32, 0, st>>>(s, len, H);
+  count_launches(1);
+}
+
+void launch_dp_bitmap(const uint8_t* s, const DpHead* H, uint64_t raw_len, uint8_t* bm, cudaStream_t st) {
+  uint64_t bytes = (raw_len + 7) / 8 * 8;
+  unsigned g = (unsigned)qmin((bytes + 255) / 256, 148ull * 8);
+  if (g == 0) g = 1;
+  k_dp_bitmap<<<g, 256, 0, st>>>(s, H, bm);
+  count_launches(1);
+}
+
+uint64_t dp_chunks(uint64_t lane_frames_bytes) { return (lane_frames_bytes + kDpChunk - 1) / kDpChunk; }
+
+void launch_dp_candidates(const uint8_t* s, uint64_t buf_len, const DpHead* H, int lane, uint64_t lane_frames_bytes,
+                          uint64_t* cnt, uint64_t* tile_tmp, uint64_t* d_ncand, DpCand* cand, uint64_t cap,
+                          cudaStream_t st) {
+  // cnt has nchunks + 1 entries: the counts, then 0, so that after the
+  // exclusive scan cnt[j + 1] - cnt[j] is chunk j's count
+  uint64_t nchunks = dp_chunks(lane_frames_bytes);
+  if (nchunks) k_dp_cand_count<<<(unsigned)nchunks, kDpThreads, 0, st>>>(s, buf_len, H, lane, cnt);
+  cudaMemsetAsync(cnt + nchunks, 0, 8, st);
+  launch_scan_sum(cnt, cnt, nchunks + 1, tile_tmp, d_ncand, st);
+  if (nchunks) k_dp_cand_write<<<(unsigned)nchunks, kDpThreads, 0, st>>>(s, buf_len, H, lane, cnt, cap, cand);
+  count_launches(nchunks ? 2 : 0);
+}
+
+void launch_dp_chain(const uint8_t* s, const DpHead* H, int lane, const uint64_t* d_nvalid, const DpCand* cand,
+                     const uint64_t* d_ncand, uint64_t cap, uint32_t* gJ, uint8_t* gmarks, const DpTables& T,
+                     DpLaneOut* out, cudaStream_t st) {
+  once_per_device(g_chain_attr, [] {
+    cudaFuncSetAttribute(k_dp_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDpChainSmem);
+  });
+  k_dp_chain<<<1, kChainThreads, kDpChainSmem, st>>>(s, H, lane, d_nvalid, cand, d_ncand, cap, gJ, gmarks, T, out);
+  k_dp_expand<<<148 * 2, 256, 0, st>>>(out, T);
+  count_launches(2);
+}
+
+}  // namespace qb

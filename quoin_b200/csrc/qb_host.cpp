@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cstddef>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -195,7 +196,7 @@ inline int plain_code(int ext) {
 enum Slot {
   S_IN, S_BM, S_RANK, S_LANE, S_GROW, S_FRAMES, S_NB, S_SIZES, S_TILE, S_SCRATCH, S_OUT, S_VTMP, S_VBLOB,
   S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_DAUX, S_SUBST, S_FMST,
-  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_ENT, S_ENTREC, S_COUNT
+  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_ENT, S_ENTREC, S_DPMISC, S_DPCAND, S_DPJ, S_COUNT
 };
 
 struct QuoinCtx {
@@ -635,6 +636,9 @@ struct LaneIdx {
   bool need_scan = false;
   uint64_t ent_bytes = 0;  // device area for the entropy-coded parts of listed frames
   uint64_t main_base = 0, pre_base = 0, fp_base = 0, list_base = 0;  // index of the first frame in the device table
+  // table sizes the decode launches use (the vectors' sizes after a host
+  // parse; the device reader's counts when the tables were built on the device)
+  uint64_t nf = 0, nmain = 0, npre = 0, nlist = 0;
 
   // Back to the empty state, keeping every buffer's capacity (a context
   // reuses its parsed index, so repeated decodes touch no fresh pages).
@@ -654,6 +658,13 @@ struct LaneIdx {
     need_scan = false;
     ent_bytes = 0;
     main_base = pre_base = fp_base = list_base = 0;
+    nf = nmain = npre = nlist = 0;
+  }
+  void take_counts() {
+    nf = frames.size();
+    nmain = main_items.size();
+    npre = pre_items.size();
+    nlist = list.size();
   }
 };
 
@@ -945,7 +956,10 @@ int parse_stream(const uint8_t* src, uint64_t len, QuoinDecodeIndex& X) {
   if (k) return k;
   X.items_bytes = layout_items(X.lanes);
   X.max_pre = 0;
-  for (auto& L : X.lanes) X.max_pre = L.pre_items.size() > X.max_pre ? L.pre_items.size() : X.max_pre;
+  for (auto& L : X.lanes) {
+    L.take_counts();
+    X.max_pre = L.npre > X.max_pre ? L.npre : X.max_pre;
+  }
   return K_OK;
 }
 
@@ -1087,12 +1101,12 @@ int upload_index(QuoinCtx* c, cudaStream_t st, QuoinDecodeIndex& X, FrameDesc* d
 ItemPlan lane_plan(const LaneIdx& L, const uint64_t* ditems) {
   ItemPlan P;
   P.main_items = reinterpret_cast<const ItemRef*>(ditems + L.main_base);
-  P.nmain = (uint32_t)L.main_items.size();
+  P.nmain = (uint32_t)L.nmain;
   P.pre_items = reinterpret_cast<const ItemRef*>(ditems + L.pre_base);
-  P.npre = (uint32_t)L.pre_items.size();
+  P.npre = (uint32_t)L.npre;
   P.frame_pre = reinterpret_cast<const uint2*>(ditems + L.fp_base);
   P.list = reinterpret_cast<const uint32_t*>(ditems + L.list_base);
-  P.nlist = (uint32_t)L.list.size();
+  P.nlist = (uint32_t)L.nlist;
   P.need_scan = L.need_scan;
   P.ent = nullptr;
   return P;
@@ -1106,7 +1120,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
   CK(cudaMemsetAsync(d_err, 0xFF, 8, st));
   const uint8_t* bm = X.has_validity ? dbm : nullptr;
   uint64_t max_nf = 1;
-  for (auto& L : X.lanes) max_nf = L.frames.size() > max_nf ? L.frames.size() : max_nf;
+  for (auto& L : X.lanes) max_nf = L.nf > max_nf ? L.nf : max_nf;
   CK(c->ensure(S_DAUX, decode_aux_bytes((int)max_nf)));
   void* daux = c->p<void>(S_DAUX);
   CK(c->ensure(S_PRE, (X.max_pre + 1) * prepass_rec_bytes()));
@@ -1140,7 +1154,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
       O.plog2 = L.plog2;
       {
         TimedRegion tr(T_DECODE, st);
-        launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, plan_of(L), dpre,
+        launch_decode_items(d_src, dfr + L.frame_base, (int)L.nf, X.wire, O, plan_of(L), dpre,
                             scr, daux, d_err, st);
       }
       if (L.n_total == 0 && X.n) CK(cudaMemsetAsync(d_out, 0, X.n * w, st));  // all null
@@ -1151,7 +1165,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
       O.plog2 = L.plog2;
       {
         TimedRegion tr(T_DECODE, st);
-        launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), X.wire, O, plan_of(L), dpre,
+        launch_decode_items(d_src, dfr + L.frame_base, (int)L.nf, X.wire, O, plan_of(L), dpre,
                             scr, daux, d_err, st);
       }
       if (X.n) {
@@ -1175,7 +1189,7 @@ int decode_indexed(QuoinCtx* c, cudaStream_t st, const QuoinDecodeIndex& X, cons
       DecodeOut O{limbs + (uint64_t)k * X.n_valid, WT_U64, nullptr, nullptr, nullptr, X.n_valid, X.n_valid};
       O.plog2 = L.plog2;
       TimedRegion tr(T_DECODE, st);
-      launch_decode_items(d_src, dfr + L.frame_base, (int)L.frames.size(), WT_U64, O, plan_of(L), dpre, scr,
+      launch_decode_items(d_src, dfr + L.frame_base, (int)L.nf, WT_U64, O, plan_of(L), dpre, scr,
                           daux, d_err, st);
     }
     if (X.n) {
@@ -1250,6 +1264,198 @@ int decompress_host(QuoinCtx* c, const uint8_t* src, uint64_t len, void* values_
   int rc = begin_decode(c, src, len, *X);
   if (rc) return rc;
   return finish_decode(c, X, values_out, validity_out);
+}
+
+// ---------------------------------------------------------------------------
+// Decode of a device-resident stream, parsed on the device (qb_dparse.cu).
+// ---------------------------------------------------------------------------
+struct DpMisc {  // the reader's small results, read back in one copy
+  DpLaneOut lanes[4];
+  uint64_t nvalid;
+  uint64_t ncand[4];
+};
+constexpr uint64_t kDpHeadOff = 0, kDpMiscOff = 512;
+static_assert(sizeof(DpHead) <= kDpMiscOff && sizeof(DpMisc) <= 512, "reader results fit their slot");
+
+// Candidate capacity of a lane whose frames span `bytes`: encoder streams
+// hold far fewer frames (one per 32,768 values for adaptive blocks); a lane
+// with more candidates is read again with the exact count.
+uint64_t dp_cap(uint64_t bytes) { return bytes / 512 + 8192; }
+
+// The host reader's route for the streams the device reader leaves to it: a
+// host copy, parsed and uploaded as for a host-buffer decode.
+int decode_device_via_host(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t len, void* d_out,
+                           uint64_t out_cap_bytes, uint8_t* d_valid_out, int32_t* wire_out, uint64_t* n_out) {
+  std::vector<uint8_t> h(len);
+  if (len) CK(cudaMemcpyAsync(h.data(), d_src, len, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  QuoinDecodeIndex& X = host_index(c);
+  int k = parse_stream(h.data(), len, X);
+  if (k) return kind_to_code(k);
+  *wire_out = X.wire;
+  *n_out = X.n;
+  if (X.n * (uint64_t)native_width(X.wire) > out_cap_bytes) return QUOIN_ERR_BUFFER_TOO_SMALL;
+  uint64_t nf = total_frames(X);
+  CK(c->ensure(S_DFRAMES, (nf + 1) * sizeof(FrameDesc)));
+  CK(c->ensure(S_DBM, X.bitmap.size() + 16));
+  CK(c->ensure(S_DRANK, ((X.n + 31) / 32 + 1) * 8));
+  CK(c->ensure(S_MISC, 64 * 8));
+  uint64_t* dvmin = c->p<uint64_t>(S_MISC) + 32;
+  CK(c->ensure(S_DSEL, sel_bytes(X)));
+  CK(c->ensure(S_DITEMS, X.items_bytes));
+  int rc = upload_index(c, st, X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK),
+                        c->p<uint64_t>(S_DSEL), dvmin, c->p<uint64_t>(S_DITEMS));
+  if (rc) return rc;
+  return decode_indexed(c, st, X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK),
+                        c->p<uint64_t>(S_DSEL), dvmin, c->p<uint64_t>(S_DITEMS), d_src, d_out, d_valid_out);
+}
+
+// Reference decoder.rs:43-118 (+ decimal.rs:100-168, lib.rs:462-508) for a
+// stream in device memory: header, validity and frame table are read by the
+// device reader, then the block decoder runs as for an indexed decode.  Three
+// host synchronisations: the header (output sizes), the frame tables (launch
+// sizes), the final status.
+int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t len, void* d_out,
+                  uint64_t out_cap_bytes, uint8_t* d_valid_out, int32_t* wire_out, uint64_t* n_out) {
+  CK(c->ensure(S_DPMISC, 1024));
+  uint8_t* misc = c->p<uint8_t>(S_DPMISC);
+  DpHead* dH = reinterpret_cast<DpHead*>(misc + kDpHeadOff);
+  DpMisc* dM = reinterpret_cast<DpMisc*>(misc + kDpMiscOff);
+  CK(cudaMemsetAsync(dM, 0, sizeof(DpMisc), st));  // the valid count stays 0 without a bitmap
+  launch_dp_head(d_src, len, dH, st);
+  DpHead H;
+  CK(read_small(c, st, &H, dH, sizeof(H)));
+  if (H.kind) return decode_device_via_host(c, st, d_src, len, d_out, out_cap_bytes, d_valid_out, wire_out, n_out);
+  *wire_out = (int32_t)H.wire;
+  *n_out = H.n;
+  uint32_t w = native_width((int)H.wire);
+  if (H.n * (uint64_t)w > out_cap_bytes) return QUOIN_ERR_BUFFER_TOO_SMALL;
+  const uint64_t n = H.n;
+  const uint64_t nw = (n + 31) / 32;
+  // validity: bitmap, word ranks, valid count, select table
+  if (H.has_validity && n) {
+    CK(c->ensure(S_DBM, (H.vblob_len + 7) / 8 * 8 + 16));
+    CK(c->ensure(S_DRANK, (nw + 1) * 8));
+    CK(c->ensure(S_TILE, (scan_tile_count(nw + 4096) + 16) * 8));
+    launch_dp_bitmap(d_src, dH, H.vblob_len, c->p<uint8_t>(S_DBM), st);
+    launch_word_popcount(c->p<uint8_t>(S_DBM), n, c->p<uint64_t>(S_DRANK), st);
+    launch_scan_sum(c->p<uint64_t>(S_DRANK), c->p<uint64_t>(S_DRANK), nw, c->p<uint64_t>(S_TILE), &dM->nvalid, st);
+    if (!H.decimal) {
+      // the valid count is only known on the device: n bounds it (every
+      // table entry the kernel writes is below the count anyway)
+      CK(c->ensure(S_DSEL, (n / 512 + 2) * 8));
+      launch_select_table(c->p<uint8_t>(S_DBM), n, c->p<uint64_t>(S_DRANK), n, c->p<uint64_t>(S_DSEL), st);
+    }
+  }
+  // per-lane regions of the candidate, frame and item tables
+  const int nl = (int)H.nl;
+  uint64_t caps[4], cnt_off[4], cand_off[4], j_off[4], fr_off[4], main_b[4], pre_b[4], fp_b[4], list_b[4], moff_b[4];
+  uint64_t caps_min[4] = {0, 0, 0, 0};
+  for (int attempt = 0; attempt < 2; attempt++) {
+    uint64_t cand_bytes = 0, j_bytes = 0, frames_n = 0, items_u64 = 0, max_chunks = 0;
+    for (int k = 0; k < nl; k++) {
+      const DpLane& L = H.lanes[k];
+      uint64_t fb = L.base + L.len - L.fstart;
+      caps[k] = dp_cap(fb) > caps_min[k] ? dp_cap(fb) : caps_min[k];
+      cnt_off[k] = cand_bytes;
+      cand_bytes += (dp_chunks(fb) + 2) * 8;
+      max_chunks = dp_chunks(fb) + 1 > max_chunks ? dp_chunks(fb) + 1 : max_chunks;
+      cand_off[k] = cand_bytes;
+      cand_bytes += caps[k] * sizeof(DpCand);
+      j_off[k] = j_bytes;
+      j_bytes += (caps[k] * 9 + 255) & ~255ull;
+      fr_off[k] = frames_n;
+      frames_n += caps[k];
+      uint64_t nmax = L.logical_n / 512 + fb / 512 + 2 * caps[k] + 16;  // items of either kind
+      main_b[k] = items_u64;
+      items_u64 += nmax;
+      pre_b[k] = items_u64;
+      items_u64 += nmax;
+      fp_b[k] = items_u64;
+      items_u64 += caps[k];
+      list_b[k] = items_u64;
+      items_u64 += (caps[k] + 1) / 2 + 1;
+      moff_b[k] = items_u64;
+      items_u64 += caps[k] + 1;
+    }
+    CK(c->ensure(S_DPCAND, cand_bytes));
+    CK(c->ensure(S_DPJ, j_bytes));
+    CK(c->ensure(S_DFRAMES, (frames_n + 1) * sizeof(FrameDesc)));
+    CK(c->ensure(S_DITEMS, items_u64 * 8 + 64));
+    CK(c->ensure(S_TILE, (scan_tile_count(max_chunks + nw + 4096) + 16) * 8));
+    uint8_t* cb = c->p<uint8_t>(S_DPCAND);
+    uint64_t* ditems = c->p<uint64_t>(S_DITEMS);
+    const uint64_t* d_nvalid = H.has_validity ? &dM->nvalid : nullptr;
+    for (int k = 0; k < nl; k++) {
+      const DpLane& L = H.lanes[k];
+      uint64_t fb = L.base + L.len - L.fstart;
+      DpCand* cand = reinterpret_cast<DpCand*>(cb + cand_off[k]);
+      launch_dp_candidates(d_src, len, dH, k, fb, reinterpret_cast<uint64_t*>(cb + cnt_off[k]),
+                           c->p<uint64_t>(S_TILE), &dM->ncand[k], cand, caps[k], st);
+      uint8_t* jb = c->p<uint8_t>(S_DPJ) + j_off[k];
+      DpTables T;
+      T.frames = c->p<FrameDesc>(S_DFRAMES) + fr_off[k];
+      T.frame_pre = reinterpret_cast<uint2*>(ditems + fp_b[k]);
+      T.main_off = ditems + moff_b[k];
+      T.list = reinterpret_cast<uint32_t*>(ditems + list_b[k]);
+      T.main_items = reinterpret_cast<ItemRef*>(ditems + main_b[k]);
+      T.pre_items = reinterpret_cast<ItemRef*>(ditems + pre_b[k]);
+      launch_dp_chain(d_src, dH, k, d_nvalid, cand, &dM->ncand[k], caps[k], reinterpret_cast<uint32_t*>(jb),
+                      jb + caps[k] * 8, T, &dM->lanes[k], st);
+    }
+    DpMisc M;
+    CK(read_small(c, st, &M, dM, sizeof(M)));
+    bool grow = false, host = false;
+    for (int k = 0; k < nl; k++) {
+      if (!M.lanes[k].status) continue;
+      if (M.lanes[k].ncand > caps[k] && attempt == 0) {
+        caps_min[k] = M.lanes[k].ncand + 1024;
+        grow = true;
+      } else {
+        host = true;
+      }
+    }
+    if (host) return decode_device_via_host(c, st, d_src, len, d_out, out_cap_bytes, d_valid_out, wire_out, n_out);
+    if (grow) continue;
+    // the index the block decoder runs from
+    QuoinDecodeIndex X;
+    X.wire = (int)H.wire;
+    X.n = n;
+    X.has_validity = H.has_validity;
+    X.decimal = H.decimal;
+    X.scale = (int8_t)H.scale;
+    X.precision = (uint8_t)H.precision;
+    X.nl = H.decimal ? nl : 0;
+    X.n_valid = H.has_validity ? M.nvalid : n;
+    X.lanes.resize(nl);
+    X.max_pre = 0;
+    for (int k = 0; k < nl; k++) {
+      LaneIdx& L = X.lanes[k];
+      const DpLaneOut& O = M.lanes[k];
+      L.dtype = (int)H.lanes[k].dtype;
+      L.plog2 = H.lanes[k].plog2;
+      L.logical_n = H.lanes[k].logical_n;
+      L.has_validity = H.lanes[k].has_validity;
+      L.n_total = (!H.decimal && L.has_validity) ? M.nvalid : L.logical_n;
+      L.any_dict = O.any_dict;
+      L.need_scan = O.need_scan;
+      L.ent_bytes = O.ent_bytes;
+      L.frame_base = fr_off[k];
+      L.main_base = main_b[k];
+      L.pre_base = pre_b[k];
+      L.fp_base = fp_b[k];
+      L.list_base = list_b[k];
+      L.nf = O.nframes;
+      L.nmain = O.nmain;
+      L.npre = O.npre;
+      L.nlist = O.nlist;
+      X.max_pre = L.npre > X.max_pre ? L.npre : X.max_pre;
+    }
+    const uint64_t* dvmin = reinterpret_cast<const uint64_t*>(misc + kDpHeadOff + offsetof(DpHead, vmin));
+    return decode_indexed(c, st, X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK),
+                          c->p<uint64_t>(S_DSEL), dvmin, ditems, d_src, d_out, d_valid_out);
+  }
+  return decode_device_via_host(c, st, d_src, len, d_out, out_cap_bytes, d_valid_out, wire_out, n_out);
 }
 
 // Host-buffer compress of a typed column (wire dtype, native little-endian values).
@@ -1719,6 +1925,24 @@ int quoin_b200_decompress_indexed_device(QuoinCtx* ctx, const QuoinDecodeIndex* 
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     return decode_indexed(c, st, *X, X->d_frames, X->d_bm, X->d_rank, X->d_sel, X->d_vmin, X->d_items, d_src,
                           d_values_out, d_validity_out);
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+int quoin_b200_decompress_column_device(QuoinCtx* ctx, const uint8_t* d_src, size_t src_len, void* d_values_out,
+                                        size_t values_cap_bytes, uint8_t* d_validity_out, int32_t* wire_out,
+                                        uint64_t* n_out, void* stream) {
+  if (!d_src || !d_values_out || !wire_out || !n_out) return QUOIN_ERR_NULL;
+  try {
+    *wire_out = 0;
+    *n_out = 0;
+    QuoinCtx* c = pick(ctx);
+    if (!c) return QUOIN_ERR_CUDA;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    return decode_device(c, st, d_src, src_len, d_values_out, values_cap_bytes, d_validity_out, wire_out, n_out);
   } catch (...) {
     return QUOIN_ERR_PANIC;
   }

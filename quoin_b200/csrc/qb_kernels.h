@@ -70,6 +70,60 @@ uint64_t prepass_rec_bytes();
 void launch_decode_items(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
                          const ItemPlan& plan, void* pre, uint64_t* scratch, void* aux, unsigned long long* err,
                          cudaStream_t st);
+// ---- device stream reader (qb_dparse.cu) ----
+// One lane stream of a column: the stream itself, or a decimal limb's.
+struct DpLane {
+  uint64_t base, len;   // the lane stream's bytes within the buffer
+  uint64_t fstart;      // offset of its first frame header
+  uint64_t logical_n;   // the lane header's value count
+  uint32_t dtype, plog2, has_validity, pad;
+};
+// The parsed header.  kind != 0: the device reader does not take this
+// stream (an error, or a form the host reader decodes), the host parses it.
+struct DpHead {
+  uint32_t kind, wire, decimal, has_validity, nl, precision;
+  int32_t scale, pad;
+  uint64_t n;
+  uint64_t vblob_off, vblob_len;  // the RAW validity bitmap's bytes
+  uint64_t vmin[4];
+  DpLane lanes[4];
+};
+// A frame-header candidate (pos = header offset; plen < 2^24).
+struct DpCand {
+  uint64_t pos;
+  uint32_t n, plen_mode;  // plen << 8 | mode
+};
+// The reader's result for one lane (status != 0: the host parses the stream;
+// ncand tells the host how many candidates the tables must hold).
+struct DpLaneOut {
+  uint32_t status, nframes, nmain, npre, nlist, need_scan, any_dict, pad;
+  uint64_t ncand, ent_bytes;
+};
+// Where k_dp_chain writes a lane's decode tables (capacity = the candidate
+// capacity; main_off one entry more).
+struct DpTables {
+  FrameDesc* frames;
+  uint2* frame_pre;
+  uint64_t* main_off;
+  uint32_t* list;
+  ItemRef* main_items;
+  ItemRef* pre_items;
+};
+constexpr uint64_t kDpChainSmem = 200 * 1024;  // successor tables in shared memory up to 22,755 candidates
+void launch_dp_head(const uint8_t* s, uint64_t len, DpHead* H, cudaStream_t st);
+void launch_dp_bitmap(const uint8_t* s, const DpHead* H, uint64_t raw_len, uint8_t* bm, cudaStream_t st);
+// Candidate chunks of a lane whose frames span `lane_frames_bytes` bytes (cnt
+// needs dp_chunks() + 1 entries; *d_ncand gets the count, at most cap written).
+uint64_t dp_chunks(uint64_t lane_frames_bytes);
+void launch_dp_candidates(const uint8_t* s, uint64_t buf_len, const DpHead* H, int lane, uint64_t lane_frames_bytes,
+                          uint64_t* cnt, uint64_t* tile_tmp, uint64_t* d_ncand, DpCand* cand, uint64_t cap,
+                          cudaStream_t st);
+// Chain resolution + item tables of lane `lane` (gJ: 8 * cap bytes, gmarks:
+// cap bytes of global scratch for lanes whose candidates exceed shared memory).
+void launch_dp_chain(const uint8_t* s, const DpHead* H, int lane, const uint64_t* d_nvalid, const DpCand* cand,
+                     const uint64_t* d_ncand, uint64_t cap, uint32_t* gJ, uint8_t* gmarks, const DpTables& T,
+                     DpLaneOut* out, cudaStream_t st);
+
 // sel[m] = position of the (512*m)-th valid value, m < ceil(nvalid / 512).
 void launch_select_table(const uint8_t* bm, uint64_t n, const uint64_t* word_rank, uint64_t nvalid, uint64_t* sel,
                          cudaStream_t st);
