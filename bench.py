@@ -46,7 +46,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "encode+decode GB/s (uncompressed bytes; Level::Fast, bit-exact round trip)"
 N_DEFAULT = 67_108_864
-TIMER_NAMES = ["compete", "emit", "decode", "finalize", "lower", "plan", "validity", "other"]
+TIMER_NAMES = ["compete", "emit", "decode", "finalize", "lower", "plan", "validity", "other", "read"]
 
 # Single-column workloads: (synth config, description, arithmetic types).
 WORKLOADS = {
@@ -58,13 +58,10 @@ WORKLOADS = {
 }
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture) of
-# one decode of the workload's three columns at 16,777,216 values each, summed
-# over k_walk_frames, k_prepass, k_prepass_scan, k_decode_items,
-# k_decode_frames and k_decimal_combine; reported
-# scaled by the values per column.  Lines still dirty in L2 when a launch ends
-# are not counted, so the figure is a lower bound on the written share.
-DECODE_TRAFFIC_16M = {"integer-lanes": 388_141_056, "float-lanes": 1_085_646_080}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per decode
+# phase of the workload's three columns, from a one-kernel ncu capture scaled
+# to the bench's column length; None until captured for the current kernels.
+DECODE_TRAFFIC = {}
 
 
 DECIMAL128_WIRE = 6  # wire dtype id of Decimal128 (reference src/dtype.rs:68-93)
@@ -317,9 +314,13 @@ def run_gpu(args, rank, world, local):
         c["len"] = olen.value
 
     def decompress_one(c):
-        rc = L.quoin_b200_decompress_indexed_device(c["ctx"], c["idx"], P(c["d_dst"].data_ptr()),
-                                                    P(c["d_out"].data_ptr()), P(c["d_vout"].data_ptr()),
-                                                    P(c["st"].cuda_stream))
+        # the stream is read on the device (header, validity, frame table)
+        # inside every timed decode: no host copy, no prebuilt index
+        w, nn = ctypes.c_int32(), ctypes.c_uint64()
+        rc = L.quoin_b200_decompress_column_device(c["ctx"], P(c["d_dst"].data_ptr()), c["len"],
+                                                   P(c["d_out"].data_ptr()), c["d_out"].numel(),
+                                                   P(c["d_vout"].data_ptr()), ctypes.byref(w), ctypes.byref(nn),
+                                                   P(c["st"].cuda_stream))
         if rc:
             raise Q.Error(rc)
 
@@ -349,19 +350,10 @@ def run_gpu(args, rank, world, local):
             s.wait_event(ev)
         return ev
 
-    # First pass: compress, build the decode index from the host copy, verify
-    # the round trip bit for bit (null slots decode to 0).
+    # First pass: compress, decompress from the device stream, verify the
+    # round trip bit for bit (null slots decode to 0).
     with torch.cuda.stream(stream):
         compress_all()
-    host_streams = []
-    for c in gcols:
-        hs = c["d_dst"][: c["len"]].cpu().numpy().tobytes()
-        host_streams.append(hs)
-        idx = P()
-        rc = L.quoin_b200_index_create(c["ctx"], hs, len(hs), ctypes.byref(idx))
-        if rc:
-            raise Q.Error(rc)
-        c["idx"] = idx
     with torch.cuda.stream(stream):
         decompress_all()
     torch.cuda.synchronize()
@@ -405,9 +397,9 @@ def run_gpu(args, rank, world, local):
         dist.barrier()
     clocks = sampler.stop()
     launches = Q.kernel_launches() - launches0
-    ms_arr = (ctypes.c_double * 8)()
-    calls_arr = (ctypes.c_uint64 * 8)()
-    L.quoin_b200_timing_read(ms_arr, calls_arr, 8)
+    ms_arr = (ctypes.c_double * len(TIMER_NAMES))()
+    calls_arr = (ctypes.c_uint64 * len(TIMER_NAMES))()
+    L.quoin_b200_timing_read(ms_arr, calls_arr, len(TIMER_NAMES))
     enc_ms = sum(ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps))
     dec_ms = sum(ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps))
     total_ms = ev[0].elapsed_time(ev[-1])
@@ -421,7 +413,7 @@ def run_gpu(args, rank, world, local):
     peak, peak_kind = load_peaks()
     dec_alg = stream_bytes + sum(n * c["w"] + ((n + 7) // 8 if c["bm"] is not None else 0) for c in gcols)
     achieved = dec_alg * args.steps / (dec_ms / 1e3) / 1e9 if dec_ms else 0.0
-    per_class = {TIMER_NAMES[i]: (ms_arr[i], int(calls_arr[i])) for i in range(8)}
+    per_class = {TIMER_NAMES[i]: (ms_arr[i], int(calls_arr[i])) for i in range(len(TIMER_NAMES))}
 
     # Per-column kernel-class breakdown (one untimed extra pass per column).
     per_column = {}
@@ -430,8 +422,8 @@ def run_gpu(args, rank, world, local):
         compress_one(c)
         decompress_one(c)
         torch.cuda.synchronize()
-        L.quoin_b200_timing_read(ms_arr, calls_arr, 8)
-        per_column[c["name"]] = {TIMER_NAMES[i]: round(ms_arr[i], 4) for i in range(8) if ms_arr[i] > 0}
+        L.quoin_b200_timing_read(ms_arr, calls_arr, len(TIMER_NAMES))
+        per_column[c["name"]] = {TIMER_NAMES[i]: round(ms_arr[i], 4) for i in range(len(TIMER_NAMES)) if ms_arr[i] > 0}
         per_column[c["name"]]["stream_bytes"] = c["len"]
     L.quoin_b200_timing_enable(0)
 
@@ -559,8 +551,6 @@ def run_gpu(args, rank, world, local):
                "sample": f"first {sample} values of each column (of {n}), oracle C restatement, {threads} threads, "
                          f"median of 3 compress+decompress runs"}
 
-    for c in gcols:
-        L.quoin_b200_index_free(c["idx"])
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -579,16 +569,17 @@ def run_gpu(args, rank, world, local):
             "ratio": round(raw_bytes / stream_bytes, 4), "bit_exact": bit_exact,
             "kernel_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in per_class.items()},
             "per_column_ms": per_column,
-            "roofline": {"bound": "hbm", "kernel": "decode (k_walk_frames, k_prepass, k_prepass_scan, "
-                                                   "k_decode_items, k_decode_frames, k_decimal_combine of the "
-                                                   "three columns in flight together)",
+            "roofline": {"bound": "hbm", "kernel": "decode phase: the device stream reader (k_dp_head, "
+                                                   "k_dp_bitmap, k_word_popcount, scans, k_select_table, "
+                                                   "k_dp_cand_count, k_dp_cand_write, k_dp_chain, k_dp_expand) "
+                                                   "and the block decoder (k_walk_frames, k_prepass, "
+                                                   "k_prepass_scan, k_decode_items, k_decode_frames, "
+                                                   "k_decimal_combine) of the three columns in flight together",
                          "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": (round(DECODE_TRAFFIC_16M[args.workload] * n / (1 << 24))
-                                     if args.workload in DECODE_TRAFFIC_16M else None),
-                         "traffic_note": ("DRAM bytes per decode phase (three decode calls), from an ncu capture "
-                                          "at 16,777,216 values per column scaled by the values processed"
-                                          if args.workload in DECODE_TRAFFIC_16M else "not captured"),
+                         "traffic": DECODE_TRAFFIC.get(args.workload),
+                         "traffic_note": ("DRAM bytes per decode phase (three decode calls) from ncu captures"
+                                          if args.workload in DECODE_TRAFFIC else "not captured for these kernels"),
                          "decode_calls_per_step": per_class["decode"][1] // max(args.steps, 1)},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

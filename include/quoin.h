@@ -238,6 +238,14 @@ int quoin_b200_decompress_column_device(QuoinCtx *ctx, const uint8_t *d_src, siz
                                         uint8_t *d_validity_out, int32_t *wire_out, uint64_t *n_out,
                                         void *stream);
 
+/* Decodes of device-resident streams since the process started: out[0] read
+ * by the device reader, out[1] read by the host reader, out[2] why the last
+ * one was (1 a header the device reader does not take, 2 a frame table it
+ * could not resolve, 3 more frame candidates than its tables held); for the
+ * last stream the device reader read, out[3] its frame-header candidates and
+ * out[4] how many times it laid out its tables (2 after a capacity retry). */
+void quoin_b200_reader_stats(uint64_t out[5]);
+
 /* No counterpart in the reference.  Allocation-free device decode for callers
  * that cannot let the library allocate device memory (an engine that owns all
  * device memory through its own pool, or a process that must keep a fixed
@@ -271,7 +279,7 @@ uint64_t quoin_b200_kernel_launches(void);
 /* Per-kernel-class device time, measured with CUDA events recorded on the
  * launching stream around each launch: 0 competition, 1 emission, 2 block
  * decode, 3 final scatter/narrow, 4 lowering, 5 probe+plan, 6 validity,
- * 7 other.  enable(1) resets and starts recording; read() returns the number
+ * 7 other, 8 the device stream reader.  enable(1) resets and starts recording; read() returns the number
  * of classes written (ms totals and call counts). */
 void quoin_b200_timing_enable(int on);
 int quoin_b200_timing_read(double *ms_out, uint64_t *calls_out, int n);

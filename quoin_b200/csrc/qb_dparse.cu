@@ -8,10 +8,11 @@
 // thread following it pays one memory latency per frame (thousands per
 // column), so the chain is resolved in parallel instead:
 //   1. every byte position of a lane whose 9 bytes could be a frame header
-//      (mode id known, 1 <= n <= 131072, plen < 2^24 and within the lane) is a
-//      candidate: one pass over the lane, with a zero-byte test on 8-byte
-//      words that rejects almost every position in a few instructions
-//      (k_dp_cand_count, a scan, k_dp_cand_write, in position order);
+//      (mode id known, 1 <= n <= 131072, plen < 2^24 and within the lane) and
+//      whose payload passes its mode's first decode checks is a candidate:
+//      one pass over the lane, with a zero-byte test on 8-byte words that
+//      rejects most positions in a few instructions (k_dp_cand_count, a scan,
+//      k_dp_cand_write, in position order);
 //   2. each candidate's successor (the candidate at pos + 9 + plen) is found
 //      by binary search; marks spread from the lane's first frame along the
 //      successors by pointer doubling, so after log2(K) rounds exactly the
@@ -39,12 +40,60 @@ constexpr int kChainThreads = 1024;
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint64_t kMaxLogicalD = 1ull << 36;  // the host reader's allocation limit (decoder.rs:105-106)
 
-__device__ inline bool dp_mode_known(uint32_t id) {  // reference mode.rs:60-84
+// Mode ids a frame candidate may carry: every mode of mode.rs:60-84 except
+// PRED (0).  A PRED payload is bare LEB128 with no tag or length, so in the
+// zero-rich bytes of bit-packed payloads "00 n n n 00 p p p 00" passes as a
+// PRED header everywhere; a stream with PRED frames (High/Max only) breaks
+// the chain and is read by the host reader instead.
+__device__ inline bool dp_mode_candidate(uint32_t id) {
   switch (id) {
-    case 0: case 1: case 2: case 3: case 4: case 5: case 7: case 9: case 11: case 17:
+    case 1: case 2: case 3: case 4: case 5: case 7: case 9: case 11: case 17:
     case 19: case 20: case 25: case 29: case 45: case 50: case 51: case 52: case 53: case 54:
       return true;
     default: return false;
+  }
+}
+
+// A varint within p[pos .. lim) (at most 10 bytes), or false.
+__device__ inline bool dp_varint(const uint8_t* s, uint64_t pos, uint64_t lim, uint64_t* v) {
+  uint64_t r = 0;
+  for (uint32_t k = 0; k < 10 && pos + k < lim; k++) {
+    uint32_t b = s[pos + k];
+    r |= (uint64_t)(b & 0x7F) << (7 * k);
+    if (!(b & 0x80)) {
+      *v = r;
+      return true;
+    }
+  }
+  return false;
+}
+
+// What every frame of `mode` that decodes satisfies (the codec decoders'
+// first checks: raw.rs, const_block.rs, stride.rs, xorz.rs:18-32,
+// for_bitpack.rs:108-120, delta_bitpack.rs:48-64, alp.rs:168-180,
+// float_mult.rs:100-110, dict.rs:150-160, rle.rs:45-55, alp_rd.rs:208-215,
+// and entropy/mod.rs:152-178 for the entropy-coded modes: a tag 0..3, then a
+// varint length no larger than the decode bound).  A frame that fails it
+// cannot decode, so leaving it out only sends damaged streams to the host
+// reader.
+__device__ bool dp_frame_plausible(const uint8_t* s, uint64_t pl0, uint32_t n, uint32_t plen, uint32_t mode,
+                                   uint32_t lane_bytes_) {
+  uint64_t lim = pl0 + plen, v = 0;
+  switch (mode) {
+    case 5: return (uint64_t)plen == (uint64_t)n * lane_bytes_;
+    case 1: return plen == 8;
+    case 2: return plen == 16;
+    case 3: return plen >= n && (uint64_t)plen <= 10ull * n && s[lim - 1] < 0x80;
+    case 50: case 9: return dp_varint(s, pl0, lim, &v) && v == n;
+    case 51: return plen >= 9 && dp_varint(s, pl0 + 8, lim, &v) && v == n;
+    case 17: return plen >= 2 && s[pl0] <= 1 && s[pl0 + 1] < 7;
+    case 19: case 53: return dp_varint(s, pl0, lim, &v) && v <= n;
+    case 52: return plen >= 2 && s[pl0] >= 1 && s[pl0] <= 63 && s[pl0 + 1] <= 8;
+    case 11: case 4: case 7: case 20: case 45: case 25: case 29: {
+      uint64_t mx = mode == 11 ? 8ull * n + 16 : (mode == 4 ? 16ull * n + 1024 : 10ull * n + 16);
+      return plen >= 2 && s[pl0] <= 3 && dp_varint(s, pl0 + 1, lim, &v) && v <= mx;
+    }
+    default: return true;  // PCO: no reader here, its decode reports it
   }
 }
 
@@ -74,16 +123,17 @@ __device__ bool dp_lane_header(const uint8_t* s, uint64_t base, uint64_t len, Dp
   return L.logical_n <= kMaxLogicalD;
 }
 
-// The RAW validity blob at s[pos .. pos + vlen) (validity.rs:73-90): tag 0
-// then ceil(n/8) bytes.
+// The validity blob at s[pos .. pos + vlen) (validity.rs:73-119): tag 0 then
+// ceil(n/8) bitmap bytes, or tag 1 then varint run lengths.
 __device__ bool dp_validity(const uint8_t* s, uint64_t len, uint64_t* pos, uint64_t n, DpHead& H) {
   uint64_t vlen;
   if (rd_varint(s, len, pos, &vlen) != E_OK || vlen > len - *pos || vlen == 0) return false;
-  if (s[*pos] != 0) return false;  // RLE blob: the host reader decodes it
+  uint32_t tag = s[*pos];
   uint64_t raw = (n + 7) / 8;
-  if (vlen - 1 < raw) return false;
+  if (tag > 1 || (tag == 0 && vlen - 1 < raw)) return false;
+  H.vtag = tag;
   H.vblob_off = *pos + 1;
-  H.vblob_len = raw;
+  H.vblob_len = tag == 0 ? raw : vlen - 1;
   *pos += vlen;
   return true;
 }
@@ -153,11 +203,133 @@ __global__ void k_dp_bitmap(const uint8_t* __restrict__ s, const DpHead* __restr
   }
 }
 
+// RLE blob (validity.rs:92-119): alternating run lengths (LEB128), nulls
+// first, read until the runs cover n positions.  One CTA reads the blob 16 KB
+// a round: terminator bytes (high bit clear) end varints, a scan numbers
+// them, the thread holding a terminator assembles its varint (at most 10
+// bytes back, as rd_varint reads), and a scan of the run lengths gives each
+// run's end position.  Anything the sequential reader would reject (a run
+// past n, a varint over 10 bytes, a blob that ends first) sets H->kind; an
+// odd byte after the last run is left unread, as the sequential reader
+// leaves it (the round's check covers only varints before the last run).
+constexpr int kRleThreads = 1024;
+__global__ void __launch_bounds__(kRleThreads) k_dp_rle_runs(const uint8_t* __restrict__ s, DpHead* __restrict__ H,
+                                                             uint64_t n, uint64_t* __restrict__ ends,
+                                                             uint64_t* __restrict__ nruns) {
+  __shared__ uint64_t s_warp[33];
+  const uint8_t* b = s + H->vblob_off;
+  const uint64_t blen = H->vblob_len;
+  const int tid = threadIdx.x;
+  uint64_t carry_pos = 0, carry_k = 0;
+  int64_t prev_term = -1;  // the last terminator before the round (blob offset)
+  bool bad = false, done = n == 0;
+  for (uint64_t base = 0; base < blen && !done; base += 16ull * kRleThreads) {
+    uint64_t a = base + 16ull * tid;
+    uint32_t tm = 0;
+    for (int i = 0; i < 16; i++)
+      if (a + i < blen && !(b[a + i] & 0x80)) tm |= 1u << i;
+    int64_t mylast = tm ? (int64_t)(a + 31 - __clz(tm)) : -1;
+    uint64_t rk, mt;
+    uint64_t k0 = block_excl_scan<ScanSum>((uint64_t)__popc(tm), s_warp, &rk);
+    // previous terminator before the thread's bytes: max over earlier threads
+    uint64_t pm = block_excl_scan<ScanMax>((uint64_t)(mylast + 1), s_warp, &mt);
+    int64_t prev = (int64_t)pm - 1 > prev_term ? (int64_t)pm - 1 : prev_term;
+    // the thread's varints: lengths summed in order; a too-long one is bad
+    uint64_t sum = 0;
+    bool mybad = false;
+    {
+      int64_t pv = prev;
+      uint32_t m = tm;
+      while (m) {
+        int64_t j = (int64_t)a + (__ffs(m) - 1);
+        m &= m - 1;
+        int64_t st = pv + 1;
+        if (j - st + 1 > 10) mybad = true;
+        uint64_t v = 0;
+        for (int64_t q = st; q <= j && q < st + 10; q++) v |= (uint64_t)(b[q] & 0x7F) << (7 * (q - st));
+        sum += v;
+        pv = j;
+      }
+    }
+    uint64_t tot;
+    uint64_t sx = block_excl_scan<ScanSum>(sum, s_warp, &tot);
+    // write run ends; the first run reaching n ends the reading
+    uint64_t pos = carry_pos + sx, k = carry_k + k0;
+    bool reach = false, over = false;
+    {
+      int64_t pv = prev;
+      uint32_t m = tm;
+      while (m) {
+        int64_t j = (int64_t)a + (__ffs(m) - 1);
+        m &= m - 1;
+        int64_t st = pv + 1;
+        uint64_t v = 0;
+        for (int64_t q = st; q <= j && q < st + 10; q++) v |= (uint64_t)(b[q] & 0x7F) << (7 * (q - st));
+        bool before_end = pos < n;  // this run is read by the sequential reader
+        if (before_end) {
+          if (v > n - pos) over = true;
+          ends[k] = pos + v;
+          if (pos + v >= n) {
+            reach = true;
+            *nruns = k + 1;
+          }
+        }
+        pos += v;
+        k++;
+        pv = j;
+      }
+    }
+    // a too-long varint counts when it starts before the covering run ends:
+    // conservatively, any in a round that reads at least one run
+    bad = __syncthreads_or(over || (mybad && carry_pos < n)) || bad;
+    done = __syncthreads_or(reach) != 0;
+    carry_pos += tot;
+    carry_k += rk;
+    if ((int64_t)mt - 1 > prev_term) prev_term = (int64_t)mt - 1;
+  }
+  if (tid == 0) {
+    if (n == 0) *nruns = 0;
+    if (bad || !done) H->kind = 1;  // the host reader reports the error
+  }
+}
+
+// Bitmap word w from the run ends: runs alternate null / valid from a null
+// run; word w's bits come from the runs overlapping [32w, 32w + 32).
+__global__ void k_dp_rle_fill(const DpHead* __restrict__ H, uint64_t n, const uint64_t* __restrict__ ends,
+                              const uint64_t* __restrict__ nruns_p, uint32_t* __restrict__ bm32) {
+  uint64_t nw = (n + 31) / 32, nr = H->kind ? 0 : *nruns_p;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw + 1; w += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = w * 32, hi = lo + 32;
+    uint32_t bits = 0;
+    if (w < nw && nr) {
+      uint64_t a = 0, z = nr;  // first run whose end is above lo
+      while (a < z) {
+        uint64_t mid = (a + z) >> 1;
+        if (ends[mid] <= lo) a = mid + 1; else z = mid;
+      }
+      for (uint64_t r = a; r < nr; r++) {
+        uint64_t st = r ? ends[r - 1] : 0, en = ends[r];
+        if (st >= hi) break;
+        if (r & 1) {
+          uint64_t x = st > lo ? st : lo, y = en < hi ? en : hi;
+          if (y > x) {
+            uint32_t len = (uint32_t)(y - x), sh = (uint32_t)(x - lo);
+            bits |= (len == 32 ? 0xFFFFFFFFu : ((1u << len) - 1u)) << sh;
+          }
+        }
+      }
+      if (hi > n) bits &= (n - lo) >= 32 ? 0xFFFFFFFFu : ((1u << (uint32_t)(n - lo)) - 1u);
+    }
+    bm32[w] = bits;  // the word past the end stays 0 (the popcount reads whole words)
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Candidates.  CTA j covers positions [fstart + j*kDpChunk, +kDpChunk) of
 // lane `lane`; thread t the 16 positions from 16t.
 // ---------------------------------------------------------------------------
-__device__ inline uint32_t dp_thread_cands(const uint8_t* __restrict__ s, uint64_t buf_len, uint64_t a, uint64_t end) {
+__device__ inline uint32_t dp_thread_cands(const uint8_t* __restrict__ s, uint64_t buf_len, uint64_t a, uint64_t end,
+                                           uint32_t lb) {
   // a = first position; end = lane end; a header at p needs p + 9 <= end
   if (a + 9 > end) return 0;
   uint64_t w0, w1, w2;
@@ -187,7 +359,9 @@ __device__ inline uint32_t dp_thread_cands(const uint8_t* __restrict__ s, uint64
     uint64_t p = a + i;
     uint32_t mode = s[p];
     uint32_t n = ld_u32(s + p + 1), plen = ld_u32(s + p + 5);
-    if (dp_mode_known(mode) && n >= 1 && n <= (uint32_t)kMaxBlock && plen <= end - p - 9) out |= 1u << i;
+    if (dp_mode_candidate(mode) && n >= 1 && n <= (uint32_t)kMaxBlock && plen <= end - p - 9 &&
+        dp_frame_plausible(s, p + 9, n, plen, mode, lb))
+      out |= 1u << i;
   }
   return out;
 }
@@ -199,7 +373,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp_cand_count(const uint8_t* __r
   const DpLane& L = H->lanes[lane];
   uint64_t end = L.base + L.len;
   uint64_t a = L.fstart + (uint64_t)blockIdx.x * kDpChunk + 16ull * threadIdx.x;
-  uint32_t c = H->kind ? 0u : (uint32_t)__popc(dp_thread_cands(s, buf_len, a, end));
+  uint32_t c = H->kind ? 0u : (uint32_t)__popc(dp_thread_cands(s, buf_len, a, end, lane_bytes((int)L.dtype)));
   for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
   __syncthreads();
@@ -222,7 +396,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp_cand_write(const uint8_t* __r
   const DpLane& L = H->lanes[lane];
   uint64_t end = L.base + L.len;
   uint64_t a = L.fstart + (uint64_t)blockIdx.x * kDpChunk + 16ull * threadIdx.x;
-  uint32_t m = dp_thread_cands(s, buf_len, a, end);
+  uint32_t m = dp_thread_cands(s, buf_len, a, end, lane_bytes((int)L.dtype));
   uint64_t at = base + block_excl_scan<ScanSum>((uint64_t)__popc(m), s_warp, nullptr);
   while (m) {
     uint32_t i = __ffs(m) - 1;
@@ -540,6 +714,15 @@ void launch_dp_bitmap(const uint8_t* s, const DpHead* H, uint64_t raw_len, uint8
   if (g == 0) g = 1;
   k_dp_bitmap<<<g, 256, 0, st>>>(s, H, bm);
   count_launches(1);
+}
+
+void launch_dp_bitmap_rle(const uint8_t* s, DpHead* H, uint64_t n, uint64_t* ends, uint64_t* nruns, uint8_t* bm,
+                          cudaStream_t st) {
+  k_dp_rle_runs<<<1, kRleThreads, 0, st>>>(s, H, n, ends, nruns);
+  uint64_t nw = (n + 31) / 32 + 1;
+  unsigned g = (unsigned)qmin((nw + 255) / 256, 148ull * 8);
+  k_dp_rle_fill<<<g, 256, 0, st>>>(H, n, ends, nruns, reinterpret_cast<uint32_t*>(bm));
+  count_launches(2);
 }
 
 uint64_t dp_chunks(uint64_t lane_frames_bytes) { return (lane_frames_bytes + kDpChunk - 1) / kDpChunk; }

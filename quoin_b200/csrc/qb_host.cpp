@@ -31,7 +31,8 @@ using namespace qb;
 // stream, resolved after the call's final synchronisation).
 // ---------------------------------------------------------------------------
 namespace {
-enum TimerClass { T_COMPETE = 0, T_EMIT, T_DECODE, T_FINALIZE, T_LOWER, T_PLAN, T_VALIDITY, T_OTHER, T_COUNT };
+enum TimerClass { T_COMPETE = 0, T_EMIT, T_DECODE, T_FINALIZE, T_LOWER, T_PLAN, T_VALIDITY, T_OTHER, T_READ,
+                  T_COUNT };
 struct Timing {
   std::atomic<bool> on{false};
   std::mutex mu;
@@ -196,7 +197,7 @@ inline int plain_code(int ext) {
 enum Slot {
   S_IN, S_BM, S_RANK, S_LANE, S_GROW, S_FRAMES, S_NB, S_SIZES, S_TILE, S_SCRATCH, S_OUT, S_VTMP, S_VBLOB,
   S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_DAUX, S_SUBST, S_FMST,
-  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_ENT, S_ENTREC, S_DPMISC, S_DPCAND, S_DPJ, S_COUNT
+  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_ENT, S_ENTREC, S_DPMISC, S_DPCAND, S_DPJ, S_DPRUNS, S_COUNT
 };
 
 struct QuoinCtx {
@@ -1273,9 +1274,16 @@ struct DpMisc {  // the reader's small results, read back in one copy
   DpLaneOut lanes[4];
   uint64_t nvalid;
   uint64_t ncand[4];
+  uint64_t nruns;  // runs of an RLE validity blob
 };
 constexpr uint64_t kDpHeadOff = 0, kDpMiscOff = 512;
 static_assert(sizeof(DpHead) <= kDpMiscOff && sizeof(DpMisc) <= 512, "reader results fit their slot");
+
+// Decodes of device streams read by the device reader, and those the host
+// reader took (with the reason of the last: 1 header, 2 a lane's chain, 3 a
+// lane still over capacity after the exact count).
+std::atomic<uint64_t> g_reads_device{0}, g_reads_host{0}, g_reads_host_reason{0};
+std::atomic<uint64_t> g_last_ncand{0}, g_last_attempts{0};  // the last device read: candidates, table rounds
 
 // Candidate capacity of a lane whose frames span `bytes`: encoder streams
 // hold far fewer frames (one per 32,768 values for adaptive blocks); a lane
@@ -1285,7 +1293,10 @@ uint64_t dp_cap(uint64_t bytes) { return bytes / 512 + 8192; }
 // The host reader's route for the streams the device reader leaves to it: a
 // host copy, parsed and uploaded as for a host-buffer decode.
 int decode_device_via_host(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t len, void* d_out,
-                           uint64_t out_cap_bytes, uint8_t* d_valid_out, int32_t* wire_out, uint64_t* n_out) {
+                           uint64_t out_cap_bytes, uint8_t* d_valid_out, int32_t* wire_out, uint64_t* n_out,
+                           int reason) {
+  g_reads_host.fetch_add(1);
+  g_reads_host_reason.store((uint64_t)reason);
   std::vector<uint8_t> h(len);
   if (len) CK(cudaMemcpyAsync(h.data(), d_src, len, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -1322,10 +1333,14 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
   DpHead* dH = reinterpret_cast<DpHead*>(misc + kDpHeadOff);
   DpMisc* dM = reinterpret_cast<DpMisc*>(misc + kDpMiscOff);
   CK(cudaMemsetAsync(dM, 0, sizeof(DpMisc), st));  // the valid count stays 0 without a bitmap
-  launch_dp_head(d_src, len, dH, st);
+  {
+    TimedRegion tr(T_READ, st);
+    launch_dp_head(d_src, len, dH, st);
+  }
   DpHead H;
   CK(read_small(c, st, &H, dH, sizeof(H)));
-  if (H.kind) return decode_device_via_host(c, st, d_src, len, d_out, out_cap_bytes, d_valid_out, wire_out, n_out);
+  if (H.kind)
+    return decode_device_via_host(c, st, d_src, len, d_out, out_cap_bytes, d_valid_out, wire_out, n_out, 1);
   *wire_out = (int32_t)H.wire;
   *n_out = H.n;
   uint32_t w = native_width((int)H.wire);
@@ -1334,10 +1349,16 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
   const uint64_t nw = (n + 31) / 32;
   // validity: bitmap, word ranks, valid count, select table
   if (H.has_validity && n) {
-    CK(c->ensure(S_DBM, (H.vblob_len + 7) / 8 * 8 + 16));
+    TimedRegion tr(T_READ, st);
+    CK(c->ensure(S_DBM, (nw + 2) * 4 + 16));
     CK(c->ensure(S_DRANK, (nw + 1) * 8));
     CK(c->ensure(S_TILE, (scan_tile_count(nw + 4096) + 16) * 8));
-    launch_dp_bitmap(d_src, dH, H.vblob_len, c->p<uint8_t>(S_DBM), st);
+    if (H.vtag == 0) {
+      launch_dp_bitmap(d_src, dH, H.vblob_len, c->p<uint8_t>(S_DBM), st);
+    } else {  // run lengths: at most one run per blob byte
+      CK(c->ensure(S_DPRUNS, (H.vblob_len + 2) * 8));
+      launch_dp_bitmap_rle(d_src, dH, n, c->p<uint64_t>(S_DPRUNS), &dM->nruns, c->p<uint8_t>(S_DBM), st);
+    }
     launch_word_popcount(c->p<uint8_t>(S_DBM), n, c->p<uint64_t>(S_DRANK), st);
     launch_scan_sum(c->p<uint64_t>(S_DRANK), c->p<uint64_t>(S_DRANK), nw, c->p<uint64_t>(S_TILE), &dM->nvalid, st);
     if (!H.decimal) {
@@ -1386,6 +1407,7 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
     uint8_t* cb = c->p<uint8_t>(S_DPCAND);
     uint64_t* ditems = c->p<uint64_t>(S_DITEMS);
     const uint64_t* d_nvalid = H.has_validity ? &dM->nvalid : nullptr;
+    TimedRegion tr(T_READ, st);
     for (int k = 0; k < nl; k++) {
       const DpLane& L = H.lanes[k];
       uint64_t fb = L.base + L.len - L.fstart;
@@ -1405,6 +1427,10 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
     }
     DpMisc M;
     CK(read_small(c, st, &M, dM, sizeof(M)));
+    uint64_t ncand = 0;
+    for (int k = 0; k < nl; k++) ncand += M.ncand[k];
+    g_last_ncand.store(ncand);
+    g_last_attempts.store((uint64_t)attempt + 1);
     bool grow = false, host = false;
     for (int k = 0; k < nl; k++) {
       if (!M.lanes[k].status) continue;
@@ -1415,7 +1441,9 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
         host = true;
       }
     }
-    if (host) return decode_device_via_host(c, st, d_src, len, d_out, out_cap_bytes, d_valid_out, wire_out, n_out);
+    if (host)
+      return decode_device_via_host(c, st, d_src, len, d_out, out_cap_bytes, d_valid_out, wire_out, n_out,
+                                    attempt ? 3 : 2);
     if (grow) continue;
     // the index the block decoder runs from
     QuoinDecodeIndex X;
@@ -1451,11 +1479,12 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
       L.nlist = O.nlist;
       X.max_pre = L.npre > X.max_pre ? L.npre : X.max_pre;
     }
+    g_reads_device.fetch_add(1);
     const uint64_t* dvmin = reinterpret_cast<const uint64_t*>(misc + kDpHeadOff + offsetof(DpHead, vmin));
     return decode_indexed(c, st, X, c->p<FrameDesc>(S_DFRAMES), c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK),
                           c->p<uint64_t>(S_DSEL), dvmin, ditems, d_src, d_out, d_valid_out);
   }
-  return decode_device_via_host(c, st, d_src, len, d_out, out_cap_bytes, d_valid_out, wire_out, n_out);
+  return decode_device_via_host(c, st, d_src, len, d_out, out_cap_bytes, d_valid_out, wire_out, n_out, 3);
 }
 
 // Host-buffer compress of a typed column (wire dtype, native little-endian values).
@@ -1946,6 +1975,15 @@ int quoin_b200_decompress_column_device(QuoinCtx* ctx, const uint8_t* d_src, siz
   } catch (...) {
     return QUOIN_ERR_PANIC;
   }
+}
+
+void quoin_b200_reader_stats(uint64_t out[5]) {
+  if (!out) return;
+  out[0] = g_reads_device.load();
+  out[1] = g_reads_host.load();
+  out[2] = g_reads_host_reason.load();
+  out[3] = g_last_ncand.load();
+  out[4] = g_last_attempts.load();
 }
 
 void quoin_b200_mode_win_counts(uint64_t out[64]) {

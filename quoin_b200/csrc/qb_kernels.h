@@ -84,7 +84,8 @@ struct DpHead {
   uint32_t kind, wire, decimal, has_validity, nl, precision;
   int32_t scale, pad;
   uint64_t n;
-  uint64_t vblob_off, vblob_len;  // the RAW validity bitmap's bytes
+  uint64_t vblob_off, vblob_len;  // the validity blob's bytes after its tag
+  uint32_t vtag, pad2;            // 0 RAW (ceil(n/8) bitmap bytes), 1 RLE (varint runs)
   uint64_t vmin[4];
   DpLane lanes[4];
 };
@@ -112,6 +113,11 @@ struct DpTables {
 constexpr uint64_t kDpChainSmem = 200 * 1024;  // successor tables in shared memory up to 22,755 candidates
 void launch_dp_head(const uint8_t* s, uint64_t len, DpHead* H, cudaStream_t st);
 void launch_dp_bitmap(const uint8_t* s, const DpHead* H, uint64_t raw_len, uint8_t* bm, cudaStream_t st);
+// RLE validity blob (validity.rs:92-119) into the n-bit bitmap bm (ceil(n/32)
+// words written); `ends` holds vblob_len entries.  A blob the sequential
+// reader would reject sets H->kind, so the host reader takes the stream.
+void launch_dp_bitmap_rle(const uint8_t* s, DpHead* H, uint64_t n, uint64_t* ends, uint64_t* nruns, uint8_t* bm,
+                          cudaStream_t st);
 // Candidate chunks of a lane whose frames span `lane_frames_bytes` bytes (cnt
 // needs dp_chunks() + 1 entries; *d_ncand gets the count, at most cap written).
 uint64_t dp_chunks(uint64_t lane_frames_bytes);
