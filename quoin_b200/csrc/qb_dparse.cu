@@ -11,17 +11,18 @@
 //      (mode id known, 1 <= n <= 131072, plen < 2^24 and within the lane) and
 //      whose payload passes its mode's first decode checks is a candidate:
 //      one pass over the lane, with a zero-byte test on 8-byte words that
-//      rejects most positions in a few instructions (k_dp_cand_count, a scan,
-//      k_dp_cand_write, in position order);
+//      rejects most positions in a few instructions (k_dp_cand_scan, a scan
+//      of the per-chunk counts, k_dp_cand_compact, in position order);
 //   2. each candidate's successor (the candidate at pos + 9 + plen) is found
-//      by binary search; marks spread from the lane's first frame along the
-//      successors by pointer doubling, so after log2(K) rounds exactly the
-//      frames on the chain are marked (every jump from a chain frame lands on
-//      a chain frame), and chain order is position order (k_dp_chain);
-//   3. the marked frames are cut where their values reach the lane's count,
-//      and each frame's warp items (512 values, or 512 XORZ payload bytes)
-//      are counted and laid out as the host reader's build_items does
-//      (k_dp_chain), then listed (k_dp_expand).
+//      by binary search (k_dp_succ, across the GPU); marks spread from the
+//      lane's first frame along the successors by pointer doubling, so after
+//      log2(K) rounds exactly the frames on the chain are marked (every jump
+//      from a chain frame lands on a chain frame), and chain order is
+//      position order (k_dp_marks, one CTA);
+//   3. the marked frames' warp items (512 values, or 512 XORZ payload bytes)
+//      are counted as the host reader's build_items does (k_dp_items, across
+//      the GPU), the frames cut where their values reach the lane's count and
+//      laid out (k_dp_layout, one CTA), and the items listed (k_dp_expand).
 // A stream the fast path cannot take (a header or validity error, an RLE
 // validity blob, a chain frame that is not a candidate, a count mismatch,
 // more candidates than the tables hold) is flagged, and the host reader
@@ -35,24 +36,12 @@ namespace qb {
 namespace {
 
 constexpr int kDpThreads = 256;
-constexpr uint64_t kDpChunk = (uint64_t)kDpThreads * 16;  // positions per candidate CTA
+constexpr int kDpSteps = 4;
+constexpr uint64_t kDpStep = (uint64_t)kDpThreads * 16;  // positions per CTA step
+constexpr uint64_t kDpChunk = kDpStep * kDpSteps;        // positions per candidate CTA
 constexpr int kChainThreads = 1024;
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint64_t kMaxLogicalD = 1ull << 36;  // the host reader's allocation limit (decoder.rs:105-106)
-
-// Mode ids a frame candidate may carry: every mode of mode.rs:60-84 except
-// PRED (0).  A PRED payload is bare LEB128 with no tag or length, so in the
-// zero-rich bytes of bit-packed payloads "00 n n n 00 p p p 00" passes as a
-// PRED header everywhere; a stream with PRED frames (High/Max only) breaks
-// the chain and is read by the host reader instead.
-__device__ inline bool dp_mode_candidate(uint32_t id) {
-  switch (id) {
-    case 1: case 2: case 3: case 4: case 5: case 7: case 9: case 11: case 17:
-    case 19: case 20: case 25: case 29: case 45: case 50: case 51: case 52: case 53: case 54:
-      return true;
-    default: return false;
-  }
-}
 
 // A varint within p[pos .. lim) (at most 10 bytes), or false.
 __device__ inline bool dp_varint(const uint8_t* s, uint64_t pos, uint64_t lim, uint64_t* v) {
@@ -188,18 +177,27 @@ __global__ void k_dp_head(const uint8_t* __restrict__ s, uint64_t len, DpHead* _
   *out = H;
 }
 
-// Bitmap bytes of the RAW blob with the bits past n cleared, and the bytes
-// after it zeroed up to the next 8 (the popcount reads whole words).
-__global__ void k_dp_bitmap(const uint8_t* __restrict__ s, const DpHead* __restrict__ H, uint8_t* __restrict__ bm) {
-  uint64_t off = H->vblob_off, nb = H->vblob_len, n = H->n;
-  uint64_t end = (nb + 7) & ~7ull;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += (uint64_t)gridDim.x * blockDim.x) {
-    uint8_t b = 0;
-    if (i < nb) {
-      b = s[off + i];
-      if (i == nb - 1 && (n & 7)) b &= (uint8_t)((1u << (n & 7)) - 1u);
+// Bitmap words of the RAW blob (bits past n cleared) and each word's
+// popcount, one word per thread; the word after the last is zeroed (readers
+// of whole words stop there).
+__global__ void k_dp_bitmap(const uint8_t* __restrict__ s, const DpHead* __restrict__ H, uint32_t* __restrict__ bm32,
+                            uint64_t* __restrict__ cnt) {
+  const uint8_t* src = s + H->vblob_off;
+  uint64_t nb = H->vblob_len, n = H->n, nw = (n + 31) / 32;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w <= nw; w += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t bits = 0;
+    if (w < nw) {
+      uint64_t b0 = 4 * w;
+      if (b0 + 4 <= nb) {
+        bits = ld_u32(src + b0);
+      } else {
+        for (uint64_t k = 0; k < 4 && b0 + k < nb; k++) bits |= (uint32_t)src[b0 + k] << (8 * k);
+      }
+      uint64_t rem = n - 32 * w;
+      if (rem < 32) bits &= (1u << rem) - 1u;
+      cnt[w] = (uint64_t)__popc(bits);
     }
-    bm[i] = b;
+    bm32[w] = bits;
   }
 }
 
@@ -296,7 +294,8 @@ __global__ void __launch_bounds__(kRleThreads) k_dp_rle_runs(const uint8_t* __re
 // Bitmap word w from the run ends: runs alternate null / valid from a null
 // run; word w's bits come from the runs overlapping [32w, 32w + 32).
 __global__ void k_dp_rle_fill(const DpHead* __restrict__ H, uint64_t n, const uint64_t* __restrict__ ends,
-                              const uint64_t* __restrict__ nruns_p, uint32_t* __restrict__ bm32) {
+                              const uint64_t* __restrict__ nruns_p, uint32_t* __restrict__ bm32,
+                              uint64_t* __restrict__ cnt) {
   uint64_t nw = (n + 31) / 32, nr = H->kind ? 0 : *nruns_p;
   for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw + 1; w += (uint64_t)gridDim.x * blockDim.x) {
     uint64_t lo = w * 32, hi = lo + 32;
@@ -320,96 +319,201 @@ __global__ void k_dp_rle_fill(const DpHead* __restrict__ H, uint64_t n, const ui
       }
       if (hi > n) bits &= (n - lo) >= 32 ? 0xFFFFFFFFu : ((1u << (uint32_t)(n - lo)) - 1u);
     }
-    bm32[w] = bits;  // the word past the end stays 0 (the popcount reads whole words)
+    if (w < nw) cnt[w] = (uint64_t)__popc(bits);
+    bm32[w] = bits;  // the word past the end stays 0
   }
 }
 
 // ---------------------------------------------------------------------------
-// Candidates.  CTA j covers positions [fstart + j*kDpChunk, +kDpChunk) of
-// lane `lane`; thread t the 16 positions from 16t.
+// Candidates: CTA j of a lane covers kDpChunk positions (dp_thread_cands).
 // ---------------------------------------------------------------------------
-__device__ inline uint32_t dp_thread_cands(const uint8_t* __restrict__ s, uint64_t buf_len, uint64_t a, uint64_t end,
-                                           uint32_t lb) {
-  // a = first position; end = lane end; a header at p needs p + 9 <= end
-  if (a + 9 > end) return 0;
-  uint64_t w0, w1, w2;
-  if (a + 24 <= buf_len) {
-    w0 = ld_u64(s + a);
-    w1 = ld_u64(s + a + 8);
-    w2 = ld_u64(s + a + 16);
+// Mode ids a frame candidate may carry, as a bit mask (every id is below 64):
+// every mode of mode.rs:60-84 except PRED (0).  A PRED payload is bare LEB128
+// with no tag or length, so in the zero-rich bytes of bit-packed payloads
+// "00 n n n 00 p p p 00" passes as a PRED header everywhere; a stream with
+// PRED frames (High/Max only) breaks the chain and is read by the host reader.
+constexpr uint64_t kCandModes = (1ull << 1) | (1ull << 2) | (1ull << 3) | (1ull << 4) | (1ull << 5) | (1ull << 7) |
+                                (1ull << 9) | (1ull << 11) | (1ull << 17) | (1ull << 19) | (1ull << 20) |
+                                (1ull << 25) | (1ull << 29) | (1ull << 45) | (1ull << 50) | (1ull << 51) |
+                                (1ull << 52) | (1ull << 53) | (1ull << 54);
+static_assert(((kCandModes >> 0) & 1) == 0, "PRED is not a candidate mode");
+
+// Bytes i .. i+7 of the window (i < 16).
+__device__ __forceinline__ uint64_t dp_bytes8(uint64_t w0, uint64_t w1, uint64_t w2, uint32_t i) {
+  uint64_t lo = i < 8 ? w0 : w1, hi = i < 8 ? w1 : w2;
+  uint32_t sh = 8 * (i & 7);
+  return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+}
+
+// Chunk j of a lane starts at the 16-byte aligned address at or below its
+// first frame offset, plus j * kDpChunk, and is read in kDpSteps steps of
+// kDpThreads * 16 positions; in a step thread t takes the 16 positions from
+// 16t: one aligned 16-byte load, and the 8 bytes after it from the next lane
+// (the last lane loads them).  Bytes past the buffer read as 0xFF, which no
+// test below takes for a header byte.  Returns the candidate positions among
+// a .. a+15 as a bit mask (bit i = position a + i).  All 32 lanes of the warp
+// call it.
+__device__ inline uint64_t dp_chunk_base(const uint8_t* s, const DpLane& L) {
+  return L.fstart - (((uintptr_t)(s + L.fstart)) & 15);
+}
+struct DpWin {
+  uint4 v;     // bytes a .. a+15
+  uint2 next;  // bytes a+16 .. a+23 (loaded by the warp's last lane only)
+};
+__device__ __forceinline__ DpWin dp_load(const uint8_t* __restrict__ s, uint64_t buf_len, uint64_t a) {
+  DpWin w;
+  if (a + 16 <= buf_len) {
+    w.v = __ldg(reinterpret_cast<const uint4*>(s + a));
   } else {
-    w0 = w1 = w2 = 0;
-#pragma unroll
-    for (int i = 0; i < 24; i++) {
-      uint64_t b = (a + i < buf_len) ? s[a + i] : 0xFF;  // past the buffer: never zero
-      if (i < 8) w0 |= b << (8 * i);
-      else if (i < 16) w1 |= b << (8 * (i - 8));
-      else w2 |= b << (8 * (i - 16));
+    uint32_t q[4] = {0, 0, 0, 0};
+    for (int i = 0; i < 16; i++) q[i >> 2] |= (uint32_t)((a + i < buf_len) ? s[a + i] : 0xFF) << (8 * (i & 3));
+    w.v = make_uint4(q[0], q[1], q[2], q[3]);
+  }
+  w.next = make_uint2(0, 0);
+  if ((threadIdx.x & 31) == 31) {
+    if (a + 24 <= buf_len) {
+      w.next = __ldg(reinterpret_cast<const uint2*>(s + a + 16));
+    } else {
+      uint32_t q[2] = {0, 0};
+      for (int i = 0; i < 8; i++) q[i >> 2] |= (uint32_t)((a + 16 + i < buf_len) ? s[a + 16 + i] : 0xFF) << (8 * (i & 3));
+      w.next = make_uint2(q[0], q[1]);
     }
   }
+  return w;
+}
+
+__device__ inline uint32_t dp_thread_cands(const uint8_t* __restrict__ s, const DpLane& L, uint64_t a,
+                                           const DpWin& W) {
+  const uint64_t end = L.base + L.len;
+  uint32_t n0 = __shfl_down_sync(0xffffffffu, W.v.x, 1), n1 = __shfl_down_sync(0xffffffffu, W.v.y, 1);
+  if ((threadIdx.x & 31) == 31) {
+    n0 = W.next.x;
+    n1 = W.next.y;
+  }
+  uint64_t w0 = W.v.x | ((uint64_t)W.v.y << 32), w1 = W.v.z | ((uint64_t)W.v.w << 32), w2 = n0 | ((uint64_t)n1 << 32);
+  // positions that can hold a header: from the first frame offset, with 9
+  // bytes before the lane's end
+  if (a + 15 < L.fstart || a + 9 > end) return 0;
   uint32_t z = zero_bytes8(w0) | (zero_bytes8(w1) << 8) | (zero_bytes8(w2) << 16);
-  // byte i+4 (top byte of n) and byte i+8 (top byte of plen) zero
-  uint32_t m = (z >> 4) & (z >> 8) & 0xFFFFu;
-  uint64_t last = end - 9;  // last position that can hold a header (>= a here)
+  // mode byte nonzero, byte i+4 (top byte of n) and byte i+8 (top byte of
+  // plen) zero
+  uint32_t m = ~z & (z >> 4) & (z >> 8) & 0xFFFFu;
+  if (a < L.fstart) m &= 0xFFFFu << (uint32_t)(L.fstart - a);
+  uint64_t last = end - 9;
   if (a + 15 > last) m &= (2u << (uint32_t)(last - a)) - 1u;
+  uint32_t lb = lane_bytes((int)L.dtype);
   uint32_t out = 0;
   while (m) {
     uint32_t i = __ffs(m) - 1;
     m &= m - 1;
+    uint64_t h = dp_bytes8(w0, w1, w2, i);  // mode, n (3 bytes; the 4th is zero), plen (3 bytes)
+    uint32_t mode = (uint32_t)(h & 0xFF), n = (uint32_t)((h >> 8) & 0xFFFFFF), plen = (uint32_t)(h >> 40);
     uint64_t p = a + i;
-    uint32_t mode = s[p];
-    uint32_t n = ld_u32(s + p + 1), plen = ld_u32(s + p + 5);
-    if (dp_mode_candidate(mode) && n >= 1 && n <= (uint32_t)kMaxBlock && plen <= end - p - 9 &&
+    if (mode < 64 && ((kCandModes >> mode) & 1) && n >= 1 && n <= (uint32_t)kMaxBlock && plen <= end - p - 9 &&
         dp_frame_plausible(s, p + 9, n, plen, mode, lb))
       out |= 1u << i;
   }
   return out;
 }
 
-__global__ void __launch_bounds__(kDpThreads) k_dp_cand_count(const uint8_t* __restrict__ s, uint64_t buf_len,
-                                                              const DpHead* __restrict__ H, int lane,
-                                                              uint64_t* __restrict__ cnt) {
-  __shared__ uint32_t red[kDpThreads / 32];
-  const DpLane& L = H->lanes[lane];
-  uint64_t end = L.base + L.len;
-  uint64_t a = L.fstart + (uint64_t)blockIdx.x * kDpChunk + 16ull * threadIdx.x;
-  uint32_t c = H->kind ? 0u : (uint32_t)__popc(dp_thread_cands(s, buf_len, a, end, lane_bytes((int)L.dtype)));
-  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t t = 0;
-    for (int w = 0; w < kDpThreads / 32; w++) t += red[w];
-    cnt[blockIdx.x] = t;
-  }
+__device__ __forceinline__ DpCand dp_cand_at(const uint8_t* __restrict__ s, uint64_t p) {
+  DpCand c;
+  c.pos = p;
+  c.n = ld_u32(s + p + 1);
+  c.plen_mode = (ld_u32(s + p + 5) << 8) | s[p];
+  return c;
 }
 
-// Writes chunk j's candidates at off[j] (off = exclusive scan of the counts
-// with one extra entry, so off[j + 1] - off[j] is chunk j's count).
-__global__ void __launch_bounds__(kDpThreads) k_dp_cand_write(const uint8_t* __restrict__ s, uint64_t buf_len,
-                                                              const DpHead* __restrict__ H, int lane,
-                                                              const uint64_t* __restrict__ off, uint64_t cap,
-                                                              DpCand* __restrict__ cand) {
+// The thread's candidate masks of its kDpSteps steps in chunk `chunk`, and
+// where its candidates go in the chunk's position order: the step-k ones
+// from at[k] (an exclusive scan over the CTA of four 16-bit counts at once).
+// Returns the chunk's count.
+constexpr uint32_t kDpSlots = 16;
+__device__ inline uint64_t dp_chunk_cands(const uint8_t* __restrict__ s, uint64_t buf_len, const DpLane& L,
+                                          uint64_t chunk, uint64_t* s_warp, uint32_t m[kDpSteps],
+                                          uint64_t a[kDpSteps], uint64_t at[kDpSteps]) {
+  const uint64_t base = dp_chunk_base(s, L) + chunk * kDpChunk + 16ull * threadIdx.x;
+  DpWin w[kDpSteps];
+#pragma unroll
+  for (int k = 0; k < kDpSteps; k++) {  // every load in flight before any is used
+    a[k] = base + (uint64_t)k * kDpStep;
+    w[k] = dp_load(s, buf_len, a[k]);
+  }
+  uint64_t packed = 0;
+#pragma unroll
+  for (int k = 0; k < kDpSteps; k++) {
+    m[k] = dp_thread_cands(s, L, a[k], w[k]);
+    packed |= (uint64_t)__popc(m[k]) << (16 * k);
+  }
+  uint64_t tot;
+  uint64_t x = block_excl_scan<ScanSum>(packed, s_warp, &tot);  // each field sums at most 16 * kDpThreads
+  uint64_t before = 0;
+#pragma unroll
+  for (int k = 0; k < kDpSteps; k++) {
+    at[k] = before + ((x >> (16 * k)) & 0xFFFF);
+    before += (tot >> (16 * k)) & 0xFFFF;
+  }
+  return before;
+}
+
+// Per chunk: its candidate count, and its first kDpSlots candidates (in
+// position order) in the chunk's slots.
+__global__ void __launch_bounds__(kDpThreads) k_dp_cand_scan(const uint8_t* __restrict__ s, uint64_t buf_len,
+                                                             const DpHead* __restrict__ H, int lane,
+                                                             uint64_t* __restrict__ cnt, DpCand* __restrict__ slots) {
   __shared__ uint64_t s_warp[33];
-  uint64_t base = off[blockIdx.x];
-  if (off[blockIdx.x + 1] == base || H->kind) return;
+  if (H->kind) {  // uniform over the CTA
+    if (threadIdx.x == 0) cnt[blockIdx.x] = 0;
+    return;
+  }
   const DpLane& L = H->lanes[lane];
-  uint64_t end = L.base + L.len;
-  uint64_t a = L.fstart + (uint64_t)blockIdx.x * kDpChunk + 16ull * threadIdx.x;
-  uint32_t m = dp_thread_cands(s, buf_len, a, end, lane_bytes((int)L.dtype));
-  uint64_t at = base + block_excl_scan<ScanSum>((uint64_t)__popc(m), s_warp, nullptr);
-  while (m) {
-    uint32_t i = __ffs(m) - 1;
-    m &= m - 1;
-    uint64_t p = a + i;
-    if (at < cap) {
-      DpCand c;
-      c.pos = p;
-      c.n = ld_u32(s + p + 1);
-      c.plen_mode = (ld_u32(s + p + 5) << 8) | s[p];
-      cand[at] = c;
+  uint32_t m[kDpSteps];
+  uint64_t a[kDpSteps], at[kDpSteps];
+  uint64_t tot = dp_chunk_cands(s, buf_len, L, blockIdx.x, s_warp, m, a, at);
+#pragma unroll
+  for (int k = 0; k < kDpSteps; k++) {
+    uint32_t mk = m[k];
+    uint64_t q = at[k];
+    while (mk && q < kDpSlots) {
+      uint32_t i = __ffs(mk) - 1;
+      mk &= mk - 1;
+      slots[(uint64_t)blockIdx.x * kDpSlots + q] = dp_cand_at(s, a[k] + i);
+      q++;
     }
-    at++;
+  }
+  if (threadIdx.x == 0) cnt[blockIdx.x] = tot;
+}
+
+// Chunk j's candidates to cand[off[j] ..] (off = exclusive scan of the
+// counts with one extra entry): from the slots, or by a second pass over a
+// chunk with more candidates than slots.
+__global__ void __launch_bounds__(kDpThreads) k_dp_cand_compact(const uint8_t* __restrict__ s, uint64_t buf_len,
+                                                                const DpHead* __restrict__ H, int lane,
+                                                                const uint64_t* __restrict__ off,
+                                                                const DpCand* __restrict__ slots, uint64_t cap,
+                                                                DpCand* __restrict__ cand) {
+  __shared__ uint64_t s_warp[33];
+  uint64_t base = off[blockIdx.x], c = off[blockIdx.x + 1] - base;
+  if (c == 0 || H->kind) return;
+  if (c <= kDpSlots) {
+    if (threadIdx.x < c && base + threadIdx.x < cap)
+      cand[base + threadIdx.x] = slots[(uint64_t)blockIdx.x * kDpSlots + threadIdx.x];
+    return;
+  }
+  const DpLane& L = H->lanes[lane];
+  uint32_t m[kDpSteps];
+  uint64_t a[kDpSteps], at[kDpSteps];
+  dp_chunk_cands(s, buf_len, L, blockIdx.x, s_warp, m, a, at);
+#pragma unroll
+  for (int k = 0; k < kDpSteps; k++) {
+    uint32_t mk = m[k];
+    uint64_t q = base + at[k];
+    while (mk) {
+      uint32_t i = __ffs(mk) - 1;
+      mk &= mk - 1;
+      if (q < cap) cand[q] = dp_cand_at(s, a[k] + i);
+      q++;
+    }
   }
 }
 
@@ -515,96 +619,82 @@ __device__ FrameItems dp_frame_items(const uint8_t* p, uint64_t n, uint64_t plen
   return r;
 }
 
-__global__ void __launch_bounds__(kChainThreads) k_dp_chain(const uint8_t* __restrict__ s, const DpHead* __restrict__ H,
-                                                            int lane, const uint64_t* __restrict__ d_nvalid,
+// Per candidate (one thread each): its successor, the candidate at
+// pos + 9 + plen (binary search over the later candidates), or ~0.
+__global__ void k_dp_succ(const DpHead* __restrict__ H, const DpCand* __restrict__ cand,
+                          const uint64_t* __restrict__ d_ncand, uint64_t cap, DpNode* __restrict__ nodes) {
+  uint64_t K = *d_ncand;
+  if (H->kind || K > cap) return;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < K; i += (uint64_t)gridDim.x * blockDim.x) {
+    DpCand c = cand[i];
+    uint64_t target = c.pos + 9 + (c.plen_mode >> 8);
+    uint64_t lo = i + 1, hi = K;
+    while (lo < hi) {
+      uint64_t mid = (lo + hi) >> 1;
+      if (cand[mid].pos < target) lo = mid + 1; else hi = mid;
+    }
+    nodes[i].succ = (lo < K && cand[lo].pos == target) ? (uint32_t)lo : kNone;
+  }
+}
+
+// The lane's value count, or ~0 when the lane cannot be read here (a decimal
+// limb whose count is not the column's valid count).
+__device__ inline uint64_t dp_lane_total(const DpHead* H, const DpLane& L, const uint64_t* d_nvalid) {
+  if (H->decimal) {
+    uint64_t nv = H->has_validity ? *d_nvalid : H->n;
+    return L.logical_n == nv ? nv : ~0ull;
+  }
+  return L.has_validity ? *d_nvalid : L.logical_n;
+}
+
+// One CTA: marks spread from the first frame (candidate 0, which must sit at
+// the lane's first frame offset) along the successors by pointer doubling,
+// then the marked candidates (the chain's frames, in position order) are
+// listed in fidx.  ctl[0] = 0 when the lane cannot be read here, ctl[1] = the
+// number of marked candidates.
+__global__ void __launch_bounds__(kChainThreads) k_dp_marks(const DpHead* __restrict__ H, int lane,
+                                                            const uint64_t* __restrict__ d_nvalid,
                                                             const DpCand* __restrict__ cand,
+                                                            const DpNode* __restrict__ nodes,
                                                             const uint64_t* __restrict__ d_ncand, uint64_t cap,
-                                                            uint32_t* __restrict__ gJ, uint8_t* __restrict__ gmarks,
-                                                            DpTables T, DpLaneOut* __restrict__ out) {
+                                                            uint32_t* __restrict__ gJ, uint8_t* __restrict__ marks,
+                                                            uint64_t* __restrict__ ctl) {
   extern __shared__ __align__(16) uint8_t dsm[];
   __shared__ uint64_t s_warp[33];
-  __shared__ uint64_t s_i0;
-  __shared__ int s_fail;
   const int tid = threadIdx.x;
-  DpLaneOut R;
-  memset(&R, 0, sizeof(R));
-  R.status = 1;
   if (H->kind) {
-    if (tid == 0) *out = R;
+    if (tid == 0) ctl[0] = ctl[1] = 0;
     return;
   }
   const DpLane& L = H->lanes[lane];
-  uint64_t K = *d_ncand;
-  R.ncand = K;
-  // values the lane's frames hold: the valid count (a plain stream with a
-  // bitmap), else the lane header's n, which a decimal limb must match
-  uint64_t n_total = L.logical_n;
-  if (H->decimal) {
-    uint64_t nv = H->has_validity ? *d_nvalid : H->n;
-    if (n_total != nv) {
-      if (tid == 0) *out = R;
-      return;
-    }
-  } else if (L.has_validity) {
-    n_total = *d_nvalid;
-  }
-  if (n_total == 0) {  // no frame is read (decoder.rs: the walk runs while counted < n)
-    R.status = 0;
+  uint64_t K = *d_ncand, n_total = dp_lane_total(H, L, d_nvalid);
+  // candidates start at the first frame offset, so the first frame is
+  // candidate 0 or not a candidate at all
+  bool good = n_total != ~0ull && (n_total == 0 || (K <= cap && K > 0 && cand[0].pos == L.fstart));
+  if (!good || n_total == 0) {
     if (tid == 0) {
-      T.main_off[0] = 0;
-      *out = R;
+      ctl[0] = good;
+      ctl[1] = 0;
     }
     return;
   }
-  if (K > cap || K == 0) {
-    if (tid == 0) *out = R;
-    return;
-  }
-  // the first frame: binary search for fstart
-  if (tid == 0) {
-    uint64_t lo = 0, hi = K;
-    while (lo < hi) {
-      uint64_t mid = (lo + hi) >> 1;
-      if (cand[mid].pos < L.fstart) lo = mid + 1; else hi = mid;
-    }
-    s_i0 = lo;
-    s_fail = (lo == K || cand[lo].pos != L.fstart);
-  }
-  __syncthreads();
-  if (s_fail) {
-    if (tid == 0) *out = R;
-    return;
-  }
-  const uint64_t i0 = s_i0;
-  const uint32_t M = (uint32_t)(K - i0);
-  const DpCand* C = cand + i0;
-  // successor tables (two, for the doubling) and marks: in shared memory when
-  // they fit, else in the global scratch
-  uint32_t *J0, *J1;
-  uint8_t* marks;
-  if ((uint64_t)M * 9 + 16 <= kDpChainSmem) {
+  const uint32_t M = (uint32_t)K;
+  uint32_t *J0, *J1;  // successor tables (two, for the doubling): shared memory when they fit
+  if ((uint64_t)M * 8 + 16 <= kDpChainSmem) {
     J0 = reinterpret_cast<uint32_t*>(dsm);
     J1 = J0 + M;
-    marks = reinterpret_cast<uint8_t*>(J1 + M);
   } else {
     J0 = gJ;
     J1 = gJ + M;
-    marks = gmarks;
   }
   for (uint32_t i = tid; i < M; i += kChainThreads) {
-    uint64_t target = C[i].pos + 9 + (C[i].plen_mode >> 8);
-    uint32_t lo = i + 1, hi = M;
-    while (lo < hi) {
-      uint32_t mid = (lo + hi) >> 1;
-      if (C[mid].pos < target) lo = mid + 1; else hi = mid;
-    }
-    J0[i] = (lo < M && C[lo].pos == target) ? lo : kNone;
+    J0[i] = nodes[i].succ;
     marks[i] = i == 0;
   }
   __syncthreads();
-  // pointer doubling: after round r every chain frame within 2^(r+1) - 1
-  // jumps of the first is marked (a mark set during a round may be used in
-  // the same round: it is a chain frame too)
+  // after round r every chain frame within 2^(r+1) - 1 jumps of the first is
+  // marked (a mark set during a round may be used in the same round: it is a
+  // chain frame too)
   uint32_t rounds = 1;
   while ((1ull << rounds) <= M) rounds++;
   for (uint32_t r = 0; r < rounds; r++) {
@@ -618,25 +708,95 @@ __global__ void __launch_bounds__(kChainThreads) k_dp_chain(const uint8_t* __res
     J0 = J1;
     J1 = t;
   }
-  // the marked frames in position order, cut at the lane's value count: the
-  // values before a marked frame only grow along the chain, so the kept
-  // frames (those starting below the count) are a prefix of the marked ones
+  // the marked candidates in order (gJ is free again: the doubling is done)
+  uint64_t carry = 0;
+  for (uint32_t t0 = 0; t0 < M; t0 += kChainThreads) {
+    uint32_t i = t0 + tid;
+    bool f = i < M && marks[i];
+    uint64_t tot;
+    uint64_t x = block_excl_scan<ScanSum>(f ? 1ull : 0ull, s_warp, &tot);
+    if (f) gJ[carry + x] = i;
+    carry += tot;
+  }
+  if (tid == 0) {
+    ctl[0] = 1;
+    ctl[1] = carry;
+  }
+}
+
+// The warp items of every marked candidate (dp_frame_items), across the GPU:
+// nodes[j] for the j-th marked candidate, its candidate index in .succ.
+__global__ void k_dp_items(const uint8_t* __restrict__ s, const DpHead* __restrict__ H, int lane,
+                           const DpCand* __restrict__ cand, const uint32_t* __restrict__ fidx,
+                           const uint64_t* __restrict__ ctl, DpNode* __restrict__ nodes) {
+  if (!ctl[0]) return;
+  uint64_t F = ctl[1];
+  uint32_t plog2 = H->lanes[lane].plog2;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < F; j += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t i = fidx[j];
+    DpCand c = cand[i];
+    FrameItems it = dp_frame_items(s + c.pos + 9, c.n, c.plen_mode >> 8, c.plen_mode & 0xFF, plog2);
+    DpNode d;
+    d.succ = i;
+    d.nmain = it.nmain;
+    d.npre = it.npre;
+    d.flags = (it.list ? 1u : 0u) | (it.scan ? 2u : 0u) | (it.dict ? 4u : 0u);
+    d.ent = it.ent;
+    nodes[j] = d;
+  }
+}
+
+// One CTA: the chain's frames (nodes[0 .. F), in position order) cut at the
+// lane's value count and laid out as the block decoder's tables (the values
+// before a frame only grow along the chain, so the kept frames, those
+// starting below the count, are a prefix).
+__global__ void __launch_bounds__(kChainThreads) k_dp_layout(const DpHead* __restrict__ H, int lane,
+                                                             const uint64_t* __restrict__ d_nvalid,
+                                                             const DpCand* __restrict__ cand,
+                                                             const DpNode* __restrict__ nodes,
+                                                             const uint64_t* __restrict__ d_ncand,
+                                                             const uint64_t* __restrict__ ctl, DpTables T,
+                                                             DpLaneOut* __restrict__ out) {
+  __shared__ uint64_t s_warp[33];
+  const int tid = threadIdx.x;
+  DpLaneOut R;
+  memset(&R, 0, sizeof(R));
+  R.status = 1;
+  R.ncand = *d_ncand;
+  if (!ctl[0]) {
+    if (tid == 0) *out = R;
+    return;
+  }
+  const DpLane& L = H->lanes[lane];
+  uint64_t n_total = dp_lane_total(H, L, d_nvalid);
+  if (n_total == 0) {  // no frame is read (decoder.rs: the walk runs while counted < n)
+    R.status = 0;
+    if (tid == 0) {
+      T.main_off[0] = 0;
+      *out = R;
+    }
+    return;
+  }
+  const uint64_t F = ctl[1];
   uint64_t carry_f = 0, carry_v = 0, carry_main = 0, carry_pre = 0, carry_list = 0, carry_ent = 0;
   bool scan = false, dict = false, stop = false, fail = false;
-  for (uint32_t t0 = 0; t0 < M && !stop; t0 += kChainThreads) {
-    uint32_t i = t0 + tid;
-    bool marked = i < M && marks[i];
+  for (uint64_t t0 = 0; t0 < F && !stop; t0 += kChainThreads) {
+    uint64_t j = t0 + tid;
+    bool have = j < F;
     DpCand c;
     c.pos = 0;
     c.n = 0;
     c.plen_mode = 0;
-    if (marked) c = C[i];
-    uint64_t vx = block_excl_scan<ScanSum>(marked ? (uint64_t)c.n : 0ull, s_warp, nullptr);
+    DpNode nd;
+    memset(&nd, 0, sizeof(nd));
+    if (have) {
+      nd = nodes[j];
+      c = cand[nd.succ];
+    }
+    uint64_t vx = block_excl_scan<ScanSum>(have ? (uint64_t)c.n : 0ull, s_warp, nullptr);
     uint64_t voff = carry_v + vx;
-    bool keep = marked && voff < n_total;
-    FrameItems it{0, 0, false, false, false, 0};
-    uint32_t mode = c.plen_mode & 0xFF, plen = c.plen_mode >> 8;
-    if (keep) it = dp_frame_items(s + c.pos + 9, c.n, plen, mode, L.plog2);
+    bool keep = have && voff < n_total;
+    bool list = keep && (nd.flags & 1);
     bool last = keep && voff + c.n >= n_total;
     stop = __syncthreads_or(last) != 0;
     // past the count: CorruptPayload, which the host reader reports
@@ -644,26 +804,26 @@ __global__ void __launch_bounds__(kChainThreads) k_dp_chain(const uint8_t* __res
     uint64_t tf, tv, tp, tl, te;
     uint64_t fx = block_excl_scan<ScanSum>(keep ? 1ull : 0ull, s_warp, &tf);
     block_excl_scan<ScanSum>(keep ? (uint64_t)c.n : 0ull, s_warp, &tv);
-    uint64_t packed = keep ? ((uint64_t)it.npre << 32 | it.nmain) : 0ull;
+    uint64_t packed = keep ? ((uint64_t)nd.npre << 32 | nd.nmain) : 0ull;
     uint64_t px = block_excl_scan<ScanSum>(packed, s_warp, &tp);
-    uint64_t lx = block_excl_scan<ScanSum>(keep && it.list ? 1ull : 0ull, s_warp, &tl);
-    uint64_t ex = block_excl_scan<ScanSum>(keep ? it.ent : 0ull, s_warp, &te);
+    uint64_t lx = block_excl_scan<ScanSum>(list ? 1ull : 0ull, s_warp, &tl);
+    uint64_t ex = block_excl_scan<ScanSum>(keep ? nd.ent : 0ull, s_warp, &te);
     if (keep) {
       uint64_t f = carry_f + fx;
       FrameDesc d;
       d.payload_off = c.pos + 9;
       d.value_off = voff;
       d.n = c.n;
-      d.plen = plen;
-      d.mode = mode;
-      d.aux = it.ent ? (uint32_t)(1 + (carry_ent + ex) / 128) : 0u;
+      d.plen = c.plen_mode >> 8;
+      d.mode = c.plen_mode & 0xFF;
+      d.aux = nd.ent ? (uint32_t)(1 + (carry_ent + ex) / 128) : 0u;
       T.frames[f] = d;
-      T.frame_pre[f] = make_uint2((uint32_t)(carry_pre + (px >> 32)), it.npre);
+      T.frame_pre[f] = make_uint2((uint32_t)(carry_pre + (px >> 32)), nd.npre);
       T.main_off[f] = carry_main + (px & 0xFFFFFFFFull);
-      if (it.list) T.list[carry_list + lx] = (uint32_t)f;
+      if (list) T.list[carry_list + lx] = (uint32_t)f;
     }
-    scan = (__syncthreads_or(keep && it.scan) != 0) || scan;
-    dict = (__syncthreads_or(keep && it.dict) != 0) || dict;
+    scan = (__syncthreads_or(keep && (nd.flags & 2)) != 0) || scan;
+    dict = (__syncthreads_or(keep && (nd.flags & 4)) != 0) || dict;
     carry_f += tf;
     carry_v += tv;
     carry_main += tp & 0xFFFFFFFFull;
@@ -708,47 +868,54 @@ void launch_dp_head(const uint8_t* s, uint64_t len, DpHead* H, cudaStream_t st) 
   count_launches(1);
 }
 
-void launch_dp_bitmap(const uint8_t* s, const DpHead* H, uint64_t raw_len, uint8_t* bm, cudaStream_t st) {
-  uint64_t bytes = (raw_len + 7) / 8 * 8;
-  unsigned g = (unsigned)qmin((bytes + 255) / 256, 148ull * 8);
-  if (g == 0) g = 1;
-  k_dp_bitmap<<<g, 256, 0, st>>>(s, H, bm);
+void launch_dp_bitmap(const uint8_t* s, const DpHead* H, uint64_t n, uint8_t* bm, uint64_t* cnt, cudaStream_t st) {
+  uint64_t nw = (n + 31) / 32 + 1;
+  unsigned g = (unsigned)qmin((nw + 255) / 256, 148ull * 16);
+  k_dp_bitmap<<<g, 256, 0, st>>>(s, H, reinterpret_cast<uint32_t*>(bm), cnt);
   count_launches(1);
 }
 
 void launch_dp_bitmap_rle(const uint8_t* s, DpHead* H, uint64_t n, uint64_t* ends, uint64_t* nruns, uint8_t* bm,
-                          cudaStream_t st) {
+                          uint64_t* cnt, cudaStream_t st) {
   k_dp_rle_runs<<<1, kRleThreads, 0, st>>>(s, H, n, ends, nruns);
   uint64_t nw = (n + 31) / 32 + 1;
   unsigned g = (unsigned)qmin((nw + 255) / 256, 148ull * 8);
-  k_dp_rle_fill<<<g, 256, 0, st>>>(H, n, ends, nruns, reinterpret_cast<uint32_t*>(bm));
+  k_dp_rle_fill<<<g, 256, 0, st>>>(H, n, ends, nruns, reinterpret_cast<uint32_t*>(bm), cnt);
   count_launches(2);
 }
 
-uint64_t dp_chunks(uint64_t lane_frames_bytes) { return (lane_frames_bytes + kDpChunk - 1) / kDpChunk; }
+uint64_t dp_chunks(uint64_t lane_frames_bytes) {
+  return lane_frames_bytes ? (lane_frames_bytes + 15 + kDpChunk - 1) / kDpChunk : 0;  // chunks start up to 15 bytes early
+}
+uint64_t dp_slot_bytes(uint64_t lane_frames_bytes) { return dp_chunks(lane_frames_bytes) * kDpSlots * sizeof(DpCand); }
 
 void launch_dp_candidates(const uint8_t* s, uint64_t buf_len, const DpHead* H, int lane, uint64_t lane_frames_bytes,
-                          uint64_t* cnt, uint64_t* tile_tmp, uint64_t* d_ncand, DpCand* cand, uint64_t cap,
-                          cudaStream_t st) {
+                          uint64_t* cnt, DpCand* slots, uint64_t* tile_tmp, uint64_t* d_ncand, DpCand* cand,
+                          uint64_t cap, cudaStream_t st) {
   // cnt has nchunks + 1 entries: the counts, then 0, so that after the
   // exclusive scan cnt[j + 1] - cnt[j] is chunk j's count
   uint64_t nchunks = dp_chunks(lane_frames_bytes);
-  if (nchunks) k_dp_cand_count<<<(unsigned)nchunks, kDpThreads, 0, st>>>(s, buf_len, H, lane, cnt);
+  if (nchunks) k_dp_cand_scan<<<(unsigned)nchunks, kDpThreads, 0, st>>>(s, buf_len, H, lane, cnt, slots);
   cudaMemsetAsync(cnt + nchunks, 0, 8, st);
   launch_scan_sum(cnt, cnt, nchunks + 1, tile_tmp, d_ncand, st);
-  if (nchunks) k_dp_cand_write<<<(unsigned)nchunks, kDpThreads, 0, st>>>(s, buf_len, H, lane, cnt, cap, cand);
+  if (nchunks)
+    k_dp_cand_compact<<<(unsigned)nchunks, kDpThreads, 0, st>>>(s, buf_len, H, lane, cnt, slots, cap, cand);
   count_launches(nchunks ? 2 : 0);
 }
 
 void launch_dp_chain(const uint8_t* s, const DpHead* H, int lane, const uint64_t* d_nvalid, const DpCand* cand,
-                     const uint64_t* d_ncand, uint64_t cap, uint32_t* gJ, uint8_t* gmarks, const DpTables& T,
-                     DpLaneOut* out, cudaStream_t st) {
+                     const uint64_t* d_ncand, uint64_t cap, DpNode* nodes, uint32_t* gJ, uint8_t* gmarks,
+                     uint64_t* d_ctl, const DpTables& T, DpLaneOut* out, cudaStream_t st) {
   once_per_device(g_chain_attr, [] {
-    cudaFuncSetAttribute(k_dp_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDpChainSmem);
+    cudaFuncSetAttribute(k_dp_marks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDpChainSmem);
   });
-  k_dp_chain<<<1, kChainThreads, kDpChainSmem, st>>>(s, H, lane, d_nvalid, cand, d_ncand, cap, gJ, gmarks, T, out);
+  unsigned g = (unsigned)qmin((cap + 255) / 256, 148ull * 4);
+  k_dp_succ<<<g, 256, 0, st>>>(H, cand, d_ncand, cap, nodes);
+  k_dp_marks<<<1, kChainThreads, kDpChainSmem, st>>>(H, lane, d_nvalid, cand, nodes, d_ncand, cap, gJ, gmarks, d_ctl);
+  k_dp_items<<<g, 256, 0, st>>>(s, H, lane, cand, gJ, d_ctl, nodes);
+  k_dp_layout<<<1, kChainThreads, 0, st>>>(H, lane, d_nvalid, cand, nodes, d_ncand, d_ctl, T, out);
   k_dp_expand<<<148 * 2, 256, 0, st>>>(out, T);
-  count_launches(2);
+  count_launches(5);
 }
 
 }  // namespace qb

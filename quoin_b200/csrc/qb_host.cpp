@@ -1275,6 +1275,7 @@ struct DpMisc {  // the reader's small results, read back in one copy
   uint64_t nvalid;
   uint64_t ncand[4];
   uint64_t nruns;  // runs of an RLE validity blob
+  uint64_t ctl[4][2];  // per lane: chain resolved, chain frames
 };
 constexpr uint64_t kDpHeadOff = 0, kDpMiscOff = 512;
 static_assert(sizeof(DpHead) <= kDpMiscOff && sizeof(DpMisc) <= 512, "reader results fit their slot");
@@ -1354,12 +1355,12 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
     CK(c->ensure(S_DRANK, (nw + 1) * 8));
     CK(c->ensure(S_TILE, (scan_tile_count(nw + 4096) + 16) * 8));
     if (H.vtag == 0) {
-      launch_dp_bitmap(d_src, dH, H.vblob_len, c->p<uint8_t>(S_DBM), st);
+      launch_dp_bitmap(d_src, dH, n, c->p<uint8_t>(S_DBM), c->p<uint64_t>(S_DRANK), st);
     } else {  // run lengths: at most one run per blob byte
       CK(c->ensure(S_DPRUNS, (H.vblob_len + 2) * 8));
-      launch_dp_bitmap_rle(d_src, dH, n, c->p<uint64_t>(S_DPRUNS), &dM->nruns, c->p<uint8_t>(S_DBM), st);
+      launch_dp_bitmap_rle(d_src, dH, n, c->p<uint64_t>(S_DPRUNS), &dM->nruns, c->p<uint8_t>(S_DBM),
+                           c->p<uint64_t>(S_DRANK), st);
     }
-    launch_word_popcount(c->p<uint8_t>(S_DBM), n, c->p<uint64_t>(S_DRANK), st);
     launch_scan_sum(c->p<uint64_t>(S_DRANK), c->p<uint64_t>(S_DRANK), nw, c->p<uint64_t>(S_TILE), &dM->nvalid, st);
     if (!H.decimal) {
       // the valid count is only known on the device: n bounds it (every
@@ -1370,7 +1371,8 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
   }
   // per-lane regions of the candidate, frame and item tables
   const int nl = (int)H.nl;
-  uint64_t caps[4], cnt_off[4], cand_off[4], j_off[4], fr_off[4], main_b[4], pre_b[4], fp_b[4], list_b[4], moff_b[4];
+  uint64_t caps[4], cnt_off[4], slot_off[4], cand_off[4], node_off[4], j_off[4], fr_off[4], main_b[4], pre_b[4],
+      fp_b[4], list_b[4], moff_b[4];
   uint64_t caps_min[4] = {0, 0, 0, 0};
   for (int attempt = 0; attempt < 2; attempt++) {
     uint64_t cand_bytes = 0, j_bytes = 0, frames_n = 0, items_u64 = 0, max_chunks = 0;
@@ -1381,8 +1383,12 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
       cnt_off[k] = cand_bytes;
       cand_bytes += (dp_chunks(fb) + 2) * 8;
       max_chunks = dp_chunks(fb) + 1 > max_chunks ? dp_chunks(fb) + 1 : max_chunks;
+      slot_off[k] = cand_bytes;
+      cand_bytes += (dp_slot_bytes(fb) + 255) & ~255ull;
       cand_off[k] = cand_bytes;
       cand_bytes += caps[k] * sizeof(DpCand);
+      node_off[k] = cand_bytes;
+      cand_bytes += (caps[k] * sizeof(DpNode) + 255) & ~255ull;
       j_off[k] = j_bytes;
       j_bytes += (caps[k] * 9 + 255) & ~255ull;
       fr_off[k] = frames_n;
@@ -1413,7 +1419,8 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
       uint64_t fb = L.base + L.len - L.fstart;
       DpCand* cand = reinterpret_cast<DpCand*>(cb + cand_off[k]);
       launch_dp_candidates(d_src, len, dH, k, fb, reinterpret_cast<uint64_t*>(cb + cnt_off[k]),
-                           c->p<uint64_t>(S_TILE), &dM->ncand[k], cand, caps[k], st);
+                           reinterpret_cast<DpCand*>(cb + slot_off[k]), c->p<uint64_t>(S_TILE), &dM->ncand[k], cand,
+                           caps[k], st);
       uint8_t* jb = c->p<uint8_t>(S_DPJ) + j_off[k];
       DpTables T;
       T.frames = c->p<FrameDesc>(S_DFRAMES) + fr_off[k];
@@ -1422,8 +1429,9 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
       T.list = reinterpret_cast<uint32_t*>(ditems + list_b[k]);
       T.main_items = reinterpret_cast<ItemRef*>(ditems + main_b[k]);
       T.pre_items = reinterpret_cast<ItemRef*>(ditems + pre_b[k]);
-      launch_dp_chain(d_src, dH, k, d_nvalid, cand, &dM->ncand[k], caps[k], reinterpret_cast<uint32_t*>(jb),
-                      jb + caps[k] * 8, T, &dM->lanes[k], st);
+      launch_dp_chain(d_src, dH, k, d_nvalid, cand, &dM->ncand[k], caps[k],
+                      reinterpret_cast<DpNode*>(cb + node_off[k]), reinterpret_cast<uint32_t*>(jb), jb + caps[k] * 8,
+                      dM->ctl[k], T, &dM->lanes[k], st);
     }
     DpMisc M;
     CK(read_small(c, st, &M, dM, sizeof(M)));

@@ -94,6 +94,13 @@ struct DpCand {
   uint64_t pos;
   uint32_t n, plen_mode;  // plen << 8 | mode
 };
+// A candidate's successor candidate (or ~0); after the chain is resolved, the
+// j-th chain frame: its candidate index (in succ) and warp items (flags: 1
+// listed, 2 needs the prepass scan, 4 uses the decode scratch).
+struct DpNode {
+  uint32_t succ, nmain, npre, flags;
+  uint64_t ent;  // entropy area bytes when listed with a coded part
+};
 // The reader's result for one lane (status != 0: the host parses the stream;
 // ncand tells the host how many candidates the tables must hold).
 struct DpLaneOut {
@@ -110,25 +117,30 @@ struct DpTables {
   ItemRef* main_items;
   ItemRef* pre_items;
 };
-constexpr uint64_t kDpChainSmem = 200 * 1024;  // successor tables in shared memory up to 22,755 candidates
+constexpr uint64_t kDpChainSmem = 200 * 1024;  // successor tables in shared memory up to 25,598 candidates
 void launch_dp_head(const uint8_t* s, uint64_t len, DpHead* H, cudaStream_t st);
-void launch_dp_bitmap(const uint8_t* s, const DpHead* H, uint64_t raw_len, uint8_t* bm, cudaStream_t st);
-// RLE validity blob (validity.rs:92-119) into the n-bit bitmap bm (ceil(n/32)
-// words written); `ends` holds vblob_len entries.  A blob the sequential
-// reader would reject sets H->kind, so the host reader takes the stream.
+// The validity bitmap of an n-value stream as 32-bit words (ceil(n/32) + 1
+// written, the last zero) and each word's popcount in cnt: from a RAW blob,
+// or from an RLE blob (validity.rs:92-119; `ends` holds vblob_len entries).
+// An RLE blob the sequential reader would reject sets H->kind, so the host
+// reader takes the stream.
+void launch_dp_bitmap(const uint8_t* s, const DpHead* H, uint64_t n, uint8_t* bm, uint64_t* cnt, cudaStream_t st);
 void launch_dp_bitmap_rle(const uint8_t* s, DpHead* H, uint64_t n, uint64_t* ends, uint64_t* nruns, uint8_t* bm,
-                          cudaStream_t st);
+                          uint64_t* cnt, cudaStream_t st);
 // Candidate chunks of a lane whose frames span `lane_frames_bytes` bytes (cnt
-// needs dp_chunks() + 1 entries; *d_ncand gets the count, at most cap written).
+// needs dp_chunks() + 1 entries, slots dp_slot_bytes(); *d_ncand gets the
+// count, at most cap written to cand).
 uint64_t dp_chunks(uint64_t lane_frames_bytes);
+uint64_t dp_slot_bytes(uint64_t lane_frames_bytes);
 void launch_dp_candidates(const uint8_t* s, uint64_t buf_len, const DpHead* H, int lane, uint64_t lane_frames_bytes,
-                          uint64_t* cnt, uint64_t* tile_tmp, uint64_t* d_ncand, DpCand* cand, uint64_t cap,
-                          cudaStream_t st);
-// Chain resolution + item tables of lane `lane` (gJ: 8 * cap bytes, gmarks:
-// cap bytes of global scratch for lanes whose candidates exceed shared memory).
+                          uint64_t* cnt, DpCand* slots, uint64_t* tile_tmp, uint64_t* d_ncand, DpCand* cand,
+                          uint64_t cap, cudaStream_t st);
+// Chain resolution + item tables of lane `lane` (nodes: cap entries; gJ: 8 *
+// cap bytes of global scratch (successor tables that exceed shared memory,
+// then the chain's candidate list); gmarks: cap bytes; d_ctl: two words).
 void launch_dp_chain(const uint8_t* s, const DpHead* H, int lane, const uint64_t* d_nvalid, const DpCand* cand,
-                     const uint64_t* d_ncand, uint64_t cap, uint32_t* gJ, uint8_t* gmarks, const DpTables& T,
-                     DpLaneOut* out, cudaStream_t st);
+                     const uint64_t* d_ncand, uint64_t cap, DpNode* nodes, uint32_t* gJ, uint8_t* gmarks,
+                     uint64_t* d_ctl, const DpTables& T, DpLaneOut* out, cudaStream_t st);
 
 // sel[m] = position of the (512*m)-th valid value, m < ceil(nvalid / 512).
 void launch_select_table(const uint8_t* bm, uint64_t n, const uint64_t* word_rank, uint64_t nvalid, uint64_t* sel,
