@@ -2112,6 +2112,179 @@ __device__ void warp_store_any(const DecodeOut& O, uint64_t c0, uint32_t cnt, V 
   if (p1 > p0) warp_store_words(O, p0 >> 5, (p1 + 31) >> 5, p0, p1, 0u, val);
 }
 
+// Half h of a FastLanes sub-block of width W <= 32 (rows 16h .. 16h+15 of
+// every lane), with the width a compile-time constant: lane l's rows sit in
+// bits [16hW, 16hW + 16W) of its word stream (word k of lane l at byte
+// 4 * (32k + l) from `words`), so the words are loaded once into registers and
+// every value is a fixed shift and mask of one or two of them.  A payload
+// offset that is not a multiple of 4 is read with aligned loads: lane l's word
+// is the funnel of its aligned word and lane l+1's (lane 31 takes lane 0's
+// next one), so each word is one load.
+template <int W, int H, class F>
+__device__ __forceinline__ void unpack_half_w(const uint8_t* words, uint64_t mn, uint32_t count, F& f) {
+  constexpr int B0 = 16 * H * W;           // first bit of the half in each lane's stream
+  constexpr int K0 = B0 >> 5;              // its word
+  constexpr int NW = ((B0 & 31) + 16 * W + 31) >> 5;  // words of the half
+  const int l = threadIdx.x & 31;
+  uint32_t wv[NW];
+  const uintptr_t addr = reinterpret_cast<uintptr_t>(words);
+  const uint32_t mis = (uint32_t)(addr & 3);
+  const uint32_t* base = reinterpret_cast<const uint32_t*>(addr - mis);
+  if (mis == 0) {
+#pragma unroll
+    for (int k = 0; k < NW; k++) wv[k] = __ldg(base + (K0 + k) * 32 + l);
+  } else {
+    uint32_t a[NW];
+#pragma unroll
+    for (int k = 0; k < NW; k++) a[k] = __ldg(base + (K0 + k) * 32 + l);
+    // lane 31's high part is lane 0's word of the next row
+    uint32_t last = l == 0 ? __ldg(base + (K0 + NW) * 32) : 0u;
+#pragma unroll
+    for (int k = 0; k < NW; k++) {
+      uint32_t nx = __shfl_down_sync(0xffffffffu, a[k], 1);
+      uint32_t n0 = __shfl_sync(0xffffffffu, k + 1 < NW ? a[k + 1 < NW ? k + 1 : k] : last, 0);
+      if (l == 31) nx = n0;
+      wv[k] = __funnelshift_r(a[k], nx, mis * 8);
+    }
+  }
+  constexpr uint32_t MASK = W == 32 ? 0xFFFFFFFFu : ((1u << W) - 1u);
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const int b = B0 + j * W - K0 * 32;  // bit within the loaded words
+    const int k = b >> 5, sh = b & 31;
+    uint32_t v = wv[k] >> sh;
+    if (sh + W > 32) v |= wv[k + 1 < NW ? k + 1 : k] << (32 - sh);
+    v &= MASK;
+    uint32_t idx = (uint32_t)((16 * H + j) * 32 + l);
+    if (idx < count) f(idx, mn + (uint64_t)v);
+  }
+}
+
+template <int W, class F>
+__device__ __forceinline__ void unpack_half_h(const uint8_t* words, uint32_t h, uint64_t mn, uint32_t count, F& f) {
+  if (h) unpack_half_w<W, 1>(words, mn, count, f);
+  else unpack_half_w<W, 0>(words, mn, count, f);
+}
+
+// warp_unpack_half with the widths up to 32 specialised.
+template <class F>
+__device__ inline void warp_unpack_half_fast(const uint8_t* p, uint32_t off, uint32_t h, uint32_t count, F f) {
+  uint32_t w = p[off];
+  if (w == 0 || w > 32) {
+    warp_unpack_half(p, off, h, count, f);
+    return;
+  }
+  uint64_t mn = ld_u64(p + off + 1);
+  const uint8_t* words = p + off + 9;
+  switch (w) {
+#define QB_UNPACK_CASE(W) case W: unpack_half_h<W>(words, h, mn, count, f); break;
+    QB_UNPACK_CASE(1) QB_UNPACK_CASE(2) QB_UNPACK_CASE(3) QB_UNPACK_CASE(4) QB_UNPACK_CASE(5) QB_UNPACK_CASE(6)
+    QB_UNPACK_CASE(7) QB_UNPACK_CASE(8) QB_UNPACK_CASE(9) QB_UNPACK_CASE(10) QB_UNPACK_CASE(11) QB_UNPACK_CASE(12)
+    QB_UNPACK_CASE(13) QB_UNPACK_CASE(14) QB_UNPACK_CASE(15) QB_UNPACK_CASE(16) QB_UNPACK_CASE(17)
+    QB_UNPACK_CASE(18) QB_UNPACK_CASE(19) QB_UNPACK_CASE(20) QB_UNPACK_CASE(21) QB_UNPACK_CASE(22)
+    QB_UNPACK_CASE(23) QB_UNPACK_CASE(24) QB_UNPACK_CASE(25) QB_UNPACK_CASE(26) QB_UNPACK_CASE(27)
+    QB_UNPACK_CASE(28) QB_UNPACK_CASE(29) QB_UNPACK_CASE(30) QB_UNPACK_CASE(31) QB_UNPACK_CASE(32)
+#undef QB_UNPACK_CASE
+    default: break;
+  }
+}
+
+// Store the run [c0, c0 + cnt) of lane values (any c0) like warp_store_any,
+// with 16-byte stores: a lane writes 16 bytes of consecutive positions (two
+// u64 or four u32 outputs) per step, so a warp's store covers 512
+// consecutive bytes.  With a bitmap, the run's bitmap words (at most 32 per
+// round) and their ranks relative to c0 are loaded once, one per lane, and
+// each lane takes its position group's word from the lane holding it.
+// Positions outside [p0, p1) (a partial group at either end) are written one
+// by one; an output not 16-byte aligned goes through warp_store_any.
+template <int KIND, class V>
+__device__ __forceinline__ void store_group(const DecodeOut& O, uint64_t pos, uint64_t p0, uint64_t p1, uint32_t sub,
+                                            uint32_t rank0, V& val) {
+  constexpr uint32_t VW = KIND == 0 ? 2 : 4;
+  // positions of the group inside [p0, p1); a valid one's value index is
+  // rank0 + the valid positions before it in the group (those outside the
+  // run count too: their values precede the run's)
+  uint32_t inr = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < VW; k++)
+    if (pos + k >= p0 && pos + k < p1) inr |= 1u << k;
+  uint64_t v[VW];
+#pragma unroll
+  for (uint32_t k = 0; k < VW; k++) {
+    v[k] = 0;
+    if ((sub & inr) >> k & 1u) v[k] = val(rank0 + __popc(sub & ((1u << k) - 1u)));
+  }
+  if (inr == (1u << VW) - 1u) {
+    if (KIND == 0) {
+      *reinterpret_cast<ulonglong2*>(reinterpret_cast<uint64_t*>(O.out) + pos) = make_ulonglong2(v[0], v[1]);
+    } else {
+      uint32_t u[VW];
+#pragma unroll
+      for (uint32_t k = 0; k < VW; k++) u[k] = KIND == 1 ? (uint32_t)v[k] : (v[k] ? f64bits_to_f32bits(v[k]) : 0u);
+      *reinterpret_cast<uint4*>(reinterpret_cast<uint32_t*>(O.out) + pos) = make_uint4(u[0], u[1], u[VW > 2 ? 2 : 0],
+                                                                                        u[VW > 3 ? 3 : 0]);
+    }
+  } else {
+#pragma unroll
+    for (uint32_t k = 0; k < VW; k++)
+      if ((inr >> k) & 1u) put_kind<KIND>(O.out, pos + k, v[k]);
+  }
+}
+
+template <int KIND, class V>
+__device__ void warp_store_vec(const DecodeOut& O, uint64_t c0, uint32_t cnt, V& val) {
+  constexpr uint32_t VW = KIND == 0 ? 2 : 4;
+  const int l = threadIdx.x & 31;
+  if (!O.bm32) {  // positions c0 .. c0 + cnt hold values 0 .. cnt
+    uint64_t g0 = c0 / VW, g1 = (c0 + cnt + VW - 1) / VW;
+    for (uint64_t g = g0 + l; g < g1; g += 32) {
+      uint64_t pos = g * VW;
+      // every position holds a value: value index = position - c0
+      store_group<KIND>(O, pos, c0, c0 + cnt, (1u << VW) - 1u, (uint32_t)(pos - c0), val);
+    }
+    return;
+  }
+  uint64_t p0, p1;
+  run_positions(O, c0, c0 + cnt, &p0, &p1);
+  if (p1 <= p0) return;
+  uint64_t wb = p0 >> 5, we = (p1 + 31) >> 5;
+  const uint64_t nw_all = (O.n + 31) >> 5;
+  for (uint64_t w0 = wb; w0 < we; w0 += 32) {
+    uint32_t nwords = (uint32_t)qmin(32, we - w0);
+    uint32_t mybits = 0, myrank = 0;
+    if ((uint32_t)l < nwords && w0 + l < nw_all) {
+      mybits = O.bm32[w0 + l];
+      myrank = (uint32_t)(O.wrank[w0 + l] - c0);  // wraps below 0 for positions before the run: never used
+    }
+    const uint32_t ngroups = nwords * (32 / VW);
+    for (uint32_t gb = 0; gb < ngroups; gb += 32) {
+      uint32_t g = gb + (uint32_t)l;
+      uint32_t j = (g * VW) >> 5, bo = (g * VW) & 31;
+      uint32_t bits = __shfl_sync(0xffffffffu, mybits, j & 31);
+      uint32_t r = __shfl_sync(0xffffffffu, myrank, j & 31);
+      if (g < ngroups) {
+        uint64_t pos = (w0 << 5) + (uint64_t)g * VW;
+        uint32_t sub = (bits >> bo) & ((1u << VW) - 1u);
+        store_group<KIND>(O, pos, p0, p1, sub, r + __popc(bits & ((1u << bo) - 1u)), val);
+      }
+    }
+  }
+}
+
+template <class V>
+__device__ void warp_store_item(const DecodeOut& O, uint64_t c0, uint32_t cnt, V val) {
+  if (cnt == 0) return;
+  if (reinterpret_cast<uintptr_t>(O.out) & 15) {
+    warp_store_any(O, c0, cnt, val);
+    return;
+  }
+  switch (out_kind(O.dtype)) {
+    case 1: warp_store_vec<1>(O, c0, cnt, val); break;
+    case 2: warp_store_vec<2>(O, c0, cnt, val); break;
+    default: warp_store_vec<0>(O, c0, cnt, val); break;
+  }
+}
+
 // In-place inclusive prefix sum (wrapping u64) of stg[skew(0 .. cnt)), cnt <=
 // 512, starting from `carry`: each lane sums 16 consecutive entries.
 __device__ inline void warp_prefix_skewed(uint64_t* stg, uint32_t cnt, uint64_t carry) {
@@ -2277,7 +2450,7 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_prepass(const uint8_t* _
     uint32_t k = it.local >> 1, h = it.local & 1;
     uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
     uint64_t s = 0;
-    warp_unpack_half(p, A.offs[0][k], h, cnt, [&](uint32_t, uint64_t v) { s += unzigzag64(v); });
+    warp_unpack_half_fast(p, A.offs[0][k], h, cnt, [&](uint32_t, uint64_t v) { s += unzigzag64(v); });
     R.a = warp_sum(s);
   } else if (d.mode == M_RLE) {
     // run chunk k: the saturating length sum (validation) and the chunk-local
@@ -2410,16 +2583,16 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
       uint64_t c0 = d.value_off + i0;
       if (d.mode == M_CONST) {
         uint64_t v = ld_u64(p);
-        warp_store_any(O, c0, cnt, [&](uint32_t) { return v; });
+        warp_store_item(O, c0, cnt, [&](uint32_t) { return v; });
       } else if (d.mode == M_STRIDE) {
         uint64_t first = ld_u64(p), stride = ld_u64(p + 8);
-        warp_store_any(O, c0, cnt, [&](uint32_t q) { return first + (i0 + q) * stride; });
+        warp_store_item(O, c0, cnt, [&](uint32_t q) { return first + (i0 + q) * stride; });
       } else if (dtype == DT_F32) {
-        warp_store_any(O, c0, cnt, [&](uint32_t q) { return f32bits_to_f64bits(ld_u32(p + 4 * (i0 + q))); });
+        warp_store_item(O, c0, cnt, [&](uint32_t q) { return f32bits_to_f64bits(ld_u32(p + 4 * (i0 + q))); });
       } else if (lane_bytes(dtype) == 4) {
-        warp_store_any(O, c0, cnt, [&](uint32_t q) { return (uint64_t)ld_u32(p + 4 * (i0 + q)); });
+        warp_store_item(O, c0, cnt, [&](uint32_t q) { return (uint64_t)ld_u32(p + 4 * (i0 + q)); });
       } else {
-        warp_store_any(O, c0, cnt, [&](uint32_t q) { return ld_u64(p + 8 * (i0 + q)); });
+        warp_store_item(O, c0, cnt, [&](uint32_t q) { return ld_u64(p + 8 * (i0 + q)); });
       }
       break;
     }
@@ -2429,17 +2602,17 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
       uint32_t hb = h * kItemVals, hc = cnt > hb ? min((uint32_t)kItemVals, cnt - hb) : 0u;
       if (d.mode == M_FLOAT_MULT) {
         double scale = kFmScales[A.a];
-        warp_unpack_half(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t v) {
+        warp_unpack_half_fast(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t v) {
           stg[skew(i - hb)] = f64_bits(__ddiv_rn(__ll2double_rn((long long)v), scale));
         });
       } else if (d.mode == M_DELTA_BITPACK) {
-        warp_unpack_half(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t v) { stg[skew(i - hb)] = unzigzag64(v); });
+        warp_unpack_half_fast(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t v) { stg[skew(i - hb)] = unzigzag64(v); });
       } else {
-        warp_unpack_half(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t v) { stg[skew(i - hb)] = v; });
+        warp_unpack_half_fast(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t v) { stg[skew(i - hb)] = v; });
       }
       __syncwarp();
       if (d.mode == M_DELTA_BITPACK) warp_prefix_skewed(stg, hc, pre[frame_pre[it.frame].x + it.local].a);
-      warp_store_any(O, d.value_off + (uint64_t)k * kSub + hb, hc, [&](uint32_t q) { return stg[skew(q)]; });
+      warp_store_item(O, d.value_off + (uint64_t)k * kSub + hb, hc, [&](uint32_t q) { return stg[skew(q)]; });
       break;
     }
     case M_ALP: {
@@ -2475,7 +2648,7 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
         }
       }
       __syncwarp();
-      warp_store_any(O, d.value_off + (uint64_t)k * kSub + hb, hc, [&](uint32_t q) { return stg[skew(q)]; });
+      warp_store_item(O, d.value_off + (uint64_t)k * kSub + hb, hc, [&](uint32_t q) { return stg[skew(q)]; });
       break;
     }
     case M_ALP_RD: {  // frames without exceptions only
@@ -2484,9 +2657,9 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
       uint32_t cnt = (uint32_t)qmin(kSub, n - (uint64_t)k * kSub);
       uint32_t hb = h * kItemVals, hc = cnt > hb ? min((uint32_t)kItemVals, cnt - hb) : 0u;
       uint32_t bad = 0;
-      warp_unpack_half(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t c) { stg[skew(i - hb)] = c; });
+      warp_unpack_half_fast(p, A.offs[0][k], h, cnt, [&](uint32_t i, uint64_t c) { stg[skew(i - hb)] = c; });
       __syncwarp();
-      warp_unpack_half(p, A.offs[1][k], h, cnt, [&](uint32_t i, uint64_t r) {
+      warp_unpack_half_fast(p, A.offs[1][k], h, cnt, [&](uint32_t i, uint64_t r) {
         uint64_t c = stg[skew(i - hb)];
         if (c >= dsz) bad = 1;
         else stg[skew(i - hb)] = (A.dict8[c] << rbw) | r;
@@ -2496,7 +2669,7 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
         e = E_CORRUPT;
         break;
       }
-      warp_store_any(O, d.value_off + (uint64_t)k * kSub + hb, hc, [&](uint32_t q) { return stg[skew(q)]; });
+      warp_store_item(O, d.value_off + (uint64_t)k * kSub + hb, hc, [&](uint32_t q) { return stg[skew(q)]; });
       break;
     }
     case M_RLE: {
@@ -2515,10 +2688,20 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
       }
       uint64_t cs = R[kc].a;
       uint32_t ck = (uint32_t)qmin(kSub, nr - (uint64_t)kc * kSub);
-      uint32_t a = 0, bb = ck;  // first run of the chunk ending after lo
-      while (a < bb) {
-        uint32_t mid = (a + bb) >> 1;
-        if (cs + ends[(uint64_t)kc * kSub + mid] > lo) bb = mid; else a = mid + 1;
+      // first run of the chunk ending after lo: a ballot over every 32nd
+      // run end, then over the 32 ends of that stretch (two dependent loads)
+      const uint32_t* ce = ends + (uint64_t)kc * kSub;
+      uint32_t a;
+      {
+        uint32_t q = 32u * (uint32_t)l + 31u;
+        bool past = q < ck ? (cs + ce[q] > lo) : true;
+        uint32_t m = __ballot_sync(0xffffffffu, past);
+        uint32_t seg = __ffs(m) - 1;  // the stretch holding the answer (a lane past ck always votes)
+        uint32_t q2 = 32u * seg + (uint32_t)l;
+        bool past2 = q2 < ck ? (cs + ce[q2] > lo) : true;
+        uint32_t m2 = __ballot_sync(0xffffffffu, past2);
+        a = 32u * seg + (uint32_t)(__ffs(m2) - 1);
+        if (a > ck) a = ck;
       }
       // expand the runs overlapping [lo, hi) into the staging buffer, one run
       // per lane at a time, then store
@@ -2542,7 +2725,7 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
         r += 32;
       }
       __syncwarp();
-      warp_store_any(O, d.value_off + lo, (uint32_t)(hi - lo), [&](uint32_t q) { return stg[skew(q)]; });
+      warp_store_item(O, d.value_off + lo, (uint32_t)(hi - lo), [&](uint32_t q) { return stg[skew(q)]; });
       break;
     }
     case M_XORZ: {
@@ -2576,7 +2759,7 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
       }
       if (vbase < n) {
         uint32_t cnt = (uint32_t)qmin((uint64_t)X.total, n - vbase);
-        warp_store_any(O, d.value_off + vbase, cnt, [&](uint32_t q) { return stg[skew(q)]; });
+        warp_store_item(O, d.value_off + vbase, cnt, [&](uint32_t q) { return stg[skew(q)]; });
       }
       break;
     }

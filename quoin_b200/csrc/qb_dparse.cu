@@ -679,10 +679,13 @@ __global__ void __launch_bounds__(kChainThreads) k_dp_marks(const DpHead* __rest
     return;
   }
   const uint32_t M = (uint32_t)K;
-  uint32_t *J0, *J1;  // successor tables (two, for the doubling): shared memory when they fit
-  if ((uint64_t)M * 8 + 16 <= kDpChainSmem) {
+  // successor tables (two, for the doubling) and the marks: shared memory
+  // when they fit
+  uint32_t *J0, *J1;
+  if ((uint64_t)M * 9 + 16 <= kDpChainSmem) {
     J0 = reinterpret_cast<uint32_t*>(dsm);
     J1 = J0 + M;
+    marks = reinterpret_cast<uint8_t*>(J1 + M);
   } else {
     J0 = gJ;
     J1 = gJ + M;
