@@ -412,6 +412,19 @@ __device__ __forceinline__ void put_out(const DecodeOut& O, uint64_t pos, uint64
   }
 }
 
+// Position of the k-th set bit of x (k < popcount(x)): halving by popcounts.
+__device__ __forceinline__ uint32_t select_in_word(uint32_t x, uint32_t k) {
+  uint32_t pos = 0, c = __popc(x & 0xFFFFu);
+  if (k >= c) { k -= c; pos += 16; x >>= 16; }
+  c = __popc(x & 0xFFu);
+  if (k >= c) { k -= c; pos += 8; x >>= 8; }
+  c = __popc(x & 0xFu);
+  if (k >= c) { k -= c; pos += 4; x >>= 4; }
+  c = __popc(x & 0x3u);
+  if (k >= c) { k -= c; pos += 2; x >>= 2; }
+  return pos + ((k >= (x & 1u)) ? 1u : 0u);
+}
+
 // Position of the c-th valid value (c < nvalid): from the 512-granular table,
 // the owning bitmap word is found 32 words at a time.
 __device__ uint64_t warp_select(const DecodeOut& O, uint64_t c) {
@@ -438,8 +451,7 @@ __device__ uint64_t warp_select(const DecodeOut& O, uint64_t c) {
       int src = __ffs(m) - 1;
       bits = __shfl_sync(0xffffffffu, bits, src);
       r = __shfl_sync(0xffffffffu, r, src);
-      for (uint64_t k = c - r; k; k--) bits &= bits - 1u;
-      return ((w0 + (uint64_t)src) << 5) + (uint64_t)(__ffs(bits) - 1);
+      return ((w0 + (uint64_t)src) << 5) + (uint64_t)select_in_word(bits, (uint32_t)(c - r));
     }
   }
   return O.n;
@@ -2022,7 +2034,8 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
 
 // ===========================================================================
 // Warp-item decoder.  The frame table is cut into warp-sized items of at most
-// 512 values (half a FastLanes sub-block) or 512 XORZ payload bytes, so every
+// 512 values (half a FastLanes sub-block) or 2048 XORZ payload bytes (four
+// rounds of 512), so every
 // warp of the grid has the same amount of work whatever the frame sizes.
 // Modes whose values depend on everything before them in the frame carry
 // state across items through a prepass:
@@ -2035,7 +2048,9 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
 // with exceptions are decoded by k_decode_frames from a frame list.
 // ===========================================================================
 constexpr int kItemVals = 512;
-constexpr int kItemBytes = 512;          // XORZ payload bytes per item
+constexpr int kItemBytes = 512;          // XORZ payload bytes per round of an item
+constexpr int kXorzRounds = 4;           // rounds per XORZ item (kXorzItemBytes = 2048 payload bytes)
+static_assert(kItemBytes * kXorzRounds == kXorzItemBytes, "XORZ item size shared with the readers");
 constexpr int kItemStage = kItemVals + kItemVals / 16;  // u64 staging with one pad per 16
 constexpr int kItemWarps = 8;
 
@@ -2232,7 +2247,7 @@ __device__ __forceinline__ void store_group(const DecodeOut& O, uint64_t pos, ui
 }
 
 template <int KIND, class V>
-__device__ void warp_store_vec(const DecodeOut& O, uint64_t c0, uint32_t cnt, V& val) {
+__device__ void warp_store_vec(const DecodeOut& O, uint64_t c0, uint32_t cnt, V& val, uint64_t* pchain) {
   constexpr uint32_t VW = KIND == 0 ? 2 : 4;
   const int l = threadIdx.x & 31;
   if (!O.bm32) {  // positions c0 .. c0 + cnt hold values 0 .. cnt
@@ -2245,7 +2260,13 @@ __device__ void warp_store_vec(const DecodeOut& O, uint64_t c0, uint32_t cnt, V&
     return;
   }
   uint64_t p0, p1;
-  run_positions(O, c0, c0 + cnt, &p0, &p1);
+  if (pchain && *pchain != ~0ull) {  // the previous run of the warp ended here
+    p0 = *pchain;
+    p1 = c0 + cnt >= O.nvalid ? O.n : warp_select(O, c0 + cnt);
+  } else {
+    run_positions(O, c0, c0 + cnt, &p0, &p1);
+  }
+  if (pchain) *pchain = p1;
   if (p1 <= p0) return;
   uint64_t wb = p0 >> 5, we = (p1 + 31) >> 5;
   const uint64_t nw_all = (O.n + 31) >> 5;
@@ -2271,17 +2292,20 @@ __device__ void warp_store_vec(const DecodeOut& O, uint64_t c0, uint32_t cnt, V&
   }
 }
 
+// pchain (optional): in, the first position of this run when a previous run
+// of the warp ended there (~0 when unknown); out, this run's end position.
 template <class V>
-__device__ void warp_store_item(const DecodeOut& O, uint64_t c0, uint32_t cnt, V val) {
+__device__ void warp_store_item(const DecodeOut& O, uint64_t c0, uint32_t cnt, V val, uint64_t* pchain = nullptr) {
   if (cnt == 0) return;
   if (reinterpret_cast<uintptr_t>(O.out) & 15) {
+    if (pchain) *pchain = ~0ull;
     warp_store_any(O, c0, cnt, val);
     return;
   }
   switch (out_kind(O.dtype)) {
-    case 1: warp_store_vec<1>(O, c0, cnt, val); break;
-    case 2: warp_store_vec<2>(O, c0, cnt, val); break;
-    default: warp_store_vec<0>(O, c0, cnt, val); break;
+    case 1: warp_store_vec<1>(O, c0, cnt, val, pchain); break;
+    case 2: warp_store_vec<2>(O, c0, cnt, val, pchain); break;
+    default: warp_store_vec<0>(O, c0, cnt, val, pchain); break;
   }
 }
 
@@ -2480,13 +2504,20 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_prepass(const uint8_t* _
     for (int o = 16; o; o >>= 1) s = qmin(s + __shfl_xor_sync(0xffffffffu, s, o), n + 1);
     R.a = s;
   } else if (d.mode == M_XORZ) {
-    XSlice X = xorz_lane_scan<true>(p, d.plen, (uint64_t)it.local * kItemBytes);
-    uint64_t xo = X.xo;
+    // the item's rounds of 512 payload bytes: contributions XOR, value count,
+    // last terminator, over-long flag, combined
+    uint64_t xo = 0;
+    for (int r = 0; r < kXorzRounds; r++) {
+      uint64_t s0 = (uint64_t)it.local * kXorzItemBytes + (uint64_t)r * kItemBytes;
+      if (s0 >= d.plen) break;
+      XSlice X = xorz_lane_scan<true>(p, d.plen, s0);
+      xo ^= X.xo;
+      R.b += X.total;
+      if (X.lastt > R.last) R.last = X.lastt;
+      R.flag |= warp_or_u32(X.bad);
+    }
     for (int o = 16; o; o >>= 1) xo ^= __shfl_xor_sync(0xffffffffu, xo, o);
     R.a = xo;
-    R.b = X.total;
-    R.last = X.lastt;
-    R.flag = warp_or_u32(X.bad);
   }
   if (l == 0) pre[g] = R;
 }
@@ -2730,36 +2761,44 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
     }
     case M_XORZ: {
       const PreRec& R = pre[frame_pre[it.frame].x + it.local];
-      uint64_t vbase = R.b;
-      XSlice X = xorz_lane_scan<false>(p, d.plen, (uint64_t)it.local * kItemBytes);
-      // one pass from a zero state (values relative to the lane's start), then
-      // the lane's carry: the item's carry and the lanes before
-      uint64_t own = xorz_lane_bytes<true, true>(X, 0ull, stg, 0);
-      uint64_t inc = own;
-      for (int o = 1; o < 32; o <<= 1) {
-        uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
-        if (l >= o) inc ^= u;
-      }
-      uint64_t base = R.a ^ inc ^ own;
-      for (uint32_t q = 0; q < X.cnt; q++) stg[skew(X.before + q)] ^= base;
-      __syncwarp();
-      // checks on the values that exist (index < n): length, and the n-th
-      // value's terminator must be the payload's last byte
-      uint32_t bad = 0;
-      uint64_t lane0 = vbase + X.before;
-      if (X.first_bad != ~0u && lane0 + X.first_bad < n) bad = 1;
-      if (n && lane0 <= n - 1 && n - 1 < lane0 + X.cnt) {
-        uint32_t m = X.tm;
-        for (uint64_t q = n - 1 - lane0; q; q--) m &= m - 1u;
-        if ((int64_t)(X.b0 + (uint64_t)(__ffs(m) - 1)) != (int64_t)d.plen - 1) bad = 1;
-      }
-      if (warp_or_u32(bad)) {
-        e = E_CORRUPT;
-        break;
-      }
-      if (vbase < n) {
-        uint32_t cnt = (uint32_t)qmin((uint64_t)X.total, n - vbase);
-        warp_store_item(O, d.value_off + vbase, cnt, [&](uint32_t q) { return stg[skew(q)]; });
+      uint64_t vbase = R.b, carry = R.a;
+      uint64_t pnext = ~0ull;  // the next round's first position (the last round's end)
+      for (int rd = 0; rd < kXorzRounds; rd++) {
+        uint64_t s0 = (uint64_t)it.local * kXorzItemBytes + (uint64_t)rd * kItemBytes;
+        if (s0 >= d.plen) break;
+        XSlice X = xorz_lane_scan<false>(p, d.plen, s0);
+        // one pass from a zero state (values relative to the lane's start),
+        // then the lane's carry: the round's carry and the lanes before
+        uint64_t own = xorz_lane_bytes<true, true>(X, 0ull, stg, 0);
+        uint64_t inc = own;
+        for (int o = 1; o < 32; o <<= 1) {
+          uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+          if (l >= o) inc ^= u;
+        }
+        uint64_t base = carry ^ inc ^ own;
+        for (uint32_t q = 0; q < X.cnt; q++) stg[skew(X.before + q)] ^= base;
+        carry ^= __shfl_sync(0xffffffffu, inc, 31);
+        __syncwarp();
+        // checks on the values that exist (index < n): length, and the n-th
+        // value's terminator must be the payload's last byte
+        uint32_t bad = 0;
+        uint64_t lane0 = vbase + X.before;
+        if (X.first_bad != ~0u && lane0 + X.first_bad < n) bad = 1;
+        if (n && lane0 <= n - 1 && n - 1 < lane0 + X.cnt) {
+          uint32_t m = X.tm;
+          for (uint64_t q = n - 1 - lane0; q; q--) m &= m - 1u;
+          if ((int64_t)(X.b0 + (uint64_t)(__ffs(m) - 1)) != (int64_t)d.plen - 1) bad = 1;
+        }
+        if (warp_or_u32(bad)) {
+          e = E_CORRUPT;
+          break;
+        }
+        if (vbase < n) {
+          uint32_t cnt = (uint32_t)qmin((uint64_t)X.total, n - vbase);
+          warp_store_item(O, d.value_off + vbase, cnt, [&](uint32_t q) { return stg[skew(q)]; }, &pnext);
+        }
+        vbase += X.total;
+        __syncwarp();  // the staging buffer is reused by the next round
       }
       break;
     }

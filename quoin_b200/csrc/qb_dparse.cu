@@ -19,7 +19,7 @@
 //      log2(K) rounds exactly the frames on the chain are marked (every jump
 //      from a chain frame lands on a chain frame), and chain order is
 //      position order (k_dp_marks, one CTA);
-//   3. the marked frames' warp items (512 values, or 512 XORZ payload bytes)
+//   3. the marked frames' warp items (512 values, or 2048 XORZ payload bytes)
 //      are counted as the host reader's build_items does (k_dp_items, across
 //      the GPU), the frames cut where their values reach the lane's count and
 //      laid out (k_dp_layout, one CTA), and the items listed (k_dp_expand).
@@ -589,7 +589,7 @@ __device__ FrameItems dp_frame_items(const uint8_t* p, uint64_t n, uint64_t plen
       r.scan = true;
       break;
     case 3:
-      r.npre = r.nmain = (uint32_t)((plen + 511) / 512);
+      r.npre = r.nmain = (uint32_t)((plen + kXorzItemBytes - 1) / kXorzItemBytes);
       r.scan = true;
       break;
     case 53: {

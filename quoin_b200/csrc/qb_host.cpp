@@ -814,7 +814,7 @@ bool entropy_frame_h(const uint8_t* p, uint64_t plen, uint32_t mode) {
   }
 }
 
-// Warp items of every frame (512 values, or 512 payload bytes for XORZ).
+// Warp items of every frame (512 values, or kXorzItemBytes payload bytes for XORZ).
 // Frames the items do not cover, or whose header cannot be read here, go to
 // the frame list; the device walk reports their errors.  Listed frames with
 // an entropy-coded part get a device area (ent_area_bytes: the mode's layout,
@@ -822,7 +822,7 @@ bool entropy_frame_h(const uint8_t* p, uint64_t plen, uint32_t mode) {
 // (128-byte units, 1 + its offset in FrameDesc::aux; 0 = none).
 void build_items(const uint8_t* src, LaneIdx& L) {
   const uint32_t V = 512, B = 512;
-  {  // one reservation (items of 512 values or 512 XORZ bytes, prepass items at most as many)
+  {  // one reservation (items of 512 values or 512+ XORZ bytes, prepass items at most as many)
     uint64_t est = 0;
     for (const FrameDesc& d : L.frames) est += (d.n + V - 1) / V + (d.plen + B - 1) / B;
     L.main_items.reserve(est);
@@ -855,7 +855,7 @@ void build_items(const uint8_t* src, LaneIdx& L) {
         L.need_scan = true;
         break;
       case 3: {  // XORZ
-        uint32_t nb = (uint32_t)((plen + B - 1) / B);
+        uint32_t nb = (uint32_t)((plen + kXorzItemBytes - 1) / kXorzItemBytes);
         add_pre(nb);
         add_main(nb);
         L.need_scan = true;

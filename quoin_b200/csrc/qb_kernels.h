@@ -11,6 +11,9 @@ struct QuoinCtx;
 namespace qb {
 
 // ---- decoder (qb_decode.cu) ----
+// Payload bytes of one XORZ warp item (the readers cut XORZ frames into
+// items of this many bytes; other modes into items of 512 values).
+constexpr uint32_t kXorzItemBytes = 2048;
 // The entropy area of a listed frame of n values (128-byte aligned pieces):
 // the mode's own layout (24 bytes per value + 1,152), the range coder's
 // 256 x 256 model (128 KB), the FCM / DFCM table of PRED, PRED_RC and PRED2
