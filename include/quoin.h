@@ -332,9 +332,11 @@ int quoin_b200_decompress_batch_device(QuoinBatch *batch, QuoinB200DecompressJob
 /* No counterpart in the reference.  A server runs compress and decompress
  * requests on device-resident buffers for many callers: requests are queued
  * in arrival order and admitted when the device memory they hold fits the
- * server's budget beside the running ones (a request above the budget on its
- * own is refused with QUOIN_ERR_OVER_BUDGET), then run on a pool of contexts.
- * Each request's bytes are those of the single-column call. */
+ * server's budget beside the running ones and the device's free memory
+ * (cudaMemGetInfo, 1 GiB kept free) at that moment (a request above the
+ * budget on its own is refused with QUOIN_ERR_OVER_BUDGET), then run on a
+ * pool of contexts.  Each request's bytes are those of the single-column
+ * call. */
 #define QUOIN_ERR_OVER_BUDGET (-23) /* a request needs more device memory than the server's budget */
 #define QUOIN_ERR_TIMEOUT     (-24) /* quoin_b200_server_wait: the request has not finished yet */
 #define QUOIN_B200_OP_COMPRESS   0

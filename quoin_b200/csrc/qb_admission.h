@@ -1,13 +1,21 @@
 // FIFO admission of requests against a device-memory budget, for the request
 // server (qb_serve.cpp).  Requests leave in arrival order: the head is handed
 // to a worker once the bytes it will hold fit beside those of the requests
-// already running; a request that alone exceeds the budget is refused when it
-// is submitted.  Host-only code (no CUDA), so the policy is testable on CPU.
+// already running and, with a free-memory probe, within the device memory
+// free at that moment (less a reserve); a request that alone exceeds the
+// budget is refused when it is submitted.  A head that fits the budget but
+// not the free memory waits (re-probing every few milliseconds) while other
+// requests run; with nothing running it is admitted anyway, so the queue
+// always moves (its allocations then fail or succeed on their own).
+// Host-only code (no CUDA; the probe is a plain function), so the policy is
+// testable on CPU.
 #pragma once
 
+#include <chrono>
 #include <condition_variable>
 #include <cstdint>
 #include <deque>
+#include <functional>
 #include <mutex>
 #include <utility>
 
@@ -17,6 +25,14 @@ template <class T>
 class AdmissionQueue {
  public:
   explicit AdmissionQueue(uint64_t budget) : budget_(budget) {}
+
+  // Device memory free right now (e.g. cudaMemGetInfo), consulted before a
+  // head request is admitted; `reserve` bytes are kept free.
+  void set_free_probe(std::function<uint64_t()> probe, uint64_t reserve) {
+    std::lock_guard<std::mutex> l(mu_);
+    probe_ = std::move(probe);
+    reserve_ = reserve;
+  }
 
   // Queues `item` holding `bytes` while it runs.  False when it can never be
   // admitted (bytes > budget) or the queue is closed.
@@ -34,8 +50,15 @@ class AdmissionQueue {
   // its bytes as in use.  False once the queue is closed and drained.
   bool pop(T* item, uint64_t* bytes) {
     std::unique_lock<std::mutex> l(mu_);
-    cv_.wait(l, [&] { return (!q_.empty() && in_use_ + q_.front().second <= budget_) || (closed_ && q_.empty()); });
-    if (q_.empty()) return false;
+    for (;;) {
+      cv_.wait(l, [&] { return (!q_.empty() && in_use_ + q_.front().second <= budget_) || (closed_ && q_.empty()); });
+      if (q_.empty()) return false;
+      if (!probe_ || in_use_ == 0) break;
+      uint64_t fr = probe_();
+      if (fr > reserve_ && q_.front().second <= fr - reserve_) break;
+      waits_for_memory_++;
+      cv_.wait_for(l, std::chrono::milliseconds(5));  // memory frees as running requests end
+    }
     *item = std::move(q_.front().first);
     *bytes = q_.front().second;
     q_.pop_front();
@@ -74,10 +97,16 @@ class AdmissionQueue {
     std::lock_guard<std::mutex> l(mu_);
     return q_.size();
   }
+  // Times a head request that fit the budget waited for free device memory.
+  uint64_t waits_for_memory() const {
+    std::lock_guard<std::mutex> l(mu_);
+    return waits_for_memory_;
+  }
 
  private:
   const uint64_t budget_;
-  uint64_t in_use_ = 0, peak_ = 0;
+  uint64_t in_use_ = 0, peak_ = 0, reserve_ = 0, waits_for_memory_ = 0;
+  std::function<uint64_t()> probe_;
   bool closed_ = false;
   std::deque<std::pair<T, uint64_t>> q_;
   mutable std::mutex mu_;

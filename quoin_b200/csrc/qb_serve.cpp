@@ -10,6 +10,8 @@
 #include <thread>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "../../include/quoin.h"
 #include "qb_admission.h"
 
@@ -85,6 +87,24 @@ extern "C" QuoinServer* quoin_b200_server_create(int workers, uint64_t budget_by
       if (!c) throw 0;
       s->ctxs.push_back(c);
     }
+    // admission also by the device memory free when a request starts (other
+    // processes and the contexts' arenas share the GPU); 1 GiB stays free
+    int dev = 0;
+    cudaGetDevice(&dev);
+    s->queue.set_free_probe(
+        [dev]() -> uint64_t {
+          int prev = 0;
+          size_t fr = 0, tot = 0;
+          cudaGetDevice(&prev);
+          if (prev != dev) cudaSetDevice(dev);
+          if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            cudaGetLastError();
+            fr = ~(size_t)0;  // unknown: the budget alone decides
+          }
+          if (prev != dev) cudaSetDevice(prev);
+          return (uint64_t)fr;
+        },
+        1ull << 30);
     for (QuoinCtx* c : s->ctxs) s->workers.emplace_back([s, c] { s->run(c); });
     return s;
   } catch (...) {

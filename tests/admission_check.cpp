@@ -21,6 +21,35 @@
 
 int main() {
   using Q = qb::AdmissionQueue<int>;
+  {  // free-memory admission: a head within the budget waits for free memory
+     // while another request runs, and is admitted once memory frees
+    Q q(1000);
+    std::atomic<uint64_t> free_mem{300};
+    q.set_free_probe([&] { return free_mem.load(); }, 50);
+    CHECK(q.push(1, 200) && q.push(2, 400));
+    int v = 0;
+    uint64_t b = 0;
+    CHECK(q.pop(&v, &b) && v == 1);  // 200 <= 300 - 50
+    std::atomic<int> got{0};
+    std::thread t([&] {
+      int w = 0;
+      uint64_t c = 0;
+      if (q.pop(&w, &c)) got = w;
+    });
+    std::this_thread::sleep_for(std::chrono::milliseconds(60));
+    CHECK(got == 0 && q.waits_for_memory() > 0);  // 400 > 300 - 50 although within the budget
+    free_mem = 600;
+    std::this_thread::sleep_for(std::chrono::milliseconds(60));
+    CHECK(got == 2);  // admitted on a re-probe, request 1 still running
+    t.join();
+    q.release(200);
+    q.release(400);
+    // with nothing running the head is admitted whatever the probe says
+    free_mem = 0;
+    CHECK(q.push(3, 500));
+    CHECK(q.pop(&v, &b) && v == 3);
+    q.release(500);
+  }
   {  // a request above the budget is refused; one at the budget is admitted
     Q q(100);
     CHECK(!q.push(1, 101));
