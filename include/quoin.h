@@ -243,8 +243,9 @@ int quoin_b200_decompress_column_device(QuoinCtx *ctx, const uint8_t *d_src, siz
  * one was (1 a header the device reader does not take, 2 a frame table it
  * could not resolve, 3 more frame candidates than its tables held); for the
  * last stream the device reader read, out[3] its frame-header candidates and
- * out[4] how many times it laid out its tables (2 after a capacity retry). */
-void quoin_b200_reader_stats(uint64_t out[5]);
+ * out[4] how many times it laid out its tables (2 after a capacity retry);
+ * out[5] the columns quoin_b200_decompress_queue_device decoded in batches. */
+void quoin_b200_reader_stats(uint64_t out[6]);
 
 /* No counterpart in the reference.  Allocation-free device decode for callers
  * that cannot let the library allocate device memory (an engine that owns all
@@ -326,6 +327,34 @@ typedef struct {
 int quoin_b200_compress_batch_device(QuoinBatch *batch, QuoinB200CompressJob *jobs, size_t njobs,
                                      const QuoinConfig *cfg);
 int quoin_b200_decompress_batch_device(QuoinBatch *batch, QuoinB200DecompressJob *jobs, size_t njobs);
+
+/* One column of quoin_b200_decompress_queue_device: a device-resident stream
+ * and the device buffers for its values (values_cap_bytes) and bitmap
+ * (optional), as for quoin_b200_decompress_column_device. */
+typedef struct {
+    const uint8_t *d_src;
+    size_t src_len;
+    void *d_values_out;
+    size_t values_cap_bytes;
+    uint8_t *d_validity_out;
+    int32_t wire;   /* out: the stream's dtype */
+    uint64_t n;     /* out: its value count */
+    int32_t status; /* out: the column's return code */
+} QuoinB200DeviceDecodeJob;
+
+/* No reference counterpart (the batched configuration).  Decodes every job's
+ * device-resident stream with one launch per kernel class for the whole
+ * batch (src/decoder.rs:43-190 per column): the headers, validity bitmaps,
+ * frame chains and warp-item tables of all columns are read by one set of
+ * launches over a device-side table of (column, chunk) and (column,
+ * candidate) work, and one launch of each block-decoder kernel decodes every
+ * column's frames, each frame writing through its column's output.  Columns
+ * this path leaves out (decimal containers, RLE validity blobs, entropy-coded
+ * frames, damaged streams, all-null columns) are decoded one by one as by
+ * quoin_b200_decompress_column_device, so every column gets its own status.
+ * Returns QUOIN_OK or the first failing job's status in job order. */
+int quoin_b200_decompress_queue_device(QuoinCtx *ctx, QuoinB200DeviceDecodeJob *jobs, size_t njobs,
+                                       void *stream);
 
 /* ---------------- Request server ---------------- */
 

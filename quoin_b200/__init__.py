@@ -136,6 +136,7 @@ def _load():
                                                       ctypes.POINTER(ctypes.c_uint64), P]
     L.quoin_b200_mode_win_counts.argtypes = [P]
     L.quoin_b200_reader_stats.argtypes = [P]
+    L.quoin_b200_decompress_queue_device.argtypes = [P, P, S, P]
     L.quoin_b200_reset_mode_win_counts.argtypes = []
     L.quoin_b200_kernel_launches.restype = ctypes.c_uint64
     return L

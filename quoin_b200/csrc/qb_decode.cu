@@ -131,10 +131,12 @@ __device__ uint32_t alprd_walk_tail(const uint8_t* p, uint64_t plen, uint64_t n,
 
 // One thread per frame.
 __global__ void k_walk_frames(const uint8_t* __restrict__ stream, const FrameDesc* __restrict__ frames, int nf,
-                              int dtype, FrameAux* __restrict__ aux, unsigned long long* __restrict__ err) {
+                              int dtype, FrameAux* __restrict__ aux, unsigned long long* __restrict__ err,
+                              BatchView bv) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nf) return;
   FrameDesc d = frames[f];
+  if (bv.cols) dtype = bv.cols[bv.frame_col[f]].dtype;
   const uint8_t* p = stream + d.payload_off;
   uint64_t plen = d.plen, n = d.n;
   FrameAux& A = aux[f];
@@ -1758,11 +1760,17 @@ __global__ void __launch_bounds__(kDecThreads) k_decode_frames(const uint8_t* __
                                                               DecodeOut O, uint64_t* __restrict__ scratch,
                                                               unsigned long long* __restrict__ err,
                                                               const uint32_t* __restrict__ list,
-                                                              uint8_t* __restrict__ ent) {
+                                                              uint8_t* __restrict__ ent, BatchView bv) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   DecSmem& S = *reinterpret_cast<DecSmem*>(smem_raw);
   if ((int)blockIdx.x >= nf) return;
   int f = list ? (int)list[blockIdx.x] : (int)blockIdx.x;
+  if (bv.cols) {  // a batch: the frame's column decides the output
+    const BatchCol& C = bv.cols[bv.frame_col[f]];
+    O = C.O;
+    dtype = C.dtype;
+    scratch = C.scratch;
+  }
   FrameAux& A = aux[f];  // written here only by thread 0 of a deferred walk, read after a barrier
   if (A.err) return;
   FrameDesc d = frames[f];
@@ -2453,7 +2461,8 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_prepass(const uint8_t* _
                                                            const FrameDesc* __restrict__ frames,
                                                            const FrameAux* __restrict__ aux,
                                                            const ItemRef* __restrict__ items, uint32_t nitems,
-                                                           PreRec* __restrict__ pre, uint64_t* __restrict__ scratch) {
+                                                           PreRec* __restrict__ pre, uint64_t* __restrict__ scratch,
+                                                           BatchView bv) {
   __shared__ uint32_t rle_stage[kItemWarps][kSub];
   uint32_t g = blockIdx.x * kItemWarps + (threadIdx.x >> 5);
   int l = threadIdx.x & 31;
@@ -2462,6 +2471,7 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_prepass(const uint8_t* _
   const FrameAux& A = aux[it.frame];
   if (A.err) return;
   FrameDesc d = frames[it.frame];
+  if (bv.cols) scratch = bv.cols[bv.frame_col[it.frame]].scratch;
   const uint8_t* p = stream + d.payload_off;
   uint64_t n = d.n;
   PreRec R;
@@ -2594,7 +2604,7 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
                                                                 const uint2* __restrict__ frame_pre,
                                                                 const PreRec* __restrict__ pre, DecodeOut O,
                                                                 const uint64_t* __restrict__ scratch,
-                                                                unsigned long long* __restrict__ err) {
+                                                                unsigned long long* __restrict__ err, BatchView bv) {
   __shared__ __align__(16) uint64_t stage_all[kItemWarps][kItemStage];
   int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
   uint32_t g = blockIdx.x * kItemWarps + warp;
@@ -2603,6 +2613,12 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8
   const FrameAux& A = aux[it.frame];
   if (A.err) return;
   FrameDesc d = frames[it.frame];
+  if (bv.cols) {  // a batch: the frame's column decides the output
+    const BatchCol& C = bv.cols[bv.frame_col[it.frame]];
+    O = C.O;
+    dtype = C.dtype;
+    scratch = C.scratch;
+  }
   const uint8_t* p = stream + d.payload_off;
   uint64_t n = d.n;
   uint64_t* stg = stage_all[warp];
@@ -2931,27 +2947,29 @@ uint64_t decode_aux_bytes(int nf) { return (uint64_t)(nf > 0 ? nf : 1) * sizeof(
 
 void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
                           uint64_t* scratch, void* aux, unsigned long long* err, cudaStream_t st) {
+  const BatchView bv{nullptr, nullptr};
   if (nf <= 0) return;
   FrameAux* A = reinterpret_cast<FrameAux*>(aux);
-  k_walk_frames<<<(nf + 127) / 128, 128, 0, st>>>(stream, frames, nf, dtype, A, err);
+  k_walk_frames<<<(nf + 127) / 128, 128, 0, st>>>(stream, frames, nf, dtype, A, err, bv);
   set_decode_frames_smem();
   k_decode_frames<<<nf, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, nf, dtype, A, out, scratch, err, nullptr,
-                                                            nullptr);
+                                                            nullptr, bv);
   count_launches(2);
 }
 
 void launch_decode_items(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
                          const ItemPlan& plan, void* pre, uint64_t* scratch, void* aux, unsigned long long* err,
-                         cudaStream_t st) {
+                         cudaStream_t st, const BatchView* batch) {
+  const BatchView bv = batch ? *batch : BatchView{nullptr, nullptr};
   if (nf <= 0) return;
   FrameAux* A = reinterpret_cast<FrameAux*>(aux);
   PreRec* P = reinterpret_cast<PreRec*>(pre);
-  k_walk_frames<<<(nf + 127) / 128, 128, 0, st>>>(stream, frames, nf, dtype, A, err);
+  k_walk_frames<<<(nf + 127) / 128, 128, 0, st>>>(stream, frames, nf, dtype, A, err, bv);
   int launches = 1;
   if (plan.npre) {
     k_prepass<<<(plan.npre + kItemWarps - 1) / kItemWarps, kItemWarps * 32, 0, st>>>(stream, frames, A,
                                                                                    plan.pre_items, plan.npre, P,
-                                                                                   scratch);
+                                                                                   scratch, bv);
     launches++;
   }
   if (plan.need_scan) {
@@ -2961,13 +2979,13 @@ void launch_decode_items(const uint8_t* stream, const FrameDesc* frames, int nf,
   }
   if (plan.nmain) {
     k_decode_items<<<(plan.nmain + kItemWarps - 1) / kItemWarps, kItemWarps * 32, 0, st>>>(
-        stream, frames, dtype, A, plan.main_items, plan.nmain, plan.frame_pre, P, out, scratch, err);
+        stream, frames, dtype, A, plan.main_items, plan.nmain, plan.frame_pre, P, out, scratch, err, bv);
     launches++;
   }
   if (plan.nlist) {
     set_decode_frames_smem();
     k_decode_frames<<<plan.nlist, kDecThreads, sizeof(DecSmem), st>>>(stream, frames, (int)plan.nlist, dtype, A, out,
-                                                                       scratch, err, plan.list, plan.ent);
+                                                                       scratch, err, plan.list, plan.ent, bv);
     launches++;
   }
   count_launches(launches);

@@ -127,9 +127,7 @@ __device__ bool dp_validity(const uint8_t* s, uint64_t len, uint64_t* pos, uint6
   return true;
 }
 
-__global__ void k_dp_head(const uint8_t* __restrict__ s, uint64_t len, DpHead* __restrict__ out) {
-  if (threadIdx.x || blockIdx.x) return;
-  DpHead H;
+__device__ void dp_parse_head(const uint8_t* __restrict__ s, uint64_t len, DpHead& H) {
   memset(&H, 0, sizeof(H));
   H.kind = 1;
   do {
@@ -174,6 +172,12 @@ __global__ void k_dp_head(const uint8_t* __restrict__ s, uint64_t len, DpHead* _
       H.kind = 0;
     }
   } while (false);
+}
+
+__global__ void k_dp_head(const uint8_t* __restrict__ s, uint64_t len, DpHead* __restrict__ out) {
+  if (threadIdx.x || blockIdx.x) return;
+  DpHead H;
+  dp_parse_head(s, len, H);
   *out = H;
 }
 
@@ -921,4 +925,476 @@ void launch_dp_chain(const uint8_t* s, const DpHead* H, int lane, const uint64_t
   count_launches(5);
 }
 
+
+// ===========================================================================
+// Batches: every column of a batch read by one launch per kernel class.  A
+// column's work items (bitmap words, candidate chunks, candidates) are found
+// from its place in the batch's arrays by binary search over the columns'
+// offsets, and the per-column steps (the chain doubling, the layout) take one
+// CTA per column.  The same device functions as the single-column reader.
+// ===========================================================================
+namespace {
+
+// The lane owning position `x` of an array laid out by the nondecreasing
+// offsets first[0 .. n] (first[n] = the total): the last i with first[i] <= x.
+__device__ inline int dp_owner(const uint64_t* first, int n, uint64_t x) {
+  int lo = 0, hi = n;  // answer in [lo, hi)
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (first[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_dpb_heads(const uint8_t* const* __restrict__ srcs, const uint64_t* __restrict__ lens, int n,
+                            DpHead* __restrict__ H) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  DpHead h;
+  dp_parse_head(srcs[i], lens[i], h);
+  H[i] = h;
+}
+
+// Bitmap words of every column with a bitmap (k_dp_bitmap's work), their
+// popcounts, and the caller's bitmap bytes.  word_first[c] = lanes[c].word0.
+__global__ void k_dpb_bitmap(DpBatch B, const uint64_t* __restrict__ word_first) {
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < B.words;
+       w += (uint64_t)gridDim.x * blockDim.x) {
+    int c = dp_owner(word_first, B.nlanes, w);
+    const DpBLane& Ln = B.lanes[c];
+    uint64_t k = w - Ln.word0;
+    uint32_t bits = 0;
+    if (Ln.L.has_validity && k < Ln.nw) {
+      const uint8_t* src = Ln.s + Ln.vblob_off;
+      uint64_t n = Ln.L.logical_n, nb = (n + 7) / 8, b0 = 4 * k;
+      if (b0 + 4 <= nb) {
+        bits = ld_u32(src + b0);
+      } else {
+        for (uint64_t q = 0; q < 4 && b0 + q < nb; q++) bits |= (uint32_t)src[b0 + q] << (8 * q);
+      }
+      uint64_t rem = n - 32 * k;
+      if (rem < 32) bits &= (1u << rem) - 1u;
+      if (Ln.valid_out)
+        for (uint64_t q = 0; q < 4 && b0 + q < nb; q++) Ln.valid_out[b0 + q] = (uint8_t)(bits >> (8 * q));
+    }
+    B.bm32[w] = bits;
+    B.ranks[w] = (uint64_t)__popc(bits);
+  }
+}
+
+// Per column: its valid count and the global rank at its first word.
+__global__ void k_dpb_lane_base(DpBatch B) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= B.nlanes) return;
+  const DpBLane& Ln = B.lanes[c];
+  uint64_t base = B.ranks[Ln.word0];
+  B.rbase[c] = base;
+  B.out[c].nvalid = Ln.L.has_validity ? B.ranks[Ln.word0 + Ln.nw] - base : Ln.L.logical_n;
+}
+
+// Column-relative ranks, then the select tables (k_select_table per column).
+__global__ void k_dpb_ranks(DpBatch B, const uint64_t* __restrict__ word_first) {
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < B.words;
+       w += (uint64_t)gridDim.x * blockDim.x) {
+    int c = dp_owner(word_first, B.nlanes, w);
+    B.ranks[w] -= B.rbase[c];
+  }
+}
+__global__ void k_dpb_select(DpBatch B, const uint64_t* __restrict__ word_first) {
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < B.words;
+       w += (uint64_t)gridDim.x * blockDim.x) {
+    int c = dp_owner(word_first, B.nlanes, w);
+    const DpBLane& Ln = B.lanes[c];
+    uint64_t k = w - Ln.word0;
+    if (!Ln.L.has_validity || k >= Ln.nw) continue;
+    uint32_t bits = B.bm32[w];
+    uint64_t r = B.ranks[w], cnt = (uint64_t)__popc(bits);
+    uint64_t m = (r + 511) / 512 * 512;
+    if (m < r + cnt) {
+      uint32_t x = bits;
+      for (uint64_t q = m - r; q; q--) x &= x - 1u;
+      B.sel[Ln.sel0 + m / 512] = k * 32 + (uint64_t)(__ffs(x) - 1);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kDpThreads) k_dpb_cand_scan(DpBatch B) {
+  __shared__ uint64_t s_warp[33];
+  __shared__ int s_c;
+  if (threadIdx.x == 0) s_c = dp_owner(B.chunk0, B.nlanes, blockIdx.x);
+  __syncthreads();
+  const DpBLane& Ln = B.lanes[s_c];
+  uint64_t chunk = blockIdx.x - Ln.chunk0;
+  uint32_t m[kDpSteps];
+  uint64_t a[kDpSteps], at[kDpSteps];
+  uint64_t tot = dp_chunk_cands(Ln.s, Ln.buf_len, Ln.L, chunk, s_warp, m, a, at);
+#pragma unroll
+  for (int k = 0; k < kDpSteps; k++) {
+    uint32_t mk = m[k];
+    uint64_t q = at[k];
+    while (mk && q < kDpSlots) {
+      uint32_t i = __ffs(mk) - 1;
+      mk &= mk - 1;
+      B.slots[(uint64_t)blockIdx.x * kDpSlots + q] = dp_cand_at(Ln.s, a[k] + i);
+      q++;
+    }
+  }
+  if (threadIdx.x == 0) B.cnt[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kDpThreads) k_dpb_cand_compact(DpBatch B) {
+  __shared__ uint64_t s_warp[33];
+  __shared__ int s_c;
+  uint64_t base = B.cnt[blockIdx.x], c = B.cnt[blockIdx.x + 1] - base;
+  if (c == 0) return;
+  if (threadIdx.x == 0) s_c = dp_owner(B.chunk0, B.nlanes, blockIdx.x);
+  __syncthreads();
+  const int lane = s_c;
+  if (c <= kDpSlots) {
+    if (threadIdx.x < c && base + threadIdx.x < B.cap) {
+      B.cand[base + threadIdx.x] = B.slots[(uint64_t)blockIdx.x * kDpSlots + threadIdx.x];
+      B.cand_lane[base + threadIdx.x] = (uint32_t)lane;
+    }
+    return;
+  }
+  const DpBLane& Ln = B.lanes[lane];
+  uint32_t m[kDpSteps];
+  uint64_t a[kDpSteps], at[kDpSteps];
+  dp_chunk_cands(Ln.s, Ln.buf_len, Ln.L, blockIdx.x - Ln.chunk0, s_warp, m, a, at);
+#pragma unroll
+  for (int k = 0; k < kDpSteps; k++) {
+    uint32_t mk = m[k];
+    uint64_t q = base + at[k];
+    while (mk) {
+      uint32_t i = __ffs(mk) - 1;
+      mk &= mk - 1;
+      if (q < B.cap) {
+        B.cand[q] = dp_cand_at(Ln.s, a[k] + i);
+        B.cand_lane[q] = (uint32_t)lane;
+      }
+      q++;
+    }
+  }
+}
+
+// The candidate range [lo, hi) of column c (the exclusive scan of the chunk
+// counts, read at the column's first chunks).
+__device__ inline void dpb_range(const DpBatch& B, int c, uint64_t* lo, uint64_t* hi) {
+  *lo = B.cnt[B.chunk0[c]];
+  *hi = B.cnt[B.chunk0[c + 1]];
+}
+
+__global__ void k_dpb_succ(DpBatch B) {
+  uint64_t K = B.cnt[B.chunks];
+  if (K > B.cap) return;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < K; i += (uint64_t)gridDim.x * blockDim.x) {
+    int c = (int)B.cand_lane[i];
+    uint64_t lo, hi;
+    dpb_range(B, c, &lo, &hi);
+    DpCand cd = B.cand[i];
+    uint64_t target = cd.pos + 9 + (cd.plen_mode >> 8);
+    uint64_t a = i + 1, z = hi;
+    while (a < z) {
+      uint64_t mid = (a + z) >> 1;
+      if (B.cand[mid].pos < target) a = mid + 1; else z = mid;
+    }
+    B.nodes[i].succ = (a < hi && B.cand[a].pos == target) ? (uint32_t)(a - lo) : kNone;  // column-relative
+  }
+}
+
+// The values a column's frames hold (its valid count or n).
+__device__ inline uint64_t dpb_total(const DpBatch& B, int c) {
+  return B.lanes[c].L.has_validity ? B.out[c].nvalid : B.lanes[c].L.logical_n;
+}
+
+// One CTA per column: k_dp_marks over the column's candidates.  nmarked = 0
+// and status 1 when the chain cannot be resolved; status 3 for a column with
+// no valid value (left to the single-column path, which zero-fills it).
+__global__ void __launch_bounds__(kChainThreads) k_dpb_marks(DpBatch B) {
+  extern __shared__ __align__(16) uint8_t dsm[];
+  __shared__ uint64_t s_warp[33];
+  const int c = blockIdx.x, tid = threadIdx.x;
+  const DpBLane& Ln = B.lanes[c];
+  uint64_t Ktot = B.cnt[B.chunks];
+  uint64_t lo, hi;
+  dpb_range(B, c, &lo, &hi);
+  uint64_t n_total = dpb_total(B, c);
+  bool good = Ktot <= B.cap && n_total > 0 && hi > lo && B.cand[lo].pos == Ln.L.fstart;
+  if (!good) {
+    if (tid == 0) {
+      B.out[c].nmarked = 0;
+      B.out[c].status = n_total == 0 && Ktot <= B.cap ? 3u : 1u;
+    }
+    return;
+  }
+  const uint32_t M = (uint32_t)(hi - lo);
+  uint32_t *J0, *J1;
+  uint8_t* marks;
+  if ((uint64_t)M * 9 + 16 <= kDpChainSmem) {
+    J0 = reinterpret_cast<uint32_t*>(dsm);
+    J1 = J0 + M;
+    marks = reinterpret_cast<uint8_t*>(J1 + M);
+  } else {
+    J0 = B.gJ + 2 * lo;
+    J1 = J0 + M;
+    marks = B.gmarks + lo;
+  }
+  for (uint32_t i = tid; i < M; i += kChainThreads) {
+    J0[i] = B.nodes[lo + i].succ;
+    marks[i] = i == 0;
+  }
+  __syncthreads();
+  uint32_t rounds = 1;
+  while ((1ull << rounds) <= M) rounds++;
+  for (uint32_t r = 0; r < rounds; r++) {
+    for (uint32_t i = tid; i < M; i += kChainThreads) {
+      uint32_t j = J0[i];
+      if (j != kNone && marks[i]) marks[j] = 1;
+      J1[i] = j == kNone ? kNone : J0[j];
+    }
+    __syncthreads();
+    uint32_t* t = J0;
+    J0 = J1;
+    J1 = t;
+  }
+  uint64_t carry = 0;
+  for (uint32_t t0 = 0; t0 < M; t0 += kChainThreads) {
+    uint32_t i = t0 + tid;
+    bool f = i < M && marks[i];
+    uint64_t tot;
+    uint64_t x = block_excl_scan<ScanSum>(f ? 1ull : 0ull, s_warp, &tot);
+    if (f) B.flist[lo + carry + x] = i;  // the chain's candidates (column-relative), in order
+    carry += tot;
+  }
+  if (tid == 0) {
+    B.out[c].nmarked = carry;
+    B.out[c].status = 0;
+  }
+}
+
+// One CTA: exclusive scans over the columns (mode 0: frame bases from the
+// chain lengths; mode 1: item, prepass and list bases from the layouts).
+__global__ void __launch_bounds__(1024) k_dpb_lane_scan(DpBatch B, int mode) {
+  __shared__ uint64_t s_warp[33];
+  uint64_t c0 = 0, c1 = 0, c2 = 0, any = 0;
+  for (int b = 0; b < B.nlanes; b += 1024) {
+    int c = b + threadIdx.x;
+    bool in = c < B.nlanes;
+    DpBLaneOut o;
+    memset(&o, 0, sizeof(o));
+    if (in) o = B.out[c];
+    if (mode == 0) {
+      uint64_t t;
+      uint64_t x = block_excl_scan<ScanSum>(in ? o.nmarked : 0ull, s_warp, &t);
+      if (in) B.out[c].fbase = c0 + x;
+      c0 += t;
+    } else {
+      bool ok = in && o.status == 0;
+      uint64_t t0, t1, t2;
+      uint64_t x0 = block_excl_scan<ScanSum>(ok ? (uint64_t)o.nmain : 0ull, s_warp, &t0);
+      uint64_t x1 = block_excl_scan<ScanSum>(ok ? (uint64_t)o.npre : 0ull, s_warp, &t1);
+      uint64_t x2 = block_excl_scan<ScanSum>(ok ? (uint64_t)o.nlist : 0ull, s_warp, &t2);
+      if (in) {
+        B.out[c].main_base = c0 + x0;
+        B.out[c].pre_base = c1 + x1;
+        B.out[c].list_base = c2 + x2;
+      }
+      any |= (uint64_t)__syncthreads_or(ok && o.need_scan);
+      c0 += t0;
+      c1 += t1;
+      c2 += t2;
+    }
+  }
+  if (threadIdx.x == 0) {
+    if (mode == 0) {
+      B.tot->nframes = c0;
+    } else {
+      B.tot->nmain = c0;
+      B.tot->npre = c1;
+      B.tot->nlist = c2;
+      B.tot->need_scan = (uint32_t)any;
+    }
+  }
+}
+
+// Warp items of every chain frame (dp_frame_items), across the GPU: slot j of
+// column c's candidate range holds its j-th chain frame.
+__global__ void k_dpb_items(DpBatch B) {
+  uint64_t K = B.cnt[B.chunks];
+  if (K > B.cap) return;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < K; j += (uint64_t)gridDim.x * blockDim.x) {
+    int c = (int)B.cand_lane[j];
+    uint64_t lo = B.cnt[B.chunk0[c]];
+    if (j - lo >= B.out[c].nmarked) continue;
+    const DpBLane& Ln = B.lanes[c];
+    uint64_t i = lo + B.flist[j];
+    DpCand cd = B.cand[i];
+    FrameItems it = dp_frame_items(Ln.s + cd.pos + 9, cd.n, cd.plen_mode >> 8, cd.plen_mode & 0xFF, Ln.L.plog2);
+    DpNode d;
+    d.succ = (uint32_t)(i - lo);
+    d.nmain = it.nmain;
+    d.npre = it.npre;
+    d.flags = (it.list ? 1u : 0u) | (it.scan ? 2u : 0u) | (it.dict ? 4u : 0u);
+    d.ent = it.ent;
+    B.nodes[j] = d;
+  }
+}
+
+// One CTA per column: k_dp_layout into the batch's frame table (dense, at the
+// column's frame base; payload offsets absolute).  A column that fails, or
+// whose frames need entropy areas (status 2: the single-column path decodes
+// it), keeps its frame slots as empty RAW frames.
+__global__ void __launch_bounds__(kChainThreads) k_dpb_layout(DpBatch B) {
+  __shared__ uint64_t s_warp[33];
+  const int c = blockIdx.x, tid = threadIdx.x;
+  const DpBLane& Ln = B.lanes[c];
+  DpBLaneOut& O = B.out[c];
+  const uint64_t F = O.nmarked, fb = O.fbase;
+  uint64_t lo = B.cnt[B.chunk0[c]];
+  const uint64_t n_total = dpb_total(B, c);
+  uint64_t carry_f = 0, carry_v = 0, carry_main = 0, carry_pre = 0, carry_list = 0, carry_ent = 0;
+  bool scan = false, dict = false, stop = false, fail = O.status != 0;
+  for (uint64_t t0 = 0; t0 < F && !stop && !fail; t0 += kChainThreads) {
+    uint64_t j = t0 + tid;
+    bool have = j < F;
+    DpCand cd;
+    cd.pos = 0;
+    cd.n = 0;
+    cd.plen_mode = 0;
+    DpNode nd;
+    memset(&nd, 0, sizeof(nd));
+    if (have) {
+      nd = B.nodes[lo + j];
+      cd = B.cand[lo + nd.succ];
+    }
+    uint64_t vx = block_excl_scan<ScanSum>(have ? (uint64_t)cd.n : 0ull, s_warp, nullptr);
+    uint64_t voff = carry_v + vx;
+    bool keep = have && voff < n_total;
+    bool list = keep && (nd.flags & 1);
+    bool last = keep && voff + cd.n >= n_total;
+    stop = __syncthreads_or(last) != 0;
+    fail = (__syncthreads_or(last && voff + cd.n > n_total) != 0) || fail;
+    uint64_t tf, tv, tp, tl, te;
+    uint64_t fx = block_excl_scan<ScanSum>(keep ? 1ull : 0ull, s_warp, &tf);
+    block_excl_scan<ScanSum>(keep ? (uint64_t)cd.n : 0ull, s_warp, &tv);
+    uint64_t packed = keep ? ((uint64_t)nd.npre << 32 | nd.nmain) : 0ull;
+    uint64_t px = block_excl_scan<ScanSum>(packed, s_warp, &tp);
+    uint64_t lx = block_excl_scan<ScanSum>(list ? 1ull : 0ull, s_warp, &tl);
+    uint64_t ex = block_excl_scan<ScanSum>(keep ? nd.ent : 0ull, s_warp, &te);
+    if (keep) {
+      uint64_t f = carry_f + fx;
+      FrameDesc d;
+      d.payload_off = (uint64_t)(uintptr_t)(Ln.s + cd.pos + 9);
+      d.value_off = voff;
+      d.n = cd.n;
+      d.plen = cd.plen_mode >> 8;
+      d.mode = cd.plen_mode & 0xFF;
+      d.aux = 0;
+      B.frames[fb + f] = d;
+      B.frame_col[fb + f] = (uint32_t)c;
+      B.ftmp[lo + f] = make_uint4((uint32_t)(carry_pre + (px >> 32)), nd.npre,
+                                  (uint32_t)(carry_main + (px & 0xFFFFFFFFull)), nd.nmain);
+      B.flist[lo + f] = list ? (uint32_t)(carry_list + lx) : kNone;
+    }
+    scan = (__syncthreads_or(keep && (nd.flags & 2)) != 0) || scan;
+    dict = (__syncthreads_or(keep && (nd.flags & 4)) != 0) || dict;
+    carry_f += tf;
+    carry_v += tv;
+    carry_main += tp & 0xFFFFFFFFull;
+    carry_pre += tp >> 32;
+    carry_list += tl;
+    carry_ent += te;
+  }
+  uint32_t status = O.status;
+  if (status == 0 && (fail || !stop || carry_v != n_total)) status = 1;
+  if (status == 0 && carry_ent) status = 2;
+  const uint64_t kept = status == 0 ? carry_f : 0;
+  // the slots past the kept frames (all of them for a column left out) hold
+  // empty frames
+  for (uint64_t f = kept + tid; f < F; f += kChainThreads) {
+    FrameDesc d;
+    d.payload_off = (uint64_t)(uintptr_t)Ln.s;
+    d.value_off = 0;
+    d.n = 0;
+    d.plen = 0;
+    d.mode = M_RAW;
+    d.aux = 0;
+    B.frames[fb + f] = d;
+    B.frame_col[fb + f] = (uint32_t)c;
+    B.frame_pre[fb + f] = make_uint2(0, 0);
+  }
+  if (tid == 0) {
+    O.status = status;
+    O.nframes = (uint32_t)kept;
+    O.nmain = status == 0 ? (uint32_t)carry_main : 0u;
+    O.npre = status == 0 ? (uint32_t)carry_pre : 0u;
+    O.nlist = status == 0 ? (uint32_t)carry_list : 0u;
+    O.need_scan = scan;
+    O.any_dict = dict;
+    O.ent = carry_ent;
+  }
+}
+
+// Item lists of the batch: one warp per kept chain frame.
+__global__ void k_dpb_expand(DpBatch B) {
+  uint64_t K = B.cnt[B.chunks];
+  if (K > B.cap) return;
+  uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  int l = threadIdx.x & 31;
+  for (uint64_t j = warp; j < K; j += nwarps) {
+    int c = (int)B.cand_lane[j];
+    const DpBLaneOut& O = B.out[c];
+    uint64_t lo = B.cnt[B.chunk0[c]], f = j - lo;
+    if (O.status != 0 || f >= O.nframes) continue;
+    uint64_t gf = O.fbase + f;
+    uint4 t = B.ftmp[j];
+    uint64_t pre0 = O.pre_base + t.x, main0 = O.main_base + t.z;
+    if (l == 0) {
+      B.frame_pre[gf] = make_uint2((uint32_t)pre0, t.y);
+      uint32_t li = B.flist[j];
+      if (li != kNone) B.list[O.list_base + li] = (uint32_t)gf;
+    }
+    for (uint32_t k = l; k < t.w; k += 32) B.main_items[main0 + k] = ItemRef{(uint32_t)gf, k};
+    for (uint32_t k = l; k < t.y; k += 32) B.pre_items[pre0 + k] = ItemRef{(uint32_t)gf, k};
+  }
+}
+
+std::atomic<unsigned long long> g_bmarks_attr{0};
+
+}  // namespace
+
+uint64_t dp_batch_slot_bytes(uint64_t chunks) { return chunks * kDpSlots * sizeof(DpCand); }
+
+void launch_dp_batch_heads(const uint8_t* const* srcs, const uint64_t* lens, int n, DpHead* H, cudaStream_t st) {
+  if (n <= 0) return;
+  k_dpb_heads<<<(n + 127) / 128, 128, 0, st>>>(srcs, lens, n, H);
+  count_launches(1);
+}
+
+void launch_dp_batch_read(const DpBatch& B, uint64_t* tile_tmp, cudaStream_t st) {
+  once_per_device(g_bmarks_attr, [] {
+    cudaFuncSetAttribute(k_dpb_marks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDpChainSmem);
+  });
+  unsigned gw = (unsigned)qmin((B.words + 255) / 256, 148ull * 8);
+  if (gw == 0) gw = 1;
+  k_dpb_bitmap<<<gw, 256, 0, st>>>(B, B.word0);
+  cudaMemsetAsync(B.ranks + B.words, 0, 8, st);
+  launch_scan_sum(B.ranks, B.ranks, B.words + 1, tile_tmp, nullptr, st);
+  k_dpb_lane_base<<<(B.nlanes + 127) / 128, 128, 0, st>>>(B);
+  k_dpb_ranks<<<gw, 256, 0, st>>>(B, B.word0);
+  k_dpb_select<<<gw, 256, 0, st>>>(B, B.word0);
+  if (B.chunks) k_dpb_cand_scan<<<(unsigned)B.chunks, kDpThreads, 0, st>>>(B);
+  cudaMemsetAsync(B.cnt + B.chunks, 0, 8, st);
+  launch_scan_sum(B.cnt, B.cnt, B.chunks + 1, tile_tmp, nullptr, st);
+  if (B.chunks) k_dpb_cand_compact<<<(unsigned)B.chunks, kDpThreads, 0, st>>>(B);
+  unsigned gc = (unsigned)qmin((B.cap + 255) / 256, 148ull * 8);
+  k_dpb_succ<<<gc, 256, 0, st>>>(B);
+  k_dpb_marks<<<B.nlanes, kChainThreads, kDpChainSmem, st>>>(B);
+  k_dpb_lane_scan<<<1, 1024, 0, st>>>(B, 0);
+  k_dpb_items<<<gc, 256, 0, st>>>(B);
+  k_dpb_layout<<<B.nlanes, kChainThreads, 0, st>>>(B);
+  k_dpb_lane_scan<<<1, 1024, 0, st>>>(B, 1);
+  k_dpb_expand<<<gc, 256, 0, st>>>(B);
+  count_launches(14);
+}
 }  // namespace qb

@@ -197,7 +197,7 @@ inline int plain_code(int ext) {
 enum Slot {
   S_IN, S_BM, S_RANK, S_LANE, S_GROW, S_FRAMES, S_NB, S_SIZES, S_TILE, S_SCRATCH, S_OUT, S_VTMP, S_VBLOB,
   S_MISC, S_LIMBS, S_LIMBOUT, S_SRC, S_DSCR, S_ERR, S_OUTVALS, S_DFRAMES, S_DBM, S_DRANK, S_DAUX, S_SUBST, S_FMST,
-  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_ENT, S_ENTREC, S_DPMISC, S_DPCAND, S_DPJ, S_DPRUNS, S_COUNT
+  S_SMP16, S_WINBITS, S_DSEL, S_DITEMS, S_PRE, S_ENT, S_ENTREC, S_DPMISC, S_DPCAND, S_DPJ, S_DPRUNS, S_BATCH, S_BSCR, S_BHOST, S_COUNT
 };
 
 struct QuoinCtx {
@@ -1285,6 +1285,7 @@ static_assert(sizeof(DpHead) <= kDpMiscOff && sizeof(DpMisc) <= 512, "reader res
 // lane still over capacity after the exact count).
 std::atomic<uint64_t> g_reads_device{0}, g_reads_host{0}, g_reads_host_reason{0};
 std::atomic<uint64_t> g_last_ncand{0}, g_last_attempts{0};  // the last device read: candidates, table rounds
+std::atomic<uint64_t> g_batch_columns{0};  // columns decoded by the batched path
 
 // Candidate capacity of a lane whose frames span `bytes`: encoder streams
 // hold far fewer frames (one per 32,768 values for adaptive blocks); a lane
@@ -1493,6 +1494,226 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
                           c->p<uint64_t>(S_DSEL), dvmin, ditems, d_src, d_out, d_valid_out);
   }
   return decode_device_via_host(c, st, d_src, len, d_out, out_cap_bytes, d_valid_out, wire_out, n_out, 3);
+}
+
+// ---------------------------------------------------------------------------
+// Batched decode of device streams (qb_dparse.cu batch reader + one launch of
+// each block-decoder kernel over all columns).
+// ---------------------------------------------------------------------------
+struct BumpAlloc {  // carves 256-byte aligned pieces out of one buffer
+  uint64_t off = 0;
+  uint64_t take(uint64_t bytes) {
+    uint64_t o = off;
+    off += (bytes + 255) & ~255ull;
+    return o;
+  }
+};
+
+int decode_queue(QuoinCtx* c, cudaStream_t st, QuoinB200DeviceDecodeJob* jobs, size_t nj) {
+  for (size_t i = 0; i < nj; i++) {
+    jobs[i].wire = 0;
+    jobs[i].n = 0;
+    jobs[i].status = QUOIN_ERR_NULL;
+  }
+  if (nj == 0) return QUOIN_OK;
+  std::vector<char> single(nj, 1);  // decoded one by one after the batch
+  // headers of every stream
+  {
+    BumpAlloc ba;
+    uint64_t o_src = ba.take(nj * 8), o_len = ba.take(nj * 8), o_h = ba.take(nj * sizeof(DpHead));
+    CK(c->ensure(S_BHOST, ba.off));
+    std::vector<uint64_t> hv(2 * nj);
+    for (size_t i = 0; i < nj; i++) {
+      hv[i] = (uint64_t)(uintptr_t)jobs[i].d_src;
+      hv[nj + i] = jobs[i].d_src ? jobs[i].src_len : 0;
+    }
+    uint8_t* base = c->p<uint8_t>(S_BHOST);
+    CK(cudaMemcpyAsync(base + o_src, hv.data(), nj * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(base + o_len, hv.data() + nj, nj * 8, cudaMemcpyHostToDevice, st));
+    launch_dp_batch_heads(reinterpret_cast<const uint8_t* const*>(base + o_src),
+                          reinterpret_cast<const uint64_t*>(base + o_len), (int)nj,
+                          reinterpret_cast<DpHead*>(base + o_h), st);
+    std::vector<DpHead> H(nj);
+    CK(cudaMemcpyAsync(H.data(), base + o_h, nj * sizeof(DpHead), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // the columns the batch takes, in job order
+    std::vector<size_t> take;
+    for (size_t i = 0; i < nj; i++) {
+      const QuoinB200DeviceDecodeJob& J = jobs[i];
+      const DpHead& h = H[i];
+      if (!J.d_src || !J.d_values_out || h.kind || h.decimal || h.n == 0) continue;
+      if (h.has_validity && h.vtag != 0) continue;
+      uint32_t w = native_width((int)h.wire);
+      if (h.n * (uint64_t)w > J.values_cap_bytes || ((uintptr_t)J.d_values_out % w) != 0) continue;
+      take.push_back(i);
+    }
+    if (!take.empty()) {
+      const int nl = (int)take.size();
+      std::vector<DpBLane> lanes(nl);
+      std::vector<uint64_t> word0(nl + 1), chunk0(nl + 1);
+      uint64_t words = 0, chunks = 0, sels = 0, cap = 0, item_cap = 0, scr = 0;
+      for (int k = 0; k < nl; k++) {
+        const QuoinB200DeviceDecodeJob& J = jobs[take[k]];
+        const DpHead& h = H[take[k]];
+        DpBLane& B = lanes[k];
+        B.s = J.d_src;
+        B.buf_len = J.src_len;
+        B.L = h.lanes[0];
+        B.vblob_off = h.vblob_off;
+        B.nw = h.has_validity ? (h.n + 31) / 32 : 0;
+        B.word0 = word0[k] = words;
+        words += B.nw + 1;
+        B.sel0 = sels;
+        sels += h.n / 512 + 2;
+        uint64_t fb = B.L.base + B.L.len - B.L.fstart;
+        B.chunk0 = chunk0[k] = chunks;
+        chunks += dp_chunks(fb);
+        uint64_t cc = dp_cap(fb);
+        cap += cc;
+        item_cap += B.L.logical_n / 512 + fb / 512 + 2 * cc + 16;
+        scr += h.n;
+        B.valid_out = h.has_validity ? J.d_validity_out : nullptr;
+      }
+      word0[nl] = words;
+      chunk0[nl] = chunks;
+      BumpAlloc a;
+      uint64_t o_lanes = a.take(nl * sizeof(DpBLane)), o_w0 = a.take((nl + 1) * 8), o_c0 = a.take((nl + 1) * 8),
+               o_out = a.take(nl * sizeof(DpBLaneOut)), o_tot = a.take(sizeof(DpBTotals)),
+               o_bm = a.take(words * 4), o_rk = a.take((words + 1) * 8), o_rb = a.take(nl * 8),
+               o_sel = a.take(sels * 8), o_cnt = a.take((chunks + 1) * 8), o_slots = a.take(dp_batch_slot_bytes(chunks)),
+               o_cand = a.take(cap * sizeof(DpCand)), o_cl = a.take(cap * 4), o_nodes = a.take(cap * sizeof(DpNode)),
+               o_J = a.take(cap * 8), o_mk = a.take(cap), o_ft = a.take(cap * 16), o_fl = a.take(cap * 4),
+               o_fr = a.take((cap + 1) * sizeof(FrameDesc)), o_fc = a.take((cap + 1) * 4),
+               o_fp = a.take((cap + 1) * 8), o_mi = a.take(item_cap * 8), o_pi = a.take(item_cap * 8),
+               o_li = a.take((cap + 1) * 4), o_cols = a.take(nl * sizeof(BatchCol)), o_err = a.take(64);
+      CK(c->ensure(S_BATCH, a.off));
+      uint8_t* bb = c->p<uint8_t>(S_BATCH);
+      CK(cudaMemcpyAsync(bb + o_lanes, lanes.data(), nl * sizeof(DpBLane), cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(bb + o_w0, word0.data(), (nl + 1) * 8, cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(bb + o_c0, chunk0.data(), (nl + 1) * 8, cudaMemcpyHostToDevice, st));
+      DpBatch B;
+      B.lanes = reinterpret_cast<DpBLane*>(bb + o_lanes);
+      B.word0 = reinterpret_cast<const uint64_t*>(bb + o_w0);
+      B.chunk0 = reinterpret_cast<const uint64_t*>(bb + o_c0);
+      B.out = reinterpret_cast<DpBLaneOut*>(bb + o_out);
+      B.tot = reinterpret_cast<DpBTotals*>(bb + o_tot);
+      B.nlanes = nl;
+      B.bm32 = reinterpret_cast<uint32_t*>(bb + o_bm);
+      B.ranks = reinterpret_cast<uint64_t*>(bb + o_rk);
+      B.rbase = reinterpret_cast<uint64_t*>(bb + o_rb);
+      B.sel = reinterpret_cast<uint64_t*>(bb + o_sel);
+      B.cnt = reinterpret_cast<uint64_t*>(bb + o_cnt);
+      B.slots = reinterpret_cast<DpCand*>(bb + o_slots);
+      B.cand = reinterpret_cast<DpCand*>(bb + o_cand);
+      B.cand_lane = reinterpret_cast<uint32_t*>(bb + o_cl);
+      B.nodes = reinterpret_cast<DpNode*>(bb + o_nodes);
+      B.gJ = reinterpret_cast<uint32_t*>(bb + o_J);
+      B.gmarks = bb + o_mk;
+      B.ftmp = reinterpret_cast<uint4*>(bb + o_ft);
+      B.flist = reinterpret_cast<uint32_t*>(bb + o_fl);
+      B.cap = cap;
+      B.words = words;
+      B.chunks = chunks;
+      B.frames = reinterpret_cast<FrameDesc*>(bb + o_fr);
+      B.frame_col = reinterpret_cast<uint32_t*>(bb + o_fc);
+      B.frame_pre = reinterpret_cast<uint2*>(bb + o_fp);
+      B.main_items = reinterpret_cast<ItemRef*>(bb + o_mi);
+      B.pre_items = reinterpret_cast<ItemRef*>(bb + o_pi);
+      B.list = reinterpret_cast<uint32_t*>(bb + o_li);
+      B.item_cap = item_cap;
+      CK(c->ensure(S_TILE, (scan_tile_count((words > chunks ? words : chunks) + 1) + 16) * 8));
+      {
+        TimedRegion tr(T_READ, st);
+        CK(cudaMemsetAsync(B.out, 0, nl * sizeof(DpBLaneOut), st));
+        launch_dp_batch_read(B, c->p<uint64_t>(S_TILE), st);
+      }
+      std::vector<DpBLaneOut> out(nl);
+      DpBTotals tot;
+      uint64_t ktot = 0;
+      CK(cudaMemcpyAsync(out.data(), B.out, nl * sizeof(DpBLaneOut), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(&tot, B.tot, sizeof(tot), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(&ktot, B.cnt + chunks, 8, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (ktot <= cap && tot.nmain <= item_cap && tot.npre <= item_cap) {
+        bool dict = false;
+        for (int k = 0; k < nl; k++) dict = dict || (out[k].status == 0 && out[k].any_dict);
+        if (dict) CK(c->ensure(S_BSCR, scr * 8 + 64));
+        std::vector<BatchCol> cols(nl);
+        uint64_t so = 0;
+        for (int k = 0; k < nl; k++) {
+          const DpHead& h = H[take[k]];
+          BatchCol& C = cols[k];
+          C = BatchCol{};
+          C.O.out = jobs[take[k]].d_values_out;
+          C.O.dtype = (int)h.wire;
+          C.O.bm32 = h.has_validity ? B.bm32 + lanes[k].word0 : nullptr;
+          C.O.wrank = B.ranks + lanes[k].word0;
+          C.O.sel = B.sel + lanes[k].sel0;
+          C.O.n = h.n;
+          C.O.nvalid = out[k].nvalid;
+          C.O.plog2 = h.lanes[0].plog2;
+          C.dtype = (int)h.wire;
+          C.scratch = dict ? c->p<uint64_t>(S_BSCR) + so : nullptr;
+          so += h.n;
+        }
+        CK(cudaMemcpyAsync(bb + o_cols, cols.data(), nl * sizeof(BatchCol), cudaMemcpyHostToDevice, st));
+        unsigned long long* d_err = reinterpret_cast<unsigned long long*>(bb + o_err);
+        CK(cudaMemsetAsync(d_err, 0xFF, 8, st));
+        CK(c->ensure(S_DAUX, decode_aux_bytes((int)(tot.nframes + 1))));
+        CK(c->ensure(S_PRE, (tot.npre + 1) * prepass_rec_bytes()));
+        ItemPlan P;
+        P.pre_items = B.pre_items;
+        P.npre = (uint32_t)tot.npre;
+        P.main_items = B.main_items;
+        P.nmain = (uint32_t)tot.nmain;
+        P.frame_pre = B.frame_pre;
+        P.list = B.list;
+        P.nlist = (uint32_t)tot.nlist;
+        P.need_scan = tot.need_scan != 0;
+        P.ent = nullptr;
+        BatchView bv{B.frame_col, reinterpret_cast<const BatchCol*>(bb + o_cols)};
+        DecodeOut none{};
+        {
+          TimedRegion tr(T_DECODE, st);
+          launch_decode_items(nullptr, B.frames, (int)tot.nframes, 0, none, P, c->p<void>(S_PRE), nullptr,
+                              c->p<void>(S_DAUX), d_err, st, &bv);
+        }
+        unsigned long long herr = 0;
+        CK(read_small(c, st, &herr, d_err, 8));
+        resolve_timing();
+        if (herr == ~0ull) {  // every batch column decoded: the others go one by one
+          for (int k = 0; k < nl; k++) {
+            if (out[k].status != 0) continue;
+            QuoinB200DeviceDecodeJob& J = jobs[take[k]];
+            J.wire = (int32_t)H[take[k]].wire;
+            J.n = H[take[k]].n;
+            J.status = QUOIN_OK;
+            single[take[k]] = 0;
+          }
+          g_batch_columns.fetch_add((uint64_t)nl);
+        }
+      }
+    }
+  }
+  // the columns left to the single-column path (and any failing batch)
+  int first = QUOIN_OK;
+  for (size_t i = 0; i < nj; i++) {
+    QuoinB200DeviceDecodeJob& J = jobs[i];
+    if (single[i]) {
+      if (!J.d_src || !J.d_values_out) {
+        J.status = QUOIN_ERR_NULL;
+      } else {
+        int32_t w = 0;
+        uint64_t n = 0;
+        J.status = decode_device(c, st, J.d_src, J.src_len, J.d_values_out, J.values_cap_bytes, J.d_validity_out,
+                                 &w, &n);
+        J.wire = w;
+        J.n = n;
+      }
+    }
+    if (J.status != QUOIN_OK && first == QUOIN_OK) first = J.status;
+  }
+  return first;
 }
 
 // Host-buffer compress of a typed column (wire dtype, native little-endian values).
@@ -1967,6 +2188,20 @@ int quoin_b200_decompress_indexed_device(QuoinCtx* ctx, const QuoinDecodeIndex* 
   }
 }
 
+int quoin_b200_decompress_queue_device(QuoinCtx* ctx, QuoinB200DeviceDecodeJob* jobs, size_t njobs, void* stream) {
+  if (!jobs && njobs) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = pick(ctx);
+    if (!c) return QUOIN_ERR_CUDA;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    return decode_queue(c, st, jobs, njobs);
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
 int quoin_b200_decompress_column_device(QuoinCtx* ctx, const uint8_t* d_src, size_t src_len, void* d_values_out,
                                         size_t values_cap_bytes, uint8_t* d_validity_out, int32_t* wire_out,
                                         uint64_t* n_out, void* stream) {
@@ -1985,13 +2220,14 @@ int quoin_b200_decompress_column_device(QuoinCtx* ctx, const uint8_t* d_src, siz
   }
 }
 
-void quoin_b200_reader_stats(uint64_t out[5]) {
+void quoin_b200_reader_stats(uint64_t out[6]) {
   if (!out) return;
   out[0] = g_reads_device.load();
   out[1] = g_reads_host.load();
   out[2] = g_reads_host_reason.load();
   out[3] = g_last_ncand.load();
   out[4] = g_last_attempts.load();
+  out[5] = g_batch_columns.load();
 }
 
 void quoin_b200_mode_win_counts(uint64_t out[64]) {

@@ -49,6 +49,19 @@ struct DecodeOut {
 };
 void launch_decode_frames(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
                           uint64_t* scratch, void* aux, unsigned long long* err, cudaStream_t st);
+// A batch of columns decoded by one launch per kernel class: frame f belongs
+// to column frame_col[f], whose output, lane dtype and decode scratch replace
+// the launch's own (payload offsets are then absolute device addresses, with
+// a null stream base).
+struct BatchCol {
+  DecodeOut O;
+  int dtype, pad;
+  uint64_t* scratch;
+};
+struct BatchView {
+  const uint32_t* frame_col;
+  const BatchCol* cols;
+};
 // Warp-item decode of one lane (every item covers at most 512 values or 512
 // XORZ payload bytes).  The host builds the tables from the frame table:
 // pre_items / main_items name (frame, item index within the frame);
@@ -72,7 +85,7 @@ struct ItemPlan {
 uint64_t prepass_rec_bytes();
 void launch_decode_items(const uint8_t* stream, const FrameDesc* frames, int nf, int dtype, const DecodeOut& out,
                          const ItemPlan& plan, void* pre, uint64_t* scratch, void* aux, unsigned long long* err,
-                         cudaStream_t st);
+                         cudaStream_t st, const BatchView* batch = nullptr);
 // ---- device stream reader (qb_dparse.cu) ----
 // One lane stream of a column: the stream itself, or a decimal limb's.
 struct DpLane {
@@ -144,6 +157,68 @@ void launch_dp_candidates(const uint8_t* s, uint64_t buf_len, const DpHead* H, i
 void launch_dp_chain(const uint8_t* s, const DpHead* H, int lane, const uint64_t* d_nvalid, const DpCand* cand,
                      const uint64_t* d_ncand, uint64_t cap, DpNode* nodes, uint32_t* gJ, uint8_t* gmarks,
                      uint64_t* d_ctl, const DpTables& T, DpLaneOut* out, cudaStream_t st);
+
+// ---- batches of device streams (qb_dparse.cu) ----
+// One column of a batch read by one launch per kernel class: its stream and
+// header facts (host-filled from the parsed headers), and where its bitmap,
+// ranks, select table, candidate chunks and decode scratch sit in the
+// batch's arrays.
+struct DpBLane {
+  const uint8_t* s;
+  uint64_t buf_len;
+  DpLane L;               // the lane (base 0: the column's own stream)
+  uint64_t vblob_off;     // the RAW validity bitmap's bytes, when L.has_validity
+  uint64_t word0, nw;     // its bitmap words (nw, then one zero word)
+  uint64_t sel0;          // its select table entries
+  uint64_t chunk0;        // its first candidate chunk (the batch has one more entry: the total)
+  uint8_t* valid_out;     // the caller's bitmap, or null
+};
+// Device-written per column.
+struct DpBLaneOut {
+  uint64_t nvalid, nmarked, fbase, main_base, pre_base, list_base, ent;
+  uint32_t status, nframes, nmain, npre, nlist, need_scan, any_dict, pad;
+};
+struct DpBTotals {
+  uint64_t nframes, nmain, npre, nlist;
+  uint32_t need_scan, pad;
+};
+// The batch reader's arrays (device).  words = sum of (nw + 1); chunks =
+// lanes[nlanes - 1].chunk0's total; cap = candidate capacity.
+struct DpBatch {
+  DpBLane* lanes;
+  const uint64_t* chunk0;  // nlanes + 1 chunk offsets (a copy of lanes[].chunk0 plus the total)
+  const uint64_t* word0;   // nlanes + 1 word offsets (a copy of lanes[].word0 plus the total)
+  DpBLaneOut* out;
+  DpBTotals* tot;
+  int nlanes;
+  uint32_t* bm32;        // words
+  uint64_t* ranks;       // words + 1
+  uint64_t* rbase;       // nlanes
+  uint64_t* sel;         // select tables
+  uint64_t* cnt;         // chunks + 1
+  DpCand* slots;         // chunks * kDpSlots (dp_batch_slot_bytes)
+  DpCand* cand;          // cap
+  uint32_t* cand_lane;   // cap
+  DpNode* nodes;         // cap
+  uint32_t* gJ;          // 2 * cap
+  uint8_t* gmarks;       // cap
+  uint4* ftmp;           // cap (per chain frame: pre offset, pre count, main offset, main count)
+  uint32_t* flist;       // cap (per chain frame: its index in the column's list, or ~0)
+  uint64_t cap, words, chunks;
+  FrameDesc* frames;     // cap
+  uint32_t* frame_col;   // cap
+  uint2* frame_pre;      // cap
+  ItemRef* main_items;   // item capacity
+  ItemRef* pre_items;    // item capacity
+  uint32_t* list;        // cap
+  uint64_t item_cap;
+};
+uint64_t dp_batch_slot_bytes(uint64_t chunks);
+// Headers of n streams (srcs[i], lens[i]) into H[i].
+void launch_dp_batch_heads(const uint8_t* const* srcs, const uint64_t* lens, int n, DpHead* H, cudaStream_t st);
+// Validity, candidates, chains and item tables of every column of the batch
+// (tile_tmp holds scan_tile_count(max(words + 1, chunks + 1)) + 16 entries).
+void launch_dp_batch_read(const DpBatch& B, uint64_t* tile_tmp, cudaStream_t st);
 
 // sel[m] = position of the (512*m)-th valid value, m < ceil(nvalid / 512).
 void launch_select_table(const uint8_t* bm, uint64_t n, const uint64_t* word_rank, uint64_t nvalid, uint64_t* sel,

@@ -64,7 +64,7 @@ def device_decode(qb, stream, cap_bytes, offset=0, ctx=None):
 
 
 def reader_stats(qb):
-    out = (ctypes.c_uint64 * 5)()
+    out = (ctypes.c_uint64 * 6)()
     qb.lib.quoin_b200_reader_stats(out)
     return out[0], out[1]
 
