@@ -624,16 +624,11 @@ def run_gpu_batched(args, rank, world, local):
                     ("n", S), ("d_values", P), ("d_validity", P), ("d_dst", P), ("dst_cap", S), ("out_len", S),
                     ("status", ctypes.c_int32)]
 
-    class DecompressJob(ctypes.Structure):
-        _fields_ = [("idx", P), ("d_src", P), ("d_values_out", P), ("d_validity_out", P),
-                    ("status", ctypes.c_int32)]
-
     L.quoin_b200_batch_create.restype = P
     L.quoin_b200_batch_create.argtypes = [ctypes.c_int]
     L.quoin_b200_batch_free.argtypes = [P]
     L.quoin_b200_compress_batch_device.argtypes = [P, ctypes.POINTER(CompressJob), S,
                                                    ctypes.POINTER(Q._QuoinConfig)]
-    L.quoin_b200_decompress_batch_device.argtypes = [P, ctypes.POINTER(DecompressJob), S]
     cfg = Q._QuoinConfig(int(Q.Level.FAST), 0, 16, 0)
     cols = synth.mixed_columns(args.columns, args.max_len)
     ctx = P(L.quoin_ctx_create(0))
@@ -656,22 +651,26 @@ def run_gpu_batched(args, rank, world, local):
                                c["db"].data_ptr() if c["db"] is not None else None, c["dd"].data_ptr(), c["cap"],
                                0, 0)
     torch.cuda.synchronize()
-    # first pass: batched compress, then indices, bit-exact round trip
+    # first pass: batched compress, then the batched device decode, bit-exact
+    # round trip
     if L.quoin_b200_compress_batch_device(batch, cjobs, len(gc), ctypes.byref(cfg)):
         raise Q.Error(next(cjobs[j].status for j in range(len(gc)) if cjobs[j].status))
+
+    class QueueJob(ctypes.Structure):
+        _fields_ = [("d_src", P), ("src_len", S), ("d_values_out", P), ("values_cap_bytes", S),
+                    ("d_validity_out", P), ("wire", ctypes.c_int32), ("n", ctypes.c_uint64),
+                    ("status", ctypes.c_int32)]
+
+    L.quoin_b200_decompress_queue_device.argtypes = [P, ctypes.POINTER(QueueJob), S, P]
     stream_bytes = 0
-    djobs = (DecompressJob * len(gc))()
+    qjobs = (QueueJob * len(gc))()
     for j, c in enumerate(gc):
         c["len"] = cjobs[j].out_len
         stream_bytes += c["len"]
-        hs = c["dd"][: c["len"]].cpu().numpy().tobytes()
-        idx = P()
-        if L.quoin_b200_index_create(ctx, hs, len(hs), ctypes.byref(idx)):
-            raise Q.Error(-14)
-        c["idx"] = idx
-        djobs[j] = DecompressJob(idx, c["dd"].data_ptr(), c["dout"].data_ptr(), c["dvb"].data_ptr(), 0)
-    if L.quoin_b200_decompress_batch_device(batch, djobs, len(gc)):
-        raise Q.Error(-14)
+        qjobs[j] = QueueJob(c["dd"].data_ptr(), c["len"], c["dout"].data_ptr(), c["dout"].numel(),
+                            c["dvb"].data_ptr(), 0, 0, 0)
+    if L.quoin_b200_decompress_queue_device(ctx, qjobs, len(gc), None):
+        raise Q.Error(next(qjobs[j].status for j in range(len(gc)) if qjobs[j].status))
     torch.cuda.synchronize()
     bit_exact = True
     for c in gc:
@@ -680,8 +679,11 @@ def run_gpu_batched(args, rank, world, local):
             raw[~np.unpackbits(c["bm"], bitorder="little")[: c["n"]].astype(bool)] = 0
         if c["dout"][: raw.size].cpu().numpy().tobytes() != raw.tobytes():
             bit_exact = False
+    rstats = (ctypes.c_uint64 * 6)()
+    L.quoin_b200_reader_stats(rstats)
+    queue_cols0 = rstats[5]
 
-    def plain():
+    def plain_compress():
         for c in gc:
             olen = ctypes.c_size_t()
             rc = L.quoin_b200_compress_column_device(
@@ -689,17 +691,28 @@ def run_gpu_batched(args, rank, world, local):
                 c["sc"], c["pr"], ctypes.byref(cfg), P(c["dd"].data_ptr()), c["cap"], ctypes.byref(olen), None)
             if rc:
                 raise Q.Error(rc)
+
+    def plain_decompress():
         for c in gc:
-            rc = L.quoin_b200_decompress_indexed_device(ctx, c["idx"], P(c["dd"].data_ptr()), P(c["dout"].data_ptr()),
-                                                        P(c["dvb"].data_ptr()), None)
+            w, nn = ctypes.c_int32(), ctypes.c_uint64()
+            rc = L.quoin_b200_decompress_column_device(ctx, P(c["dd"].data_ptr()), c["len"], P(c["dout"].data_ptr()),
+                                                       c["dout"].numel(), P(c["dvb"].data_ptr()), ctypes.byref(w),
+                                                       ctypes.byref(nn), None)
             if rc:
                 raise Q.Error(rc)
+
+    def plain():
+        plain_compress()
+        plain_decompress()
+
+    def batched_decompress():
+        if L.quoin_b200_decompress_queue_device(ctx, qjobs, len(gc), None):
+            raise Q.Error(-14)
 
     def batched():
         if L.quoin_b200_compress_batch_device(batch, cjobs, len(gc), ctypes.byref(cfg)):
             raise Q.Error(-14)
-        if L.quoin_b200_decompress_batch_device(batch, djobs, len(gc)):
-            raise Q.Error(-14)
+        batched_decompress()
 
     stream = torch.cuda.current_stream(dev)
 
@@ -723,10 +736,12 @@ def run_gpu_batched(args, rank, world, local):
     batched_ms = timed(batched)
     clocks = sampler.stop()
     plain_ms = timed(plain)
+    dec_batched_ms = timed(batched_decompress)
+    dec_plain_ms = timed(plain_decompress)
+    L.quoin_b200_reader_stats(rstats)
+    queue_cols = (rstats[5] - queue_cols0) // max(2 * (args.warmup + args.steps), 1)
     value = whole_job_gbs(raw_bytes, world, args.steps, batched_ms / 1e3)
     plain_gbs = whole_job_gbs(raw_bytes, world, args.steps, plain_ms / 1e3)
-    for c in gc:
-        L.quoin_b200_index_free(c["idx"])
     L.quoin_b200_batch_free(batch)
     L.quoin_ctx_free(ctx)
     if rank == 0:
@@ -741,10 +756,15 @@ def run_gpu_batched(args, rank, world, local):
                        "uncompressed_bytes": raw_bytes, "workers": args.workers,
                        "parallelism": f"replicas x{world}"},
             "plain_gbs": round(plain_gbs, 3), "batched_over_plain": round(value / plain_gbs, 3) if plain_gbs else None,
+            "decode": {"batched_gbs": round(whole_job_gbs(raw_bytes, world, args.steps, dec_batched_ms / 1e3), 3),
+                       "plain_gbs": round(whole_job_gbs(raw_bytes, world, args.steps, dec_plain_ms / 1e3), 3),
+                       "columns_per_batched_call": int(queue_cols)},
             "ratio": round(raw_bytes / stream_bytes, 4), "bit_exact": bit_exact,
             "cpu_baseline": None, "clocks": clocks,
-            "note": "plain = per-column compress_column_device / decompress_indexed_device calls on one context; "
-                    "value = the same columns through the batch calls",
+            "note": "plain = per-column compress_column_device / decompress_column_device calls on one context; "
+                    "value = the same columns through the batch compress (a pool of contexts) and the batched "
+                    "device decode (quoin_b200_decompress_queue_device: one launch per kernel class for the "
+                    "batch)",
         }
         print(json.dumps(line), flush=True)
     if world > 1:

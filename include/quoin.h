@@ -349,8 +349,8 @@ typedef struct {
  * launches over a device-side table of (column, chunk) and (column,
  * candidate) work, and one launch of each block-decoder kernel decodes every
  * column's frames, each frame writing through its column's output.  Columns
- * this path leaves out (decimal containers, RLE validity blobs, entropy-coded
- * frames, damaged streams, all-null columns) are decoded one by one as by
+ * this path leaves out (entropy-coded frames, damaged streams, all-null
+ * columns) are decoded one by one as by
  * quoin_b200_decompress_column_device, so every column gets its own status.
  * Returns QUOIN_OK or the first failing job's status in job order. */
 int quoin_b200_decompress_queue_device(QuoinCtx *ctx, QuoinB200DeviceDecodeJob *jobs, size_t njobs,

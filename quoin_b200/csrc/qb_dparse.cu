@@ -215,12 +215,10 @@ __global__ void k_dp_bitmap(const uint8_t* __restrict__ s, const DpHead* __restr
 // odd byte after the last run is left unread, as the sequential reader
 // leaves it (the round's check covers only varints before the last run).
 constexpr int kRleThreads = 1024;
-__global__ void __launch_bounds__(kRleThreads) k_dp_rle_runs(const uint8_t* __restrict__ s, DpHead* __restrict__ H,
-                                                             uint64_t n, uint64_t* __restrict__ ends,
-                                                             uint64_t* __restrict__ nruns) {
-  __shared__ uint64_t s_warp[33];
-  const uint8_t* b = s + H->vblob_off;
-  const uint64_t blen = H->vblob_len;
+// The whole CTA: run ends of the RLE blob b[0 .. blen) covering n positions;
+// false when the sequential reader would reject it.
+__device__ bool dp_rle_runs(const uint8_t* __restrict__ b, uint64_t blen, uint64_t n, uint64_t* __restrict__ ends,
+                            uint64_t* __restrict__ nruns, uint64_t* s_warp) {
   const int tid = threadIdx.x;
   uint64_t carry_pos = 0, carry_k = 0;
   int64_t prev_term = -1;  // the last terminator before the round (blob offset)
@@ -289,11 +287,45 @@ __global__ void __launch_bounds__(kRleThreads) k_dp_rle_runs(const uint8_t* __re
     carry_k += rk;
     if ((int64_t)mt - 1 > prev_term) prev_term = (int64_t)mt - 1;
   }
-  if (tid == 0) {
-    if (n == 0) *nruns = 0;
-    if (bad || !done) H->kind = 1;  // the host reader reports the error
-  }
+  if (tid == 0 && n == 0) *nruns = 0;
+  return !bad && done;
 }
+
+__global__ void __launch_bounds__(kRleThreads) k_dp_rle_runs(const uint8_t* __restrict__ s, DpHead* __restrict__ H,
+                                                             uint64_t n, uint64_t* __restrict__ ends,
+                                                             uint64_t* __restrict__ nruns) {
+  __shared__ uint64_t s_warp[33];
+  bool ok = dp_rle_runs(s + H->vblob_off, H->vblob_len, n, ends, nruns, s_warp);
+  if (threadIdx.x == 0 && !ok) H->kind = 1;  // the host reader reports the error
+}
+
+// Bitmap word w (of an n-bit bitmap) from nr run ends: runs alternate null /
+// valid from a null run; the word's bits come from the runs overlapping
+// [32w, 32w + 32).
+__device__ uint32_t dp_rle_word(const uint64_t* __restrict__ ends, uint64_t nr, uint64_t n, uint64_t w) {
+  uint64_t lo = w * 32, hi = lo + 32;
+  uint32_t bits = 0;
+  if (!nr || lo >= n) return 0;
+  uint64_t a = 0, z = nr;  // first run whose end is above lo
+  while (a < z) {
+    uint64_t mid = (a + z) >> 1;
+    if (ends[mid] <= lo) a = mid + 1; else z = mid;
+  }
+  for (uint64_t r = a; r < nr; r++) {
+    uint64_t st = r ? ends[r - 1] : 0, en = ends[r];
+    if (st >= hi) break;
+    if (r & 1) {
+      uint64_t x = st > lo ? st : lo, y = en < hi ? en : hi;
+      if (y > x) {
+        uint32_t len = (uint32_t)(y - x), sh = (uint32_t)(x - lo);
+        bits |= (len == 32 ? 0xFFFFFFFFu : ((1u << len) - 1u)) << sh;
+      }
+    }
+  }
+  if (hi > n) bits &= (n - lo) >= 32 ? 0xFFFFFFFFu : ((1u << (uint32_t)(n - lo)) - 1u);
+  return bits;
+}
+
 
 // Bitmap word w from the run ends: runs alternate null / valid from a null
 // run; word w's bits come from the runs overlapping [32w, 32w + 32).
@@ -302,27 +334,7 @@ __global__ void k_dp_rle_fill(const DpHead* __restrict__ H, uint64_t n, const ui
                               uint64_t* __restrict__ cnt) {
   uint64_t nw = (n + 31) / 32, nr = H->kind ? 0 : *nruns_p;
   for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw + 1; w += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t lo = w * 32, hi = lo + 32;
-    uint32_t bits = 0;
-    if (w < nw && nr) {
-      uint64_t a = 0, z = nr;  // first run whose end is above lo
-      while (a < z) {
-        uint64_t mid = (a + z) >> 1;
-        if (ends[mid] <= lo) a = mid + 1; else z = mid;
-      }
-      for (uint64_t r = a; r < nr; r++) {
-        uint64_t st = r ? ends[r - 1] : 0, en = ends[r];
-        if (st >= hi) break;
-        if (r & 1) {
-          uint64_t x = st > lo ? st : lo, y = en < hi ? en : hi;
-          if (y > x) {
-            uint32_t len = (uint32_t)(y - x), sh = (uint32_t)(x - lo);
-            bits |= (len == 32 ? 0xFFFFFFFFu : ((1u << len) - 1u)) << sh;
-          }
-        }
-      }
-      if (hi > n) bits &= (n - lo) >= 32 ? 0xFFFFFFFFu : ((1u << (uint32_t)(n - lo)) - 1u);
-    }
+    uint32_t bits = w < nw ? dp_rle_word(ends, nr, n, w) : 0u;
     if (w < nw) cnt[w] = (uint64_t)__popc(bits);
     bm32[w] = bits;  // the word past the end stays 0
   }
@@ -955,8 +967,24 @@ __global__ void k_dpb_heads(const uint8_t* const* __restrict__ srcs, const uint6
   H[i] = h;
 }
 
-// Bitmap words of every column with a bitmap (k_dp_bitmap's work), their
-// popcounts, and the caller's bitmap bytes.  word_first[c] = lanes[c].word0.
+// The run ends of every lane with an RLE validity blob: one CTA each
+// (rle_cols lists them).  A blob the sequential reader rejects marks the
+// lane (status 1), which the single-column path then reads.
+__global__ void __launch_bounds__(kRleThreads) k_dpb_rle_runs(DpBatch B) {
+  __shared__ uint64_t s_warp[33];
+  int c = (int)B.rle_cols[blockIdx.x];
+  const DpBLane& Ln = B.lanes[c];
+  bool ok = dp_rle_runs(Ln.s + Ln.vblob_off, Ln.vblob_len, Ln.bm_n, B.rle_ends + Ln.rle_off, B.rle_nruns + c,
+                        s_warp);
+  if (threadIdx.x == 0 && !ok) {
+    B.out[c].status = 1;
+    B.rle_nruns[c] = 0;
+  }
+}
+
+// Bitmap words of every column with a bitmap (k_dp_bitmap's and
+// k_dp_rle_fill's work), their popcounts, and the caller's bitmap bytes.
+// word_first[c] = lanes[c].word0.
 __global__ void k_dpb_bitmap(DpBatch B, const uint64_t* __restrict__ word_first) {
   for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < B.words;
        w += (uint64_t)gridDim.x * blockDim.x) {
@@ -964,9 +992,14 @@ __global__ void k_dpb_bitmap(DpBatch B, const uint64_t* __restrict__ word_first)
     const DpBLane& Ln = B.lanes[c];
     uint64_t k = w - Ln.word0;
     uint32_t bits = 0;
-    if (Ln.L.has_validity && k < Ln.nw) {
+    if (Ln.has_bm && k < Ln.nw && Ln.vtag == 1) {
+      uint64_t n = Ln.bm_n, nb = (n + 7) / 8, b0 = 4 * k;
+      bits = dp_rle_word(B.rle_ends + Ln.rle_off, B.rle_nruns[c], n, k);
+      if (Ln.valid_out)
+        for (uint64_t q = 0; q < 4 && b0 + q < nb; q++) Ln.valid_out[b0 + q] = (uint8_t)(bits >> (8 * q));
+    } else if (Ln.has_bm && k < Ln.nw) {
       const uint8_t* src = Ln.s + Ln.vblob_off;
-      uint64_t n = Ln.L.logical_n, nb = (n + 7) / 8, b0 = 4 * k;
+      uint64_t n = Ln.bm_n, nb = (n + 7) / 8, b0 = 4 * k;
       if (b0 + 4 <= nb) {
         bits = ld_u32(src + b0);
       } else {
@@ -989,7 +1022,7 @@ __global__ void k_dpb_lane_base(DpBatch B) {
   const DpBLane& Ln = B.lanes[c];
   uint64_t base = B.ranks[Ln.word0];
   B.rbase[c] = base;
-  B.out[c].nvalid = Ln.L.has_validity ? B.ranks[Ln.word0 + Ln.nw] - base : Ln.L.logical_n;
+  B.out[c].nvalid = Ln.has_bm ? B.ranks[Ln.word0 + Ln.nw] - base : Ln.bm_n;
 }
 
 // Column-relative ranks, then the select tables (k_select_table per column).
@@ -1006,7 +1039,7 @@ __global__ void k_dpb_select(DpBatch B, const uint64_t* __restrict__ word_first)
     int c = dp_owner(word_first, B.nlanes, w);
     const DpBLane& Ln = B.lanes[c];
     uint64_t k = w - Ln.word0;
-    if (!Ln.L.has_validity || k >= Ln.nw) continue;
+    if (!Ln.has_bm || Ln.decimal || k >= Ln.nw) continue;
     uint32_t bits = B.bm32[w];
     uint64_t r = B.ranks[w], cnt = (uint64_t)__popc(bits);
     uint64_t m = (r + 511) / 512 * 512;
@@ -1103,8 +1136,15 @@ __global__ void k_dpb_succ(DpBatch B) {
 }
 
 // The values a column's frames hold (its valid count or n).
+// (~0 for a decimal limb lane whose count is not the container's valid
+// count: the single-column path reports it.)
 __device__ inline uint64_t dpb_total(const DpBatch& B, int c) {
-  return B.lanes[c].L.has_validity ? B.out[c].nvalid : B.lanes[c].L.logical_n;
+  const DpBLane& Ln = B.lanes[c];
+  if (Ln.decimal) {
+    uint64_t nv = B.out[Ln.vlane].nvalid;
+    return Ln.L.logical_n == nv ? nv : ~0ull;
+  }
+  return Ln.has_bm ? B.out[c].nvalid : Ln.L.logical_n;
 }
 
 // One CTA per column: k_dp_marks over the column's candidates.  nmarked = 0
@@ -1119,11 +1159,13 @@ __global__ void __launch_bounds__(kChainThreads) k_dpb_marks(DpBatch B) {
   uint64_t lo, hi;
   dpb_range(B, c, &lo, &hi);
   uint64_t n_total = dpb_total(B, c);
-  bool good = Ktot <= B.cap && n_total > 0 && hi > lo && B.cand[lo].pos == Ln.L.fstart;
+  bool good = Ktot <= B.cap && n_total > 0 && n_total != ~0ull && hi > lo && B.cand[lo].pos == Ln.L.fstart &&
+              B.out[c].status == 0;
   if (!good) {
+    __syncthreads();  // every thread has read the status
     if (tid == 0) {
       B.out[c].nmarked = 0;
-      B.out[c].status = n_total == 0 && Ktot <= B.cap ? 3u : 1u;
+      if (B.out[c].status == 0) B.out[c].status = n_total == 0 && Ktot <= B.cap ? 3u : 1u;  // 3: no value
     }
     return;
   }
@@ -1377,6 +1419,7 @@ void launch_dp_batch_read(const DpBatch& B, uint64_t* tile_tmp, cudaStream_t st)
   });
   unsigned gw = (unsigned)qmin((B.words + 255) / 256, 148ull * 8);
   if (gw == 0) gw = 1;
+  if (B.nrle) k_dpb_rle_runs<<<B.nrle, kRleThreads, 0, st>>>(B);
   k_dpb_bitmap<<<gw, 256, 0, st>>>(B, B.word0);
   cudaMemsetAsync(B.ranks + B.words, 0, 8, st);
   launch_scan_sum(B.ranks, B.ranks, B.words + 1, tile_tmp, nullptr, st);

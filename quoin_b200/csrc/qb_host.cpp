@@ -1541,26 +1541,51 @@ int decode_queue(QuoinCtx* c, cudaStream_t st, QuoinB200DeviceDecodeJob* jobs, s
     for (size_t i = 0; i < nj; i++) {
       const QuoinB200DeviceDecodeJob& J = jobs[i];
       const DpHead& h = H[i];
-      if (!J.d_src || !J.d_values_out || h.kind || h.decimal || h.n == 0) continue;
-      if (h.has_validity && h.vtag != 0) continue;
+      if (!J.d_src || !J.d_values_out || h.kind || h.n == 0) continue;
       uint32_t w = native_width((int)h.wire);
       if (h.n * (uint64_t)w > J.values_cap_bytes || ((uintptr_t)J.d_values_out % w) != 0) continue;
       take.push_back(i);
     }
     if (!take.empty()) {
-      const int nl = (int)take.size();
+      // one batch lane per plain column, one per limb of a decimal container
+      // (its first limb lane reads the container's bitmap)
+      std::vector<int> lane_job, lane_limb, col_lane0(take.size());
+      for (size_t t = 0; t < take.size(); t++) {
+        const DpHead& h = H[take[t]];
+        col_lane0[t] = (int)lane_job.size();
+        int nlimb = h.decimal ? (int)h.nl : 1;
+        for (int k = 0; k < nlimb; k++) {
+          lane_job.push_back((int)t);
+          lane_limb.push_back(k);
+        }
+      }
+      const int nl = (int)lane_job.size();
       std::vector<DpBLane> lanes(nl);
-      std::vector<uint64_t> word0(nl + 1), chunk0(nl + 1);
-      uint64_t words = 0, chunks = 0, sels = 0, cap = 0, item_cap = 0, scr = 0;
+      std::vector<uint64_t> word0(nl + 1), chunk0(nl + 1), limb_off(nl, 0);
+      uint64_t words = 0, chunks = 0, sels = 0, cap = 0, item_cap = 0, scr = 0, rle_len = 0, limbs = 0;
+      std::vector<uint32_t> rle_cols;
       for (int k = 0; k < nl; k++) {
-        const QuoinB200DeviceDecodeJob& J = jobs[take[k]];
-        const DpHead& h = H[take[k]];
+        const QuoinB200DeviceDecodeJob& J = jobs[take[lane_job[k]]];
+        const DpHead& h = H[take[lane_job[k]]];
+        const int limb = lane_limb[k];
         DpBLane& B = lanes[k];
+        B = DpBLane{};
         B.s = J.d_src;
         B.buf_len = J.src_len;
-        B.L = h.lanes[0];
+        B.L = h.lanes[limb];
+        B.decimal = h.decimal;
+        B.vlane = col_lane0[lane_job[k]];
+        B.has_bm = h.has_validity && limb == 0;
+        B.bm_n = h.n;
         B.vblob_off = h.vblob_off;
-        B.nw = h.has_validity ? (h.n + 31) / 32 : 0;
+        B.vblob_len = h.vblob_len;
+        B.vtag = B.has_bm ? h.vtag : 0;
+        B.rle_off = rle_len;
+        if (B.has_bm && h.vtag == 1) {
+          rle_cols.push_back((uint32_t)k);
+          rle_len += h.vblob_len + 2;
+        }
+        B.nw = B.has_bm ? (h.n + 31) / 32 : 0;
         B.word0 = word0[k] = words;
         words += B.nw + 1;
         B.sel0 = sels;
@@ -1572,7 +1597,11 @@ int decode_queue(QuoinCtx* c, cudaStream_t st, QuoinB200DeviceDecodeJob* jobs, s
         cap += cc;
         item_cap += B.L.logical_n / 512 + fb / 512 + 2 * cc + 16;
         scr += h.n;
-        B.valid_out = h.has_validity ? J.d_validity_out : nullptr;
+        B.valid_out = B.has_bm ? J.d_validity_out : nullptr;
+        if (h.decimal) {  // the limb's values, n at most (the stride of k_decimal_combine)
+          limb_off[k] = limbs;
+          limbs += h.n;
+        }
       }
       word0[nl] = words;
       chunk0[nl] = chunks;
@@ -1585,12 +1614,16 @@ int decode_queue(QuoinCtx* c, cudaStream_t st, QuoinB200DeviceDecodeJob* jobs, s
                o_J = a.take(cap * 8), o_mk = a.take(cap), o_ft = a.take(cap * 16), o_fl = a.take(cap * 4),
                o_fr = a.take((cap + 1) * sizeof(FrameDesc)), o_fc = a.take((cap + 1) * 4),
                o_fp = a.take((cap + 1) * 8), o_mi = a.take(item_cap * 8), o_pi = a.take(item_cap * 8),
-               o_li = a.take((cap + 1) * 4), o_cols = a.take(nl * sizeof(BatchCol)), o_err = a.take(64);
+               o_li = a.take((cap + 1) * 4), o_cols = a.take(nl * sizeof(BatchCol)), o_err = a.take(64),
+               o_rle = a.take((rle_len + 1) * 8), o_rln = a.take(nl * 8), o_rlc = a.take((rle_cols.size() + 1) * 4),
+               o_vmin = a.take(take.size() * 32), o_limbs = a.take((limbs + 1) * 8);
       CK(c->ensure(S_BATCH, a.off));
       uint8_t* bb = c->p<uint8_t>(S_BATCH);
       CK(cudaMemcpyAsync(bb + o_lanes, lanes.data(), nl * sizeof(DpBLane), cudaMemcpyHostToDevice, st));
       CK(cudaMemcpyAsync(bb + o_w0, word0.data(), (nl + 1) * 8, cudaMemcpyHostToDevice, st));
       CK(cudaMemcpyAsync(bb + o_c0, chunk0.data(), (nl + 1) * 8, cudaMemcpyHostToDevice, st));
+      if (!rle_cols.empty())
+        CK(cudaMemcpyAsync(bb + o_rlc, rle_cols.data(), rle_cols.size() * 4, cudaMemcpyHostToDevice, st));
       DpBatch B;
       B.lanes = reinterpret_cast<DpBLane*>(bb + o_lanes);
       B.word0 = reinterpret_cast<const uint64_t*>(bb + o_w0);
@@ -1621,6 +1654,10 @@ int decode_queue(QuoinCtx* c, cudaStream_t st, QuoinB200DeviceDecodeJob* jobs, s
       B.pre_items = reinterpret_cast<ItemRef*>(bb + o_pi);
       B.list = reinterpret_cast<uint32_t*>(bb + o_li);
       B.item_cap = item_cap;
+      B.rle_ends = reinterpret_cast<uint64_t*>(bb + o_rle);
+      B.rle_nruns = reinterpret_cast<uint64_t*>(bb + o_rln);
+      B.rle_cols = reinterpret_cast<const uint32_t*>(bb + o_rlc);
+      B.nrle = (int)rle_cols.size();
       CK(c->ensure(S_TILE, (scan_tile_count((words > chunks ? words : chunks) + 1) + 16) * 8));
       {
         TimedRegion tr(T_READ, st);
@@ -1640,22 +1677,40 @@ int decode_queue(QuoinCtx* c, cudaStream_t st, QuoinB200DeviceDecodeJob* jobs, s
         if (dict) CK(c->ensure(S_BSCR, scr * 8 + 64));
         std::vector<BatchCol> cols(nl);
         uint64_t so = 0;
+        uint64_t* limb_base = reinterpret_cast<uint64_t*>(bb + o_limbs);
         for (int k = 0; k < nl; k++) {
-          const DpHead& h = H[take[k]];
+          const DpHead& h = H[take[lane_job[k]]];
           BatchCol& C = cols[k];
           C = BatchCol{};
-          C.O.out = jobs[take[k]].d_values_out;
-          C.O.dtype = (int)h.wire;
-          C.O.bm32 = h.has_validity ? B.bm32 + lanes[k].word0 : nullptr;
-          C.O.wrank = B.ranks + lanes[k].word0;
-          C.O.sel = B.sel + lanes[k].sel0;
-          C.O.n = h.n;
-          C.O.nvalid = out[k].nvalid;
-          C.O.plog2 = h.lanes[0].plog2;
-          C.dtype = (int)h.wire;
+          if (h.decimal) {  // limbs, dense, into the limb area
+            uint64_t nv = out[lanes[k].vlane].nvalid;
+            C.O.out = limb_base + limb_off[k];
+            C.O.dtype = WT_U64;
+            C.O.n = nv;
+            C.O.nvalid = nv;
+            C.dtype = WT_U64;
+          } else {
+            C.O.out = jobs[take[lane_job[k]]].d_values_out;
+            C.O.dtype = (int)h.wire;
+            C.O.bm32 = h.has_validity ? B.bm32 + lanes[k].word0 : nullptr;
+            C.O.wrank = B.ranks + lanes[k].word0;
+            C.O.sel = B.sel + lanes[k].sel0;
+            C.O.n = h.n;
+            C.O.nvalid = out[k].nvalid;
+            C.dtype = (int)h.wire;
+          }
+          C.O.plog2 = lanes[k].L.plog2;
           C.scratch = dict ? c->p<uint64_t>(S_BSCR) + so : nullptr;
           so += h.n;
         }
+        // a decimal column is batched when all its limb lanes are
+        std::vector<char> col_ok(take.size(), 1);
+        for (int k = 0; k < nl; k++)
+          if (out[k].status != 0) col_ok[lane_job[k]] = 0;
+        std::vector<uint64_t> vmins(take.size() * 4, 0);
+        for (size_t t = 0; t < take.size(); t++)
+          for (int q = 0; q < 4; q++) vmins[4 * t + q] = H[take[t]].vmin[q];
+        CK(cudaMemcpyAsync(bb + o_vmin, vmins.data(), vmins.size() * 8, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(bb + o_cols, cols.data(), nl * sizeof(BatchCol), cudaMemcpyHostToDevice, st));
         unsigned long long* d_err = reinterpret_cast<unsigned long long*>(bb + o_err);
         CK(cudaMemsetAsync(d_err, 0xFF, 8, st));
@@ -1678,19 +1733,35 @@ int decode_queue(QuoinCtx* c, cudaStream_t st, QuoinB200DeviceDecodeJob* jobs, s
           launch_decode_items(nullptr, B.frames, (int)tot.nframes, 0, none, P, c->p<void>(S_PRE), nullptr,
                               c->p<void>(S_DAUX), d_err, st, &bv);
         }
+        {  // decimal containers: vmin + the limbs, through the container's bitmap
+          TimedRegion tr(T_FINALIZE, st);
+          for (size_t t = 0; t < take.size(); t++) {
+            const DpHead& h = H[take[t]];
+            if (!h.decimal || !col_ok[t]) continue;
+            int k0 = col_lane0[t];
+            const bool bm = h.has_validity != 0;
+            launch_decimal_combine(limb_base + limb_off[k0], h.n, (int)h.nl,
+                                   reinterpret_cast<const uint64_t*>(bb + o_vmin) + 4 * t,
+                                   bm ? reinterpret_cast<const uint8_t*>(B.bm32 + lanes[k0].word0) : nullptr,
+                                   bm ? B.ranks + lanes[k0].word0 : nullptr, h.n,
+                                   static_cast<uint8_t*>(jobs[take[t]].d_values_out), st);
+          }
+        }
         unsigned long long herr = 0;
         CK(read_small(c, st, &herr, d_err, 8));
         resolve_timing();
         if (herr == ~0ull) {  // every batch column decoded: the others go one by one
-          for (int k = 0; k < nl; k++) {
-            if (out[k].status != 0) continue;
-            QuoinB200DeviceDecodeJob& J = jobs[take[k]];
-            J.wire = (int32_t)H[take[k]].wire;
-            J.n = H[take[k]].n;
+          uint64_t ncols = 0;
+          for (size_t t = 0; t < take.size(); t++) {
+            if (!col_ok[t]) continue;
+            QuoinB200DeviceDecodeJob& J = jobs[take[t]];
+            J.wire = (int32_t)H[take[t]].wire;
+            J.n = H[take[t]].n;
             J.status = QUOIN_OK;
-            single[take[k]] = 0;
+            single[take[t]] = 0;
+            ncols++;
           }
-          g_batch_columns.fetch_add((uint64_t)nl);
+          g_batch_columns.fetch_add(ncols);
         }
       }
     }

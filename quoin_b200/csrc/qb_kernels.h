@@ -167,7 +167,15 @@ struct DpBLane {
   const uint8_t* s;
   uint64_t buf_len;
   DpLane L;               // the lane (base 0: the column's own stream)
-  uint64_t vblob_off;     // the RAW validity bitmap's bytes, when L.has_validity
+  uint64_t vblob_off;     // the validity blob's bytes after its tag, when has_bm
+  uint64_t vblob_len;
+  uint32_t vtag, pad;     // 0 RAW, 1 RLE
+  uint64_t rle_off;       // an RLE blob's run ends in the batch's run-end array
+  uint64_t bm_n;          // the column's value count (its bitmap's bits)
+  uint32_t has_bm;        // this lane reads the column's bitmap (a plain column's, or a decimal's first limb)
+  uint32_t decimal;       // a limb lane of a decimal container
+  int32_t vlane;          // the lane holding the column's bitmap and valid count (itself for a plain column)
+  uint32_t pad2;
   uint64_t word0, nw;     // its bitmap words (nw, then one zero word)
   uint64_t sel0;          // its select table entries
   uint64_t chunk0;        // its first candidate chunk (the batch has one more entry: the total)
@@ -212,6 +220,10 @@ struct DpBatch {
   ItemRef* pre_items;    // item capacity
   uint32_t* list;        // cap
   uint64_t item_cap;
+  uint64_t* rle_ends;         // the RLE columns' run ends (sum of their blob lengths)
+  uint64_t* rle_nruns;        // nlanes
+  const uint32_t* rle_cols;   // nrle lane indices
+  int nrle;
 };
 uint64_t dp_batch_slot_bytes(uint64_t chunks);
 // Headers of n streams (srcs[i], lens[i]) into H[i].

@@ -2,9 +2,10 @@
 launch per kernel class reads and decodes every column of the batch.  Each
 column's values, bitmap, dtype and count equal the single-column device
 decode's (quoin_b200_decompress_column_device), whichever path takes it:
-the batch for plain and nullable columns of every dtype and mode mix, the
-single-column path for decimal containers, RLE validity blobs,
-entropy-coded frames, all-null and damaged streams, and short buffers.
+the batch for plain and nullable columns of every dtype and mode mix (RAW
+and RLE validity blobs) and for decimal containers (a lane per limb), the
+single-column path for entropy-coded frames, all-null and damaged streams,
+and short buffers.
 """
 import ctypes
 
@@ -81,16 +82,15 @@ def check_batch(qb, streams, caps, has_bitmap):
 
 def test_queue_mixed_columns(qb):
     cols = synth.mixed_columns(48, 1 << 17)
-    streams, caps, hb, plain = [], [], [], 0
+    streams, caps, hb = [], [], []
     for name, dt, v, bm in cols:
         sc, pr = (4, 18) if dt == 6 else (0, 0)
         s = qb.compress_column(v, bm, qb.Config(level=qb.Level.FAST), dtype=dt, scale=sc, precision=pr)
         streams.append(s)
         caps.append(len(v) * NW[dt])
         hb.append(bm is not None)
-        plain += dt != 6
     batched = check_batch(qb, streams, caps, hb)
-    assert batched > 0 and batched <= plain
+    assert batched == len(cols)  # every column of the mix, decimal containers included
 
 
 def test_queue_special_columns(qb):
@@ -109,12 +109,19 @@ def test_queue_special_columns(qb):
         ((np.round(rng.normal(25, 5, 40_000) * 10) / 10).astype(np.float32), 5, None, {}),      # f32 DICT
         (np.zeros(0, np.int64), 1, None, {}),                                                   # empty
     ]
+    dec = np.zeros((30_000, 16), np.uint8)
+    dec[:, :8] = (rng.integers(-10**12, 10**12, 30_000)).view(np.uint8).reshape(-1, 8)
+    dec[:, 8:] = np.where(dec[:, 7:8] >= 128, 255, 0)
     streams, caps, hb = [], [], []
     for v, dt, bm, kw in cases:
         s = qb.compress_column(v, bm, qb.Config(level=qb.Level(kw.get("level", 1)), block_size=kw.get("block_size")),
                                dtype=dt)
         streams.append(s)
         caps.append(len(v) * NW[dt])
+        hb.append(bm is not None)
+    for bm in (None, bitmap_from_bools(vb[:30_000]), bitmap_from_bools(clustered[:30_000])):  # decimal containers
+        streams.append(qb.compress_column(dec, bm, qb.Config(level=qb.Level.FAST), dtype=6, scale=3, precision=20))
+        caps.append(30_000 * 16)
         hb.append(bm is not None)
     # a damaged stream, a short output buffer and a stream that is not one
     streams.append(streams[0][:len(streams[0]) // 2])
@@ -127,4 +134,4 @@ def test_queue_special_columns(qb):
     caps.append(caps[5])
     hb.append(False)
     batched = check_batch(qb, streams, caps, hb)
-    assert batched >= 4
+    assert batched >= 9
