@@ -571,7 +571,8 @@ def run_gpu(args, rank, world, local):
             "per_column_ms": per_column,
             "roofline": {"bound": "hbm", "kernel": "decode phase: the device stream reader (k_dp_head, "
                                                    "k_dp_bitmap, k_word_popcount, scans, k_select_table, "
-                                                   "k_dp_cand_count, k_dp_cand_write, k_dp_chain, k_dp_expand) "
+                                                   "k_dp_cand_scan, k_dp_cand_compact, k_dp_succ, k_dp_marks, "
+                                                   "k_dp_items, k_dp_layout, k_dp_expand) "
                                                    "and the block decoder (k_walk_frames, k_prepass, "
                                                    "k_prepass_scan, k_decode_items, k_decode_frames, "
                                                    "k_decimal_combine) of the three columns in flight together",

@@ -201,6 +201,35 @@ int quoin_b200_compress_column_device(QuoinCtx *ctx, int32_t wire_dtype, size_t 
                                       uint8_t *d_dst, size_t dst_cap, size_t *out_len,
                                       void *stream);
 
+/* Parts of a compress, for a column split across devices (one process per
+ * GPU; blocks are independent, reference src/encoder.rs:7-8).
+ *
+ * quoin_b200_probe_windows_device: the block plan's probe (src/encoder.rs:154-178,
+ * probe_block_features src/encoder.rs:705-750) over the column's valid values:
+ * grow_out[w] = 1 where plan_blocks grows a block that starts at 32,768-value
+ * window w to 131,072 values, else 0; *n_windows = ceil(valid values / 32,768)
+ * (QUOIN_ERR_BUFFER_TOO_SMALL when it exceeds grow_cap).  grow_out is HOST
+ * memory.  A part of a column that starts at a window boundary of the valid
+ * values probes that part's windows, so the plan of the whole column is the
+ * plan_blocks scan over the concatenated bytes.
+ *
+ * quoin_b200_stream_prefix_device: the bytes before a stream's first frame
+ * (src/encoder.rs:184-214): the 16-byte header for n values and, when the
+ * bitmap has a null, the validity blob.  The stream of the whole column is
+ * this prefix followed by the frames of its blocks in order, and the frames of
+ * a run of whole blocks are the stream of those blocks' valid values (no
+ * validity) without its 16-byte header.
+ *
+ * Decimal dtypes return QUOIN_ERR_UNSUPPORTED (their container holds limb
+ * streams). */
+int quoin_b200_probe_windows_device(QuoinCtx *ctx, int32_t wire_dtype, size_t n,
+                                    const void *d_values, const uint8_t *d_validity,
+                                    uint8_t *grow_out, size_t grow_cap, uint64_t *n_windows,
+                                    void *stream);
+int quoin_b200_stream_prefix_device(QuoinCtx *ctx, int32_t wire_dtype, size_t n,
+                                    const uint8_t *d_validity, const QuoinConfig *cfg,
+                                    uint8_t *d_dst, size_t dst_cap, size_t *out_len, void *stream);
+
 /* A decode index: the header, validity and frame table of a stream, parsed
  * and validated once on the host (src/decoder.rs:43-94) and kept resident on
  * the device so the stream can be decoded again without re-walking it. */

@@ -93,6 +93,7 @@ def lib():
         L.oq_validity_encode.argtypes = [P, S, ctypes.POINTER(U8P), ctypes.POINTER(S)]
         L.oq_validity_decode.argtypes = [P, S, S, P]
         L.oq_mode_win_counts.argtypes = [P]
+        L.oq_probe_windows.argtypes = [P, S, P]
         _lib = L
     return _lib
 
@@ -337,6 +338,14 @@ def unpack64(packed: np.ndarray, width: int) -> np.ndarray:
     out = np.zeros(1024, dtype=np.uint64)
     lib().oq_unpack64(p.ctypes.data, width, out.ctypes.data)
     return out
+
+
+def probe_windows(lane: np.ndarray) -> np.ndarray:
+    """plan_blocks' probe byte for every 32,768-value window of a u64 lane."""
+    lane = np.ascontiguousarray(lane, dtype=np.uint64)
+    flags = np.zeros(max((lane.size + 32767) // 32768, 1), dtype=np.uint8)
+    lib().oq_probe_windows(_ptr(lane), lane.size, _ptr(flags))
+    return flags[: (lane.size + 32767) // 32768]
 
 
 def mode_win_counts() -> np.ndarray:

@@ -2327,6 +2327,16 @@ static void encode_block(const uint64_t *b, size_t n, int dtype, int level, buf_
 }
 
 /* encoder.rs:154-178 */
+/* plan_blocks' probe (encoder.rs:168-170) for every 32,768-value window of a
+ * lane: flags[w] = 1 where a block starting at window w grows to MAX_QUANTUM. */
+void oq_probe_windows(const uint64_t *v, size_t n, uint8_t *flags) {
+    for (size_t w = 0; w * 32768 < n; w++) {
+        size_t s = w * 32768, e = s + 32768 < n ? s + 32768 : n;
+        feats_t f = probe_block_features(v + s, e - s);
+        flags[w] = (f.distinct_low || f.repeats) ? 1 : 0;
+    }
+}
+
 static size_t plan_blocks(const uint64_t *v, size_t n, long block_size, size_t **starts_out) {
     size_t cap = n / 32768 + 2, nb = 0;
     if (block_size > 0) {

@@ -96,6 +96,8 @@ int oq_encode_mode(int mode, const uint64_t *vals, size_t n, int dtype, int leve
 /* Decode one frame payload of `mode` into n lane words. */
 int oq_decode_mode(int mode, const uint8_t *payload, size_t plen, size_t n, int dtype,
                    uint64_t *out);
+/* plan_blocks' probe for every 32,768-value window of a lane (encoder.rs:154-178). */
+void oq_probe_windows(const uint64_t *lane, size_t n, uint8_t *flags);
 /* Validity blob (src/validity.rs). */
 int oq_validity_encode(const uint8_t *bitmap, size_t n, uint8_t **out, size_t *out_len);
 int oq_validity_decode(const uint8_t *blob, size_t len, size_t n, uint8_t *bitmap_out);

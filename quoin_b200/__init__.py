@@ -138,6 +138,9 @@ def _load():
     L.quoin_b200_reader_stats.argtypes = [P]
     L.quoin_b200_decompress_queue_device.argtypes = [P, P, S, P]
     L.quoin_b200_reset_mode_win_counts.argtypes = []
+    L.quoin_b200_probe_windows_device.argtypes = [P, ctypes.c_int32, S, P, P, P, S, ctypes.POINTER(ctypes.c_uint64), P]
+    L.quoin_b200_stream_prefix_device.argtypes = [P, ctypes.c_int32, S, P, ctypes.POINTER(_QuoinConfig), P, S,
+                                                  ctypes.POINTER(S), P]
     L.quoin_b200_kernel_launches.restype = ctypes.c_uint64
     return L
 

@@ -2061,6 +2061,11 @@ constexpr int kXorzRounds = 4;           // rounds per XORZ item (kXorzItemBytes
 static_assert(kItemBytes * kXorzRounds == kXorzItemBytes, "XORZ item size shared with the readers");
 constexpr int kItemStage = kItemVals + kItemVals / 16;  // u64 staging with one pad per 16
 constexpr int kItemWarps = 8;
+// Resident CTAs per SM the item kernel is compiled for (its register cap):
+// 6 gives 40 registers a thread.
+#ifndef QB_ITEM_MIN_BLOCKS
+#define QB_ITEM_MIN_BLOCKS 6
+#endif
 
 struct PreRec {
   uint64_t a;     // DELTA/RLE: sum; XORZ: XOR of values ending in the item.  After the scan: carry / start / XOR carry
@@ -2597,7 +2602,7 @@ __global__ void k_prepass_scan(const uint8_t* __restrict__ stream, const FrameDe
 }
 
 // Main items: one warp per item.
-__global__ void __launch_bounds__(kItemWarps * 32, 6) k_decode_items(const uint8_t* __restrict__ stream,
+__global__ void __launch_bounds__(kItemWarps * 32, QB_ITEM_MIN_BLOCKS) k_decode_items(const uint8_t* __restrict__ stream,
                                                                 const FrameDesc* __restrict__ frames,
                                                                 int dtype, const FrameAux* __restrict__ aux,
                                                                 const ItemRef* __restrict__ items, uint32_t nitems,

@@ -23,10 +23,13 @@
 //      are counted as the host reader's build_items does (k_dp_items, across
 //      the GPU), the frames cut where their values reach the lane's count and
 //      laid out (k_dp_layout, one CTA), and the items listed (k_dp_expand).
-// A stream the fast path cannot take (a header or validity error, an RLE
-// validity blob, a chain frame that is not a candidate, a count mismatch,
-// more candidates than the tables hold) is flagged, and the host reader
-// parses a host copy instead, so every error kind stays the reference's.
+// Validity blobs are read here too: RAW bitmaps copied into words, RLE
+// varint runs expanded by a run table.  A stream the fast path cannot take
+// (a header or validity error, a chain frame that is not a candidate, a count
+// mismatch, more candidates than the tables hold) is flagged, and the host
+// reader parses a host copy instead, so every error kind stays the
+// reference's.  The batched reader (k_dpb_*) flags columns with
+// entropy-coded frames as well; those decode one by one.
 #include "qb_common.cuh"
 #include "qb_kernels.h"
 #include "qb_layout.h"
@@ -86,16 +89,9 @@ __device__ bool dp_frame_plausible(const uint8_t* s, uint64_t pl0, uint32_t n, u
   }
 }
 
-// One bit per byte of w (bit k for byte k): set where the byte is zero.
-__device__ __forceinline__ uint32_t zero_bytes8(uint64_t w) {
-  uint64_t t = (w & 0x7F7F7F7F7F7F7F7Full) + 0x7F7F7F7F7F7F7F7Full;
-  t = ~(t | w | 0x7F7F7F7F7F7F7F7Full);  // 0x80 in every zero byte, nothing else
-  return (uint32_t)(((t >> 7) * 0x0102040810204080ull) >> 56);
-}
-
 // ---------------------------------------------------------------------------
 // Header (one thread).  Any error, or a form the device reader leaves to the
-// host (an RLE validity blob, a limb lane with its own bitmap), sets kind = 1.
+// host (a limb lane with its own bitmap), sets kind = 1.
 // ---------------------------------------------------------------------------
 __device__ bool dp_lane_header(const uint8_t* s, uint64_t base, uint64_t len, DpLane& L) {
   const uint8_t* h = s + base;
@@ -354,13 +350,6 @@ constexpr uint64_t kCandModes = (1ull << 1) | (1ull << 2) | (1ull << 3) | (1ull 
                                 (1ull << 52) | (1ull << 53) | (1ull << 54);
 static_assert(((kCandModes >> 0) & 1) == 0, "PRED is not a candidate mode");
 
-// Bytes i .. i+7 of the window (i < 16).
-__device__ __forceinline__ uint64_t dp_bytes8(uint64_t w0, uint64_t w1, uint64_t w2, uint32_t i) {
-  uint64_t lo = i < 8 ? w0 : w1, hi = i < 8 ? w1 : w2;
-  uint32_t sh = 8 * (i & 7);
-  return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
-}
-
 // Chunk j of a lane starts at the 16-byte aligned address at or below its
 // first frame offset, plus j * kDpChunk, and is read in kDpSteps steps of
 // kDpThreads * 16 positions; in a step thread t takes the 16 positions from
@@ -398,6 +387,16 @@ __device__ __forceinline__ DpWin dp_load(const uint8_t* __restrict__ s, uint64_t
   return w;
 }
 
+// Per byte of x, 0x80 where the byte AND ~keep is zero (keep = the bits a
+// byte may hold), else 0: ((x & 0x7F..) + 0x7F..) sets bit 7 of every byte
+// with a low bit set, and x's own bit 7 the others.
+template <uint32_t kKeep>
+__device__ __forceinline__ uint32_t bytes_within(uint32_t x) {
+  constexpr uint32_t kClear = ~(kKeep * 0x01010101u);
+  uint32_t t = (x & kClear & 0x7F7F7F7Fu) + 0x7F7F7F7Fu;
+  return ~(t | (x & kClear) | 0x7F7F7F7Fu);
+}
+
 __device__ inline uint32_t dp_thread_cands(const uint8_t* __restrict__ s, const DpLane& L, uint64_t a,
                                            const DpWin& W) {
   const uint64_t end = L.base + L.len;
@@ -406,28 +405,44 @@ __device__ inline uint32_t dp_thread_cands(const uint8_t* __restrict__ s, const 
     n0 = W.next.x;
     n1 = W.next.y;
   }
-  uint64_t w0 = W.v.x | ((uint64_t)W.v.y << 32), w1 = W.v.z | ((uint64_t)W.v.w << 32), w2 = n0 | ((uint64_t)n1 << 32);
   // positions that can hold a header: from the first frame offset, with 9
   // bytes before the lane's end
   if (a + 15 < L.fstart || a + 9 > end) return 0;
-  uint32_t z = zero_bytes8(w0) | (zero_bytes8(w1) << 8) | (zero_bytes8(w2) << 16);
-  // mode byte nonzero, byte i+4 (top byte of n) and byte i+8 (top byte of
-  // plen) zero
-  uint32_t m = ~z & (z >> 4) & (z >> 8) & 0xFFFFu;
-  if (a < L.fstart) m &= 0xFFFFu << (uint32_t)(L.fstart - a);
-  uint64_t last = end - 9;
-  if (a + 15 > last) m &= (2u << (uint32_t)(last - a)) - 1u;
+  const uint32_t x[6] = {W.v.x, W.v.y, W.v.z, W.v.w, n0, n1};
+  // per byte, 0x80 flags: z = zero; the 4-byte word k of positions 4k..4k+3
+  // keeps a position whose mode byte is in 1..63 and whose bytes +4 (top
+  // byte of n) and +8 (top byte of plen) are zero
+  uint32_t z[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) z[k] = bytes_within<0>(x[k]);
+  uint32_t mk[4], any = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    mk[k] = bytes_within<0x3F>(x[k]) & ~z[k] & z[k + 1] & z[k + 2];
+    any |= mk[k];
+  }
+  if (!any) return 0;
+  const uint32_t lo = a < L.fstart ? (uint32_t)(L.fstart - a) : 0u;  // first position in range
+  const uint64_t last = end - 9;
+  const uint32_t hi = a + 15 > last ? (uint32_t)(last - a) : 15u;   // last position in range
   uint32_t lb = lane_bytes((int)L.dtype);
   uint32_t out = 0;
-  while (m) {
-    uint32_t i = __ffs(m) - 1;
-    m &= m - 1;
-    uint64_t h = dp_bytes8(w0, w1, w2, i);  // mode, n (3 bytes; the 4th is zero), plen (3 bytes)
-    uint32_t mode = (uint32_t)(h & 0xFF), n = (uint32_t)((h >> 8) & 0xFFFFFF), plen = (uint32_t)(h >> 40);
-    uint64_t p = a + i;
-    if (mode < 64 && ((kCandModes >> mode) & 1) && n >= 1 && n <= (uint32_t)kMaxBlock && plen <= end - p - 9 &&
-        dp_frame_plausible(s, p + 9, n, plen, mode, lb))
-      out |= 1u << i;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    uint32_t m = mk[k];
+    while (m) {
+      uint32_t j = (uint32_t)(__ffs(m) - 1) >> 3;
+      m &= m - 1;
+      uint32_t i = 4 * k + j;
+      if (i < lo || i > hi) continue;
+      uint32_t h0 = __funnelshift_r(x[k], x[k + 1], 8 * j);      // mode, n (low 3 bytes)
+      uint32_t h1 = __funnelshift_r(x[k + 1], x[k + 2], 8 * j);  // byte +4 (zero), plen (3 bytes)
+      uint32_t mode = h0 & 0xFF, n = h0 >> 8, plen = h1 >> 8;
+      uint64_t p = a + i;
+      if (((kCandModes >> mode) & 1) && n >= 1 && n <= (uint32_t)kMaxBlock && plen <= end - p - 9 &&
+          dp_frame_plausible(s, p + 9, n, plen, mode, lb))
+        out |= 1u << i;
+    }
   }
   return out;
 }

@@ -582,6 +582,32 @@ int compress_decimal_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, 
 }
 
 // compress_column (reference lib.rs:429-455) with device buffers.
+// Lowers a non-decimal column to its lane (valid values as u64) on the
+// device, as compress_column_device does; *lane points at the input itself
+// when no copy is needed.
+int lower_column(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, const void* d_values,
+                 const uint8_t* d_validity, const uint64_t** lane, uint64_t* n_valid, const uint8_t** d_bm,
+                 bool* vb_raw) {
+  *n_valid = n;
+  *d_bm = nullptr;
+  *vb_raw = false;
+  if (d_validity && n) {
+    int rc = device_valid_count(c, st, d_validity, n, n_valid, vb_raw);
+    if (rc) return rc;
+    if (*n_valid < n) *d_bm = d_validity;
+  }
+  bool direct = !*d_bm && lane_bytes_h(wire) == 8 && wire != WT_F32 && ((uintptr_t)d_values & 7) == 0;
+  if (direct) {
+    *lane = (const uint64_t*)d_values;
+    return QUOIN_OK;
+  }
+  CK(c->ensure(S_LANE, *n_valid * 8 + 64));
+  TimedRegion tr(T_LOWER, st);
+  launch_lower(d_values, wire, *d_bm, *d_bm ? c->p<uint64_t>(S_RANK) : nullptr, n, c->p<uint64_t>(S_LANE), st);
+  *lane = c->p<uint64_t>(S_LANE);
+  return QUOIN_OK;
+}
+
 int compress_column_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, const void* d_values,
                            const uint8_t* d_validity, int8_t scale, uint8_t precision, const QuoinConfig* cfg,
                            uint8_t* d_dst, size_t dst_cap, size_t* out_len) {
@@ -597,22 +623,73 @@ int compress_column_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, c
   uint64_t n_valid = n;
   const uint8_t* d_bm = nullptr;
   bool vb_raw = false;
+  const uint64_t* lane = nullptr;
+  rc = lower_column(c, st, wire, n, d_values, d_validity, &lane, &n_valid, &d_bm, &vb_raw);
+  if (rc) return rc;
+  LaneJob j{lane, n_valid, wire, n, d_bm, level, bs, plog2, vb_raw};
+  return encode_lane(c, st, j, d_dst, dst_cap, out_len);
+}
+
+// The block plan's window probe over a column's lane (reference
+// encoder.rs:154-178, probe_block_features encoder.rs:705-750): one byte per
+// 32,768-value window of the valid values, 1 where plan_blocks grows a block
+// starting at that window to 131,072 values.  The plan itself is a scan over
+// these bytes, so a column split at window boundaries can be probed in parts.
+int probe_windows_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, const void* d_values,
+                         const uint8_t* d_validity, uint8_t* grow_out, uint64_t grow_cap, uint64_t* n_windows) {
+  if (wire < 0 || wire > 7) return QUOIN_ERR_BAD_ARG;
+  if (wire == WT_DEC128 || wire == WT_DEC256) return QUOIN_ERR_UNSUPPORTED;
+  const uint64_t* lane = nullptr;
+  uint64_t nv = 0;
+  const uint8_t* d_bm = nullptr;
+  bool vb_raw = false;
+  int rc = lower_column(c, st, wire, n, d_values, d_validity, &lane, &nv, &d_bm, &vb_raw);
+  if (rc) return rc;
+  uint64_t nwin = (nv + kBaseQuantumH - 1) / kBaseQuantumH;
+  *n_windows = nwin;
+  if (nwin > grow_cap) return QUOIN_ERR_BUFFER_TOO_SMALL;
+  if (!nwin) return QUOIN_OK;
+  uint64_t items = sub_stats_items(nv, 0);
+  bool fl = wire == WT_F64 || wire == WT_F32;
+  CK(c->ensure(S_GROW, nwin + 16));
+  CK(c->ensure(S_SUBST, (items + 1) * sub_stats_bytes()));
+  CK(c->ensure(S_WINBITS, (nwin + 1) * kWinWords * 4));
+  if (fl) {
+    CK(c->ensure(S_FMST, (items + 1) * fm_stats_bytes()));
+    CK(c->ensure(S_SMP16, (nv / 16 + 2) * 8));
+  }
+  {
+    TimedRegion tr(T_PLAN, st);
+    launch_sub_stats(lane, nv, 0, wire, QUOIN_LEVEL_FAST, c->p<void>(S_SUBST), fl ? c->p<void>(S_FMST) : nullptr,
+                     fl ? c->p<uint64_t>(S_SMP16) : nullptr, c->p<uint8_t>(S_GROW), c->p<uint32_t>(S_WINBITS), st);
+  }
+  CK(cudaMemcpyAsync(grow_out, c->p<uint8_t>(S_GROW), nwin, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  resolve_timing();
+  for (uint64_t w = 0; w < nwin; w++) grow_out[w] = grow_out[w] ? 1 : 0;
+  return QUOIN_OK;
+}
+
+// The bytes of a stream before its first frame (reference encoder.rs:184-214):
+// the 16-byte header and, when the column has nulls, the validity blob.
+int stream_prefix_device(QuoinCtx* c, cudaStream_t st, int wire, uint64_t n, const uint8_t* d_validity,
+                         const QuoinConfig* cfg, uint8_t* d_dst, size_t dst_cap, size_t* out_len) {
+  if (wire < 0 || wire > 7) return QUOIN_ERR_BAD_ARG;
+  if (wire == WT_DEC128 || wire == WT_DEC256) return QUOIN_ERR_UNSUPPORTED;
+  int level;
+  uint64_t bs;
+  uint8_t plog2;
+  int rc = check_level(cfg, &level, &bs, &plog2);
+  if (rc) return rc;
+  uint64_t n_valid = n;
+  const uint8_t* d_bm = nullptr;
+  bool vb_raw = false;
   if (d_validity && n) {
     rc = device_valid_count(c, st, d_validity, n, &n_valid, &vb_raw);
     if (rc) return rc;
     if (n_valid < n) d_bm = d_validity;
   }
-  const uint64_t* lane;
-  bool direct = !d_bm && lane_bytes_h(wire) == 8 && wire != WT_F32 && ((uintptr_t)d_values & 7) == 0;
-  if (direct) {
-    lane = (const uint64_t*)d_values;
-  } else {
-    CK(c->ensure(S_LANE, n_valid * 8 + 64));
-    TimedRegion tr(T_LOWER, st);
-    launch_lower(d_values, wire, d_bm, d_bm ? c->p<uint64_t>(S_RANK) : nullptr, n, c->p<uint64_t>(S_LANE), st);
-    lane = c->p<uint64_t>(S_LANE);
-  }
-  LaneJob j{lane, n_valid, wire, n, d_bm, level, bs, plog2, vb_raw};
+  LaneJob j{nullptr, 0, wire, n, d_bm, level, bs, plog2, vb_raw};  // no values: no frames
   return encode_lane(c, st, j, d_dst, dst_cap, out_len);
 }
 
@@ -1414,8 +1491,8 @@ int decode_device(QuoinCtx* c, cudaStream_t st, const uint8_t* d_src, uint64_t l
     uint8_t* cb = c->p<uint8_t>(S_DPCAND);
     uint64_t* ditems = c->p<uint64_t>(S_DITEMS);
     const uint64_t* d_nvalid = H.has_validity ? &dM->nvalid : nullptr;
-    TimedRegion tr(T_READ, st);
     for (int k = 0; k < nl; k++) {
+      TimedRegion tr(T_READ, st);
       const DpLane& L = H.lanes[k];
       uint64_t fb = L.base + L.len - L.fstart;
       DpCand* cand = reinterpret_cast<DpCand*>(cb + cand_off[k]);
@@ -2169,6 +2246,38 @@ int quoin_b200_compress_column_device(QuoinCtx* ctx, int32_t wire, size_t n, con
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     return compress_column_device(c, st, wire, n, d_values, d_validity, scale, precision, cfg, d_dst, dst_cap,
                                   out_len);
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+int quoin_b200_probe_windows_device(QuoinCtx* ctx, int32_t wire, size_t n, const void* d_values,
+                                    const uint8_t* d_validity, uint8_t* grow_out, size_t grow_cap,
+                                    uint64_t* n_windows, void* stream) {
+  if (!n_windows || (!d_values && n) || (!grow_out && grow_cap)) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = pick(ctx);
+    if (!c) return QUOIN_ERR_CUDA;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    return probe_windows_device(c, st, wire, n, d_values, d_validity, grow_out, grow_cap, n_windows);
+  } catch (...) {
+    return QUOIN_ERR_PANIC;
+  }
+}
+
+int quoin_b200_stream_prefix_device(QuoinCtx* ctx, int32_t wire, size_t n, const uint8_t* d_validity,
+                                    const QuoinConfig* cfg, uint8_t* d_dst, size_t dst_cap, size_t* out_len,
+                                    void* stream) {
+  if (!out_len || !d_dst) return QUOIN_ERR_NULL;
+  try {
+    QuoinCtx* c = pick(ctx);
+    if (!c) return QUOIN_ERR_CUDA;
+    std::lock_guard<std::mutex> l(c->mu);
+    DeviceScope ds(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    return stream_prefix_device(c, st, wire, n, d_validity, cfg, d_dst, dst_cap, out_len);
   } catch (...) {
     return QUOIN_ERR_PANIC;
   }

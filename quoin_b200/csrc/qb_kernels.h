@@ -123,7 +123,7 @@ struct DpLaneOut {
   uint32_t status, nframes, nmain, npre, nlist, need_scan, any_dict, pad;
   uint64_t ncand, ent_bytes;
 };
-// Where k_dp_chain writes a lane's decode tables (capacity = the candidate
+// Where k_dp_layout and k_dp_expand write a lane's decode tables (capacity = the candidate
 // capacity; main_off one entry more).
 struct DpTables {
   FrameDesc* frames;
