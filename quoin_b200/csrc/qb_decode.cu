@@ -2062,9 +2062,10 @@ static_assert(kItemBytes * kXorzRounds == kXorzItemBytes, "XORZ item size shared
 constexpr int kItemStage = kItemVals + kItemVals / 16;  // u64 staging with one pad per 16
 constexpr int kItemWarps = 8;
 // Resident CTAs per SM the item kernel is compiled for (its register cap):
-// 6 gives 40 registers a thread.
+// 5 gives 48 registers a thread, and the kernel's 39 KB of shared memory
+// holds five CTAs on an SM.
 #ifndef QB_ITEM_MIN_BLOCKS
-#define QB_ITEM_MIN_BLOCKS 6
+#define QB_ITEM_MIN_BLOCKS 5
 #endif
 
 struct PreRec {
@@ -2346,26 +2347,24 @@ __device__ inline void warp_prefix_skewed(uint64_t* stg, uint32_t cnt, uint64_t 
   __syncwarp();
 }
 
-// One XORZ item: payload bytes [s, s + 512) of a frame with plen bytes.  Lane l
-// owns bytes [s + 16l, s + 16l + 16).  XOR is linear, so the value v_i = x_1 ^
-// ... ^ x_i is the XOR of every byte's contribution (b & 0x7f) << 7j (j = the
-// byte's index inside its LEB128 value) up to value i's terminator: each lane
-// folds its bytes into a running state and a terminator emits the state.
-// Pass 1 (xorz_lane_scan) gives per lane its values, contribution XOR and the
-// terminator bookkeeping; pass 2 (xorz_lane_emit) re-runs the bytes from the
-// lane's starting state.  Bytes at or beyond a value's 11th are ignored and
-// a terminator there marks the value over-long (xorz.rs / varint.rs limits).
-struct XSlice {
-  uint32_t cnt, before, total;  // lane values, values in lanes before, item values
-  uint64_t xo;                  // XOR of the lane's byte contributions
-  int64_t lastt;                // item's last terminator (-1 none)
-  uint32_t bad;                 // lane ended an over-long value
-  uint32_t first_bad;           // lane-local index of the first such value (~0 none)
-  uint32_t tm;                  // lane's terminator mask over its 16 bytes
-  uint64_t b0;                  // lane's first byte
-  uint32_t j0;                  // index inside its value of the lane's first byte (capped at 10)
-  uint32_t nb;                  // lane's bytes inside the payload
-  uint64_t w0, w1;              // the lane's 16 bytes
+// XORZ rounds (reference codecs/xorz.rs:18-32: LEB128 of v_i ^ v_{i-1}).  A
+// round is payload bytes [s0, s0 + 512) of a frame with plen bytes; lane l
+// owns bytes [s0 + 16l, s0 + 16l + 16) and decodes the values whose
+// terminator (a byte below 0x80) lies there, one value per step.  The round's
+// bytes, with the 16 bytes before it, sit in a per-warp shared buffer, so a
+// value that began in another lane or the previous round is read whole: its
+// bytes, loaded as 8 (or 16) at its start, are masked to its length and
+// their 7-bit groups packed together.  A value longer than 10 bytes is
+// over-long (varint.rs limits); bytes 9 and 10 contribute 7 bits and 1 bit as
+// the sequential reader's shifts by 56 and 63 leave them.
+constexpr int kXorzBufWords = 68;  // 16 bytes before the round, 512 of it, 16 after
+
+struct XLane {
+  uint64_t b0;                  // lane's first payload byte
+  uint32_t tm;                  // terminators among the lane's bytes (bit q: byte b0 + q)
+  uint32_t cnt, before, total;  // lane values, values in lanes before, round values
+  int64_t prev;                 // last terminator before b0 (-1: the frame's first byte starts a value)
+  int64_t lastt;                // round's last terminator (-1 none)
 };
 
 __device__ __forceinline__ uint32_t term_mask8(uint64_t w) {
@@ -2373,66 +2372,38 @@ __device__ __forceinline__ uint32_t term_mask8(uint64_t w) {
   return (uint32_t)((t * 0x0102040810204080ull) >> 56);
 }
 
-template <bool EMIT, bool CHECK>
-__device__ __forceinline__ uint64_t xorz_lane_bytes(XSlice& X, uint64_t state, uint64_t* stg, uint32_t k) {
-  uint32_t j = X.j0;
-#pragma unroll
-  for (int q = 0; q < 16; q++) {
-    if ((uint32_t)q < X.nb) {
-      uint32_t b = (uint32_t)(((q < 8) ? (X.w0 >> (8 * q)) : (X.w1 >> (8 * (q - 8)))) & 0xFFu);
-      if (j < 10) state ^= (uint64_t)(b & 0x7Fu) << (7 * j);
-      if (!(b & 0x80u)) {
-        if (CHECK && j >= 10) {
-          if (!X.bad) X.first_bad = k;
-          X.bad = 1;
-        }
-        if (EMIT) stg[skew(X.before + k)] = state;
-        k++;
-        j = 0;
-      } else {
-        j = j < 10 ? j + 1 : 10;
-      }
-    }
-  }
-  return state;
-}
-
-// BYTES: also run the lane's bytes once for their contribution XOR (xo) and
-// the over-long flags (the prepass); the item kernel folds that into its
-// emitting pass.
-template <bool BYTES>
-__device__ XSlice xorz_lane_scan(const uint8_t* p, uint64_t plen, uint64_t s) {
+// Loads the round into xb and finds the lanes' terminators.
+__device__ XLane xorz_round(const uint8_t* p, uint64_t plen, uint64_t s0, uint64_t* xb) {
   int l = threadIdx.x & 31;
-  XSlice X;
-  X.b0 = s + (uint64_t)l * 16;
-  X.nb = X.b0 < plen ? (uint32_t)qmin(16, plen - X.b0) : 0u;
-  if (X.nb == 16) {
-    X.w0 = ld_u64(p + X.b0);
-    X.w1 = ld_u64(p + X.b0 + 8);
+  XLane X;
+  X.b0 = s0 + (uint64_t)l * 16;
+  uint32_t nb = X.b0 < plen ? (uint32_t)qmin(16, plen - X.b0) : 0u;
+  uint64_t w0 = 0, w1 = 0;
+  if (nb == 16) {
+    w0 = ld_u64(p + X.b0);
+    w1 = ld_u64(p + X.b0 + 8);
   } else {
-    X.w0 = 0;
-    X.w1 = 0;
-    for (uint32_t q = 0; q < X.nb; q++) {
+    for (uint32_t q = 0; q < nb; q++) {
       uint64_t b = p[X.b0 + q];
-      if (q < 8) X.w0 |= b << (8 * q); else X.w1 |= b << (8 * (q - 8));
+      if (q < 8) w0 |= b << (8 * q); else w1 |= b << (8 * (q - 8));
     }
   }
-  uint32_t tm = term_mask8(X.w0) | (term_mask8(X.w1) << 8);
-  if (X.nb < 16) tm &= (1u << X.nb) - 1u;
+  xb[2 + 2 * l] = w0;
+  xb[3 + 2 * l] = w1;
+  uint64_t pre = 0;  // lanes 0, 1: the 16 bytes before the round
+  if (l < 2 && s0 >= 16) pre = ld_u64(p + s0 - 16 + 8 * l);
+  if (l < 2) xb[l] = pre;
+  if (l >= 2 && l < 4) xb[64 + l] = 0;
+  uint32_t pm = l < 2 ? term_mask8(pre) << (8 * l) : 0u;
+  pm |= __shfl_sync(0xffffffffu, pm, 1);
+  pm = __shfl_sync(0xffffffffu, pm, 0);
+  // no terminator among the 16 bytes before: the value in progress is over-long
+  int64_t item_prev = s0 == 0 ? -1 : (pm ? (int64_t)s0 - 16 + (31 - __clz(pm)) : (int64_t)s0 - 17);
+  uint32_t tm = term_mask8(w0) | (term_mask8(w1) << 8);
+  if (nb < 16) tm &= (1u << nb) - 1u;
   X.tm = tm;
   X.cnt = __popc(tm);
   int64_t mylast = tm ? (int64_t)(X.b0 + 31 - __clz(tm)) : -1;
-  // the terminator before the item: look back at most 10 bytes
-  int64_t found = -1;
-  if (s > 0 && l < 10 && (uint64_t)l < s) {
-    uint64_t q = s - 1 - (uint64_t)l;
-    if (!(p[q] & 0x80)) found = (int64_t)q;
-  }
-  for (int o = 16; o; o >>= 1) {
-    int64_t u = __shfl_xor_sync(0xffffffffu, found, o);
-    found = u > found ? u : found;
-  }
-  int64_t item_prev = s == 0 ? -1 : (found >= 0 ? found : (s >= 11 ? (int64_t)s - 11 : -1));
   uint32_t inc = X.cnt;
   int64_t mx = mylast;
   for (int o = 1; o < 32; o <<= 1) {
@@ -2447,13 +2418,74 @@ __device__ XSlice xorz_lane_scan(const uint8_t* p, uint64_t plen, uint64_t s) {
   X.total = __shfl_sync(0xffffffffu, inc, 31);
   X.lastt = __shfl_sync(0xffffffffu, mx, 31);
   int64_t prev = __shfl_up_sync(0xffffffffu, mx, 1);  // last terminator in the lanes before
-  if (l == 0 || prev < item_prev) prev = item_prev;
-  uint64_t dist = X.b0 - (uint64_t)(prev + 1);
-  X.j0 = (uint32_t)qmin(dist, 10);
-  X.bad = 0;
-  X.first_bad = ~0u;
-  X.xo = BYTES ? xorz_lane_bytes<false, true>(X, 0ull, nullptr, 0) : 0ull;
+  X.prev = (l == 0 || prev < item_prev) ? item_prev : prev;
+  __syncwarp();
   return X;
+}
+
+// The value whose bytes start at xb byte o and number len (1..10): up to 4
+// bytes in 32-bit arithmetic, else from two (three) 64-bit words.
+__device__ __forceinline__ uint64_t xorz_value(const uint64_t* xb, uint32_t o, uint32_t len) {
+  if (len <= 4) {
+    const uint32_t* x32 = reinterpret_cast<const uint32_t*>(xb);
+    uint32_t w = __funnelshift_r(x32[o >> 2], x32[(o >> 2) + 1], (o & 3) * 8);
+    if (len < 4) w &= (1u << (8 * len)) - 1u;
+    w = (w & 0x007F007Fu) | ((w >> 1) & 0x3F803F80u);
+    return (uint64_t)((w & 0x3FFFu) | ((w >> 2) & 0x0FFFC000u));
+  }
+  const uint32_t wi = o >> 3, sh = (o & 7) * 8;
+  uint64_t a = xb[wi], b = xb[wi + 1];
+  uint64_t w = sh ? (a >> sh) | (b << (64 - sh)) : a;
+  if (len < 8) w &= (1ull << (8 * len)) - 1ull;
+  w = (w & 0x007F007F007F007Full) | ((w >> 1) & 0x3F803F803F803F80ull);  // 14 bits per 16
+  w = (w & 0x00003FFF00003FFFull) | ((w >> 2) & 0x0FFFC0000FFFC000ull);  // 28 bits per 32
+  w = (w & 0x000000000FFFFFFFull) | ((w >> 4) & 0x00FFFFFFF0000000ull);  // 56 bits
+  if (len > 8) {
+    uint64_t c = xb[wi + 2];
+    uint64_t hi = sh ? (b >> sh) | (c << (64 - sh)) : b;  // the value's bytes 9 and 10
+    w |= (hi & 0x7Full) << 56;
+    if (len > 9) w |= (hi >> 8) << 63;
+  }
+  return w;
+}
+
+// The lane's values in order: XOR-prefix from the lane's start, stored at
+// stg[skew(before + k)] when STORE.  bad: an over-long value with index < n
+// (every index when n = ~0), or (STORE) value n-1 not ending at the last
+// payload byte.  Returns the XOR of the lane's values.  Positions are
+// relative to s0 (the lane's last terminator before it is at least s0 - 17).
+template <bool STORE>
+__device__ __forceinline__ uint64_t xorz_lane_values(const XLane& X, const uint64_t* xb, uint64_t s0,
+                                                     uint64_t* stg, uint64_t vbase, uint64_t n, uint64_t plen,
+                                                     uint32_t& bad) {
+  uint32_t m = X.tm, k = X.before;
+  const int32_t b0 = (int32_t)(X.b0 - s0);
+  int32_t prev = (int32_t)(X.prev - (int64_t)s0);
+  // the round index of value n-1 and the payload's last byte, when in the round
+  const int64_t kn = (int64_t)n - 1 - (int64_t)vbase;
+  const uint32_t klast = (kn >= 0 && kn < 4096) ? (uint32_t)kn : ~0u;
+  const int64_t el = (int64_t)plen - 1 - (int64_t)s0;
+  const int32_t elast = (el >= 0 && el < 4096) ? (int32_t)el : -1000;
+  const uint64_t lim = n > vbase ? n - vbase : 0;  // values with an index below n
+  uint64_t acc = 0;
+  while (m) {
+    uint32_t q = __ffs(m) - 1;
+    m &= m - 1u;
+    int32_t end = b0 + (int32_t)q;
+    int32_t len = end - prev;
+    if (len <= 10) {
+      acc ^= xorz_value(xb, (uint32_t)(prev + 17), (uint32_t)len);
+    } else if (k < lim) {
+      bad = 1;
+    }
+    if (STORE) {
+      stg[skew(k)] = acc;
+      if (k == klast && end != elast) bad = 1;
+    }
+    k++;
+    prev = end;
+  }
+  return acc;
 }
 
 __device__ inline uint32_t warp_or_u32(uint32_t v) {
@@ -2468,7 +2500,8 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_prepass(const uint8_t* _
                                                            const ItemRef* __restrict__ items, uint32_t nitems,
                                                            PreRec* __restrict__ pre, uint64_t* __restrict__ scratch,
                                                            BatchView bv) {
-  __shared__ uint32_t rle_stage[kItemWarps][kSub];
+  __shared__ __align__(16) uint32_t rle_stage[kItemWarps][kSub];  // XORZ: the round's byte buffer
+  static_assert(kSub * 4 >= kXorzBufWords * 8, "the XORZ buffer fits a warp's stage");
   uint32_t g = blockIdx.x * kItemWarps + (threadIdx.x >> 5);
   int l = threadIdx.x & 31;
   if (g >= nitems) return;
@@ -2519,17 +2552,20 @@ __global__ void __launch_bounds__(kItemWarps * 32, 6) k_prepass(const uint8_t* _
     for (int o = 16; o; o >>= 1) s = qmin(s + __shfl_xor_sync(0xffffffffu, s, o), n + 1);
     R.a = s;
   } else if (d.mode == M_XORZ) {
-    // the item's rounds of 512 payload bytes: contributions XOR, value count,
-    // last terminator, over-long flag, combined
+    // the item's rounds of 512 payload bytes: XOR of the values ending in
+    // the item, value count, last terminator, over-long flag
+    uint64_t* xb = reinterpret_cast<uint64_t*>(rle_stage[threadIdx.x >> 5]);
     uint64_t xo = 0;
     for (int r = 0; r < kXorzRounds; r++) {
       uint64_t s0 = (uint64_t)it.local * kXorzItemBytes + (uint64_t)r * kItemBytes;
       if (s0 >= d.plen) break;
-      XSlice X = xorz_lane_scan<true>(p, d.plen, s0);
-      xo ^= X.xo;
+      XLane X = xorz_round(p, d.plen, s0, xb);
+      uint32_t bad = 0;
+      xo ^= xorz_lane_values<false>(X, xb, s0, nullptr, 0, ~0ull, d.plen, bad);
       R.b += X.total;
       if (X.lastt > R.last) R.last = X.lastt;
-      R.flag |= warp_or_u32(X.bad);
+      R.flag |= warp_or_u32(bad);
+      __syncwarp();  // the buffer is reused by the next round
     }
     for (int o = 16; o; o >>= 1) xo ^= __shfl_xor_sync(0xffffffffu, xo, o);
     R.a = xo;
@@ -2611,6 +2647,7 @@ __global__ void __launch_bounds__(kItemWarps * 32, QB_ITEM_MIN_BLOCKS) k_decode_
                                                                 const uint64_t* __restrict__ scratch,
                                                                 unsigned long long* __restrict__ err, BatchView bv) {
   __shared__ __align__(16) uint64_t stage_all[kItemWarps][kItemStage];
+  __shared__ __align__(16) uint64_t xbuf_all[kItemWarps][kXorzBufWords];  // XORZ rounds' bytes
   int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
   uint32_t g = blockIdx.x * kItemWarps + warp;
   if (g >= nitems) return;
@@ -2782,15 +2819,17 @@ __global__ void __launch_bounds__(kItemWarps * 32, QB_ITEM_MIN_BLOCKS) k_decode_
     }
     case M_XORZ: {
       const PreRec& R = pre[frame_pre[it.frame].x + it.local];
-      uint64_t vbase = R.b, carry = R.a;
+      uint64_t vbase = R.b, carry = R.a;  // values before the item, the last one's value
+      uint64_t* xb = xbuf_all[warp];
       uint64_t pnext = ~0ull;  // the next round's first position (the last round's end)
       for (int rd = 0; rd < kXorzRounds; rd++) {
         uint64_t s0 = (uint64_t)it.local * kXorzItemBytes + (uint64_t)rd * kItemBytes;
         if (s0 >= d.plen) break;
-        XSlice X = xorz_lane_scan<false>(p, d.plen, s0);
-        // one pass from a zero state (values relative to the lane's start),
-        // then the lane's carry: the round's carry and the lanes before
-        uint64_t own = xorz_lane_bytes<true, true>(X, 0ull, stg, 0);
+        XLane X = xorz_round(p, d.plen, s0, xb);
+        uint32_t bad = 0;
+        // the lane's values relative to its start, then the carry of the
+        // values before: the item's, the earlier rounds' and lanes'
+        uint64_t own = xorz_lane_values<true>(X, xb, s0, stg, vbase, n, d.plen, bad);
         uint64_t inc = own;
         for (int o = 1; o < 32; o <<= 1) {
           uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
@@ -2800,16 +2839,6 @@ __global__ void __launch_bounds__(kItemWarps * 32, QB_ITEM_MIN_BLOCKS) k_decode_
         for (uint32_t q = 0; q < X.cnt; q++) stg[skew(X.before + q)] ^= base;
         carry ^= __shfl_sync(0xffffffffu, inc, 31);
         __syncwarp();
-        // checks on the values that exist (index < n): length, and the n-th
-        // value's terminator must be the payload's last byte
-        uint32_t bad = 0;
-        uint64_t lane0 = vbase + X.before;
-        if (X.first_bad != ~0u && lane0 + X.first_bad < n) bad = 1;
-        if (n && lane0 <= n - 1 && n - 1 < lane0 + X.cnt) {
-          uint32_t m = X.tm;
-          for (uint64_t q = n - 1 - lane0; q; q--) m &= m - 1u;
-          if ((int64_t)(X.b0 + (uint64_t)(__ffs(m) - 1)) != (int64_t)d.plen - 1) bad = 1;
-        }
         if (warp_or_u32(bad)) {
           e = E_CORRUPT;
           break;
@@ -2819,7 +2848,7 @@ __global__ void __launch_bounds__(kItemWarps * 32, QB_ITEM_MIN_BLOCKS) k_decode_
           warp_store_item(O, d.value_off + vbase, cnt, [&](uint32_t q) { return stg[skew(q)]; }, &pnext);
         }
         vbase += X.total;
-        __syncwarp();  // the staging buffer is reused by the next round
+        __syncwarp();  // the staging buffers are reused by the next round
       }
       break;
     }
