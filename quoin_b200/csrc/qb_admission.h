@@ -5,7 +5,8 @@
 // free at that moment (less a reserve); a request that alone exceeds the
 // budget is refused when it is submitted.  A head that fits the budget but
 // not the free memory waits (re-probing every few milliseconds) while other
-// requests run; with nothing running it is admitted anyway, so the queue
+// requests run; the probe is called outside the lock and its value reused
+// for a short while; with nothing running it is admitted anyway, so the queue
 // always moves (its allocations then fail or succeed on their own).
 // Host-only code (no CUDA; the probe is a plain function), so the policy is
 // testable on CPU.
@@ -48,16 +49,41 @@ class AdmissionQueue {
 
   // Blocks until the head request fits the budget, then removes it and counts
   // its bytes as in use.  False once the queue is closed and drained.
+  // The probe runs without the lock (it may wait inside the driver while
+  // running requests allocate or free), one caller at a time, and its value
+  // is reused for kProbeTtl less the bytes admitted since; it is only
+  // consulted again sooner when that estimate says the head does not fit.
   bool pop(T* item, uint64_t* bytes) {
     std::unique_lock<std::mutex> l(mu_);
     for (;;) {
-      cv_.wait(l, [&] { return (!q_.empty() && in_use_ + q_.front().second <= budget_) || (closed_ && q_.empty()); });
+      cv_.wait(l, [&] {
+        return (!q_.empty() && in_use_ + q_.front().second <= budget_ && !probing_) || (closed_ && q_.empty());
+      });
       if (q_.empty()) return false;
       if (!probe_ || in_use_ == 0) break;
+      const uint64_t need = q_.front().second;
+      const auto now = std::chrono::steady_clock::now();
+      if (have_probe_ && now - probed_at_ < kProbeTtl && in_use_ >= in_use_at_probe_) {
+        uint64_t since = in_use_ - in_use_at_probe_;
+        uint64_t est = free_at_probe_ > since ? free_at_probe_ - since : 0;
+        if (est > reserve_ && need <= est - reserve_) break;
+      }
+      probing_ = true;
+      l.unlock();
       uint64_t fr = probe_();
-      if (fr > reserve_ && q_.front().second <= fr - reserve_) break;
+      l.lock();
+      probing_ = false;
+      have_probe_ = true;
+      probed_at_ = std::chrono::steady_clock::now();
+      free_at_probe_ = fr;
+      in_use_at_probe_ = in_use_;
+      cv_.notify_all();
+      if (q_.empty()) continue;
+      if (in_use_ == 0 || (in_use_ + q_.front().second <= budget_ && fr > reserve_ && q_.front().second <= fr - reserve_))
+        break;
       waits_for_memory_++;
-      cv_.wait_for(l, std::chrono::milliseconds(5));  // memory frees as running requests end
+      have_probe_ = false;  // re-probe after the wait: memory frees as running requests end
+      cv_.wait_for(l, std::chrono::milliseconds(5));
     }
     *item = std::move(q_.front().first);
     *bytes = q_.front().second;
@@ -107,6 +133,10 @@ class AdmissionQueue {
   const uint64_t budget_;
   uint64_t in_use_ = 0, peak_ = 0, reserve_ = 0, waits_for_memory_ = 0;
   std::function<uint64_t()> probe_;
+  static constexpr std::chrono::milliseconds kProbeTtl{50};
+  bool probing_ = false, have_probe_ = false;
+  std::chrono::steady_clock::time_point probed_at_{};
+  uint64_t free_at_probe_ = 0, in_use_at_probe_ = 0;
   bool closed_ = false;
   std::deque<std::pair<T, uint64_t>> q_;
   mutable std::mutex mu_;
