@@ -68,7 +68,7 @@ __device__ inline bool dp_varint(const uint8_t* s, uint64_t pos, uint64_t lim, u
 // varint length no larger than the decode bound).  A frame that fails it
 // cannot decode, so leaving it out only sends damaged streams to the host
 // reader.
-__device__ bool dp_frame_plausible(const uint8_t* s, uint64_t pl0, uint32_t n, uint32_t plen, uint32_t mode,
+__device__ __noinline__ bool dp_frame_plausible(const uint8_t* s, uint64_t pl0, uint32_t n, uint32_t plen, uint32_t mode,
                                    uint32_t lane_bytes_) {
   uint64_t lim = pl0 + plen, v = 0;
   switch (mode) {
@@ -397,6 +397,32 @@ __device__ __forceinline__ uint32_t bytes_within(uint32_t x) {
   return ~(t | (x & kClear) | 0x7F7F7F7Fu);
 }
 
+// The candidates among survivor positions m (bit i: position a + i passed
+// the byte tests): mode id, n and plen ranges, then the mode's first decode
+// checks.  Out of line: survivors are rare, and one copy of this code keeps
+// the scan loop small.
+__device__ __noinline__ uint32_t dp_check_survivors(const uint8_t* __restrict__ s, const DpLane& L, uint64_t a,
+                                                    uint32_t m, uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3,
+                                                    uint32_t x4, uint32_t x5) {
+  const uint32_t x[6] = {x0, x1, x2, x3, x4, x5};
+  const uint64_t end = L.base + L.len;
+  const uint32_t lb = lane_bytes((int)L.dtype);
+  uint32_t out = 0;
+  while (m) {
+    uint32_t i = __ffs(m) - 1;
+    m &= m - 1;
+    uint32_t k = i >> 2, j = i & 3;
+    uint32_t h0 = __funnelshift_r(x[k], x[k + 1], 8 * j);      // mode, n (low 3 bytes)
+    uint32_t h1 = __funnelshift_r(x[k + 1], x[k + 2], 8 * j);  // byte +4 (zero), plen (3 bytes)
+    uint32_t mode = h0 & 0xFF, n = h0 >> 8, plen = h1 >> 8;
+    uint64_t p = a + i;
+    if (((kCandModes >> mode) & 1) && n >= 1 && n <= (uint32_t)kMaxBlock && plen <= end - p - 9 &&
+        dp_frame_plausible(s, p + 9, n, plen, mode, lb))
+      out |= 1u << i;
+  }
+  return out;
+}
+
 __device__ inline uint32_t dp_thread_cands(const uint8_t* __restrict__ s, const DpLane& L, uint64_t a,
                                            const DpWin& W) {
   const uint64_t end = L.base + L.len;
@@ -415,36 +441,19 @@ __device__ inline uint32_t dp_thread_cands(const uint8_t* __restrict__ s, const 
   uint32_t z[6];
 #pragma unroll
   for (int k = 0; k < 6; k++) z[k] = bytes_within<0>(x[k]);
-  uint32_t mk[4], any = 0;
+  uint32_t m = 0;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    mk[k] = bytes_within<0x3F>(x[k]) & ~z[k] & z[k + 1] & z[k + 2];
-    any |= mk[k];
+    uint32_t f = bytes_within<0x3F>(x[k]) & ~z[k] & z[k + 1] & z[k + 2];  // bits 7, 15, 23, 31
+    m |= (((f >> 7) & 1u) | ((f >> 14) & 2u) | ((f >> 21) & 4u) | ((f >> 28) & 8u)) << (4 * k);
   }
-  if (!any) return 0;
+  if (!m) return 0;
   const uint32_t lo = a < L.fstart ? (uint32_t)(L.fstart - a) : 0u;  // first position in range
   const uint64_t last = end - 9;
   const uint32_t hi = a + 15 > last ? (uint32_t)(last - a) : 15u;   // last position in range
-  uint32_t lb = lane_bytes((int)L.dtype);
-  uint32_t out = 0;
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    uint32_t m = mk[k];
-    while (m) {
-      uint32_t j = (uint32_t)(__ffs(m) - 1) >> 3;
-      m &= m - 1;
-      uint32_t i = 4 * k + j;
-      if (i < lo || i > hi) continue;
-      uint32_t h0 = __funnelshift_r(x[k], x[k + 1], 8 * j);      // mode, n (low 3 bytes)
-      uint32_t h1 = __funnelshift_r(x[k + 1], x[k + 2], 8 * j);  // byte +4 (zero), plen (3 bytes)
-      uint32_t mode = h0 & 0xFF, n = h0 >> 8, plen = h1 >> 8;
-      uint64_t p = a + i;
-      if (((kCandModes >> mode) & 1) && n >= 1 && n <= (uint32_t)kMaxBlock && plen <= end - p - 9 &&
-          dp_frame_plausible(s, p + 9, n, plen, mode, lb))
-        out |= 1u << i;
-    }
-  }
-  return out;
+  m &= (0xFFFFu << lo) & ((2u << hi) - 1u);
+  if (!m) return 0;
+  return dp_check_survivors(s, L, a, m, x[0], x[1], x[2], x[3], x[4], x[5]);
 }
 
 __device__ __forceinline__ DpCand dp_cand_at(const uint8_t* __restrict__ s, uint64_t p) {
