@@ -59,9 +59,10 @@ WORKLOADS = {
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per decode
-# phase of the workload's three columns, from a one-kernel ncu capture scaled
-# to the bench's column length; None until captured for the current kernels.
-DECODE_TRAFFIC = {}
+# phase of the workload's three columns at the default 67,108,864 values per
+# column: a one-pass ncu capture of every decode launch at 16,777,216 values
+# per column (562.9 MB), scaled by the values processed (x4).
+DECODE_TRAFFIC = {"integer-lanes": 2_251_622_400}
 
 
 DECIMAL128_WIRE = 6  # wire dtype id of Decimal128 (reference src/dtype.rs:68-93)
@@ -578,9 +579,11 @@ def run_gpu(args, rank, world, local):
                                                    "k_decimal_combine) of the three columns in flight together",
                          "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": DECODE_TRAFFIC.get(args.workload),
-                         "traffic_note": ("DRAM bytes per decode phase (three decode calls) from ncu captures"
-                                          if args.workload in DECODE_TRAFFIC else "not captured for these kernels"),
+                         "traffic": DECODE_TRAFFIC.get(args.workload) if n == N_DEFAULT else None,
+                         "traffic_note": ("DRAM bytes per decode phase (three decode calls): a one-pass ncu capture "
+                                          "at 16,777,216 values per column scaled x4"
+                                          if args.workload in DECODE_TRAFFIC and n == N_DEFAULT
+                                          else "not captured for this workload and size"),
                          "decode_calls_per_step": per_class["decode"][1] // max(args.steps, 1)},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
