@@ -149,7 +149,6 @@ struct DictArea {
   uint64_t hkey[kHashCap];
   uint32_t hval[kHashCap];
   uint64_t sorted[kHashCap];
-  uint32_t lb[kLbBits / 32];
 };
 struct RleArea {
   uint32_t starts[kRunsSmem];
@@ -699,10 +698,10 @@ __device__ inline int rd_code(const EncSmem& S, uint64_t left) {
 // buffer that holds the sorted keys.  All threads of a kEncThreads CTA; the
 // per-warp digit counters live in the dictionary smem area.
 __device__ uint64_t* block_radix_sort(EncSmem& S, uint64_t* a, uint64_t* b, uint32_t m) {
-  static_assert(kEncThreads >= 256 && kEncWarps * 256 * 4 <= sizeof(S.big.dict.sorted) + sizeof(S.big.dict.lb),
+  static_assert(kEncThreads >= 256 && kEncWarps * 256 * 4 <= sizeof(S.big.dict.sorted),
                 "one thread per digit in the offset scan; per-warp digit counters fit the dictionary area");
-  // per-warp digit counters [kEncWarps][256] over the sorted-keys and
-  // lower-bound arrays of the dictionary area (neither is in use here)
+  // per-warp digit counters [kEncWarps][256] over the sorted-keys array of
+  // the dictionary area (not in use here)
   uint32_t* hist = reinterpret_cast<uint32_t*>(S.big.dict.sorted);
   int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   uint64_t k0 = m ? a[0] : 0ull, diff = 0;
@@ -861,8 +860,6 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
     D.hkey[i] = kEmpty64;
     D.hval[i] = 0;
   }
-  if (!have_lb)
-    for (uint32_t i = threadIdx.x; i < kLbBits / 32; i += blockDim.x) D.lb[i] = 0;
   if (threadIdx.x == 0) {
     S.ovf = 0;
     S.card = 0;
@@ -870,23 +867,15 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
     S.flag = 0;
   }
   __syncthreads();
+  // the shared-memory hash until it holds kHashLimit keys; the lower-bound
+  // bitset is only built (below) for a block that overflows it
   for (uint32_t base = 0; base < n; base += blockDim.x * 8) {
+    if (*(volatile uint32_t*)&S.ovf) break;
     uint64_t xs[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
       uint32_t iq = base + q * blockDim.x + threadIdx.x;
       xs[q] = iq < n ? v[iq] : 0ull;
-    }
-    if (!have_lb) {
-#pragma unroll
-      for (int q = 0; q < 8; q++) {
-        if (base + q * blockDim.x + threadIdx.x < n) {
-          uint32_t b = dict_lb_bucket(xs[q]);
-          atomicOr(&D.lb[b >> 5], 1u << (b & 31));
-        }
-      }
-    } else if (*(volatile uint32_t*)&S.ovf) {
-      break;
     }
 #pragma unroll
     for (int q = 0; q < 8; q++)
@@ -924,21 +913,48 @@ __device__ DictView dict_prepare(EncSmem& S, const uint64_t* v, uint32_t n, uint
     dv.card = card;
     return dv;
   }
-  // Overflow: the lower-bound bitset may prove the bail outright.
-  if (have_lb) {
-    if (threadIdx.x == 0) S.cnt32 = lb_pre;
-    __syncthreads();
-  } else {
-    uint32_t lbc = 0;
-    for (uint32_t i = threadIdx.x; i < kLbBits / 32; i += blockDim.x) lbc += __popc(D.lb[i]);
-    lbc = warp_sum(lbc);
-    if ((threadIdx.x & 31) == 0) S.red32[threadIdx.x >> 5] = lbc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
+  // Overflow: a lower bound on the cardinality may prove the bail outright:
+  // the window's 17-bit bucket count when the statistics pass computed it,
+  // and, when that does not prove it, the distinct buckets of a 2^20-bit set
+  // (fewer for a short block) built in the block's scratch range with
+  // fire-and-forget atomics, whose collisions stay few at any cardinality
+  // near the bail threshold.
+  {
+    uint32_t lb = have_lb ? lb_pre : 0u;
+    if (lb <= max_card) {
+      uint32_t lgb = 20;
+      while (lgb > 10 && (1ull << (lgb - 3)) > (uint64_t)n * kEncScratchPerValue) lgb--;
+      const uint32_t words = (1u << lgb) / 32;
+      uint32_t* bits = reinterpret_cast<uint32_t*>(scratch);
+      for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bits[i] = 0;
+      __syncthreads();
+      for (uint32_t base = 0; base < n; base += blockDim.x * 8) {
+        uint64_t xs[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          uint32_t iq = base + q * blockDim.x + threadIdx.x;
+          xs[q] = iq < n ? v[iq] : 0ull;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          if (base + q * blockDim.x + threadIdx.x < n) {
+            uint32_t h = (uint32_t)((xs[q] * 0xD6E8FEB86659FD93ull) >> (64 - lgb));
+            atomicOr(&bits[h >> 5], 1u << (h & 31));
+          }
+        }
+      }
+      __syncthreads();
+      uint32_t c = 0;
+      for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) c += __popc(bits[i]);
+      c = warp_sum(c);
+      if ((threadIdx.x & 31) == 0) S.red32[threadIdx.x >> 5] = c;
+      __syncthreads();
       uint32_t t = 0;
       for (int w = 0; w < kEncWarps; w++) t += S.red32[w];
-      S.cnt32 = t;
+      lb = t > lb ? t : lb;
     }
+    __syncthreads();
+    if (threadIdx.x == 0) S.cnt32 = lb;
     __syncthreads();
   }
   if (S.cnt32 > max_card) {
@@ -2610,19 +2626,15 @@ __device__ void emit_dict(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* sc
   block_for(S, out + pos + 1, n, false, [&](uint32_t i) { return (uint64_t)dict_rank(S, dv, v[i]); });
 }
 
-__device__ void emit_rle(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scr, uint8_t* out) {
-  // transitions per sub-block (the competition's counts are not kept)
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// The block's run starts from its transitions per sub-block, which the
+// statistics pass counted: the sub-block's own plus its first value against
+// the previous sub-block's last (as the competition counts them).
+__device__ void emit_rle(EncSmem& S, const uint64_t* v, uint32_t n, const SubStats* ss, uint8_t* scr,
+                         uint8_t* out) {
   uint32_t nsub = (n + kSub - 1) / kSub;
-  for (uint32_t k = warp; k < nsub; k += kEncWarps) {
-    uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
-    uint32_t nq = 0;
-    for (uint32_t i = lane; i < cnt; i += 32) {
-      uint32_t idx = base + i;
-      nq += (idx && v[idx] != v[idx - 1]) ? 1u : 0u;
-    }
-    nq = warp_sum(nq);
-    if (lane == 0) S.neq_k[k] = nq;
+  for (uint32_t k = threadIdx.x; k < nsub; k += blockDim.x) {
+    const SubStats& R = ss[k];
+    S.neq_k[k] = R.neq + ((k && R.first != ss[k - 1].last) ? 1u : 0u);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -2741,7 +2753,7 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
     case M_ALP: emit_alp(S, v, n, ss ? ss + g0 : nullptr, out); break;
     case M_ALP_RD: emit_alprd(S, v, n, fd.aux, scr, out, erp); break;
     case M_DICT: emit_dict(S, v, n, scr, out, erp); break;
-    case M_RLE: emit_rle(S, v, n, scr, out); break;
+    case M_RLE: emit_rle(S, v, n, ss + g0, scr, out); break;
     default: break;
   }
 }
