@@ -643,12 +643,18 @@ __device__ FrameItems dp_frame_items(const uint8_t* p, uint64_t n, uint64_t plen
       r.scan = true;
       break;
     }
-    case 52: {
+    case 52: {  // one walk of the exception list gives both the items and the entropy rule
       uint64_t nexc = 1;
       uint32_t ct = 1, rt = 1;
-      if (dp_alprd_tags(p, plen, &nexc, &ct, &rt) && nexc == 0 && ct == 0 && rt == 0) r.nmain = nv;
-      else r.list = true;
-      break;
+      bool ok = dp_alprd_tags(p, plen, &nexc, &ct, &rt);
+      r.dict = true;
+      if (ok && nexc == 0 && ct == 0 && rt == 0) {
+        r.nmain = nv;
+      } else {
+        r.list = true;
+        if (!ok || ct == 1 || rt == 1) r.ent = ent_area_bytes(n, mode, plog2);
+      }
+      return r;
     }
     default:
       r.list = true;
@@ -767,18 +773,37 @@ __global__ void __launch_bounds__(kChainThreads) k_dp_marks(const DpHead* __rest
   }
 }
 
+// An ALP-RD frame's exception list (records of a varint position and an
+// 8-byte left part) is walked record by record, each read depending on the
+// one before; the warp first pulls the list's cache lines into L1 so that the
+// walk's reads hit there.
+__device__ __forceinline__ void dp_warp_prefetch_alprd(const uint8_t* p, uint64_t plen, uint32_t mode) {
+  if (mode != 52 || plen < 2) return;
+  const int l = threadIdx.x & 31;
+  uint64_t pos = 2 + 8ull * p[1], nexc = 0;
+  if (pos > plen || rd_varint(p, plen, &pos, &nexc) != E_OK) return;
+  uint64_t end = nexc > plen ? plen : qmin(plen, pos + 18 * nexc + 32);
+  for (uint64_t o = pos + 128ull * l; o < end; o += 128ull * 32)
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p + o));
+}
+
 // The warp items of every marked candidate (dp_frame_items), across the GPU:
-// nodes[j] for the j-th marked candidate, its candidate index in .succ.
+// nodes[j] for the j-th marked candidate, its candidate index in .succ.  One
+// warp per frame: the prefetch above, then lane 0 counts the items.
 __global__ void k_dp_items(const uint8_t* __restrict__ s, const DpHead* __restrict__ H, int lane,
                            const DpCand* __restrict__ cand, const uint32_t* __restrict__ fidx,
                            const uint64_t* __restrict__ ctl, DpNode* __restrict__ nodes) {
   if (!ctl[0]) return;
   uint64_t F = ctl[1];
   uint32_t plog2 = H->lanes[lane].plog2;
-  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < F; j += (uint64_t)gridDim.x * blockDim.x) {
+  const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t j = w0; j < F; j += nw) {
     uint32_t i = fidx[j];
     DpCand c = cand[i];
-    FrameItems it = dp_frame_items(s + c.pos + 9, c.n, c.plen_mode >> 8, c.plen_mode & 0xFF, plog2);
+    const uint8_t* p = s + c.pos + 9;
+    dp_warp_prefetch_alprd(p, c.plen_mode >> 8, c.plen_mode & 0xFF);
+    if ((threadIdx.x & 31) != 0) continue;
+    FrameItems it = dp_frame_items(p, c.n, c.plen_mode >> 8, c.plen_mode & 0xFF, plog2);
     DpNode d;
     d.succ = i;
     d.nmain = it.nmain;
@@ -1288,13 +1313,16 @@ __global__ void __launch_bounds__(1024) k_dpb_lane_scan(DpBatch B, int mode) {
 __global__ void k_dpb_items(DpBatch B) {
   uint64_t K = B.cnt[B.chunks];
   if (K > B.cap) return;
-  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < K; j += (uint64_t)gridDim.x * blockDim.x) {
+  const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t j = w0; j < K; j += nw) {  // one warp per slot, as k_dp_items
     int c = (int)B.cand_lane[j];
     uint64_t lo = B.cnt[B.chunk0[c]];
     if (j - lo >= B.out[c].nmarked) continue;
     const DpBLane& Ln = B.lanes[c];
     uint64_t i = lo + B.flist[j];
     DpCand cd = B.cand[i];
+    dp_warp_prefetch_alprd(Ln.s + cd.pos + 9, cd.plen_mode >> 8, cd.plen_mode & 0xFF);
+    if ((threadIdx.x & 31) != 0) continue;
     FrameItems it = dp_frame_items(Ln.s + cd.pos + 9, cd.n, cd.plen_mode >> 8, cd.plen_mode & 0xFF, Ln.L.plog2);
     DpNode d;
     d.succ = (uint32_t)(i - lo);
