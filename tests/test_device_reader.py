@@ -96,6 +96,15 @@ def decimal_bytes(v, width=16):
     return out
 
 
+def prices_with_exceptions(rng, n, frac=0.03):
+    v = np.floor(rng.random(n) * 1_000_000 + 0.5) / 100.0
+    bits = rng.integers(0, 1 << 62, n, dtype=np.int64).view(np.uint64) | (rng.integers(0, 2, n).astype(np.uint64) << np.uint64(63))
+    bits = bits & ~(np.uint64(0x7FF) << np.uint64(52)) | (rng.integers(0, 0x7FF, n).astype(np.uint64) << np.uint64(52))
+    pick = rng.random(n) < frac
+    v[pick] = bits[pick].view(np.float64)
+    return v
+
+
 def reader_cases():
     rng = np.random.default_rng(4321)
     vb = rng.random(300_000) > 0.1
@@ -123,6 +132,9 @@ def reader_cases():
         ("rle_blob_leading_valid", np.arange(5000, dtype=np.int64), I64,
          bitmap_from_bools(np.arange(5000) < 4000), {}),
         ("prices_alp", np.floor(rng.random(200_000) * 1_000_000 + 0.5) / 100.0, F64, None, {}),
+        # two-decimal prices with 3 % random-bit values: ALP-RD frames with
+        # about a thousand exceptions each, whose lists the reader walks
+        ("prices_alprd_exceptions", prices_with_exceptions(rng, 200_000), F64, None, {}),
         ("walk_f64", 20.0 + np.cumsum(rng.normal(0, 1e-3, 200_000)), F64, None, {}),
         ("sensor_f32", (np.round(rng.normal(25, 5, 200_000) * 10) / 10).astype(np.float32), F32, None, {}),
         ("xorz_f64", np.sin(np.arange(100_000) * 1e-4), F64, None, {}),
