@@ -45,6 +45,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "encode+decode GB/s (uncompressed bytes; Level::Fast, bit-exact round trip)"
+# --level: (C-ABI level id, oracle level id, name in the metric) for the
+# single-column workloads; Fast is the headline.
+LEVELS = {"fastest": (0, 0, "Fastest"), "fast": (1, 1, "Fast"), "balanced-inpool": (258, 2, "Balanced-in-pool")}
+
+
+def metric_for(level: str) -> str:
+    return METRIC.replace("Level::Fast", "Level::" + LEVELS[level][2])
 N_DEFAULT = 67_108_864
 N_PRICES = 1_048_576  # the prices column's length
 L2_FLUSH_BYTES = 256 << 20  # written between timed phases when the inputs fit the 126 MB L2
@@ -188,7 +195,7 @@ def whole_job_gbs(bytes_per_rank, world, steps, seconds):
 # ---------------------------------------------------------------------------
 # Reference arm: the reference's CPU algorithm (C restatement) on host cores.
 # ---------------------------------------------------------------------------
-def cpu_reference_run(cols, threads: int, sample: int):
+def cpu_reference_run(cols, threads: int, sample: int, level: int = 1):
     from oracle import oracle as O
     enc_s = dec_s = 0.0
     nbytes = 0
@@ -197,7 +204,7 @@ def cpu_reference_run(cols, threads: int, sample: int):
         bs = None if bm is None else bm[: (sample + 7) // 8]
         t0 = time.perf_counter()
         sc, pr = decimal_args(dt)
-        s = O.compress_column(vs, dt, bs, level=O.LEVEL_FAST, scale=sc, precision=pr, threads=threads)
+        s = O.compress_column(vs, dt, bs, level=level, scale=sc, precision=pr, threads=threads)
         t1 = time.perf_counter()
         O.decompress_column(s, threads=threads)
         t2 = time.perf_counter()
@@ -211,6 +218,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return 0
     synth = load_synth()
+    olevel = LEVELS[args.level][1]
     threads = os.cpu_count() or 1
     # the GPU arm's workload: whole columns (batched / served: an equal share
     # of --cpu-sample per column)
@@ -226,14 +234,15 @@ def run_reference(args, rank, world):
               "mixed (f64/f32/i64/u64/i32/u32/decimal128)")
     else:
         wl = WORKLOADS[args.workload]
+        wl = (wl[0], wl[1].replace("Level::Fast", "Level::" + LEVELS[args.level][2]), wl[2])
         cols = synth.benchmark_columns(wl[0], sample)
     for _ in range(args.warmup):
-        cpu_reference_run(cols, threads, sample)
+        cpu_reference_run(cols, threads, sample, olevel)
     tot_b = 0
     tot_s = 0.0
     e_s = d_s = 0.0
     for _ in range(args.steps):
-        b, e, d = cpu_reference_run(cols, threads, sample)
+        b, e, d = cpu_reference_run(cols, threads, sample, olevel)
         tot_b += b
         tot_s += e + d
         e_s += e
@@ -243,9 +252,9 @@ def run_reference(args, rank, world):
     # all-core figure
     one = max(min(args.single_thread_sample, sample), 1)
     cols1 = [(nm, dt, v[:one], None if bm is None else bm[: (min(len(v), one) + 7) // 8]) for nm, dt, v, bm in cols]
-    b1, e1, d1 = cpu_reference_run(cols1, 1, one)
+    b1, e1, d1 = cpu_reference_run(cols1, 1, one, olevel)
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(gbs, 4), "unit": "GB/s", "n_gpus": world,
+        "impl": "reference", "metric": metric_for(args.level), "value": round(gbs, 4), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot_s / args.steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl[2],
         "data": "synthetic",
@@ -284,6 +293,7 @@ def run_gpu(args, rank, world, local):
     dev = torch.device("cuda", local)
     n = args.n
     wl = WORKLOADS[args.workload]
+    wl = (wl[0], wl[1].replace("Level::Fast", "Level::" + LEVELS[args.level][2]), wl[2])
     cols = synth.benchmark_columns(wl[0], n)
     L = Q.lib
     # One context (CUDA stream + device arenas) and one host thread per column:
@@ -292,7 +302,7 @@ def run_gpu(args, rank, world, local):
     ctxs = [ctypes.c_void_p(L.quoin_ctx_create(0)) for _ in cols]
     stream, ctx = streams[0], ctxs[0]
     pool = ThreadPoolExecutor(max_workers=len(cols))
-    cfg = Q._QuoinConfig(int(Q.Level.FAST), 0, 16)
+    cfg = Q._QuoinConfig(LEVELS[args.level][0], 0, 16)
     P = ctypes.c_void_p
 
     gcols = []
@@ -574,7 +584,7 @@ def run_gpu(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         sample = args.cpu_sample
-        runs = [cpu_reference_run(cols, threads, sample) for _ in range(3)]
+        runs = [cpu_reference_run(cols, threads, sample, LEVELS[args.level][1]) for _ in range(3)]
         gb = sorted(b / (e + d) / 1e9 for b, e, d in runs)[1]
         cpu = {"value": round(gb, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                "sample": f"first {sample} values of each column (of {n}), oracle C restatement, {threads} threads, "
@@ -582,7 +592,8 @@ def run_gpu(args, rank, world, local):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "metric": metric_for(args.level), "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": wl[2], "data": "synthetic",
             "config": {"workload": wl[1], "values_per_column": n, "columns": len(gcols),
@@ -996,6 +1007,8 @@ def main():
     ap.add_argument("--workload", default="integer-lanes",
                     choices=["integer-lanes", "float-lanes", "prices", "batched", "served"],
                     help="batched: many uneven columns (plain vs batch calls); served: the request stream")
+    ap.add_argument("--level", default="fast", choices=list(LEVELS),
+                    help="single-column workloads: compression level (Fast is the headline)")
     ap.add_argument("--columns", type=int, default=256, help="batched: number of columns")
     ap.add_argument("--max-len", type=int, default=1 << 21, help="batched: longest column")
     ap.add_argument("--workers", type=int, default=8, help="batched / served: contexts in the batch / server")
@@ -1003,6 +1016,8 @@ def main():
     ap.add_argument("--max-bytes", type=int, default=256 << 20, help="served: largest column")
     ap.add_argument("--requests", type=int, default=600, help="served: requests per offered load")
     args = ap.parse_args()
+    if args.level != "fast" and args.workload in ("batched", "served"):
+        ap.error("--level applies to the single-column workloads")
     if args.n is None:
         args.n = N_PRICES if args.workload == "prices" else N_DEFAULT
     rank, world, local = dist_env()
