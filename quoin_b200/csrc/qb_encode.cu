@@ -164,6 +164,7 @@ struct RansArea {
   uint2 fc[256];                    // (frequency, cumulative frequency) per symbol
   uint8_t buf[2][kRansChunk];       // double-buffered input bytes
   uint32_t hdr, emitted;
+  uint32_t bound;  // a lower bound on the coded bytes (rans_plan)
 };
 
 struct EncSmem {
@@ -1222,8 +1223,22 @@ __device__ uint32_t rans_plan(RansArea& R, uint32_t m, B byte_at) {
     }
 #pragma unroll
     for (int j = 0; j < 8; j++) R.fc[lane + 32 * j].x = f[j];
+    // A lower bound on the coded bytes: any static model codes the sequence
+    // in at least its empirical entropy (Gibbs), and a byte-renormalising
+    // four-state coder emits at most 32 bits less (the states' growth from
+    // 2^23 to below 2^31) and loses under 2^-11 bits a symbol to the state
+    // rounding; a margin of 64 bits covers the floating-point sum.
+    double e = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      uint32_t c = R.hist[lane + 32 * j];
+      if (c) e += (double)c * log2((double)m / (double)c);
+    }
+    for (int o = 16; o; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    double bits = e * (1.0 - 1e-9) - 0.001 * (double)m - 96.0;
     __syncwarp();
     if (lane == 0) {
+      R.bound = bits > 0.0 ? (uint32_t)(bits / 8.0) : 0u;
       uint32_t c = 0, present = 0, h = 0;
       for (int sym = 0; sym < 256; sym++) {
         uint32_t fs = R.fc[sym].x;
@@ -1346,8 +1361,13 @@ __device__ uint32_t rans_run(RansArea& R, uint32_t m, B byte_at, uint8_t* wend) 
 // Length of code_residuals(byte_at(0 .. m)) with the rANS tag: the coded part
 // entropy_pick keeps at lambda >= 2 (m > 0).
 template <class B>
-__device__ uint32_t coded_len(RansArea& R, uint32_t m, B byte_at) {
+// Callers only ask whether the length is below `limit`: when the entropy
+// bound already reaches it, the serial sizing pass is skipped and a length at
+// or above the limit (the bound) comes back.
+__device__ uint32_t coded_len(RansArea& R, uint32_t m, B byte_at, uint64_t limit = ~0ull) {
   uint32_t h = rans_plan(R, m, byte_at);
+  uint32_t lo = 1 + h + 16 + R.bound;  // uniform: R is read after rans_plan's barrier
+  if ((uint64_t)lo >= limit) return lo;
   return 1 + h + 16 + rans_run<false>(R, m, byte_at, nullptr);
 }
 
@@ -2089,7 +2109,7 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
       c_fm.len = 2 + vl + tot;
       if (ENT) {  // FM_ENTROPY, kept when strictly smaller (float_mult.rs:80-92)
         uint32_t m = fm_delta_bytes(S, v, n, (int)fm_scale, scr);
-        uint32_t el = coded_len(S.ra, m, [&](uint32_t i) { return (uint32_t)scr[i]; });
+        uint32_t el = coded_len(S.ra, m, [&](uint32_t i) { return (uint32_t)scr[i]; }, c_fm.len - 2);
         if (el < c_fm.len - 2) {
           c_fm.len = 2 + el;
           er.flags |= kEntFm;
@@ -2173,7 +2193,7 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
         uint32_t cl = coded_len(S.ra, n, [&](uint32_t i) {
           int c = rd_code(S, v[i] >> rbw);
           return (uint32_t)(c < 0 ? 0 : c);
-        });
+        }, clen);
         if (cl < clen) {
           clen = cl;
           er.flags |= kEntRdCodes;
@@ -2181,7 +2201,7 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
         }
         uint8_t* rdst = stage_dst(S, scr, n, rlen);
         uint32_t rb = (uint32_t)block_for(S, rdst, n, false, [&](uint32_t i) { return v[i] & rmask; });
-        uint32_t rl = coded_len(S.ra, rb, [&](uint32_t i) { return (uint32_t)rdst[i]; });
+        uint32_t rl = coded_len(S.ra, rb, [&](uint32_t i) { return (uint32_t)rdst[i]; }, rlen);
         if (rl < rlen) {
           rlen = rl;
           er.flags |= kEntRdRights;
@@ -2246,10 +2266,12 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
     __syncthreads();
     bool repeats = (uint64_t)(n - S.neq) * 2 > (uint64_t)n;
     if (S.exp_hi - S.exp_lo <= 64 || repeats) {
+      // BYTE_TRANSPOSE wins only below best_score less its decode penalty
+      uint64_t pen = (lambda * decode_weight(M_BYTE_TRANSPOSE) * decoded_bytes) >> 8;
       uint32_t bl = coded_len(S.ra, 8 * n, [&](uint32_t i) {
         uint32_t pl = i / n;
         return (uint32_t)(v[i - pl * n] >> (8 * pl)) & 255u;
-      });
+      }, best_score > pen ? best_score - pen : 0ull);
       er.bt = bl;
       consider(M_BYTE_TRANSPOSE, bl);
     }
@@ -2272,7 +2294,7 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
         uint32_t tl = coded_len(S.ra, 8 * card, [&](uint32_t i) {
           uint32_t pl = i / card;
           return (uint32_t)(sv[i - pl * card] >> (8 * pl)) & 255u;
-        });
+        }, vlen);
         if (tl < vlen) {
           vlen = tl;
           vtag = 2;
@@ -2296,7 +2318,8 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
         uint64_t el = 1;
         uint32_t pls[2] = {0, 0};
         for (uint32_t pl = 0; pl < nb; pl++) {
-          pls[pl] = coded_len(S.ra, n, [&](uint32_t i) { return (dict_rank(S, dv, v[i]) >> (8 * pl)) & 255u; });
+          pls[pl] = coded_len(S.ra, n, [&](uint32_t i) { return (dict_rank(S, dv, v[i]) >> (8 * pl)) & 255u; },
+                              clen);
           el += varint_len(pls[pl]) + pls[pl];
         }
         if (el < clen) {
