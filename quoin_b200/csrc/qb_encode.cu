@@ -2283,6 +2283,11 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
     bool one_win = !fixed_bs && (fd.value_off % kBaseQuantum) == 0 && n <= (uint32_t)kBaseQuantum;
     uint32_t lb_pre = one_win ? winbits[(fd.value_off / kBaseQuantum) * kWinWords + 1024] : kNoLb;
     bool want_dict = !SAMPLE || win == M_DICT;
+    // A DICT payload holds at least 22 bytes (card, value tag and length, 8
+    // value bytes, code tag, varint(n) and one 9-byte sub-block header): when
+    // that and DICT's decode penalty already reach the best score, it cannot
+    // win (strict <) and its passes are skipped.
+    if (!SAMPLE && best_score <= 22 + ((lambda * decode_weight(M_DICT) * decoded_bytes) >> 8)) want_dict = false;
     DictView dv;
     if (want_dict) dv = dict_prepare(S, v, n, scr, lb_pre);
     if (want_dict && !S.flag) {
@@ -2334,7 +2339,11 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
     __syncthreads();
     // RLE (rle.rs:10-42)
     uint32_t neq = S.neq;
-    if ((!SAMPLE || win == M_RLE) && neq <= n / 2 + 1) {
+    // likewise RLE's floor: the run values and two varint(runs) plus a 9-byte
+    // header per 1,024 run lengths
+    const uint64_t rle_floor = 2 * varint_len(neq + 1) + 8ull * (neq + 1) + 9ull * ((neq + 1 + kSub - 1) / kSub) +
+                               ((lambda * decode_weight(M_RLE) * decoded_bytes) >> 8);
+    if ((!SAMPLE || win == M_RLE) && neq <= n / 2 + 1 && (SAMPLE || best_score > rle_floor)) {
       uint32_t runs = neq + 1;
       uint32_t* st = rle_starts(S, v, n, runs, scr);
       uint64_t lens = block_for(S, nullptr, runs, false, [&](uint32_t r) {
