@@ -2143,6 +2143,44 @@ __global__ void __launch_bounds__(kEncThreads) k_decide(const uint64_t* __restri
     rd_lbw = (SAMPLE && win != M_ALP_RD) ? 0u
                                          : rd_choose_cut(S, v, n, pre_s ? smp16 + fd.value_off / 16 : nullptr,
                                                          step / 16);
+    if (rd_lbw && !SAMPLE && !ENT) {
+      // The rights' FoR size is exact from one cheap pass (each sub-block's
+      // range of x & rmask); with the smallest possible rest of the payload
+      // (a 2-byte header, varint(nexc), the tags and lengths, one 9-byte
+      // header per code sub-block) and ALP-RD's decode penalty, it may
+      // already reach the best score of the candidates sized so far, and
+      // ALP-RD cannot win (strict <): its dictionary and exception passes are
+      // skipped.
+      uint32_t rbw = 64 - rd_lbw;
+      uint64_t rmask = (1ull << rbw) - 1ull;
+      if (t == 0) S.acc64 = 0;
+      __syncthreads();
+      for (uint32_t k = warp; k < nsub; k += kEncWarps) {
+        uint32_t base = k * kSub, cnt = min((uint32_t)kSub, n - base);
+        uint64_t rmn = kEmpty64, rmx = 0;
+        for (uint32_t i = lane_id; i < cnt; i += 32) {
+          uint64_t r = v[base + i] & rmask;
+          rmn = u64min(rmn, r);
+          rmx = u64max(rmx, r);
+        }
+        rmn = warp_min(rmn);
+        rmx = warp_max(rmx);
+        if (lane_id == 0) atomicAdd(&S.acc64, (unsigned long long)(9 + 128ull * bit_width64(rmx - rmn)));
+      }
+      __syncthreads();
+      uint64_t floor_len = 6 + 2 * vl + 9ull * nsub + S.acc64;
+      uint64_t best = decoded_bytes + ((lambda * decode_weight(M_RAW) * decoded_bytes) >> 8);
+      auto sc_of = [&](int m, uint64_t len) { return len + ((lambda * decode_weight(m) * decoded_bytes) >> 8); };
+      if (S.umin == S.umax) best = u64min(best, sc_of(M_CONST, 8));
+      if (n >= 2 && !S.stride_bad) best = u64min(best, sc_of(M_STRIDE, 16));
+      if (!reduced) best = u64min(best, sc_of(M_XORZ, S.xor_bytes));
+      best = u64min(best, sc_of(M_FOR_BITPACK, sz_for));
+      best = u64min(best, sc_of(M_DELTA_BITPACK, sz_delta));
+      if (c_fm.ok) best = u64min(best, sc_of(M_FLOAT_MULT, c_fm.len));
+      if (c_alp.ok) best = u64min(best, sc_of(M_ALP, c_alp.len));
+      if (sc_of(M_ALP_RD, floor_len) >= best) rd_lbw = 0;
+      __syncthreads();
+    }
     if (rd_lbw) {
       rd_top8(S, v, n, rd_lbw, scr);
       uint32_t rbw = 64 - rd_lbw;
