@@ -2644,7 +2644,8 @@ __device__ void emit_alprd(EncSmem& S, const uint64_t* v, uint32_t n, uint32_t l
   }
 }
 
-__device__ void emit_dict(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* scr, uint8_t* out, const EntRec* er) {
+__device__ void emit_dict(EncSmem& S, const uint64_t* v, uint32_t n, const SubStats* ss, uint8_t* scr, uint8_t* out,
+                          const EntRec* er) {
   DictView dv = dict_prepare(S, v, n, scr, kNoLb);
   uint32_t vtag;
   uint64_t vlen = dict_values_len(S, dv, &vtag);
@@ -2693,7 +2694,17 @@ __device__ void emit_dict(EncSmem& S, const uint64_t* v, uint32_t n, uint8_t* sc
     return;
   }
   if (threadIdx.x == 0) put_u8(out + pos, 0);
-  block_for(S, out + pos + 1, n, false, [&](uint32_t i) { return (uint64_t)dict_rank(S, dv, v[i]); });
+  // The dictionary is sorted, so a sub-block's codes run from the rank of its
+  // smallest value to the rank of its largest (the statistics' unsigned
+  // min / max): the FoR widths and bases without a pass over the codes.
+  uint32_t nsub = (n + kSub - 1) / kSub;
+  for (uint32_t k = threadIdx.x; k < nsub; k += blockDim.x) {
+    uint32_t r0 = dict_rank(S, dv, ss[k].umin), r1 = dict_rank(S, dv, ss[k].umax);
+    S.w_a[k] = (uint8_t)bit_width64((uint64_t)(r1 - r0));
+    S.submin[k] = r0;
+  }
+  __syncthreads();
+  block_for_write(S, out + pos + 1, n, [&](uint32_t i) { return (uint64_t)dict_rank(S, dv, v[i]); });
 }
 
 // The block's run starts from its transitions per sub-block, which the
@@ -2822,7 +2833,7 @@ __global__ void __launch_bounds__(kEncThreads) k_emit(const uint64_t* __restrict
       break;
     case M_ALP: emit_alp(S, v, n, ss ? ss + g0 : nullptr, out); break;
     case M_ALP_RD: emit_alprd(S, v, n, fd.aux, scr, out, erp); break;
-    case M_DICT: emit_dict(S, v, n, scr, out, erp); break;
+    case M_DICT: emit_dict(S, v, n, ss + g0, scr, out, erp); break;
     case M_RLE: emit_rle(S, v, n, ss + g0, scr, out); break;
     default: break;
   }
